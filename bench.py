@@ -1,0 +1,343 @@
+"""Benchmark of the per-tile halo-finding path (run_tile) on B200.
+
+Workload (default): single periodic tile, nmesh = 384^3 Float32, box 768 Mpc/h
+(alatt 2), 2LPT, Eisenstein-Hu no-wiggle P(k) normalised to sigma8 = 0.808
+(Om 0.315, Ob 0.049, OL 0.685, h 0.674, ns 0.965), 20 top-hat filters
+Rf = 1.5 * 20^(i/19) Mpc/h, nbuff = 32, rmax2rs = 0, ioutshear = 1 (33-field
+records), collapse table = the reference's 50 x 20 x 20 make_table output
+(tests/golden/HomelTab_julia.dat), seed 7.  A "step" is one full run_tile of
+that tile: noise, fields, filter bank + peaks, shells, records.
+
+Usage:
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--plain]
+Under torchrun each rank runs independent tiles on its own GPU (run_tile
+does not shard: replicas) with its own seed; the job value is the tiles of
+all ranks over the slowest rank's device time.
+
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "peakpatch.jl_b200"))
+
+N_DEFAULT = 384
+BOX_PER_CELL = 2.0
+FILTERS = [1.5 * 20.0 ** (i / 19.0) for i in range(20)]
+SEED = 7
+METRIC = "tiles/s"
+
+
+def tile_config(n: int):
+    import peakpatch_b200 as pp
+    return pp.PipelineConfig(Omx=0.315 - 0.049, OmB=0.049, Omvac=0.685, h=0.674, n=n, boxsize=BOX_PER_CELL * n,
+                             nbuff=32, z_out=0.0, z_max=0.0, ievol=0, ilpt=2, ioutshear=1, wsmooth=1, rmax2rs=0.0)
+
+
+def workload_name(n: int) -> str:
+    return f"run_tile nmesh={n}^3 box={BOX_PER_CELL * n:g}Mpc/h 2LPT 20 top-hat filters ioutshear=1"
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as td
+            td.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.td = td
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            self.td.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64)
+        self.td.all_reduce(t, op=self.td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.td.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clock sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (a C++/OpenMP restatement of the reference's CPU
+# run_tile) on a bounded sample of the same workload
+# ---------------------------------------------------------------------------
+def cpu_baseline(n: int, budget_s: float = 20.0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from peakpatch_b200 import powerspec
+    oracle.build()
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    k, P = powerspec.eh_table()
+    T = oracle.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat"))
+    cfg = tile_config(n)
+    ocfg = oracle.Config(**{f: getattr(cfg, f) for f in oracle.Config.__dataclass_fields__})
+    filters = [(i + 1, 1.686, R) for i, R in enumerate(FILTERS)]
+    # sample: fields + filter bank + peaks at full size, the shell analysis on
+    # a random subset of the peaks sized to the time budget, extrapolated
+    tm = {}
+    probe = oracle.run_tile_stages(ocfg, SEED, k, P, filters, T, peak_sample=np.arange(0), timings=tm)
+    npk = len(probe["peaks"]["ipp"])
+    rng = np.random.default_rng(0)
+    sub = np.sort(rng.choice(npk, size=min(npk, 200), replace=False)) if npk else np.arange(0)
+    t0 = time.perf_counter()
+    if len(sub):
+        oracle.analyse_peaks(probe["fields"], probe["peaks"]["ipp"][sub], probe["Rf"][sub], probe["ir2min"][sub],
+                             probe["ZZon"][sub], probe["fcrit"], probe["alatt"], probe["shells"], T, nbuff=32)
+    per_peak = (time.perf_counter() - t0) / max(1, len(sub))
+    want = int(min(npk, max(len(sub), budget_s / max(per_peak, 1e-9))))
+    sub2 = np.sort(rng.choice(npk, size=want, replace=False)) if npk else np.arange(0)
+    t0 = time.perf_counter()
+    if len(sub2):
+        oracle.analyse_peaks(probe["fields"], probe["peaks"]["ipp"][sub2], probe["Rf"][sub2], probe["ir2min"][sub2],
+                             probe["ZZon"][sub2], probe["fcrit"], probe["alatt"], probe["shells"], T, nbuff=32)
+    shells_s = (time.perf_counter() - t0) * npk / max(1, len(sub2))
+    tile_s = tm["fields_s"] + tm["peaks_s"] + shells_s
+    return {"value": 1.0 / tile_s, "unit": METRIC, "cores": cores, "kind": "port",
+            "sample": (f"{workload_name(n)}: fields + 20-filter peak finding at full size "
+                       f"({tm['fields_s'] + tm['peaks_s']:.1f} s), shell analysis on {len(sub2)} of {npk} peaks "
+                       f"extrapolated ({shells_s:.1f} s); oracle C++/OpenMP + threaded pocketfft"),
+            "stages_s": {"fields": tm["fields_s"], "peaks": tm["peaks_s"], "shells_extrapolated": shells_s},
+            "npeaks": npk}
+
+
+def run_reference(args, dist: Dist):
+    if dist.rank != 0:
+        return
+    n = args.n
+    vals = []
+    for _ in range(args.warmup):
+        pass   # the oracle has no warm-up state beyond its first build
+    res = None
+    for _ in range(args.steps):
+        res = cpu_baseline(n, budget_s=args.cpu_budget)
+        vals.append(res["value"])
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 shell sums", "data": "synthetic",
+            "config": {"workload": workload_name(n), "nmesh": n, "filters": 20, "seed": SEED},
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+def run_ours(args, dist: Dist):
+    import peakpatch_b200 as pp
+    from peakpatch_b200 import powerspec
+    n = args.n
+    gpu = dist.local
+    ctx = pp.Context(gpu)
+    k, P = powerspec.eh_table()
+    T = pp.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat"))
+    ctx.set_pk_table(k, P)
+    ctx.set_collapse_table(T)
+    cfg = tile_config(n)
+    seed0 = SEED + 1000 * dist.rank
+    cap = 4_000_000
+    dev_out = ctx.alloc_device(cap * 33 * 4)
+    host_out = ctx.alloc_host(cap * 33 * 4)
+    for w in range(args.warmup):
+        ctx.run_tile_into(cfg, seed0, FILTERS, dev_out, cap, plain=args.plain)
+    # ---- device-resident throughput (value) ----
+    dist.barrier()
+    ctx.synchronize()
+    clocks = ClockSampler(gpu)
+    clocks.start()
+    l0 = ctx.launch_count()
+    ctx.event_record(0)
+    shell_ms, shell_visits, npk_tot, nh_tot, stage = 0.0, 0, 0, 0, None
+    for s in range(args.steps):
+        cnt, rmax, npk, dms = ctx.run_tile_into(cfg, seed0, FILTERS, dev_out, cap, plain=args.plain)
+        st = ctx.shell_stats()
+        shell_ms += st["ms"]
+        shell_visits += st["visits"]
+        npk_tot += npk
+        nh_tot += cnt
+        stage = ctx.stage_ms()
+    ctx.event_record(1)
+    ctx.synchronize()
+    launches = ctx.launch_count() - l0
+    dev_ms = ctx.event_elapsed(0, 1)
+    clk = clocks.stop()
+    # ---- end to end through the public API with host output (e2e) ----
+    dist.barrier()
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    ctx.event_record(2)
+    h2d = d2h = 0
+    for s in range(args.steps):
+        cnt, rmax, npk, dms = ctx.run_tile_into(cfg, seed0, FILTERS, host_out, cap, plain=args.plain)
+        d2h += cnt * 33 * 4 + 64
+        h2d += len(FILTERS) * 8 + 4 * len(FILTERS)
+    ctx.event_record(3)
+    ctx.synchronize()
+    e2e_ms = ctx.event_elapsed(2, 3)
+    wall_e2e = time.perf_counter() - t0
+    dist.barrier()
+    dev_ms_max = dist.max(dev_ms)
+    e2e_ms_max = dist.max(max(e2e_ms, wall_e2e * 1000.0))
+    tiles = dist.sum(float(args.steps))
+    value = tiles / (dev_ms_max / 1000.0)
+    e2e = tiles / (e2e_ms_max / 1000.0)
+    # roofline of the dominant own kernel (the shell kernel): algorithmic
+    # bytes = in-bounds cell visits x 32 B gather record + 248 B result per peak
+    bytes_alg = shell_visits * 32 + npk_tot * 31 * 8
+    achieved = bytes_alg / (shell_ms / 1000.0) / 1e9 if shell_ms > 0 else 0.0
+    peaks = _measured_peaks()
+    line = None
+    if dist.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, compensated-f32 shell sums, f64 collapse walk",
+            "data": "synthetic (seeded Threefry noise, EH P(k))",
+            "config": {"workload": workload_name(n), "nmesh": n, "boxsize": BOX_PER_CELL * n, "filters": 20,
+                       "nbuff": 32, "ilpt": 2, "ioutshear": 1, "seed": SEED, "path": "plain" if args.plain else "optimised",
+                       "l2": "inputs larger than L2 (each field 226 MB at 384^3)", "parallelism": f"replicas x{dist.world}"},
+            "peaks_per_s": npk_tot / (dev_ms / 1000.0), "halos_per_tile": nh_tot / args.steps,
+            "peaks_per_tile": npk_tot / args.steps,
+            "stage_ms_last_step": stage,
+            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d // args.steps,
+                    "d2h_bytes_per_step": d2h // args.steps},
+            "gpu_launches": int(launches),
+            "roofline": {"kernel": "shell_kernel (gather + collapse walk)", "bound": "hbm",
+                         "achieved": achieved, "peak": peaks[0], "unit": "GB/s",
+                         "frac": achieved / peaks[0] if peaks[0] else None, "traffic": None,
+                         "peak_source": peaks[1],
+                         "alg_bytes_per_launch": bytes_alg / max(1, args.steps),
+                         "kernel_ms_per_launch": shell_ms / max(1, args.steps)},
+            "clocks": clk,
+        }
+    ctx.free_device(dev_out)
+    ctx.free_host(host_out)
+    ctx.close()
+    return line
+
+
+def _measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--plain", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist)
+            return
+        line = run_ours(args, dist)
+        if dist.rank == 0 and line is not None:
+            if dist.world == 1 and not args.no_cpu_baseline:
+                cb = cpu_baseline(args.n, budget_s=args.cpu_budget)
+                line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

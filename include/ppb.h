@@ -1,0 +1,190 @@
+/*
+ * ppb.h — C ABI of libppb, a B200 (sm_100a) implementation of PeakPatch.jl's
+ * per-tile halo-finding path.
+ *
+ * Every entry point returns an int32 status (PPB_OK or a negative PPB_ERR_*
+ * code); no C++ exception crosses this boundary.  On failure the context
+ * keeps a message retrievable with ppb_last_error().
+ *
+ * Conventions shared with the reference (PeakPatch.jl):
+ *  - 3-D fields are n1 x n2 x n3 Float32 arrays in column-major order
+ *    (i fastest), exactly as Julia stores Array{Float32,3}.
+ *  - Peak indices i, j, k and the flat index ipp are 1-based
+ *    (ipp = i + (j-1) n1 + (k-1) n1 n2), as in PeakFind.PeakCandidate.
+ *  - "No collapse" is RTHL = -1 and zvir_half = -1 (RadialShell.no_collapse).
+ *  - Pointers may be host or device memory: the library asks the CUDA driver
+ *    which one it was given and copies host data in and out itself.  The
+ *    caller keeps ownership of every buffer it passes.
+ *
+ * Reference interfaces each entry point replaces are cited per function
+ * (paths inside the PeakPatch.jl repository).
+ */
+#ifndef PPB_H
+#define PPB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PPB_ABI_VERSION 1
+
+enum {
+  PPB_OK = 0,
+  PPB_ERR_INVALID = -1,      /* bad argument (null pointer, size out of range, ...) */
+  PPB_ERR_CUDA = -2,         /* a CUDA runtime / cuFFT call failed */
+  PPB_ERR_NOMEM = -3,        /* device allocation failed */
+  PPB_ERR_ADMISSION = -4,    /* request larger than the context's HBM budget */
+  PPB_ERR_TIMEOUT = -5,      /* a bounded wait ran out */
+  PPB_ERR_UNSUPPORTED = -6,  /* option not implemented on this path */
+  PPB_ERR_CAPACITY = -7,     /* caller buffer too small; required size reported */
+  PPB_ERR_NOT_FOUND = -8     /* unknown ticket */
+};
+
+typedef struct ppb_ctx ppb_ctx;
+
+/* Tile parameters: the fields of PipelineConfig used by run_tile
+ * (src/IO/Parameters.jl:17-46) plus the seed of run_tile(cfg; seed).
+ * Omx is the CDM-only density; the total matter density is Omx + OmB. */
+typedef struct ppb_tile_params {
+  double Omx, OmB, Omvac, h;
+  int32_t n;
+  double boxsize;
+  int32_t nbuff;
+  double z_out, z_max;
+  int32_t ievol;
+  double cenx, ceny, cenz;
+  int32_t ilpt;
+  int32_t ioutshear;
+  int32_t wsmooth;
+  double rmax2rs;
+  uint64_t seed;
+  /* path selection: 0 = optimised path (adaptive shell truncation,
+   * compensated FP32 shell sums, persistent launches), 1 = plain path
+   * (full spheres, FP64 shell sums, one block per peak) */
+  int32_t plain;
+  int32_t reserved[7];
+} ppb_tile_params;
+
+/* Halo output: caller-allocated record buffer.  On PPB_ERR_CAPACITY `count`
+ * holds the number of records needed. */
+typedef struct ppb_halo_buf {
+  float* records;       /* capacity x nfields floats (host or device) */
+  int64_t capacity;     /* in records */
+  int64_t count;        /* out: records written */
+  int32_t nfields;      /* out: 11 (ioutshear == 0) or 33 */
+  float RTHLmax;        /* out: max RTHL (Mpc/h), 0 when empty (Pipeline.jl:314-318) */
+  int64_t npeaks;       /* out: peak candidates found over the filter bank */
+} ppb_halo_buf;
+
+typedef struct ppb_stats {
+  int64_t tiles_done;
+  int64_t peaks_done;
+  int64_t halos_done;
+  double p50_ms, p99_ms;      /* request latency, arrival -> result */
+  double tiles_per_s;
+  uint64_t hbm_in_use;        /* bytes held by the context */
+  uint64_t hbm_budget;
+  int32_t in_flight;
+  int32_t queued;
+} ppb_stats;
+
+/* ---- context ------------------------------------------------------------ */
+/* One context per GPU (set_cuda_device!, ext/CUDAExt.jl:3322-3325).
+ * hbm_budget = 0 means 90% of the free device memory at creation. */
+int32_t ppb_ctx_create(int32_t device, uint64_t hbm_budget, ppb_ctx** out);
+int32_t ppb_ctx_destroy(ppb_ctx* ctx);
+int32_t ppb_last_error(ppb_ctx* ctx, char* buf, size_t len);
+int32_t ppb_abi_version(void);
+
+/* ---- resident tables ---------------------------------------------------- */
+/* Collapse table zvir(log10 F, e, p/e) = 1 + z_vir, Nx x Ny x Nz Float32
+ * column-major, grid range(X1, X2, length=Nx) etc.; outside -> -1.
+ * Replaces read_homeltab + CollapseTableInterp
+ * (src/EllipsoidalCollapse/CollapseTable.jl:102-145). */
+int32_t ppb_set_collapse_table(ppb_ctx* ctx, const float* tab, int32_t nx, int32_t ny, int32_t nz,
+                               double x1, double x2, double y1, double y2, double z1, double z2);
+/* P(k) table (k in h/Mpc, P in the reference's file convention) for the
+ * log-log interpolant of load_pk (src/InitialConditions/PowerSpectrum.jl:189-201). */
+int32_t ppb_set_pk_table(ppb_ctx* ctx, const double* k, const double* pk, int32_t n);
+
+/* ---- the drop-in for run_tile ------------------------------------------ */
+/* Pipeline.run_tile(cfg; seed) (src/Pipeline.jl:66-325): noise -> sqrt(P)
+ * convolution -> 1LPT/2LPT -> filter bank + peak finding -> radial-shell
+ * collapse -> 11/33-field records, in peak order.  Rf holds the filter radii
+ * (Mpc/h, any order; sorted descending inside as Pipeline.jl:82 does).
+ * Writing the .pksc file is left to the caller (ppb_write_pksc). */
+int32_t ppb_run_tile(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, int32_t nfilt,
+                     ppb_halo_buf* out);
+
+/* Same as ppb_run_tile but the timing of the device work is returned in
+ * *device_ms (CUDA events on the context stream). */
+int32_t ppb_run_tile_timed(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, int32_t nfilt,
+                           ppb_halo_buf* out, float* device_ms);
+
+/* write_pksc (src/IO/Catalog.jl:53-94): Int32 N, Float32 RTHLmax, Float32 z_out,
+ * then N x nfields Float32 (little endian). */
+int32_t ppb_write_pksc(const char* path, const float* records, int64_t n, int32_t nfields,
+                       float RTHLmax, float z_out);
+
+/* ---- stub-level entry points ------------------------------------------- */
+/* fill_noise_threefry! (src/InitialConditions/RandomField.jl:70-83):
+ * Gaussian white noise, n^3 Float32, column-major. */
+int32_t ppb_noise_threefry(ppb_ctx* ctx, float* out, int32_t n, uint64_t seed);
+
+/* find_peaks (src/HaloFinder/PeakFind.jl:123-186) on one field; mask (Int8,
+ * n^3) is read and updated.  Peaks are returned in the reference's scan order
+ * (k, then j, then i).  Outputs (capacity max_peaks): 1-based i, j, k, ipp
+ * (int64) and delta (Float32); *npeaks receives the count. */
+int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n1, int32_t n2,
+                       int32_t n3, int32_t nbuff, float fcrit, int64_t max_peaks, int64_t* pi,
+                       int64_t* pj, int64_t* pk, int64_t* ipp, float* pdelta, int64_t* npeaks);
+
+/* analyse_peak over a batch of peaks (src/HaloFinder/RadialShell.jl:282-891;
+ * GPU stub analyse_peaks_gpu_cuda_multirf, src/PeakPatch.jl:231-253).
+ * Fields are n^3 Float32 column-major (cubic grid); eta2* and lapd may be
+ * NULL.  Per peak: 1-based flat index ipp, Rf (Mpc/h), ir2min, ZZon = 1+z and
+ * fcrit.  nhunt is the shell radius (precompute_shells(nhunt)).  Output:
+ * npk x 31 doubles per peak:
+ *   0 RTHL, 1 Srb, 2-4 Sbar, 5-7 Sbar2, 8-16 strain (column-major 3x3),
+ *   17-19 gradpk, 20-22 gradpkrf, 23 Fbarx, 24 e_v, 25 p_v, 26 zvir_half,
+ *   27-29 gradpkf, 30 d2F.
+ * rmax2rs > 0 is rejected with PPB_ERR_UNSUPPORTED (the reference's result
+ * then depends on thread scheduling). */
+int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, const float* etay,
+                          const float* etaz, const float* eta2x, const float* eta2y,
+                          const float* eta2z, const float* lapd, int32_t n, int32_t nhunt,
+                          int64_t npk, const int64_t* ipp, const double* Rf, const int64_t* ir2min,
+                          const double* ZZon, const double* fcrit, double alatt, int32_t plain,
+                          double* out);
+
+/* ---- memory helpers ----------------------------------------------------- */
+/* Page-locked host memory (fast, asynchronous copies of records) and device
+ * memory on the context's GPU, for callers that have no CUDA runtime of
+ * their own (a Julia or Python host).  Free with the matching call. */
+int32_t ppb_alloc_host(ppb_ctx* ctx, size_t bytes, void** out);
+int32_t ppb_free_host(ppb_ctx* ctx, void* p);
+int32_t ppb_alloc_device(ppb_ctx* ctx, size_t bytes, void** out);
+int32_t ppb_free_device(ppb_ctx* ctx, void* p);
+
+/* ---- timing helpers ----------------------------------------------------- */
+/* Named CUDA events on the context stream (slot 0..15). */
+int32_t ppb_event_record(ppb_ctx* ctx, int32_t slot);
+int32_t ppb_event_elapsed(ppb_ctx* ctx, int32_t a, int32_t b, float* ms);
+int32_t ppb_synchronize(ppb_ctx* ctx);
+/* Count of kernel launches issued by this library since context creation. */
+int32_t ppb_launch_count(ppb_ctx* ctx, int64_t* count);
+/* Shell-kernel statistics of the last run: in-bounds cell visits, the five
+ * dump-reason counters of src/HaloFinder/RadialShell.jl:15-34 (premask,
+ * no_fcrit, m0_one, no_collapse, rthl_neg) and the kernel's device time. */
+int32_t ppb_last_shell_stats(ppb_ctx* ctx, int64_t* visits, int64_t* dumps5, float* ms);
+/* Per-stage device times (ms) of the last ppb_run_tile_timed call:
+ * [0] fields, [1] filter bank + peaks, [2] shell analysis, [3] records. */
+int32_t ppb_last_stage_ms(ppb_ctx* ctx, float* ms4);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PPB_H */

@@ -1,0 +1,463 @@
+"""CPU oracle for PeakPatch.jl's per-tile halo-finding path (run_tile).
+
+TEST INFRASTRUCTURE ONLY: the parity tests, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` use this module as the checker.  The product
+(``peakpatch.jl_b200``) never imports it.
+
+The arithmetic lives in ``oracle.cpp`` (a double-precision C++ restatement of
+the reference's Julia code, built by ``oracle/Makefile`` into
+``oracle/_build/libppb_oracle.so``); this module drives it and supplies the
+FFTs.  The reference uses FFTW in single precision; here every transform is
+done in double precision (scipy.fft / pocketfft, threaded) and rounded to
+single precision where the reference holds a Float32 array, so the oracle's
+fields are the correctly rounded values of the same transforms.
+
+Reference files restated (PeakPatch.jl):
+  src/Pipeline.jl:66-325            run_tile
+  src/InitialConditions/*.jl        noise, P(k), 1LPT/2LPT
+  src/HaloFinder/*.jl               filters, peak finding, radial shells
+  src/EllipsoidalCollapse/CollapseTable.jl:85-145   HomelTab I/O, lookup
+  src/Cosmology/Cosmology.jl        growth tables, chi(z)
+  src/IO/Catalog.jl:53-160          .pksc
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import struct
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libppb_oracle.so")
+_lib = None
+
+R_N = 31  # doubles per analyse_peak result (layout documented in oracle.cpp)
+
+
+def build() -> str:
+    """Compile the oracle library with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+P = ctypes.c_void_p
+I64 = ctypes.c_int64
+D = ctypes.c_double
+
+
+def _declare(L):
+    L.ora_num_threads.restype = ctypes.c_int
+    L.ora_set_threads.argtypes = [ctypes.c_int]
+    L.ora_noise.argtypes = [P, I64, ctypes.c_uint64]
+    L.ora_noise_libm.argtypes = [P, I64, ctypes.c_uint64]
+    L.ora_noise_region.argtypes = [P, I64, ctypes.c_uint64, I64, I64, I64, I64, I64, I64]
+    L.ora_pk.argtypes = [P, P, ctypes.c_int, D]
+    L.ora_pk.restype = D
+    L.ora_convolve.argtypes = [P, I64, D, P, P, ctypes.c_int]
+    for f in ("ora_lpt1", "ora_phi", "ora_lpt2", "ora_lapd_k"):
+        getattr(L, f).argtypes = [P, P, I64, D]
+    L.ora_src2.argtypes = [P, P, I64]
+    L.ora_window.argtypes = [D, D, ctypes.c_int]
+    L.ora_window.restype = D
+    L.ora_smooth_k.argtypes = [P, P, I64, D, D, ctypes.c_int]
+    L.ora_find_peaks.argtypes = [P, P, I64, I64, I64, D, D, D, D, I64, ctypes.c_float, I64,
+                                 P, P, P, P, P, P, P, P]
+    L.ora_find_peaks.restype = I64
+    L.ora_hRinteg.argtypes = [D, D]
+    L.ora_hRinteg.restype = D
+    L.ora_atab4.argtypes = [P]
+    L.ora_shells.argtypes = [ctypes.c_int, P]
+    L.ora_shells.restype = I64
+    L.ora_eig3.argtypes = [P, P]
+    L.ora_table_interp.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D, D, D, D, D, D, D, D]
+    L.ora_table_interp.restype = D
+    L.ora_dlinear.argtypes = [D, D, D, D, P, ctypes.c_int, P]
+    L.ora_fsc_of_z.argtypes = [D, D, D, D, D]
+    L.ora_fsc_of_z.restype = D
+    L.ora_chi.argtypes = [D, D, D, D]
+    L.ora_chi.restype = D
+    L.ora_chi2z.argtypes = [D, D, D, D, P, ctypes.c_int, P]
+    L.ora_analyse_peaks.argtypes = [P] * 9 + [I64, I64, I64, P, I64, P, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, D, D, D, D, D, D, I64, P, P, P, P, P, D,
+                                              I64, D, ctypes.c_int, P]
+    L.ora_dump_counts.argtypes = [P]
+    L.ora_pack_records.argtypes = [D, D, D, D, I64, P, P, P, P, P, P, P, D, ctypes.c_int, D, D, D, D,
+                                   D, ctypes.c_int, ctypes.c_int, P, P]
+    L.ora_pack_records.restype = I64
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def set_threads(n: int) -> None:
+    lib().ora_set_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(lib().ora_num_threads())
+
+
+# --------------------------------------------------------------------------
+# File formats (reference readers restated)
+# --------------------------------------------------------------------------
+def read_pk(path: str):
+    """2-column ASCII (k, P); '#' comments.  PowerSpectrum.jl:189-192."""
+    d = np.loadtxt(path, comments="#")
+    return np.ascontiguousarray(d[:, 0], dtype=np.float64), np.ascontiguousarray(d[:, 1], dtype=np.float64)
+
+
+def read_filterbank(path: str):
+    """Line 1: count; then 'id fcrit Rf'.  Filters.jl:46-58."""
+    with open(path) as f:
+        lines = f.read().splitlines()
+    nic = int(lines[0].strip())
+    out = []
+    for i in range(nic):
+        p = lines[i + 1].split()
+        out.append((int(p[0]), float(p[1]), float(p[2])))
+    return out
+
+
+@dataclass
+class Table:
+    data: np.ndarray  # float32, shape (nz, ny, nx) C-order == column-major (nx, ny, nz)
+    nx: int
+    ny: int
+    nz: int
+    x1: float
+    x2: float
+    y1: float
+    y2: float
+    z1: float
+    z2: float
+
+
+def read_homeltab(path: str) -> Table:
+    """3 x Int32 + 6 x Float32 header, then Float32 column-major data.
+    CollapseTable.jl:102-122."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    nx, ny, nz = struct.unpack("<3i", raw[:12])
+    x1, x2, y1, y2, z1, z2 = (float(v) for v in struct.unpack("<6f", raw[12:36]))
+    data = np.frombuffer(raw[36:36 + 4 * nx * ny * nz], dtype="<f4").reshape(nz, ny, nx).copy()
+    return Table(data, nx, ny, nz, x1, x2, y1, y2, z1, z2)
+
+
+def write_pksc(path: str, rec: np.ndarray, RTHLmax: float, z_out: float) -> None:
+    """Int32 N, Float32 RTHLmax, Float32 z_out, then N x (11|33) Float32.
+    Catalog.jl:53-94."""
+    rec = np.ascontiguousarray(rec, dtype="<f4")
+    with open(path, "wb") as f:
+        f.write(struct.pack("<i", rec.shape[0]))
+        f.write(struct.pack("<f", RTHLmax))
+        f.write(struct.pack("<f", z_out))
+        f.write(rec.tobytes())
+
+
+# --------------------------------------------------------------------------
+# FFTs (double precision, rounded to single where the reference stores F32)
+# --------------------------------------------------------------------------
+def _fft_workers() -> int:
+    return max(1, num_threads())
+
+
+def rfft3(x: np.ndarray) -> np.ndarray:
+    import scipy.fft as sf
+    return sf.rfftn(x.astype(np.float64), workers=_fft_workers()).astype(np.complex64)
+
+
+def irfft3(c: np.ndarray, n: int) -> np.ndarray:
+    import scipy.fft as sf
+    return sf.irfftn(c.astype(np.complex128), s=(n, n, n), workers=_fft_workers()).astype(np.float32)
+
+
+# --------------------------------------------------------------------------
+# Step functions (arrays are C-order [k][j][i] == Julia column-major [i,j,k])
+# --------------------------------------------------------------------------
+def noise(n: int, seed: int) -> np.ndarray:
+    out = np.empty((n, n, n), dtype=np.float32)
+    lib().ora_noise(_p(out), n, ctypes.c_uint64(seed))
+    return out
+
+
+def noise_libm(n: int, seed: int) -> np.ndarray:
+    """Noise with the platform libm in the Box-Muller step (cross-check)."""
+    out = np.empty((n, n, n), dtype=np.float32)
+    lib().ora_noise_libm(_p(out), n, ctypes.c_uint64(seed))
+    return out
+
+
+def noise_region(n, seed, irange, jrange, krange) -> np.ndarray:
+    """Sub-region with 0-based half-open ranges (RandomField.jl:95-109)."""
+    (i0, i1), (j0, j1), (k0, k1) = irange, jrange, krange
+    out = np.empty((k1 - k0, j1 - j0, i1 - i0), dtype=np.float32)
+    lib().ora_noise_region(_p(out), n, ctypes.c_uint64(seed), i0, i1 - i0, j0, j1 - j0, k0, k1 - k0)
+    return out
+
+
+def convolve(noise_arr: np.ndarray, pk_k, pk_p, boxsize: float) -> np.ndarray:
+    n = noise_arr.shape[0]
+    nk = rfft3(noise_arr)
+    lib().ora_convolve(_p(nk), n, boxsize, _p(pk_k), _p(pk_p), len(pk_k))
+    return irfft3(nk, n)
+
+
+def generate_grf(n, pk_k, pk_p, boxsize, seed) -> np.ndarray:
+    """RandomField.jl:123-128."""
+    return convolve(noise(n, seed), pk_k, pk_p, boxsize)
+
+
+def lpt1(delta_k, n, boxsize):
+    out = np.empty((3,) + delta_k.shape, dtype=np.complex64)
+    lib().ora_lpt1(_p(delta_k), _p(out), n, boxsize)
+    return [irfft3(out[c], n) for c in range(3)]
+
+
+def lpt2(delta_k, n, boxsize):
+    phik = np.empty((6,) + delta_k.shape, dtype=np.complex64)
+    lib().ora_phi(_p(delta_k), _p(phik), n, boxsize)
+    phi = np.stack([irfft3(phik[c], n) for c in range(6)])
+    src2 = np.empty((n, n, n), dtype=np.float32)
+    lib().ora_src2(_p(phi), _p(src2), n ** 3)
+    s2k = rfft3(src2)
+    out = np.empty((3,) + delta_k.shape, dtype=np.complex64)
+    lib().ora_lpt2(_p(s2k), _p(out), n, boxsize)
+    return [irfft3(out[c], n) for c in range(3)]
+
+
+def laplacian(delta_k, n, boxsize):
+    """Pipeline.jl:35-51: irfft(k^2 delta_k) / n^3 (Float32 division)."""
+    lk = np.empty_like(delta_k)
+    lib().ora_lapd_k(_p(delta_k), _p(lk), n, boxsize)
+    return (irfft3(lk, n) / np.float32(float(n) ** 3)).astype(np.float32)
+
+
+def smooth_field(delta_k, n, boxsize, Rf, wsmooth):
+    out = np.empty_like(delta_k)
+    lib().ora_smooth_k(_p(delta_k), _p(out), n, boxsize, Rf, wsmooth)
+    return irfft3(out, n)
+
+
+def window(kR: float, k: float, wsmooth: int) -> float:
+    return float(lib().ora_window(kR, k, wsmooth))
+
+
+def find_peaks(delta, mask, xbx, ybx, zbx, alatt, nbuff, fcrit, max_peaks=2000000):
+    """PeakFind.jl:123-186.  delta: C-order (n3,n2,n1) float32; mask int8
+    (mutated).  Returns dict of arrays; i, j, k, ipp are 1-based."""
+    n3, n2, n1 = delta.shape
+    cap = int(min(max_peaks, delta.size))
+    cap = max(cap, 1)
+    bufs = {k: np.empty(cap, dtype=np.int64) for k in ("i", "j", "k", "ipp")}
+    bufs.update({k: np.empty(cap, dtype=np.float64) for k in ("x", "y", "z")})
+    bufs["delta"] = np.empty(cap, dtype=np.float32)
+    npk = lib().ora_find_peaks(_p(delta), _p(mask), n1, n2, n3, xbx, ybx, zbx, alatt, nbuff,
+                               ctypes.c_float(fcrit), max_peaks, _p(bufs["i"]), _p(bufs["j"]),
+                               _p(bufs["k"]), _p(bufs["ipp"]), _p(bufs["x"]), _p(bufs["y"]),
+                               _p(bufs["z"]), _p(bufs["delta"]))
+    return {k: v[:npk].copy() for k, v in bufs.items()}
+
+
+def hRinteg(u0, u12):
+    return float(lib().ora_hRinteg(u0, u12))
+
+
+def atab4():
+    a = np.empty(1101, dtype=np.float64)
+    lib().ora_atab4(_p(a))
+    return a
+
+
+def precompute_shells(rmax: int) -> np.ndarray:
+    n = lib().ora_shells(rmax, None)
+    out = np.empty((n, 4), dtype=np.int32)
+    lib().ora_shells(rmax, _p(out))
+    return out
+
+
+def eigvals_sym(m) -> np.ndarray:
+    a = np.ascontiguousarray(m, dtype=np.float64)
+    lam = np.empty(3, dtype=np.float64)
+    lib().ora_eig3(_p(a), _p(lam))
+    return lam
+
+
+def table_interp(T: Table, x, y, z) -> float:
+    return float(lib().ora_table_interp(_p(T.data), T.nx, T.ny, T.nz, T.x1, T.x2, T.y1, T.y2, T.z1,
+                                        T.z2, x, y, z))
+
+
+def dlinear(Om, OB, OL, h, a) -> np.ndarray:
+    a = np.ascontiguousarray(np.atleast_1d(a), dtype=np.float64)
+    out = np.empty_like(a)
+    lib().ora_dlinear(Om, OB, OL, h, _p(a), len(a), _p(out))
+    return out
+
+
+def fsc_of_z(Om, OB, OL, h, z) -> float:
+    return float(lib().ora_fsc_of_z(Om, OB, OL, h, z))
+
+
+def chi(Om, OL, h, z) -> float:
+    return float(lib().ora_chi(Om, OL, h, z))
+
+
+def chi_to_z(Om, OL, h, zmax, chis) -> np.ndarray:
+    c = np.ascontiguousarray(np.atleast_1d(chis), dtype=np.float64)
+    out = np.empty_like(c)
+    lib().ora_chi2z(Om, OL, h, zmax, _p(c), len(c), _p(out))
+    return out
+
+
+def analyse_peaks(fields, ipp, Rf, ir2min, ZZon, fcrit, alatt, shells, T: Table, nbuff=0,
+                  rmax2rs=0.0, mask=None, serial_mask=False) -> np.ndarray:
+    """RadialShell.jl:282-891 for a batch of peaks.  fields: dict with delta,
+    etax, etay, etaz and optional eta2x/eta2y/eta2z/lapd (C-order float32).
+    Returns (npk, 31) float64 results."""
+    d = fields["delta"]
+    n3, n2, n1 = d.shape
+    npk = len(ipp)
+    arr = lambda a, t: np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=t), (npk,)))
+    ipp_a, Rf_a, ir_a, Z_a, fc_a = arr(ipp, np.int64), arr(Rf, np.float64), arr(ir2min, np.int64), \
+        arr(ZZon, np.float64), arr(fcrit, np.float64)
+    out = np.empty((npk, R_N), dtype=np.float64)
+    g = lambda k: fields.get(k)
+    sh = np.ascontiguousarray(shells, dtype=np.int32)
+    lib().ora_analyse_peaks(_p(d), _p(g("etax")), _p(g("etay")), _p(g("etaz")), _p(g("eta2x")),
+                            _p(g("eta2y")), _p(g("eta2z")), _p(g("lapd")), _p(mask), n1, n2, n3,
+                            _p(sh), sh.shape[0], _p(T.data), T.nx, T.ny, T.nz, T.x1, T.x2, T.y1, T.y2,
+                            T.z1, T.z2, npk, _p(ipp_a), _p(Rf_a), _p(ir_a), _p(Z_a), _p(fc_a), alatt,
+                            nbuff, rmax2rs, int(bool(serial_mask)), _p(out))
+    return out
+
+
+def dump_counts():
+    a = np.zeros(5, dtype=np.int64)
+    lib().ora_dump_counts(_p(a))
+    return dict(zip(("premask", "no_fcrit", "m0_one", "no_collapse", "rthl_neg"), a.tolist()))
+
+
+# --------------------------------------------------------------------------
+# run_tile (Pipeline.jl:66-325)
+# --------------------------------------------------------------------------
+@dataclass
+class Config:
+    """PipelineConfig fields used on the path (src/IO/Parameters.jl:17-46)."""
+    Omx: float = 0.266
+    OmB: float = 0.049
+    Omvac: float = 0.685
+    h: float = 0.674
+    n: int = 142
+    boxsize: float = 200.0
+    nbuff: int = 4
+    z_out: float = 0.0
+    z_max: float = 0.0
+    ievol: int = 0
+    cenx: float = 0.0
+    ceny: float = 0.0
+    cenz: float = 0.0
+    ilpt: int = 2
+    ioutshear: int = 0
+    wsmooth: int = 0
+    rmax2rs: float = 1.0
+
+
+def run_tile_stages(cfg: Config, seed: int, pk_k, pk_p, filters, T: Table, peak_sample=None,
+                    timings: dict | None = None):
+    """Runs run_tile and returns all intermediate products (fields, peaks,
+    per-peak results, records).  `peak_sample` (optional index array) limits
+    the shell analysis to a subset of peaks (CPU-baseline sampling)."""
+    import time
+    tm = timings if timings is not None else {}
+    t0 = time.perf_counter()
+    Om = cfg.Omx + cfg.OmB
+    filters = sorted(filters, key=lambda f: -f[2])
+    n, box = cfg.n, cfg.boxsize
+    alatt = box / n
+    fcrit_val = fsc_of_z(Om, cfg.OmB, cfg.Omvac, cfg.h, cfg.z_out)
+    Rfmax = filters[0][2]
+    nhunt = min(cfg.nbuff - 1, int(np.floor(Rfmax * 1.75 / alatt)))
+    shells = precompute_shells(nhunt)
+    delta = generate_grf(n, pk_k, pk_p, box, seed)
+    fcrit = np.float32(fcrit_val)
+    delta_k = rfft3(delta)
+    psi = lpt1(delta_k, n, box)
+    psi2 = lpt2(delta_k, n, box) if cfg.ilpt >= 2 else [None, None, None]
+    t1 = time.perf_counter()
+    tm["fields_s"] = t1 - t0
+    mask = np.zeros((n, n, n), dtype=np.int8)
+    peaks = {k: [] for k in ("i", "j", "k", "ipp", "x", "y", "z", "delta")}
+    pRf, pFc, pd2 = [], [], []
+    for (_, _, Rf) in filters:
+        ds = smooth_field(delta_k, n, box, Rf, cfg.wsmooth)
+        ls = smooth_field(delta_k, n, box, Rf, 3) if cfg.ioutshear >= 1 else None
+        pk = find_peaks(ds, mask, 0.0, 0.0, 0.0, alatt, cfg.nbuff, fcrit)
+        for k in peaks:
+            peaks[k].append(pk[k])
+        npk = len(pk["ipp"])
+        pRf.append(np.full(npk, Rf))
+        lin = pk["ipp"] - 1
+        pFc.append(ds.reshape(-1)[lin])
+        pd2.append(ls.reshape(-1)[lin] if ls is not None else np.zeros(npk, np.float32))
+    peaks = {k: np.concatenate(v) for k, v in peaks.items()}
+    pRf, pFc, pd2 = np.concatenate(pRf), np.concatenate(pFc).astype(np.float32), \
+        np.concatenate(pd2).astype(np.float32)
+    t2 = time.perf_counter()
+    tm["peaks_s"] = t2 - t1
+    mask[:] = 0
+    lapd = laplacian(delta_k, n, box) if cfg.ioutshear >= 1 else None
+    fields = dict(delta=delta, etax=psi[0], etay=psi[1], etaz=psi[2], eta2x=psi2[0], eta2y=psi2[1],
+                  eta2z=psi2[2], lapd=lapd)
+    npk = len(peaks["ipp"])
+    ir2min = np.minimum(np.floor((1.75 * pRf / alatt) ** 2), np.floor((40.0 / alatt - 1) ** 2)).astype(np.int64)
+    # per-peak ZZon
+    if cfg.ievol == 1:
+        dx = peaks["x"] - cfg.cenx
+        dy = peaks["y"] - cfg.ceny
+        dz = peaks["z"] - cfg.cenz
+        zpk = chi_to_z(Om, cfg.Omvac, cfg.h, cfg.z_max + 1.0, np.sqrt(dx * dx + dy * dy + dz * dz))
+        ZZon = 1.0 + zpk
+        fc_pp = np.array([fsc_of_z(Om, cfg.OmB, cfg.Omvac, cfg.h, z - 1.0) for z in ZZon])
+    else:
+        ZZon = np.full(npk, 1.0 + cfg.z_out)
+        fc_pp = np.full(npk, fcrit_val)
+    # analyse_peak computes fcrit from ZZon via fsc_of_z (growth tables given)
+    sel = np.arange(npk) if peak_sample is None else np.asarray(peak_sample)
+    res = np.zeros((npk, R_N))
+    res[:, 0] = -1.0
+    res[sel] = analyse_peaks(fields, peaks["ipp"][sel], pRf[sel], ir2min[sel], ZZon[sel], fc_pp[sel],
+                             alatt, shells, T, nbuff=cfg.nbuff, rmax2rs=cfg.rmax2rs, mask=mask)
+    t3 = time.perf_counter()
+    tm["shells_s"] = t3 - t2
+    tm["n_analysed"] = int(len(sel))
+    nf = 33 if cfg.ioutshear >= 1 else 11
+    rec = np.empty((max(npk, 1), nf), dtype=np.float32)
+    zz = np.empty(max(npk, 1))
+    L = lib()
+    nh = L.ora_pack_records(Om, cfg.OmB, cfg.Omvac, cfg.h, npk, _p(peaks["x"]), _p(peaks["y"]),
+                            _p(peaks["z"]), _p(np.ascontiguousarray(pRf)), _p(pFc), _p(pd2), _p(res),
+                            alatt, cfg.ievol, cfg.z_out, cfg.z_max, cfg.cenx, cfg.ceny, cfg.cenz,
+                            cfg.ioutshear, cfg.ilpt, _p(rec), _p(zz))
+    rec = rec[:nh].copy()
+    tm["total_s"] = time.perf_counter() - t0
+    return dict(fields=fields, delta_k=delta_k, peaks=peaks, Rf=pRf, FcollvRf=pFc, d2FRf=pd2,
+                ir2min=ir2min, ZZon=ZZon, fcrit=fcrit_val, results=res, records=rec, shells=shells,
+                nhunt=nhunt, alatt=alatt)
+
+
+def run_tile(cfg: Config, seed: int, pk_k, pk_p, filters, T: Table) -> np.ndarray:
+    return run_tile_stages(cfg, seed, pk_k, pk_p, filters, T)["records"]

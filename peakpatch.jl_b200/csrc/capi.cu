@@ -1,0 +1,395 @@
+// capi.cu — the extern "C" boundary of libppb (declared in include/ppb.h) and
+// the context methods.  No C++ exception crosses the boundary: every entry
+// point catches ppb::Error (and anything else) and returns a status code,
+// keeping the message for ppb_last_error().
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "ppb_ctx.h"
+
+using namespace ppb;
+
+namespace ppb {
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+void copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  PPB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s));
+  PPB_CUDA(cudaStreamSynchronize(s));
+}
+
+// device copy of a caller buffer (host or device); returns a device pointer
+const void* stage_in(DevBuf& buf, const void* src, size_t bytes, cudaStream_t s) {
+  if (!src) return nullptr;
+  if (is_device_ptr(src)) return src;
+  buf.ensure(bytes);
+  PPB_CUDA(cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, s));
+  return buf.p;
+}
+
+// SPH kernel table akk (RadialShell.jl:133-150)
+static std::vector<double> make_atab4() {
+  std::vector<double> akk(1101);
+  const double pi = 3.141592653589793, ca = 3.0 / (2.0 * pi), cb = 1.0 / (4.0 * pi);
+  for (int i = 1; i <= 1100; i++) {
+    const double u = (i - 1) * 0.01, ru = std::sqrt(u);
+    double v;
+    if (ru < 1.0) v = ca * (2.0 / 3.0 - u + 0.5 * u * ru);
+    else if (ru <= 2.0) v = cb * (2.0 - ru) * (2.0 - ru) * (2.0 - ru);
+    else v = 0.0;
+    akk[i - 1] = v;
+  }
+  akk[1100] = 0.0;
+  return akk;
+}
+
+}  // namespace ppb
+
+// ---------------------------------------------------------------------------
+// context methods
+// ---------------------------------------------------------------------------
+const GrowthTable& ppb_ctx::growth(double Om, double OB, double OL, double h) {
+  if (!(gkey[0] == Om && gkey[1] == OB && gkey[2] == OL && gkey[3] == h)) {
+    gcache = make_growth_table(Om, OB, OL, h);
+    gkey[0] = Om; gkey[1] = OB; gkey[2] = OL; gkey[3] = h;
+    const size_t ng = gcache.a.size();
+    g_a.ensure(ng * 8);
+    g_D.ensure(ng * 8);
+    g_f.ensure(ng * 8);
+    PPB_CUDA(cudaMemcpyAsync(g_a.p, gcache.a.data(), ng * 8, cudaMemcpyHostToDevice, stream));
+    PPB_CUDA(cudaMemcpyAsync(g_D.p, gcache.D.data(), ng * 8, cudaMemcpyHostToDevice, stream));
+    PPB_CUDA(cudaMemcpyAsync(g_f.p, gcache.f.data(), ng * 8, cudaMemcpyHostToDevice, stream));
+    PPB_CUDA(cudaStreamSynchronize(stream));
+  }
+  return gcache;
+}
+
+DevCosmo ppb_ctx::dev_cosmo(const GrowthTable& G, double Om, double OL, double h, double zmax, bool need_chi) {
+  DevCosmo C{};
+  C.ga = g_a.as<double>();
+  C.gD = g_D.as<double>();
+  C.gf = g_f.as<double>();
+  C.ng = (int)G.a.size();
+  C.amin = G.amin; C.amax = G.amax; C.Dinf = G.Dinf; C.D0 = G.D0; C.Hinf = G.Hinf; C.H0 = G.H0;
+  if (need_chi) {
+    if (!(chikey[0] == Om && chikey[1] == OL && chikey[2] == h && chikey[3] == zmax)) {
+      chicache = make_chi_table(Om, OL, h, zmax, 2000);
+      chikey[0] = Om; chikey[1] = OL; chikey[2] = h; chikey[3] = zmax;
+      chi.ensure(chicache.size() * 8);
+      PPB_CUDA(cudaMemcpyAsync(chi.p, chicache.data(), chicache.size() * 8, cudaMemcpyHostToDevice, stream));
+      PPB_CUDA(cudaStreamSynchronize(stream));
+    }
+    C.chis = chi.as<double>();
+    C.nchi = (int)chicache.size();
+    C.chi_zmax = zmax;
+  }
+  return C;
+}
+
+TileRes& ppb_ctx::tile(int n) {
+  auto it = tiles.find(n);
+  if (it == tiles.end()) {
+    // one grid size resident at a time keeps the footprint bounded
+    tiles.clear();
+    it = tiles.emplace(n, std::make_unique<TileRes>()).first;
+  }
+  return *it->second;
+}
+
+ShellArgs ppb_ctx::shell_args(int n, double alatt, const float4* aos, const float* lapd) {
+  ShellArgs a{};
+  a.aos = aos;
+  a.lapd = lapd;
+  a.n = n;
+  a.alatt = alatt;
+  a.cells = shells.d_cells.as<int4>();
+  a.sh_start = shells.d_start.as<int32_t>();
+  a.sh_count = shells.d_count.as<int32_t>();
+  a.rad = shells.d_rad.as<double>();
+  a.r2m = shells.d_r2m.as<int32_t>();
+  a.nshell = shells.nshell;
+  a.mmax = std::max(shells.nshell - 1, 1);
+  a.npart = shells.ncells;
+  a.tab = dtab;
+  a.akk = akk.as<double>();
+  return a;
+}
+
+void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st) {
+  if (shell_blocks == 0) {
+    int b1 = 0, b2 = 0;
+    PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, shell_kernel_ptr(true, true), 32 * shell_wpb, 0));
+    PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, shell_kernel_ptr(false, false), 32 * shell_wpb, 0));
+    shell_blocks = nsm * std::max(1, std::min(b1, b2));
+  }
+  const int64_t stride = shell_scratch_doubles_per_warp(a.nshell);
+  const int64_t slots = (int64_t)shell_blocks * shell_wpb;
+  scratch.ensure((size_t)(slots * stride * 8));
+  counters.ensure(16 * 8);
+  queue.ensure(64);
+  PPB_CUDA(cudaMemsetAsync(counters.p, 0, 16 * 8, stream));
+  PPB_CUDA(cudaMemsetAsync(queue.p, 0, 4, stream));
+  a.scratch = scratch.as<double>();
+  a.scratch_stride = stride;
+  a.queue = queue.as<int>();
+  a.counters = counters.as<unsigned long long>();
+  PPB_CUDA(cudaEventRecord(ev[14], stream));
+  launch_shell(Launch{stream, &launches}, a, comp, adaptive, shell_blocks, shell_wpb);
+  PPB_CUDA(cudaEventRecord(ev[15], stream));
+  unsigned long long c[16];
+  PPB_CUDA(cudaMemcpyAsync(c, counters.p, sizeof(c), cudaMemcpyDeviceToHost, stream));
+  PPB_CUDA(cudaStreamSynchronize(stream));
+  ShellStats s{};
+  s.visits = c[0];
+  for (int i = 0; i < 5; i++) s.dump[i] = c[1 + i];
+  s.guard = c[6];
+  s.akk = c[7];
+  PPB_CUDA(cudaEventElapsedTime(&s.ms, ev[14], ev[15]));
+  last_shell = s;
+  if (st) *st = s;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+#define PPB_GUARD_BEGIN try {
+#define PPB_GUARD_END(ctx)                                                    \
+  }                                                                           \
+  catch (const ppb::Error& e) {                                               \
+    if (ctx) (ctx)->err = e.msg;                                              \
+    return e.code;                                                            \
+  }                                                                           \
+  catch (const std::exception& e) {                                           \
+    if (ctx) (ctx)->err = e.what();                                           \
+    return PPB_ERR_INVALID;                                                   \
+  }                                                                           \
+  catch (...) {                                                               \
+    if (ctx) (ctx)->err = "unknown error";                                    \
+    return PPB_ERR_INVALID;                                                   \
+  }
+
+extern "C" {
+
+int32_t ppb_abi_version(void) { return PPB_ABI_VERSION; }
+
+int32_t ppb_ctx_create(int32_t device, uint64_t hbm_budget, ppb_ctx** out) {
+  if (!out) return PPB_ERR_INVALID;
+  *out = nullptr;
+  ppb_ctx* ctx = nullptr;
+  try {
+    int ndev = 0;
+    PPB_CUDA(cudaGetDeviceCount(&ndev));
+    PPB_REQUIRE(device >= 0 && device < ndev, "device index out of range");
+    PPB_CUDA(cudaSetDevice(device));
+    ctx = new ppb_ctx();
+    ctx->device = device;
+    PPB_CUDA(cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device));
+    PPB_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    for (auto& e : ctx->ev) PPB_CUDA(cudaEventCreate(&e));
+    for (auto& e : ctx->stage_ev) PPB_CUDA(cudaEventCreate(&e));
+    size_t fr = 0, tot = 0;
+    PPB_CUDA(cudaMemGetInfo(&fr, &tot));
+    ctx->hbm_budget = hbm_budget ? hbm_budget : (uint64_t)(0.9 * (double)fr);
+    const std::vector<double> akk = make_atab4();
+    ctx->akk.ensure(akk.size() * 8);
+    PPB_CUDA(cudaMemcpy(ctx->akk.p, akk.data(), akk.size() * 8, cudaMemcpyHostToDevice));
+    *out = ctx;
+    return PPB_OK;
+  } catch (const ppb::Error& e) {
+    delete ctx;
+    fprintf(stderr, "ppb_ctx_create: %s\n", e.msg.c_str());
+    return e.code;
+  } catch (...) {
+    delete ctx;
+    return PPB_ERR_INVALID;
+  }
+}
+
+int32_t ppb_ctx_destroy(ppb_ctx* ctx) {
+  if (!ctx) return PPB_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->tiles.clear();
+  for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+  for (auto& e : ctx->stage_ev) if (e) cudaEventDestroy(e);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return PPB_OK;
+}
+
+int32_t ppb_last_error(ppb_ctx* ctx, char* buf, size_t len) {
+  if (!ctx || !buf || len == 0) return PPB_ERR_INVALID;
+  std::snprintf(buf, len, "%s", ctx->err.c_str());
+  return PPB_OK;
+}
+
+int32_t ppb_set_collapse_table(ppb_ctx* ctx, const float* tab, int32_t nx, int32_t ny, int32_t nz, double x1,
+                               double x2, double y1, double y2, double z1, double z2) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  PPB_GUARD_BEGIN
+  PPB_REQUIRE(tab != nullptr, "table is null");
+  PPB_REQUIRE(nx >= 2 && ny >= 2 && nz >= 2, "table needs at least 2 nodes per axis");
+  PPB_REQUIRE(x2 > x1 && y2 > y1 && z2 > z1, "table ranges must be increasing");
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  const size_t bytes = (size_t)nx * ny * nz * 4;
+  ctx->tab.ensure(bytes);
+  PPB_CUDA(cudaMemcpy(ctx->tab.p, tab, bytes, cudaMemcpyDefault));
+  ctx->dtab = DevTable{ctx->tab.as<float>(), nx, ny, nz, x1, x2, y1, y2, z1, z2};
+  ctx->has_tab = true;
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_set_pk_table(ppb_ctx* ctx, const double* k, const double* pk, int32_t n) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  PPB_GUARD_BEGIN
+  PPB_REQUIRE(k && pk && n >= 2, "P(k) table needs >= 2 rows");
+  std::vector<double> lk(n), lp(n);
+  for (int i = 0; i < n; i++) {
+    PPB_REQUIRE(k[i] > 0 && pk[i] > 0, "P(k) table entries must be positive (log-log interpolation)");
+    if (i) PPB_REQUIRE(k[i] > k[i - 1], "P(k) table k must increase");
+    lk[i] = std::log(k[i]);
+    lp[i] = std::log(pk[i]);
+  }
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  ctx->pk_lk.ensure(n * 8);
+  ctx->pk_lp.ensure(n * 8);
+  PPB_CUDA(cudaMemcpy(ctx->pk_lk.p, lk.data(), n * 8, cudaMemcpyHostToDevice));
+  PPB_CUDA(cudaMemcpy(ctx->pk_lp.p, lp.data(), n * 8, cudaMemcpyHostToDevice));
+  ctx->pk_n = n;
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_run_tile(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, int32_t nfilt, ppb_halo_buf* out) {
+  return ppb_run_tile_timed(ctx, p, Rf, nfilt, out, nullptr);
+}
+
+int32_t ppb_run_tile_timed(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, int32_t nfilt,
+                           ppb_halo_buf* out, float* device_ms) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  return run_tile_impl(ctx, p, Rf, nfilt, out, device_ms);
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_write_pksc(const char* path, const float* records, int64_t n, int32_t nfields, float RTHLmax,
+                       float z_out) {
+  if (!path || n < 0 || (n > 0 && !records) || (nfields != 11 && nfields != 33)) return PPB_ERR_INVALID;
+  if (n > INT32_MAX) return PPB_ERR_INVALID;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return PPB_ERR_INVALID;
+  const int32_t nn = (int32_t)n;
+  bool ok = std::fwrite(&nn, 4, 1, f) == 1 && std::fwrite(&RTHLmax, 4, 1, f) == 1 && std::fwrite(&z_out, 4, 1, f) == 1;
+  if (ok && n > 0) ok = std::fwrite(records, 4, (size_t)n * nfields, f) == (size_t)n * nfields;
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? PPB_OK : PPB_ERR_INVALID;
+}
+
+int32_t ppb_noise_threefry(ppb_ctx* ctx, float* out, int32_t n, uint64_t seed) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  PPB_GUARD_BEGIN
+  PPB_REQUIRE(out != nullptr && n >= 1 && n <= 4096, "bad noise arguments");
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  const size_t bytes = (size_t)n * n * n * 4;
+  if (is_device_ptr(out)) {
+    launch_noise(Launch{ctx->stream, &ctx->launches}, out, n, seed);
+    PPB_CUDA(cudaStreamSynchronize(ctx->stream));
+  } else {
+    DevBuf tmp;
+    tmp.ensure(bytes);
+    launch_noise(Launch{ctx->stream, &ctx->launches}, tmp.as<float>(), n, seed);
+    copy_out(out, tmp.p, bytes, ctx->stream);
+  }
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_alloc_host(ppb_ctx* ctx, size_t bytes, void** out) {
+  if (!ctx || !out || bytes == 0) return PPB_ERR_INVALID;
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  PPB_CUDA(cudaMallocHost(out, bytes));
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_free_host(ppb_ctx* ctx, void* p) {
+  if (!ctx) return PPB_ERR_INVALID;
+  PPB_GUARD_BEGIN
+  if (p) PPB_CUDA(cudaFreeHost(p));
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_alloc_device(ppb_ctx* ctx, size_t bytes, void** out) {
+  if (!ctx || !out || bytes == 0) return PPB_ERR_INVALID;
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  PPB_CUDA(cudaMalloc(out, bytes));
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_free_device(ppb_ctx* ctx, void* p) {
+  if (!ctx) return PPB_ERR_INVALID;
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  if (p) PPB_CUDA(cudaFree(p));
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_event_record(ppb_ctx* ctx, int32_t slot) {
+  if (!ctx || slot < 0 || slot >= 14) return PPB_ERR_INVALID;
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaEventRecord(ctx->ev[slot], ctx->stream));
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_event_elapsed(ppb_ctx* ctx, int32_t a, int32_t b, float* ms) {
+  if (!ctx || !ms || a < 0 || b < 0 || a >= 16 || b >= 16) return PPB_ERR_INVALID;
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaEventSynchronize(ctx->ev[b]));
+  PPB_CUDA(cudaEventElapsedTime(ms, ctx->ev[a], ctx->ev[b]));
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_synchronize(ppb_ctx* ctx) {
+  if (!ctx) return PPB_ERR_INVALID;
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaStreamSynchronize(ctx->stream));
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_launch_count(ppb_ctx* ctx, int64_t* count) {
+  if (!ctx || !count) return PPB_ERR_INVALID;
+  *count = ctx->launches;
+  return PPB_OK;
+}
+
+int32_t ppb_last_stage_ms(ppb_ctx* ctx, float* ms4) {
+  if (!ctx || !ms4) return PPB_ERR_INVALID;
+  std::memcpy(ms4, ctx->stage_ms, sizeof(ctx->stage_ms));
+  return PPB_OK;
+}
+
+}  // extern "C"

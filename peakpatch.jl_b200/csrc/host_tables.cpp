@@ -1,0 +1,253 @@
+// host_tables.cpp — host-side tables of the path, in double precision:
+// the sorted shell-cell list (precompute_shells), the linear growth table
+// (Dlinear_tables / Dlinear_ab / fsc_of_z) and the chi -> z table.
+#include <algorithm>
+#include <cmath>
+#include <utility>
+
+#include "ppb_internal.h"
+
+namespace ppb {
+
+// precompute_shells (src/HaloFinder/RadialShell.jl:160-175): all offsets with
+// r^2 <= nhunt^2 in construction order dk, dj, di, stable-sorted by r^2.
+void build_shell_table(ShellTable& st, int nhunt) {
+  PPB_REQUIRE(nhunt >= 1 && nhunt <= 64, "nhunt must be in [1, 64]");
+  if (st.nhunt == nhunt) return;
+  st.cells.clear();
+  const int r2max = nhunt * nhunt;
+  for (int dk = -nhunt; dk <= nhunt; dk++)
+    for (int dj = -nhunt; dj <= nhunt; dj++)
+      for (int di = -nhunt; di <= nhunt; di++) {
+        const int r2 = di * di + dj * dj + dk * dk;
+        if (r2 <= r2max) st.cells.push_back(make_int4(di, dj, dk, r2));
+      }
+  std::stable_sort(st.cells.begin(), st.cells.end(), [](const int4& a, const int4& b) { return a.w < b.w; });
+  st.ncells = (int64_t)st.cells.size();
+  st.shell_start.clear();
+  st.shell_count.clear();
+  st.shell_r2.clear();
+  for (int64_t i = 0; i < st.ncells; i++) {
+    if (i == 0 || st.cells[i].w != st.cells[i - 1].w) {
+      st.shell_start.push_back((int32_t)i);
+      st.shell_count.push_back(0);
+      st.shell_r2.push_back(st.cells[i].w);
+    }
+    st.shell_count.back()++;
+  }
+  st.nshell = (int)st.shell_r2.size();
+  // shell m (1-based) = distinct value m-1; rad[m] = sqrt(r2)
+  st.rad.assign(st.nshell + 1, 0.0);
+  st.r2m.assign(st.nshell + 1, 0);
+  for (int m = 1; m <= st.nshell; m++) {
+    st.r2m[m] = st.shell_r2[m - 1];
+    st.rad[m] = std::sqrt((double)st.r2m[m]);
+  }
+  st.nhunt = nhunt;
+  st.d_cells.release();   // force re-upload
+}
+
+void upload_shell_table(ShellTable& st, cudaStream_t s) {
+  if (st.d_cells.p && st.d_cells.bytes >= st.cells.size() * sizeof(int4)) return;
+  st.d_cells.ensure(st.cells.size() * sizeof(int4));
+  st.d_start.ensure(st.shell_start.size() * sizeof(int32_t));
+  st.d_count.ensure(st.shell_count.size() * sizeof(int32_t));
+  st.d_r2m.ensure(st.r2m.size() * sizeof(int32_t));
+  st.d_rad.ensure(st.rad.size() * sizeof(double));
+  PPB_CUDA(cudaMemcpyAsync(st.d_cells.p, st.cells.data(), st.cells.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+  PPB_CUDA(cudaMemcpyAsync(st.d_start.p, st.shell_start.data(), st.shell_start.size() * 4, cudaMemcpyHostToDevice, s));
+  PPB_CUDA(cudaMemcpyAsync(st.d_count.p, st.shell_count.data(), st.shell_count.size() * 4, cudaMemcpyHostToDevice, s));
+  PPB_CUDA(cudaMemcpyAsync(st.d_r2m.p, st.r2m.data(), st.r2m.size() * 4, cudaMemcpyHostToDevice, s));
+  PPB_CUDA(cudaMemcpyAsync(st.d_rad.p, st.rad.data(), st.rad.size() * 8, cudaMemcpyHostToDevice, s));
+  PPB_CUDA(cudaStreamSynchronize(s));
+}
+
+// ---------------------------------------------------------------------------
+// Linear growth: RK4 in ln a over 2000 steps from a = 1e-7 to 2, tabulating
+// a in [1/1001, 2] (src/Cosmology/Cosmology.jl:121-202 and 148-202 of the
+// Dlinear_tables listing; the derivative set is the reference's
+// _deriv_Dlin! with no radiation, decaying or hot components).
+// ---------------------------------------------------------------------------
+namespace {
+struct DerivArgs {
+  double h, Omnr, Omvac, Omcurv, OmX, OmB;
+};
+void deriv(const DerivArgs& q, const double* y, double* d, double a) {
+  const double a3 = a * a * a;
+  const double hub = q.Omnr + q.Omvac * a3 + q.Omcurv * a;
+  d[0] = 1.0 / (q.h * std::sqrt(hub / a3));
+  const double fb = y[2];
+  d[1] = fb;
+  const double qs = 0.5 / hub;
+  const double qv = qs * (q.Omnr - 2.0 * q.Omvac * a3);
+  double fnr = (q.OmX + q.OmB) / q.Omnr;
+  if (q.OmB != 0.0 && a <= 1.0e-3) fnr = q.OmX / q.Omnr;
+  const double qf = qs * (q.Omnr * fnr);
+  d[2] = 3.0 * qf - fb * fb - (1.0 - qv) * fb;
+  d[3] = 0.0;
+  d[4] = d[0] / a;
+}
+}  // namespace
+
+GrowthTable make_growth_table(double Om, double OB, double OL, double h) {
+  DerivArgs q{h, Om, OL, 1.0 - Om - OL, Om - OB, OB};
+  const double amaxtab = 2.0, amintab_target = 1.0 / 1001.0, ainit = 1.0e-7;
+  const int nmax = 2000;
+  double a = ainit, alogn = std::log(ainit);
+  const double hh = (std::log(amaxtab) - alogn) / nmax;
+  const double t0 = 1.0 / h / std::sqrt(Om);
+  const double ya = std::sqrt(a);
+  double y[5] = {t0 * (2.0 / 3.0 * (ya * ya * ya)), std::log(a),
+                 0.25 * (std::sqrt(24.0 * q.OmX / Om + 1.0) - 1.0), 0.0, t0 * 2.0 * ya};
+  GrowthTable G;
+  int lnorm = 1, ip0 = 0;
+  double bnorm = 1.0;
+  for (int i = 0; i < nmax; i++) {
+    double w1[5], w2[5], w3[5], w4[5], yt[5];
+    deriv(q, y, w1, a);
+    const double ah = std::exp(alogn + hh * 0.5);
+    for (int c = 0; c < 5; c++) yt[c] = y[c] + hh * w1[c] * 0.5;
+    deriv(q, yt, w2, ah);
+    for (int c = 0; c < 5; c++) yt[c] = y[c] + hh * w2[c] * 0.5;
+    deriv(q, yt, w3, ah);
+    const double an = alogn + hh, anew = std::exp(an);
+    for (int c = 0; c < 5; c++) yt[c] = y[c] + hh * w3[c];
+    deriv(q, yt, w4, anew);
+    for (int c = 0; c < 5; c++) y[c] = y[c] + hh / 6.0 * (w1[c] + w4[c] + 2.0 * (w2[c] + w3[c]));
+    alogn = an;
+    a = anew;
+    if (lnorm == 1 && a >= 0.001) {
+      lnorm = 0;
+      bnorm = std::exp(y[1]) / a;
+    }
+    if (a >= amintab_target && a <= amaxtab) {
+      G.a.push_back(a);
+      G.D.push_back(std::exp(y[1]) / a);
+      G.f.push_back(y[2]);
+      if (a >= 1.0 && ip0 == 0) ip0 = (int)G.a.size();
+    }
+  }
+  double fac;
+  if (ip0 > 1) {
+    const double ai = (G.a[ip0 - 1] - 1.0) / (G.a[ip0 - 1] - G.a[ip0 - 2]);
+    const double Dag = (G.D[ip0 - 1] * (1.0 - ai) + G.D[ip0 - 2] * ai) / bnorm;
+    fac = 1.0 / (Dag * bnorm);
+  } else {
+    fac = 1.0 / bnorm;
+  }
+  for (auto& v : G.D) v *= fac;
+  G.amin = G.a.front();
+  G.amax = G.a.back();
+  G.Dinf = G.D.front();
+  G.D0 = G.D.back();
+  G.Hinf = G.f.front();
+  G.H0 = G.f.back();
+  return G;
+}
+
+// Dlinear_ab (Cosmology.jl:420-440 of the listing): bisection "hunt", then a
+// 4-point (2-point at the ends) Lagrange interpolation of D(a)/a and dlnD/dlna.
+void dlinear_ab(const GrowthTable& G, double ai, double* Dl, double* HD, double* Da) {
+  const int ntab = (int)G.a.size();
+  if (ai > G.amin && ai < G.amax) {
+    int jlo = 0, jhi = ntab + 1;
+    while (jhi - jlo > 1) {
+      const int jm = (jhi + jlo) / 2;
+      if (ai > G.a[jm - 1]) jlo = jm; else jhi = jm;
+    }
+    const int kk = jlo;
+    int nl, kkl;
+    if (kk < 2 || kk >= ntab) { nl = 2; kkl = std::max(kk - 1, 1); } else { nl = 4; kkl = kk - 2; }
+    const double* xa = &G.a[kkl - 1];
+    const double* v1 = &G.D[kkl - 1];
+    const double* v2 = &G.f[kkl - 1];
+    const double x = ai;
+    double p1, p2;
+    if (nl == 4) {
+      const double a1 = (x - xa[1]) / (xa[0] - xa[1]) * (x - xa[2]) / (xa[0] - xa[2]) * (x - xa[3]) / (xa[0] - xa[3]);
+      const double a2 = (x - xa[0]) / (xa[1] - xa[0]) * (x - xa[2]) / (xa[1] - xa[2]) * (x - xa[3]) / (xa[1] - xa[3]);
+      const double a3 = (x - xa[0]) / (xa[2] - xa[0]) * (x - xa[1]) / (xa[2] - xa[1]) * (x - xa[3]) / (xa[2] - xa[3]);
+      const double a4 = (x - xa[0]) / (xa[3] - xa[0]) * (x - xa[1]) / (xa[3] - xa[1]) * (x - xa[2]) / (xa[3] - xa[2]);
+      p1 = a1 * v1[0] + a2 * v1[1] + a3 * v1[2] + a4 * v1[3];
+      p2 = a1 * v2[0] + a2 * v2[1] + a3 * v2[2] + a4 * v2[3];
+    } else {
+      const double a1 = (x - xa[1]) / (xa[0] - xa[1]);
+      const double a2 = 1.0 - a1;
+      p1 = a1 * v1[0] + a2 * v1[1];
+      p2 = a1 * v2[0] + a2 * v2[1];
+    }
+    *Dl = p1 * ai;
+    *HD = p2;
+    *Da = p1;
+  } else if (ai >= G.amax) {
+    *Dl = G.D0 * ai; *HD = G.H0; *Da = G.D0;
+  } else {
+    *Dl = G.Dinf * ai; *HD = G.Hinf; *Da = G.Dinf;
+  }
+}
+
+// fsc_of_z (RadialShell.jl:191-196): 1.686 D(1/(1+z))
+double fsc_of_z(const GrowthTable& G, double z) {
+  double d, hd, da;
+  dlinear_ab(G, 1.0 / (1.0 + z), &d, &hd, &da);
+  return 1.686 * d;
+}
+
+// chi(z) in Mpc/h = (c/100) h * int_0^z dz'/E(z'), flat LCDM
+// (Cosmology.jl:15-24); adaptive 7/15-point Gauss-Kronrod quadrature.
+namespace {
+double gk15(double Om, double OL, double a, double b, double* err) {
+  static const double xk[8] = {0.991455371120812639206854697526329, 0.949107912342758524526189684047851,
+                               0.864864423359769072789712788640926, 0.741531185599394439863864773280788,
+                               0.586087235467691130294144845693013, 0.405845151377397166906606412076961,
+                               0.207784955007898467600689403773245, 0.0};
+  static const double wk[8] = {0.022935322010529224963732008058970, 0.063092092629978553290700663189204,
+                               0.104790010322250183839876322541518, 0.140653259715525918745189590510238,
+                               0.169004726639267902826583426598550, 0.190350578064785409913256402421014,
+                               0.204432940075298892414161999234649, 0.209482141084727828012999174891714};
+  static const double wg[4] = {0.129484966168869693270611432679082, 0.279705391489276667901467771423780,
+                               0.381830050505118944950369775488975, 0.417959183673469387755102040816327};
+  auto f = [&](double z) { return 1.0 / std::sqrt(Om * (1 + z) * (1 + z) * (1 + z) + OL); };
+  const double c = 0.5 * (a + b), hl = 0.5 * (b - a);
+  const double fc = f(c);
+  double rk = fc * wk[7], rg = fc * wg[3];
+  for (int j = 0; j < 7; j++) {
+    const double dx = hl * xk[j];
+    const double s = f(c - dx) + f(c + dx);
+    rk += wk[j] * s;
+    if (j % 2 == 1) rg += wg[j / 2] * s;
+  }
+  *err = std::fabs((rk - rg) * hl);
+  return rk * hl;
+}
+double chi_of_z(double Om, double OL, double h, double z) {
+  if (z == 0.0) return 0.0;
+  std::vector<std::pair<double, double>> st{{0.0, z}};
+  double tot = 0.0;
+  while (!st.empty()) {
+    const auto ab = st.back();
+    st.pop_back();
+    double e;
+    const double v = gk15(Om, OL, ab.first, ab.second, &e);
+    if (e <= 1e-14 * std::fabs(v) || (ab.second - ab.first) < 1e-9) tot += v;
+    else {
+      const double m = 0.5 * (ab.first + ab.second);
+      st.push_back({ab.first, m});
+      st.push_back({m, ab.second});
+    }
+  }
+  return (2.998e5 / 100.0) * h * tot;
+}
+}  // namespace
+
+// build_chi_to_z (Cosmology.jl:144-148): chi at npts redshifts 0..zmax
+std::vector<double> make_chi_table(double Om, double OL, double h, double zmax, int npts) {
+  std::vector<double> c(npts);
+  for (int i = 0; i < npts; i++) {
+    const double z = npts == 1 ? 0.0 : zmax * (double)i / (double)(npts - 1);
+    c[i] = chi_of_z(Om, OL, h, z);
+  }
+  return c;
+}
+
+}  // namespace ppb

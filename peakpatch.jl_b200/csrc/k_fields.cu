@@ -1,0 +1,461 @@
+// k_fields.cu — field-generation kernels of the tile pipeline:
+// Threefry noise, the k-space multipliers (sqrt P, 1LPT, phi_ij, 2LPT,
+// Laplacian, filter windows), the Hermitian projection applied before every
+// complex-to-real transform, the 2LPT source term, the gather-field pack and
+// the peak finder.
+//
+// Layouts: real fields are n^3 floats, C order [k][j][i] (= Julia column-major
+// [i,j,k]); half-spectra are (n/2+1) x n x n float2 with ix fastest, the
+// layout cuFFT's R2C produces for that real array and the layout of Julia's
+// rfft(delta).  Every multiplier folds in the 1/n^3 normalisation of the
+// following inverse transform (cuFFT's C2R is unnormalised, Julia's irfft is
+// normalised), passed as `post_scale`.
+#include "ppb_internal.h"
+#include "ppb_math.h"
+
+namespace ppb {
+
+namespace {
+
+constexpr double kPi = 3.141592653589793;
+
+// AbstractFFTs frequency of 0-based index idx: fftfreq keeps idx < ceil(n/2)
+// non-negative, the rest wrap to idx - n; rfftfreq is idx itself.
+__device__ __forceinline__ double fftfreq(int idx, int n, double mult) {
+  const int v = idx < (n + 1) / 2 ? idx : idx - n;
+  return (double)v * mult;
+}
+
+// mode decomposition for a (nh x n) plane per blockIdx.y = iz
+struct Mode {
+  int ix, iy, iz;
+  int64_t id;
+  bool ok;
+};
+__device__ __forceinline__ Mode mode_of(int n, int nh) {
+  Mode m;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int plane = nh * n;
+  m.iz = blockIdx.y;
+  m.ok = r < plane;
+  m.ix = r % nh;
+  m.iy = r / nh;
+  m.id = (int64_t)r + (int64_t)plane * m.iz;
+  return m;
+}
+inline dim3 mode_grid(int n) {
+  const int nh = n / 2 + 1;
+  return dim3((unsigned)((nh * n + 255) / 256), (unsigned)n, 1);
+}
+
+// ---------------------------------------------------------------------------
+// noise: one thread per Threefry pair -> cells 2p and 2p+1
+// (RandomField.jl:70-83)
+// ---------------------------------------------------------------------------
+__global__ void noise_kernel(float* __restrict__ out, int64_t ncell, uint64_t seed) {
+  const int64_t npair = (ncell + 1) / 2;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < npair;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    double g1, g2;
+    ppbm::threefry_gaussian_pair(seed, (uint64_t)p, &g1, &g2);
+    const int64_t c = 2 * p;
+    if (c + 1 < ncell) {
+      reinterpret_cast<float2*>(out)[p] = make_float2((float)g1, (float)g2);
+    } else {
+      out[c] = (float)g1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// P(k): log-log linear interpolation with linear extrapolation
+// (PowerSpectrum.jl:189-201)
+// ---------------------------------------------------------------------------
+__device__ double pk_eval(const double* __restrict__ lk, const double* __restrict__ lp, int np, double k) {
+  const double x = log(k);
+  int i;
+  if (x <= lk[0]) i = 0;
+  else if (x >= lk[np - 1]) i = np - 2;
+  else {
+    int lo = 0, hi = np - 1;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (lk[mid] <= x) lo = mid; else hi = mid;
+    }
+    i = lo;
+  }
+  const double t = (x - lk[i]) / (lk[i + 1] - lk[i]);
+  return exp(lp[i] * (1.0 - t) + lp[i + 1] * t);
+}
+
+// noise_k *= sqrt(P(k) dk^3 n^3), DC := 0  (RandomField.jl:136-168)
+__global__ void convolve_kernel(float2* __restrict__ nk, int n, double dk, double mult,
+                                const double* __restrict__ lk, const double* __restrict__ lp, int np,
+                                double post_scale) {
+  const int nh = n / 2 + 1;
+  const Mode md = mode_of(n, nh);
+  if (!md.ok) return;
+  const double kx = (double)md.ix * mult, ky = fftfreq(md.iy, n, mult), kz = fftfreq(md.iz, n, mult);
+  const double k2 = kx * kx + ky * ky + kz * kz;
+  float2 v = nk[md.id];
+  if (k2 == 0.0) {
+    v = make_float2(0.f, 0.f);
+  } else {
+    const double nd = (double)n;
+    const double amp = sqrt(pk_eval(lk, lp, np, sqrt(k2)) * (dk * dk * dk) * (nd * nd * nd)) * post_scale;
+    v = make_float2((float)((double)v.x * amp), (float)((double)v.y * amp));
+  }
+  nk[md.id] = v;
+}
+
+// psi_c = i k_c / k^2 delta_k, Nyquist planes and DC zeroed (LPT.jl:21-71)
+__global__ void lpt1_kernel(const float2* __restrict__ dk, float2* __restrict__ out, int n,
+                            double mult, double post_scale) {
+  const int nh = n / 2 + 1;
+  const Mode md = mode_of(n, nh);
+  if (!md.ok) return;
+  const int64_t M = (int64_t)nh * n * n;
+  const double kv[3] = {(double)md.ix * mult, fftfreq(md.iy, n, mult), fftfreq(md.iz, n, mult)};
+  const double k2 = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
+  const bool zero = (k2 == 0.0) || md.ix == nh - 1 || md.iy == n / 2 || md.iz == n / 2;
+  const float2 d = dk[md.id];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    float2 o = make_float2(0.f, 0.f);
+    if (!zero) {
+      const double q = kv[c] / k2 * post_scale;
+      o = make_float2((float)(-q * (double)d.y), (float)(q * (double)d.x));
+    }
+    out[c * M + md.id] = o;
+  }
+}
+
+// phi_ij = -k_i k_j / k^2 delta_k, order 11 22 33 12 13 23, no Nyquist
+// zeroing (LPT.jl:103-128)
+__global__ void phi_kernel(const float2* __restrict__ dk, float2* __restrict__ out, int n, double mult,
+                           double post_scale) {
+  const int nh = n / 2 + 1;
+  const Mode md = mode_of(n, nh);
+  if (!md.ok) return;
+  const int64_t M = (int64_t)nh * n * n;
+  const double kv[3] = {(double)md.ix * mult, fftfreq(md.iy, n, mult), fftfreq(md.iz, n, mult)};
+  const double k2 = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
+  const float2 d = dk[md.id];
+  const int pa[6] = {0, 1, 2, 0, 0, 1}, pb[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int c = 0; c < 6; c++) {
+    float2 o = make_float2(0.f, 0.f);
+    if (k2 != 0.0) {
+      const double q = (-kv[pa[c]]) * kv[pb[c]] / k2 * post_scale;
+      o = make_float2((float)(q * (double)d.x), (float)(q * (double)d.y));
+    }
+    out[c * M + md.id] = o;
+  }
+}
+
+// src2 = phi11 phi22 - phi12^2 + phi11 phi33 - phi13^2 + phi22 phi33 - phi23^2,
+// single precision, left to right, no fused multiply-add (LPT.jl:141-143)
+__global__ void src2_kernel(const float* __restrict__ phi, float* __restrict__ out, int64_t N) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    const float a = phi[i], b = phi[N + i], c = phi[2 * N + i], d = phi[3 * N + i], e = phi[4 * N + i],
+                f = phi[5 * N + i];
+    float t = __fmul_rn(a, b);
+    t = __fsub_rn(t, __fmul_rn(d, d));
+    t = __fadd_rn(t, __fmul_rn(a, c));
+    t = __fsub_rn(t, __fmul_rn(e, e));
+    t = __fadd_rn(t, __fmul_rn(b, c));
+    t = __fsub_rn(t, __fmul_rn(f, f));
+    out[i] = t;
+  }
+}
+
+// psi2_c = -i k_c / k^2 src2_k with Nyquist zeroing (LPT.jl:155-182)
+__global__ void lpt2_kernel(const float2* __restrict__ sk, float2* __restrict__ out, int n, double mult,
+                            double post_scale) {
+  const int nh = n / 2 + 1;
+  const Mode md = mode_of(n, nh);
+  if (!md.ok) return;
+  const int64_t M = (int64_t)nh * n * n;
+  const double kv[3] = {(double)md.ix * mult, fftfreq(md.iy, n, mult), fftfreq(md.iz, n, mult)};
+  const double k2 = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
+  const bool zero = (k2 == 0.0) || md.ix == nh - 1 || md.iy == n / 2 || md.iz == n / 2;
+  const float2 s = sk[md.id];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    float2 o = make_float2(0.f, 0.f);
+    if (!zero) {
+      const double q = kv[c] / k2 * post_scale;
+      o = make_float2((float)(q * (double)s.y), (float)(-q * (double)s.x));
+    }
+    out[c * M + md.id] = o;
+  }
+}
+
+// k^2 delta_k with single-precision k (Pipeline.jl:35-51); post_scale folds
+// both 1/n^3 factors of that function.
+__global__ void lapd_kernel(const float2* __restrict__ dk, float2* __restrict__ out, int n, float dkf,
+                            float post_scale) {
+  const int nh = n / 2 + 1;
+  const Mode md = mode_of(n, nh);
+  if (!md.ok) return;
+  const int nyq = n / 2;
+  const float kx = __fmul_rn((float)md.ix, dkf);
+  const float ky = __fmul_rn((float)(md.iy <= nyq ? md.iy : md.iy - n), dkf);
+  const float kz = __fmul_rn((float)(md.iz <= nyq ? md.iz : md.iz - n), dkf);
+  float k2 = __fmul_rn(kx, kx);
+  k2 = __fadd_rn(k2, __fmul_rn(ky, ky));
+  k2 = __fadd_rn(k2, __fmul_rn(kz, kz));
+  const float2 d = dk[md.id];
+  out[md.id] = make_float2(__fmul_rn(__fmul_rn(k2, d.x), post_scale), __fmul_rn(__fmul_rn(k2, d.y), post_scale));
+}
+
+// filter windows (Filters.jl:18-36, smooth_field :79-106):
+// 0: exp(-(kR/2)^2/2), 1: top-hat 3(sin x - x cos x)/x^3, 3: Gaussian * k^2.
+__device__ __forceinline__ double window_w(double kR, double k, int ws) {
+  if (ws == 0) { const double h = kR / 2; return exp(-h * h / 2); }
+  if (ws == 3) { const double h = kR / 2; return exp(-h * h / 2) * (k * k); }
+  double s, c;
+  sincos(kR, &s, &c);
+  return 3.0 * (s - kR * c) / (kR * kR * kR);
+}
+
+__global__ void window_kernel(const float2* __restrict__ dk, float2* __restrict__ out0,
+                              float2* __restrict__ out1, int n, double dkk, double Rf, int wsmooth,
+                              double post_scale) {
+  const int nh = n / 2 + 1;
+  const Mode md = mode_of(n, nh);
+  if (!md.ok) return;
+  const double kx = dkk * (double)md.ix, ky = dkk * fftfreq(md.iy, n, 1.0), kz = dkk * fftfreq(md.iz, n, 1.0);
+  const double k = sqrt(kx * kx + ky * ky + kz * kz);
+  const double fkR = k * Rf;
+  const float2 d = dk[md.id];
+  const float ps = (float)post_scale;
+  if (fkR == 0.0) {
+    out0[md.id] = make_float2(d.x * ps, d.y * ps);
+    if (out1) out1[md.id] = make_float2(d.x * ps, d.y * ps);
+    return;
+  }
+  const float w0 = (float)window_w(fkR, k, wsmooth);
+  out0[md.id] = make_float2(__fmul_rn(__fmul_rn(d.x, w0), ps), __fmul_rn(__fmul_rn(d.y, w0), ps));
+  if (out1) {
+    const float w1 = (float)window_w(fkR, k, 3);
+    out1[md.id] = make_float2(__fmul_rn(__fmul_rn(d.x, w1), ps), __fmul_rn(__fmul_rn(d.y, w1), ps));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Hermitian projection of the ix = 0 and ix = n/2 planes:
+// X(k) <- (X(k) + conj(X(-k)))/2.  FFTW's and pocketfft's multi-dimensional
+// complex-to-real transforms act on a half-spectrum as if this projection had
+// been applied (the last, real transform drops the imaginary parts of its
+// DC and Nyquist inputs); cuFFT gives no such guarantee for inputs that are
+// not Hermitian, e.g. phi_ij off the diagonal on the Nyquist lines.
+// ---------------------------------------------------------------------------
+__global__ void hermitise_kernel(float2* __restrict__ data, int n, int nbatch) {
+  const int nh = n / 2 + 1;
+  const int64_t M = (int64_t)nh * n * n;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int per_plane = n * n;
+  const int planes = (n % 2 == 0) ? 2 : 1;
+  if (t >= per_plane * planes * nbatch) return;
+  const int b = t / (per_plane * planes);
+  const int r = t % (per_plane * planes);
+  const int pl = r / per_plane;
+  const int q = r % per_plane;
+  const int iy = q % n, iz = q / n;
+  const int ix = pl == 0 ? 0 : n / 2;
+  const int jy = (n - iy) % n, jz = (n - iz) % n;
+  const int64_t a_id = ix + (int64_t)nh * (iy + (int64_t)n * iz);
+  const int64_t b_id = ix + (int64_t)nh * (jy + (int64_t)n * jz);
+  float2* base = data + b * M;
+  if (a_id == b_id) {
+    base[a_id].y = 0.f;
+    return;
+  }
+  // each unordered pair handled once, by its smaller index
+  if (a_id > b_id) return;
+  const float2 x = base[a_id], y = base[b_id];
+  const float re = 0.5f * (x.x + y.x), im = 0.5f * (x.y - y.y);
+  base[a_id] = make_float2(re, im);
+  base[b_id] = make_float2(re, -im);
+}
+
+// ---------------------------------------------------------------------------
+// gather-field pack: per cell two float4 = (delta, deltaT, psi_x, psi_y),
+// (psi_z, psi2_x, psi2_y, psi2_z).  deltaT at (a,b,c) is delta(c,a,b): the
+// transposed read delta[iv3, iv1, iv2] of RadialShell.jl:448, made into a
+// plain array so the shell gather reads one 32-byte record per cell.
+// Block: 32 x 8 threads over a 32 (a) x 32 (c) tile at fixed b.
+// ---------------------------------------------------------------------------
+__global__ void pack_kernel(float4* __restrict__ aos, const float* __restrict__ delta,
+                            const float* __restrict__ psi, const float* __restrict__ psi2, int n) {
+  __shared__ float tile[32][33];
+  const int b = blockIdx.z;
+  const int a0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  const int64_t n2 = (int64_t)n * n, N = n2 * n;
+  // load delta(c, a, b) for c in [c0, c0+32), a in [a0, a0+32): lin = c + n a + n^2 b
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int a = a0 + r, c = c0 + threadIdx.x;
+    if (a < n && c < n) tile[r][threadIdx.x] = delta[c + (int64_t)n * a + n2 * b];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int a = a0 + threadIdx.x, c = c0 + r;
+    if (a >= n || c >= n) continue;
+    const int64_t lin = a + (int64_t)n * b + n2 * c;
+    const float dT = tile[threadIdx.x][r];
+    float4 v0, v1;
+    v0.x = delta[lin];
+    v0.y = dT;
+    v0.z = psi[lin];
+    v0.w = psi[N + lin];
+    v1.x = psi[2 * N + lin];
+    if (psi2) {
+      v1.y = psi2[lin];
+      v1.z = psi2[N + lin];
+      v1.w = psi2[2 * N + lin];
+    } else {
+      v1.y = v1.z = v1.w = 0.f;
+    }
+    aos[2 * lin] = v0;
+    aos[2 * lin + 1] = v1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// peak finder for one filter (PeakFind.jl:123-186).  A cell of the inner cube
+// (nbuff < i <= n - nbuff, 1-based) is a peak when it is not masked, is not
+// below fcrit, and no neighbour of the 3x3x3 block is strictly larger.  The
+// cell's mask is set; within one filter only a peak's own cell is written,
+// so the cells can be tested in parallel.  Order is restored afterwards by
+// sorting the (filter, flat index) keys.
+// ---------------------------------------------------------------------------
+__global__ void peakfind_kernel(const float* __restrict__ ds, const float* __restrict__ ls,
+                                uint8_t* __restrict__ mask, int n1, int n2, int n3, int nbuff, float fcrit,
+                                int fidx, PeakBuf pb) {
+  const int i = nbuff + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = nbuff + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = nbuff + blockIdx.z;
+  const int64_t n12 = (int64_t)n1 * n2;
+  bool peak = false;
+  int64_t lin = 0;
+  float ff = 0.f;
+  if (i < n1 - nbuff && j < n2 - nbuff && k < n3 - nbuff) {
+    lin = i + (int64_t)n1 * j + n12 * k;
+    ff = ds[lin];
+    if (mask[lin] != 1 && !(ff < fcrit)) {
+      peak = true;
+#pragma unroll
+      for (int dk = -1; dk <= 1; dk++)
+#pragma unroll
+        for (int dj = -1; dj <= 1; dj++)
+#pragma unroll
+          for (int di = -1; di <= 1; di++) {
+            const float v = __ldg(ds + lin + di + (int64_t)n1 * dj + n12 * dk);
+            if (ff < v) peak = false;
+          }
+    }
+  }
+  const unsigned full = 0xffffffffu;
+  const unsigned ball = __ballot_sync(full, peak);
+  if (ball == 0) return;
+  const int lane = threadIdx.x + blockDim.x * threadIdx.y;   // blockDim.x*y == 32k; lanes per warp
+  const int wl = lane & 31;
+  const int leader = __ffs(ball) - 1;
+  int base = 0;
+  if (wl == leader) base = atomicAdd(pb.count, __popc(ball));
+  base = __shfl_sync(full, base, leader);
+  if (peak) {
+    mask[lin] = 1;
+    const int slot = base + __popc(ball & ((1u << wl) - 1u));
+    if (slot < pb.cap) {
+      pb.keys[slot] = ((unsigned long long)fidx << 40) | (unsigned long long)lin;
+      pb.vals[slot] = (uint32_t)slot;
+      pb.ff[slot] = ff;
+      pb.lap[slot] = ls ? ls[lin] : 0.f;
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+void launch_noise(Launch L, float* out, int64_t n, uint64_t seed) {
+  const int64_t ncell = n * n * n;
+  const int64_t npair = (ncell + 1) / 2;
+  const int threads = 256;
+  const int64_t blocks = std::min<int64_t>((npair + threads - 1) / threads, 148 * 32);
+  noise_kernel<<<(unsigned)blocks, threads, 0, L.s>>>(out, ncell, seed);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_convolve(Launch L, float2* nk, int n, double boxsize, const double* lk, const double* lp,
+                     int np, double post_scale) {
+  const double dk = 2.0 * kPi / boxsize;
+  const double mult = (n * dk) / (double)n;
+  convolve_kernel<<<mode_grid(n), 256, 0, L.s>>>(nk, n, dk, mult, lk, lp, np, post_scale);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_lpt1(Launch L, const float2* dk, float2* out, int n, double boxsize, double post_scale) {
+  const double dkk = 2.0 * kPi / boxsize;
+  lpt1_kernel<<<mode_grid(n), 256, 0, L.s>>>(dk, out, n, (n * dkk) / (double)n, post_scale);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_phi(Launch L, const float2* dk, float2* out, int n, double boxsize, double post_scale) {
+  const double dkk = 2.0 * kPi / boxsize;
+  phi_kernel<<<mode_grid(n), 256, 0, L.s>>>(dk, out, n, (n * dkk) / (double)n, post_scale);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_src2(Launch L, const float* phi, float* out, int64_t N) {
+  const int64_t blocks = std::min<int64_t>((N + 255) / 256, 148 * 32);
+  src2_kernel<<<(unsigned)blocks, 256, 0, L.s>>>(phi, out, N);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_lpt2(Launch L, const float2* s2k, float2* out, int n, double boxsize, double post_scale) {
+  const double dkk = 2.0 * kPi / boxsize;
+  lpt2_kernel<<<mode_grid(n), 256, 0, L.s>>>(s2k, out, n, (n * dkk) / (double)n, post_scale);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_lapd(Launch L, const float2* dk, float2* out, int n, double boxsize, float post_scale) {
+  lapd_kernel<<<mode_grid(n), 256, 0, L.s>>>(dk, out, n, (float)(2.0 * kPi / boxsize), post_scale);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_window(Launch L, const float2* dk, float2* out0, float2* out1, int n, double boxsize,
+                   double Rf, int wsmooth, double post_scale) {
+  window_kernel<<<mode_grid(n), 256, 0, L.s>>>(dk, out0, out1, n, 2.0 * kPi / boxsize, Rf, wsmooth,
+                                               post_scale);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_hermitise(Launch L, float2* data, int n, int nbatch) {
+  const int planes = (n % 2 == 0) ? 2 : 1;
+  const int total = n * n * planes * nbatch;
+  hermitise_kernel<<<(total + 255) / 256, 256, 0, L.s>>>(data, n, nbatch);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_pack(Launch L, float4* aos, const float* delta, const float* psi, const float* psi2, int n) {
+  dim3 grid((n + 31) / 32, (n + 31) / 32, n);
+  pack_kernel<<<grid, dim3(32, 8), 0, L.s>>>(aos, delta, psi, psi2, n);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_peakfind(Launch L, const float* ds, const float* ls, uint8_t* mask, int n1, int n2, int n3,
+                     int nbuff, float fcrit, int fidx, PeakBuf pb) {
+  const int w1 = n1 - 2 * nbuff, w2 = n2 - 2 * nbuff, w3 = n3 - 2 * nbuff;
+  if (w1 <= 0 || w2 <= 0 || w3 <= 0) return;
+  dim3 block(32, 4);
+  dim3 grid((w1 + 31) / 32, (w2 + 3) / 4, w3);
+  peakfind_kernel<<<grid, block, 0, L.s>>>(ds, ls, mask, n1, n2, n3, nbuff, fcrit, fidx, pb);
+  PPB_LAUNCHED(*L.count);
+}
+
+}  // namespace ppb

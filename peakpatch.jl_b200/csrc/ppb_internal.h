@@ -1,0 +1,202 @@
+// ppb_internal.h — shared declarations of libppb (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ppb.h"
+
+namespace ppb {
+
+// ---------------------------------------------------------------------------
+// error plumbing: every failing CUDA call is turned into a status + message
+// ---------------------------------------------------------------------------
+struct Error {
+  int32_t code;
+  std::string msg;
+};
+
+#define PPB_CUDA(call)                                                                    \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      throw ::ppb::Error{e_ == cudaErrorMemoryAllocation ? PPB_ERR_NOMEM : PPB_ERR_CUDA,  \
+                         std::string(#call) + ": " + cudaGetErrorString(e_)};             \
+  } while (0)
+
+#define PPB_CUFFT(call)                                                                   \
+  do {                                                                                    \
+    cufftResult r_ = (call);                                                              \
+    if (r_ != CUFFT_SUCCESS)                                                              \
+      throw ::ppb::Error{r_ == CUFFT_ALLOC_FAILED ? PPB_ERR_NOMEM : PPB_ERR_CUDA,         \
+                         std::string(#call) + ": cufft status " + std::to_string((int)r_)}; \
+  } while (0)
+
+#define PPB_REQUIRE(cond, msg)                                                            \
+  do {                                                                                    \
+    if (!(cond)) throw ::ppb::Error{PPB_ERR_INVALID, std::string(msg)};                   \
+  } while (0)
+
+// after each kernel launch: catch launch-configuration errors immediately
+#define PPB_LAUNCHED(ctr)                                                                 \
+  do {                                                                                    \
+    PPB_CUDA(cudaGetLastError());                                                         \
+    (ctr)++;                                                                              \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  void ensure(size_t b) {
+    if (b <= bytes) return;
+    release();
+    PPB_CUDA(cudaMalloc(&p, b));
+    bytes = b;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// geometry of the sorted shell-cell list (precompute_shells)
+// ---------------------------------------------------------------------------
+struct ShellTable {
+  int nhunt = -1;
+  int64_t ncells = 0;                 // cells with r2 <= nhunt^2 (including the centre)
+  int nshell = 0;                     // distinct r2 values (including 0)
+  std::vector<int4> cells;            // (di, dj, dk, r2), stable-sorted by r2
+  std::vector<int32_t> shell_start;   // per distinct r2 value: first cell index
+  std::vector<int32_t> shell_count;
+  std::vector<int32_t> shell_r2;
+  std::vector<double> rad;            // rad[m] (m = 0..nshell), rad[1] = 0
+  std::vector<int32_t> r2m;           // r2 of shell m (m = 0..nshell)
+  DevBuf d_cells, d_start, d_count, d_r2m, d_rad;
+};
+void build_shell_table(ShellTable& st, int nhunt);
+void upload_shell_table(ShellTable& st, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// linear-growth and chi->z tables (host, double precision)
+// ---------------------------------------------------------------------------
+struct GrowthTable {
+  std::vector<double> a, D, f;
+  double amin = 0, amax = 0, Dinf = 0, D0 = 0, Hinf = 0, H0 = 0;
+};
+GrowthTable make_growth_table(double Om, double OB, double OL, double h);
+void dlinear_ab(const GrowthTable& G, double ai, double* Dl, double* HD, double* Da);
+double fsc_of_z(const GrowthTable& G, double z);
+std::vector<double> make_chi_table(double Om, double OL, double h, double zmax, int npts);
+
+// device view of the tables used per peak (lightcone ZZon / fcrit / D(z))
+struct DevCosmo {
+  const double* ga;   // growth a
+  const double* gD;   // D(a)/a normalised
+  const double* gf;   // dlnD/dlna
+  int ng;
+  double amin, amax, Dinf, D0, Hinf, H0;
+  const double* chis;  // chi(z_i), z_i = zmax * i/(npts-1)
+  int nchi;
+  double chi_zmax;
+};
+
+// collapse table on the device
+struct DevTable {
+  const float* t;
+  int nx, ny, nz;
+  double x1, x2, y1, y2, z1, z2;
+};
+
+// ---------------------------------------------------------------------------
+// per-peak parameters and results on the device
+// ---------------------------------------------------------------------------
+constexpr int RES_N = 31;   // doubles per peak result (layout in ppb.h)
+
+struct PeakParams {          // SoA, length npk
+  const int64_t* lin;       // 0-based flat index i + n j + n^2 k
+  const double* Rf;
+  const int32_t* ir2min;
+  const double* ZZon;
+  const double* fcrit;
+};
+
+struct ShellArgs {
+  const float4* aos;        // 2 float4 per cell: (delta, deltaT, psi1x, psi1y), (psi1z, psi2x, psi2y, psi2z)
+  const float* lapd;        // may be null
+  int n;
+  double alatt;
+  // shell geometry
+  const int4* cells;
+  const int32_t* sh_start;
+  const int32_t* sh_count;
+  const double* rad;        // rad[m], m = 0..nshell (index 0 unused); rad[1] = 0
+  const int32_t* r2m;       // r^2 of shell m, m = 1..nshell (shell nshell is the unfinalised last group)
+  int nshell;               // distinct r2 values in the list (incl. 0)
+  int mmax;                 // finalised shells: nshell - 1
+  int64_t npart;            // cells used (full list here)
+  DevTable tab;
+  const double* akk;        // 1101-entry SPH kernel table
+  PeakParams pk;
+  int64_t npk;
+  double* out;              // npk x RES_N
+  double* scratch;          // per-warp profile scratch
+  int64_t scratch_stride;   // doubles per warp slot
+  int* queue;               // work counter for the persistent kernel
+  unsigned long long* counters;   // [0] cell visits, [1..5] dump reasons
+};
+
+// ---------------------------------------------------------------------------
+// kernel launchers (k_*.cu)
+// ---------------------------------------------------------------------------
+struct Launch {
+  cudaStream_t s;
+  int64_t* count;
+};
+
+void launch_noise(Launch L, float* out, int64_t n, uint64_t seed);
+void launch_convolve(Launch L, float2* nk, int n, double boxsize, const double* lk, const double* lp,
+                     int np, double post_scale);
+void launch_lpt1(Launch L, const float2* dk, float2* out, int n, double boxsize, double post_scale);
+void launch_phi(Launch L, const float2* dk, float2* out, int n, double boxsize, double post_scale);
+void launch_src2(Launch L, const float* phi, float* out, int64_t N);
+void launch_lpt2(Launch L, const float2* s2k, float2* out, int n, double boxsize, double post_scale);
+void launch_lapd(Launch L, const float2* dk, float2* out, int n, double boxsize, float post_scale);
+void launch_window(Launch L, const float2* dk, float2* out0, float2* out1, int n, double boxsize,
+                   double Rf, int wsmooth, double post_scale);
+void launch_hermitise(Launch L, float2* data, int n, int nbatch);
+void launch_pack(Launch L, float4* aos, const float* delta, const float* psi, const float* psi2, int n);
+
+struct PeakBuf {
+  unsigned long long* keys;   // (filter << 40) | lin
+  uint32_t* vals;
+  float* ff;                  // smoothed delta at the peak
+  float* lap;                 // k^2-weighted smoothed delta at the peak
+  int* count;
+  int64_t cap;
+};
+void launch_peakfind(Launch L, const float* ds, const float* ls, uint8_t* mask, int n1, int n2, int n3,
+                     int nbuff, float fcrit, int fidx, PeakBuf pb);
+
+int64_t shell_scratch_doubles_per_warp(int nshell);
+// comp: compensated single-precision sums (else double); adaptive: radial
+// truncation of the gather (else full spheres).  Persistent grid of
+// blocks x warps_per_block warps; a.scratch must hold one profile per warp.
+void launch_shell(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks, int warps_per_block);
+
+}  // namespace ppb

@@ -1,0 +1,550 @@
+// tile.cu — run_tile on one GPU (src/Pipeline.jl:66-325).
+//
+// Phase 0 (host): cosmology tables, fcrit = fsc_of_z(z_out), filter bank
+//   sorted by Rf descending, nhunt = min(nbuff-1, floor(1.75 Rfmax/alatt)).
+// Phase 1: Threefry noise -> R2C -> sqrt(P) -> C2R = delta; delta_k = R2C(delta);
+//   1LPT (3 C2R), 2LPT (6 C2R, src2, R2C, 3 C2R), Laplacian (ioutshear >= 1).
+// Phase 2: per filter (largest first): window -> C2R -> peak finder with a
+//   mask that persists across filters; peaks sorted to (filter, scan order).
+// Phase 4: radial-shell collapse per peak.
+// Record packing: RTHL > 0 (and z <= z_max on the lightcone), 11/33 floats.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "ppb_ctx.h"
+
+namespace ppb {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// device cosmology helpers (lightcone per-peak redshift, fcrit and D(z))
+// ---------------------------------------------------------------------------
+__device__ void dlinear_ab_dev(const DevCosmo& C, double ai, double* Dl, double* Da) {
+  const int ntab = C.ng;
+  if (ai > C.amin && ai < C.amax) {
+    int jlo = 0, jhi = ntab + 1;
+    while (jhi - jlo > 1) {
+      const int jm = (jhi + jlo) / 2;
+      if (ai > C.ga[jm - 1]) jlo = jm; else jhi = jm;
+    }
+    const int kk = jlo;
+    int nl, kkl;
+    if (kk < 2 || kk >= ntab) { nl = 2; kkl = kk - 1 > 1 ? kk - 1 : 1; } else { nl = 4; kkl = kk - 2; }
+    const double* xa = C.ga + kkl - 1;
+    const double* v1 = C.gD + kkl - 1;
+    const double x = ai;
+    double p1;
+    if (nl == 4) {
+      const double a1 = (x - xa[1]) / (xa[0] - xa[1]) * (x - xa[2]) / (xa[0] - xa[2]) * (x - xa[3]) / (xa[0] - xa[3]);
+      const double a2 = (x - xa[0]) / (xa[1] - xa[0]) * (x - xa[2]) / (xa[1] - xa[2]) * (x - xa[3]) / (xa[1] - xa[3]);
+      const double a3 = (x - xa[0]) / (xa[2] - xa[0]) * (x - xa[1]) / (xa[2] - xa[1]) * (x - xa[3]) / (xa[2] - xa[3]);
+      const double a4 = (x - xa[0]) / (xa[3] - xa[0]) * (x - xa[1]) / (xa[3] - xa[1]) * (x - xa[2]) / (xa[3] - xa[2]);
+      p1 = a1 * v1[0] + a2 * v1[1] + a3 * v1[2] + a4 * v1[3];
+    } else {
+      const double a1 = (x - xa[1]) / (xa[0] - xa[1]);
+      p1 = a1 * v1[0] + (1.0 - a1) * v1[1];
+    }
+    *Dl = p1 * ai;
+    *Da = p1;
+  } else if (ai >= C.amax) {
+    *Dl = C.D0 * ai; *Da = C.D0;
+  } else {
+    *Dl = C.Dinf * ai; *Da = C.Dinf;
+  }
+}
+
+// chi_to_z (Cosmology.jl:155-169)
+__device__ double chi_to_z_dev(const DevCosmo& C, double c) {
+  if (c <= C.chis[0]) return 0.0;
+  if (c >= C.chis[C.nchi - 1]) return C.chi_zmax;
+  int lo = 1, hi = C.nchi;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (C.chis[mid - 1] <= c) lo = mid; else hi = mid;
+  }
+  const double zl = C.chi_zmax * (double)(lo - 1) / (double)(C.nchi - 1);
+  const double zh = C.chi_zmax * (double)(hi - 1) / (double)(C.nchi - 1);
+  const double fr = (c - C.chis[lo - 1]) / (C.chis[hi - 1] - C.chis[lo - 1]);
+  return zl + fr * (zh - zl);
+}
+
+struct PrepArgs {
+  const unsigned long long* keys;
+  const uint32_t* vals;
+  const float* ff;
+  const float* lap;
+  int npk;
+  int n;
+  double alatt;
+  const double* fRf;
+  const int32_t* fir2;
+  int ievol;
+  double z_out, fcrit0;
+  double obs[3];
+  DevCosmo C;
+  int64_t* lin;
+  double* Rf;
+  int32_t* ir2;
+  double* Z;
+  double* fc;
+  float* FcRf;
+  float* d2Rf;
+  double* pos;   // 3 x npk
+};
+
+__global__ void prep_kernel(PrepArgs a) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= a.npk) return;
+  const unsigned long long key = a.keys[q];
+  const uint32_t slot = a.vals[q];
+  const int f = (int)(key >> 40);
+  const int64_t lin = (int64_t)(key & ((1ull << 40) - 1));
+  const int n = a.n;
+  const int i = (int)(lin % n) + 1, j = (int)((lin / n) % n) + 1, k = (int)(lin / ((int64_t)n * n)) + 1;
+  const double cen = 0.5 * (n + 1);
+  const double x = a.alatt * (i - cen), y = a.alatt * (j - cen), z = a.alatt * (k - cen);
+  a.lin[q] = lin;
+  a.Rf[q] = a.fRf[f];
+  a.ir2[q] = a.fir2[f];
+  a.FcRf[q] = a.ff[slot];
+  a.d2Rf[q] = a.lap[slot];
+  a.pos[q] = x;
+  a.pos[a.npk + q] = y;
+  a.pos[2 * a.npk + q] = z;
+  if (a.ievol == 1) {
+    const double dx = x - a.obs[0], dy = y - a.obs[1], dz = z - a.obs[2];
+    const double zpk = chi_to_z_dev(a.C, sqrt(dx * dx + dy * dy + dz * dz));
+    const double ZZ = 1.0 + zpk;
+    a.Z[q] = ZZ;
+    double Dl, Da;
+    dlinear_ab_dev(a.C, 1.0 / (1.0 + (ZZ - 1.0)), &Dl, &Da);
+    a.fc[q] = 1.686 * Dl;
+  } else {
+    a.Z[q] = 1.0 + a.z_out;
+    a.fc[q] = a.fcrit0;
+  }
+}
+
+struct RecArgs {
+  const double* res;
+  const double* pos;
+  const double* Rf;
+  const float* FcRf;
+  const float* d2Rf;
+  const double* Z;
+  int npk;
+  int ievol;
+  double z_max;
+  double alatt;
+  double Omnr, OL;
+  int ilpt;
+  int nf;
+  DevCosmo C;
+  int* flags;
+  const int* offs;
+  float* rec;
+  float* rthl;   // per record RTHL (for the max)
+};
+
+__global__ void flag_kernel(RecArgs a) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= a.npk) return;
+  const double R = a.res[(int64_t)q * RES_N];
+  bool ok = R > 0.0;
+  if (a.ievol == 1 && a.Z[q] - 1.0 > a.z_max) ok = false;
+  a.flags[q] = ok ? 1 : 0;
+}
+
+// record layout: Pipeline.jl:263-306, Catalog.jl:26-46
+__global__ void record_kernel(RecArgs a) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= a.npk || !a.flags[q]) return;
+  const double* r = a.res + (int64_t)q * RES_N;
+  const double ZZ = a.Z[q];
+  const double a_pk = 1.0 / ZZ;
+  double Dl, Dpk;
+  dlinear_ab_dev(a.C, a_pk, &Dl, &Dpk);   // third return value of Dlinear_ab (Pipeline.jl:259)
+  double v2f = 0.0;
+  if (a.ilpt >= 2) {
+    const double a3 = a_pk * a_pk * a_pk;
+    const double Oma = a.Omnr * a3 / (a.Omnr * a3 + a.OL);
+    v2f = -(-3.0 / 7.0 * pow(Oma, -1.0 / 143) * (Dpk * Dpk));
+  }
+  float* o = a.rec + (int64_t)a.offs[q] * a.nf;
+  o[0] = (float)a.pos[q];
+  o[1] = (float)a.pos[a.npk + q];
+  o[2] = (float)a.pos[2 * a.npk + q];
+  for (int L = 0; L < 3; L++) o[3 + L] = (float)(r[2 + L] * Dpk);
+  const float RTHLp = (float)(r[0] * a.alatt);
+  o[6] = RTHLp;
+  for (int L = 0; L < 3; L++) o[7 + L] = (float)(r[5 + L] * v2f);
+  o[10] = (float)r[23];
+  a.rthl[a.offs[q]] = RTHLp;
+  if (a.nf == 33) {
+    const double* s = r + 8;   // column-major strain
+    o[11] = (float)r[24];
+    o[12] = (float)r[25];
+    o[13] = (float)s[0];
+    o[14] = (float)s[4];
+    o[15] = (float)s[8];
+    o[16] = (float)s[1 + 3 * 2];
+    o[17] = (float)s[0 + 3 * 2];
+    o[18] = (float)s[0 + 3 * 1];
+    o[19] = (float)r[30];
+    o[20] = (float)r[26];
+    for (int L = 0; L < 3; L++) {
+      o[21 + L] = (float)r[17 + L];
+      o[24 + L] = (float)r[27 + L];
+    }
+    o[27] = (float)a.Rf[q];
+    o[28] = a.FcRf[q];
+    o[29] = a.d2Rf[q];
+    for (int L = 0; L < 3; L++) o[30 + L] = (float)r[20 + L];
+  }
+}
+
+__global__ void zero_counters(unsigned long long* c, int nc, int* q, int* pcount) {
+  const int t = threadIdx.x;
+  if (t < nc) c[t] = 0;
+  if (t == 0) {
+    if (q) *q = 0;
+    if (pcount) *pcount = 0;
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// plans and buffers for one grid size
+// ---------------------------------------------------------------------------
+static cufftHandle make_plan(int n, cufftType t, int batch) {
+  cufftHandle h;
+  int dims[3] = {n, n, n};
+  PPB_CUFFT(cufftPlanMany(&h, 3, dims, nullptr, 1, 0, nullptr, 1, 0, t, batch));
+  return h;
+}
+
+TileRes::~TileRes() {
+  for (cufftHandle h : {r2c, c2r1, c2r2, c2r3, c2r6})
+    if (h) cufftDestroy(h);
+}
+
+void TileRes::setup(int nn, cudaStream_t s) {
+  if (n == nn) return;
+  for (cufftHandle* h : {&r2c, &c2r1, &c2r2, &c2r3, &c2r6})
+    if (*h) { cufftDestroy(*h); *h = 0; }
+  n = nn;
+  const int64_t N = (int64_t)n * n * n, M = (int64_t)(n / 2 + 1) * n * n;
+  r2c = make_plan(n, CUFFT_R2C, 1);
+  c2r1 = make_plan(n, CUFFT_C2R, 1);
+  c2r2 = make_plan(n, CUFFT_C2R, 2);
+  c2r3 = make_plan(n, CUFFT_C2R, 3);
+  c2r6 = make_plan(n, CUFFT_C2R, 6);
+  for (cufftHandle h : {r2c, c2r1, c2r2, c2r3, c2r6}) PPB_CUFFT(cufftSetStream(h, s));
+  delta.ensure(N * 4);
+  dk.ensure(M * 8);
+  psi.ensure(3 * N * 4);
+  psi2.ensure(3 * N * 4);
+  lapd.ensure(N * 4);
+  aos.ensure(N * 32);
+  kw.ensure(6 * M * 8);
+  rw.ensure(6 * N * 4);
+  mask.ensure(N);
+  count.ensure(64);
+}
+
+void TileRes::ensure_peaks(int64_t c) {
+  if (c <= cap) return;
+  cap = c;
+  keys.ensure(cap * 8);
+  vals.ensure(cap * 4);
+  ff.ensure(cap * 4);
+  lap.ensure(cap * 4);
+  keys_s.ensure(cap * 8);
+  vals_s.ensure(cap * 4);
+  p_lin.ensure(cap * 8);
+  p_Rf.ensure(cap * 8);
+  p_ir2.ensure(cap * 4);
+  p_Z.ensure(cap * 8);
+  p_fc.ensure(cap * 8);
+  p_FcRf.ensure(cap * 4);
+  p_d2Rf.ensure(cap * 4);
+  p_pos.ensure(cap * 24);
+  res.ensure(cap * RES_N * 8);
+  flags.ensure(cap * 4 + 4);
+  offs.ensure(cap * 4 + 4);
+  rec.ensure(cap * 33 * 4);
+  rthl.ensure(cap * 4);
+  size_t t1 = 0, t2 = 0;
+  PPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, t1, keys.as<unsigned long long>(), keys_s.as<unsigned long long>(),
+                                           vals.as<uint32_t>(), vals_s.as<uint32_t>(), (int)cap, 0, 64));
+  PPB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t2, flags.as<int>(), offs.as<int>(), (int)cap + 1));
+  size_t t3 = 0;
+  PPB_CUDA(cub::DeviceReduce::Max(nullptr, t3, rthl.as<float>(), rthl.as<float>(), (int)cap));
+  tmp.ensure(std::max(std::max(t1, t2), t3) + 256);
+}
+
+// ---------------------------------------------------------------------------
+// the pipeline
+// ---------------------------------------------------------------------------
+static void check_params(const ppb_tile_params* p, const double* Rf, int nfilt) {
+  PPB_REQUIRE(p != nullptr, "params is null");
+  PPB_REQUIRE(p->n >= 8 && p->n <= 2048, "n must be in [8, 2048]");
+  PPB_REQUIRE(p->boxsize > 0, "boxsize must be positive");
+  PPB_REQUIRE(p->nbuff >= 2 && 2 * p->nbuff < p->n, "nbuff must satisfy 2 <= nbuff and 2 nbuff < n");
+  PPB_REQUIRE(Rf != nullptr && nfilt >= 1 && nfilt <= 4096, "need 1..4096 filter radii");
+  for (int i = 0; i < nfilt; i++) PPB_REQUIRE(Rf[i] > 0, "filter radii must be positive");
+  PPB_REQUIRE(p->ilpt == 1 || p->ilpt == 2, "ilpt must be 1 or 2");
+  PPB_REQUIRE(p->wsmooth == 0 || p->wsmooth == 1 || p->wsmooth == 3, "wsmooth must be 0, 1 or 3");
+  PPB_REQUIRE(p->ievol == 0 || p->ievol == 1, "ievol must be 0 or 1");
+  if (p->rmax2rs != 0.0)
+    throw Error{PPB_ERR_UNSUPPORTED,
+                "rmax2rs > 0 is not supported: the reference's result then depends on thread scheduling "
+                "(mask writes of RadialShell.jl:793-802 race with the pre-mask read at :311-316)"};
+}
+
+int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, int nfilt, ppb_halo_buf* out,
+                  float* device_ms) {
+  check_params(p, Rf_in, nfilt);
+  PPB_REQUIRE(ctx->pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
+  PPB_REQUIRE(ctx->has_tab, "collapse table not set (ppb_set_collapse_table)");
+  PPB_REQUIRE(out != nullptr, "output buffer is null");
+  cudaStream_t s = ctx->stream;
+  Launch L{s, &ctx->launches};
+  const int n = p->n;
+  const double box = p->boxsize, alatt = box / n;
+  const double Om = p->Omx + p->OmB;
+  const int64_t N = (int64_t)n * n * n, M = (int64_t)(n / 2 + 1) * n * n;
+  const bool plain = p->plain != 0;
+
+  // ---- phase 0 (host) ----
+  std::vector<double> Rf(Rf_in, Rf_in + nfilt);
+  std::stable_sort(Rf.begin(), Rf.end(), [](double a, double b) { return a > b; });
+  const GrowthTable& G = ctx->growth(Om, p->OmB, p->Omvac, p->h);
+  const double fcrit_val = fsc_of_z(G, p->z_out);
+  const float fcrit = (float)fcrit_val;
+  const int nhunt = std::min(p->nbuff - 1, (int)std::floor(Rf[0] * 1.75 / alatt));
+  PPB_REQUIRE(nhunt >= 1, "nhunt = min(nbuff-1, floor(1.75 Rfmax/alatt)) must be >= 1");
+  build_shell_table(ctx->shells, nhunt);
+  upload_shell_table(ctx->shells, s);
+  std::vector<int32_t> fir2(nfilt);
+  for (int f = 0; f < nfilt; f++)
+    fir2[f] = (int32_t)std::min(std::floor((1.75 * Rf[f] / alatt) * (1.75 * Rf[f] / alatt)),
+                                std::floor((40.0 / alatt - 1) * (40.0 / alatt - 1)));
+  DevCosmo C = ctx->dev_cosmo(G, Om, p->Omvac, p->h, p->ievol == 1 ? p->z_max + 1.0 : 0.0, p->ievol == 1);
+  ctx->filt_Rf.ensure(nfilt * 8);
+  ctx->filt_ir2.ensure(nfilt * 4);
+  PPB_CUDA(cudaMemcpyAsync(ctx->filt_Rf.p, Rf.data(), nfilt * 8, cudaMemcpyHostToDevice, s));
+  PPB_CUDA(cudaMemcpyAsync(ctx->filt_ir2.p, fir2.data(), nfilt * 4, cudaMemcpyHostToDevice, s));
+
+  TileRes& T = ctx->tile(n);
+  T.setup(n, s);
+  if (T.cap == 0) T.ensure_peaks(std::max<int64_t>(1 << 16, std::min<int64_t>(N / 64, 1 << 22)));
+
+  cudaEvent_t* ev = ctx->stage_ev;
+  PPB_CUDA(cudaEventRecord(ev[0], s));
+  const double inv_n3 = 1.0 / (double)N;
+  float2* dkp = T.dk.as<float2>();
+  float2* kw = T.kw.as<float2>();
+  float* rw = T.rw.as<float>();
+
+  // ---- phase 1: fields ----
+  launch_noise(L, T.rw.as<float>(), n, p->seed);
+  PPB_CUFFT(cufftExecR2C(T.r2c, T.rw.as<cufftReal>(), (cufftComplex*)kw));
+  launch_convolve(L, kw, n, box, ctx->pk_lk.as<double>(), ctx->pk_lp.as<double>(), ctx->pk_n, inv_n3);
+  launch_hermitise(L, kw, n, 1);
+  PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)kw, T.delta.as<cufftReal>()));
+  PPB_CUFFT(cufftExecR2C(T.r2c, T.delta.as<cufftReal>(), (cufftComplex*)dkp));
+  // 1LPT
+  launch_lpt1(L, dkp, kw, n, box, inv_n3);
+  launch_hermitise(L, kw, n, 3);
+  if (plain) {
+    for (int c = 0; c < 3; c++)
+      PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)(kw + c * M), T.psi.as<cufftReal>() + c * N));
+  } else {
+    PPB_CUFFT(cufftExecC2R(T.c2r3, (cufftComplex*)kw, T.psi.as<cufftReal>()));
+  }
+  // 2LPT
+  if (p->ilpt >= 2) {
+    launch_phi(L, dkp, kw, n, box, inv_n3);
+    launch_hermitise(L, kw, n, 6);
+    if (plain) {
+      for (int c = 0; c < 6; c++) PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)(kw + c * M), rw + c * N));
+    } else {
+      PPB_CUFFT(cufftExecC2R(T.c2r6, (cufftComplex*)kw, rw));
+    }
+    launch_src2(L, rw, T.lapd.as<float>(), N);   // lapd buffer as scratch for src2
+    PPB_CUFFT(cufftExecR2C(T.r2c, T.lapd.as<cufftReal>(), (cufftComplex*)kw));
+    launch_lpt2(L, kw, kw + M, n, box, inv_n3);
+    launch_hermitise(L, kw + M, n, 3);
+    if (plain) {
+      for (int c = 0; c < 3; c++)
+        PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)(kw + (1 + c) * M), T.psi2.as<cufftReal>() + c * N));
+    } else {
+      PPB_CUFFT(cufftExecC2R(T.c2r3, (cufftComplex*)(kw + M), T.psi2.as<cufftReal>()));
+    }
+  }
+  // Laplacian field (Pipeline.jl:35-51): irfft(k^2 delta_k) / n^3
+  const bool want_lap = p->ioutshear >= 1;
+  if (want_lap) {
+    launch_lapd(L, dkp, kw, n, box, (float)(inv_n3 * inv_n3));
+    launch_hermitise(L, kw, n, 1);
+    PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)kw, T.lapd.as<cufftReal>()));
+  }
+  launch_pack(L, T.aos.as<float4>(), T.delta.as<float>(), T.psi.as<float>(),
+              p->ilpt >= 2 ? T.psi2.as<float>() : nullptr, n);
+  PPB_CUDA(cudaEventRecord(ev[1], s));
+
+  // ---- phase 2: filter bank and peaks ----
+  int64_t npk = 0;
+  for (int attempt = 0; attempt < 2; attempt++) {
+    PPB_CUDA(cudaMemsetAsync(T.mask.p, 0, N, s));
+    PPB_CUDA(cudaMemsetAsync(T.count.p, 0, 64, s));
+    PeakBuf pb{T.keys.as<unsigned long long>(), T.vals.as<uint32_t>(), T.ff.as<float>(), T.lap.as<float>(),
+               T.count.as<int>(), T.cap};
+    for (int f = 0; f < nfilt; f++) {
+      float2* o1 = want_lap ? kw + M : nullptr;
+      launch_window(L, dkp, kw, o1, n, box, Rf[f], p->wsmooth, inv_n3);
+      launch_hermitise(L, kw, n, want_lap ? 2 : 1);
+      if (want_lap && !plain) {
+        PPB_CUFFT(cufftExecC2R(T.c2r2, (cufftComplex*)kw, rw));
+      } else {
+        PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)kw, rw));
+        if (want_lap) PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)(kw + M), rw + N));
+      }
+      launch_peakfind(L, rw, want_lap ? rw + N : nullptr, T.mask.as<uint8_t>(), n, n, n, p->nbuff, fcrit, f, pb);
+    }
+    int cnt = 0;
+    PPB_CUDA(cudaMemcpyAsync(&cnt, T.count.p, 4, cudaMemcpyDeviceToHost, s));
+    PPB_CUDA(cudaStreamSynchronize(s));
+    npk = cnt;
+    if (npk <= T.cap) break;
+    PPB_REQUIRE(attempt == 0, "peak capacity exceeded twice");
+    T.ensure_peaks((int64_t)(npk * 1.25) + 1024);   // grow and redo the filter bank
+  }
+  PPB_CUDA(cudaEventRecord(ev[2], s));
+
+  // ---- sort peaks to (filter, scan order), per-peak parameters ----
+  int fbits = 1;
+  while ((1 << fbits) < nfilt) fbits++;
+  if (npk > 0) {
+    size_t tb = T.tmp.bytes;
+    PPB_CUDA(cub::DeviceRadixSort::SortPairs(T.tmp.p, tb, T.keys.as<unsigned long long>(),
+                                             T.keys_s.as<unsigned long long>(), T.vals.as<uint32_t>(),
+                                             T.vals_s.as<uint32_t>(), (int)npk, 0, 40 + fbits, s));
+    ctx->launches++;
+    PrepArgs pa{};
+    pa.keys = T.keys_s.as<unsigned long long>();
+    pa.vals = T.vals_s.as<uint32_t>();
+    pa.ff = T.ff.as<float>();
+    pa.lap = T.lap.as<float>();
+    pa.npk = (int)npk;
+    pa.n = n;
+    pa.alatt = alatt;
+    pa.fRf = ctx->filt_Rf.as<double>();
+    pa.fir2 = ctx->filt_ir2.as<int32_t>();
+    pa.ievol = p->ievol;
+    pa.z_out = p->z_out;
+    pa.fcrit0 = fcrit_val;
+    pa.obs[0] = p->cenx; pa.obs[1] = p->ceny; pa.obs[2] = p->cenz;
+    pa.C = C;
+    pa.lin = T.p_lin.as<int64_t>();
+    pa.Rf = T.p_Rf.as<double>();
+    pa.ir2 = T.p_ir2.as<int32_t>();
+    pa.Z = T.p_Z.as<double>();
+    pa.fc = T.p_fc.as<double>();
+    pa.FcRf = T.p_FcRf.as<float>();
+    pa.d2Rf = T.p_d2Rf.as<float>();
+    pa.pos = T.p_pos.as<double>();
+    prep_kernel<<<(unsigned)((npk + 255) / 256), 256, 0, s>>>(pa);
+    PPB_LAUNCHED(ctx->launches);
+  }
+
+  // ---- phase 4: shells ----
+  ShellStats st{};
+  if (npk > 0) {
+    ShellArgs a = ctx->shell_args(n, alatt, T.aos.as<float4>(), want_lap ? T.lapd.as<float>() : nullptr);
+    a.pk = PeakParams{T.p_lin.as<int64_t>(), T.p_Rf.as<double>(), T.p_ir2.as<int32_t>(), T.p_Z.as<double>(),
+                      T.p_fc.as<double>()};
+    a.npk = npk;
+    a.out = T.res.as<double>();
+    ctx->run_shells(a, !plain, !plain, &st);
+  }
+  PPB_CUDA(cudaEventRecord(ev[3], s));
+
+  // ---- records ----
+  const int nf = p->ioutshear >= 1 ? 33 : 11;
+  int64_t nrec = 0;
+  float rmax = 0.f;
+  if (npk > 0) {
+    RecArgs r{};
+    r.res = T.res.as<double>();
+    r.pos = T.p_pos.as<double>();
+    r.Rf = T.p_Rf.as<double>();
+    r.FcRf = T.p_FcRf.as<float>();
+    r.d2Rf = T.p_d2Rf.as<float>();
+    r.Z = T.p_Z.as<double>();
+    r.npk = (int)npk;
+    r.ievol = p->ievol;
+    r.z_max = p->z_max;
+    r.alatt = alatt;
+    r.Omnr = Om;
+    r.OL = p->Omvac;
+    r.ilpt = p->ilpt;
+    r.nf = nf;
+    r.C = C;
+    r.flags = T.flags.as<int>();
+    r.offs = T.offs.as<int>();
+    r.rec = T.rec.as<float>();
+    r.rthl = T.rthl.as<float>();
+    const unsigned gb = (unsigned)((npk + 255) / 256);
+    flag_kernel<<<gb, 256, 0, s>>>(r);
+    PPB_LAUNCHED(ctx->launches);
+    PPB_CUDA(cudaMemsetAsync(T.flags.as<int>() + npk, 0, 4, s));
+    size_t tb = T.tmp.bytes;
+    PPB_CUDA(cub::DeviceScan::ExclusiveSum(T.tmp.p, tb, T.flags.as<int>(), T.offs.as<int>(), (int)npk + 1, s));
+    ctx->launches++;
+    record_kernel<<<gb, 256, 0, s>>>(r);
+    PPB_LAUNCHED(ctx->launches);
+    int nr = 0;
+    PPB_CUDA(cudaMemcpyAsync(&nr, T.offs.as<int>() + npk, 4, cudaMemcpyDeviceToHost, s));
+    PPB_CUDA(cudaStreamSynchronize(s));
+    nrec = nr;
+    if (nrec > 0) {
+      size_t tb2 = T.tmp.bytes;
+      float* dmax = T.count.as<float>() + 8;
+      PPB_CUDA(cub::DeviceReduce::Max(T.tmp.p, tb2, T.rthl.as<float>(), dmax, (int)nrec, s));
+      ctx->launches++;
+      PPB_CUDA(cudaMemcpyAsync(&rmax, dmax, 4, cudaMemcpyDeviceToHost, s));
+    }
+  }
+  PPB_CUDA(cudaEventRecord(ev[4], s));
+  PPB_CUDA(cudaStreamSynchronize(s));
+  if (st.guard != 0)
+    throw Error{PPB_ERR_CUDA, "shell truncation guard tripped: a profile read beyond the gathered shells"};
+  if (st.akk != 0)
+    throw Error{PPB_ERR_INVALID, "kernel_strain SPH table index out of range (the reference raises here too)"};
+
+  out->nfields = nf;
+  out->count = nrec;
+  out->npeaks = npk;
+  out->RTHLmax = nrec > 0 ? rmax : 0.f;
+  ctx->last_visits = st.visits;
+  ctx->last_npk = npk;
+  float ms[4];
+  for (int i = 0; i < 4; i++) PPB_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+  std::memcpy(ctx->stage_ms, ms, sizeof(ms));
+  if (device_ms) *device_ms = ms[0] + ms[1] + ms[2] + ms[3];
+  if (nrec > out->capacity) return PPB_ERR_CAPACITY;
+  if (nrec > 0) {
+    PPB_REQUIRE(out->records != nullptr, "records buffer is null");
+    copy_out(out->records, T.rec.p, (size_t)nrec * nf * 4, s);
+  }
+  return PPB_OK;
+}
+
+}  // namespace ppb

@@ -1,0 +1,522 @@
+"""peakpatch_b200 — Python host mirror of PeakPatch.jl's per-tile halo-finding
+API over the C-ABI library libppb.so (sm_100a CUDA).
+
+Names, argument meanings and error behaviour follow the reference
+(PeakPatch.jl):
+
+  PipelineConfig            src/IO/Parameters.jl:17-125 (kwdef + TOML)
+  run_tile(cfg; seed)       src/Pipeline.jl:66-325
+  fill_noise_threefry!      src/InitialConditions/RandomField.jl:70-83
+  find_peaks                src/HaloFinder/PeakFind.jl:123-186
+  analyse_peak (batched)    src/HaloFinder/RadialShell.jl:282-891
+  read_homeltab             src/EllipsoidalCollapse/CollapseTable.jl:102-122
+  read_filterbank           src/HaloFinder/Filters.jl:46-58
+  load_pk (table part)      src/InitialConditions/PowerSpectrum.jl:189-201
+  write_pksc / read_pksc    src/IO/Catalog.jl:53-160
+
+Arrays are numpy arrays in C order with shape (n3, n2, n1), which is the
+memory layout of Julia's column-major Array{Float32,3} of size (n1, n2, n3);
+peak indices i, j, k, ipp are 1-based as in the reference.  All compute runs
+in libppb.so on a CUDA device; there is no CPU fallback: without the library
+or a GPU the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import struct
+from dataclasses import dataclass, field, fields, replace
+from typing import Optional, Sequence
+
+import numpy as np
+
+__all__ = [
+    "PipelineConfig", "Context", "run_tile", "fill_noise_threefry", "find_peaks", "analyse_peaks",
+    "read_homeltab", "read_filterbank", "read_pk_table", "write_pksc", "read_pksc", "PPBError",
+    "library_path", "load_library", "EXT_FIELDS", "BASIC_FIELDS", "RESULT_FIELDS",
+]
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(os.path.dirname(_PKG), "libppb.so")
+
+BASIC_FIELDS = ("x", "y", "z", "vx", "vy", "vz", "RTHL", "vx2", "vy2", "vz2", "overdensity")
+EXT_FIELDS = BASIC_FIELDS + (
+    "e_v", "p_v", "strain_11", "strain_22", "strain_33", "strain_23", "strain_13", "strain_12",
+    "d2F", "zform", "grad_x", "grad_y", "grad_z", "gradf_x", "gradf_y", "gradf_z", "Rf",
+    "FcollvRf", "d2FRf", "gradrf_x", "gradrf_y", "gradrf_z")
+# per-peak analyse_peak output layout (31 doubles), see include/ppb.h
+RESULT_FIELDS = {"RTHL": 0, "Srb": 1, "Sbar": slice(2, 5), "Sbar2": slice(5, 8), "strain": slice(8, 17),
+                 "gradpk": slice(17, 20), "gradpkrf": slice(20, 23), "Fbarx": 23, "e_v": 24, "p_v": 25,
+                 "zvir_half": 26, "gradpkf": slice(27, 30), "d2F": 30}
+
+PPB_OK = 0
+_ERRNAMES = {-1: "INVALID", -2: "CUDA", -3: "NOMEM", -4: "ADMISSION", -5: "TIMEOUT", -6: "UNSUPPORTED",
+             -7: "CAPACITY", -8: "NOT_FOUND"}
+
+
+class PPBError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libppb error {code} ({_ERRNAMES.get(code, '?')}): {msg}")
+        self.code = code
+
+
+# --------------------------------------------------------------------------
+# library loading
+# --------------------------------------------------------------------------
+class _TileParams(ctypes.Structure):
+    _fields_ = [("Omx", ctypes.c_double), ("OmB", ctypes.c_double), ("Omvac", ctypes.c_double),
+                ("h", ctypes.c_double), ("n", ctypes.c_int32), ("boxsize", ctypes.c_double),
+                ("nbuff", ctypes.c_int32), ("z_out", ctypes.c_double), ("z_max", ctypes.c_double),
+                ("ievol", ctypes.c_int32), ("cenx", ctypes.c_double), ("ceny", ctypes.c_double),
+                ("cenz", ctypes.c_double), ("ilpt", ctypes.c_int32), ("ioutshear", ctypes.c_int32),
+                ("wsmooth", ctypes.c_int32), ("rmax2rs", ctypes.c_double), ("seed", ctypes.c_uint64),
+                ("plain", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7)]
+
+
+class _HaloBuf(ctypes.Structure):
+    _fields_ = [("records", ctypes.c_void_p), ("capacity", ctypes.c_int64), ("count", ctypes.c_int64),
+                ("nfields", ctypes.c_int32), ("RTHLmax", ctypes.c_float), ("npeaks", ctypes.c_int64)]
+
+
+_lib = None
+
+# every function include/ppb.h declares (checked by the CPU test suite)
+EXPORTED = (
+    "ppb_ctx_create", "ppb_ctx_destroy", "ppb_last_error", "ppb_abi_version", "ppb_set_collapse_table",
+    "ppb_set_pk_table", "ppb_run_tile", "ppb_run_tile_timed", "ppb_write_pksc", "ppb_noise_threefry",
+    "ppb_find_peaks", "ppb_analyse_peaks", "ppb_event_record", "ppb_event_elapsed", "ppb_synchronize",
+    "ppb_launch_count", "ppb_last_shell_stats", "ppb_last_stage_ms", "ppb_alloc_host", "ppb_free_host",
+    "ppb_alloc_device", "ppb_free_device",
+)
+
+
+def library_path() -> str:
+    return os.environ.get("PPB_LIBRARY", _LIB_PATH)
+
+
+def load_library():
+    """Load libppb.so (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise PPBError(-1, f"{path} not found: build it with `python peakpatch.jl_b200/build.py`")
+    L = ctypes.CDLL(path)
+    P, I32, I64, D = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    L.ppb_ctx_create.argtypes = [I32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]
+    L.ppb_ctx_destroy.argtypes = [P]
+    L.ppb_last_error.argtypes = [P, ctypes.c_char_p, ctypes.c_size_t]
+    L.ppb_set_collapse_table.argtypes = [P, P, I32, I32, I32, D, D, D, D, D, D]
+    L.ppb_set_pk_table.argtypes = [P, P, P, I32]
+    L.ppb_run_tile.argtypes = [P, ctypes.POINTER(_TileParams), P, I32, ctypes.POINTER(_HaloBuf)]
+    L.ppb_run_tile_timed.argtypes = [P, ctypes.POINTER(_TileParams), P, I32, ctypes.POINTER(_HaloBuf),
+                                     ctypes.POINTER(ctypes.c_float)]
+    L.ppb_write_pksc.argtypes = [ctypes.c_char_p, P, I64, I32, ctypes.c_float, ctypes.c_float]
+    L.ppb_noise_threefry.argtypes = [P, P, I32, ctypes.c_uint64]
+    L.ppb_find_peaks.argtypes = [P, P, P, I32, I32, I32, I32, ctypes.c_float, I64, P, P, P, P, P,
+                                 ctypes.POINTER(ctypes.c_int64)]
+    L.ppb_analyse_peaks.argtypes = [P] * 9 + [I32, I32, I64, P, P, P, P, P, D, I32, P]
+    L.ppb_event_record.argtypes = [P, I32]
+    L.ppb_event_elapsed.argtypes = [P, I32, I32, ctypes.POINTER(ctypes.c_float)]
+    L.ppb_synchronize.argtypes = [P]
+    L.ppb_launch_count.argtypes = [P, ctypes.POINTER(ctypes.c_int64)]
+    L.ppb_last_shell_stats.argtypes = [P, ctypes.POINTER(ctypes.c_int64), P, ctypes.POINTER(ctypes.c_float)]
+    L.ppb_last_stage_ms.argtypes = [P, P]
+    for f in ("ppb_alloc_host", "ppb_alloc_device"):
+        getattr(L, f).argtypes = [P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
+    for f in ("ppb_free_host", "ppb_free_device"):
+        getattr(L, f).argtypes = [P, P]
+    _lib = L
+    return L
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+# --------------------------------------------------------------------------
+# PipelineConfig (src/IO/Parameters.jl:17-125)
+# --------------------------------------------------------------------------
+@dataclass
+class PipelineConfig:
+    Omx: float = 0.266
+    OmB: float = 0.049
+    Omvac: float = 0.685
+    h: float = 0.674
+    n: int = 142
+    boxsize: float = 200.0
+    nbuff: int = 4
+    z_out: float = 0.0
+    z_max: float = 0.0
+    ievol: int = 0
+    cenx: float = 0.0
+    ceny: float = 0.0
+    cenz: float = 0.0
+    ilpt: int = 2
+    ioutshear: int = 0
+    wsmooth: int = 0
+    rmax2rs: float = 1.0
+    NonGauss: int = 0
+    fNL: float = 0.0
+    pkfile: str = "pk.dat"
+    filterfile: str = "filters.dat"
+    tabfile: str = "HomelTab.dat"
+    fileout: str = "catalog.pksc"
+
+    @classmethod
+    def from_toml(cls, config: dict) -> "PipelineConfig":
+        """PipelineConfig(config::Dict) of Parameters.jl:88-125."""
+        cosmo, grid, run, files = (config.get(k, {}) for k in ("cosmology", "grid", "run", "files"))
+        Om_total = float(cosmo.get("Om", 0.315))
+        OmB = float(cosmo.get("OB", 0.049))
+        z_out = float(run.get("z_out", 0.0))
+        return cls(Omx=Om_total - OmB, OmB=OmB, Omvac=float(cosmo.get("OL", 0.685)), h=float(cosmo.get("h", 0.674)),
+                   n=int(grid.get("n", 142)), boxsize=float(grid.get("boxsize", grid.get("dL_box", 200.0))),
+                   nbuff=int(grid.get("nbuff", 4)), z_out=z_out, z_max=float(run.get("z_max", z_out)),
+                   ievol=int(run.get("ievol", 0)), cenx=float(grid.get("cenx", 0.0)),
+                   ceny=float(grid.get("ceny", 0.0)), cenz=float(grid.get("cenz", 0.0)),
+                   ilpt=int(run.get("ilpt", 2)), ioutshear=int(run.get("ioutshear", 0)),
+                   wsmooth=int(run.get("wsmooth", 0)), rmax2rs=float(run.get("rmax2rs", 1.0)),
+                   NonGauss=int(run.get("NonGauss", 0)), fNL=float(run.get("fNL", 0.0)),
+                   pkfile=files.get("pk", "pk.dat"), filterfile=files.get("filterbank", "filters.dat"),
+                   tabfile=files.get("homeltab", "HomelTab.dat"), fileout=files.get("output", "catalog.pksc"))
+
+    @classmethod
+    def from_toml_file(cls, path: str) -> "PipelineConfig":
+        import tomllib
+        with open(path, "rb") as f:
+            return cls.from_toml(tomllib.load(f))
+
+
+# --------------------------------------------------------------------------
+# file formats
+# --------------------------------------------------------------------------
+@dataclass
+class CollapseTable:
+    data: np.ndarray          # float32 (Nz, Ny, Nx) C order == column-major (Nx, Ny, Nz)
+    X1: float
+    X2: float
+    Y1: float
+    Y2: float
+    Z1: float
+    Z2: float
+
+    @property
+    def shape_xyz(self):
+        nz, ny, nx = self.data.shape
+        return nx, ny, nz
+
+
+def read_homeltab(path: str) -> CollapseTable:
+    """36-byte header (3 Int32, 6 Float32) + Float32 column-major table."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    nx, ny, nz = struct.unpack("<3i", raw[:12])
+    x1, x2, y1, y2, z1, z2 = (float(v) for v in struct.unpack("<6f", raw[12:36]))
+    need = 36 + 4 * nx * ny * nz
+    if len(raw) < need:
+        raise ValueError(f"{path}: truncated collapse table ({len(raw)} < {need} bytes)")
+    data = np.frombuffer(raw[36:need], dtype="<f4").reshape(nz, ny, nx).copy()
+    return CollapseTable(data, x1, x2, y1, y2, z1, z2)
+
+
+def write_homeltab(path: str, t: CollapseTable) -> None:
+    nx, ny, nz = t.shape_xyz
+    with open(path, "wb") as f:
+        f.write(struct.pack("<3i", nx, ny, nz))
+        f.write(struct.pack("<6f", t.X1, t.X2, t.Y1, t.Y2, t.Z1, t.Z2))
+        f.write(np.ascontiguousarray(t.data, dtype="<f4").tobytes())
+
+
+def read_filterbank(path: str):
+    """Returns [(id, fcrit, Rf), ...] in file order."""
+    with open(path) as f:
+        lines = f.read().splitlines()
+    nic = int(lines[0].strip())
+    out = []
+    for i in range(nic):
+        p = lines[i + 1].split()
+        out.append((int(p[0]), float(p[1]), float(p[2])))
+    return out
+
+
+def write_filterbank(path: str, Rfs: Sequence[float], fcrit: float = 1.686) -> None:
+    with open(path, "w") as f:
+        f.write(f"{len(Rfs)}\n")
+        for i, R in enumerate(Rfs):
+            f.write(f"{i + 1}  {fcrit}  {R!r}\n")
+
+
+def read_pk_table(path: str):
+    d = np.loadtxt(path, comments="#")
+    return np.ascontiguousarray(d[:, 0], np.float64), np.ascontiguousarray(d[:, 1], np.float64)
+
+
+def write_pksc(path: str, records: np.ndarray, RTHLmax: float, z_out: float) -> None:
+    rec = np.ascontiguousarray(records, dtype="<f4")
+    with open(path, "wb") as f:
+        f.write(struct.pack("<i", rec.shape[0]))
+        f.write(struct.pack("<f", RTHLmax))
+        f.write(struct.pack("<f", z_out))
+        f.write(rec.tobytes())
+
+
+def read_pksc(path: str):
+    """Returns (records (N, 11|33) float32, RTHLmax, z_out); the field count
+    is inferred from the file size as Catalog.jl:100-120 does."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    nh = struct.unpack("<i", raw[:4])[0]
+    rthl, zo = struct.unpack("<2f", raw[4:12])
+    nf = (len(raw) - 12) // (nh * 4) if nh > 0 else 11
+    rec = np.frombuffer(raw[12:12 + 4 * nh * nf], dtype="<f4").reshape(nh, nf).copy()
+    return rec, rthl, zo
+
+
+# --------------------------------------------------------------------------
+# context
+# --------------------------------------------------------------------------
+class Context:
+    """One libppb context on one CUDA device (tables stay resident)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self.L = load_library()
+        h = ctypes.c_void_p()
+        rc = self.L.ppb_ctx_create(device, hbm_budget, ctypes.byref(h))
+        if rc != PPB_OK:
+            raise PPBError(rc, "ppb_ctx_create failed (is a CUDA device visible?)")
+        self.h = h
+        self._table_key = None
+        self._pk_key = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ppb_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != PPB_OK:
+            buf = ctypes.create_string_buffer(1024)
+            self.L.ppb_last_error(self.h, buf, 1024)
+            raise PPBError(rc, buf.value.decode(errors="replace"))
+
+    # tables
+    def set_collapse_table(self, t: CollapseTable):
+        key = (id(t.data), t.data.shape)
+        if key == self._table_key:
+            return
+        d = np.ascontiguousarray(t.data, dtype=np.float32)
+        nz, ny, nx = d.shape
+        self._check(self.L.ppb_set_collapse_table(self.h, _p(d), nx, ny, nz, t.X1, t.X2, t.Y1, t.Y2, t.Z1, t.Z2))
+        self._table_key = key
+
+    def set_pk_table(self, k: np.ndarray, pk: np.ndarray):
+        k = np.ascontiguousarray(k, np.float64)
+        pk = np.ascontiguousarray(pk, np.float64)
+        self._check(self.L.ppb_set_pk_table(self.h, _p(k), _p(pk), len(k)))
+
+    def launch_count(self) -> int:
+        c = ctypes.c_int64()
+        self._check(self.L.ppb_launch_count(self.h, ctypes.byref(c)))
+        return c.value
+
+    def shell_stats(self):
+        v = ctypes.c_int64()
+        d = np.zeros(5, np.int64)
+        ms = ctypes.c_float()
+        self._check(self.L.ppb_last_shell_stats(self.h, ctypes.byref(v), _p(d), ctypes.byref(ms)))
+        return {"visits": v.value, "dumps": dict(zip(("premask", "no_fcrit", "m0_one", "no_collapse", "rthl_neg"),
+                                                      d.tolist())), "ms": ms.value}
+
+    def stage_ms(self):
+        a = np.zeros(4, np.float32)
+        self._check(self.L.ppb_last_stage_ms(self.h, _p(a)))
+        return dict(zip(("fields", "peaks", "shells", "records"), a.tolist()))
+
+    def event_record(self, slot: int):
+        self._check(self.L.ppb_event_record(self.h, slot))
+
+    def event_elapsed(self, a: int, b: int) -> float:
+        ms = ctypes.c_float()
+        self._check(self.L.ppb_event_elapsed(self.h, a, b, ctypes.byref(ms)))
+        return ms.value
+
+    def synchronize(self):
+        self._check(self.L.ppb_synchronize(self.h))
+
+    # ---- memory helpers ----
+    def alloc_host(self, nbytes: int) -> int:
+        p = ctypes.c_void_p()
+        self._check(self.L.ppb_alloc_host(self.h, nbytes, ctypes.byref(p)))
+        return p.value
+
+    def free_host(self, ptr: int):
+        self._check(self.L.ppb_free_host(self.h, ctypes.c_void_p(ptr)))
+
+    def alloc_device(self, nbytes: int) -> int:
+        p = ctypes.c_void_p()
+        self._check(self.L.ppb_alloc_device(self.h, nbytes, ctypes.byref(p)))
+        return p.value
+
+    def free_device(self, ptr: int):
+        self._check(self.L.ppb_free_device(self.h, ctypes.c_void_p(ptr)))
+
+    @staticmethod
+    def _params(cfg: PipelineConfig, seed: int, plain: bool) -> _TileParams:
+        if cfg.NonGauss not in (0,):
+            raise PPBError(-6, "NonGauss modes are outside this path")
+        return _TileParams(Omx=cfg.Omx, OmB=cfg.OmB, Omvac=cfg.Omvac, h=cfg.h, n=cfg.n, boxsize=cfg.boxsize,
+                           nbuff=cfg.nbuff, z_out=cfg.z_out, z_max=cfg.z_max, ievol=cfg.ievol, cenx=cfg.cenx,
+                           ceny=cfg.ceny, cenz=cfg.cenz, ilpt=cfg.ilpt, ioutshear=cfg.ioutshear,
+                           wsmooth=cfg.wsmooth, rmax2rs=cfg.rmax2rs, seed=int(seed) & (2**64 - 1),
+                           plain=1 if plain else 0)
+
+    def run_tile_into(self, cfg: PipelineConfig, seed: int, Rf: Sequence[float], ptr: int, capacity: int,
+                      plain: bool = False):
+        """run_tile writing records to a caller pointer (pinned host or
+        device memory).  Returns (count, RTHLmax, npeaks, device_ms)."""
+        p = self._params(cfg, seed, plain)
+        rf = np.ascontiguousarray(np.asarray(Rf, dtype=np.float64))
+        hb = _HaloBuf(records=ptr, capacity=capacity)
+        ms = ctypes.c_float()
+        self._check(self.L.ppb_run_tile_timed(self.h, ctypes.byref(p), _p(rf), len(rf), ctypes.byref(hb),
+                                              ctypes.byref(ms)))
+        return int(hb.count), float(hb.RTHLmax), int(hb.npeaks), ms.value
+
+    # ---- path entry points ----
+    def run_tile_arrays(self, cfg: PipelineConfig, seed: int, Rf: Sequence[float], plain: bool = False,
+                        capacity: int = 0, timed: bool = False):
+        """run_tile with the tables already set.  Returns (records, RTHLmax,
+        npeaks[, device_ms])."""
+        if cfg.NonGauss not in (0,):
+            raise PPBError(-6, "NonGauss modes are outside this path")
+        p = _TileParams(Omx=cfg.Omx, OmB=cfg.OmB, Omvac=cfg.Omvac, h=cfg.h, n=cfg.n, boxsize=cfg.boxsize,
+                        nbuff=cfg.nbuff, z_out=cfg.z_out, z_max=cfg.z_max, ievol=cfg.ievol, cenx=cfg.cenx,
+                        ceny=cfg.ceny, cenz=cfg.cenz, ilpt=cfg.ilpt, ioutshear=cfg.ioutshear,
+                        wsmooth=cfg.wsmooth, rmax2rs=cfg.rmax2rs, seed=int(seed) & (2**64 - 1),
+                        plain=1 if plain else 0)
+        rf = np.ascontiguousarray(np.asarray(Rf, dtype=np.float64))
+        nf = 33 if cfg.ioutshear >= 1 else 11
+        cap = capacity or max(1024, getattr(self, "_last_count", 0) * 2)
+        for _ in range(2):
+            rec = np.empty((cap, nf), dtype=np.float32)
+            hb = _HaloBuf(records=rec.ctypes.data, capacity=cap)
+            ms = ctypes.c_float()
+            rc = self.L.ppb_run_tile_timed(self.h, ctypes.byref(p), _p(rf), len(rf), ctypes.byref(hb),
+                                           ctypes.byref(ms))
+            if rc == -7:   # capacity: the tile ran; enlarge and rerun
+                cap = int(hb.count) + 16
+                continue
+            self._check(rc)
+            self._last_count = int(hb.count)
+            out = (rec[:hb.count].copy(), float(hb.RTHLmax), int(hb.npeaks))
+            return out + (ms.value,) if timed else out
+        raise PPBError(-7, "record capacity")
+
+    def run_tile(self, cfg: PipelineConfig, seed: int = 42, plain: bool = False, write: bool = True):
+        """Pipeline.run_tile(cfg; seed): reads cfg.pkfile / filterfile /
+        tabfile, runs the tile, writes cfg.fileout (.pksc) and returns the
+        (N, 11|33) float32 records."""
+        k, pk = read_pk_table(cfg.pkfile)
+        self.set_pk_table(k, pk)
+        self.set_collapse_table(read_homeltab(cfg.tabfile))
+        Rf = [f[2] for f in read_filterbank(cfg.filterfile)]
+        rec, rthlmax, _ = self.run_tile_arrays(cfg, seed, Rf, plain=plain)
+        if write:
+            write_pksc(cfg.fileout, rec, rthlmax, cfg.z_out)
+        return rec
+
+    def fill_noise_threefry(self, n: int, seed: int) -> np.ndarray:
+        out = np.empty((n, n, n), dtype=np.float32)
+        self._check(self.L.ppb_noise_threefry(self.h, _p(out), n, int(seed) & (2**64 - 1)))
+        return out
+
+    def find_peaks(self, delta: np.ndarray, mask: np.ndarray, xbx: float, ybx: float, zbx: float, alatt: float,
+                   nbuff: int, fcrit: float, Rsmooth: float = 0.0, max_peaks: int = 2000000):
+        """find_peaks(delta, mask, xbx, ybx, zbx, alatt, nbuff, fcrit, Rsmooth):
+        mask (int8) is updated in place.  Returns a dict of arrays (i, j, k,
+        ipp 1-based; x, y, z physical; delta; Rsmooth)."""
+        if delta.dtype != np.float32 or not delta.flags.c_contiguous:
+            raise ValueError("delta must be a C-contiguous float32 array")
+        if mask.dtype != np.int8 or not mask.flags.c_contiguous or mask.shape != delta.shape:
+            raise ValueError("mask must be a C-contiguous int8 array of delta's shape")
+        n3, n2, n1 = delta.shape
+        cap = int(min(max_peaks, max(1, (n1 - 2 * nbuff) * (n2 - 2 * nbuff) * (n3 - 2 * nbuff))))
+        cap = max(cap, 1)
+        bi, bj, bk, bp = (np.empty(cap, np.int64) for _ in range(4))
+        bd = np.empty(cap, np.float32)
+        npk = ctypes.c_int64()
+        self._check(self.L.ppb_find_peaks(self.h, _p(delta), _p(mask), n1, n2, n3, nbuff, ctypes.c_float(fcrit),
+                                          max_peaks, _p(bi), _p(bj), _p(bk), _p(bp), _p(bd), ctypes.byref(npk)))
+        m = npk.value
+        i, j, k = bi[:m].copy(), bj[:m].copy(), bk[:m].copy()
+        cen = lambda nn: 0.5 * (nn + 1)
+        return {"i": i, "j": j, "k": k, "ipp": bp[:m].copy(), "x": xbx + alatt * (i - cen(n1)),
+                "y": ybx + alatt * (j - cen(n2)), "z": zbx + alatt * (k - cen(n3)), "delta": bd[:m].copy(),
+                "Rsmooth": np.full(m, float(Rsmooth))}
+
+    def analyse_peaks(self, fields: dict, ipp, Rf, ir2min, ZZon, fcrit, alatt: float, nhunt: int,
+                      plain: bool = False) -> np.ndarray:
+        """analyse_peak over a batch (rmax2rs = 0).  fields: delta, etax, etay,
+        etaz and optional eta2x/eta2y/eta2z/lapd (C-order float32, cubic).
+        Returns (npk, 31) float64 (layout RESULT_FIELDS)."""
+        d = fields["delta"]
+        n = d.shape[0]
+        if d.shape != (n, n, n):
+            raise ValueError("analyse_peaks needs a cubic grid")
+        npk = len(ipp)
+        arr = lambda a, t: np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=t), (npk,)))
+        g = lambda key: None if fields.get(key) is None else np.ascontiguousarray(fields[key], np.float32)
+        f = {k: g(k) for k in ("delta", "etax", "etay", "etaz", "eta2x", "eta2y", "eta2z", "lapd")}
+        out = np.empty((npk, 31), dtype=np.float64)
+        a_ipp, a_Rf, a_ir2, a_Z, a_fc = arr(ipp, np.int64), arr(Rf, np.float64), arr(ir2min, np.int64), \
+            arr(ZZon, np.float64), arr(fcrit, np.float64)
+        self._check(self.L.ppb_analyse_peaks(self.h, _p(f["delta"]), _p(f["etax"]), _p(f["etay"]), _p(f["etaz"]),
+                                             _p(f["eta2x"]), _p(f["eta2y"]), _p(f["eta2z"]), _p(f["lapd"]), n,
+                                             nhunt, npk, _p(a_ipp), _p(a_Rf), _p(a_ir2), _p(a_Z), _p(a_fc), alatt,
+                                             1 if plain else 0, _p(out)))
+        return out
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def run_tile(cfg: PipelineConfig, seed: int = 42, verbose: bool = False, plain: bool = False):
+    """Drop-in for Pipeline.run_tile(cfg; seed): returns the halo records and
+    writes cfg.fileout."""
+    rec = default_context().run_tile(cfg, seed=seed, plain=plain)
+    if verbose:
+        print(f"run_tile: {rec.shape[0]} halos -> {cfg.fileout}")
+    return rec
+
+
+def fill_noise_threefry(n: int, seed: int) -> np.ndarray:
+    return default_context().fill_noise_threefry(n, seed)
+
+
+def find_peaks(delta, mask, xbx, ybx, zbx, alatt, nbuff, fcrit, Rsmooth=0.0, max_peaks=2000000):
+    return default_context().find_peaks(delta, mask, xbx, ybx, zbx, alatt, nbuff, fcrit, Rsmooth, max_peaks)
+
+
+def analyse_peaks(fields, ipp, Rf, ir2min, ZZon, fcrit, alatt, nhunt, plain=False):
+    return default_context().analyse_peaks(fields, ipp, Rf, ir2min, ZZon, fcrit, alatt, nhunt, plain)
