@@ -239,6 +239,7 @@ def run_ours(args, dist: Dist):
     for s in range(args.steps):
         cnt, rmax, npk, dms = ctx.run_tile_into(cfg, seed0, FILTERS, dev_out, cap, plain=args.plain)
         st = ctx.shell_stats()
+        last_shell_stats = st
         shell_ms += st["ms"]
         shell_visits += st["visits"]
         npk_tot += npk
@@ -287,6 +288,7 @@ def run_ours(args, dist: Dist):
             "peaks_per_s": npk_tot / (dev_ms / 1000.0), "halos_per_tile": nh_tot / args.steps,
             "peaks_per_tile": npk_tot / args.steps,
             "stage_ms_last_step": stage,
+            "shell_stats_last_step": last_shell_stats,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
             "gpu_launches": int(launches),

@@ -180,6 +180,11 @@ int32_t ppb_launch_count(ppb_ctx* ctx, int64_t* count);
  * dump-reason counters of src/HaloFinder/RadialShell.jl:15-34 (premask,
  * no_fcrit, m0_one, no_collapse, rthl_neg) and the kernel's device time. */
 int32_t ppb_last_shell_stats(ppb_ctx* ctx, int64_t* visits, int64_t* dumps5, float* ms);
+/* All 16 raw shell-kernel counters of the last run: [0] cell visits,
+ * [1..5] dump reasons as above, [6] profile reads beyond the gathered shells
+ * (must be 0), [7] SPH-table overruns (the reference raises there),
+ * [8] invalid peak inputs, [9] collapse-walk rounds, others reserved. */
+int32_t ppb_shell_counters(ppb_ctx* ctx, int64_t* out16);
 /* Per-stage device times (ms) of the last ppb_run_tile_timed call:
  * [0] fields, [1] filter bank + peaks, [2] shell analysis, [3] records. */
 int32_t ppb_last_stage_ms(ppb_ctx* ctx, float* ms4);

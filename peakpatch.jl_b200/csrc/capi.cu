@@ -37,22 +37,6 @@ const void* stage_in(DevBuf& buf, const void* src, size_t bytes, cudaStream_t s)
   return buf.p;
 }
 
-// SPH kernel table akk (RadialShell.jl:133-150)
-static std::vector<double> make_atab4() {
-  std::vector<double> akk(1101);
-  const double pi = 3.141592653589793, ca = 3.0 / (2.0 * pi), cb = 1.0 / (4.0 * pi);
-  for (int i = 1; i <= 1100; i++) {
-    const double u = (i - 1) * 0.01, ru = std::sqrt(u);
-    double v;
-    if (ru < 1.0) v = ca * (2.0 / 3.0 - u + 0.5 * u * ru);
-    else if (ru <= 2.0) v = cb * (2.0 - ru) * (2.0 - ru) * (2.0 - ru);
-    else v = 0.0;
-    akk[i - 1] = v;
-  }
-  akk[1100] = 0.0;
-  return akk;
-}
-
 }  // namespace ppb
 
 // ---------------------------------------------------------------------------
@@ -117,6 +101,21 @@ ShellArgs ppb_ctx::shell_args(int n, double alatt, const float4* aos, const floa
   a.sh_count = shells.d_count.as<int32_t>();
   a.rad = shells.d_rad.as<double>();
   a.r2m = shells.d_r2m.as<int32_t>();
+  a.win_lo = shells.d_wlo.as<int32_t>();
+  a.win_hi = shells.d_whi.as<int32_t>();
+  a.win_off = shells.d_woff.as<int32_t>();
+  a.wts = shells.d_wts.as<double>();
+  a.w1 = shells.d_w1.as<double>();
+  a.need = shells.d_need.as<int32_t>();
+  a.rad5 = shells.d_rad5.as<double>();
+  a.grp_a = shells.d_grp_a.as<int32_t>();
+  a.grp_b = shells.d_grp_b.as<int32_t>();
+  a.grp_c = shells.d_grp_c.as<int32_t>();
+  a.ck_s = shells.d_ck_s.as<int32_t>();
+  a.ck_n = shells.d_ck_n.as<int32_t>();
+  a.sh_c0 = shells.d_sh_c0.as<int32_t>();
+  a.sh_nc = shells.d_sh_nc.as<int32_t>();
+  a.ngroups = shells.ngroups;
   a.nshell = shells.nshell;
   a.mmax = std::max(shells.nshell - 1, 1);
   a.npart = shells.ncells;
@@ -127,9 +126,11 @@ ShellArgs ppb_ctx::shell_args(int n, double alatt, const float4* aos, const floa
 
 void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st) {
   if (shell_blocks == 0) {
+    shell_prepare(shell_wpb);
+    const size_t shm = shell_smem_bytes(shell_wpb);
     int b1 = 0, b2 = 0;
-    PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, shell_kernel_ptr(true, true), 32 * shell_wpb, 0));
-    PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, shell_kernel_ptr(false, false), 32 * shell_wpb, 0));
+    PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, shell_kernel_ptr(true, true), 32 * shell_wpb, shm));
+    PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, shell_kernel_ptr(false, false), 32 * shell_wpb, shm));
     shell_blocks = nsm * std::max(1, std::min(b1, b2));
   }
   const int64_t stride = shell_scratch_doubles_per_warp(a.nshell);
@@ -154,6 +155,7 @@ void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st)
   for (int i = 0; i < 5; i++) s.dump[i] = c[1 + i];
   s.guard = c[6];
   s.akk = c[7];
+  for (int i = 0; i < 16; i++) s.raw[i] = c[i];
   PPB_CUDA(cudaEventElapsedTime(&s.ms, ev[14], ev[15]));
   last_shell = s;
   if (st) *st = s;

@@ -43,8 +43,126 @@ void build_shell_table(ShellTable& st, int nhunt) {
     st.r2m[m] = st.shell_r2[m - 1];
     st.rad[m] = std::sqrt((double)st.r2m[m]);
   }
+  // kernel_strain windows and weights for centre shells mp = 2..mmax
+  const int mmax = std::max(st.nshell - 1, 1);
+  st.win_lo.assign(st.nshell + 1, 0);
+  st.win_hi.assign(st.nshell + 1, -1);
+  st.win_off.assign(st.nshell + 1, 0);
+  st.wts.clear();
+  for (int mp = 2; mp <= mmax; mp++) {
+    int lo = -1, hi = -2;
+    for (int m1 = 1; m1 <= mmax; m1++) {
+      const double u0 = st.rad[mp] - st.rad[m1];
+      if (u0 * u0 < 4.0) {
+        if (lo < 0) lo = m1;
+        hi = m1;
+      }
+    }
+    st.win_lo[mp] = lo;
+    st.win_hi[mp] = hi;
+    st.win_off[mp] = (int32_t)st.wts.size();
+    for (int m1 = lo; m1 <= hi; m1++) {
+      const double u0 = st.rad[mp] - st.rad[m1];
+      const double u02 = u0 * u0;
+      const double u12 = st.rad[mp] * st.rad[mp] + st.rad[m1] * st.rad[m1];
+      const double d = u12 - u02;
+      st.wts.push_back(hRinteg(u0, u12) / (d * d));
+    }
+  }
+  // mp == 1 weights
+  const std::vector<double> akk = make_atab4();
+  st.w1.assign(st.nshell + 1, 0.0);
+  for (int m1 = 1; m1 <= mmax; m1++) {
+    const double u0 = st.rad[m1];
+    const double con = 100.0 * u0 * u0;
+    const long long icon = (long long)std::floor(con);
+    if (icon + 1 > 1100) {
+      st.w1[m1] = std::nan("");
+      continue;
+    }
+    const double diff = con - (double)icon;
+    const double aww = akk[icon] + diff * (akk[icon + 1] - akk[icon]);
+    st.w1[m1] = 0.5 * aww / st.rad[m1];
+  }
+  // gather truncation targets
+  st.need.assign(st.nshell + 1, mmax);
+  for (int m = 1; m <= mmax; m++) {
+    int l = m;
+    while (l + 1 <= mmax && st.rad[l + 1] <= st.rad[m] + 2.0) l++;
+    st.need[m] = std::min(mmax, l + 2);
+  }
+  st.rad5.assign(st.nshell + 1, 0.0);
+  for (int m = 1; m <= st.nshell; m++) st.rad5[m] = std::pow(st.rad[m], 5);
+  // gather schedule (shells 2..mmax; shell m is distinct value m-1)
+  st.grp_a.clear(); st.grp_b.clear(); st.grp_c.clear();
+  st.ck_s.clear(); st.ck_n.clear();
+  st.sh_c0.assign(st.nshell + 1, 0);
+  st.sh_nc.assign(st.nshell + 1, 0);
+  int in_group = 0;
+  for (int m = 2; m <= mmax; m++) {
+    const int cnt = st.shell_count[m - 1], s0 = st.shell_start[m - 1];
+    int nck = (cnt + kChunkCells - 1) / kChunkCells;
+    if (nck > 32) nck = 32;
+    if (nck < 1) nck = 1;
+    if (in_group + nck > 32 || st.grp_a.empty()) {   // open a new group
+      if (!st.grp_a.empty()) st.grp_b.back() = m - 1;
+      st.grp_a.push_back(m);
+      st.grp_b.push_back(m);
+      st.grp_c.push_back((int32_t)st.ck_s.size());
+      in_group = 0;
+    }
+    st.sh_c0[m] = (int32_t)st.ck_s.size();
+    st.sh_nc[m] = nck;
+    for (int c = 0; c < nck; c++) {   // near-equal chunk sizes
+      const int a = (int)((int64_t)cnt * c / nck), b = (int)((int64_t)cnt * (c + 1) / nck);
+      st.ck_s.push_back(s0 + a);
+      st.ck_n.push_back(b - a);
+    }
+    in_group += nck;
+    st.grp_b.back() = m;
+  }
+  st.ngroups = (int)st.grp_a.size();
+  st.grp_c.push_back((int32_t)st.ck_s.size());
   st.nhunt = nhunt;
   st.d_cells.release();   // force re-upload
+}
+
+// hRinteg (src/HaloFinder/RadialShell.jl:100-127)
+double hRinteg(double u0, double u12) {
+  const double x0 = std::fabs(u0);
+  if (x0 >= 2.0) return 0.0;
+  const double one7 = 1.0 / 7.0;
+  double result = 1.6 * u12 - 6.4 * one7;
+  const double x02 = x0 * x0, x04 = x02 * x02;
+  if (x0 >= 1.0) {
+    const double h1 = x04 * (2.0 - x0 * (2.4 - x0 * (1.0 - x0 * one7)));
+    const double h2 = x02 * (4.0 - x0 * (4.0 - x0 * (1.5 - x0 * 0.2)));
+    result = result - h2 * u12 + h1;
+  } else {
+    result = result - 0.2 * (u12 - one7);
+    if (x0 > 0.0) {
+      const double h1 = x04 * (1.0 - x02 * (1.0 - 3.0 * x0 * one7));
+      const double h2 = x02 * (2.0 - x02 * (1.5 - 0.6 * x0));
+      result = result - h2 * u12 + h1;
+    }
+  }
+  return result;
+}
+
+// SPH kernel table akk (RadialShell.jl:133-150), 1101 entries, 0-based
+std::vector<double> make_atab4() {
+  std::vector<double> akk(1101);
+  const double pi = 3.141592653589793, ca = 3.0 / (2.0 * pi), cb = 1.0 / (4.0 * pi);
+  for (int i = 1; i <= 1100; i++) {
+    const double u = (i - 1) * 0.01, ru = std::sqrt(u);
+    double v;
+    if (ru < 1.0) v = ca * (2.0 / 3.0 - u + 0.5 * u * ru);
+    else if (ru <= 2.0) v = cb * (2.0 - ru) * (2.0 - ru) * (2.0 - ru);
+    else v = 0.0;
+    akk[i - 1] = v;
+  }
+  akk[1100] = 0.0;
+  return akk;
 }
 
 void upload_shell_table(ShellTable& st, cudaStream_t s) {
@@ -59,6 +177,24 @@ void upload_shell_table(ShellTable& st, cudaStream_t s) {
   PPB_CUDA(cudaMemcpyAsync(st.d_count.p, st.shell_count.data(), st.shell_count.size() * 4, cudaMemcpyHostToDevice, s));
   PPB_CUDA(cudaMemcpyAsync(st.d_r2m.p, st.r2m.data(), st.r2m.size() * 4, cudaMemcpyHostToDevice, s));
   PPB_CUDA(cudaMemcpyAsync(st.d_rad.p, st.rad.data(), st.rad.size() * 8, cudaMemcpyHostToDevice, s));
+  auto up = [&](DevBuf& b, const void* src, size_t bytes) {
+    b.ensure(std::max<size_t>(bytes, 8));
+    if (bytes) PPB_CUDA(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, s));
+  };
+  up(st.d_wlo, st.win_lo.data(), st.win_lo.size() * 4);
+  up(st.d_whi, st.win_hi.data(), st.win_hi.size() * 4);
+  up(st.d_woff, st.win_off.data(), st.win_off.size() * 4);
+  up(st.d_wts, st.wts.data(), st.wts.size() * 8);
+  up(st.d_w1, st.w1.data(), st.w1.size() * 8);
+  up(st.d_need, st.need.data(), st.need.size() * 4);
+  up(st.d_rad5, st.rad5.data(), st.rad5.size() * 8);
+  up(st.d_grp_a, st.grp_a.data(), st.grp_a.size() * 4);
+  up(st.d_grp_b, st.grp_b.data(), st.grp_b.size() * 4);
+  up(st.d_grp_c, st.grp_c.data(), st.grp_c.size() * 4);
+  up(st.d_ck_s, st.ck_s.data(), st.ck_s.size() * 4);
+  up(st.d_ck_n, st.ck_n.data(), st.ck_n.size() * 4);
+  up(st.d_sh_c0, st.sh_c0.data(), st.sh_c0.size() * 4);
+  up(st.d_sh_nc, st.sh_nc.data(), st.sh_nc.size() * 4);
   PPB_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -20,28 +20,37 @@
 //     extends the cumulative profile Fbar and stops as soon as every shell
 //     the collapse walk can read has been gathered.  Every index used below
 //     the gather is bounded by rad <= rad[M] + 2 (+ one shell) with
-//     M = max(crossing shell, first shell beyond ir2min, Rf shell), because
+//     M = max(crossing shell, first shell beyond ir2min, Rf window), because
 //     kernel_strain's weight vanishes for |rad[mp] - rad[m1]| >= 2 and the
 //     walk only moves inward from the crossing; the one exception (no
 //     crossing at all) gathers every shell.  A device-side guard counts any
 //     read past the gathered range (it must stay 0; the host fails loudly).
-//  3. Collapse walk in double precision, executed redundantly by all lanes
-//     (warp-uniform control flow); the shell window sums of kernel_strain are
-//     split across lanes and combined with a butterfly reduction.
+//  3. Collapse walk in double precision.  kernel_strain(mp) only depends on
+//     the shells with (rad[mp] - rad[m1])^2 < 4 (the reference's running
+//     mlow/mupp always bracket that set), so the walk steps are independent:
+//     each lane evaluates one step (window sum, eigenvalues, table lookup)
+//     and a ballot finds the first step that collapses, 31 steps per round.
+//     The window weights hRinteg/(u12-u0^2)^2 depend only on the radii and
+//     come from a host table.  The ten zvir_half radii run on ten lanes.
 #include "ppb_internal.h"
 
 namespace ppb {
 
 namespace {
 
-constexpr int NV = 21;   // profile values per shell
-enum { PV_FBAR = 0, PV_N = 1, PV_S = 2, PV_S2 = 5, PV_G = 8, PV_GF = 11, PV_Q = 14, PV_DF = 20 };
+constexpr int NV = 20;   // profile values per shell
+enum { PV_FBAR = 0, PV_N = 1, PV_S = 2, PV_S2 = 5, PV_G = 8, PV_GF = 11, PV_Q = 14 };
 constexpr int NACC = 19; // gather accumulators: F, S3, S2_3, G3, Gf3, Q6 (xx yy zz xy xz yz)
+// shells a warp keeps in shared memory (peaks needing more move their
+// profile to global scratch), and the per-warp shared-memory footprint:
+// the profile plus the chunk-partial table of the gather
+constexpr int SMEM_SHELLS = 80;
+constexpr int SMEM_WARP_DOUBLES = NV * (SMEM_SHELLS + 1) + (NACC + 1) * 32;
 constexpr unsigned FULL = 0xffffffffu;
 
 // counters layout
 enum { CNT_VISITS = 0, CNT_PREMASK = 1, CNT_NOFCRIT = 2, CNT_M0ONE = 3, CNT_NOCOLL = 4, CNT_RTHLNEG = 5,
-       CNT_GUARD = 6, CNT_AKK = 7, CNT_LAPD = 8 };
+       CNT_GUARD = 6, CNT_AKK = 7, CNT_BADPEAK = 8, CNT_WALK = 9 };
 
 // ---------------------------------------------------------------------------
 // accumulators
@@ -91,7 +100,7 @@ __device__ __forceinline__ void accumulate_cell(Acc<COMP>& A, const float4 a, co
 }
 
 // ---------------------------------------------------------------------------
-// small double-precision helpers
+// small helpers
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -103,113 +112,94 @@ __device__ __forceinline__ long long warp_sum_ll(long long v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
   return v;
 }
-
-// RadialShell.jl:100-127
-__device__ double hRinteg(double u0, double u12) {
-  const double x0 = fabs(u0);
-  if (x0 >= 2.0) return 0.0;
-  const double one7 = 1.0 / 7.0;
-  double r = 1.6 * u12 - 6.4 * one7;
-  const double x02 = x0 * x0, x04 = x02 * x02;
-  if (x0 >= 1.0) {
-    const double h1 = x04 * (2.0 - x0 * (2.4 - x0 * (1.0 - x0 * one7)));
-    const double h2 = x02 * (4.0 - x0 * (4.0 - x0 * (1.5 - x0 * 0.2)));
-    r = r - h2 * u12 + h1;
-  } else {
-    r = r - 0.2 * (u12 - one7);
-    if (x0 > 0.0) {
-      const double h1 = x04 * (1.0 - x02 * (1.0 - 3.0 * x0 * one7));
-      const double h2 = x02 * (2.0 - x02 * (1.5 - 0.6 * x0));
-      r = r - h2 * u12 + h1;
-    }
-  }
-  return r;
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
+  return v;
 }
 
-// symmetric 3x3 eigenvalues (ascending) by cyclic Jacobi rotations.
-// m = (xx, yy, zz, xy, xz, yz)
-__device__ void eig3(const double m[6], double lam[3]) {
-  double A[3][3] = {{m[0], m[3], m[4]}, {m[3], m[1], m[5]}, {m[4], m[5], m[2]}};
-  for (int sweep = 0; sweep < 64; sweep++) {
-    const double off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
-    const double dia = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
-    if (off == 0.0 || off < 1e-36 * dia) break;
-#pragma unroll
-    for (int pq = 0; pq < 3; pq++) {
-      const int p = pq == 2 ? 1 : 0, q = pq == 0 ? 1 : 2;
-      if (A[p][q] == 0.0) continue;
-      const double theta = (A[q][q] - A[p][p]) / (2.0 * A[p][q]);
-      const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-      const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
-#pragma unroll
-      for (int k = 0; k < 3; k++) {
-        const double akp = A[k][p], akq = A[k][q];
-        A[k][p] = c * akp - s * akq;
-        A[k][q] = s * akp + c * akq;
-      }
-#pragma unroll
-      for (int k = 0; k < 3; k++) {
-        const double apk = A[p][k], aqk = A[q][k];
-        A[p][k] = c * apk - s * aqk;
-        A[q][k] = s * apk + c * aqk;
-      }
-    }
+// Symmetric 3x3 eigenvalues, ascending: the trigonometric solution of the
+// characteristic cubic (O. K. Smith, "Eigenvalues of a symmetric 3 x 3
+// matrix", Comm. ACM 4 (1961) 168).  m = (xx, yy, zz, xy, xz, yz).
+__device__ __noinline__ void eig3(const double* m, double* lam) {
+  const double a00 = m[0], a11 = m[1], a22 = m[2], a01 = m[3], a02 = m[4], a12 = m[5];
+  const double p1 = a01 * a01 + a02 * a02 + a12 * a12;
+  double e1, e2, e3;
+  if (p1 == 0.0) {
+    e1 = a00; e2 = a11; e3 = a22;
+  } else {
+    const double q = (a00 + a11 + a22) / 3.0;
+    const double b00 = a00 - q, b11 = a11 - q, b22 = a22 - q;
+    const double p = sqrt((b00 * b00 + b11 * b11 + b22 * b22 + 2.0 * p1) / 6.0);
+    const double ip = 1.0 / p;
+    const double c00 = b00 * ip, c11 = b11 * ip, c22 = b22 * ip, c01 = a01 * ip, c02 = a02 * ip, c12 = a12 * ip;
+    double r = 0.5 * (c00 * (c11 * c22 - c12 * c12) - c01 * (c01 * c22 - c12 * c02) + c02 * (c01 * c12 - c11 * c02));
+    r = r < -1.0 ? -1.0 : (r > 1.0 ? 1.0 : r);
+    const double phi = acos(r) / 3.0;
+    e1 = q + 2.0 * p * cos(phi);
+    e3 = q + 2.0 * p * cos(phi + 2.0943951023931957);   // + 2 pi / 3
+    e2 = 3.0 * q - e1 - e3;
   }
-  double a = A[0][0], b = A[1][1], c = A[2][2], t;
-  if (a > b) { t = a; a = b; b = t; }
-  if (b > c) { t = b; b = c; c = t; }
-  if (a > b) { t = a; a = b; b = t; }
-  lam[0] = a; lam[1] = b; lam[2] = c;
+  double t;
+  if (e1 > e2) { t = e1; e1 = e2; e2 = t; }
+  if (e2 > e3) { t = e2; e2 = e3; e3 = t; }
+  if (e1 > e2) { t = e1; e1 = e2; e2 = t; }
+  lam[0] = e1; lam[1] = e2; lam[2] = e3;
 }
 
 // trilinear lookup, outside the box -> -1 (CollapseTable.jl:128-145)
-__device__ double tab_interp(const DevTable& T, double x, double y, double z) {
+__device__ __noinline__ double tab_interp(const DevTable& T, double x, double y, double z) {
   if (!(x >= T.x1 && x <= T.x2 && y >= T.y1 && y <= T.y2 && z >= T.z1 && z <= T.z2)) return -1.0;
-  int ix, iy, iz;
-  double wx, wy, wz;
-  {
-    const double pos = (x - T.x1) / ((T.x2 - T.x1) / (T.nx - 1));
-    int i = (int)floor(pos); i = i < 0 ? 0 : (i > T.nx - 2 ? T.nx - 2 : i);
-    ix = i; wx = pos - i;
-  }
-  {
-    const double pos = (y - T.y1) / ((T.y2 - T.y1) / (T.ny - 1));
-    int i = (int)floor(pos); i = i < 0 ? 0 : (i > T.ny - 2 ? T.ny - 2 : i);
-    iy = i; wy = pos - i;
-  }
-  {
-    const double pos = (z - T.z1) / ((T.z2 - T.z1) / (T.nz - 1));
-    int i = (int)floor(pos); i = i < 0 ? 0 : (i > T.nz - 2 ? T.nz - 2 : i);
-    iz = i; wz = pos - i;
-  }
-  auto A = [&](int a, int b, int c) {
-    return (double)__ldg(T.t + (ix + a) + (int64_t)T.nx * ((iy + b) + (int64_t)T.ny * (iz + c)));
-  };
-  const double c00 = (1 - wx) * A(0, 0, 0) + wx * A(1, 0, 0);
-  const double c10 = (1 - wx) * A(0, 1, 0) + wx * A(1, 1, 0);
-  const double c01 = (1 - wx) * A(0, 0, 1) + wx * A(1, 0, 1);
-  const double c11 = (1 - wx) * A(0, 1, 1) + wx * A(1, 1, 1);
+  const double px = (x - T.x1) / ((T.x2 - T.x1) / (T.nx - 1));
+  const double py = (y - T.y1) / ((T.y2 - T.y1) / (T.ny - 1));
+  const double pz = (z - T.z1) / ((T.z2 - T.z1) / (T.nz - 1));
+  int ix = (int)floor(px), iy = (int)floor(py), iz = (int)floor(pz);
+  ix = ix < 0 ? 0 : (ix > T.nx - 2 ? T.nx - 2 : ix);
+  iy = iy < 0 ? 0 : (iy > T.ny - 2 ? T.ny - 2 : iy);
+  iz = iz < 0 ? 0 : (iz > T.nz - 2 ? T.nz - 2 : iz);
+  const double wx = px - ix, wy = py - iy, wz = pz - iz;
+  const float* b = T.t + ix + (int64_t)T.nx * (iy + (int64_t)T.ny * iz);
+  const int64_t sy = T.nx, sz = (int64_t)T.nx * T.ny;
+  const double c00 = (1 - wx) * (double)__ldg(b) + wx * (double)__ldg(b + 1);
+  const double c10 = (1 - wx) * (double)__ldg(b + sy) + wx * (double)__ldg(b + sy + 1);
+  const double c01 = (1 - wx) * (double)__ldg(b + sz) + wx * (double)__ldg(b + sz + 1);
+  const double c11 = (1 - wx) * (double)__ldg(b + sz + sy) + wx * (double)__ldg(b + sz + sy + 1);
   const double c0 = (1 - wy) * c00 + wy * c10;
   const double c1 = (1 - wy) * c01 + wy * c11;
   return (1 - wz) * c0 + wz * c1;
 }
 
 // ---------------------------------------------------------------------------
-// per-warp profile (scratch): value v of shell m at p[v*MS + m]
+// per-warp radial profile: value v of shell m at p[v*MS + m].  It lives in
+// the warp's shared-memory slice while the peak needs at most `cap` shells
+// and moves to the warp's global scratch slot when the gather grows beyond.
 // ---------------------------------------------------------------------------
 struct Prof {
   double* p;
   int MS;
   int mdone;                        // shells 1..mdone are valid
   unsigned long long* counters;
+  int cap;                          // largest shell index the current storage holds
+  double* global;                   // the warp's scratch slot
+  int MS_global;
   __device__ __forceinline__ double get(int v, int m) const {
     if (m > mdone) {                // never taken when the truncation rule holds
-      if ((threadIdx.x & 31) == 0) atomicAdd(counters + CNT_GUARD, 1ull);
+      atomicAdd(counters + CNT_GUARD, 1ull);
       return 0.0;
     }
     return p[(int64_t)v * MS + m];
   }
   __device__ __forceinline__ void set(int v, int m, double x) { p[(int64_t)v * MS + m] = x; }
+  // copy shells 1..upto to global scratch and continue there (whole warp)
+  __device__ void spill(int upto) {
+    const int lane = threadIdx.x & 31;
+    for (int v = 0; v < NV; v++)
+      for (int m = 1 + lane; m <= upto; m += 32) global[(int64_t)v * MS_global + m] = p[v * MS + m];
+    __syncwarp();
+    p = global;
+    MS = MS_global;
+    cap = 1 << 30;
+  }
 };
 
 struct KS {
@@ -217,61 +207,78 @@ struct KS {
   double g[3], gf[3];
 };
 
-// kernel_strain (RadialShell.jl:228-277), lanes split m1 in [mlow, mupp]
-__device__ KS kernel_strain(const Prof& P, const double* __restrict__ rad, int mp, int mlow, int mupp,
-                            const double* __restrict__ akk, double wRnor, double aRnor,
-                            unsigned long long* counters) {
+struct Walk {                       // one evaluated walk step
+  KS k;
+  double Fh, ev, pv, Fr, zv;
+};
+
+// kernel_strain (RadialShell.jl:228-277) for centre shell mp over m1 in
+// [lo, hi].  For mp > 1 only the shells with (rad[mp]-rad[m1])^2 < 4
+// contribute (the table window); for mp == 1 the SPH table weights apply to
+// every m1 of [lo, hi].  The warp is split into aligned groups of G lanes
+// (G a power of two); each group evaluates its own mp (mp < 1: no work), its
+// lanes striding over m1, and the group's partial sums are combined with a
+// butterfly, leaving the result in every lane of the group.  Every lane of
+// the warp must call it.
+__device__ __noinline__ void ks_multi(const Prof& P, const ShellArgs& a, int mp, int lo, int hi, int G,
+                                      double wRnor, double aRnor, KS* out) {
   const int lane = threadIdx.x & 31;
+  const int sub = lane & (G - 1);
   double E[6] = {0, 0, 0, 0, 0, 0}, g[3] = {0, 0, 0}, gf[3] = {0, 0, 0};
-  const double rmp = rad[mp];
-  for (int m1 = mlow + lane; m1 <= mupp; m1 += 32) {
-    double wt;
-    bool use = true;
+  double scale = 0.0;
+  if (mp >= 1) {
+    const double* w;
     if (mp > 1) {
-      const double u0 = rmp - rad[m1];
-      const double u02 = u0 * u0;
-      if (u02 < 4.0) {
-        const double u12 = rmp * rmp + rad[m1] * rad[m1];
-        const double d = u12 - u02;
-        wt = hRinteg(u0, u12) / (d * d);
-      } else {
-        use = false;
-        wt = 0.0;
-      }
+      const int wl = a.win_lo[mp], wh = a.win_hi[mp];
+      lo = max(lo, wl);
+      hi = min(hi, wh);
+      w = a.wts + a.win_off[mp] - wl;
+      scale = wRnor / a.rad[mp];
     } else {
-      const double u0 = rad[m1];
-      const double con = 100.0 * u0 * u0;
-      long long icon = (long long)floor(con);
-      const double diff = con - (double)icon;
-      if (icon + 1 > 1100) {      // the reference raises a BoundsError here
-        atomicAdd(counters + CNT_AKK, 1ull);
-        icon = 1099;
-      }
-      const double aww = akk[icon] + diff * (akk[icon + 1] - akk[icon]);
-      wt = 0.5 * aww / rad[m1];
+      w = a.w1;
+      scale = aRnor;
     }
-    if (use) {
+    if (hi > P.mdone) {                 // never taken when the truncation rule holds
+      atomicAdd(P.counters + CNT_GUARD, 1ull);
+      hi = P.mdone;
+    }
+    const double* pg = P.p + PV_G * P.MS;
+    const double* pf = P.p + PV_GF * P.MS;
+    const double* pq = P.p + PV_Q * P.MS;
+    const int MS = P.MS;
+    for (int m1 = lo + sub; m1 <= hi; m1 += G) {
+      const double wt = w[m1];
+      if (mp == 1 && isnan(wt)) atomicAdd(P.counters + CNT_AKK, 1ull);
 #pragma unroll
       for (int L = 0; L < 3; L++) {
-        g[L] += wt * P.get(PV_G + L, m1);
-        gf[L] += wt * P.get(PV_GF + L, m1);
+        g[L] += wt * pg[L * MS + m1];
+        gf[L] += wt * pf[L * MS + m1];
       }
 #pragma unroll
-      for (int q = 0; q < 6; q++) E[q] -= 0.5 * wt * P.get(PV_Q + q, m1);
+      for (int q = 0; q < 6; q++) E[q] -= 0.5 * wt * pq[q * MS + m1];
+    }
+  }
+  for (int o = G >> 1; o > 0; o >>= 1) {
+#pragma unroll
+    for (int q = 0; q < 6; q++) E[q] += __shfl_xor_sync(FULL, E[q], o);
+#pragma unroll
+    for (int L = 0; L < 3; L++) {
+      g[L] += __shfl_xor_sync(FULL, g[L], o);
+      gf[L] += __shfl_xor_sync(FULL, gf[L], o);
     }
   }
   KS r;
-  const double sc = mp > 1 ? wRnor / rmp : aRnor;
 #pragma unroll
-  for (int q = 0; q < 6; q++) r.E[q] = warp_sum(E[q]) * sc;
+  for (int q = 0; q < 6; q++) r.E[q] = E[q] * scale;
 #pragma unroll
   for (int L = 0; L < 3; L++) {
-    r.g[L] = warp_sum(g[L]) * sc;
-    r.gf[L] = warp_sum(gf[L]) * sc;
+    r.g[L] = g[L] * scale;
+    r.gf[L] = gf[L] * scale;
   }
-  return r;
+  *out = r;
 }
 
+// eigen-decomposition -> (trace, e_v, p_v) as the reference (:571-577)
 __device__ __forceinline__ void ev_pv(const double E[6], double* Frho, double* ev, double* pv) {
   double lam[3];
   eig3(E, lam);
@@ -283,6 +290,24 @@ __device__ __forceinline__ void ev_pv(const double E[6], double* Frho, double* e
     *ev = 0.5 * (lam[2] - lam[0]) / F;
     *pv = 0.5 * (lam[2] + lam[0] - 2.0 * lam[1]) / F;
   }
+}
+
+__device__ __forceinline__ double zvir_of(const DevTable& T, double Fr, double ev, double pv) {
+  if (!(Fr > 0.0)) return -1.0;
+  const double poe = ev < 1e-5 ? 0.0 : pv / ev;
+  return tab_interp(T, log10(Fr), ev, poe);
+}
+
+__device__ __forceinline__ KS shfl_ks(const KS& k, int src) {
+  KS r;
+#pragma unroll
+  for (int q = 0; q < 6; q++) r.E[q] = __shfl_sync(FULL, k.E[q], src);
+#pragma unroll
+  for (int L = 0; L < 3; L++) {
+    r.g[L] = __shfl_sync(FULL, k.g[L], src);
+    r.gf[L] = __shfl_sync(FULL, k.gf[L], src);
+  }
+  return r;
 }
 
 // ---------------------------------------------------------------------------
@@ -304,14 +329,6 @@ __device__ __forceinline__ int last_lt(const double* rad, int lo, int hi, double
   }
   return hi;
 }
-// largest m in [lo, hi] with rad[m] <= x, or lo-1
-__device__ __forceinline__ int last_le(const double* rad, int lo, int hi, double x) {
-  while (lo <= hi) {
-    const int mid = (lo + hi) >> 1;
-    if (rad[mid] <= x) lo = mid + 1; else hi = mid - 1;
-  }
-  return hi;
-}
 
 __device__ __forceinline__ void write_no_collapse(double* o) {
   const int lane = threadIdx.x & 31;
@@ -322,29 +339,35 @@ __device__ __forceinline__ void write_no_collapse(double* o) {
 // the per-peak body
 // ---------------------------------------------------------------------------
 template <bool COMP, bool ADAPTIVE>
-__device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
+__device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base, double* smem) {
   const int lane = threadIdx.x & 31;
   const int n = a.n;
   const int64_t n2 = (int64_t)n * n;
   const int64_t lin = a.pk.lin[p];
+  double* out = a.out + p * RES_N;
+  const double ZZon = a.pk.ZZon[p];
+  if (lin < 0 || lin >= n2 * n || !(ZZon > -1.0)) {   // invalid peak index or redshift from the caller
+    if (lane == 0) atomicAdd(a.counters + CNT_BADPEAK, 1ull);
+    write_no_collapse(out);
+    return;
+  }
   const int pk = (int)(lin / n2), pj = (int)((lin / n) % n), pi = (int)(lin % n);
   const double Rf = a.pk.Rf[p];
   const int ir2min = a.pk.ir2min[p];
-  const double ZZon = a.pk.ZZon[p];
   const double fcrit = a.pk.fcrit[p];
   const double alatt = a.alatt;
   const double* __restrict__ rad = a.rad;
   const int mmax = a.mmax;
-  double* out = a.out + p * RES_N;
 
-  Prof P{prof_base, a.nshell + 1, 0, a.counters};
+  Prof P{smem, SMEM_SHELLS + 1, 0, a.counters, SMEM_SHELLS, prof_base, a.nshell + 1};
+  double* part = smem + NV * (SMEM_SHELLS + 1);   // chunk partials [value][lane]
 
   // ---- geometry that depends only on the shell radii --------------------
   // m0 of the gather loop (RadialShell.jl:392-399): first finalised shell with
   // r^2 > ir2min, else the last finalised shell.
   int m0_init;
   {
-    int lo = 2, hi = mmax;   // first m in [2, mmax] with r2m[m] > ir2min
+    int lo = 2, hi = mmax;
     while (lo <= hi) {
       const int mid = (lo + hi) >> 1;
       if (a.r2m[mid] > ir2min) hi = mid - 1; else lo = mid + 1;
@@ -357,12 +380,9 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
   int mrf = 1;
   {
     const double rq = (Rf / alatt) * (Rf / alatt);
-    const int K = a.nshell - 1;          // nonzero distinct r^2 values: s = 1..K
-    // first s with r2_s >= rq (r2_s = rad[s+1]^2 for s <= K-1; the last group
-    // is not finalised, its r^2 comes from the cell list)
-    int lo = 1, hi = K;
-    // r^2 of the s-th nonzero distinct value is the r^2 of shell s+1
+    const int K = a.nshell - 1;
     auto r2s = [&](int s) -> double { return (double)a.r2m[s + 1]; };
+    int lo = 1, hi = K;
     while (lo <= hi) {
       const int mid = (lo + hi) >> 1;
       if (r2s(mid) >= rq) hi = mid - 1; else lo = mid + 1;
@@ -390,7 +410,6 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
 
   // ---- gather -----------------------------------------------------------
   const float4* __restrict__ aos = a.aos;
-  // centre cell (shell 1)
   {
     const float4 c0 = aos[2 * lin], c1 = aos[2 * lin + 1];
     if (lane == 0) {
@@ -406,70 +425,101 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
       for (int v = 0; v < 3; v++) { P.set(PV_G + v, 1, 0.0); P.set(PV_GF + v, 1, 0.0); }
 #pragma unroll
       for (int v = 0; v < 6; v++) P.set(PV_Q + v, 1, 0.0);
-      P.set(PV_DF, 1, (double)c0.x);
     }
   }
   const int rext = (int)ceil(rad[mmax]) + 1;
   const bool inside = pi - rext >= 0 && pj - rext >= 0 && pk - rext >= 0 && pi + rext < n && pj + rext < n &&
                       pk + rext < n;
-  // truncation state (warp-uniform)
   int state = 0;          // 0 unknown, 1 inward, 2 crossing found, 3 no crossing
   int mcross = 0;
-  int mtarget = mmax;     // last shell to gather
+  int mtarget = ADAPTIVE ? -1 : mmax;   // last shell to gather (-1: not known yet)
   int mdone = 1;
   double fbar_prev = (double)aos[2 * lin].x, df_prev = fbar_prev;
   long long visits = 0;
-  if (ADAPTIVE) {
-    // before any crossing information the walk needs at least the shells
-    // around m0_init and around the Rf window
-    mtarget = -1;
-  }
-  for (int base = 2; base <= mmax; base += 32) {
-    if (ADAPTIVE && mtarget >= 0 && base > mtarget) break;
-    const int m = base + lane;
-    const int mlim = ADAPTIVE && mtarget >= 0 ? mtarget : mmax;
-    if (m <= mlim) {
+  for (int g = 0; g < a.ngroups; g++) {
+    const int base = a.grp_a[g], gend = a.grp_b[g];
+    if (mtarget >= 0 && base > mtarget) break;
+    if (gend > P.cap) P.spill(mdone);   // profile outgrows shared memory
+    const int c0g = a.grp_c[g], ncg = a.grp_c[g + 1] - c0g;
+    // (a) lane l sums chunk c0g + l into the shared partial table
+    if (lane < ncg) {
       Acc<COMP> A;
       A.zero();
-      const int s0 = a.sh_start[m - 1], cnt = a.sh_count[m - 1];
+      const int s0 = a.ck_s[c0g + lane], cnt = a.ck_n[c0g + lane];
       int nsh = 0;
+      // loads of the next cell are issued before the current cell is summed
+      int4 cl = __ldg(a.cells + s0);
+      auto in_grid = [&](const int4& c) {
+        const int iv1 = pi + c.x, iv2 = pj + c.y, iv3 = pk + c.z;
+        return inside || (iv1 >= 0 && iv1 < n && iv2 >= 0 && iv2 < n && iv3 >= 0 && iv3 < n);
+      };
+      auto rec = [&](const int4& c) { return (int64_t)(pi + c.x) + (int64_t)n * (pj + c.y) + n2 * (pk + c.z); };
+      bool ok = in_grid(cl);
+      float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vb = va;
+      if (ok) { const int64_t li = rec(cl); va = __ldg(aos + 2 * li); vb = __ldg(aos + 2 * li + 1); }
       for (int c = 0; c < cnt; c++) {
-        const int4 cl = __ldg(a.cells + s0 + c);
-        const int iv1 = pi + cl.x, iv2 = pj + cl.y, iv3 = pk + cl.z;
-        if (!inside && (iv1 < 0 || iv1 >= n || iv2 < 0 || iv2 >= n || iv3 < 0 || iv3 >= n)) continue;
-        nsh++;
-        const int64_t li = iv1 + (int64_t)n * iv2 + n2 * iv3;
-        const float4 va = __ldg(aos + 2 * li), vb = __ldg(aos + 2 * li + 1);
-        accumulate_cell<COMP>(A, va, vb, (float)cl.x, (float)cl.y, (float)cl.z);
+        int4 cn = cl;
+        bool okn = false;
+        float4 van = va, vbn = vb;
+        if (c + 1 < cnt) {
+          cn = __ldg(a.cells + s0 + c + 1);
+          okn = in_grid(cn);
+          if (okn) { const int64_t li = rec(cn); van = __ldg(aos + 2 * li); vbn = __ldg(aos + 2 * li + 1); }
+        }
+        if (ok) {
+          nsh++;
+          accumulate_cell<COMP>(A, va, vb, (float)cl.x, (float)cl.y, (float)cl.z);
+        }
+        cl = cn; ok = okn; va = van; vb = vbn;
       }
       visits += nsh;
-      const double r = rad[m];
-      const double F = A.get(0);
-      P.set(PV_N, m, (double)nsh);
-      P.set(PV_DF, m, nsh > 0 ? F / nsh : 0.0);
 #pragma unroll
-      for (int L = 0; L < 3; L++) {
-        P.set(PV_S + L, m, A.get(1 + L));
-        P.set(PV_S2 + L, m, A.get(4 + L));
-        P.set(PV_G + L, m, A.get(7 + L) / r);
-        P.set(PV_GF + L, m, A.get(10 + L) / r);
-      }
-      P.set(PV_Q + 0, m, (2.0 * A.get(13)) / r);
-      P.set(PV_Q + 1, m, (2.0 * A.get(14)) / r);
-      P.set(PV_Q + 2, m, (2.0 * A.get(15)) / r);
-      P.set(PV_Q + 3, m, A.get(16) / r);
-      P.set(PV_Q + 4, m, A.get(17) / r);
-      P.set(PV_Q + 5, m, A.get(18) / r);
+      for (int v = 0; v < NACC; v++) part[v * 32 + lane] = A.get(v);
+      part[NACC * 32 + lane] = (double)nsh;
     }
     __syncwarp();
-    const int mend = min(base + 31, mlim);
-    // cumulative mean overdensity (RadialShell.jl:386-390), sequential
+    // (b) lane l finalises shell base + l from its chunks (double-precision
+    // sum of the chunk partials, each of which is exact to ~2^-48)
+    const int m = base + lane;
+    double my_dF = 0.0;
+    if (m <= gend) {
+      double t[NACC + 1];
+#pragma unroll
+      for (int v = 0; v <= NACC; v++) t[v] = 0.0;
+      const int k0 = a.sh_c0[m] - c0g, nk = a.sh_nc[m];
+      for (int k = k0; k < k0 + nk; k++) {
+#pragma unroll
+        for (int v = 0; v <= NACC; v++) t[v] += part[v * 32 + k];
+      }
+      const double r = rad[m];
+      const double nsh = t[NACC];
+      P.set(PV_N, m, nsh);
+      my_dF = nsh > 0 ? t[0] / nsh : 0.0;
+#pragma unroll
+      for (int L = 0; L < 3; L++) {
+        P.set(PV_S + L, m, t[1 + L]);
+        P.set(PV_S2 + L, m, t[4 + L]);
+        P.set(PV_G + L, m, t[7 + L] / r);
+        P.set(PV_GF + L, m, t[10 + L] / r);
+      }
+      P.set(PV_Q + 0, m, (2.0 * t[13]) / r);
+      P.set(PV_Q + 1, m, (2.0 * t[14]) / r);
+      P.set(PV_Q + 2, m, (2.0 * t[15]) / r);
+      P.set(PV_Q + 3, m, t[16] / r);
+      P.set(PV_Q + 4, m, t[17] / r);
+      P.set(PV_Q + 5, m, t[18] / r);
+    }
+    __syncwarp();
+    const int mend = gend;
+    // cumulative mean overdensity (RadialShell.jl:386-390), in shell order;
+    // every lane runs the recursion, the owner lane of shell mm keeps Fbar
+    double my_fb = 0.0;
     for (int mm = base; mm <= mend; mm++) {
-      const double dF = P.p[(int64_t)PV_DF * P.MS + mm];
+      const double dF = __shfl_sync(FULL, my_dF, mm - base);
       const double r3p = rad[mm - 1] * rad[mm - 1] * rad[mm - 1];
       const double r3 = rad[mm] * rad[mm] * rad[mm];
       const double fb = (r3p * fbar_prev + 0.5 * (df_prev + dF) * (r3 - r3p)) / r3;
-      if (lane == 0) P.set(PV_FBAR, mm, fb);
+      if (lane == mm - base) my_fb = fb;
       fbar_prev = fb;
       df_prev = dF;
       if (ADAPTIVE && state == 0 && mm >= m0_init) {
@@ -481,17 +531,14 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
         }
       }
     }
+    if (m <= mend) P.set(PV_FBAR, m, my_fb);
     mdone = mend;
     if (ADAPTIVE) {
       if (state == 0 && mdone >= mmax) state = 3;
       if (state != 0) {
-        int M = max(m0_init, mrf);
-        M = max(M, mupp_rf);
+        int M = max(max(m0_init, mrf), mupp_rf);
         if (state == 2) M = max(M, mcross);
-        if (state == 3) M = mmax;
-        // last shell with rad <= rad[M] + 2, plus two more
-        const int l = last_le(rad, M, mmax, rad[M] + 2.0);
-        mtarget = min(mmax, max(l, M) + 2);
+        mtarget = state == 3 ? mmax : a.need[M];
       }
     }
     __syncwarp();
@@ -503,27 +550,20 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
     if (lane == 0) atomicAdd(a.counters + CNT_VISITS, (unsigned long long)tv);
   }
 
-  // ---- post-process (double precision, warp-uniform) ---------------------
+  // ---- post-process (double precision) -----------------------------------
   const double hlatt = 1.0, anor = 1.0;
   const double aRnor = 3.0 * anor / alatt, wnor = anor / (4.0 * 3.141592653589793), wRnor = 3.0 * wnor / alatt;
   const int m = mmax;
 
   // Phase 3: gradient at the filter scale
-  const KS krf = kernel_strain(P, rad, mrf, mlow_rf, mupp_rf, a.akk, wRnor, aRnor, a.counters);
+  KS krf;
+  ks_multi(P, a, mrf, mlow_rf, mupp_rf, 32, wRnor, aRnor, &krf);
 
   // Phase 4: fcrit crossing (RadialShell.jl:494-537)
   int m0 = m0_init;
-  int mupp;
   if (P.get(PV_FBAR, m0) >= fcrit) {
-    bool found = false;
     for (int mm = m0; mm <= m; mm++) {
-      if (P.get(PV_FBAR, mm) < fcrit) { m0 = mm; found = true; break; }
-    }
-    if (!found) {
-      mupp = m;
-    } else {
-      const int l = last_lt(rad, m0 + 1, m, rad[m0] + 2.0);
-      mupp = l >= m0 + 1 ? l : m0;
+      if (P.get(PV_FBAR, mm) < fcrit) { m0 = mm; break; }
     }
   } else {
     const int mstart = max(m0 - 1, 1);
@@ -537,82 +577,61 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
       write_no_collapse(out);
       return;
     }
-    const int l = last_lt(rad, m0 + 1, m, rad[m0] + 2.0);
-    mupp = l >= m0 + 1 ? l : m0;
+  }
+  if (m0 == 1) {   // zvir1p at m0 is forced to -1 < ZZon (RadialShell.jl:581-622)
+    if (lane == 0) atomicAdd(a.counters + CNT_M0ONE, 1ull);
+    write_no_collapse(out);
+    return;
   }
 
-  // Phase 5: inward walk (RadialShell.jl:541-704)
-  int mlow = m0;
-  if (m0 > 1) {
-    const double rlow = fmax(rad[m0] - 2.0, 0.0);
-    const int f = first_gt(rad, 1, m0 - 1, rlow);
-    if (f <= m0 - 1) mlow = f;
-  }
+  // Phase 5: inward walk (RadialShell.jl:566-699).  Each round evaluates K
+  // consecutive steps top, top-1, ..., top-K+1 on K lane groups of G = 32/K
+  // lanes; group 0 repeats the last step of the previous round (the m0 step
+  // in round 0, whose zvir is forced to -1), so the step before a collapse is
+  // always the group to the left.  Most peaks collapse within a few steps of
+  // m0: round 0 uses 4 steps of 8 lanes, later rounds 32 steps of 1 lane.
+  // At mp = 1 the reference's running window is [2, last shell with rad < 2].
+  const int hi1 = last_lt(rad, 2, m, 2.0);
+  Walk last, prev;
   double zvir1 = -1.0, zvir1p = -1.0;
-  KS last, prev;     // (Ebar, grad, gradf) of the current and of the previous step
-  double Frhoh, Frho, e_v, p_v;
   bool collapsed = false;
-  {
-    const KS k0 = kernel_strain(P, rad, m0, mlow, mupp, a.akk, wRnor, aRnor, a.counters);
-    double F0, e0, p0;
-    ev_pv(k0.E, &F0, &e0, &p0);
-    // zvir1p at m0 is forced to -1 (RadialShell.jl:581-583), never >= ZZon > 0
-    zvir1 = -1.0;
-    prev = k0;   // strain_mat / gradpk_prev / gradpkf_prev
-    last = k0;   // Ebar_last / gradpk_last / gradpkf_last
-    Frhoh = F0;
-    Frho = P.get(PV_FBAR, m0);
-    e_v = e0;
-    p_v = p0;
-    if (-1.0 >= ZZon) {
-      collapsed = true;
-    } else {
-      if (m0 == 1) {
-        if (lane == 0) atomicAdd(a.counters + CNT_M0ONE, 1ull);
-        write_no_collapse(out);
-        return;
-      }
-      for (int mp = m0 - 1; mp >= 1; mp--) {
-        const double rupp_mp = rad[mp] + 2.0;
-        const double rlow_mp = fmax(rad[mp] - 2.0, 0.0);
-        if (rad[mupp] > rupp_mp) {
-          const int l = last_lt(rad, mp + 1, mupp, rupp_mp);
-          mupp = l >= mp + 1 ? l : mp;
-        }
-        if (mlow > 1 && rad[mlow - 1] > rlow_mp) {
-          const int f = first_gt(rad, 1, mlow - 1, rlow_mp);
-          if (f <= mlow - 1) mlow = f;
-        }
-        const KS kmp = kernel_strain(P, rad, mp, mlow, mupp, a.akk, wRnor, aRnor, a.counters);
-        double Fh, ev, pv;
-        ev_pv(kmp.E, &Fh, &ev, &pv);
-        const double Fr = P.get(PV_FBAR, mp);
-        double zp = -1.0;
-        if (Fr > 0.0) {
-          const double poe = ev < 1e-5 ? 0.0 : pv / ev;
-          zp = tab_interp(a.tab, log10(Fr), ev, poe);
-        }
-        if (zp >= ZZon) {
-          m0 = mp + 1;
-          zvir1p = zp;
-          last = kmp;
-          Frhoh = Fh;
-          Frho = Fr;
-          e_v = ev;
-          p_v = pv;
-          collapsed = true;
-          break;
-        }
-        zvir1 = zp;
-        prev = kmp;
-        last = kmp;
-        Frhoh = Fh;
-        Frho = Fr;
-        e_v = ev;
-        p_v = pv;
-      }
+  int rounds = 0;
+  int top = m0;
+  for (int b = 0;; b++) {
+    rounds++;
+    const int G = b == 0 ? 8 : 1;
+    const int K = 32 / G;
+    const int grp = lane / G;
+    const int mp = top - grp;
+    Walk w;
+    w.zv = -1.0;
+    // the running mlow never reaches shell 1 (rad 0 is not > max(rad-2, 0))
+    ks_multi(P, a, mp, 2, mp > 1 ? m : hi1, G, wRnor, aRnor, &w.k);
+    const bool act = mp >= 1;
+    if (act) {
+      ev_pv(w.k.E, &w.Fh, &w.ev, &w.pv);
+      w.Fr = P.get(PV_FBAR, mp);
+      if (!(b == 0 && grp == 0)) w.zv = zvir_of(a.tab, w.Fr, w.ev, w.pv);
     }
+    const unsigned bal = __ballot_sync(FULL, act && grp >= 1 && (lane & (G - 1)) == 0 && w.zv >= ZZon);
+    if (bal) {
+      const int L = __ffs(bal) - 1;
+      last.k = shfl_ks(w.k, L);
+      prev.k = shfl_ks(w.k, L - G);
+      last.Fh = __shfl_sync(FULL, w.Fh, L);
+      last.Fr = __shfl_sync(FULL, w.Fr, L);
+      last.ev = __shfl_sync(FULL, w.ev, L);
+      last.pv = __shfl_sync(FULL, w.pv, L);
+      zvir1p = __shfl_sync(FULL, w.zv, L);
+      zvir1 = __shfl_sync(FULL, w.zv, L - G);   // -1 when group L/G - 1 is the m0 step
+      m0 = top - L / G + 1;
+      collapsed = true;
+      break;
+    }
+    if (top - (K - 1) <= 1) break;   // reached mp = 1 without collapse
+    top -= K - 1;
   }
+  if (lane == 0) atomicAdd(a.counters + CNT_WALK, (unsigned long long)rounds);
   if (!collapsed) {
     if (lane == 0) atomicAdd(a.counters + CNT_NOCOLL, 1ull);
     write_no_collapse(out);
@@ -645,18 +664,18 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
     const double fr = (RTHL3 - rad3p) / drad3;
     Fbarx = Fa + fr * dFb;
 #pragma unroll
-    for (int q = 0; q < 6; q++) S[q] = last.E[q] + fr * (prev.E[q] - last.E[q]);
+    for (int q = 0; q < 6; q++) S[q] = last.k.E[q] + fr * (prev.k.E[q] - last.k.E[q]);
 #pragma unroll
     for (int L = 0; L < 3; L++) {
-      gk[L] = last.g[L] + fr * (prev.g[L] - last.g[L]);
-      gkf[L] = last.gf[L] + fr * (prev.gf[L] - last.gf[L]);
+      gk[L] = last.k.g[L] + fr * (prev.k.g[L] - last.k.g[L]);
+      gkf[L] = last.k.gf[L] + fr * (prev.k.gf[L] - last.k.gf[L]);
     }
   } else {
     Fbarx = Fa;
 #pragma unroll
-    for (int q = 0; q < 6; q++) S[q] = last.E[q];
+    for (int q = 0; q < 6; q++) S[q] = last.k.E[q];
 #pragma unroll
-    for (int L = 0; L < 3; L++) { gk[L] = prev.g[L]; gkf[L] = prev.gf[L]; }
+    for (int L = 0; L < 3; L++) { gk[L] = prev.k.g[L]; gkf[L] = prev.k.gf[L]; }
   }
   // normalize_strain then eigenvalues (RadialShell.jl:748-752)
   {
@@ -669,10 +688,9 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
   }
   double Frhoc, e_v_f, p_v_f;
   ev_pv(S, &Frhoc, &e_v_f, &p_v_f);
-  if (!(Frhoc > 0.0)) { e_v_f = 0.0; p_v_f = 0.0; }
   double smat[6];
 #pragma unroll
-  for (int q = 0; q < 6; q++) smat[q] = last.E[q] * (Fbarx / Frhoh);
+  for (int q = 0; q < 6; q++) smat[q] = last.k.E[q] * (Fbarx / last.Fh);
 
   // Phase 7: Sbar, Sbar2 (RadialShell.jl:758-773), Srb (:776-790)
   double sb[6] = {0, 0, 0, 0, 0, 0};
@@ -689,7 +707,7 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
       nS += (long long)nn;
     }
     if (m1 >= 2) {
-      const double r5 = pow(rad[m1], 5.0), r5p = m1 - 1 >= 2 ? pow(rad[m1 - 1], 5.0) : 0.0;
+      const double r5 = a.rad5[m1], r5p = m1 - 1 >= 2 ? a.rad5[m1 - 1] : 0.0;
       srb += 0.5 * (P.get(PV_FBAR, m1 - 1) + P.get(PV_FBAR, m1)) * (r5 - r5p);
     }
   }
@@ -701,7 +719,7 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
 #pragma unroll
     for (int q = 0; q < 6; q++) sb[q] /= (double)nS;
   }
-  const double rad5p = (m0 - 1 >= 2) ? pow(rad[m0 - 1], 5.0) : 0.0;
+  const double rad5p = (m0 - 1 >= 2) ? a.rad5[m0 - 1] : 0.0;
   if (zvir1 > 0.0 && dZvir != 0.0) srb += 0.5 * (Fa + Fbarx) * (RTHL5 - rad5p);
   if (Fbarx * RTHL5 > 0.0) srb /= (Fbarx * RTHL5);
 
@@ -731,7 +749,6 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
         stop = true;
       }
       if (valid) { acc += (double)v; navg++; }
-      // all later cells have larger r2; stop once the whole chunk is beyond RTHL
       const int4 last_cell = __ldg(a.cells + min(c0 + 31, a.npart - 1));
       if (sqrt((double)last_cell.w) > RTHL) stop = true;
     }
@@ -740,85 +757,92 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base) {
     if (navg > 0) d2F = acc / (double)navg;
   }
 
-  // zvir_half (RadialShell.jl:825-885)
+  // zvir_half (RadialShell.jl:825-885): the ten radii on lane pairs 0..19
   double zvir_half = -1.0;
   if (RTHL / hlatt >= 3.0) {
-    for (int jj = 1; jj <= 10; jj++) {
-      const double rcur = RTHL * pow((jj - 1) / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
-      const double rupp_rc = rcur + 2.0 * hlatt;
-      int mupp_rc = 1;
-      for (int m1 = 2; m1 <= m - 1; m1++) {
-        if (rad[m1] > rupp_rc) { mupp_rc = m1; break; }
-        else if (rad[m1] == 0.0) { mupp_rc = m1 - 1; break; }
-        mupp_rc = m1;
-      }
-      const double rlow_rc = fmax(rcur - 2.0 * hlatt, 0.0);
-      int mlow_rc = 1;
-      {
-        const int f = first_gt(rad, 1, m - 1, rlow_rc);
-        if (f <= m - 1) mlow_rc = f;
-      }
-      int m0_rc = 1;
-      {
-        const int f = first_gt(rad, 1, m - 1, rcur);
-        m0_rc = (f <= m - 1) ? f : max(m - 1, 1);
-      }
-      const KS krc = kernel_strain(P, rad, m0_rc, mlow_rc, mupp_rc, a.akk, wRnor, aRnor, a.counters);
+    const int e = lane >> 1;   // radius index jj - 1
+    int m0_rc = 0, mlow_rc = 1, mupp_rc = 1;
+    if (e < 10) {
+      const double rcur = RTHL * pow(e / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
+      // first m1 in [2, m-1] with rad > rcur + 2 (the loop's break), else m-1
+      const int fu = first_gt(rad, 2, m - 1, rcur + 2.0 * hlatt);
+      mupp_rc = fu <= m - 1 ? fu : (m - 1 >= 2 ? m - 1 : 1);
+      const int fl = first_gt(rad, 1, m - 1, fmax(rcur - 2.0 * hlatt, 0.0));
+      if (fl <= m - 1) mlow_rc = fl;
+      const int f0 = first_gt(rad, 1, m - 1, rcur);
+      m0_rc = (f0 <= m - 1) ? f0 : max(m - 1, 1);
+    }
+    KS krc;
+    ks_multi(P, a, m0_rc, mlow_rc, mupp_rc, 2, wRnor, aRnor, &krc);
+    double zl = -1.0;
+    if (e < 10) {
       double Fr, ev, pv;
       ev_pv(krc.E, &Fr, &ev, &pv);
-      const double Frc = P.get(PV_FBAR, m0_rc);
-      const double poe = ev < 1e-5 ? 0.0 : pv / ev;
-      double zrc = -1.0;
-      if (Frc > 0.0) zrc = tab_interp(a.tab, log10(Frc), ev, poe);
-      zvir_half = fmax(zrc - 1.0, zvir_half);
+      zl = zvir_of(a.tab, P.get(PV_FBAR, m0_rc), ev, pv) - 1.0;
     }
+    zvir_half = fmax(warp_max(zl), -1.0);
   }
 
   // results (layout in ppb.h)
-  double r[RES_N];
-  r[0] = RTHL;
-  r[1] = srb;
-#pragma unroll
-  for (int L = 0; L < 3; L++) {
-    r[2 + L] = sb[L];
-    r[5 + L] = sb[3 + L];
-    r[17 + L] = gk[L];
-    r[20 + L] = krf.g[L];
-    r[27 + L] = gkf[L];
-  }
-  // strain column-major 3x3 from (xx yy zz xy xz yz)
-  r[8] = smat[0]; r[9] = smat[3]; r[10] = smat[4];
-  r[11] = smat[3]; r[12] = smat[1]; r[13] = smat[5];
-  r[14] = smat[4]; r[15] = smat[5]; r[16] = smat[2];
-  r[23] = Fbarx;
-  r[24] = e_v_f;
-  r[25] = p_v_f;
-  r[26] = zvir_half;
-  r[30] = d2F;
   if (lane == 0) {
+    double r[RES_N];
+    r[0] = RTHL;
+    r[1] = srb;
+#pragma unroll
+    for (int L = 0; L < 3; L++) {
+      r[2 + L] = sb[L];
+      r[5 + L] = sb[3 + L];
+      r[17 + L] = gk[L];
+      r[20 + L] = krf.g[L];
+      r[27 + L] = gkf[L];
+    }
+    r[8] = smat[0]; r[9] = smat[3]; r[10] = smat[4];
+    r[11] = smat[3]; r[12] = smat[1]; r[13] = smat[5];
+    r[14] = smat[4]; r[15] = smat[5]; r[16] = smat[2];
+    r[23] = Fbarx;
+    r[24] = e_v_f;
+    r[25] = p_v_f;
+    r[26] = zvir_half;
+    r[30] = d2F;
 #pragma unroll
     for (int q = 0; q < RES_N; q++) out[q] = r[q];
   }
-  (void)Frho; (void)e_v; (void)p_v;
 }
 
 template <bool COMP, bool ADAPTIVE>
-__global__ void __launch_bounds__(128) shell_kernel(ShellArgs a) {
+__global__ void __launch_bounds__(128, 3) shell_kernel(ShellArgs a) {
   const int lane = threadIdx.x & 31;
   const int warp_in_block = threadIdx.x >> 5;
   const int64_t slot = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_in_block;
   double* prof = a.scratch + slot * a.scratch_stride;
+  extern __shared__ double shm[];
+  double* smem = shm + (size_t)warp_in_block * SMEM_WARP_DOUBLES;
   while (true) {
     int p = 0;
     if (lane == 0) p = atomicAdd(a.queue, 1);
     p = __shfl_sync(FULL, p, 0);
     if (p >= a.npk) break;
-    analyse_one<COMP, ADAPTIVE>(a, p, prof);
+    analyse_one<COMP, ADAPTIVE>(a, p, prof, smem);
     __syncwarp();
   }
 }
 
+template <bool C, bool A>
+void launch_variant(const ShellArgs& a, dim3 grid, dim3 block, size_t shm, cudaStream_t s) {
+  shell_kernel<C, A><<<grid, block, shm, s>>>(a);
+}
+
 }  // namespace
+
+// allow the dynamic shared memory of the chosen block size (once per process
+// and device; called before occupancy queries and launches)
+void shell_prepare(int warps_per_block) {
+  const int shm = (int)((size_t)warps_per_block * SMEM_WARP_DOUBLES * 8);
+  PPB_CUDA(cudaFuncSetAttribute(shell_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
+  PPB_CUDA(cudaFuncSetAttribute(shell_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
+  PPB_CUDA(cudaFuncSetAttribute(shell_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
+  PPB_CUDA(cudaFuncSetAttribute(shell_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
+}
 
 const void* shell_kernel_ptr(bool comp, bool adaptive) {
   if (comp && adaptive) return (const void*)shell_kernel<true, true>;
@@ -829,12 +853,15 @@ const void* shell_kernel_ptr(bool comp, bool adaptive) {
 
 int64_t shell_scratch_doubles_per_warp(int nshell) { return (int64_t)NV * (nshell + 1); }
 
+size_t shell_smem_bytes(int warps_per_block) { return (size_t)warps_per_block * SMEM_WARP_DOUBLES * 8; }
+
 void launch_shell(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks, int warps_per_block) {
   dim3 grid(blocks), block(32 * warps_per_block);
-  if (comp && adaptive) shell_kernel<true, true><<<grid, block, 0, L.s>>>(a);
-  else if (comp && !adaptive) shell_kernel<true, false><<<grid, block, 0, L.s>>>(a);
-  else if (!comp && adaptive) shell_kernel<false, true><<<grid, block, 0, L.s>>>(a);
-  else shell_kernel<false, false><<<grid, block, 0, L.s>>>(a);
+  const size_t shm = shell_smem_bytes(warps_per_block);
+  if (comp && adaptive) launch_variant<true, true>(a, grid, block, shm, L.s);
+  else if (comp && !adaptive) launch_variant<true, false>(a, grid, block, shm, L.s);
+  else if (!comp && adaptive) launch_variant<false, true>(a, grid, block, shm, L.s);
+  else launch_variant<false, false>(a, grid, block, shm, L.s);
   PPB_LAUNCHED(*L.count);
 }
 

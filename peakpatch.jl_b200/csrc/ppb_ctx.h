@@ -26,6 +26,7 @@ struct TileRes {
 struct ShellStats {
   unsigned long long visits = 0, guard = 0, akk = 0;
   unsigned long long dump[5] = {0, 0, 0, 0, 0};
+  unsigned long long raw[16] = {};
   float ms = 0.f;
 };
 

@@ -77,6 +77,8 @@ struct DevBuf {
 // ---------------------------------------------------------------------------
 // geometry of the sorted shell-cell list (precompute_shells)
 // ---------------------------------------------------------------------------
+constexpr int kChunkCells = 24;   // gather chunk size (cells per lane per group)
+
 struct ShellTable {
   int nhunt = -1;
   int64_t ncells = 0;                 // cells with r2 <= nhunt^2 (including the centre)
@@ -87,9 +89,32 @@ struct ShellTable {
   std::vector<int32_t> shell_r2;
   std::vector<double> rad;            // rad[m] (m = 0..nshell), rad[1] = 0
   std::vector<int32_t> r2m;           // r2 of shell m (m = 0..nshell)
-  DevBuf d_cells, d_start, d_count, d_r2m, d_rad;
+  // kernel_strain weights (RadialShell.jl:234-253): for centre shell mp >= 2
+  // the shells m1 with (rad[mp] - rad[m1])^2 < 4 form the contiguous window
+  // [win_lo[mp], win_hi[mp]]; wts[win_off[mp] + (m1 - win_lo[mp])] holds
+  // hRinteg(u0, u12) / (u12 - u0^2)^2 for that pair.
+  std::vector<int32_t> win_lo, win_hi, win_off;
+  std::vector<double> wts;
+  // mp == 1 weights 0.5 * akk(rad[m1]) / rad[m1] (:255-271); NaN where the
+  // reference's akk lookup would run past the table
+  std::vector<double> w1;
+  // first shell m' with rad[m'] > rad[m] + 2, plus one (gather truncation)
+  std::vector<int32_t> need;
+  // rad[m]^5 (Srb integral, RadialShell.jl:776-790)
+  std::vector<double> rad5;
+  // gather schedule: shells m >= 2 split into chunks of at most
+  // kChunkCells cells; consecutive chunks packed into groups of at most 32
+  // (one chunk per lane) that end on a shell boundary.  Group g covers shells
+  // [grp_a[g], grp_b[g]] and chunks [grp_c[g], grp_c[g+1]); chunk c holds
+  // ck_n[c] cells from ck_s[c]; shell m's chunks start at sh_c0[m] (sh_nc[m]).
+  std::vector<int32_t> grp_a, grp_b, grp_c, ck_s, ck_n, sh_c0, sh_nc;
+  int ngroups = 0;
+  DevBuf d_cells, d_start, d_count, d_r2m, d_rad, d_wlo, d_whi, d_woff, d_wts, d_w1, d_need, d_rad5;
+  DevBuf d_grp_a, d_grp_b, d_grp_c, d_ck_s, d_ck_n, d_sh_c0, d_sh_nc;
 };
 void build_shell_table(ShellTable& st, int nhunt);
+double hRinteg(double u0, double u12);
+std::vector<double> make_atab4();
 void upload_shell_table(ShellTable& st, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
@@ -147,6 +172,15 @@ struct ShellArgs {
   const int32_t* sh_count;
   const double* rad;        // rad[m], m = 0..nshell (index 0 unused); rad[1] = 0
   const int32_t* r2m;       // r^2 of shell m, m = 1..nshell (shell nshell is the unfinalised last group)
+  const int32_t* win_lo;    // kernel_strain windows and weights (see ShellTable)
+  const int32_t* win_hi;
+  const int32_t* win_off;
+  const double* wts;
+  const double* w1;
+  const int32_t* need;
+  const double* rad5;
+  const int32_t *grp_a, *grp_b, *grp_c, *ck_s, *ck_n, *sh_c0, *sh_nc;
+  int ngroups;
   int nshell;               // distinct r2 values in the list (incl. 0)
   int mmax;                 // finalised shells: nshell - 1
   int64_t npart;            // cells used (full list here)
@@ -194,6 +228,8 @@ void launch_peakfind(Launch L, const float* ds, const float* ls, uint8_t* mask, 
                      int nbuff, float fcrit, int fidx, PeakBuf pb);
 
 int64_t shell_scratch_doubles_per_warp(int nshell);
+size_t shell_smem_bytes(int warps_per_block);
+void shell_prepare(int warps_per_block);
 // comp: compensated single-precision sums (else double); adaptive: radial
 // truncation of the gather (else full spheres).  Persistent grid of
 // blocks x warps_per_block warps; a.scratch must hold one profile per warp.

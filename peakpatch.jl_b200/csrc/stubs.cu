@@ -225,4 +225,10 @@ int32_t ppb_last_shell_stats(ppb_ctx* ctx, int64_t* visits, int64_t* dumps5, flo
   return PPB_OK;
 }
 
+int32_t ppb_shell_counters(ppb_ctx* ctx, int64_t* out16) {
+  if (!ctx || !out16) return PPB_ERR_INVALID;
+  for (int i = 0; i < 16; i++) out16[i] = (int64_t)ctx->last_shell.raw[i];
+  return PPB_OK;
+}
+
 }  // extern "C"

@@ -86,7 +86,7 @@ EXPORTED = (
     "ppb_set_pk_table", "ppb_run_tile", "ppb_run_tile_timed", "ppb_write_pksc", "ppb_noise_threefry",
     "ppb_find_peaks", "ppb_analyse_peaks", "ppb_event_record", "ppb_event_elapsed", "ppb_synchronize",
     "ppb_launch_count", "ppb_last_shell_stats", "ppb_last_stage_ms", "ppb_alloc_host", "ppb_free_host",
-    "ppb_alloc_device", "ppb_free_device",
+    "ppb_alloc_device", "ppb_free_device", "ppb_shell_counters",
 )
 
 
@@ -123,6 +123,7 @@ def load_library():
     L.ppb_launch_count.argtypes = [P, ctypes.POINTER(ctypes.c_int64)]
     L.ppb_last_shell_stats.argtypes = [P, ctypes.POINTER(ctypes.c_int64), P, ctypes.POINTER(ctypes.c_float)]
     L.ppb_last_stage_ms.argtypes = [P, P]
+    L.ppb_shell_counters.argtypes = [P, P]
     for f in ("ppb_alloc_host", "ppb_alloc_device"):
         getattr(L, f).argtypes = [P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
     for f in ("ppb_free_host", "ppb_free_device"):
@@ -338,8 +339,11 @@ class Context:
         d = np.zeros(5, np.int64)
         ms = ctypes.c_float()
         self._check(self.L.ppb_last_shell_stats(self.h, ctypes.byref(v), _p(d), ctypes.byref(ms)))
+        raw = np.zeros(16, np.int64)
+        self._check(self.L.ppb_shell_counters(self.h, _p(raw)))
         return {"visits": v.value, "dumps": dict(zip(("premask", "no_fcrit", "m0_one", "no_collapse", "rthl_neg"),
-                                                      d.tolist())), "ms": ms.value}
+                                                      d.tolist())), "ms": ms.value, "guard": int(raw[6]),
+                "akk_overrun": int(raw[7]), "bad_peaks": int(raw[8]), "walk_rounds": int(raw[9])}
 
     def stage_ms(self):
         a = np.zeros(4, np.float32)

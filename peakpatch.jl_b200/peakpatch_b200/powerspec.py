@@ -72,7 +72,7 @@ def write_pk(path: str, k: np.ndarray, P: np.ndarray, header: str = "") -> None:
             for line in header.splitlines():
                 f.write(f"# {line}\n")
         for kk, pp in zip(k, P):
-            f.write(f"{kk!r}  {pp!r}\n")
+            f.write(f"{float(kk)!r}  {float(pp)!r}\n")
 
 
 def rescale_sigma8(P: np.ndarray, sigma8_new: float, sigma8_ref: float = 0.808) -> np.ndarray:
