@@ -142,6 +142,21 @@ int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n
                        int32_t n3, int32_t nbuff, float fcrit, int64_t max_peaks, int64_t* pi,
                        int64_t* pj, int64_t* pk, int64_t* ipp, float* pdelta, int64_t* npeaks);
 
+/* ppb_find_peaks for callers that cannot allocate device memory at call time
+ * (memory owned by another runtime's pool, or a fixed-footprint service loop
+ * where cudaMalloc/cudaFree are not allowed).  No counterpart in the
+ * reference: it is an addition of this library.  Same results as
+ * ppb_find_peaks, but every array argument must be device memory owned by the
+ * caller (npeaks is a host pointer) and the call allocates nothing: its
+ * scratch is a 2 MiB array built into the library, which limits the inner
+ * cube to 268,435,456 cells (larger inputs return PPB_ERR_INVALID).  All
+ * calls on a device share that array, so calls that overlap on the GPU race
+ * and must be serialised; the first call on a device looks up the array's
+ * address and should come before any stream capture. */
+int32_t ppb_find_peaks_noalloc(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n1, int32_t n2,
+                               int32_t n3, int32_t nbuff, float fcrit, int64_t max_peaks, int64_t* pi,
+                               int64_t* pj, int64_t* pk, int64_t* ipp, float* pdelta, int64_t* npeaks);
+
 /* analyse_peak over a batch of peaks (src/HaloFinder/RadialShell.jl:282-891;
  * GPU stub analyse_peaks_gpu_cuda_multirf, src/PeakPatch.jl:231-253).
  * Fields are n^3 Float32 column-major (cubic grid); eta2* and lapd may be

@@ -86,7 +86,7 @@ EXPORTED = (
     "ppb_set_pk_table", "ppb_run_tile", "ppb_run_tile_timed", "ppb_write_pksc", "ppb_noise_threefry",
     "ppb_find_peaks", "ppb_analyse_peaks", "ppb_event_record", "ppb_event_elapsed", "ppb_synchronize",
     "ppb_launch_count", "ppb_last_shell_stats", "ppb_last_stage_ms", "ppb_alloc_host", "ppb_free_host",
-    "ppb_alloc_device", "ppb_free_device", "ppb_shell_counters",
+    "ppb_alloc_device", "ppb_free_device", "ppb_shell_counters", "ppb_find_peaks_noalloc",
 )
 
 
@@ -116,6 +116,7 @@ def load_library():
     L.ppb_noise_threefry.argtypes = [P, P, I32, ctypes.c_uint64]
     L.ppb_find_peaks.argtypes = [P, P, P, I32, I32, I32, I32, ctypes.c_float, I64, P, P, P, P, P,
                                  ctypes.POINTER(ctypes.c_int64)]
+    L.ppb_find_peaks_noalloc.argtypes = L.ppb_find_peaks.argtypes
     L.ppb_analyse_peaks.argtypes = [P] * 9 + [I32, I32, I64, P, P, P, P, P, D, I32, P]
     L.ppb_event_record.argtypes = [P, I32]
     L.ppb_event_elapsed.argtypes = [P, I32, I32, ctypes.POINTER(ctypes.c_float)]
