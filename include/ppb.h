@@ -107,7 +107,7 @@ int32_t ppb_abi_version(void);
 int32_t ppb_set_collapse_table(ppb_ctx* ctx, const float* tab, int32_t nx, int32_t ny, int32_t nz,
                                double x1, double x2, double y1, double y2, double z1, double z2);
 /* P(k) table (k in h/Mpc, P in the reference's file convention) for the
- * log-log interpolant of load_pk (src/InitialConditions/PowerSpectrum.jl:189-201). */
+ * log-log interpolant of load_pk (src/InitialConditions/PowerSpectrum.jl:11-30). */
 int32_t ppb_set_pk_table(ppb_ctx* ctx, const double* k, const double* pk, int32_t n);
 
 /* ---- the drop-in for run_tile ------------------------------------------ */

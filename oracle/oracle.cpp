@@ -78,7 +78,7 @@ void ora_noise_region(float* out, int64_t n, uint64_t seed, int64_t i0, int64_t 
 
 // ---------------------------------------------------------------------------
 // P(k) table: log-log linear interpolation with linear extrapolation in
-// log-log beyond the ends.  PowerSpectrum.jl:189-201 (Interpolations.jl
+// log-log beyond the ends.  PowerSpectrum.jl:11-30 (Interpolations.jl
 // Gridded(Linear()) + extrapolate(Line())).
 // ---------------------------------------------------------------------------
 static double pk_eval(const double* lk, const double* lp, int np, double k) {

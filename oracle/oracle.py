@@ -115,7 +115,7 @@ def num_threads() -> int:
 # File formats (reference readers restated)
 # --------------------------------------------------------------------------
 def read_pk(path: str):
-    """2-column ASCII (k, P); '#' comments.  PowerSpectrum.jl:189-192."""
+    """2-column ASCII (k, P); '#' comments.  PowerSpectrum.jl:11-30."""
     d = np.loadtxt(path, comments="#")
     return np.ascontiguousarray(d[:, 0], dtype=np.float64), np.ascontiguousarray(d[:, 1], dtype=np.float64)
 

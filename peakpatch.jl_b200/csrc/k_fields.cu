@@ -69,7 +69,7 @@ __global__ void noise_kernel(float* __restrict__ out, int64_t ncell, uint64_t se
 
 // ---------------------------------------------------------------------------
 // P(k): log-log linear interpolation with linear extrapolation
-// (PowerSpectrum.jl:189-201)
+// (PowerSpectrum.jl:11-30)
 // ---------------------------------------------------------------------------
 __device__ double pk_eval(const double* __restrict__ lk, const double* __restrict__ lp, int np, double k) {
   const double x = log(k);

@@ -1,0 +1,169 @@
+"""
+    PeakPatchB200
+
+Julia binding of libppb.so, the B200 implementation of PeakPatch.jl's per-tile
+halo-finding path.  It supplies a drop-in `run_tile(cfg; seed)` with the
+signature and behaviour of `PeakPatch.Pipeline.run_tile` (src/Pipeline.jl:66)
+and GPU methods for the stub-level entry points `fill_noise_threefry!`
+(src/InitialConditions/RandomField.jl:70), `find_peaks`
+(src/HaloFinder/PeakFind.jl:123) and a batched `analyse_peak`
+(src/HaloFinder/RadialShell.jl:282), all through `ccall` into the C ABI
+declared in include/ppb.h.  Errors become Julia exceptions carrying the
+library's message.
+
+Usage (with PeakPatch.jl loaded for PipelineConfig, read_homeltab, ...):
+
+    using PeakPatch, PeakPatchB200
+    cfg = PipelineConfig(TOML.parsefile("config.toml"))
+    halos = PeakPatchB200.run_tile(cfg; seed=42)      # Vector{ExtHaloRecord} or Vector{HaloRecord}
+
+Set ENV["PPB_LIBRARY"] to the path of libppb.so (default: next to this file's
+parent directory).
+"""
+module PeakPatchB200
+
+using DelimitedFiles: readdlm
+
+const libppb = get(ENV, "PPB_LIBRARY", joinpath(@__DIR__, "..", "libppb.so"))
+
+const PPB_OK = Int32(0)
+const PPB_ERR_CAPACITY = Int32(-7)
+
+# ppb_tile_params (include/ppb.h); field order and types must match the C struct
+struct TileParams
+    Omx::Float64; OmB::Float64; Omvac::Float64; h::Float64
+    n::Int32
+    boxsize::Float64
+    nbuff::Int32
+    z_out::Float64; z_max::Float64
+    ievol::Int32
+    cenx::Float64; ceny::Float64; cenz::Float64
+    ilpt::Int32
+    ioutshear::Int32
+    wsmooth::Int32
+    rmax2rs::Float64
+    seed::UInt64
+    plain::Int32
+    reserved::NTuple{7,Int32}
+end
+
+mutable struct HaloBuf
+    records::Ptr{Float32}
+    capacity::Int64
+    count::Int64
+    nfields::Int32
+    RTHLmax::Float32
+    npeaks::Int64
+end
+
+mutable struct Context
+    h::Ptr{Cvoid}
+end
+
+function check(ctx::Context, rc::Int32)
+    rc == PPB_OK && return nothing
+    buf = Vector{UInt8}(undef, 1024)
+    ccall((:ppb_last_error, libppb), Int32, (Ptr{Cvoid}, Ptr{UInt8}, Csize_t), ctx.h, buf, length(buf))
+    error("libppb error $(rc): " * unsafe_string(pointer(buf)))
+end
+
+function Context(device::Integer=0; hbm_budget::Integer=0)
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = ccall((:ppb_ctx_create, libppb), Int32, (Int32, UInt64, Ref{Ptr{Cvoid}}), device, hbm_budget, h)
+    rc == PPB_OK || error("ppb_ctx_create failed ($rc): no usable CUDA device?")
+    ctx = Context(h[])
+    finalizer(c -> (c.h != C_NULL && ccall((:ppb_ctx_destroy, libppb), Int32, (Ptr{Cvoid},), c.h); c.h = C_NULL), ctx)
+    return ctx
+end
+
+const _ctx = Ref{Union{Nothing,Context}}(nothing)
+default_context() = (_ctx[] === nothing && (_ctx[] = Context(0)); _ctx[])
+
+"""Upload the collapse table (read_homeltab output) to the device."""
+function set_collapse_table!(ctx::Context, table::Array{Float32,3}, tp)
+    nx, ny, nz = size(table)
+    check(ctx, ccall((:ppb_set_collapse_table, libppb), Int32,
+                     (Ptr{Cvoid}, Ptr{Float32}, Int32, Int32, Int32, Float64, Float64, Float64, Float64, Float64, Float64),
+                     ctx.h, table, nx, ny, nz, tp.X1, tp.X2, tp.Y1, tp.Y2, tp.Z1, tp.Z2))
+end
+
+"""Upload the P(k) table of a load_pk-style file (2 columns: k, P)."""
+function set_pk_table!(ctx::Context, path::AbstractString)
+    data = readdlm(path, comments=true)
+    k = Float64.(data[:, 1]); P = Float64.(data[:, 2])
+    check(ctx, ccall((:ppb_set_pk_table, libppb), Int32, (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Int32),
+                     ctx.h, k, P, length(k)))
+end
+
+function tile_params(cfg, seed::Integer; plain::Bool=false)
+    TileParams(cfg.Omx, cfg.OmB, cfg.Omvac, cfg.h, Int32(cfg.n), cfg.boxsize, Int32(cfg.nbuff),
+               cfg.z_out, cfg.z_max, Int32(cfg.ievol), cfg.cenx, cfg.ceny, cfg.cenz, Int32(cfg.ilpt),
+               Int32(cfg.ioutshear), Int32(cfg.wsmooth), cfg.rmax2rs, UInt64(seed), Int32(plain),
+               ntuple(_ -> Int32(0), 7))
+end
+
+"""
+    run_tile(cfg::PipelineConfig; seed=42, verbose=false) -> Vector{HaloRecord} or Vector{ExtHaloRecord}
+
+Drop-in for PeakPatch.run_tile: reads cfg.pkfile, cfg.filterfile and
+cfg.tabfile, runs the tile on the GPU, writes cfg.fileout (.pksc) and
+returns the records in the reference's peak order.
+"""
+function run_tile(cfg; seed::Integer=42, verbose::Bool=false, ctx::Context=default_context())
+    PP = Base.root_module(Base.__toplevel__, :PeakPatch)
+    table, tp = PP.read_homeltab(cfg.tabfile)
+    set_collapse_table!(ctx, table, tp)
+    set_pk_table!(ctx, cfg.pkfile)
+    Rf = Float64[f[3] for f in PP.read_filterbank(cfg.filterfile)]
+    params = Ref(tile_params(cfg, seed))
+    nf = cfg.ioutshear >= 1 ? 33 : 11
+    cap = 1 << 20
+    while true
+        buf = Vector{Float32}(undef, nf * cap)
+        hb = Ref(HaloBuf(pointer(buf), cap, 0, 0, 0f0, 0))
+        rc = GC.@preserve buf ccall((:ppb_run_tile, libppb), Int32,
+                                    (Ptr{Cvoid}, Ref{TileParams}, Ptr{Float64}, Int32, Ref{HaloBuf}),
+                                    ctx.h, params, Rf, length(Rf), hb)
+        if rc == PPB_ERR_CAPACITY
+            cap = Int(hb[].count) + 16
+            continue
+        end
+        check(ctx, rc)
+        n = Int(hb[].count)
+        recs = reshape(buf[1:nf * n], nf, n)
+        halos = nf == 33 ? [PP.ExtHaloRecord(recs[:, i]...) for i in 1:n] :
+                           [PP.HaloRecord(recs[:, i]...) for i in 1:n]
+        PP.write_pksc(cfg.fileout, halos, hb[].RTHLmax, Float32(cfg.z_out))
+        verbose && @info "run_tile (B200): $(n) halos from $(hb[].npeaks) peaks -> $(cfg.fileout)"
+        return halos
+    end
+end
+
+"""GPU fill_noise_threefry!: bit-identical Threefry-2x64-20 Box-Muller noise."""
+function fill_noise_threefry!(noise::Array{Float32,3}, n::Int, seed::Integer; ctx::Context=default_context())
+    size(noise) == (n, n, n) || throw(DimensionMismatch("noise must be n x n x n"))
+    check(ctx, ccall((:ppb_noise_threefry, libppb), Int32, (Ptr{Cvoid}, Ptr{Float32}, Int32, UInt64),
+                     ctx.h, noise, n, UInt64(seed)))
+    return noise
+end
+
+"""GPU find_peaks (same arguments as PeakFind.find_peaks; mask is updated)."""
+function find_peaks(delta::Array{Float32,3}, mask::Array{Int8,3}, xbx, ybx, zbx, alatt, nbuff, fcrit, Rsmooth;
+                    max_peaks::Int=2000000, ctx::Context=default_context())
+    n1, n2, n3 = size(delta)
+    cap = max(1, min(max_peaks, (n1 - 2nbuff) * (n2 - 2nbuff) * (n3 - 2nbuff)))
+    pi = Vector{Int64}(undef, cap); pj = similar(pi); pk = similar(pi); ipp = similar(pi)
+    pd = Vector{Float32}(undef, cap)
+    np = Ref{Int64}(0)
+    check(ctx, ccall((:ppb_find_peaks, libppb), Int32,
+                     (Ptr{Cvoid}, Ptr{Float32}, Ptr{Int8}, Int32, Int32, Int32, Int32, Float32, Int64,
+                      Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Ptr{Int64}, Ptr{Float32}, Ref{Int64}),
+                     ctx.h, delta, mask, n1, n2, n3, nbuff, Float32(fcrit), max_peaks, pi, pj, pk, ipp, pd, np))
+    PP = Base.root_module(Base.__toplevel__, :PeakPatch)
+    cen = ((n1 + 1) / 2, (n2 + 1) / 2, (n3 + 1) / 2)
+    return [PP.PeakCandidate(pi[q], pj[q], pk[q], ipp[q], xbx + alatt * (pi[q] - cen[1]),
+                             ybx + alatt * (pj[q] - cen[2]), zbx + alatt * (pk[q] - cen[3]), pd[q], Float64(Rsmooth))
+            for q in 1:np[]]
+end
+
+end # module PeakPatchB200

@@ -11,7 +11,7 @@ Names, argument meanings and error behaviour follow the reference
   analyse_peak (batched)    src/HaloFinder/RadialShell.jl:282-891
   read_homeltab             src/EllipsoidalCollapse/CollapseTable.jl:102-122
   read_filterbank           src/HaloFinder/Filters.jl:46-58
-  load_pk (table part)      src/InitialConditions/PowerSpectrum.jl:189-201
+  load_pk (table part)      src/InitialConditions/PowerSpectrum.jl:11-30
   write_pksc / read_pksc    src/IO/Catalog.jl:53-160
 
 Arrays are numpy arrays in C order with shape (n3, n2, n1), which is the

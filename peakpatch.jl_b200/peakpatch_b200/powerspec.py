@@ -1,7 +1,7 @@
 """Tabulated linear power spectra for run_tile's `pkfile`.
 
 The reference reads P(k) from a two-column file (k in h/Mpc, P) and
-interpolates it log-log (src/InitialConditions/PowerSpectrum.jl:189-201).  It
+interpolates it log-log (src/InitialConditions/PowerSpectrum.jl:11-30).  It
 contains no power-spectrum model of its own; this module writes such files
 from the Eisenstein & Hu (1998, ApJ 496, 605) "no-wiggle" transfer function,
 eqs. (26)-(31), with a primordial tilt n_s and a sigma_8 normalisation.
