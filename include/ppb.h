@@ -191,15 +191,19 @@ int32_t ppb_event_elapsed(ppb_ctx* ctx, int32_t a, int32_t b, float* ms);
 int32_t ppb_synchronize(ppb_ctx* ctx);
 /* Count of kernel launches issued by this library since context creation. */
 int32_t ppb_launch_count(ppb_ctx* ctx, int64_t* count);
-/* Shell-kernel statistics of the last run: in-bounds cell visits, the five
+/* Shell-stage statistics of the last run: in-bounds cell visits, the five
  * dump-reason counters of src/HaloFinder/RadialShell.jl:15-34 (premask,
- * no_fcrit, m0_one, no_collapse, rthl_neg) and the kernel's device time. */
+ * no_fcrit, m0_one, no_collapse, rthl_neg) and the stage's device time. */
 int32_t ppb_last_shell_stats(ppb_ctx* ctx, int64_t* visits, int64_t* dumps5, float* ms);
-/* All 16 raw shell-kernel counters of the last run: [0] cell visits,
+/* All 16 raw shell-stage counters of the last run: [0] cell visits,
  * [1..5] dump reasons as above, [6] profile reads beyond the gathered shells
  * (must be 0), [7] SPH-table overruns (the reference raises there),
- * [8] invalid peak inputs, [9] collapse-walk rounds, others reserved. */
+ * [8] invalid peak inputs, [9] collapse-walk steps evaluated, others reserved. */
 int32_t ppb_shell_counters(ppb_ctx* ctx, int64_t* out16);
+/* Device time (ms) of the shell stage's three kernels in the last run:
+ * [0] gather, [1] collapse walk, [2] d2F; *rows = profile rows written
+ * (ROW = 24 doubles each), *batches = peak batches the stage ran in. */
+int32_t ppb_last_shell_times(ppb_ctx* ctx, float* ms3, int64_t* rows, int32_t* batches);
 /* Per-stage device times (ms) of the last ppb_run_tile_timed call:
  * [0] fields, [1] filter bank + peaks, [2] shell analysis, [3] records. */
 int32_t ppb_last_stage_ms(ppb_ctx* ctx, float* ms4);

@@ -96,7 +96,8 @@ ShellArgs ppb_ctx::shell_args(int n, double alatt, const float4* aos, const floa
   a.lapd = lapd;
   a.n = n;
   a.alatt = alatt;
-  a.cells = shells.d_cells.as<int4>();
+  PPB_REQUIRE(n <= 4096, "grid size above 4096");
+  a.cell8 = shells.d_cell8.as<int32_t>();
   a.sh_start = shells.d_start.as<int32_t>();
   a.sh_count = shells.d_count.as<int32_t>();
   a.rad = shells.d_rad.as<double>();
@@ -125,38 +126,86 @@ ShellArgs ppb_ctx::shell_args(int n, double alatt, const float4* aos, const floa
 }
 
 void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st) {
-  if (shell_blocks == 0) {
-    shell_prepare(shell_wpb);
-    const size_t shm = shell_smem_bytes(shell_wpb);
-    int b1 = 0, b2 = 0;
-    PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, shell_kernel_ptr(true, true), 32 * shell_wpb, shm));
-    PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, shell_kernel_ptr(false, false), 32 * shell_wpb, shm));
-    shell_blocks = nsm * std::max(1, std::min(b1, b2));
-  }
-  const int64_t stride = shell_scratch_doubles_per_warp(a.nshell);
-  const int64_t slots = (int64_t)shell_blocks * shell_wpb;
-  scratch.ensure((size_t)(slots * stride * 8));
+  Launch L{stream, &launches};
+  int& bps = gather_bps[comp][adaptive];
+  if (bps == 0) bps = shell_gather_blocks_per_sm(comp, adaptive);
+  const int gblocks = nsm * bps;
+  const int64_t stride = shell_stage_doubles_per_warp(a.nshell);
+  stage.ensure((size_t)((int64_t)gblocks * kGatherWarps * stride * 8));
   counters.ensure(16 * 8);
-  queue.ensure(64);
+  ctl.ensure(64);
+  hdr.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(PeakHdr));
   PPB_CUDA(cudaMemsetAsync(counters.p, 0, 16 * 8, stream));
-  PPB_CUDA(cudaMemsetAsync(queue.p, 0, 4, stream));
-  a.scratch = scratch.as<double>();
-  a.scratch_stride = stride;
-  a.queue = queue.as<int>();
-  a.counters = counters.as<unsigned long long>();
-  PPB_CUDA(cudaEventRecord(ev[14], stream));
-  launch_shell(Launch{stream, &launches}, a, comp, adaptive, shell_blocks, shell_wpb);
-  PPB_CUDA(cudaEventRecord(ev[15], stream));
-  unsigned long long c[16];
-  PPB_CUDA(cudaMemcpyAsync(c, counters.p, sizeof(c), cudaMemcpyDeviceToHost, stream));
-  PPB_CUDA(cudaStreamSynchronize(stream));
+  // profile pool: sized from the rows per peak of the previous call; peaks
+  // run in batches that fit the pool budget, and a batch whose rows overflow
+  // the pool runs again with a larger pool or fewer peaks
+  size_t fr = 0, tot = 0;
+  PPB_CUDA(cudaMemGetInfo(&fr, &tot));
+  const size_t row_bytes = ROW * sizeof(double);
+  const int64_t budget_rows = std::max<int64_t>(
+      1 << 16, (int64_t)(std::min<size_t>((size_t)32 << 30, (fr + pool.bytes) / 2) / row_bytes));
+  double& rpp = rows_per_peak[adaptive];
+  if (rpp <= 0.0) rpp = adaptive ? 64.0 : (double)(a.mmax + 1);
   ShellStats s{};
+  unsigned long long before[16] = {}, c[16] = {};
+  int64_t p0 = 0;
+  while (p0 < a.npk) {
+    const double want = std::max(1.0, rpp * 1.25);
+    int64_t nb = std::min<int64_t>(a.npk - p0, std::max<int64_t>(1, (int64_t)((double)budget_rows / want)));
+    const int64_t cap = std::min<int64_t>(budget_rows, (int64_t)((double)nb * want) + 4096);
+    pool.ensure((size_t)cap * row_bytes);
+    ShellArgs b = a;
+    b.pk.lin = a.pk.lin + p0;
+    b.pk.Rf = a.pk.Rf + p0;
+    b.pk.ir2min = a.pk.ir2min + p0;
+    b.pk.ZZon = a.pk.ZZon + p0;
+    b.pk.fcrit = a.pk.fcrit + p0;
+    b.npk = nb;
+    b.out = a.out + p0 * RES_N;
+    b.hdr = hdr.as<PeakHdr>() + p0;
+    b.pool = pool.as<double>();
+    b.pool_cap = cap;
+    b.pool_ctr = reinterpret_cast<unsigned long long*>(ctl.as<char>() + 8);
+    b.queue = ctl.as<int>();
+    b.stage = stage.as<double>();
+    b.stage_stride = stride;
+    b.counters = counters.as<unsigned long long>();
+    for (int e = 0; e < 10; e++) b.fhalf[e] = std::pow(e / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
+    PPB_CUDA(cudaMemsetAsync(ctl.p, 0, 16, stream));
+    PPB_CUDA(cudaEventRecord(shell_ev[0], stream));
+    launch_shell_gather(L, b, comp, adaptive, gblocks);
+    PPB_CUDA(cudaEventRecord(shell_ev[1], stream));
+    launch_shell_collapse(L, b);
+    PPB_CUDA(cudaEventRecord(shell_ev[2], stream));
+    launch_shell_d2f(L, b, nsm * 16);
+    PPB_CUDA(cudaEventRecord(shell_ev[3], stream));
+    unsigned long long used = 0;
+    PPB_CUDA(cudaMemcpyAsync(&used, b.pool_ctr, sizeof(used), cudaMemcpyDeviceToHost, stream));
+    PPB_CUDA(cudaMemcpyAsync(c, counters.p, sizeof(c), cudaMemcpyDeviceToHost, stream));
+    PPB_CUDA(cudaStreamSynchronize(stream));
+    if ((int64_t)used > cap) {   // overflow: undo this batch's counts and run it again
+      PPB_CUDA(cudaMemcpyAsync(counters.p, before, sizeof(before), cudaMemcpyHostToDevice, stream));
+      PPB_CUDA(cudaStreamSynchronize(stream));
+      const double seen = (double)used / (double)nb;
+      PPB_REQUIRE(seen * 1.25 > rpp, "profile pool overflow without growth");
+      rpp = seen;
+      continue;
+    }
+    float k[3];
+    for (int e = 0; e < 3; e++) PPB_CUDA(cudaEventElapsedTime(&k[e], shell_ev[e], shell_ev[e + 1]));
+    for (int e = 0; e < 3; e++) s.kms[e] += k[e];
+    s.ms += k[0] + k[1] + k[2];
+    s.pool_rows += used;
+    s.batches++;
+    if (nb == a.npk - p0 || nb >= 1024) rpp = std::max(1.0, (double)used / (double)nb);
+    std::memcpy(before, c, sizeof(c));
+    p0 += nb;
+  }
   s.visits = c[0];
   for (int i = 0; i < 5; i++) s.dump[i] = c[1 + i];
   s.guard = c[6];
   s.akk = c[7];
   for (int i = 0; i < 16; i++) s.raw[i] = c[i];
-  PPB_CUDA(cudaEventElapsedTime(&s.ms, ev[14], ev[15]));
   last_shell = s;
   if (st) *st = s;
 }
@@ -199,6 +248,7 @@ int32_t ppb_ctx_create(int32_t device, uint64_t hbm_budget, ppb_ctx** out) {
     PPB_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     for (auto& e : ctx->ev) PPB_CUDA(cudaEventCreate(&e));
     for (auto& e : ctx->stage_ev) PPB_CUDA(cudaEventCreate(&e));
+    for (auto& e : ctx->shell_ev) PPB_CUDA(cudaEventCreate(&e));
     size_t fr = 0, tot = 0;
     PPB_CUDA(cudaMemGetInfo(&fr, &tot));
     ctx->hbm_budget = hbm_budget ? hbm_budget : (uint64_t)(0.9 * (double)fr);
@@ -224,6 +274,7 @@ int32_t ppb_ctx_destroy(ppb_ctx* ctx) {
   ctx->tiles.clear();
   for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
   for (auto& e : ctx->stage_ev) if (e) cudaEventDestroy(e);
+  for (auto& e : ctx->shell_ev) if (e) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return PPB_OK;

@@ -36,6 +36,11 @@ void build_shell_table(ShellTable& st, int nhunt) {
     st.shell_count.back()++;
   }
   st.nshell = (int)st.shell_r2.size();
+  st.cell8.resize(st.cells.size());
+  for (size_t i = 0; i < st.cells.size(); i++) {
+    const int4 c = st.cells[i];
+    st.cell8[i] = (int32_t)((uint32_t)(c.x & 0xff) | ((uint32_t)(c.y & 0xff) << 8) | ((uint32_t)(c.z & 0xff) << 16));
+  }
   // shell m (1-based) = distinct value m-1; rad[m] = sqrt(r2)
   st.rad.assign(st.nshell + 1, 0.0);
   st.r2m.assign(st.nshell + 1, 0);
@@ -124,7 +129,7 @@ void build_shell_table(ShellTable& st, int nhunt) {
   st.ngroups = (int)st.grp_a.size();
   st.grp_c.push_back((int32_t)st.ck_s.size());
   st.nhunt = nhunt;
-  st.d_cells.release();   // force re-upload
+  st.d_cell8.release();   // force re-upload
 }
 
 // hRinteg (src/HaloFinder/RadialShell.jl:100-127)
@@ -166,13 +171,13 @@ std::vector<double> make_atab4() {
 }
 
 void upload_shell_table(ShellTable& st, cudaStream_t s) {
-  if (st.d_cells.p && st.d_cells.bytes >= st.cells.size() * sizeof(int4)) return;
-  st.d_cells.ensure(st.cells.size() * sizeof(int4));
+  if (st.d_cell8.p && st.d_cell8.bytes >= st.cell8.size() * sizeof(int32_t)) return;
+  st.d_cell8.ensure(st.cell8.size() * sizeof(int32_t));
   st.d_start.ensure(st.shell_start.size() * sizeof(int32_t));
   st.d_count.ensure(st.shell_count.size() * sizeof(int32_t));
   st.d_r2m.ensure(st.r2m.size() * sizeof(int32_t));
   st.d_rad.ensure(st.rad.size() * sizeof(double));
-  PPB_CUDA(cudaMemcpyAsync(st.d_cells.p, st.cells.data(), st.cells.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+  PPB_CUDA(cudaMemcpyAsync(st.d_cell8.p, st.cell8.data(), st.cell8.size() * 4, cudaMemcpyHostToDevice, s));
   PPB_CUDA(cudaMemcpyAsync(st.d_start.p, st.shell_start.data(), st.shell_start.size() * 4, cudaMemcpyHostToDevice, s));
   PPB_CUDA(cudaMemcpyAsync(st.d_count.p, st.shell_count.data(), st.shell_count.size() * 4, cudaMemcpyHostToDevice, s));
   PPB_CUDA(cudaMemcpyAsync(st.d_r2m.p, st.r2m.data(), st.r2m.size() * 4, cudaMemcpyHostToDevice, s));

@@ -5,47 +5,44 @@
 // get_evals (:217-222) and the collapse-table lookup
 // (src/EllipsoidalCollapse/CollapseTable.jl:128-145).
 //
-// Design (one warp per peak, persistent grid, peaks taken from a queue in
-// list order, i.e. largest filter radius first):
-//  1. Gather.  Lane l owns shell m = base + l of a group of 32 consecutive
-//     shells (shell m >= 2 holds the cells with the (m-1)-th distinct r^2 of
-//     the sorted cell list; shell 1 is the peak cell).  A lane walks its own
-//     shell's cells, reading one 32-byte record per cell from the packed
-//     field array, so no cross-lane reduction is needed.  Sums are either
-//     compensated single precision (two-sum, error-free per addend; the
-//     optimised path) or double precision (the plain path); in both cases
-//     the addends are the single-precision products the reference forms
-//     (Float32 field times Int32 offset).
-//  2. Adaptive truncation (optimised path only).  After each group the warp
-//     extends the cumulative profile Fbar and stops as soon as every shell
-//     the collapse walk can read has been gathered.  Every index used below
-//     the gather is bounded by rad <= rad[M] + 2 (+ one shell) with
-//     M = max(crossing shell, first shell beyond ir2min, Rf window), because
-//     kernel_strain's weight vanishes for |rad[mp] - rad[m1]| >= 2 and the
-//     walk only moves inward from the crossing; the one exception (no
-//     crossing at all) gathers every shell.  A device-side guard counts any
-//     read past the gathered range (it must stay 0; the host fails loudly).
-//  3. Collapse walk in double precision.  kernel_strain(mp) only depends on
-//     the shells with (rad[mp] - rad[m1])^2 < 4 (the reference's running
-//     mlow/mupp always bracket that set), so the walk steps are independent:
-//     each lane evaluates one step (window sum, eigenvalues, table lookup)
-//     and a ballot finds the first step that collapses, 31 steps per round.
-//     The window weights hRinteg/(u12-u0^2)^2 depend only on the radii and
-//     come from a host table.  The ten zvir_half radii run on ten lanes.
+// The stage runs as three kernels on one stream:
+//
+//  gather_kernel (persistent, one warp per peak, peaks taken from a queue in
+//    list order, i.e. largest filter radius first).  A host-built schedule
+//    splits the shells (distinct r^2 of the sorted cell list; shell 1 is the
+//    peak cell) into chunks of at most 24 cells and packs 32 chunks per
+//    group, groups ending on shell boundaries.  Lane l sums chunk l of the
+//    group (four cells per step, so that eight 16-byte record loads are in
+//    flight per lane), lane l then finalises shell l of the group from the
+//    chunk partials, and the cumulative profile Fbar comes from a warp scan
+//    of r^3 Fbar.  Sums are compensated single precision (two-sum, error-free
+//    per addend) on the optimised path and double precision on the plain
+//    path; in both the addends are the single-precision products the
+//    reference forms (Float32 field times Int32 offset).
+//    Adaptive truncation (optimised path): the warp stops gathering once
+//    every shell later read is in, i.e. all shells up to rad[M] + 2 with
+//    M = max(crossing shell, first shell beyond ir2min, Rf window):
+//    kernel_strain's weight vanishes for |rad[mp] - rad[m1]| >= 2 and the
+//    walk only moves inward from the crossing (with no crossing at all every
+//    shell is gathered).  A device guard counts any read past the gathered
+//    range; it must stay 0 and the host fails loudly otherwise.
+//    The kernel ends with the fcrit crossing m0 (RadialShell.jl:494-537) and
+//    moves the peak's rows from its staging slot to a pool.
+//
+//  collapse_kernel (one thread per peak).  kernel_strain windows, the inward
+//    collapse walk, RTHL, Sbar/Srb and zvir_half in double precision, in the
+//    reference's summation order.  The window weights hRinteg/(u12-u0^2)^2
+//    depend only on the radii and come from a host table.
+//
+//  d2f_kernel (one warp per collapsed peak).  Mean Laplacian over the cells
+//    within RTHL in list order, stopping at the first out-of-grid cell.
 #include "ppb_internal.h"
 
 namespace ppb {
 
 namespace {
 
-constexpr int NV = 20;   // profile values per shell
-enum { PV_FBAR = 0, PV_N = 1, PV_S = 2, PV_S2 = 5, PV_G = 8, PV_GF = 11, PV_Q = 14 };
-constexpr int NACC = 19; // gather accumulators: F, S3, S2_3, G3, Gf3, Q6 (xx yy zz xy xz yz)
-// shells a warp keeps in shared memory (peaks needing more move their
-// profile to global scratch), and the per-warp shared-memory footprint:
-// the profile plus the chunk-partial table of the gather
-constexpr int SMEM_SHELLS = 80;
-constexpr int SMEM_WARP_DOUBLES = NV * (SMEM_SHELLS + 1) + (NACC + 1) * 32;
+constexpr int NACC = 19;   // gather accumulators: F, S3, S2_3, G3, Gf3, Q6 (xx yy zz xy xz yz)
 constexpr unsigned FULL = 0xffffffffu;
 
 // counters layout
@@ -102,21 +99,355 @@ __device__ __forceinline__ void accumulate_cell(Acc<COMP>& A, const float4 a, co
 // ---------------------------------------------------------------------------
 // small helpers
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-  return v;
-}
 __device__ __forceinline__ long long warp_sum_ll(long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
   return v;
 }
-__device__ __forceinline__ double warp_max(double v) {
+__device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
   return v;
 }
+
+// smallest m in [lo, hi] with rad[m] > x, or hi+1
+__device__ __forceinline__ int first_gt(const double* rad, int lo, int hi, double x) {
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(rad + mid) > x) hi = mid - 1; else lo = mid + 1;
+  }
+  return lo;
+}
+// largest m in [lo, hi] with rad[m] < x, or lo-1
+__device__ __forceinline__ int last_lt(const double* rad, int lo, int hi, double x) {
+  while (lo <= hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(rad + mid) < x) lo = mid + 1; else hi = mid - 1;
+  }
+  return hi;
+}
+
+// geometry that depends only on the shell radii and the peak's Rf / ir2min
+struct Geo {
+  int m0_init;   // first finalised shell with r^2 > ir2min, else the last one (RadialShell.jl:392-399)
+  int mrf;       // the per-cell Rf search (RadialShell.jl:457-471)
+  int mlow_rf, mupp_rf;
+};
+
+__device__ __forceinline__ Geo geometry(const ShellArgs& a, double Rf, int ir2min) {
+  Geo g;
+  const int mmax = a.mmax;
+  {
+    int lo = 2, hi = mmax;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(a.r2m + mid) > ir2min) hi = mid - 1; else lo = mid + 1;
+    }
+    g.m0_init = (lo <= mmax) ? lo : (mmax >= 2 ? mmax : 1);
+  }
+  // the per-cell scan is decided by the first cell of each distinct r^2;
+  // group s (s-th nonzero r^2) reports index max(s-1, 1); earliest strict
+  // minimum of |r^2 - (Rf/alatt)^2| below 10
+  g.mrf = 1;
+  {
+    const double rq = (Rf / a.alatt) * (Rf / a.alatt);
+    const int K = a.nshell - 1;
+    int lo = 1, hi = K;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      if ((double)__ldg(a.r2m + mid + 1) >= rq) hi = mid - 1; else lo = mid + 1;
+    }
+    double best = 10.0;
+    int sbest = 0;
+    for (int s = lo - 1; s <= lo; s++) {
+      if (s < 1 || s > K) continue;
+      const double dv = fabs((double)__ldg(a.r2m + s + 1) - rq);
+      if (dv < best) { best = dv; sbest = s; }
+    }
+    if (sbest > 0) g.mrf = sbest > 1 ? sbest - 1 : 1;
+  }
+  const double* rad = a.rad;
+  g.mlow_rf = g.mrf;
+  if (g.mrf > 1) {
+    const double rlow = fmax(__ldg(rad + g.mrf) - 2.0, 0.0);
+    const int f = first_gt(rad, 1, g.mrf - 1, rlow);
+    if (f <= g.mrf - 1) g.mlow_rf = f;
+  }
+  g.mupp_rf = g.mrf;
+  {
+    const int l = last_lt(rad, g.mrf + 1, mmax, __ldg(rad + g.mrf) + 2.0);
+    if (l >= g.mrf + 1) g.mupp_rf = l;
+  }
+  return g;
+}
+
+// ===========================================================================
+// gather kernel
+// ===========================================================================
+// decode a packed cell offset
+__device__ __forceinline__ void unpack_cell(int w, int& di, int& dj, int& dk) {
+  di = (w << 24) >> 24;
+  dj = (w << 16) >> 24;
+  dk = (w << 8) >> 24;
+}
+
+template <bool COMP, bool ADAPTIVE>
+__device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double* part) {
+  const int lane = threadIdx.x & 31;
+  PeakHdr* hdr = a.hdr + p;
+  const int n = a.n;
+  const int64_t n2 = (int64_t)n * n;
+  const int64_t lin = a.pk.lin[p];
+  const double ZZon = a.pk.ZZon[p];
+  if (lin < 0 || lin >= n2 * n || !(ZZon > -1.0)) {   // invalid peak index or redshift from the caller
+    if (lane == 0) {
+      atomicAdd(a.counters + CNT_BADPEAK, 1ull);
+      hdr->status = HS_BAD;
+    }
+    return;
+  }
+  const int pk = (int)(lin / n2), pj = (int)((lin / n) % n), pi = (int)(lin % n);
+  const double fcrit = a.pk.fcrit[p];
+  const double* __restrict__ rad = a.rad;
+  const int mmax = a.mmax;
+  const Geo geo = geometry(a, a.pk.Rf[p], a.pk.ir2min[p]);
+  const int m0_init = geo.m0_init;
+
+  // ---- the peak cell (shell 1) ------------------------------------------
+  const float4* __restrict__ aos = a.aos;
+  const float4 c0 = __ldg(aos + 2 * lin), c1 = __ldg(aos + 2 * lin + 1);
+  if (lane < ROW) {
+    double v = 0.0;
+    if (lane == R_FBAR) v = (double)c0.x;
+    else if (lane == R_N) v = 1.0;
+    else if (lane == R_S) v = (double)c0.z;
+    else if (lane == R_S + 1) v = (double)c0.w;
+    else if (lane == R_S + 2) v = (double)c1.x;
+    else if (lane == R_S2) v = (double)c1.y;
+    else if (lane == R_S2 + 1) v = (double)c1.z;
+    else if (lane == R_S2 + 2) v = (double)c1.w;
+    stage[ROW + lane] = v;
+  }
+  const int rext = (int)ceil(__ldg(rad + mmax)) + 1;
+  const bool inside = pi - rext >= 0 && pj - rext >= 0 && pk - rext >= 0 && pi + rext < n && pj + rext < n &&
+                      pk + rext < n;
+  int state = 0;          // 0 unknown, 1 inward, 2 crossing found
+  int mcross = 0;
+  int mtarget = ADAPTIVE ? -1 : mmax;   // last shell to gather (-1: not known yet)
+  int mdone = 1;
+  double FB = 0.0;                      // r^3 Fbar of shell mdone (0 at the peak cell, rad[1] = 0)
+  double dF_prev = (double)c0.x;        // shell-mean delta of shell mdone
+  long long visits = 0;
+  for (int g = 0; g < a.ngroups; g++) {
+    const int base = __ldg(a.grp_a + g), gend = __ldg(a.grp_b + g);
+    if (mtarget >= 0 && base > mtarget) break;
+    const int c0g = __ldg(a.grp_c + g), ncg = __ldg(a.grp_c + g + 1) - c0g;
+    // (a) lane l sums chunk c0g + l into the shared partial table
+    if (lane < ncg) {
+      Acc<COMP> A;
+      A.zero();
+      const int s0 = __ldg(a.ck_s + c0g + lane), cnt = __ldg(a.ck_n + c0g + lane);
+      int nsh = 0;
+      for (int c = 0; c < cnt; c += 4) {
+        float4 ra[4], rb[4];
+        float fd[4][3];
+        bool ok[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int w = (c + u < cnt) ? __ldg(a.cell8 + s0 + c + u) : 0;
+          int di, dj, dk;
+          unpack_cell(w, di, dj, dk);
+          const int iv1 = pi + di, iv2 = pj + dj, iv3 = pk + dk;
+          ok[u] = (c + u < cnt) &&
+                  (inside || (iv1 >= 0 && iv1 < n && iv2 >= 0 && iv2 < n && iv3 >= 0 && iv3 < n));
+          // out-of-range cells read the peak cell and contribute nothing
+          const int64_t li = ok[u] ? lin + di + (int64_t)n * dj + n2 * dk : lin;
+          ra[u] = __ldg(aos + 2 * li);
+          rb[u] = __ldg(aos + 2 * li + 1);
+          fd[u][0] = (float)di; fd[u][1] = (float)dj; fd[u][2] = (float)dk;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          if (ok[u]) {
+            nsh++;
+            accumulate_cell<COMP>(A, ra[u], rb[u], fd[u][0], fd[u][1], fd[u][2]);
+          }
+        }
+      }
+      visits += nsh;
+#pragma unroll
+      for (int v = 0; v < NACC; v++) part[v * 32 + lane] = A.get(v);
+      part[NACC * 32 + lane] = (double)nsh;
+    }
+    __syncwarp();
+    // (b) lane l finalises shell base + l from its chunks (double-precision
+    // sum of the chunk partials, each of which is exact to ~2^-48)
+    const int m = base + lane;
+    const bool own = m <= gend;
+    double my_dF = 0.0, g0 = 0.0;
+    if (own) {
+      double t[NACC + 1];
+#pragma unroll
+      for (int v = 0; v <= NACC; v++) t[v] = 0.0;
+      const int k0 = __ldg(a.sh_c0 + m) - c0g, nk = __ldg(a.sh_nc + m);
+      for (int k = k0; k < k0 + nk; k++) {
+#pragma unroll
+        for (int v = 0; v <= NACC; v++) t[v] += part[v * 32 + k];
+      }
+      const double r = __ldg(rad + m);
+      const double nsh = t[NACC];
+      my_dF = nsh > 0 ? t[0] / nsh : 0.0;
+      double row[ROW];
+#pragma unroll
+      for (int v = 0; v < ROW; v++) row[v] = 0.0;
+      row[R_N] = nsh;
+#pragma unroll
+      for (int L = 0; L < 3; L++) {
+        row[R_S + L] = t[1 + L];
+        row[R_S2 + L] = t[4 + L];
+        row[R_G + L] = t[7 + L] / r;
+        row[R_GF + L] = t[10 + L] / r;
+      }
+      row[R_Q + 0] = (2.0 * t[13]) / r;
+      row[R_Q + 1] = (2.0 * t[14]) / r;
+      row[R_Q + 2] = (2.0 * t[15]) / r;
+      row[R_Q + 3] = t[16] / r;
+      row[R_Q + 4] = t[17] / r;
+      row[R_Q + 5] = t[18] / r;
+      double2* dst = reinterpret_cast<double2*>(stage + (int64_t)m * ROW);
+#pragma unroll
+      for (int v = 1; v < ROW / 2; v++) dst[v] = make_double2(row[2 * v], row[2 * v + 1]);
+      g0 = row[1];   // slots 0 (Fbar, after the scan) and 1 are stored together
+    }
+    __syncwarp();
+    // (c) cumulative mean overdensity (RadialShell.jl:386-390) as a scan of
+    // FB[m] = r3[m] Fbar[m] = FB[m-1] + (dF[m-1] + dF[m]) / 2 * (r3[m] - r3[m-1])
+    double prev_dF = __shfl_up_sync(FULL, my_dF, 1);
+    if (lane == 0) prev_dF = dF_prev;
+    const double rm = __ldg(rad + (own ? m : base)), rp = __ldg(rad + (own ? m - 1 : base - 1));
+    const double r3 = rm * rm * rm, r3p = rp * rp * rp;
+    double x = own ? 0.5 * (prev_dF + my_dF) * (r3 - r3p) : 0.0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double y = __shfl_up_sync(FULL, x, o);
+      if (lane >= o) x += y;
+    }
+    const double FBm = FB + x;
+    const double fb = FBm / r3;
+    if (own) {
+      double2* dst = reinterpret_cast<double2*>(stage + (int64_t)m * ROW);
+      dst[0] = make_double2(fb, g0);
+    }
+    const int last = gend - base;
+    FB = __shfl_sync(FULL, FBm, last);
+    dF_prev = __shfl_sync(FULL, my_dF, last);
+    // (d) crossing state, in shell order: at m0_init Fbar < fcrit means the
+    // crossing lies inward; beyond it the first Fbar < fcrit is the crossing
+    if (state == 0) {
+      const unsigned bi = __ballot_sync(FULL, own && m == m0_init && fb < fcrit);
+      if (bi) {
+        state = 1;
+      } else {
+        const unsigned bc = __ballot_sync(FULL, own && m > m0_init && fb < fcrit);
+        if (bc) {
+          state = 2;
+          mcross = base + __ffs(bc) - 1;
+        }
+      }
+    }
+    mdone = gend;
+    if (ADAPTIVE && mtarget < 0 && (state != 0 || mdone >= mmax)) {
+      int M = max(max(m0_init, geo.mrf), geo.mupp_rf);
+      if (state == 2) M = max(M, mcross);
+      mtarget = state == 0 ? mmax : __ldg(a.need + M);
+    }
+    __syncwarp();
+  }
+  {
+    const long long tv = warp_sum_ll(visits);
+    if (lane == 0) atomicAdd(a.counters + CNT_VISITS, (unsigned long long)tv);
+  }
+
+  // ---- fcrit crossing m0 (RadialShell.jl:494-537) ------------------------
+  int m0 = m0_init;
+  int status = HS_OK;
+  if (state == 2) {
+    m0 = mcross;
+  } else if (state == 1) {
+    // inward: m0 = one above the first shell below m0_init (going down)
+    // with Fbar >= fcrit; none -> no fcrit crossing
+    bool found = false;
+    for (int top = m0_init - 1; top >= 1 && !found; top -= 32) {
+      const int mp = top - lane;
+      const bool ge = mp >= 1 && stage[(int64_t)mp * ROW + R_FBAR] >= fcrit;
+      const unsigned b = __ballot_sync(FULL, ge);
+      if (b) {
+        found = true;
+        m0 = top - (__ffs(b) - 1) + 1;
+      }
+    }
+    if (!found) status = HS_NOFCRIT;
+  }
+  if (status == HS_OK && m0 == 1) status = HS_M0ONE;   // zvir1p at m0 is forced to -1 < ZZon (:581-622)
+  if (status != HS_OK) {
+    if (lane == 0) {
+      atomicAdd(a.counters + (status == HS_NOFCRIT ? CNT_NOFCRIT : CNT_M0ONE), 1ull);
+      PeakHdr h;
+      h.off = 0; h.mdone = mdone; h.m0 = m0; h.status = status; h.pad = 0;
+      *hdr = h;
+    }
+    return;
+  }
+
+  // ---- move the rows 1..mdone to the pool ---------------------------------
+  long long off = 0;
+  if (lane == 0) off = (long long)atomicAdd(a.pool_ctr, (unsigned long long)(mdone + 1));
+  off = __shfl_sync(FULL, off, 0);
+  if (off + mdone + 1 > a.pool_cap) {   // the host grows the pool and runs the batch again
+    if (lane == 0) {
+      PeakHdr h;
+      h.off = 0; h.mdone = mdone; h.m0 = m0; h.status = HS_OVERFLOW; h.pad = 0;
+      *hdr = h;
+    }
+    return;
+  }
+  {
+    const double2* src = reinterpret_cast<const double2*>(stage + ROW);
+    double2* dst = reinterpret_cast<double2*>(a.pool + (off + 1) * ROW);
+    const int nv = mdone * (ROW / 2);
+    for (int i = lane; i < nv; i += 32) dst[i] = src[i];
+  }
+  if (lane == 0) {
+    PeakHdr h;
+    h.off = off; h.mdone = mdone; h.m0 = m0; h.status = HS_OK; h.pad = 0;
+    *hdr = h;
+  }
+}
+
+template <bool COMP, bool ADAPTIVE>
+__global__ void __launch_bounds__(32 * kGatherWarps) gather_kernel(ShellArgs a) {
+  __shared__ double part_all[kGatherWarps][(NACC + 1) * 32];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int64_t slot = (int64_t)blockIdx.x * kGatherWarps + wib;
+  double* stage = a.stage + slot * a.stage_stride;
+  while (true) {
+    int p = 0;
+    if (lane == 0) p = atomicAdd(a.queue, 1);
+    p = __shfl_sync(FULL, p, 0);
+    if (p >= a.npk) break;
+    gather_one<COMP, ADAPTIVE>(a, p, stage, part_all[wib]);
+    __syncwarp();
+  }
+}
+
+// ===========================================================================
+// collapse kernel (one thread per peak)
+// ===========================================================================
+struct KS {
+  double E[6];   // xx yy zz xy xz yz
+  double g[3], gf[3];
+};
 
 // Symmetric 3x3 eigenvalues, ascending: the trigonometric solution of the
 // characteristic cubic (O. K. Smith, "Eigenvalues of a symmetric 3 x 3
@@ -169,115 +500,6 @@ __device__ __noinline__ double tab_interp(const DevTable& T, double x, double y,
   return (1 - wz) * c0 + wz * c1;
 }
 
-// ---------------------------------------------------------------------------
-// per-warp radial profile: value v of shell m at p[v*MS + m].  It lives in
-// the warp's shared-memory slice while the peak needs at most `cap` shells
-// and moves to the warp's global scratch slot when the gather grows beyond.
-// ---------------------------------------------------------------------------
-struct Prof {
-  double* p;
-  int MS;
-  int mdone;                        // shells 1..mdone are valid
-  unsigned long long* counters;
-  int cap;                          // largest shell index the current storage holds
-  double* global;                   // the warp's scratch slot
-  int MS_global;
-  __device__ __forceinline__ double get(int v, int m) const {
-    if (m > mdone) {                // never taken when the truncation rule holds
-      atomicAdd(counters + CNT_GUARD, 1ull);
-      return 0.0;
-    }
-    return p[(int64_t)v * MS + m];
-  }
-  __device__ __forceinline__ void set(int v, int m, double x) { p[(int64_t)v * MS + m] = x; }
-  // copy shells 1..upto to global scratch and continue there (whole warp)
-  __device__ void spill(int upto) {
-    const int lane = threadIdx.x & 31;
-    for (int v = 0; v < NV; v++)
-      for (int m = 1 + lane; m <= upto; m += 32) global[(int64_t)v * MS_global + m] = p[v * MS + m];
-    __syncwarp();
-    p = global;
-    MS = MS_global;
-    cap = 1 << 30;
-  }
-};
-
-struct KS {
-  double E[6];   // xx yy zz xy xz yz
-  double g[3], gf[3];
-};
-
-struct Walk {                       // one evaluated walk step
-  KS k;
-  double Fh, ev, pv, Fr, zv;
-};
-
-// kernel_strain (RadialShell.jl:228-277) for centre shell mp over m1 in
-// [lo, hi].  For mp > 1 only the shells with (rad[mp]-rad[m1])^2 < 4
-// contribute (the table window); for mp == 1 the SPH table weights apply to
-// every m1 of [lo, hi].  The warp is split into aligned groups of G lanes
-// (G a power of two); each group evaluates its own mp (mp < 1: no work), its
-// lanes striding over m1, and the group's partial sums are combined with a
-// butterfly, leaving the result in every lane of the group.  Every lane of
-// the warp must call it.
-__device__ __noinline__ void ks_multi(const Prof& P, const ShellArgs& a, int mp, int lo, int hi, int G,
-                                      double wRnor, double aRnor, KS* out) {
-  const int lane = threadIdx.x & 31;
-  const int sub = lane & (G - 1);
-  double E[6] = {0, 0, 0, 0, 0, 0}, g[3] = {0, 0, 0}, gf[3] = {0, 0, 0};
-  double scale = 0.0;
-  if (mp >= 1) {
-    const double* w;
-    if (mp > 1) {
-      const int wl = a.win_lo[mp], wh = a.win_hi[mp];
-      lo = max(lo, wl);
-      hi = min(hi, wh);
-      w = a.wts + a.win_off[mp] - wl;
-      scale = wRnor / a.rad[mp];
-    } else {
-      w = a.w1;
-      scale = aRnor;
-    }
-    if (hi > P.mdone) {                 // never taken when the truncation rule holds
-      atomicAdd(P.counters + CNT_GUARD, 1ull);
-      hi = P.mdone;
-    }
-    const double* pg = P.p + PV_G * P.MS;
-    const double* pf = P.p + PV_GF * P.MS;
-    const double* pq = P.p + PV_Q * P.MS;
-    const int MS = P.MS;
-    for (int m1 = lo + sub; m1 <= hi; m1 += G) {
-      const double wt = w[m1];
-      if (mp == 1 && isnan(wt)) atomicAdd(P.counters + CNT_AKK, 1ull);
-#pragma unroll
-      for (int L = 0; L < 3; L++) {
-        g[L] += wt * pg[L * MS + m1];
-        gf[L] += wt * pf[L * MS + m1];
-      }
-#pragma unroll
-      for (int q = 0; q < 6; q++) E[q] -= 0.5 * wt * pq[q * MS + m1];
-    }
-  }
-  for (int o = G >> 1; o > 0; o >>= 1) {
-#pragma unroll
-    for (int q = 0; q < 6; q++) E[q] += __shfl_xor_sync(FULL, E[q], o);
-#pragma unroll
-    for (int L = 0; L < 3; L++) {
-      g[L] += __shfl_xor_sync(FULL, g[L], o);
-      gf[L] += __shfl_xor_sync(FULL, gf[L], o);
-    }
-  }
-  KS r;
-#pragma unroll
-  for (int q = 0; q < 6; q++) r.E[q] = E[q] * scale;
-#pragma unroll
-  for (int L = 0; L < 3; L++) {
-    r.g[L] = g[L] * scale;
-    r.gf[L] = gf[L] * scale;
-  }
-  *out = r;
-}
-
 // eigen-decomposition -> (trace, e_v, p_v) as the reference (:571-577)
 __device__ __forceinline__ void ev_pv(const double E[6], double* Frho, double* ev, double* pv) {
   double lam[3];
@@ -298,342 +520,125 @@ __device__ __forceinline__ double zvir_of(const DevTable& T, double Fr, double e
   return tab_interp(T, log10(Fr), ev, poe);
 }
 
-__device__ __forceinline__ KS shfl_ks(const KS& k, int src) {
-  KS r;
+// one peak's profile rows (row m of shell m, m = 1..mdone)
+struct Rows {
+  const double* r;
+  int mdone;
+  unsigned long long* counters;
+  __device__ __forceinline__ double get(int v, int m) const {
+    if (m > mdone) {                  // never taken when the truncation rule holds
+      atomicAdd(counters + CNT_GUARD, 1ull);
+      return 0.0;
+    }
+    return r[(int64_t)m * ROW + v];
+  }
+};
+
+// kernel_strain (RadialShell.jl:228-277) for centre shell mp over m1 in
+// [lo, hi], summed in m1 order.  For mp > 1 only the shells with
+// (rad[mp] - rad[m1])^2 < 4 contribute (the table window); for mp == 1 the
+// SPH table weights apply to every m1 of [lo, hi].
+__device__ __noinline__ void kernel_strain(const ShellArgs& a, const Rows& R, int mp, int lo, int hi,
+                                           double wRnor, double aRnor, KS* out) {
+  double E[6] = {0, 0, 0, 0, 0, 0}, g[3] = {0, 0, 0}, gf[3] = {0, 0, 0};
+  const double* w;
+  double scale;
+  if (mp > 1) {
+    const int wl = __ldg(a.win_lo + mp), wh = __ldg(a.win_hi + mp);
+    lo = max(lo, wl);
+    hi = min(hi, wh);
+    w = a.wts + __ldg(a.win_off + mp) - wl;
+    scale = wRnor / __ldg(a.rad + mp);
+  } else {
+    w = a.w1;
+    scale = aRnor;
+  }
+  if (hi > R.mdone) {                 // never taken when the truncation rule holds
+    atomicAdd(R.counters + CNT_GUARD, 1ull);
+    hi = R.mdone;
+  }
+  for (int m1 = lo; m1 <= hi; m1++) {
+    const double wt = __ldg(w + m1);
+    if (mp == 1 && isnan(wt)) atomicAdd(R.counters + CNT_AKK, 1ull);
+    const double2* row = reinterpret_cast<const double2*>(R.r + (int64_t)m1 * ROW);
+    const double2 v0 = row[0], v1 = row[1], v2 = row[2], v3 = row[3], v4 = row[4], v5 = row[5], v6 = row[6];
+    // v0 = (Fbar, G0), v1 = (G1, G2), v2 = (Gf0, Gf1), v3 = (Gf2, Q0), v4 = (Q1, Q2), v5 = (Q3, Q4), v6 = (Q5, -)
+    g[0] += wt * v0.y; g[1] += wt * v1.x; g[2] += wt * v1.y;
+    gf[0] += wt * v2.x; gf[1] += wt * v2.y; gf[2] += wt * v3.x;
+    E[0] -= 0.5 * wt * v3.y; E[1] -= 0.5 * wt * v4.x; E[2] -= 0.5 * wt * v4.y;
+    E[3] -= 0.5 * wt * v5.x; E[4] -= 0.5 * wt * v5.y; E[5] -= 0.5 * wt * v6.x;
+  }
 #pragma unroll
-  for (int q = 0; q < 6; q++) r.E[q] = __shfl_sync(FULL, k.E[q], src);
+  for (int q = 0; q < 6; q++) out->E[q] = E[q] * scale;
 #pragma unroll
   for (int L = 0; L < 3; L++) {
-    r.g[L] = __shfl_sync(FULL, k.g[L], src);
-    r.gf[L] = __shfl_sync(FULL, k.gf[L], src);
+    out->g[L] = g[L] * scale;
+    out->gf[L] = gf[L] * scale;
   }
-  return r;
-}
-
-// ---------------------------------------------------------------------------
-// geometry helpers over rad[] (increasing for m >= 1)
-// ---------------------------------------------------------------------------
-// smallest m in [lo, hi] with rad[m] > x, or hi+1
-__device__ __forceinline__ int first_gt(const double* rad, int lo, int hi, double x) {
-  while (lo <= hi) {
-    const int mid = (lo + hi) >> 1;
-    if (rad[mid] > x) hi = mid - 1; else lo = mid + 1;
-  }
-  return lo;
-}
-// largest m in [lo, hi] with rad[m] < x, or lo-1
-__device__ __forceinline__ int last_lt(const double* rad, int lo, int hi, double x) {
-  while (lo <= hi) {
-    const int mid = (lo + hi) >> 1;
-    if (rad[mid] < x) lo = mid + 1; else hi = mid - 1;
-  }
-  return hi;
 }
 
 __device__ __forceinline__ void write_no_collapse(double* o) {
-  const int lane = threadIdx.x & 31;
-  if (lane < RES_N) o[lane] = (lane == 0 || lane == 26) ? -1.0 : 0.0;
+#pragma unroll
+  for (int q = 0; q < RES_N; q++) o[q] = (q == 0 || q == 26) ? -1.0 : 0.0;
 }
 
-// ---------------------------------------------------------------------------
-// the per-peak body
-// ---------------------------------------------------------------------------
-template <bool COMP, bool ADAPTIVE>
-__device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base, double* smem) {
-  const int lane = threadIdx.x & 31;
-  const int n = a.n;
-  const int64_t n2 = (int64_t)n * n;
-  const int64_t lin = a.pk.lin[p];
+__device__ void collapse_one(const ShellArgs& a, int64_t p) {
   double* out = a.out + p * RES_N;
-  const double ZZon = a.pk.ZZon[p];
-  if (lin < 0 || lin >= n2 * n || !(ZZon > -1.0)) {   // invalid peak index or redshift from the caller
-    if (lane == 0) atomicAdd(a.counters + CNT_BADPEAK, 1ull);
+  const PeakHdr h = a.hdr[p];
+  if (h.status != HS_OK) {
     write_no_collapse(out);
     return;
   }
-  const int pk = (int)(lin / n2), pj = (int)((lin / n) % n), pi = (int)(lin % n);
-  const double Rf = a.pk.Rf[p];
-  const int ir2min = a.pk.ir2min[p];
-  const double fcrit = a.pk.fcrit[p];
-  const double alatt = a.alatt;
   const double* __restrict__ rad = a.rad;
-  const int mmax = a.mmax;
-
-  Prof P{smem, SMEM_SHELLS + 1, 0, a.counters, SMEM_SHELLS, prof_base, a.nshell + 1};
-  double* part = smem + NV * (SMEM_SHELLS + 1);   // chunk partials [value][lane]
-
-  // ---- geometry that depends only on the shell radii --------------------
-  // m0 of the gather loop (RadialShell.jl:392-399): first finalised shell with
-  // r^2 > ir2min, else the last finalised shell.
-  int m0_init;
-  {
-    int lo = 2, hi = mmax;
-    while (lo <= hi) {
-      const int mid = (lo + hi) >> 1;
-      if (a.r2m[mid] > ir2min) hi = mid - 1; else lo = mid + 1;
-    }
-    m0_init = (lo <= mmax) ? lo : (mmax >= 2 ? mmax : 1);
-  }
-  // mrf (RadialShell.jl:457-471): the per-cell scan is decided by the first
-  // cell of each distinct r^2; group s (s-th nonzero r^2) reports index
-  // max(s-1, 1); earliest strict minimum of |r^2 - (Rf/alatt)^2| below 10.
-  int mrf = 1;
-  {
-    const double rq = (Rf / alatt) * (Rf / alatt);
-    const int K = a.nshell - 1;
-    auto r2s = [&](int s) -> double { return (double)a.r2m[s + 1]; };
-    int lo = 1, hi = K;
-    while (lo <= hi) {
-      const int mid = (lo + hi) >> 1;
-      if (r2s(mid) >= rq) hi = mid - 1; else lo = mid + 1;
-    }
-    double best = 10.0;
-    int sbest = 0;
-    for (int s = lo - 1; s <= lo; s++) {
-      if (s < 1 || s > K) continue;
-      const double dv = fabs(r2s(s) - rq);
-      if (dv < best) { best = dv; sbest = s; }
-    }
-    if (sbest > 0) mrf = sbest > 1 ? sbest - 1 : 1;
-  }
-  int mlow_rf = mrf;
-  if (mrf > 1) {
-    const double rlow = fmax(rad[mrf] - 2.0, 0.0);
-    const int f = first_gt(rad, 1, mrf - 1, rlow);
-    if (f <= mrf - 1) mlow_rf = f;
-  }
-  int mupp_rf = mrf;
-  {
-    const int l = last_lt(rad, mrf + 1, mmax, rad[mrf] + 2.0);
-    if (l >= mrf + 1) mupp_rf = l;
-  }
-
-  // ---- gather -----------------------------------------------------------
-  const float4* __restrict__ aos = a.aos;
-  {
-    const float4 c0 = aos[2 * lin], c1 = aos[2 * lin + 1];
-    if (lane == 0) {
-      P.set(PV_FBAR, 1, (double)c0.x);
-      P.set(PV_N, 1, 1.0);
-      P.set(PV_S + 0, 1, (double)c0.z);
-      P.set(PV_S + 1, 1, (double)c0.w);
-      P.set(PV_S + 2, 1, (double)c1.x);
-      P.set(PV_S2 + 0, 1, (double)c1.y);
-      P.set(PV_S2 + 1, 1, (double)c1.z);
-      P.set(PV_S2 + 2, 1, (double)c1.w);
-#pragma unroll
-      for (int v = 0; v < 3; v++) { P.set(PV_G + v, 1, 0.0); P.set(PV_GF + v, 1, 0.0); }
-#pragma unroll
-      for (int v = 0; v < 6; v++) P.set(PV_Q + v, 1, 0.0);
-    }
-  }
-  const int rext = (int)ceil(rad[mmax]) + 1;
-  const bool inside = pi - rext >= 0 && pj - rext >= 0 && pk - rext >= 0 && pi + rext < n && pj + rext < n &&
-                      pk + rext < n;
-  int state = 0;          // 0 unknown, 1 inward, 2 crossing found, 3 no crossing
-  int mcross = 0;
-  int mtarget = ADAPTIVE ? -1 : mmax;   // last shell to gather (-1: not known yet)
-  int mdone = 1;
-  double fbar_prev = (double)aos[2 * lin].x, df_prev = fbar_prev;
-  long long visits = 0;
-  for (int g = 0; g < a.ngroups; g++) {
-    const int base = a.grp_a[g], gend = a.grp_b[g];
-    if (mtarget >= 0 && base > mtarget) break;
-    if (gend > P.cap) P.spill(mdone);   // profile outgrows shared memory
-    const int c0g = a.grp_c[g], ncg = a.grp_c[g + 1] - c0g;
-    // (a) lane l sums chunk c0g + l into the shared partial table
-    if (lane < ncg) {
-      Acc<COMP> A;
-      A.zero();
-      const int s0 = a.ck_s[c0g + lane], cnt = a.ck_n[c0g + lane];
-      int nsh = 0;
-      // loads of the next cell are issued before the current cell is summed
-      int4 cl = __ldg(a.cells + s0);
-      auto in_grid = [&](const int4& c) {
-        const int iv1 = pi + c.x, iv2 = pj + c.y, iv3 = pk + c.z;
-        return inside || (iv1 >= 0 && iv1 < n && iv2 >= 0 && iv2 < n && iv3 >= 0 && iv3 < n);
-      };
-      auto rec = [&](const int4& c) { return (int64_t)(pi + c.x) + (int64_t)n * (pj + c.y) + n2 * (pk + c.z); };
-      bool ok = in_grid(cl);
-      float4 va = make_float4(0.f, 0.f, 0.f, 0.f), vb = va;
-      if (ok) { const int64_t li = rec(cl); va = __ldg(aos + 2 * li); vb = __ldg(aos + 2 * li + 1); }
-      for (int c = 0; c < cnt; c++) {
-        int4 cn = cl;
-        bool okn = false;
-        float4 van = va, vbn = vb;
-        if (c + 1 < cnt) {
-          cn = __ldg(a.cells + s0 + c + 1);
-          okn = in_grid(cn);
-          if (okn) { const int64_t li = rec(cn); van = __ldg(aos + 2 * li); vbn = __ldg(aos + 2 * li + 1); }
-        }
-        if (ok) {
-          nsh++;
-          accumulate_cell<COMP>(A, va, vb, (float)cl.x, (float)cl.y, (float)cl.z);
-        }
-        cl = cn; ok = okn; va = van; vb = vbn;
-      }
-      visits += nsh;
-#pragma unroll
-      for (int v = 0; v < NACC; v++) part[v * 32 + lane] = A.get(v);
-      part[NACC * 32 + lane] = (double)nsh;
-    }
-    __syncwarp();
-    // (b) lane l finalises shell base + l from its chunks (double-precision
-    // sum of the chunk partials, each of which is exact to ~2^-48)
-    const int m = base + lane;
-    double my_dF = 0.0;
-    if (m <= gend) {
-      double t[NACC + 1];
-#pragma unroll
-      for (int v = 0; v <= NACC; v++) t[v] = 0.0;
-      const int k0 = a.sh_c0[m] - c0g, nk = a.sh_nc[m];
-      for (int k = k0; k < k0 + nk; k++) {
-#pragma unroll
-        for (int v = 0; v <= NACC; v++) t[v] += part[v * 32 + k];
-      }
-      const double r = rad[m];
-      const double nsh = t[NACC];
-      P.set(PV_N, m, nsh);
-      my_dF = nsh > 0 ? t[0] / nsh : 0.0;
-#pragma unroll
-      for (int L = 0; L < 3; L++) {
-        P.set(PV_S + L, m, t[1 + L]);
-        P.set(PV_S2 + L, m, t[4 + L]);
-        P.set(PV_G + L, m, t[7 + L] / r);
-        P.set(PV_GF + L, m, t[10 + L] / r);
-      }
-      P.set(PV_Q + 0, m, (2.0 * t[13]) / r);
-      P.set(PV_Q + 1, m, (2.0 * t[14]) / r);
-      P.set(PV_Q + 2, m, (2.0 * t[15]) / r);
-      P.set(PV_Q + 3, m, t[16] / r);
-      P.set(PV_Q + 4, m, t[17] / r);
-      P.set(PV_Q + 5, m, t[18] / r);
-    }
-    __syncwarp();
-    const int mend = gend;
-    // cumulative mean overdensity (RadialShell.jl:386-390), in shell order;
-    // every lane runs the recursion, the owner lane of shell mm keeps Fbar
-    double my_fb = 0.0;
-    for (int mm = base; mm <= mend; mm++) {
-      const double dF = __shfl_sync(FULL, my_dF, mm - base);
-      const double r3p = rad[mm - 1] * rad[mm - 1] * rad[mm - 1];
-      const double r3 = rad[mm] * rad[mm] * rad[mm];
-      const double fb = (r3p * fbar_prev + 0.5 * (df_prev + dF) * (r3 - r3p)) / r3;
-      if (lane == mm - base) my_fb = fb;
-      fbar_prev = fb;
-      df_prev = dF;
-      if (ADAPTIVE && state == 0 && mm >= m0_init) {
-        if (mm == m0_init && fb < fcrit) {
-          state = 1;
-        } else if (fb < fcrit) {
-          state = 2;
-          mcross = mm;
-        }
-      }
-    }
-    if (m <= mend) P.set(PV_FBAR, m, my_fb);
-    mdone = mend;
-    if (ADAPTIVE) {
-      if (state == 0 && mdone >= mmax) state = 3;
-      if (state != 0) {
-        int M = max(max(m0_init, mrf), mupp_rf);
-        if (state == 2) M = max(M, mcross);
-        mtarget = state == 3 ? mmax : a.need[M];
-      }
-    }
-    __syncwarp();
-  }
-  P.mdone = mdone;
-  __syncwarp();
-  {
-    const long long tv = warp_sum_ll(visits);
-    if (lane == 0) atomicAdd(a.counters + CNT_VISITS, (unsigned long long)tv);
-  }
-
-  // ---- post-process (double precision) -----------------------------------
+  const Rows R{a.pool + h.off * ROW, h.mdone, a.counters};
+  const double ZZon = a.pk.ZZon[p];
+  const double alatt = a.alatt;
+  const int m = a.mmax;
+  const Geo geo = geometry(a, a.pk.Rf[p], a.pk.ir2min[p]);
   const double hlatt = 1.0, anor = 1.0;
   const double aRnor = 3.0 * anor / alatt, wnor = anor / (4.0 * 3.141592653589793), wRnor = 3.0 * wnor / alatt;
-  const int m = mmax;
 
   // Phase 3: gradient at the filter scale
-  KS krf;
-  ks_multi(P, a, mrf, mlow_rf, mupp_rf, 32, wRnor, aRnor, &krf);
-
-  // Phase 4: fcrit crossing (RadialShell.jl:494-537)
-  int m0 = m0_init;
-  if (P.get(PV_FBAR, m0) >= fcrit) {
-    for (int mm = m0; mm <= m; mm++) {
-      if (P.get(PV_FBAR, mm) < fcrit) { m0 = mm; break; }
-    }
-  } else {
-    const int mstart = max(m0 - 1, 1);
-    bool found = false;
-    for (int mp = mstart; mp >= 1; mp--) {
-      if (P.get(PV_FBAR, mp) >= fcrit) { found = true; break; }
-      m0 = mp;
-    }
-    if (!found) {
-      if (lane == 0) atomicAdd(a.counters + CNT_NOFCRIT, 1ull);
-      write_no_collapse(out);
-      return;
-    }
-  }
-  if (m0 == 1) {   // zvir1p at m0 is forced to -1 < ZZon (RadialShell.jl:581-622)
-    if (lane == 0) atomicAdd(a.counters + CNT_M0ONE, 1ull);
-    write_no_collapse(out);
-    return;
+  double grf[3];
+  {
+    KS krf;
+    kernel_strain(a, R, geo.mrf, geo.mlow_rf, geo.mupp_rf, wRnor, aRnor, &krf);
+#pragma unroll
+    for (int L = 0; L < 3; L++) grf[L] = krf.g[L];
   }
 
-  // Phase 5: inward walk (RadialShell.jl:566-699).  Each round evaluates K
-  // consecutive steps top, top-1, ..., top-K+1 on K lane groups of G = 32/K
-  // lanes; group 0 repeats the last step of the previous round (the m0 step
-  // in round 0, whose zvir is forced to -1), so the step before a collapse is
-  // always the group to the left.  Most peaks collapse within a few steps of
-  // m0: round 0 uses 4 steps of 8 lanes, later rounds 32 steps of 1 lane.
-  // At mp = 1 the reference's running window is [2, last shell with rad < 2].
+  // Phase 5: inward walk (RadialShell.jl:566-699) from the crossing m0; the
+  // m0 step's zvir is forced to -1.  At mp = 1 the reference's running window
+  // is [2, last shell with rad < 2].
   const int hi1 = last_lt(rad, 2, m, 2.0);
-  Walk last, prev;
-  double zvir1 = -1.0, zvir1p = -1.0;
+  int m0 = h.m0;
+  KS prev, last;
+  kernel_strain(a, R, m0, 2, m0 > 1 ? m : hi1, wRnor, aRnor, &prev);
+  double zprev = -1.0, zvir1 = -1.0, zvir1p = -1.0, lastFh = 0.0;
   bool collapsed = false;
-  int rounds = 0;
-  int top = m0;
-  for (int b = 0;; b++) {
-    rounds++;
-    const int G = b == 0 ? 8 : 1;
-    const int K = 32 / G;
-    const int grp = lane / G;
-    const int mp = top - grp;
-    Walk w;
-    w.zv = -1.0;
-    // the running mlow never reaches shell 1 (rad 0 is not > max(rad-2, 0))
-    ks_multi(P, a, mp, 2, mp > 1 ? m : hi1, G, wRnor, aRnor, &w.k);
-    const bool act = mp >= 1;
-    if (act) {
-      ev_pv(w.k.E, &w.Fh, &w.ev, &w.pv);
-      w.Fr = P.get(PV_FBAR, mp);
-      if (!(b == 0 && grp == 0)) w.zv = zvir_of(a.tab, w.Fr, w.ev, w.pv);
-    }
-    const unsigned bal = __ballot_sync(FULL, act && grp >= 1 && (lane & (G - 1)) == 0 && w.zv >= ZZon);
-    if (bal) {
-      const int L = __ffs(bal) - 1;
-      last.k = shfl_ks(w.k, L);
-      prev.k = shfl_ks(w.k, L - G);
-      last.Fh = __shfl_sync(FULL, w.Fh, L);
-      last.Fr = __shfl_sync(FULL, w.Fr, L);
-      last.ev = __shfl_sync(FULL, w.ev, L);
-      last.pv = __shfl_sync(FULL, w.pv, L);
-      zvir1p = __shfl_sync(FULL, w.zv, L);
-      zvir1 = __shfl_sync(FULL, w.zv, L - G);   // -1 when group L/G - 1 is the m0 step
-      m0 = top - L / G + 1;
+  long long steps = 1;
+  for (int mp = m0 - 1; mp >= 1; mp--) {
+    KS cur;
+    kernel_strain(a, R, mp, 2, mp > 1 ? m : hi1, wRnor, aRnor, &cur);
+    steps++;
+    double Fh, ev, pv;
+    ev_pv(cur.E, &Fh, &ev, &pv);
+    const double zv = zvir_of(a.tab, R.get(R_FBAR, mp), ev, pv);
+    if (zv >= ZZon) {
+      last = cur;
+      lastFh = Fh;
+      zvir1p = zv;
+      zvir1 = zprev;
+      m0 = mp + 1;
       collapsed = true;
       break;
     }
-    if (top - (K - 1) <= 1) break;   // reached mp = 1 without collapse
-    top -= K - 1;
+    prev = cur;
+    zprev = zv;
   }
-  if (lane == 0) atomicAdd(a.counters + CNT_WALK, (unsigned long long)rounds);
+  atomicAdd(a.counters + CNT_WALK, (unsigned long long)steps);
   if (!collapsed) {
-    if (lane == 0) atomicAdd(a.counters + CNT_NOCOLL, 1ull);
+    atomicAdd(a.counters + CNT_NOCOLL, 1ull);
     write_no_collapse(out);
     return;
   }
@@ -641,7 +646,7 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base, do
   // Phase 6: collapse radius (RadialShell.jl:707-754)
   const double dZvir = zvir1p - zvir1;
   double RTHL;
-  const double ra = rad[m0 - 1], rb = rad[m0];
+  const double ra = __ldg(rad + m0 - 1), rb = __ldg(rad + m0);
   const double rad3p = ra * ra * ra, rad3 = rb * rb * rb;
   if (zvir1 > 0.0 && dZvir != 0.0) {
     const double R3 = rad3p + (rad3 - rad3p) * (zvir1p - ZZon) / dZvir;
@@ -650,13 +655,13 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base, do
     RTHL = ra;
   }
   if (RTHL <= 0.0) {
-    if (lane == 0) atomicAdd(a.counters + CNT_RTHLNEG, 1ull);
+    atomicAdd(a.counters + CNT_RTHLNEG, 1ull);
     write_no_collapse(out);
     return;
   }
   const double RTHL3 = RTHL * RTHL * RTHL, RTHL5 = RTHL3 * RTHL * RTHL;
   const double drad3 = rad3 - rad3p;
-  const double Fa = P.get(PV_FBAR, m0 - 1), Fb = P.get(PV_FBAR, m0);
+  const double Fa = R.get(R_FBAR, m0 - 1), Fb = R.get(R_FBAR, m0);
   const double dFb = Fb - Fa;
   double Fbarx;
   double S[6], gk[3], gkf[3];
@@ -664,18 +669,18 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base, do
     const double fr = (RTHL3 - rad3p) / drad3;
     Fbarx = Fa + fr * dFb;
 #pragma unroll
-    for (int q = 0; q < 6; q++) S[q] = last.k.E[q] + fr * (prev.k.E[q] - last.k.E[q]);
+    for (int q = 0; q < 6; q++) S[q] = last.E[q] + fr * (prev.E[q] - last.E[q]);
 #pragma unroll
     for (int L = 0; L < 3; L++) {
-      gk[L] = last.k.g[L] + fr * (prev.k.g[L] - last.k.g[L]);
-      gkf[L] = last.k.gf[L] + fr * (prev.k.gf[L] - last.k.gf[L]);
+      gk[L] = last.g[L] + fr * (prev.g[L] - last.g[L]);
+      gkf[L] = last.gf[L] + fr * (prev.gf[L] - last.gf[L]);
     }
   } else {
     Fbarx = Fa;
 #pragma unroll
-    for (int q = 0; q < 6; q++) S[q] = last.k.E[q];
+    for (int q = 0; q < 6; q++) S[q] = last.E[q];
 #pragma unroll
-    for (int L = 0; L < 3; L++) { gk[L] = prev.k.g[L]; gkf[L] = prev.k.gf[L]; }
+    for (int L = 0; L < 3; L++) { gk[L] = prev.g[L]; gkf[L] = prev.gf[L]; }
   }
   // normalize_strain then eigenvalues (RadialShell.jl:748-752)
   {
@@ -690,178 +695,160 @@ __device__ void analyse_one(const ShellArgs& a, int64_t p, double* prof_base, do
   ev_pv(S, &Frhoc, &e_v_f, &p_v_f);
   double smat[6];
 #pragma unroll
-  for (int q = 0; q < 6; q++) smat[q] = last.k.E[q] * (Fbarx / last.Fh);
+  for (int q = 0; q < 6; q++) smat[q] = last.E[q] * (Fbarx / lastFh);
 
   // Phase 7: Sbar, Sbar2 (RadialShell.jl:758-773), Srb (:776-790)
   double sb[6] = {0, 0, 0, 0, 0, 0};
   long long nS = 0;
   double srb = 0.0;
-  for (int m1 = 1 + lane; m1 <= m0 - 1; m1 += 32) {
-    const double nn = P.get(PV_N, m1);
+  for (int m1 = 1; m1 <= m0 - 1; m1++) {
+    const double nn = R.get(R_N, m1);
     if (nn > 0) {
 #pragma unroll
       for (int L = 0; L < 3; L++) {
-        sb[L] += P.get(PV_S + L, m1);
-        sb[3 + L] += P.get(PV_S2 + L, m1);
+        sb[L] += R.get(R_S + L, m1);
+        sb[3 + L] += R.get(R_S2 + L, m1);
       }
       nS += (long long)nn;
     }
     if (m1 >= 2) {
-      const double r5 = a.rad5[m1], r5p = m1 - 1 >= 2 ? a.rad5[m1 - 1] : 0.0;
-      srb += 0.5 * (P.get(PV_FBAR, m1 - 1) + P.get(PV_FBAR, m1)) * (r5 - r5p);
+      const double r5 = __ldg(a.rad5 + m1), r5p = m1 - 1 >= 2 ? __ldg(a.rad5 + m1 - 1) : 0.0;
+      srb += 0.5 * (R.get(R_FBAR, m1 - 1) + R.get(R_FBAR, m1)) * (r5 - r5p);
     }
   }
-#pragma unroll
-  for (int q = 0; q < 6; q++) sb[q] = warp_sum(sb[q]);
-  nS = warp_sum_ll(nS);
-  srb = warp_sum(srb);
   if (nS > 0) {
 #pragma unroll
     for (int q = 0; q < 6; q++) sb[q] /= (double)nS;
   }
-  const double rad5p = (m0 - 1 >= 2) ? a.rad5[m0 - 1] : 0.0;
+  const double rad5p = (m0 - 1 >= 2) ? __ldg(a.rad5 + m0 - 1) : 0.0;
   if (zvir1 > 0.0 && dZvir != 0.0) srb += 0.5 * (Fa + Fbarx) * (RTHL5 - rad5p);
   if (Fbarx * RTHL5 > 0.0) srb /= (Fbarx * RTHL5);
 
-  // d2F: mean lapd over cells (centre excluded) with sqrt(r2) <= RTHL, in
-  // list order, stopping at the first out-of-grid cell (RadialShell.jl:805-819)
-  double d2F = 0.0;
-  if (a.lapd) {
-    double acc = 0.0;
-    long long navg = 0;
-    bool stop = false;
-    for (int64_t c0 = 1; c0 < a.npart && !stop; c0 += 32) {
-      const int64_t c = c0 + lane;
-      bool valid = false, oob = false;
-      float v = 0.f;
-      if (c < a.npart) {
-        const int4 cl = __ldg(a.cells + c);
-        if (!(sqrt((double)cl.w) > RTHL)) {
-          const int iv1 = pi + cl.x, iv2 = pj + cl.y, iv3 = pk + cl.z;
-          if (iv1 < 0 || iv1 >= n || iv2 < 0 || iv2 >= n || iv3 < 0 || iv3 >= n) oob = true;
-          else { valid = true; v = a.lapd[iv1 + (int64_t)n * iv2 + n2 * iv3]; }
-        }
-      }
-      const unsigned ob = __ballot_sync(FULL, oob);
-      if (ob) {
-        const int first = __ffs(ob) - 1;
-        if (lane >= first) valid = false;
-        stop = true;
-      }
-      if (valid) { acc += (double)v; navg++; }
-      const int4 last_cell = __ldg(a.cells + min(c0 + 31, a.npart - 1));
-      if (sqrt((double)last_cell.w) > RTHL) stop = true;
-    }
-    acc = warp_sum(acc);
-    navg = warp_sum_ll(navg);
-    if (navg > 0) d2F = acc / (double)navg;
-  }
-
-  // zvir_half (RadialShell.jl:825-885): the ten radii on lane pairs 0..19
+  // zvir_half (RadialShell.jl:825-885): ten radii RTHL (e/18 + 1/2)^(1/3)
   double zvir_half = -1.0;
   if (RTHL / hlatt >= 3.0) {
-    const int e = lane >> 1;   // radius index jj - 1
-    int m0_rc = 0, mlow_rc = 1, mupp_rc = 1;
-    if (e < 10) {
-      const double rcur = RTHL * pow(e / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
+    for (int e = 0; e < 10; e++) {
+      const double rcur = RTHL * a.fhalf[e];
       // first m1 in [2, m-1] with rad > rcur + 2 (the loop's break), else m-1
       const int fu = first_gt(rad, 2, m - 1, rcur + 2.0 * hlatt);
-      mupp_rc = fu <= m - 1 ? fu : (m - 1 >= 2 ? m - 1 : 1);
+      const int mupp_rc = fu <= m - 1 ? fu : (m - 1 >= 2 ? m - 1 : 1);
+      int mlow_rc = 1;
       const int fl = first_gt(rad, 1, m - 1, fmax(rcur - 2.0 * hlatt, 0.0));
       if (fl <= m - 1) mlow_rc = fl;
       const int f0 = first_gt(rad, 1, m - 1, rcur);
-      m0_rc = (f0 <= m - 1) ? f0 : max(m - 1, 1);
-    }
-    KS krc;
-    ks_multi(P, a, m0_rc, mlow_rc, mupp_rc, 2, wRnor, aRnor, &krc);
-    double zl = -1.0;
-    if (e < 10) {
+      const int m0_rc = (f0 <= m - 1) ? f0 : max(m - 1, 1);
+      KS krc;
+      kernel_strain(a, R, m0_rc, mlow_rc, mupp_rc, wRnor, aRnor, &krc);
       double Fr, ev, pv;
       ev_pv(krc.E, &Fr, &ev, &pv);
-      zl = zvir_of(a.tab, P.get(PV_FBAR, m0_rc), ev, pv) - 1.0;
+      zvir_half = fmax(zvir_half, zvir_of(a.tab, R.get(R_FBAR, m0_rc), ev, pv) - 1.0);
     }
-    zvir_half = fmax(warp_max(zl), -1.0);
   }
 
-  // results (layout in ppb.h)
-  if (lane == 0) {
-    double r[RES_N];
-    r[0] = RTHL;
-    r[1] = srb;
+  // results (layout in ppb.h); d2F (30) comes from d2f_kernel
+  double r[RES_N];
+  r[0] = RTHL;
+  r[1] = srb;
 #pragma unroll
-    for (int L = 0; L < 3; L++) {
-      r[2 + L] = sb[L];
-      r[5 + L] = sb[3 + L];
-      r[17 + L] = gk[L];
-      r[20 + L] = krf.g[L];
-      r[27 + L] = gkf[L];
-    }
-    r[8] = smat[0]; r[9] = smat[3]; r[10] = smat[4];
-    r[11] = smat[3]; r[12] = smat[1]; r[13] = smat[5];
-    r[14] = smat[4]; r[15] = smat[5]; r[16] = smat[2];
-    r[23] = Fbarx;
-    r[24] = e_v_f;
-    r[25] = p_v_f;
-    r[26] = zvir_half;
-    r[30] = d2F;
-#pragma unroll
-    for (int q = 0; q < RES_N; q++) out[q] = r[q];
+  for (int L = 0; L < 3; L++) {
+    r[2 + L] = sb[L];
+    r[5 + L] = sb[3 + L];
+    r[17 + L] = gk[L];
+    r[20 + L] = grf[L];
+    r[27 + L] = gkf[L];
   }
+  r[8] = smat[0]; r[9] = smat[3]; r[10] = smat[4];
+  r[11] = smat[3]; r[12] = smat[1]; r[13] = smat[5];
+  r[14] = smat[4]; r[15] = smat[5]; r[16] = smat[2];
+  r[23] = Fbarx;
+  r[24] = e_v_f;
+  r[25] = p_v_f;
+  r[26] = zvir_half;
+  r[30] = 0.0;
+#pragma unroll
+  for (int q = 0; q < RES_N; q++) out[q] = r[q];
 }
 
-template <bool COMP, bool ADAPTIVE>
-__global__ void __launch_bounds__(128, 3) shell_kernel(ShellArgs a) {
+__global__ void __launch_bounds__(128) collapse_kernel(ShellArgs a) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < a.npk) collapse_one(a, p);
+}
+
+// ===========================================================================
+// d2F kernel (one warp per collapsed peak, grid-stride)
+// ===========================================================================
+// mean lapd over the cells (centre excluded) with sqrt(r2) <= RTHL, in list
+// order, stopping at the first out-of-grid cell (RadialShell.jl:805-819).
+// The cells with sqrt(r2) <= RTHL are a prefix of the sorted list: the cells
+// before the first shell with rad > RTHL.
+__global__ void __launch_bounds__(128) d2f_kernel(ShellArgs a) {
   const int lane = threadIdx.x & 31;
-  const int warp_in_block = threadIdx.x >> 5;
-  const int64_t slot = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp_in_block;
-  double* prof = a.scratch + slot * a.scratch_stride;
-  extern __shared__ double shm[];
-  double* smem = shm + (size_t)warp_in_block * SMEM_WARP_DOUBLES;
-  while (true) {
-    int p = 0;
-    if (lane == 0) p = atomicAdd(a.queue, 1);
-    p = __shfl_sync(FULL, p, 0);
-    if (p >= a.npk) break;
-    analyse_one<COMP, ADAPTIVE>(a, p, prof, smem);
-    __syncwarp();
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int n = a.n;
+  const int64_t n2 = (int64_t)n * n;
+  for (int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); p < a.npk; p += nwarps) {
+    double* out = a.out + p * RES_N;
+    const double RTHL = out[0];
+    if (!(RTHL > 0.0)) continue;
+    const int64_t lin = a.pk.lin[p];
+    const int pk = (int)(lin / n2), pj = (int)((lin / n) % n), pi = (int)(lin % n);
+    const int mR = first_gt(a.rad, 1, a.nshell, RTHL);   // 1-based shell; distinct r2 index mR - 1
+    const int64_t cend = mR <= a.nshell ? (int64_t)__ldg(a.sh_start + mR - 1) : a.npart;
+    double acc = 0.0;
+    long long navg = 0;
+    for (int64_t c0 = 1; c0 < cend; c0 += 32) {
+      const int64_t c = c0 + lane;
+      bool valid = false, oob = false;
+      float v = 0.f;
+      if (c < cend) {
+        int di, dj, dk;
+        unpack_cell(__ldg(a.cell8 + c), di, dj, dk);
+        const int iv1 = pi + di, iv2 = pj + dj, iv3 = pk + dk;
+        if (iv1 < 0 || iv1 >= n || iv2 < 0 || iv2 >= n || iv3 < 0 || iv3 >= n) oob = true;
+        else { valid = true; v = __ldg(a.lapd + iv1 + (int64_t)n * iv2 + n2 * iv3); }
+      }
+      const unsigned ob = __ballot_sync(FULL, oob);
+      if (ob && lane >= __ffs(ob) - 1) valid = false;
+      if (valid) { acc += (double)v; navg++; }
+      if (ob) break;
+    }
+    acc = warp_sum(acc);
+    navg = warp_sum_ll(navg);
+    if (lane == 0) out[30] = navg > 0 ? acc / (double)navg : 0.0;
   }
-}
-
-template <bool C, bool A>
-void launch_variant(const ShellArgs& a, dim3 grid, dim3 block, size_t shm, cudaStream_t s) {
-  shell_kernel<C, A><<<grid, block, shm, s>>>(a);
 }
 
 }  // namespace
 
-// allow the dynamic shared memory of the chosen block size (once per process
-// and device; called before occupancy queries and launches)
-void shell_prepare(int warps_per_block) {
-  const int shm = (int)((size_t)warps_per_block * SMEM_WARP_DOUBLES * 8);
-  PPB_CUDA(cudaFuncSetAttribute(shell_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
-  PPB_CUDA(cudaFuncSetAttribute(shell_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
-  PPB_CUDA(cudaFuncSetAttribute(shell_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
-  PPB_CUDA(cudaFuncSetAttribute(shell_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, shm));
+int64_t shell_stage_doubles_per_warp(int nshell) { return (int64_t)ROW * (nshell + 1); }
+
+int shell_gather_blocks_per_sm(bool comp, bool adaptive) {
+  const void* f = comp ? (adaptive ? (const void*)gather_kernel<true, true> : (const void*)gather_kernel<true, false>)
+                       : (adaptive ? (const void*)gather_kernel<false, true> : (const void*)gather_kernel<false, false>);
+  int b = 0;
+  PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, 32 * kGatherWarps, 0));
+  return b > 0 ? b : 1;
 }
 
-const void* shell_kernel_ptr(bool comp, bool adaptive) {
-  if (comp && adaptive) return (const void*)shell_kernel<true, true>;
-  if (comp) return (const void*)shell_kernel<true, false>;
-  if (adaptive) return (const void*)shell_kernel<false, true>;
-  return (const void*)shell_kernel<false, false>;
+void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks) {
+  const dim3 grid(blocks), block(32 * kGatherWarps);
+  if (comp && adaptive) gather_kernel<true, true><<<grid, block, 0, L.s>>>(a);
+  else if (comp) gather_kernel<true, false><<<grid, block, 0, L.s>>>(a);
+  else if (adaptive) gather_kernel<false, true><<<grid, block, 0, L.s>>>(a);
+  else gather_kernel<false, false><<<grid, block, 0, L.s>>>(a);
+  PPB_LAUNCHED(*L.count);
 }
 
-int64_t shell_scratch_doubles_per_warp(int nshell) { return (int64_t)NV * (nshell + 1); }
+void launch_shell_collapse(Launch L, const ShellArgs& a) {
+  const int64_t blocks = (a.npk + 127) / 128;
+  if (blocks == 0) return;
+  collapse_kernel<<<(unsigned)blocks, 128, 0, L.s>>>(a);
+  PPB_LAUNCHED(*L.count);
+}
 
-size_t shell_smem_bytes(int warps_per_block) { return (size_t)warps_per_block * SMEM_WARP_DOUBLES * 8; }
-
-void launch_shell(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks, int warps_per_block) {
-  dim3 grid(blocks), block(32 * warps_per_block);
-  const size_t shm = shell_smem_bytes(warps_per_block);
-  if (comp && adaptive) launch_variant<true, true>(a, grid, block, shm, L.s);
-  else if (comp && !adaptive) launch_variant<true, false>(a, grid, block, shm, L.s);
-  else if (!comp && adaptive) launch_variant<false, true>(a, grid, block, shm, L.s);
-  else launch_variant<false, false>(a, grid, block, shm, L.s);
+void launch_shell_d2f(Launch L, const ShellArgs& a, int blocks) {
+  if (a.npk == 0 || !a.lapd) return;
+  d2f_kernel<<<blocks, 128, 0, L.s>>>(a);
   PPB_LAUNCHED(*L.count);
 }
 

@@ -27,11 +27,11 @@ struct ShellStats {
   unsigned long long visits = 0, guard = 0, akk = 0;
   unsigned long long dump[5] = {0, 0, 0, 0, 0};
   unsigned long long raw[16] = {};
-  float ms = 0.f;
+  float ms = 0.f;                 // the whole stage
+  float kms[3] = {0.f, 0.f, 0.f}; // gather, collapse, d2f kernels
+  unsigned long long pool_rows = 0;   // profile rows written
+  int batches = 0;
 };
-
-// kernel entry points used for occupancy queries (k_shell.cu)
-const void* shell_kernel_ptr(bool comp, bool adaptive);
 
 }  // namespace ppb
 
@@ -54,7 +54,10 @@ struct ppb_ctx {
   ppb::DevTable dtab{};
   ppb::DevBuf akk;
   ppb::ShellTable shells;
-  ppb::DevBuf scratch, counters, queue;
+  ppb::DevBuf stage, counters, ctl, hdr, pool;
+  cudaEvent_t shell_ev[4] = {};
+  int gather_bps[2][2] = {{0, 0}, {0, 0}};    // gather blocks per SM by [comp][adaptive]
+  double rows_per_peak[2] = {0.0, 0.0};       // pool rows per peak seen last, by adaptive
   ppb::DevBuf filt_Rf, filt_ir2;
   ppb::DevBuf g_a, g_D, g_f, chi;
   // growth-table cache
@@ -65,7 +68,6 @@ struct ppb_ctx {
   std::map<int, std::unique_ptr<ppb::TileRes>> tiles;
   int64_t last_visits = 0, last_npk = 0;
   ppb::ShellStats last_shell{};
-  int shell_blocks = 0, shell_wpb = 4;
 
   const ppb::GrowthTable& growth(double Om, double OB, double OL, double h);
   ppb::DevCosmo dev_cosmo(const ppb::GrowthTable& G, double Om, double OL, double h, double zmax, bool need_chi);

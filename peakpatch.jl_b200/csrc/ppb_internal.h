@@ -109,7 +109,10 @@ struct ShellTable {
   // ck_n[c] cells from ck_s[c]; shell m's chunks start at sh_c0[m] (sh_nc[m]).
   std::vector<int32_t> grp_a, grp_b, grp_c, ck_s, ck_n, sh_c0, sh_nc;
   int ngroups = 0;
-  DevBuf d_cells, d_start, d_count, d_r2m, d_rad, d_wlo, d_whi, d_woff, d_wts, d_w1, d_need, d_rad5;
+  // cell offsets packed one per 32-bit word: bytes 0..2 = di, dj, dk as
+  // signed 8-bit values (|d| <= nhunt <= 64)
+  std::vector<int32_t> cell8;
+  DevBuf d_cell8, d_start, d_count, d_r2m, d_rad, d_wlo, d_whi, d_woff, d_wts, d_w1, d_need, d_rad5;
   DevBuf d_grp_a, d_grp_b, d_grp_c, d_ck_s, d_ck_n, d_sh_c0, d_sh_nc;
 };
 void build_shell_table(ShellTable& st, int nhunt);
@@ -161,13 +164,37 @@ struct PeakParams {          // SoA, length npk
   const double* fcrit;
 };
 
+// Per-shell profile row of one peak (ROW doubles, written by the gather
+// kernel, read by the collapse kernel).  The first 16 values are what a
+// kernel_strain window reads, the rest what Sbar/Srb read.
+constexpr int ROW = 24;
+enum {
+  R_FBAR = 0,   // cumulative mean overdensity Fbar (RadialShell.jl:386-390)
+  R_G = 1,      // sum delta * d / r            (3)
+  R_GF = 4,     // sum deltaT * d / r           (3)
+  R_Q = 7,      // sum psi_L d_K / r, symmetric (6: xx yy zz xy xz yz)
+  R_N = 16,     // in-grid cells of the shell
+  R_S = 17,     // sum psi1                     (3)
+  R_S2 = 20     // sum psi2                     (3)
+};
+
+// gather -> collapse hand-off, one per peak
+enum { HS_OK = 0, HS_NOFCRIT = 1, HS_M0ONE = 2, HS_BAD = 3, HS_OVERFLOW = 4 };
+struct PeakHdr {
+  long long off;   // first pool row of the peak (row m of shell m at off + m)
+  int mdone;       // shells 1..mdone gathered
+  int m0;          // fcrit crossing shell (RadialShell.jl:494-537)
+  int status;      // HS_*
+  int pad;
+};
+
 struct ShellArgs {
   const float4* aos;        // 2 float4 per cell: (delta, deltaT, psi1x, psi1y), (psi1z, psi2x, psi2y, psi2z)
   const float* lapd;        // may be null
   int n;
   double alatt;
   // shell geometry
-  const int4* cells;
+  const int32_t* cell8;     // packed cell offsets (ShellTable::cell8)
   const int32_t* sh_start;
   const int32_t* sh_count;
   const double* rad;        // rad[m], m = 0..nshell (index 0 unused); rad[1] = 0
@@ -189,9 +216,14 @@ struct ShellArgs {
   PeakParams pk;
   int64_t npk;
   double* out;              // npk x RES_N
-  double* scratch;          // per-warp profile scratch
-  int64_t scratch_stride;   // doubles per warp slot
-  int* queue;               // work counter for the persistent kernel
+  PeakHdr* hdr;             // npk
+  double* pool;             // profile rows, pool_cap rows of ROW doubles
+  int64_t pool_cap;
+  unsigned long long* pool_ctr;   // rows handed out
+  double* stage;            // per-warp staging rows of the gather kernel
+  int64_t stage_stride;     // doubles per warp slot
+  double fhalf[10];         // ((e/9) / 2 + 1/2)^(1/3), e = 0..9 (zvir_half radii)
+  int* queue;               // work counter for the persistent gather kernel
   unsigned long long* counters;   // [0] cell visits, [1..5] dump reasons
 };
 
@@ -227,12 +259,17 @@ struct PeakBuf {
 void launch_peakfind(Launch L, const float* ds, const float* ls, uint8_t* mask, int n1, int n2, int n3,
                      int nbuff, float fcrit, int fidx, PeakBuf pb);
 
-int64_t shell_scratch_doubles_per_warp(int nshell);
-size_t shell_smem_bytes(int warps_per_block);
-void shell_prepare(int warps_per_block);
-// comp: compensated single-precision sums (else double); adaptive: radial
-// truncation of the gather (else full spheres).  Persistent grid of
-// blocks x warps_per_block warps; a.scratch must hold one profile per warp.
-void launch_shell(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks, int warps_per_block);
+// Shell stage = three launches on one stream:
+//  gather   (persistent, one warp per peak): profile rows + PeakHdr
+//  collapse (one thread per peak): results except d2F
+//  d2f      (one warp per collapsed peak): result 30
+// comp: compensated single-precision gather sums (else double); adaptive:
+// radial truncation of the gather (else full spheres).
+constexpr int kGatherWarps = 4;   // warps per gather block
+int64_t shell_stage_doubles_per_warp(int nshell);
+int shell_gather_blocks_per_sm(bool comp, bool adaptive);
+void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks);
+void launch_shell_collapse(Launch L, const ShellArgs& a);
+void launch_shell_d2f(Launch L, const ShellArgs& a, int blocks);
 
 }  // namespace ppb

@@ -87,6 +87,7 @@ EXPORTED = (
     "ppb_find_peaks", "ppb_analyse_peaks", "ppb_event_record", "ppb_event_elapsed", "ppb_synchronize",
     "ppb_launch_count", "ppb_last_shell_stats", "ppb_last_stage_ms", "ppb_alloc_host", "ppb_free_host",
     "ppb_alloc_device", "ppb_free_device", "ppb_shell_counters", "ppb_find_peaks_noalloc",
+    "ppb_last_shell_times",
 )
 
 
@@ -125,6 +126,7 @@ def load_library():
     L.ppb_last_shell_stats.argtypes = [P, ctypes.POINTER(ctypes.c_int64), P, ctypes.POINTER(ctypes.c_float)]
     L.ppb_last_stage_ms.argtypes = [P, P]
     L.ppb_shell_counters.argtypes = [P, P]
+    L.ppb_last_shell_times.argtypes = [P, P, P, P]
     for f in ("ppb_alloc_host", "ppb_alloc_device"):
         getattr(L, f).argtypes = [P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
     for f in ("ppb_free_host", "ppb_free_device"):
@@ -342,9 +344,15 @@ class Context:
         self._check(self.L.ppb_last_shell_stats(self.h, ctypes.byref(v), _p(d), ctypes.byref(ms)))
         raw = np.zeros(16, np.int64)
         self._check(self.L.ppb_shell_counters(self.h, _p(raw)))
+        kms = np.zeros(3, np.float32)
+        rows = ctypes.c_int64()
+        nb = ctypes.c_int32()
+        self._check(self.L.ppb_last_shell_times(self.h, _p(kms), ctypes.byref(rows), ctypes.byref(nb)))
         return {"visits": v.value, "dumps": dict(zip(("premask", "no_fcrit", "m0_one", "no_collapse", "rthl_neg"),
                                                       d.tolist())), "ms": ms.value, "guard": int(raw[6]),
-                "akk_overrun": int(raw[7]), "bad_peaks": int(raw[8]), "walk_rounds": int(raw[9])}
+                "akk_overrun": int(raw[7]), "bad_peaks": int(raw[8]), "walk_steps": int(raw[9]),
+                "kernel_ms": dict(zip(("gather", "collapse", "d2f"), kms.tolist())),
+                "pool_rows": rows.value, "batches": nb.value}
 
     def stage_ms(self):
         a = np.zeros(4, np.float32)
