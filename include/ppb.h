@@ -200,10 +200,10 @@ int32_t ppb_last_shell_stats(ppb_ctx* ctx, int64_t* visits, int64_t* dumps5, flo
  * (must be 0), [7] SPH-table overruns (the reference raises there),
  * [8] invalid peak inputs, [9] collapse-walk steps evaluated, others reserved. */
 int32_t ppb_shell_counters(ppb_ctx* ctx, int64_t* out16);
-/* Device time (ms) of the shell stage's three kernels in the last run:
- * [0] gather, [1] collapse walk, [2] d2F; *rows = profile rows written
- * (ROW = 24 doubles each), *batches = peak batches the stage ran in. */
-int32_t ppb_last_shell_times(ppb_ctx* ctx, float* ms3, int64_t* rows, int32_t* batches);
+/* Device time (ms) of the shell stage's four kernels in the last run:
+ * [0] gather, [1] collapse walk, [2] zvir_half, [3] d2F; *rows = profile
+ * rows written (24 doubles each), *batches = peak batches the stage ran in. */
+int32_t ppb_last_shell_times(ppb_ctx* ctx, float* ms4, int64_t* rows, int32_t* batches);
 /* Per-stage device times (ms) of the last ppb_run_tile_timed call:
  * [0] fields, [1] filter bank + peaks, [2] shell analysis, [3] records. */
 int32_t ppb_last_stage_ms(ppb_ctx* ctx, float* ms4);

@@ -98,6 +98,8 @@ ShellArgs ppb_ctx::shell_args(int n, double alatt, const float4* aos, const floa
   a.alatt = alatt;
   PPB_REQUIRE(n <= 4096, "grid size above 4096");
   a.cell8 = shells.d_cell8.as<int32_t>();
+  upload_cellf(shells, n, stream);
+  a.cellf = shells.d_cellf.as<float4>();
   a.sh_start = shells.d_start.as<int32_t>();
   a.sh_count = shells.d_count.as<int32_t>();
   a.rad = shells.d_rad.as<double>();
@@ -135,6 +137,7 @@ void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st)
   counters.ensure(16 * 8);
   ctl.ensure(64);
   hdr.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(PeakHdr));
+  geo.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(int4));
   PPB_CUDA(cudaMemsetAsync(counters.p, 0, 16 * 8, stream));
   // profile pool: sized from the rows per peak of the previous call; peaks
   // run in batches that fit the pool budget, and a batch whose rows overflow
@@ -163,6 +166,7 @@ void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st)
     b.npk = nb;
     b.out = a.out + p0 * RES_N;
     b.hdr = hdr.as<PeakHdr>() + p0;
+    b.geo = geo.as<int4>() + p0;
     b.pool = pool.as<double>();
     b.pool_cap = cap;
     b.pool_ctr = reinterpret_cast<unsigned long long*>(ctl.as<char>() + 8);
@@ -173,12 +177,15 @@ void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st)
     for (int e = 0; e < 10; e++) b.fhalf[e] = std::pow(e / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
     PPB_CUDA(cudaMemsetAsync(ctl.p, 0, 16, stream));
     PPB_CUDA(cudaEventRecord(shell_ev[0], stream));
+    launch_shell_geo(L, b);
     launch_shell_gather(L, b, comp, adaptive, gblocks);
     PPB_CUDA(cudaEventRecord(shell_ev[1], stream));
     launch_shell_collapse(L, b);
     PPB_CUDA(cudaEventRecord(shell_ev[2], stream));
-    launch_shell_d2f(L, b, nsm * 16);
+    launch_shell_zhalf(L, b);
     PPB_CUDA(cudaEventRecord(shell_ev[3], stream));
+    launch_shell_d2f(L, b, nsm * 16);
+    PPB_CUDA(cudaEventRecord(shell_ev[4], stream));
     unsigned long long used = 0;
     PPB_CUDA(cudaMemcpyAsync(&used, b.pool_ctr, sizeof(used), cudaMemcpyDeviceToHost, stream));
     PPB_CUDA(cudaMemcpyAsync(c, counters.p, sizeof(c), cudaMemcpyDeviceToHost, stream));
@@ -191,10 +198,10 @@ void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st)
       rpp = seen;
       continue;
     }
-    float k[3];
-    for (int e = 0; e < 3; e++) PPB_CUDA(cudaEventElapsedTime(&k[e], shell_ev[e], shell_ev[e + 1]));
-    for (int e = 0; e < 3; e++) s.kms[e] += k[e];
-    s.ms += k[0] + k[1] + k[2];
+    float k[4];
+    for (int e = 0; e < 4; e++) PPB_CUDA(cudaEventElapsedTime(&k[e], shell_ev[e], shell_ev[e + 1]));
+    for (int e = 0; e < 4; e++) s.kms[e] += k[e];
+    s.ms += k[0] + k[1] + k[2] + k[3];
     s.pool_rows += used;
     s.batches++;
     if (nb == a.npk - p0 || nb >= 1024) rpp = std::max(1.0, (double)used / (double)nb);

@@ -219,26 +219,42 @@ __device__ __forceinline__ double window_w(double kR, double k, int ws) {
   return 3.0 * (s - kR * c) / (kR * kR * kR);
 }
 
+// Window tables of a filter bank: W depends on k only through the integer
+// q = ix^2 + fy^2 + fz^2 (fy, fz the signed frequencies), so each filter's
+// two windows are tabulated once over q in double precision and rounded to
+// Float32 as the reference rounds them (Tf(w)).  k = dk sqrt(q); q = 0 keeps
+// the mode (the reference skips fkR == 0).
+__global__ void window_table_kernel(float* __restrict__ tab, int qn, double dkk, const double* __restrict__ Rf,
+                                    int wsmooth, int want_lap) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = blockIdx.y;
+  if (q >= qn) return;
+  const double k = dkk * sqrt((double)q);
+  const double fkR = k * Rf[f];
+  float w0 = 1.f, w1 = 1.f;
+  if (fkR != 0.0) {
+    w0 = (float)window_w(fkR, k, wsmooth);
+    if (want_lap) w1 = (float)window_w(fkR, k, 3);
+  }
+  float* t = tab + (int64_t)f * 2 * qn;
+  t[q] = w0;
+  t[qn + q] = w1;
+}
+
 __global__ void window_kernel(const float2* __restrict__ dk, float2* __restrict__ out0,
-                              float2* __restrict__ out1, int n, double dkk, double Rf, int wsmooth,
-                              double post_scale) {
+                              float2* __restrict__ out1, int n, const float* __restrict__ tab, int qn,
+                              float ps) {
   const int nh = n / 2 + 1;
   const Mode md = mode_of(n, nh);
   if (!md.ok) return;
-  const double kx = dkk * (double)md.ix, ky = dkk * fftfreq(md.iy, n, 1.0), kz = dkk * fftfreq(md.iz, n, 1.0);
-  const double k = sqrt(kx * kx + ky * ky + kz * kz);
-  const double fkR = k * Rf;
+  const int nyq = n / 2;
+  const int fy = md.iy <= nyq ? md.iy : md.iy - n, fz = md.iz <= nyq ? md.iz : md.iz - n;
+  const int q = md.ix * md.ix + fy * fy + fz * fz;
   const float2 d = dk[md.id];
-  const float ps = (float)post_scale;
-  if (fkR == 0.0) {
-    out0[md.id] = make_float2(d.x * ps, d.y * ps);
-    if (out1) out1[md.id] = make_float2(d.x * ps, d.y * ps);
-    return;
-  }
-  const float w0 = (float)window_w(fkR, k, wsmooth);
+  const float w0 = __ldg(tab + q);
   out0[md.id] = make_float2(__fmul_rn(__fmul_rn(d.x, w0), ps), __fmul_rn(__fmul_rn(d.y, w0), ps));
   if (out1) {
-    const float w1 = (float)window_w(fkR, k, 3);
+    const float w1 = __ldg(tab + qn + q);
     out1[md.id] = make_float2(__fmul_rn(__fmul_rn(d.x, w1), ps), __fmul_rn(__fmul_rn(d.y, w1), ps));
   }
 }
@@ -377,6 +393,71 @@ __global__ void peakfind_kernel(const float* __restrict__ ds, const float* __res
   }
 }
 
+// Four consecutive cells along i per thread (one 16-byte load of the field
+// and one 4-byte load of the mask), for rows whose inner part starts on a
+// 4-cell boundary (n1 and nbuff multiples of 4).  Same test and append as
+// peakfind_kernel; the neighbours of a candidate are read one by one (few
+// cells reach fcrit).
+__global__ void peakfind4_kernel(const float* __restrict__ ds, const float* __restrict__ ls,
+                                 uint8_t* __restrict__ mask, int n1, int n2, int n3, int nbuff, float fcrit,
+                                 int fidx, PeakBuf pb) {
+  const int i0 = nbuff + 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = nbuff + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = nbuff + blockIdx.z;
+  const int64_t n12 = (int64_t)n1 * n2;
+  const int64_t lin0 = i0 + (int64_t)n1 * j + n12 * k;
+  bool pk[4] = {false, false, false, false};
+  float f[4] = {0.f, 0.f, 0.f, 0.f};
+  if (i0 < n1 - nbuff && j < n2 - nbuff && k < n3 - nbuff) {
+    const float4 v = *reinterpret_cast<const float4*>(ds + lin0);
+    const uchar4 m = *reinterpret_cast<const uchar4*>(mask + lin0);
+    f[0] = v.x; f[1] = v.y; f[2] = v.z; f[3] = v.w;
+    const uint8_t mm[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      if (i0 + u >= n1 - nbuff || mm[u] == 1 || f[u] < fcrit) continue;
+      const int64_t lin = lin0 + u;
+      bool peak = true;
+      for (int dk = -1; dk <= 1 && peak; dk++)
+        for (int dj = -1; dj <= 1; dj++)
+#pragma unroll
+          for (int di = -1; di <= 1; di++) {
+            const float w = __ldg(ds + lin + di + (int64_t)n1 * dj + n12 * dk);
+            if (f[u] < w) peak = false;
+          }
+      pk[u] = peak;
+    }
+  }
+  const unsigned full = 0xffffffffu;
+  const int cnt = (int)pk[0] + (int)pk[1] + (int)pk[2] + (int)pk[3];
+  if (__ballot_sync(full, cnt > 0) == 0) return;
+  const int wl = (threadIdx.x + blockDim.x * threadIdx.y) & 31;
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(full, incl, o);
+    if (wl >= o) incl += y;
+  }
+  const int total = __shfl_sync(full, incl, 31);
+  int base = 0;
+  if (wl == 31) base = atomicAdd(pb.count, total);
+  base = __shfl_sync(full, base, 31);
+  int slot = base + incl - cnt;
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    if (!pk[u]) continue;
+    const int64_t lin = lin0 + u;
+    mask[lin] = 1;
+    if (slot < pb.cap) {
+      pb.keys[slot] = ((unsigned long long)fidx << 40) | (unsigned long long)lin;
+      pb.vals[slot] = (uint32_t)slot;
+      pb.ff[slot] = f[u];
+      pb.lap[slot] = ls ? ls[lin] : 0.f;
+    }
+    slot++;
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -428,10 +509,19 @@ void launch_lapd(Launch L, const float2* dk, float2* out, int n, double boxsize,
   PPB_LAUNCHED(*L.count);
 }
 
-void launch_window(Launch L, const float2* dk, float2* out0, float2* out1, int n, double boxsize,
-                   double Rf, int wsmooth, double post_scale) {
-  window_kernel<<<mode_grid(n), 256, 0, L.s>>>(dk, out0, out1, n, 2.0 * kPi / boxsize, Rf, wsmooth,
-                                               post_scale);
+int window_table_size(int n) { return 3 * (n / 2) * (n / 2) + 1; }
+
+void launch_window_tables(Launch L, float* tab, int n, double boxsize, const double* Rf, int nfilt, int wsmooth,
+                          bool want_lap) {
+  const int qn = window_table_size(n);
+  window_table_kernel<<<dim3((unsigned)((qn + 255) / 256), (unsigned)nfilt), 256, 0, L.s>>>(
+      tab, qn, 2.0 * kPi / boxsize, Rf, wsmooth, want_lap ? 1 : 0);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_window(Launch L, const float2* dk, float2* out0, float2* out1, int n, const float* tab,
+                   double post_scale) {
+  window_kernel<<<mode_grid(n), 256, 0, L.s>>>(dk, out0, out1, n, tab, window_table_size(n), (float)post_scale);
   PPB_LAUNCHED(*L.count);
 }
 
@@ -453,8 +543,16 @@ void launch_peakfind(Launch L, const float* ds, const float* ls, uint8_t* mask, 
   const int w1 = n1 - 2 * nbuff, w2 = n2 - 2 * nbuff, w3 = n3 - 2 * nbuff;
   if (w1 <= 0 || w2 <= 0 || w3 <= 0) return;
   dim3 block(32, 4);
-  dim3 grid((w1 + 31) / 32, (w2 + 3) / 4, w3);
-  peakfind_kernel<<<grid, block, 0, L.s>>>(ds, ls, mask, n1, n2, n3, nbuff, fcrit, fidx, pb);
+  const bool vec = n1 % 4 == 0 && nbuff % 4 == 0 && reinterpret_cast<uintptr_t>(ds) % 16 == 0 &&
+                   reinterpret_cast<uintptr_t>(mask) % 4 == 0;
+  if (vec) {
+    const int q1 = (w1 + 3) / 4;
+    dim3 grid((q1 + 31) / 32, (w2 + 3) / 4, w3);
+    peakfind4_kernel<<<grid, block, 0, L.s>>>(ds, ls, mask, n1, n2, n3, nbuff, fcrit, fidx, pb);
+  } else {
+    dim3 grid((w1 + 31) / 32, (w2 + 3) / 4, w3);
+    peakfind_kernel<<<grid, block, 0, L.s>>>(ds, ls, mask, n1, n2, n3, nbuff, fcrit, fidx, pb);
+  }
   PPB_LAUNCHED(*L.count);
 }
 

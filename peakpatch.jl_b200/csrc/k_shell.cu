@@ -5,7 +5,7 @@
 // get_evals (:217-222) and the collapse-table lookup
 // (src/EllipsoidalCollapse/CollapseTable.jl:128-145).
 //
-// The stage runs as three kernels on one stream:
+// The stage runs as four kernels on one stream:
 //
 //  gather_kernel (persistent, one warp per peak, peaks taken from a queue in
 //    list order, i.e. largest filter radius first).  A host-built schedule
@@ -30,12 +30,16 @@
 //    moves the peak's rows from its staging slot to a pool.
 //
 //  collapse_kernel (one thread per peak).  kernel_strain windows, the inward
-//    collapse walk, RTHL, Sbar/Srb and zvir_half in double precision, in the
-//    reference's summation order.  The window weights hRinteg/(u12-u0^2)^2
-//    depend only on the radii and come from a host table.
+//    collapse walk, RTHL and Sbar/Srb in double precision, in the reference's
+//    summation order.  The window weights hRinteg/(u12-u0^2)^2 depend only on
+//    the radii and come from a host table.
+//
+//  zhalf_kernel (sixteen threads per collapsed peak, ten radii).  zvir_half.
 //
 //  d2f_kernel (one warp per collapsed peak).  Mean Laplacian over the cells
 //    within RTHL in list order, stopping at the first out-of-grid cell.
+#include <type_traits>
+
 #include "ppb_internal.h"
 
 namespace ppb {
@@ -54,24 +58,7 @@ enum { CNT_VISITS = 0, CNT_PREMASK = 1, CNT_NOFCRIT = 2, CNT_M0ONE = 3, CNT_NOCO
 // ---------------------------------------------------------------------------
 template <bool COMP> struct Acc;
 
-template <> struct Acc<true> {       // compensated single precision
-  float s[NACC], c[NACC];
-  __device__ __forceinline__ void zero() {
-#pragma unroll
-    for (int i = 0; i < NACC; i++) { s[i] = 0.f; c[i] = 0.f; }
-  }
-  __device__ __forceinline__ void add(int i, float x) {
-    // two-sum (Knuth): t + e == s + x exactly
-    const float t = __fadd_rn(s[i], x);
-    const float bp = __fsub_rn(t, s[i]);
-    const float e = __fadd_rn(__fsub_rn(s[i], __fsub_rn(t, bp)), __fsub_rn(x, bp));
-    s[i] = t;
-    c[i] = __fadd_rn(c[i], e);
-  }
-  __device__ __forceinline__ double get(int i) const { return (double)s[i] + (double)c[i]; }
-};
-
-template <> struct Acc<false> {      // double precision (the reference's Float64 sums)
+template <> struct Acc<false> {      // double precision (the reference's Float64 sums; plain path)
   double s[NACC];
   __device__ __forceinline__ void zero() {
 #pragma unroll
@@ -80,6 +67,88 @@ template <> struct Acc<false> {      // double precision (the reference's Float6
   __device__ __forceinline__ void add(int i, float x) { s[i] = __dadd_rn(s[i], (double)x); }
   __device__ __forceinline__ double get(int i) const { return s[i]; }
 };
+
+// Compensated single precision (optimised path).  The 22 addends of a cell
+// go to 11 packed FP32x2 accumulators plus one scalar, pairing values that
+// arrive in adjacent registers of the two 16-byte record loads, so that one
+// instruction serves two sums.  Each component keeps (s, c) with the
+// two-sum (Knuth) t = s + x, b' = t - s, e = (s - (t - b')) + (x - b'), so
+// that t + e == s + x exactly; c collects the e.  Component map:
+//   P0 = (delta, deltaT)  P1 = (psi_x, psi_y)  P2 = (psi_z, psi2_x)  P3 = (psi2_y, psi2_z)
+//   P4..P6 = (delta, deltaT) * d_i, d_j, d_k
+//   P7 = (psi_x d_i, psi_y d_j)  P8 = (psi_x d_j, psi_y d_i)
+//   P9 = (psi_x d_k, psi_y d_k)  P10 = (psi_z d_i, psi_z d_j)  scalar = psi_z d_k
+// (the deltaT sum of P0.y is not used).
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) {   // a - b, rounded once
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
+struct AccP {
+  float2 s[11], c[11];
+  float s1, c1;
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int i = 0; i < 11; i++) { s[i] = make_float2(0.f, 0.f); c[i] = make_float2(0.f, 0.f); }
+    s1 = 0.f;
+    c1 = 0.f;
+  }
+  __device__ __forceinline__ void add(int i, float2 x) {
+    const float2 t = __fadd2_rn(s[i], x);
+    const float2 bp = fsub2(t, s[i]);
+    const float2 e = __fadd2_rn(fsub2(s[i], fsub2(t, bp)), fsub2(x, bp));
+    s[i] = t;
+    c[i] = __fadd2_rn(c[i], e);
+  }
+  __device__ __forceinline__ void add1(float x) {
+    const float t = __fadd_rn(s1, x);
+    const float bp = __fsub_rn(t, s1);
+    const float e = __fadd_rn(__fsub_rn(s1, __fsub_rn(t, bp)), __fsub_rn(x, bp));
+    s1 = t;
+    c1 = __fadd_rn(c1, e);
+  }
+  __device__ __forceinline__ double X(int i) const { return (double)s[i].x + (double)c[i].x; }
+  __device__ __forceinline__ double Y(int i) const { return (double)s[i].y + (double)c[i].y; }
+  // the 19 sums in the order of accumulate_cell
+  __device__ __forceinline__ double get(int v) const {
+    switch (v) {
+      case 0: return X(0);
+      case 1: return X(1);
+      case 2: return Y(1);
+      case 3: return X(2);
+      case 4: return Y(2);
+      case 5: return X(3);
+      case 6: return Y(3);
+      case 7: return X(4);
+      case 8: return X(5);
+      case 9: return X(6);
+      case 10: return Y(4);
+      case 11: return Y(5);
+      case 12: return Y(6);
+      case 13: return X(7);
+      case 14: return Y(7);
+      case 15: return (double)s1 + (double)c1;
+      case 16: return X(8) + Y(8);
+      case 17: return X(9) + X(10);
+      default: return Y(9) + Y(10);
+    }
+  }
+};
+
+__device__ __forceinline__ void accumulate_cell_packed(AccP& A, const float4 a, const float4 b, float di, float dj,
+                                                       float dk) {
+  const float2 p0 = make_float2(a.x, a.y), p1 = make_float2(a.z, a.w);
+  A.add(0, p0);
+  A.add(1, p1);
+  A.add(2, make_float2(b.x, b.y));
+  A.add(3, make_float2(b.z, b.w));
+  A.add(4, __fmul2_rn(p0, make_float2(di, di)));
+  A.add(5, __fmul2_rn(p0, make_float2(dj, dj)));
+  A.add(6, __fmul2_rn(p0, make_float2(dk, dk)));
+  A.add(7, __fmul2_rn(p1, make_float2(di, dj)));
+  A.add(8, __fmul2_rn(p1, make_float2(dj, di)));
+  A.add(9, __fmul2_rn(p1, make_float2(dk, dk)));
+  A.add(10, __fmul2_rn(make_float2(b.x, b.x), make_float2(di, dj)));
+  A.add1(__fmul_rn(b.x, dk));
+}
 
 template <bool COMP>
 __device__ __forceinline__ void accumulate_cell(Acc<COMP>& A, const float4 a, const float4 b, float di,
@@ -191,6 +260,70 @@ __device__ __forceinline__ void unpack_cell(int w, int& di, int& dj, int& dk) {
   dk = (w << 8) >> 24;
 }
 
+// Build-time tuning of the gather (measured on B200 at 384^3: 4 cells per
+// step, no entry prefetch and a 128-register cap, i.e. 16 warps per SM, are
+// fastest; 2- and 8-cell steps, prefetching and other caps are slower).
+#ifndef PPB_GATHER_BATCH
+#define PPB_GATHER_BATCH 4
+#endif
+#ifndef PPB_GATHER_PREFETCH
+#define PPB_GATHER_PREFETCH 0
+#endif
+constexpr int GB = PPB_GATHER_BATCH;   // cells per lane per step
+// shared memory of one gather warp, in doubles: the chunk partials
+constexpr int GATHER_WARP_DOUBLES = (NACC + 1) * 32;
+
+// Sum one chunk (cells s0 .. s0+cnt-1 of the sorted list) into A, GB cells
+// per step: the 2 GB record loads of a step are issued together, and the
+// cell-table entries of the next step are loaded before the current step is
+// summed.  Returns the number of in-grid cells.
+template <class AccT, bool COMP>
+__device__ __forceinline__ int sum_chunk(const ShellArgs& a, int s0, int cnt, int64_t lin, bool inside, int pi,
+                                         int pj, int pk, AccT& A) {
+  const int n = a.n;
+  const float4* __restrict__ aos = a.aos;
+  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 cfn[GB];
+#pragma unroll
+  for (int u = 0; u < GB; u++) cfn[u] = u < cnt ? __ldg(a.cellf + s0 + u) : zero4;
+  int nsh = 0;
+  for (int c = 0; c < cnt; c += GB) {
+    float4 ra[GB], rb[GB], cf[GB];
+    bool ok[GB];
+#pragma unroll
+    for (int u = 0; u < GB; u++) {
+      cf[u] = cfn[u];
+      bool in = c + u < cnt;
+      if (!inside) {
+        const int iv1 = pi + (int)cf[u].x, iv2 = pj + (int)cf[u].y, iv3 = pk + (int)cf[u].z;
+        in = in && iv1 >= 0 && iv1 < n && iv2 >= 0 && iv2 < n && iv3 >= 0 && iv3 < n;
+      }
+      ok[u] = in;
+      // cells past the chunk or off the grid read the peak cell and are skipped
+      const int64_t li = lin + (ok[u] ? __float_as_int(cf[u].w) : 0);
+      ra[u] = __ldg(aos + 2 * li);
+      rb[u] = __ldg(aos + 2 * li + 1);
+    }
+    if (PPB_GATHER_PREFETCH) {
+#pragma unroll
+      for (int u = 0; u < GB; u++) cfn[u] = c + GB + u < cnt ? __ldg(a.cellf + s0 + c + GB + u) : zero4;
+    }
+#pragma unroll
+    for (int u = 0; u < GB; u++) {
+      if (ok[u]) {
+        nsh++;
+        if constexpr (COMP) accumulate_cell_packed(A, ra[u], rb[u], cf[u].x, cf[u].y, cf[u].z);
+        else accumulate_cell<false>(A, ra[u], rb[u], cf[u].x, cf[u].y, cf[u].z);
+      }
+    }
+    if (!PPB_GATHER_PREFETCH) {
+#pragma unroll
+      for (int u = 0; u < GB; u++) cfn[u] = c + GB + u < cnt ? __ldg(a.cellf + s0 + c + GB + u) : zero4;
+    }
+  }
+  return nsh;
+}
+
 template <bool COMP, bool ADAPTIVE>
 __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double* part) {
   const int lane = threadIdx.x & 31;
@@ -210,8 +343,8 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
   const double fcrit = a.pk.fcrit[p];
   const double* __restrict__ rad = a.rad;
   const int mmax = a.mmax;
-  const Geo geo = geometry(a, a.pk.Rf[p], a.pk.ir2min[p]);
-  const int m0_init = geo.m0_init;
+  const int4 gq = a.geo[p];
+  const int m0_init = gq.x, mrf = gq.y, mupp_rf = gq.w;
 
   // ---- the peak cell (shell 1) ------------------------------------------
   const float4* __restrict__ aos = a.aos;
@@ -244,36 +377,10 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
     const int c0g = __ldg(a.grp_c + g), ncg = __ldg(a.grp_c + g + 1) - c0g;
     // (a) lane l sums chunk c0g + l into the shared partial table
     if (lane < ncg) {
-      Acc<COMP> A;
+      typename std::conditional<COMP, AccP, Acc<false>>::type A;
       A.zero();
       const int s0 = __ldg(a.ck_s + c0g + lane), cnt = __ldg(a.ck_n + c0g + lane);
-      int nsh = 0;
-      for (int c = 0; c < cnt; c += 4) {
-        float4 ra[4], rb[4];
-        float fd[4][3];
-        bool ok[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const int w = (c + u < cnt) ? __ldg(a.cell8 + s0 + c + u) : 0;
-          int di, dj, dk;
-          unpack_cell(w, di, dj, dk);
-          const int iv1 = pi + di, iv2 = pj + dj, iv3 = pk + dk;
-          ok[u] = (c + u < cnt) &&
-                  (inside || (iv1 >= 0 && iv1 < n && iv2 >= 0 && iv2 < n && iv3 >= 0 && iv3 < n));
-          // out-of-range cells read the peak cell and contribute nothing
-          const int64_t li = ok[u] ? lin + di + (int64_t)n * dj + n2 * dk : lin;
-          ra[u] = __ldg(aos + 2 * li);
-          rb[u] = __ldg(aos + 2 * li + 1);
-          fd[u][0] = (float)di; fd[u][1] = (float)dj; fd[u][2] = (float)dk;
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          if (ok[u]) {
-            nsh++;
-            accumulate_cell<COMP>(A, ra[u], rb[u], fd[u][0], fd[u][1], fd[u][2]);
-          }
-        }
-      }
+      const int nsh = sum_chunk<decltype(A), COMP>(a, s0, cnt, lin, inside, pi, pj, pk, A);
       visits += nsh;
 #pragma unroll
       for (int v = 0; v < NACC; v++) part[v * 32 + lane] = A.get(v);
@@ -357,7 +464,7 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
     }
     mdone = gend;
     if (ADAPTIVE && mtarget < 0 && (state != 0 || mdone >= mmax)) {
-      int M = max(max(m0_init, geo.mrf), geo.mupp_rf);
+      int M = max(max(m0_init, mrf), mupp_rf);
       if (state == 2) M = max(M, mcross);
       mtarget = state == 0 ? mmax : __ldg(a.need + M);
     }
@@ -415,7 +522,19 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
     const double2* src = reinterpret_cast<const double2*>(stage + ROW);
     double2* dst = reinterpret_cast<double2*>(a.pool + (off + 1) * ROW);
     const int nv = mdone * (ROW / 2);
-    for (int i = lane; i < nv; i += 32) dst[i] = src[i];
+    for (int i0 = 0; i0 < nv; i0 += 128) {   // four loads in flight per lane
+      double2 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int i = i0 + 32 * u + lane;
+        if (i < nv) v[u] = src[i];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int i = i0 + 32 * u + lane;
+        if (i < nv) dst[i] = v[u];
+      }
+    }
   }
   if (lane == 0) {
     PeakHdr h;
@@ -425,20 +544,32 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
 }
 
 template <bool COMP, bool ADAPTIVE>
-__global__ void __launch_bounds__(32 * kGatherWarps) gather_kernel(ShellArgs a) {
-  __shared__ double part_all[kGatherWarps][(NACC + 1) * 32];
+#ifndef PPB_GATHER_MINB
+#define PPB_GATHER_MINB 4
+#endif
+__global__ void __launch_bounds__(32 * kGatherWarps, PPB_GATHER_MINB) gather_kernel(ShellArgs a) {
+  extern __shared__ double gsm[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int64_t slot = (int64_t)blockIdx.x * kGatherWarps + wib;
   double* stage = a.stage + slot * a.stage_stride;
+  double* part = gsm + (size_t)wib * GATHER_WARP_DOUBLES;
   while (true) {
     int p = 0;
     if (lane == 0) p = atomicAdd(a.queue, 1);
     p = __shfl_sync(FULL, p, 0);
     if (p >= a.npk) break;
-    gather_one<COMP, ADAPTIVE>(a, p, stage, part_all[wib]);
+    gather_one<COMP, ADAPTIVE>(a, p, stage, part);
     __syncwarp();
   }
+}
+
+// per-peak geometry (thread per peak)
+__global__ void geo_kernel(ShellArgs a) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.npk) return;
+  const Geo g = geometry(a, a.pk.Rf[p], a.pk.ir2min[p]);
+  a.geo[p] = make_int4(g.m0_init, g.mrf, g.mlow_rf, g.mupp_rf);
 }
 
 // ===========================================================================
@@ -594,8 +725,10 @@ __device__ void collapse_one(const ShellArgs& a, int64_t p) {
   const double ZZon = a.pk.ZZon[p];
   const double alatt = a.alatt;
   const int m = a.mmax;
-  const Geo geo = geometry(a, a.pk.Rf[p], a.pk.ir2min[p]);
-  const double hlatt = 1.0, anor = 1.0;
+  const int4 gq = a.geo[p];
+  Geo geo;
+  geo.m0_init = gq.x; geo.mrf = gq.y; geo.mlow_rf = gq.z; geo.mupp_rf = gq.w;
+  const double anor = 1.0;
   const double aRnor = 3.0 * anor / alatt, wnor = anor / (4.0 * 3.141592653589793), wRnor = 3.0 * wnor / alatt;
 
   // Phase 3: gradient at the filter scale
@@ -724,28 +857,8 @@ __device__ void collapse_one(const ShellArgs& a, int64_t p) {
   if (zvir1 > 0.0 && dZvir != 0.0) srb += 0.5 * (Fa + Fbarx) * (RTHL5 - rad5p);
   if (Fbarx * RTHL5 > 0.0) srb /= (Fbarx * RTHL5);
 
-  // zvir_half (RadialShell.jl:825-885): ten radii RTHL (e/18 + 1/2)^(1/3)
-  double zvir_half = -1.0;
-  if (RTHL / hlatt >= 3.0) {
-    for (int e = 0; e < 10; e++) {
-      const double rcur = RTHL * a.fhalf[e];
-      // first m1 in [2, m-1] with rad > rcur + 2 (the loop's break), else m-1
-      const int fu = first_gt(rad, 2, m - 1, rcur + 2.0 * hlatt);
-      const int mupp_rc = fu <= m - 1 ? fu : (m - 1 >= 2 ? m - 1 : 1);
-      int mlow_rc = 1;
-      const int fl = first_gt(rad, 1, m - 1, fmax(rcur - 2.0 * hlatt, 0.0));
-      if (fl <= m - 1) mlow_rc = fl;
-      const int f0 = first_gt(rad, 1, m - 1, rcur);
-      const int m0_rc = (f0 <= m - 1) ? f0 : max(m - 1, 1);
-      KS krc;
-      kernel_strain(a, R, m0_rc, mlow_rc, mupp_rc, wRnor, aRnor, &krc);
-      double Fr, ev, pv;
-      ev_pv(krc.E, &Fr, &ev, &pv);
-      zvir_half = fmax(zvir_half, zvir_of(a.tab, R.get(R_FBAR, m0_rc), ev, pv) - 1.0);
-    }
-  }
-
-  // results (layout in ppb.h); d2F (30) comes from d2f_kernel
+  // results (layout in ppb.h); zvir_half (26) comes from zhalf_kernel and
+  // d2F (30) from d2f_kernel
   double r[RES_N];
   r[0] = RTHL;
   r[1] = srb;
@@ -763,7 +876,7 @@ __device__ void collapse_one(const ShellArgs& a, int64_t p) {
   r[23] = Fbarx;
   r[24] = e_v_f;
   r[25] = p_v_f;
-  r[26] = zvir_half;
+  r[26] = -1.0;
   r[30] = 0.0;
 #pragma unroll
   for (int q = 0; q < RES_N; q++) out[q] = r[q];
@@ -772,6 +885,51 @@ __device__ void collapse_one(const ShellArgs& a, int64_t p) {
 __global__ void __launch_bounds__(128) collapse_kernel(ShellArgs a) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p < a.npk) collapse_one(a, p);
+}
+
+// ===========================================================================
+// zvir_half kernel (RadialShell.jl:825-885): for halos with RTHL >= 3 cells,
+// the largest zvir - 1 over ten radii RTHL ((e/9)/2 + 1/2)^(1/3), e = 0..9,
+// each from kernel_strain on [first shell beyond rcur - 2, first shell beyond
+// rcur + 2] around the first shell beyond rcur.  Sixteen threads per peak,
+// ten of them with a radius.
+// ===========================================================================
+__global__ void __launch_bounds__(128) zhalf_kernel(ShellArgs a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t p = t >> 4;
+  const int e = (int)(t & 15);
+  const double hlatt = 1.0;
+  double zl = -1.0;
+  bool act = false;
+  if (p < a.npk) {
+    const double RTHL = a.out[p * RES_N];
+    act = RTHL / hlatt >= 3.0;
+    if (act && e < 10) {
+      const PeakHdr h = a.hdr[p];
+      const Rows R{a.pool + h.off * ROW, h.mdone, a.counters};
+      const double* __restrict__ rad = a.rad;
+      const int m = a.mmax;
+      const double alatt = a.alatt, anor = 1.0;
+      const double aRnor = 3.0 * anor / alatt, wRnor = 3.0 * (anor / (4.0 * 3.141592653589793)) / alatt;
+      const double rcur = RTHL * a.fhalf[e];
+      // first m1 in [2, m-1] with rad > rcur + 2 (the loop's break), else m-1
+      const int fu = first_gt(rad, 2, m - 1, rcur + 2.0 * hlatt);
+      const int mupp_rc = fu <= m - 1 ? fu : (m - 1 >= 2 ? m - 1 : 1);
+      int mlow_rc = 1;
+      const int fl = first_gt(rad, 1, m - 1, fmax(rcur - 2.0 * hlatt, 0.0));
+      if (fl <= m - 1) mlow_rc = fl;
+      const int f0 = first_gt(rad, 1, m - 1, rcur);
+      const int m0_rc = (f0 <= m - 1) ? f0 : max(m - 1, 1);
+      KS krc;
+      kernel_strain(a, R, m0_rc, mlow_rc, mupp_rc, wRnor, aRnor, &krc);
+      double Fr, ev, pv;
+      ev_pv(krc.E, &Fr, &ev, &pv);
+      zl = zvir_of(a.tab, R.get(R_FBAR, m0_rc), ev, pv) - 1.0;
+    }
+  }
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) zl = fmax(zl, __shfl_xor_sync(FULL, zl, o));
+  if (act && e == 0) a.out[p * RES_N + 26] = fmax(zl, -1.0);
 }
 
 // ===========================================================================
@@ -822,20 +980,31 @@ __global__ void __launch_bounds__(128) d2f_kernel(ShellArgs a) {
 
 int64_t shell_stage_doubles_per_warp(int nshell) { return (int64_t)ROW * (nshell + 1); }
 
+constexpr size_t kGatherSmem = (size_t)kGatherWarps * GATHER_WARP_DOUBLES * sizeof(double);
+
 int shell_gather_blocks_per_sm(bool comp, bool adaptive) {
   const void* f = comp ? (adaptive ? (const void*)gather_kernel<true, true> : (const void*)gather_kernel<true, false>)
                        : (adaptive ? (const void*)gather_kernel<false, true> : (const void*)gather_kernel<false, false>);
+  PPB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem));
   int b = 0;
-  PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, 32 * kGatherWarps, 0));
+  PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, 32 * kGatherWarps, kGatherSmem));
   return b > 0 ? b : 1;
+}
+
+void launch_shell_geo(Launch L, const ShellArgs& a) {
+  const int64_t blocks = (a.npk + 127) / 128;
+  if (blocks == 0) return;
+  geo_kernel<<<(unsigned)blocks, 128, 0, L.s>>>(a);
+  PPB_LAUNCHED(*L.count);
 }
 
 void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks) {
   const dim3 grid(blocks), block(32 * kGatherWarps);
-  if (comp && adaptive) gather_kernel<true, true><<<grid, block, 0, L.s>>>(a);
-  else if (comp) gather_kernel<true, false><<<grid, block, 0, L.s>>>(a);
-  else if (adaptive) gather_kernel<false, true><<<grid, block, 0, L.s>>>(a);
-  else gather_kernel<false, false><<<grid, block, 0, L.s>>>(a);
+  const size_t sm = kGatherSmem;
+  if (comp && adaptive) gather_kernel<true, true><<<grid, block, sm, L.s>>>(a);
+  else if (comp) gather_kernel<true, false><<<grid, block, sm, L.s>>>(a);
+  else if (adaptive) gather_kernel<false, true><<<grid, block, sm, L.s>>>(a);
+  else gather_kernel<false, false><<<grid, block, sm, L.s>>>(a);
   PPB_LAUNCHED(*L.count);
 }
 
@@ -843,6 +1012,13 @@ void launch_shell_collapse(Launch L, const ShellArgs& a) {
   const int64_t blocks = (a.npk + 127) / 128;
   if (blocks == 0) return;
   collapse_kernel<<<(unsigned)blocks, 128, 0, L.s>>>(a);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_shell_zhalf(Launch L, const ShellArgs& a) {
+  const int64_t blocks = (a.npk * 16 + 127) / 128;
+  if (blocks == 0) return;
+  zhalf_kernel<<<(unsigned)blocks, 128, 0, L.s>>>(a);
   PPB_LAUNCHED(*L.count);
 }
 

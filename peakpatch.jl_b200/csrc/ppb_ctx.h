@@ -13,7 +13,7 @@ namespace ppb {
 struct TileRes {
   int n = 0;
   cufftHandle r2c = 0, c2r1 = 0, c2r2 = 0, c2r3 = 0, c2r6 = 0;
-  DevBuf delta, dk, psi, psi2, lapd, aos, kw, rw, mask, count;
+  DevBuf delta, dk, psi, psi2, lapd, aos, kw, rw, mask, count, wtab;
   // peaks
   int64_t cap = 0;
   DevBuf keys, vals, ff, lap, keys_s, vals_s, tmp;
@@ -28,7 +28,7 @@ struct ShellStats {
   unsigned long long dump[5] = {0, 0, 0, 0, 0};
   unsigned long long raw[16] = {};
   float ms = 0.f;                 // the whole stage
-  float kms[3] = {0.f, 0.f, 0.f}; // gather, collapse, d2f kernels
+  float kms[4] = {0.f, 0.f, 0.f, 0.f};   // gather, collapse, zvir_half, d2f kernels
   unsigned long long pool_rows = 0;   // profile rows written
   int batches = 0;
 };
@@ -54,8 +54,8 @@ struct ppb_ctx {
   ppb::DevTable dtab{};
   ppb::DevBuf akk;
   ppb::ShellTable shells;
-  ppb::DevBuf stage, counters, ctl, hdr, pool;
-  cudaEvent_t shell_ev[4] = {};
+  ppb::DevBuf stage, counters, ctl, hdr, geo, pool;
+  cudaEvent_t shell_ev[5] = {};
   int gather_bps[2][2] = {{0, 0}, {0, 0}};    // gather blocks per SM by [comp][adaptive]
   double rows_per_peak[2] = {0.0, 0.0};       // pool rows per peak seen last, by adaptive
   ppb::DevBuf filt_Rf, filt_ir2;

@@ -112,6 +112,10 @@ struct ShellTable {
   // cell offsets packed one per 32-bit word: bytes 0..2 = di, dj, dk as
   // signed 8-bit values (|d| <= nhunt <= 64)
   std::vector<int32_t> cell8;
+  // per grid size n: (di, dj, dk, linear offset di + n dj + n^2 dk as int
+  // bits) as one 16-byte load per cell for the gather
+  int cellf_n = -1;
+  DevBuf d_cellf;
   DevBuf d_cell8, d_start, d_count, d_r2m, d_rad, d_wlo, d_whi, d_woff, d_wts, d_w1, d_need, d_rad5;
   DevBuf d_grp_a, d_grp_b, d_grp_c, d_ck_s, d_ck_n, d_sh_c0, d_sh_nc;
 };
@@ -119,6 +123,7 @@ void build_shell_table(ShellTable& st, int nhunt);
 double hRinteg(double u0, double u12);
 std::vector<double> make_atab4();
 void upload_shell_table(ShellTable& st, cudaStream_t s);
+void upload_cellf(ShellTable& st, int n, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // linear-growth and chi->z tables (host, double precision)
@@ -195,6 +200,7 @@ struct ShellArgs {
   double alatt;
   // shell geometry
   const int32_t* cell8;     // packed cell offsets (ShellTable::cell8)
+  const float4* cellf;      // cell offsets for grid size n (ShellTable::d_cellf)
   const int32_t* sh_start;
   const int32_t* sh_count;
   const double* rad;        // rad[m], m = 0..nshell (index 0 unused); rad[1] = 0
@@ -217,6 +223,7 @@ struct ShellArgs {
   int64_t npk;
   double* out;              // npk x RES_N
   PeakHdr* hdr;             // npk
+  int4* geo;                // npk: (m0_init, mrf, mlow_rf, mupp_rf)
   double* pool;             // profile rows, pool_cap rows of ROW doubles
   int64_t pool_cap;
   unsigned long long* pool_ctr;   // rows handed out
@@ -243,8 +250,14 @@ void launch_phi(Launch L, const float2* dk, float2* out, int n, double boxsize, 
 void launch_src2(Launch L, const float* phi, float* out, int64_t N);
 void launch_lpt2(Launch L, const float2* s2k, float2* out, int n, double boxsize, double post_scale);
 void launch_lapd(Launch L, const float2* dk, float2* out, int n, double boxsize, float post_scale);
-void launch_window(Launch L, const float2* dk, float2* out0, float2* out1, int n, double boxsize,
-                   double Rf, int wsmooth, double post_scale);
+// window tables: per filter f, 2 * window_table_size(n) floats at
+// tab + f * 2 * window_table_size(n) (W_wsmooth, then the k^2-weighted
+// Gaussian of the Laplacian diagnostic); Rf is a device array of nfilt radii
+int window_table_size(int n);
+void launch_window_tables(Launch L, float* tab, int n, double boxsize, const double* Rf, int nfilt, int wsmooth,
+                          bool want_lap);
+void launch_window(Launch L, const float2* dk, float2* out0, float2* out1, int n, const float* tab,
+                   double post_scale);
 void launch_hermitise(Launch L, float2* data, int n, int nbatch);
 void launch_pack(Launch L, float4* aos, const float* delta, const float* psi, const float* psi2, int n);
 
@@ -259,17 +272,21 @@ struct PeakBuf {
 void launch_peakfind(Launch L, const float* ds, const float* ls, uint8_t* mask, int n1, int n2, int n3,
                      int nbuff, float fcrit, int fidx, PeakBuf pb);
 
-// Shell stage = three launches on one stream:
+// Shell stage = five launches on one stream:
+//  geo      (one thread per peak): per-peak shell geometry
 //  gather   (persistent, one warp per peak): profile rows + PeakHdr
-//  collapse (one thread per peak): results except d2F
+//  collapse (one thread per peak): results except zvir_half and d2F
+//  zhalf    (sixteen threads per peak): result 26
 //  d2f      (one warp per collapsed peak): result 30
 // comp: compensated single-precision gather sums (else double); adaptive:
 // radial truncation of the gather (else full spheres).
 constexpr int kGatherWarps = 4;   // warps per gather block
 int64_t shell_stage_doubles_per_warp(int nshell);
 int shell_gather_blocks_per_sm(bool comp, bool adaptive);
+void launch_shell_geo(Launch L, const ShellArgs& a);
 void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks);
 void launch_shell_collapse(Launch L, const ShellArgs& a);
+void launch_shell_zhalf(Launch L, const ShellArgs& a);
 void launch_shell_d2f(Launch L, const ShellArgs& a, int blocks);
 
 }  // namespace ppb

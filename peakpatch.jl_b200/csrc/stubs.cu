@@ -231,10 +231,10 @@ int32_t ppb_shell_counters(ppb_ctx* ctx, int64_t* out16) {
   return PPB_OK;
 }
 
-int32_t ppb_last_shell_times(ppb_ctx* ctx, float* ms3, int64_t* rows, int32_t* batches) {
+int32_t ppb_last_shell_times(ppb_ctx* ctx, float* ms4, int64_t* rows, int32_t* batches) {
   if (!ctx) return PPB_ERR_INVALID;
-  if (ms3)
-    for (int i = 0; i < 3; i++) ms3[i] = ctx->last_shell.kms[i];
+  if (ms4)
+    for (int i = 0; i < 4; i++) ms4[i] = ctx->last_shell.kms[i];
   if (rows) *rows = (int64_t)ctx->last_shell.pool_rows;
   if (batches) *batches = ctx->last_shell.batches;
   return PPB_OK;

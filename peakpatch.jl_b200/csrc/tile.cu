@@ -359,6 +359,9 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
   launch_hermitise(L, kw, n, 1);
   PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)kw, T.delta.as<cufftReal>()));
   PPB_CUFFT(cufftExecR2C(T.r2c, T.delta.as<cufftReal>(), (cufftComplex*)dkp));
+  // one Hermitian projection of delta_k: every filter output W(|k|) delta_k
+  // (and k^2 W delta_k) is then Hermitian as it stands
+  launch_hermitise(L, dkp, n, 1);
   // 1LPT
   launch_lpt1(L, dkp, kw, n, box, inv_n3);
   launch_hermitise(L, kw, n, 3);
@@ -400,6 +403,9 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
   PPB_CUDA(cudaEventRecord(ev[1], s));
 
   // ---- phase 2: filter bank and peaks ----
+  const int qn = window_table_size(n);
+  T.wtab.ensure((size_t)nfilt * 2 * qn * sizeof(float));
+  launch_window_tables(L, T.wtab.as<float>(), n, box, ctx->filt_Rf.as<double>(), nfilt, p->wsmooth, want_lap);
   int64_t npk = 0;
   for (int attempt = 0; attempt < 2; attempt++) {
     PPB_CUDA(cudaMemsetAsync(T.mask.p, 0, N, s));
@@ -408,8 +414,7 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
                T.count.as<int>(), T.cap};
     for (int f = 0; f < nfilt; f++) {
       float2* o1 = want_lap ? kw + M : nullptr;
-      launch_window(L, dkp, kw, o1, n, box, Rf[f], p->wsmooth, inv_n3);
-      launch_hermitise(L, kw, n, want_lap ? 2 : 1);
+      launch_window(L, dkp, kw, o1, n, T.wtab.as<float>() + (size_t)f * 2 * qn, inv_n3);
       if (want_lap && !plain) {
         PPB_CUFFT(cufftExecC2R(T.c2r2, (cufftComplex*)kw, rw));
       } else {

@@ -344,14 +344,14 @@ class Context:
         self._check(self.L.ppb_last_shell_stats(self.h, ctypes.byref(v), _p(d), ctypes.byref(ms)))
         raw = np.zeros(16, np.int64)
         self._check(self.L.ppb_shell_counters(self.h, _p(raw)))
-        kms = np.zeros(3, np.float32)
+        kms = np.zeros(4, np.float32)
         rows = ctypes.c_int64()
         nb = ctypes.c_int32()
         self._check(self.L.ppb_last_shell_times(self.h, _p(kms), ctypes.byref(rows), ctypes.byref(nb)))
         return {"visits": v.value, "dumps": dict(zip(("premask", "no_fcrit", "m0_one", "no_collapse", "rthl_neg"),
                                                       d.tolist())), "ms": ms.value, "guard": int(raw[6]),
                 "akk_overrun": int(raw[7]), "bad_peaks": int(raw[8]), "walk_steps": int(raw[9]),
-                "kernel_ms": dict(zip(("gather", "collapse", "d2f"), kms.tolist())),
+                "kernel_ms": dict(zip(("gather", "collapse", "zvir_half", "d2f"), kms.tolist())),
                 "pool_rows": rows.value, "batches": nb.value}
 
     def stage_ms(self):
