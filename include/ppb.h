@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PPB_ABI_VERSION 1
+#define PPB_ABI_VERSION 2
 
 enum {
   PPB_OK = 0,
@@ -62,10 +62,14 @@ typedef struct ppb_tile_params {
   double rmax2rs;
   uint64_t seed;
   /* path selection: 0 = optimised path (adaptive shell truncation,
-   * compensated FP32 shell sums, persistent launches), 1 = plain path
-   * (full spheres, FP64 shell sums, one block per peak) */
+   * compensated FP32 shell sums), 1 = plain path (full spheres, FP64 shell
+   * sums, unbatched transforms) */
   int32_t plain;
-  int32_t reserved[7];
+  int32_t reserved0;
+  /* P(k) multiplier for this tile (0 means 1): a sigma8 rescale of the
+   * resident table is pk_scale = (sigma8 / sigma8_table)^2 */
+  double pk_scale;
+  int32_t reserved[4];
 } ppb_tile_params;
 
 /* Halo output: caller-allocated record buffer.  On PPB_ERR_CAPACITY `count`
@@ -79,16 +83,19 @@ typedef struct ppb_halo_buf {
   int64_t npeaks;       /* out: peak candidates found over the filter bank */
 } ppb_halo_buf;
 
+/* Serving statistics (ppb_stats_get). */
 typedef struct ppb_stats {
-  int64_t tiles_done;
+  int64_t tiles_done;         /* requests finished (successfully or not) */
   int64_t peaks_done;
   int64_t halos_done;
-  double p50_ms, p99_ms;      /* request latency, arrival -> result */
-  double tiles_per_s;
-  uint64_t hbm_in_use;        /* bytes held by the context */
+  double p50_ms, p99_ms;      /* request latency, submit -> result ready */
+  double tiles_per_s;         /* tiles_done / (last completion - first submit) */
+  uint64_t hbm_in_use;        /* device bytes reserved by the serving slots */
   uint64_t hbm_budget;
-  int32_t in_flight;
-  int32_t queued;
+  int32_t in_flight;          /* requests running on a slot */
+  int32_t queued;             /* requests waiting for a slot or for memory */
+  int32_t slots;
+  int32_t failed;             /* requests that ended with an error */
 } ppb_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -183,6 +190,32 @@ int32_t ppb_alloc_host(ppb_ctx* ctx, size_t bytes, void** out);
 int32_t ppb_free_host(ppb_ctx* ctx, void* p);
 int32_t ppb_alloc_device(ppb_ctx* ctx, size_t bytes, void** out);
 int32_t ppb_free_device(ppb_ctx* ctx, void* p);
+
+/* ---- serving ------------------------------------------------------------ */
+/* A serving loop over the same tables (no reference counterpart: the
+ * reference runs one run_tile at a time).  Requests of any grid size, seed
+ * and cosmology are queued by ppb_submit and run on `slots` execution slots,
+ * each with its own CUDA stream and buffers, so that tiles of different
+ * requests overlap on the device.  A request is started as soon as a slot is
+ * idle and the HBM budget of the context admits its footprint (fields,
+ * transforms, peak and shell buffers of its grid size); a request that could
+ * never fit fails with PPB_ERR_ADMISSION.  The collapse and P(k) tables stay
+ * resident and are shared; ppb_set_* waits for the runs in flight.
+ * Results are the same as ppb_run_tile's for the same parameters.
+ *
+ * ppb_serve_config sets the number of slots (1..32, default 4) before the
+ * first submit.  ppb_submit copies params and Rf and returns a ticket.
+ * ppb_wait blocks up to timeout_ms (< 0: no limit) for the ticket's result and
+ * copies the records into `out` like ppb_run_tile (PPB_ERR_TIMEOUT leaves the
+ * request in place; PPB_ERR_CAPACITY reports the count needed and keeps the
+ * result for another wait).  A failed request returns its error code and
+ * message.  Each ticket is waited for once. */
+int32_t ppb_serve_config(ppb_ctx* ctx, int32_t slots);
+int32_t ppb_submit(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, int32_t nfilt, uint64_t* ticket);
+int32_t ppb_wait(ppb_ctx* ctx, uint64_t ticket, int32_t timeout_ms, ppb_halo_buf* out);
+int32_t ppb_stats_get(ppb_ctx* ctx, ppb_stats* out);
+/* Clears the latency record and counters of ppb_stats (not the queue). */
+int32_t ppb_stats_reset(ppb_ctx* ctx);
 
 /* ---- timing helpers ----------------------------------------------------- */
 /* Named CUDA events on the context stream (slot 0..15). */

@@ -40,57 +40,129 @@ const void* stage_in(DevBuf& buf, const void* src, size_t bytes, cudaStream_t s)
 }  // namespace ppb
 
 // ---------------------------------------------------------------------------
-// context methods
+// slots
 // ---------------------------------------------------------------------------
-const GrowthTable& ppb_ctx::growth(double Om, double OB, double OL, double h) {
-  if (!(gkey[0] == Om && gkey[1] == OB && gkey[2] == OL && gkey[3] == h)) {
-    gcache = make_growth_table(Om, OB, OL, h);
-    gkey[0] = Om; gkey[1] = OB; gkey[2] = OL; gkey[3] = h;
-    const size_t ng = gcache.a.size();
-    g_a.ensure(ng * 8);
-    g_D.ensure(ng * 8);
-    g_f.ensure(ng * 8);
-    PPB_CUDA(cudaMemcpyAsync(g_a.p, gcache.a.data(), ng * 8, cudaMemcpyHostToDevice, stream));
-    PPB_CUDA(cudaMemcpyAsync(g_D.p, gcache.D.data(), ng * 8, cudaMemcpyHostToDevice, stream));
-    PPB_CUDA(cudaMemcpyAsync(g_f.p, gcache.f.data(), ng * 8, cudaMemcpyHostToDevice, stream));
-    PPB_CUDA(cudaStreamSynchronize(stream));
-  }
-  return gcache;
+namespace ppb {
+
+void Slot::init(int dev) {
+  device = dev;
+  PPB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  for (auto& e : stage_ev) PPB_CUDA(cudaEventCreate(&e));
+  for (auto& e : shell_ev) PPB_CUDA(cudaEventCreate(&e));
 }
 
-DevCosmo ppb_ctx::dev_cosmo(const GrowthTable& G, double Om, double OL, double h, double zmax, bool need_chi) {
+void Slot::release_buffers() {
+  tile.reset();
+  for (DevBuf* b : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool})
+    b->release();
+}
+
+size_t Slot::bytes_held() const {
+  size_t b = tile ? tile->bytes() : 0;
+  for (const DevBuf* d : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool})
+    b += d->bytes;
+  return b;
+}
+
+TileRes& Slot::tile_for(int n) {
+  if (!tile || tile->n != n) {
+    tile.reset();   // one grid size resident per slot keeps the footprint bounded
+    tile = std::make_unique<TileRes>();
+  }
+  return *tile;
+}
+
+Slot::~Slot() {
+  if (stream) cudaStreamSynchronize(stream);
+  release_buffers();
+  for (auto& e : stage_ev) if (e) cudaEventDestroy(e);
+  for (auto& e : shell_ev) if (e) cudaEventDestroy(e);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+}  // namespace ppb
+
+// ---------------------------------------------------------------------------
+// context methods
+// ---------------------------------------------------------------------------
+void ppb_ctx::set_error(const std::string& m) {
+  std::lock_guard<std::mutex> lk(err_mu);
+  err = m;
+}
+
+
+
+const GrowthTable& ppb_ctx::growth(double Om, double OB, double OL, double h) {
+  std::lock_guard<std::mutex> lk(sh.cache_mu);
+  auto& e = sh.growth[{Om, OB, OL, h}];
+  if (!e) e = std::make_unique<GrowthTable>(make_growth_table(Om, OB, OL, h));
+  return *e;
+}
+
+const std::vector<double>& ppb_ctx::chi_table(double Om, double OL, double h, double zmax) {
+  std::lock_guard<std::mutex> lk(sh.cache_mu);
+  auto& e = sh.chi[{Om, OL, h, zmax}];
+  if (!e) e = std::make_unique<std::vector<double>>(make_chi_table(Om, OL, h, zmax, 2000));
+  return *e;
+}
+
+ShellTable& ppb_ctx::shell_table(int nhunt, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(sh.cache_mu);
+  auto& e = sh.shells[nhunt];
+  if (!e) {
+    auto t = std::make_unique<ShellTable>();
+    build_shell_table(*t, nhunt);
+    upload_shell_table(*t, s);
+    e = std::move(t);
+  }
+  return *e;
+}
+
+const float4* ppb_ctx::cellf(ShellTable& st, int n, cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(sh.cache_mu);
+  auto& e = st.cellf[n];
+  if (!e) {
+    std::vector<float4> f;
+    build_cellf(st, n, f);
+    auto b = std::make_unique<DevBuf>();
+    b->ensure(f.size() * sizeof(float4));
+    PPB_CUDA(cudaMemcpyAsync(b->p, f.data(), f.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
+    PPB_CUDA(cudaStreamSynchronize(s));
+    e = std::move(b);
+  }
+  return e->as<float4>();
+}
+
+// device copies of the run's growth (and chi) tables on the slot; the host
+// tables are cache entries that outlive the asynchronous copies
+DevCosmo ppb_ctx::dev_cosmo(Slot& sl, const GrowthTable& G, double Om, double OL, double h, double zmax,
+                            bool need_chi) {
+  const size_t ng = G.a.size();
+  sl.g_a.ensure(ng * 8);
+  sl.g_D.ensure(ng * 8);
+  sl.g_f.ensure(ng * 8);
+  PPB_CUDA(cudaMemcpyAsync(sl.g_a.p, G.a.data(), ng * 8, cudaMemcpyHostToDevice, sl.stream));
+  PPB_CUDA(cudaMemcpyAsync(sl.g_D.p, G.D.data(), ng * 8, cudaMemcpyHostToDevice, sl.stream));
+  PPB_CUDA(cudaMemcpyAsync(sl.g_f.p, G.f.data(), ng * 8, cudaMemcpyHostToDevice, sl.stream));
   DevCosmo C{};
-  C.ga = g_a.as<double>();
-  C.gD = g_D.as<double>();
-  C.gf = g_f.as<double>();
-  C.ng = (int)G.a.size();
+  C.ga = sl.g_a.as<double>();
+  C.gD = sl.g_D.as<double>();
+  C.gf = sl.g_f.as<double>();
+  C.ng = (int)ng;
   C.amin = G.amin; C.amax = G.amax; C.Dinf = G.Dinf; C.D0 = G.D0; C.Hinf = G.Hinf; C.H0 = G.H0;
   if (need_chi) {
-    if (!(chikey[0] == Om && chikey[1] == OL && chikey[2] == h && chikey[3] == zmax)) {
-      chicache = make_chi_table(Om, OL, h, zmax, 2000);
-      chikey[0] = Om; chikey[1] = OL; chikey[2] = h; chikey[3] = zmax;
-      chi.ensure(chicache.size() * 8);
-      PPB_CUDA(cudaMemcpyAsync(chi.p, chicache.data(), chicache.size() * 8, cudaMemcpyHostToDevice, stream));
-      PPB_CUDA(cudaStreamSynchronize(stream));
-    }
-    C.chis = chi.as<double>();
-    C.nchi = (int)chicache.size();
+    const std::vector<double>& chi = chi_table(Om, OL, h, zmax);
+    sl.chi.ensure(chi.size() * 8);
+    PPB_CUDA(cudaMemcpyAsync(sl.chi.p, chi.data(), chi.size() * 8, cudaMemcpyHostToDevice, sl.stream));
+    C.chis = sl.chi.as<double>();
+    C.nchi = (int)chi.size();
     C.chi_zmax = zmax;
   }
   return C;
 }
 
-TileRes& ppb_ctx::tile(int n) {
-  auto it = tiles.find(n);
-  if (it == tiles.end()) {
-    // one grid size resident at a time keeps the footprint bounded
-    tiles.clear();
-    it = tiles.emplace(n, std::make_unique<TileRes>()).first;
-  }
-  return *it->second;
-}
-
-ShellArgs ppb_ctx::shell_args(int n, double alatt, const float4* aos, const float* lapd) {
+ShellArgs ppb_ctx::shell_args(Slot& sl, ShellTable& shells, int n, double alatt, const float4* aos,
+                              const float* lapd) {
   ShellArgs a{};
   a.aos = aos;
   a.lapd = lapd;
@@ -98,8 +170,7 @@ ShellArgs ppb_ctx::shell_args(int n, double alatt, const float4* aos, const floa
   a.alatt = alatt;
   PPB_REQUIRE(n <= 4096, "grid size above 4096");
   a.cell8 = shells.d_cell8.as<int32_t>();
-  upload_cellf(shells, n, stream);
-  a.cellf = shells.d_cellf.as<float4>();
+  a.cellf = cellf(shells, n, sl.stream);
   a.sh_start = shells.d_start.as<int32_t>();
   a.sh_count = shells.d_count.as<int32_t>();
   a.rad = shells.d_rad.as<double>();
@@ -122,23 +193,24 @@ ShellArgs ppb_ctx::shell_args(int n, double alatt, const float4* aos, const floa
   a.nshell = shells.nshell;
   a.mmax = std::max(shells.nshell - 1, 1);
   a.npart = shells.ncells;
-  a.tab = dtab;
-  a.akk = akk.as<double>();
+  a.tab = sh.dtab;
+  a.akk = sh.akk.as<double>();
   return a;
 }
 
-void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st) {
-  Launch L{stream, &launches};
-  int& bps = gather_bps[comp][adaptive];
+void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, ShellStats* st) {
+  cudaStream_t stream = sl.stream;
+  Launch L{stream, &sl.launches};
+  int& bps = sl.gather_bps[comp][adaptive];
   if (bps == 0) bps = shell_gather_blocks_per_sm(comp, adaptive);
   const int gblocks = nsm * bps;
   const int64_t stride = shell_stage_doubles_per_warp(a.nshell);
-  stage.ensure((size_t)((int64_t)gblocks * kGatherWarps * stride * 8));
-  counters.ensure(16 * 8);
-  ctl.ensure(64);
-  hdr.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(PeakHdr));
-  geo.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(int4));
-  PPB_CUDA(cudaMemsetAsync(counters.p, 0, 16 * 8, stream));
+  sl.stage.ensure((size_t)((int64_t)gblocks * kGatherWarps * stride * 8));
+  sl.counters.ensure(16 * 8);
+  sl.ctl.ensure(64);
+  sl.hdr.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(PeakHdr));
+  sl.geo.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(int4));
+  PPB_CUDA(cudaMemsetAsync(sl.counters.p, 0, 16 * 8, stream));
   // profile pool: sized from the rows per peak of the previous call; peaks
   // run in batches that fit the pool budget, and a batch whose rows overflow
   // the pool runs again with a larger pool or fewer peaks
@@ -146,8 +218,8 @@ void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st)
   PPB_CUDA(cudaMemGetInfo(&fr, &tot));
   const size_t row_bytes = ROW * sizeof(double);
   const int64_t budget_rows = std::max<int64_t>(
-      1 << 16, (int64_t)(std::min<size_t>((size_t)32 << 30, (fr + pool.bytes) / 2) / row_bytes));
-  double& rpp = rows_per_peak[adaptive];
+      1 << 16, (int64_t)(std::min<size_t>((size_t)32 << 30, (fr + sl.pool.bytes) / 2) / row_bytes));
+  double& rpp = sl.rows_per_peak[adaptive];
   if (rpp <= 0.0) rpp = adaptive ? 64.0 : (double)(a.mmax + 1);
   ShellStats s{};
   unsigned long long before[16] = {}, c[16] = {};
@@ -156,7 +228,7 @@ void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st)
     const double want = std::max(1.0, rpp * 1.25);
     int64_t nb = std::min<int64_t>(a.npk - p0, std::max<int64_t>(1, (int64_t)((double)budget_rows / want)));
     const int64_t cap = std::min<int64_t>(budget_rows, (int64_t)((double)nb * want) + 4096);
-    pool.ensure((size_t)cap * row_bytes);
+    sl.pool.ensure((size_t)cap * row_bytes);
     ShellArgs b = a;
     b.pk.lin = a.pk.lin + p0;
     b.pk.Rf = a.pk.Rf + p0;
@@ -165,33 +237,33 @@ void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st)
     b.pk.fcrit = a.pk.fcrit + p0;
     b.npk = nb;
     b.out = a.out + p0 * RES_N;
-    b.hdr = hdr.as<PeakHdr>() + p0;
-    b.geo = geo.as<int4>() + p0;
-    b.pool = pool.as<double>();
+    b.hdr = sl.hdr.as<PeakHdr>() + p0;
+    b.geo = sl.geo.as<int4>() + p0;
+    b.pool = sl.pool.as<double>();
     b.pool_cap = cap;
-    b.pool_ctr = reinterpret_cast<unsigned long long*>(ctl.as<char>() + 8);
-    b.queue = ctl.as<int>();
-    b.stage = stage.as<double>();
+    b.pool_ctr = reinterpret_cast<unsigned long long*>(sl.ctl.as<char>() + 8);
+    b.queue = sl.ctl.as<int>();
+    b.stage = sl.stage.as<double>();
     b.stage_stride = stride;
-    b.counters = counters.as<unsigned long long>();
+    b.counters = sl.counters.as<unsigned long long>();
     for (int e = 0; e < 10; e++) b.fhalf[e] = std::pow(e / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
-    PPB_CUDA(cudaMemsetAsync(ctl.p, 0, 16, stream));
-    PPB_CUDA(cudaEventRecord(shell_ev[0], stream));
+    PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, 16, stream));
+    PPB_CUDA(cudaEventRecord(sl.shell_ev[0], stream));
     launch_shell_geo(L, b);
     launch_shell_gather(L, b, comp, adaptive, gblocks);
-    PPB_CUDA(cudaEventRecord(shell_ev[1], stream));
+    PPB_CUDA(cudaEventRecord(sl.shell_ev[1], stream));
     launch_shell_collapse(L, b);
-    PPB_CUDA(cudaEventRecord(shell_ev[2], stream));
+    PPB_CUDA(cudaEventRecord(sl.shell_ev[2], stream));
     launch_shell_zhalf(L, b);
-    PPB_CUDA(cudaEventRecord(shell_ev[3], stream));
+    PPB_CUDA(cudaEventRecord(sl.shell_ev[3], stream));
     launch_shell_d2f(L, b, nsm * 16);
-    PPB_CUDA(cudaEventRecord(shell_ev[4], stream));
+    PPB_CUDA(cudaEventRecord(sl.shell_ev[4], stream));
     unsigned long long used = 0;
     PPB_CUDA(cudaMemcpyAsync(&used, b.pool_ctr, sizeof(used), cudaMemcpyDeviceToHost, stream));
-    PPB_CUDA(cudaMemcpyAsync(c, counters.p, sizeof(c), cudaMemcpyDeviceToHost, stream));
+    PPB_CUDA(cudaMemcpyAsync(c, sl.counters.p, sizeof(c), cudaMemcpyDeviceToHost, stream));
     PPB_CUDA(cudaStreamSynchronize(stream));
     if ((int64_t)used > cap) {   // overflow: undo this batch's counts and run it again
-      PPB_CUDA(cudaMemcpyAsync(counters.p, before, sizeof(before), cudaMemcpyHostToDevice, stream));
+      PPB_CUDA(cudaMemcpyAsync(sl.counters.p, before, sizeof(before), cudaMemcpyHostToDevice, stream));
       PPB_CUDA(cudaStreamSynchronize(stream));
       const double seen = (double)used / (double)nb;
       PPB_REQUIRE(seen * 1.25 > rpp, "profile pool overflow without growth");
@@ -199,7 +271,7 @@ void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st)
       continue;
     }
     float k[4];
-    for (int e = 0; e < 4; e++) PPB_CUDA(cudaEventElapsedTime(&k[e], shell_ev[e], shell_ev[e + 1]));
+    for (int e = 0; e < 4; e++) PPB_CUDA(cudaEventElapsedTime(&k[e], sl.shell_ev[e], sl.shell_ev[e + 1]));
     for (int e = 0; e < 4; e++) s.kms[e] += k[e];
     s.ms += k[0] + k[1] + k[2] + k[3];
     s.pool_rows += used;
@@ -213,7 +285,7 @@ void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st)
   s.guard = c[6];
   s.akk = c[7];
   for (int i = 0; i < 16; i++) s.raw[i] = c[i];
-  last_shell = s;
+  sl.last_shell = s;
   if (st) *st = s;
 }
 
@@ -224,15 +296,15 @@ void ppb_ctx::run_shells(ShellArgs& a, bool comp, bool adaptive, ShellStats* st)
 #define PPB_GUARD_END(ctx)                                                    \
   }                                                                           \
   catch (const ppb::Error& e) {                                               \
-    if (ctx) (ctx)->err = e.msg;                                              \
+    if (ctx) (ctx)->set_error(e.msg);                                         \
     return e.code;                                                            \
   }                                                                           \
   catch (const std::exception& e) {                                           \
-    if (ctx) (ctx)->err = e.what();                                           \
+    if (ctx) (ctx)->set_error(e.what());                                      \
     return PPB_ERR_INVALID;                                                   \
   }                                                                           \
   catch (...) {                                                               \
-    if (ctx) (ctx)->err = "unknown error";                                    \
+    if (ctx) (ctx)->set_error("unknown error");                               \
     return PPB_ERR_INVALID;                                                   \
   }
 
@@ -252,16 +324,14 @@ int32_t ppb_ctx_create(int32_t device, uint64_t hbm_budget, ppb_ctx** out) {
     ctx = new ppb_ctx();
     ctx->device = device;
     PPB_CUDA(cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, device));
-    PPB_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->sync.init(device);
     for (auto& e : ctx->ev) PPB_CUDA(cudaEventCreate(&e));
-    for (auto& e : ctx->stage_ev) PPB_CUDA(cudaEventCreate(&e));
-    for (auto& e : ctx->shell_ev) PPB_CUDA(cudaEventCreate(&e));
     size_t fr = 0, tot = 0;
     PPB_CUDA(cudaMemGetInfo(&fr, &tot));
     ctx->hbm_budget = hbm_budget ? hbm_budget : (uint64_t)(0.9 * (double)fr);
     const std::vector<double> akk = make_atab4();
-    ctx->akk.ensure(akk.size() * 8);
-    PPB_CUDA(cudaMemcpy(ctx->akk.p, akk.data(), akk.size() * 8, cudaMemcpyHostToDevice));
+    ctx->sh.akk.ensure(akk.size() * 8);
+    PPB_CUDA(cudaMemcpy(ctx->sh.akk.p, akk.data(), akk.size() * 8, cudaMemcpyHostToDevice));
     *out = ctx;
     return PPB_OK;
   } catch (const ppb::Error& e) {
@@ -277,18 +347,14 @@ int32_t ppb_ctx_create(int32_t device, uint64_t hbm_budget, ppb_ctx** out) {
 int32_t ppb_ctx_destroy(ppb_ctx* ctx) {
   if (!ctx) return PPB_ERR_INVALID;
   cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
-  ctx->tiles.clear();
-  for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
-  for (auto& e : ctx->stage_ev) if (e) cudaEventDestroy(e);
-  for (auto& e : ctx->shell_ev) if (e) cudaEventDestroy(e);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  server_stop(ctx);
   delete ctx;
   return PPB_OK;
 }
 
 int32_t ppb_last_error(ppb_ctx* ctx, char* buf, size_t len) {
   if (!ctx || !buf || len == 0) return PPB_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->err_mu);
   std::snprintf(buf, len, "%s", ctx->err.c_str());
   return PPB_OK;
 }
@@ -298,15 +364,16 @@ int32_t ppb_set_collapse_table(ppb_ctx* ctx, const float* tab, int32_t nx, int32
   if (!ctx) return PPB_ERR_INVALID;
   std::lock_guard<std::recursive_mutex> lk(ctx->mu);
   PPB_GUARD_BEGIN
+  std::unique_lock<std::shared_mutex> wl(ctx->sh.mu);   // waits for runs in flight
   PPB_REQUIRE(tab != nullptr, "table is null");
   PPB_REQUIRE(nx >= 2 && ny >= 2 && nz >= 2, "table needs at least 2 nodes per axis");
   PPB_REQUIRE(x2 > x1 && y2 > y1 && z2 > z1, "table ranges must be increasing");
   PPB_CUDA(cudaSetDevice(ctx->device));
   const size_t bytes = (size_t)nx * ny * nz * 4;
-  ctx->tab.ensure(bytes);
-  PPB_CUDA(cudaMemcpy(ctx->tab.p, tab, bytes, cudaMemcpyDefault));
-  ctx->dtab = DevTable{ctx->tab.as<float>(), nx, ny, nz, x1, x2, y1, y2, z1, z2};
-  ctx->has_tab = true;
+  ctx->sh.tab.ensure(bytes);
+  PPB_CUDA(cudaMemcpy(ctx->sh.tab.p, tab, bytes, cudaMemcpyDefault));
+  ctx->sh.dtab = DevTable{ctx->sh.tab.as<float>(), nx, ny, nz, x1, x2, y1, y2, z1, z2};
+  ctx->sh.has_tab = true;
   return PPB_OK;
   PPB_GUARD_END(ctx)
 }
@@ -324,11 +391,12 @@ int32_t ppb_set_pk_table(ppb_ctx* ctx, const double* k, const double* pk, int32_
     lp[i] = std::log(pk[i]);
   }
   PPB_CUDA(cudaSetDevice(ctx->device));
-  ctx->pk_lk.ensure(n * 8);
-  ctx->pk_lp.ensure(n * 8);
-  PPB_CUDA(cudaMemcpy(ctx->pk_lk.p, lk.data(), n * 8, cudaMemcpyHostToDevice));
-  PPB_CUDA(cudaMemcpy(ctx->pk_lp.p, lp.data(), n * 8, cudaMemcpyHostToDevice));
-  ctx->pk_n = n;
+  std::unique_lock<std::shared_mutex> wl(ctx->sh.mu);   // waits for runs in flight
+  ctx->sh.pk_lk.ensure(n * 8);
+  ctx->sh.pk_lp.ensure(n * 8);
+  PPB_CUDA(cudaMemcpy(ctx->sh.pk_lk.p, lk.data(), n * 8, cudaMemcpyHostToDevice));
+  PPB_CUDA(cudaMemcpy(ctx->sh.pk_lp.p, lp.data(), n * 8, cudaMemcpyHostToDevice));
+  ctx->sh.pk_n = n;
   return PPB_OK;
   PPB_GUARD_END(ctx)
 }
@@ -343,7 +411,21 @@ int32_t ppb_run_tile_timed(ppb_ctx* ctx, const ppb_tile_params* p, const double*
   std::lock_guard<std::recursive_mutex> lk(ctx->mu);
   PPB_GUARD_BEGIN
   PPB_CUDA(cudaSetDevice(ctx->device));
-  return run_tile_impl(ctx, p, Rf, nfilt, out, device_ms);
+  PPB_REQUIRE(out != nullptr, "output buffer is null");
+  std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
+  TileOut o;
+  run_tile_core(ctx, ctx->sync, p, Rf, nfilt, &o);
+  out->nfields = o.nfields;
+  out->count = o.count;
+  out->npeaks = o.npeaks;
+  out->RTHLmax = o.RTHLmax;
+  if (device_ms) *device_ms = o.device_ms;
+  if (o.count > out->capacity) return PPB_ERR_CAPACITY;
+  if (o.count > 0) {
+    PPB_REQUIRE(out->records != nullptr, "records buffer is null");
+    copy_out(out->records, o.d_records, (size_t)o.count * o.nfields * 4, ctx->sync.stream);
+  }
+  return PPB_OK;
   PPB_GUARD_END(ctx)
 }
 
@@ -367,14 +449,15 @@ int32_t ppb_noise_threefry(ppb_ctx* ctx, float* out, int32_t n, uint64_t seed) {
   PPB_REQUIRE(out != nullptr && n >= 1 && n <= 4096, "bad noise arguments");
   PPB_CUDA(cudaSetDevice(ctx->device));
   const size_t bytes = (size_t)n * n * n * 4;
+  Slot& sl = ctx->sync;
   if (is_device_ptr(out)) {
-    launch_noise(Launch{ctx->stream, &ctx->launches}, out, n, seed);
-    PPB_CUDA(cudaStreamSynchronize(ctx->stream));
+    launch_noise(Launch{sl.stream, &sl.launches}, out, n, seed);
+    PPB_CUDA(cudaStreamSynchronize(sl.stream));
   } else {
     DevBuf tmp;
     tmp.ensure(bytes);
-    launch_noise(Launch{ctx->stream, &ctx->launches}, tmp.as<float>(), n, seed);
-    copy_out(out, tmp.p, bytes, ctx->stream);
+    launch_noise(Launch{sl.stream, &sl.launches}, tmp.as<float>(), n, seed);
+    copy_out(out, tmp.p, bytes, sl.stream);
   }
   return PPB_OK;
   PPB_GUARD_END(ctx)
@@ -418,7 +501,7 @@ int32_t ppb_free_device(ppb_ctx* ctx, void* p) {
 int32_t ppb_event_record(ppb_ctx* ctx, int32_t slot) {
   if (!ctx || slot < 0 || slot >= 14) return PPB_ERR_INVALID;
   PPB_GUARD_BEGIN
-  PPB_CUDA(cudaEventRecord(ctx->ev[slot], ctx->stream));
+  PPB_CUDA(cudaEventRecord(ctx->ev[slot], ctx->sync.stream));
   return PPB_OK;
   PPB_GUARD_END(ctx)
 }
@@ -435,20 +518,20 @@ int32_t ppb_event_elapsed(ppb_ctx* ctx, int32_t a, int32_t b, float* ms) {
 int32_t ppb_synchronize(ppb_ctx* ctx) {
   if (!ctx) return PPB_ERR_INVALID;
   PPB_GUARD_BEGIN
-  PPB_CUDA(cudaStreamSynchronize(ctx->stream));
+  PPB_CUDA(cudaStreamSynchronize(ctx->sync.stream));
   return PPB_OK;
   PPB_GUARD_END(ctx)
 }
 
 int32_t ppb_launch_count(ppb_ctx* ctx, int64_t* count) {
   if (!ctx || !count) return PPB_ERR_INVALID;
-  *count = ctx->launches;
+  *count = ctx->launches_total();
   return PPB_OK;
 }
 
 int32_t ppb_last_stage_ms(ppb_ctx* ctx, float* ms4) {
   if (!ctx || !ms4) return PPB_ERR_INVALID;
-  std::memcpy(ms4, ctx->stage_ms, sizeof(ctx->stage_ms));
+  std::memcpy(ms4, ctx->sync.stage_ms, sizeof(ctx->sync.stage_ms));
   return PPB_OK;
 }
 

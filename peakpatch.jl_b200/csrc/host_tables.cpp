@@ -131,23 +131,18 @@ void build_shell_table(ShellTable& st, int nhunt) {
   st.grp_c.push_back((int32_t)st.ck_s.size());
   st.nhunt = nhunt;
   st.d_cell8.release();   // force re-upload
-  st.cellf_n = -1;
+  st.cellf.clear();
 }
 
-void upload_cellf(ShellTable& st, int n, cudaStream_t s) {
-  if (st.cellf_n == n) return;
-  std::vector<float4> f(st.cells.size());
+void build_cellf(const ShellTable& st, int n, std::vector<float4>& out) {
+  out.resize(st.cells.size());
   for (size_t i = 0; i < st.cells.size(); i++) {
     const int4 c = st.cells[i];
     const int32_t off = c.x + n * (c.y + n * c.z);
     float w;
     std::memcpy(&w, &off, 4);
-    f[i] = make_float4((float)c.x, (float)c.y, (float)c.z, w);
+    out[i] = make_float4((float)c.x, (float)c.y, (float)c.z, w);
   }
-  st.d_cellf.ensure(f.size() * sizeof(float4));
-  PPB_CUDA(cudaMemcpyAsync(st.d_cellf.p, f.data(), f.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
-  PPB_CUDA(cudaStreamSynchronize(s));
-  st.cellf_n = n;
 }
 
 // hRinteg (src/HaloFinder/RadialShell.jl:100-127)

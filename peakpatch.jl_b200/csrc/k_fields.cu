@@ -91,7 +91,7 @@ __device__ double pk_eval(const double* __restrict__ lk, const double* __restric
 // noise_k *= sqrt(P(k) dk^3 n^3), DC := 0  (RandomField.jl:136-168)
 __global__ void convolve_kernel(float2* __restrict__ nk, int n, double dk, double mult,
                                 const double* __restrict__ lk, const double* __restrict__ lp, int np,
-                                double post_scale) {
+                                double pk_scale, double post_scale) {
   const int nh = n / 2 + 1;
   const Mode md = mode_of(n, nh);
   if (!md.ok) return;
@@ -102,7 +102,7 @@ __global__ void convolve_kernel(float2* __restrict__ nk, int n, double dk, doubl
     v = make_float2(0.f, 0.f);
   } else {
     const double nd = (double)n;
-    const double amp = sqrt(pk_eval(lk, lp, np, sqrt(k2)) * (dk * dk * dk) * (nd * nd * nd)) * post_scale;
+    const double amp = sqrt(pk_eval(lk, lp, np, sqrt(k2)) * pk_scale * (dk * dk * dk) * (nd * nd * nd)) * post_scale;
     v = make_float2((float)((double)v.x * amp), (float)((double)v.y * amp));
   }
   nk[md.id] = v;
@@ -473,10 +473,10 @@ void launch_noise(Launch L, float* out, int64_t n, uint64_t seed) {
 }
 
 void launch_convolve(Launch L, float2* nk, int n, double boxsize, const double* lk, const double* lp,
-                     int np, double post_scale) {
+                     int np, double pk_scale, double post_scale) {
   const double dk = 2.0 * kPi / boxsize;
   const double mult = (n * dk) / (double)n;
-  convolve_kernel<<<mode_grid(n), 256, 0, L.s>>>(nk, n, dk, mult, lk, lp, np, post_scale);
+  convolve_kernel<<<mode_grid(n), 256, 0, L.s>>>(nk, n, dk, mult, lk, lp, np, pk_scale, post_scale);
   PPB_LAUNCHED(*L.count);
 }
 

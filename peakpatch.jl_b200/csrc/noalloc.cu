@@ -204,27 +204,27 @@ extern "C" int32_t ppb_find_peaks_noalloc(ppb_ctx* ctx, const float* delta, int8
       }
       scratch = g_sym_addr[ctx->device];
     }
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = ctx->sync.stream;
     const Grid3 g{n1, n2, n3, nbuff, w1, w2, w3};
     // the total slot is the only value read before this call writes it
     PPB_CUDA(cudaMemsetAsync(scratch + 2 * kMaxBlocks, 0, sizeof(unsigned int), s));
     count_kernel<<<(unsigned)nblocks, kThreads, 0, s>>>(delta, mask, g, fcrit, ninner, scratch);
-    PPB_LAUNCHED(ctx->launches);
+    PPB_LAUNCHED(ctx->sync.launches);
     scan_kernel<<<1, kThreads, 0, s>>>(scratch, (int)nblocks);
-    PPB_LAUNCHED(ctx->launches);
+    PPB_LAUNCHED(ctx->sync.launches);
     write_kernel<<<(unsigned)nblocks, kThreads, 0, s>>>(delta, mask, g, fcrit, ninner, max_peaks, scratch, pi, pj,
                                                        pk, ipp, pdelta);
-    PPB_LAUNCHED(ctx->launches);
+    PPB_LAUNCHED(ctx->sync.launches);
     unsigned int total = 0;
     PPB_CUDA(cudaMemcpyAsync(&total, scratch + 2 * kMaxBlocks, sizeof(total), cudaMemcpyDeviceToHost, s));
     PPB_CUDA(cudaStreamSynchronize(s));
     *npeaks = (int64_t)total < max_peaks ? (int64_t)total : max_peaks;
     return PPB_OK;
   } catch (const ppb::Error& e) {
-    ctx->err = e.msg;
+    ctx->set_error(e.msg);
     return e.code;
   } catch (...) {
-    ctx->err = "unknown error";
+    ctx->set_error("unknown error");
     return PPB_ERR_INVALID;
   }
 }

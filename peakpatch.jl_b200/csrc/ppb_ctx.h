@@ -1,8 +1,12 @@
-// ppb_ctx.h — the library context (one per GPU) and per-grid-size resources.
+// ppb_ctx.h — the library context (one per GPU), its execution slots and the
+// resident tables the slots share.
 #pragma once
+#include <array>
+#include <atomic>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <shared_mutex>
 #include <string>
 
 #include "ppb_internal.h"
@@ -21,68 +25,118 @@ struct TileRes {
   ~TileRes();
   void setup(int n, cudaStream_t s);
   void ensure_peaks(int64_t c);
+  size_t bytes() const;
 };
 
 struct ShellStats {
   unsigned long long visits = 0, guard = 0, akk = 0;
   unsigned long long dump[5] = {0, 0, 0, 0, 0};
   unsigned long long raw[16] = {};
-  float ms = 0.f;                 // the whole stage
+  float ms = 0.f;                        // the whole stage
   float kms[4] = {0.f, 0.f, 0.f, 0.f};   // gather, collapse, zvir_half, d2f kernels
-  unsigned long long pool_rows = 0;   // profile rows written
+  unsigned long long pool_rows = 0;      // profile rows written
   int batches = 0;
 };
+
+// An execution slot: one CUDA stream and every buffer a tile run writes.
+// Runs on different slots overlap on the device; one slot runs one tile at a
+// time.
+struct Slot {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t launches = 0;
+  cudaEvent_t stage_ev[5] = {};
+  cudaEvent_t shell_ev[5] = {};
+  float stage_ms[4] = {0, 0, 0, 0};
+  std::unique_ptr<TileRes> tile;                    // one grid size at a time
+  DevBuf filt_Rf, filt_ir2;                         // filter bank of the run
+  DevBuf g_a, g_D, g_f, chi;                        // growth / chi tables of the run
+  DevBuf stage, counters, ctl, hdr, geo, pool;      // shell stage
+  int gather_bps[2][2] = {{0, 0}, {0, 0}};          // gather blocks per SM by [comp][adaptive]
+  double rows_per_peak[2] = {0.0, 0.0};             // pool rows per peak seen last, by adaptive
+  ShellStats last_shell{};
+  int64_t last_visits = 0, last_npk = 0;
+  void init(int device);
+  void release_buffers();
+  size_t bytes_held() const;
+  TileRes& tile_for(int n);
+  ~Slot();
+};
+
+// the record buffer of a finished run, still on the device
+struct TileOut {
+  const float* d_records = nullptr;
+  int64_t count = 0;
+  int32_t nfields = 0;
+  float RTHLmax = 0.f;
+  int64_t npeaks = 0;
+  float device_ms = 0.f;
+};
+
+// Resident tables shared by all slots.  `mu` is held shared by every run
+// and exclusively by the table uploads; `cache_mu` guards the lazily built
+// caches (entries are never removed while the context lives, so references
+// handed out stay valid).
+struct Shared {
+  std::shared_mutex mu;
+  DevBuf pk_lk, pk_lp;
+  int pk_n = 0;
+  DevBuf tab;
+  bool has_tab = false;
+  DevTable dtab{};
+  DevBuf akk;
+  std::mutex cache_mu;
+  std::map<int, std::unique_ptr<ShellTable>> shells;                           // by nhunt
+  std::map<std::array<double, 4>, std::unique_ptr<GrowthTable>> growth;        // by (Om, OB, OL, h)
+  std::map<std::array<double, 4>, std::unique_ptr<std::vector<double>>> chi;   // by (Om, OL, h, zmax)
+};
+
+struct Server;   // serve.cu
 
 }  // namespace ppb
 
 struct ppb_ctx {
   int device = 0;
   int nsm = 148;
-  cudaStream_t stream = nullptr;
-  std::recursive_mutex mu;
+  std::recursive_mutex mu;   // serialises the synchronous entry points
+  std::mutex err_mu;
   std::string err;
-  int64_t launches = 0;
-  cudaEvent_t ev[16] = {};
-  cudaEvent_t stage_ev[5] = {};
-  float stage_ms[4] = {0, 0, 0, 0};
   uint64_t hbm_budget = 0;
-  // resident tables
-  ppb::DevBuf pk_lk, pk_lp;
-  int pk_n = 0;
-  ppb::DevBuf tab;
-  bool has_tab = false;
-  ppb::DevTable dtab{};
-  ppb::DevBuf akk;
-  ppb::ShellTable shells;
-  ppb::DevBuf stage, counters, ctl, hdr, geo, pool;
-  cudaEvent_t shell_ev[5] = {};
-  int gather_bps[2][2] = {{0, 0}, {0, 0}};    // gather blocks per SM by [comp][adaptive]
-  double rows_per_peak[2] = {0.0, 0.0};       // pool rows per peak seen last, by adaptive
-  ppb::DevBuf filt_Rf, filt_ir2;
-  ppb::DevBuf g_a, g_D, g_f, chi;
-  // growth-table cache
-  double gkey[4] = {-1, -1, -1, -1};
-  ppb::GrowthTable gcache;
-  double chikey[4] = {-1, -1, -1, -1};
-  std::vector<double> chicache;
-  std::map<int, std::unique_ptr<ppb::TileRes>> tiles;
-  int64_t last_visits = 0, last_npk = 0;
-  ppb::ShellStats last_shell{};
+  cudaEvent_t ev[16] = {};   // user events on the synchronous slot's stream
+  ppb::Shared sh;
+  ppb::Slot sync;            // the slot of the synchronous entry points
+  std::unique_ptr<ppb::Server> server;
+  int serve_slots = 4;
 
+  void set_error(const std::string& m);
   const ppb::GrowthTable& growth(double Om, double OB, double OL, double h);
-  ppb::DevCosmo dev_cosmo(const ppb::GrowthTable& G, double Om, double OL, double h, double zmax, bool need_chi);
-  ppb::TileRes& tile(int n);
-  ppb::ShellArgs shell_args(int n, double alatt, const float4* aos, const float* lapd);
-  void run_shells(ppb::ShellArgs& a, bool comp, bool adaptive, ppb::ShellStats* st);
+  const std::vector<double>& chi_table(double Om, double OL, double h, double zmax);
+  ppb::ShellTable& shell_table(int nhunt, cudaStream_t s);
+  const float4* cellf(ppb::ShellTable& st, int n, cudaStream_t s);
+  ppb::DevCosmo dev_cosmo(ppb::Slot& sl, const ppb::GrowthTable& G, double Om, double OL, double h, double zmax,
+                          bool need_chi);
+  ppb::ShellArgs shell_args(ppb::Slot& sl, ppb::ShellTable& st, int n, double alatt, const float4* aos,
+                            const float* lapd);
+  void run_shells(ppb::Slot& sl, ppb::ShellArgs& a, bool comp, bool adaptive, ppb::ShellStats* st);
+  int64_t launches_total() const;
+  ppb_ctx();
+  ~ppb_ctx();
 };
 
 namespace ppb {
-int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, int nfilt, ppb_halo_buf* out,
-                  float* device_ms);
+// run_tile (src/Pipeline.jl:66-325) on one slot; the records stay on the
+// device (o->d_records) until the slot's next run.  The caller holds
+// ctx->sh.mu shared.
+void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf, int nfilt, TileOut* o);
+void check_params(const ppb_tile_params* p, const double* Rf, int nfilt);
+// device bytes a run of this grid size holds at most (admission estimate)
+uint64_t tile_footprint(const ppb_tile_params* p);
 // copy `bytes` from device memory to dst (host or device)
 void copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);
 // true when p points to device memory
 bool is_device_ptr(const void* p);
 // device copy of a caller buffer (host or device); returns a device pointer
 const void* stage_in(DevBuf& buf, const void* src, size_t bytes, cudaStream_t s);
+// serving (serve.cu)
+void server_stop(ppb_ctx* ctx);
 }  // namespace ppb

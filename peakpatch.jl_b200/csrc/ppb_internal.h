@@ -114,8 +114,7 @@ struct ShellTable {
   std::vector<int32_t> cell8;
   // per grid size n: (di, dj, dk, linear offset di + n dj + n^2 dk as int
   // bits) as one 16-byte load per cell for the gather
-  int cellf_n = -1;
-  DevBuf d_cellf;
+  std::map<int, std::unique_ptr<DevBuf>> cellf;
   DevBuf d_cell8, d_start, d_count, d_r2m, d_rad, d_wlo, d_whi, d_woff, d_wts, d_w1, d_need, d_rad5;
   DevBuf d_grp_a, d_grp_b, d_grp_c, d_ck_s, d_ck_n, d_sh_c0, d_sh_nc;
 };
@@ -123,7 +122,7 @@ void build_shell_table(ShellTable& st, int nhunt);
 double hRinteg(double u0, double u12);
 std::vector<double> make_atab4();
 void upload_shell_table(ShellTable& st, cudaStream_t s);
-void upload_cellf(ShellTable& st, int n, cudaStream_t s);
+void build_cellf(const ShellTable& st, int n, std::vector<float4>& out);
 
 // ---------------------------------------------------------------------------
 // linear-growth and chi->z tables (host, double precision)
@@ -243,8 +242,9 @@ struct Launch {
 };
 
 void launch_noise(Launch L, float* out, int64_t n, uint64_t seed);
+// pk_scale multiplies P(k) (a sigma8 rescale is pk_scale = (sigma8 / sigma8_table)^2)
 void launch_convolve(Launch L, float2* nk, int n, double boxsize, const double* lk, const double* lp,
-                     int np, double post_scale);
+                     int np, double pk_scale, double post_scale);
 void launch_lpt1(Launch L, const float2* dk, float2* out, int n, double boxsize, double post_scale);
 void launch_phi(Launch L, const float2* dk, float2* out, int n, double boxsize, double post_scale);
 void launch_src2(Launch L, const float* phi, float* out, int64_t N);

@@ -51,7 +51,7 @@ int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n
     PPB_REQUIRE(n1 >= 3 && n2 >= 3 && n3 >= 3 && nbuff >= 1, "grid must be >= 3 cells with nbuff >= 1");
     PPB_REQUIRE(max_peaks >= 0, "max_peaks must be >= 0");
     PPB_CUDA(cudaSetDevice(ctx->device));
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = ctx->sync.stream;
     const int64_t N = (int64_t)n1 * n2 * n3;
     PPB_REQUIRE(N < (1ll << 40), "grid too large");
     DevBuf d_delta, d_mask, keys, vals, ff, cnt, keys_s, vals_s, tmp, o_i, o_j, o_k, o_ipp, o_d;
@@ -83,7 +83,7 @@ int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n
     DevBuf lapdummy;
     lapdummy.ensure(cap * 4);
     pb.lap = lapdummy.as<float>();
-    launch_peakfind(Launch{s, &ctx->launches}, dd, nullptr, dm, n1, n2, n3, nbuff, fcrit, 0, pb);
+    launch_peakfind(Launch{s, &ctx->sync.launches}, dd, nullptr, dm, n1, n2, n3, nbuff, fcrit, 0, pb);
     int c = 0;
     PPB_CUDA(cudaMemcpyAsync(&c, cnt.p, 4, cudaMemcpyDeviceToHost, s));
     PPB_CUDA(cudaStreamSynchronize(s));
@@ -97,13 +97,13 @@ int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n
       tmp.ensure(tb + 16);
       PPB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, keys.as<unsigned long long>(), keys_s.as<unsigned long long>(),
                                                vals.as<uint32_t>(), vals_s.as<uint32_t>(), (int)np, 0, 40, s));
-      ctx->launches++;
+      ctx->sync.launches++;
       // the reference stops scanning after max_peaks (PeakFind.jl:178-180):
       // later cells are neither reported nor masked
       if (np > max_peaks) {
         const int from = (int)max_peaks, to = (int)np;
         unmask_kernel<<<(to - from + 255) / 256, 256, 0, s>>>(keys_s.as<unsigned long long>(), from, to, dm);
-        PPB_LAUNCHED(ctx->launches);
+        PPB_LAUNCHED(ctx->sync.launches);
         np = max_peaks;
       }
       if (np > 0) {
@@ -111,7 +111,7 @@ int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n
         peaks_out_kernel<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(
             keys_s.as<unsigned long long>(), vals_s.as<uint32_t>(), ff.as<float>(), (int)np, n1, n2,
             o_i.as<int64_t>(), o_j.as<int64_t>(), o_k.as<int64_t>(), o_ipp.as<int64_t>(), o_d.as<float>());
-        PPB_LAUNCHED(ctx->launches);
+        PPB_LAUNCHED(ctx->sync.launches);
         copy_out(pi, o_i.p, np * 8, s);
         copy_out(pj, o_j.p, np * 8, s);
         copy_out(pk, o_k.p, np * 8, s);
@@ -124,10 +124,10 @@ int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n
     *npeaks = np;
     return PPB_OK;
   } catch (const ppb::Error& e) {
-    ctx->err = e.msg;
+    ctx->set_error(e.msg);
     return e.code;
   } catch (...) {
-    ctx->err = "unknown error";
+    ctx->set_error("unknown error");
     return PPB_ERR_INVALID;
   }
 }
@@ -146,14 +146,14 @@ int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, c
     PPB_REQUIRE(n >= 2 && n <= 4096, "n out of range");
     PPB_REQUIRE(npk >= 0 && npk < (1ll << 31), "npk out of range");
     PPB_REQUIRE(alatt > 0, "alatt must be positive");
-    PPB_REQUIRE(ctx->has_tab, "collapse table not set (ppb_set_collapse_table)");
+    PPB_REQUIRE(ctx->sh.has_tab, "collapse table not set (ppb_set_collapse_table)");
     PPB_CUDA(cudaSetDevice(ctx->device));
     if (npk == 0) return PPB_OK;
-    cudaStream_t s = ctx->stream;
-    Launch L{s, &ctx->launches};
+    cudaStream_t s = ctx->sync.stream;
+    Launch L{s, &ctx->sync.launches};
     const int64_t N = (int64_t)n * n * n;
-    build_shell_table(ctx->shells, nhunt);
-    upload_shell_table(ctx->shells, s);
+    std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
+    ShellTable& shells = ctx->shell_table(nhunt, s);
     // fields -> contiguous device staging -> packed gather records
     DevBuf st_delta, st_psi, st_psi2, st_lapd, aos, d_ipp, d_lin, d_Rf, d_ir2in, d_ir2, d_Z, d_fc, d_out;
     st_psi.ensure(3 * N * 4);
@@ -183,8 +183,8 @@ int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, c
     d_lin.ensure(npk * 8);
     d_ir2.ensure(npk * 4);
     ipp_to_lin<<<(unsigned)((npk + 255) / 256), 256, 0, s>>>(dipp, d_lin.as<int64_t>(), dir2, d_ir2.as<int32_t>(), npk);
-    PPB_LAUNCHED(ctx->launches);
-    ShellArgs a = ctx->shell_args(n, alatt, aos.as<float4>(), dl);
+    PPB_LAUNCHED(ctx->sync.launches);
+    ShellArgs a = ctx->shell_args(ctx->sync, shells, n, alatt, aos.as<float4>(), dl);
     a.pk = PeakParams{d_lin.as<int64_t>(), dRf, d_ir2.as<int32_t>(), dZ, dfc};
     a.npk = npk;
     double* dout = out;
@@ -194,9 +194,9 @@ int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, c
     }
     a.out = dout;
     ShellStats stt{};
-    ctx->run_shells(a, plain == 0, plain == 0, &stt);
-    ctx->last_visits = stt.visits;
-    ctx->last_npk = npk;
+    ctx->run_shells(ctx->sync, a, plain == 0, plain == 0, &stt);
+    ctx->sync.last_visits = stt.visits;
+    ctx->sync.last_npk = npk;
     if (stt.guard != 0)
       throw Error{PPB_ERR_CUDA, "shell truncation guard tripped: a profile read beyond the gathered shells"};
     if (stt.akk != 0)
@@ -205,10 +205,10 @@ int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, c
     PPB_CUDA(cudaStreamSynchronize(s));
     return PPB_OK;
   } catch (const ppb::Error& e) {
-    ctx->err = e.msg;
+    ctx->set_error(e.msg);
     return e.code;
   } catch (...) {
-    ctx->err = "unknown error";
+    ctx->set_error("unknown error");
     return PPB_ERR_INVALID;
   }
 }
@@ -218,25 +218,25 @@ int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, c
 // no_collapse, rthl_neg), plus the kernel's device time in ms.
 int32_t ppb_last_shell_stats(ppb_ctx* ctx, int64_t* visits, int64_t* dumps5, float* ms) {
   if (!ctx) return PPB_ERR_INVALID;
-  if (visits) *visits = (int64_t)ctx->last_shell.visits;
+  if (visits) *visits = (int64_t)ctx->sync.last_shell.visits;
   if (dumps5)
-    for (int i = 0; i < 5; i++) dumps5[i] = (int64_t)ctx->last_shell.dump[i];
-  if (ms) *ms = ctx->last_shell.ms;
+    for (int i = 0; i < 5; i++) dumps5[i] = (int64_t)ctx->sync.last_shell.dump[i];
+  if (ms) *ms = ctx->sync.last_shell.ms;
   return PPB_OK;
 }
 
 int32_t ppb_shell_counters(ppb_ctx* ctx, int64_t* out16) {
   if (!ctx || !out16) return PPB_ERR_INVALID;
-  for (int i = 0; i < 16; i++) out16[i] = (int64_t)ctx->last_shell.raw[i];
+  for (int i = 0; i < 16; i++) out16[i] = (int64_t)ctx->sync.last_shell.raw[i];
   return PPB_OK;
 }
 
 int32_t ppb_last_shell_times(ppb_ctx* ctx, float* ms4, int64_t* rows, int32_t* batches) {
   if (!ctx) return PPB_ERR_INVALID;
   if (ms4)
-    for (int i = 0; i < 4; i++) ms4[i] = ctx->last_shell.kms[i];
-  if (rows) *rows = (int64_t)ctx->last_shell.pool_rows;
-  if (batches) *batches = ctx->last_shell.batches;
+    for (int i = 0; i < 4; i++) ms4[i] = ctx->sync.last_shell.kms[i];
+  if (rows) *rows = (int64_t)ctx->sync.last_shell.pool_rows;
+  if (batches) *batches = ctx->sync.last_shell.batches;
   return PPB_OK;
 }
 

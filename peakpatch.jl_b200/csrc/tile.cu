@@ -207,15 +207,6 @@ __global__ void record_kernel(RecArgs a) {
   }
 }
 
-__global__ void zero_counters(unsigned long long* c, int nc, int* q, int* pcount) {
-  const int t = threadIdx.x;
-  if (t < nc) c[t] = 0;
-  if (t == 0) {
-    if (q) *q = 0;
-    if (pcount) *pcount = 0;
-  }
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -257,6 +248,15 @@ void TileRes::setup(int nn, cudaStream_t s) {
   count.ensure(64);
 }
 
+size_t TileRes::bytes() const {
+  size_t b = 0;
+  for (const DevBuf* d : {&delta, &dk, &psi, &psi2, &lapd, &aos, &kw, &rw, &mask, &count, &wtab, &keys, &vals, &ff,
+                          &lap, &keys_s, &vals_s, &tmp, &p_lin, &p_Rf, &p_ir2, &p_Z, &p_fc, &p_FcRf, &p_d2Rf,
+                          &p_pos, &res, &flags, &offs, &rec, &rthl})
+    b += d->bytes;
+  return b;
+}
+
 void TileRes::ensure_peaks(int64_t c) {
   if (c <= cap) return;
   cap = c;
@@ -291,7 +291,7 @@ void TileRes::ensure_peaks(int64_t c) {
 // ---------------------------------------------------------------------------
 // the pipeline
 // ---------------------------------------------------------------------------
-static void check_params(const ppb_tile_params* p, const double* Rf, int nfilt) {
+void check_params(const ppb_tile_params* p, const double* Rf, int nfilt) {
   PPB_REQUIRE(p != nullptr, "params is null");
   PPB_REQUIRE(p->n >= 8 && p->n <= 2048, "n must be in [8, 2048]");
   PPB_REQUIRE(p->boxsize > 0, "boxsize must be positive");
@@ -301,20 +301,27 @@ static void check_params(const ppb_tile_params* p, const double* Rf, int nfilt) 
   PPB_REQUIRE(p->ilpt == 1 || p->ilpt == 2, "ilpt must be 1 or 2");
   PPB_REQUIRE(p->wsmooth == 0 || p->wsmooth == 1 || p->wsmooth == 3, "wsmooth must be 0, 1 or 3");
   PPB_REQUIRE(p->ievol == 0 || p->ievol == 1, "ievol must be 0 or 1");
+  PPB_REQUIRE(p->pk_scale >= 0.0, "pk_scale must be >= 0 (0 means 1)");
   if (p->rmax2rs != 0.0)
     throw Error{PPB_ERR_UNSUPPORTED,
                 "rmax2rs > 0 is not supported: the reference's result then depends on thread scheduling "
                 "(mask writes of RadialShell.jl:793-802 race with the pre-mask read at :311-316)"};
 }
 
-int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, int nfilt, ppb_halo_buf* out,
-                  float* device_ms) {
+uint64_t tile_footprint(const ppb_tile_params* p) {
+  const uint64_t n = (uint64_t)p->n, N = n * n * n, M = (n / 2 + 1) * n * n;
+  // TileRes fields: delta, psi (3), psi2 (3), lapd, rw (6), mask, aos (8 floats), dk + kw (7 complex)
+  const uint64_t fields = N * 4 * (1 + 3 + 3 + 1 + 6) + N + N * 32 + M * 8 * 7;
+  // peaks, results, records and the shell-stage pool: about 120 bytes per cell
+  return fields + N * 120 + ((uint64_t)64 << 20);
+}
+
+void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf_in, int nfilt, TileOut* o) {
   check_params(p, Rf_in, nfilt);
-  PPB_REQUIRE(ctx->pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
-  PPB_REQUIRE(ctx->has_tab, "collapse table not set (ppb_set_collapse_table)");
-  PPB_REQUIRE(out != nullptr, "output buffer is null");
-  cudaStream_t s = ctx->stream;
-  Launch L{s, &ctx->launches};
+  PPB_REQUIRE(ctx->sh.pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
+  PPB_REQUIRE(ctx->sh.has_tab, "collapse table not set (ppb_set_collapse_table)");
+  cudaStream_t s = sl.stream;
+  Launch L{s, &sl.launches};
   const int n = p->n;
   const double box = p->boxsize, alatt = box / n;
   const double Om = p->Omx + p->OmB;
@@ -329,23 +336,22 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
   const float fcrit = (float)fcrit_val;
   const int nhunt = std::min(p->nbuff - 1, (int)std::floor(Rf[0] * 1.75 / alatt));
   PPB_REQUIRE(nhunt >= 1, "nhunt = min(nbuff-1, floor(1.75 Rfmax/alatt)) must be >= 1");
-  build_shell_table(ctx->shells, nhunt);
-  upload_shell_table(ctx->shells, s);
+  ShellTable& shells = ctx->shell_table(nhunt, s);
   std::vector<int32_t> fir2(nfilt);
   for (int f = 0; f < nfilt; f++)
     fir2[f] = (int32_t)std::min(std::floor((1.75 * Rf[f] / alatt) * (1.75 * Rf[f] / alatt)),
                                 std::floor((40.0 / alatt - 1) * (40.0 / alatt - 1)));
-  DevCosmo C = ctx->dev_cosmo(G, Om, p->Omvac, p->h, p->ievol == 1 ? p->z_max + 1.0 : 0.0, p->ievol == 1);
-  ctx->filt_Rf.ensure(nfilt * 8);
-  ctx->filt_ir2.ensure(nfilt * 4);
-  PPB_CUDA(cudaMemcpyAsync(ctx->filt_Rf.p, Rf.data(), nfilt * 8, cudaMemcpyHostToDevice, s));
-  PPB_CUDA(cudaMemcpyAsync(ctx->filt_ir2.p, fir2.data(), nfilt * 4, cudaMemcpyHostToDevice, s));
+  DevCosmo C = ctx->dev_cosmo(sl, G, Om, p->Omvac, p->h, p->ievol == 1 ? p->z_max + 1.0 : 0.0, p->ievol == 1);
+  sl.filt_Rf.ensure(nfilt * 8);
+  sl.filt_ir2.ensure(nfilt * 4);
+  PPB_CUDA(cudaMemcpyAsync(sl.filt_Rf.p, Rf.data(), nfilt * 8, cudaMemcpyHostToDevice, s));
+  PPB_CUDA(cudaMemcpyAsync(sl.filt_ir2.p, fir2.data(), nfilt * 4, cudaMemcpyHostToDevice, s));
 
-  TileRes& T = ctx->tile(n);
+  TileRes& T = sl.tile_for(n);
   T.setup(n, s);
   if (T.cap == 0) T.ensure_peaks(std::max<int64_t>(1 << 16, std::min<int64_t>(N / 64, 1 << 22)));
 
-  cudaEvent_t* ev = ctx->stage_ev;
+  cudaEvent_t* ev = sl.stage_ev;
   PPB_CUDA(cudaEventRecord(ev[0], s));
   const double inv_n3 = 1.0 / (double)N;
   float2* dkp = T.dk.as<float2>();
@@ -355,7 +361,8 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
   // ---- phase 1: fields ----
   launch_noise(L, T.rw.as<float>(), n, p->seed);
   PPB_CUFFT(cufftExecR2C(T.r2c, T.rw.as<cufftReal>(), (cufftComplex*)kw));
-  launch_convolve(L, kw, n, box, ctx->pk_lk.as<double>(), ctx->pk_lp.as<double>(), ctx->pk_n, inv_n3);
+  launch_convolve(L, kw, n, box, ctx->sh.pk_lk.as<double>(), ctx->sh.pk_lp.as<double>(), ctx->sh.pk_n,
+                  p->pk_scale > 0.0 ? p->pk_scale : 1.0, inv_n3);
   launch_hermitise(L, kw, n, 1);
   PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)kw, T.delta.as<cufftReal>()));
   PPB_CUFFT(cufftExecR2C(T.r2c, T.delta.as<cufftReal>(), (cufftComplex*)dkp));
@@ -405,7 +412,7 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
   // ---- phase 2: filter bank and peaks ----
   const int qn = window_table_size(n);
   T.wtab.ensure((size_t)nfilt * 2 * qn * sizeof(float));
-  launch_window_tables(L, T.wtab.as<float>(), n, box, ctx->filt_Rf.as<double>(), nfilt, p->wsmooth, want_lap);
+  launch_window_tables(L, T.wtab.as<float>(), n, box, sl.filt_Rf.as<double>(), nfilt, p->wsmooth, want_lap);
   int64_t npk = 0;
   for (int attempt = 0; attempt < 2; attempt++) {
     PPB_CUDA(cudaMemsetAsync(T.mask.p, 0, N, s));
@@ -441,7 +448,7 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
     PPB_CUDA(cub::DeviceRadixSort::SortPairs(T.tmp.p, tb, T.keys.as<unsigned long long>(),
                                              T.keys_s.as<unsigned long long>(), T.vals.as<uint32_t>(),
                                              T.vals_s.as<uint32_t>(), (int)npk, 0, 40 + fbits, s));
-    ctx->launches++;
+    sl.launches++;
     PrepArgs pa{};
     pa.keys = T.keys_s.as<unsigned long long>();
     pa.vals = T.vals_s.as<uint32_t>();
@@ -450,8 +457,8 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
     pa.npk = (int)npk;
     pa.n = n;
     pa.alatt = alatt;
-    pa.fRf = ctx->filt_Rf.as<double>();
-    pa.fir2 = ctx->filt_ir2.as<int32_t>();
+    pa.fRf = sl.filt_Rf.as<double>();
+    pa.fir2 = sl.filt_ir2.as<int32_t>();
     pa.ievol = p->ievol;
     pa.z_out = p->z_out;
     pa.fcrit0 = fcrit_val;
@@ -466,18 +473,18 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
     pa.d2Rf = T.p_d2Rf.as<float>();
     pa.pos = T.p_pos.as<double>();
     prep_kernel<<<(unsigned)((npk + 255) / 256), 256, 0, s>>>(pa);
-    PPB_LAUNCHED(ctx->launches);
+    PPB_LAUNCHED(sl.launches);
   }
 
   // ---- phase 4: shells ----
   ShellStats st{};
   if (npk > 0) {
-    ShellArgs a = ctx->shell_args(n, alatt, T.aos.as<float4>(), want_lap ? T.lapd.as<float>() : nullptr);
+    ShellArgs a = ctx->shell_args(sl, shells, n, alatt, T.aos.as<float4>(), want_lap ? T.lapd.as<float>() : nullptr);
     a.pk = PeakParams{T.p_lin.as<int64_t>(), T.p_Rf.as<double>(), T.p_ir2.as<int32_t>(), T.p_Z.as<double>(),
                       T.p_fc.as<double>()};
     a.npk = npk;
     a.out = T.res.as<double>();
-    ctx->run_shells(a, !plain, !plain, &st);
+    ctx->run_shells(sl, a, !plain, !plain, &st);
   }
   PPB_CUDA(cudaEventRecord(ev[3], s));
 
@@ -508,13 +515,13 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
     r.rthl = T.rthl.as<float>();
     const unsigned gb = (unsigned)((npk + 255) / 256);
     flag_kernel<<<gb, 256, 0, s>>>(r);
-    PPB_LAUNCHED(ctx->launches);
+    PPB_LAUNCHED(sl.launches);
     PPB_CUDA(cudaMemsetAsync(T.flags.as<int>() + npk, 0, 4, s));
     size_t tb = T.tmp.bytes;
     PPB_CUDA(cub::DeviceScan::ExclusiveSum(T.tmp.p, tb, T.flags.as<int>(), T.offs.as<int>(), (int)npk + 1, s));
-    ctx->launches++;
+    sl.launches++;
     record_kernel<<<gb, 256, 0, s>>>(r);
-    PPB_LAUNCHED(ctx->launches);
+    PPB_LAUNCHED(sl.launches);
     int nr = 0;
     PPB_CUDA(cudaMemcpyAsync(&nr, T.offs.as<int>() + npk, 4, cudaMemcpyDeviceToHost, s));
     PPB_CUDA(cudaStreamSynchronize(s));
@@ -523,7 +530,7 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
       size_t tb2 = T.tmp.bytes;
       float* dmax = T.count.as<float>() + 8;
       PPB_CUDA(cub::DeviceReduce::Max(T.tmp.p, tb2, T.rthl.as<float>(), dmax, (int)nrec, s));
-      ctx->launches++;
+      sl.launches++;
       PPB_CUDA(cudaMemcpyAsync(&rmax, dmax, 4, cudaMemcpyDeviceToHost, s));
     }
   }
@@ -534,22 +541,17 @@ int run_tile_impl(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf_in, i
   if (st.akk != 0)
     throw Error{PPB_ERR_INVALID, "kernel_strain SPH table index out of range (the reference raises here too)"};
 
-  out->nfields = nf;
-  out->count = nrec;
-  out->npeaks = npk;
-  out->RTHLmax = nrec > 0 ? rmax : 0.f;
-  ctx->last_visits = st.visits;
-  ctx->last_npk = npk;
+  o->nfields = nf;
+  o->count = nrec;
+  o->npeaks = npk;
+  o->RTHLmax = nrec > 0 ? rmax : 0.f;
+  o->d_records = T.rec.as<float>();
+  sl.last_visits = st.visits;
+  sl.last_npk = npk;
   float ms[4];
   for (int i = 0; i < 4; i++) PPB_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
-  std::memcpy(ctx->stage_ms, ms, sizeof(ms));
-  if (device_ms) *device_ms = ms[0] + ms[1] + ms[2] + ms[3];
-  if (nrec > out->capacity) return PPB_ERR_CAPACITY;
-  if (nrec > 0) {
-    PPB_REQUIRE(out->records != nullptr, "records buffer is null");
-    copy_out(out->records, T.rec.p, (size_t)nrec * nf * 4, s);
-  }
-  return PPB_OK;
+  std::memcpy(sl.stage_ms, ms, sizeof(ms));
+  o->device_ms = ms[0] + ms[1] + ms[2] + ms[3];
 }
 
 }  // namespace ppb

@@ -70,7 +70,15 @@ class _TileParams(ctypes.Structure):
                 ("ievol", ctypes.c_int32), ("cenx", ctypes.c_double), ("ceny", ctypes.c_double),
                 ("cenz", ctypes.c_double), ("ilpt", ctypes.c_int32), ("ioutshear", ctypes.c_int32),
                 ("wsmooth", ctypes.c_int32), ("rmax2rs", ctypes.c_double), ("seed", ctypes.c_uint64),
-                ("plain", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7)]
+                ("plain", ctypes.c_int32), ("reserved0", ctypes.c_int32), ("pk_scale", ctypes.c_double),
+                ("reserved", ctypes.c_int32 * 4)]
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("tiles_done", ctypes.c_int64), ("peaks_done", ctypes.c_int64), ("halos_done", ctypes.c_int64),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("tiles_per_s", ctypes.c_double),
+                ("hbm_in_use", ctypes.c_uint64), ("hbm_budget", ctypes.c_uint64), ("in_flight", ctypes.c_int32),
+                ("queued", ctypes.c_int32), ("slots", ctypes.c_int32), ("failed", ctypes.c_int32)]
 
 
 class _HaloBuf(ctypes.Structure):
@@ -87,7 +95,7 @@ EXPORTED = (
     "ppb_find_peaks", "ppb_analyse_peaks", "ppb_event_record", "ppb_event_elapsed", "ppb_synchronize",
     "ppb_launch_count", "ppb_last_shell_stats", "ppb_last_stage_ms", "ppb_alloc_host", "ppb_free_host",
     "ppb_alloc_device", "ppb_free_device", "ppb_shell_counters", "ppb_find_peaks_noalloc",
-    "ppb_last_shell_times",
+    "ppb_last_shell_times", "ppb_serve_config", "ppb_submit", "ppb_wait", "ppb_stats_get", "ppb_stats_reset",
 )
 
 
@@ -127,6 +135,11 @@ def load_library():
     L.ppb_last_stage_ms.argtypes = [P, P]
     L.ppb_shell_counters.argtypes = [P, P]
     L.ppb_last_shell_times.argtypes = [P, P, P, P]
+    L.ppb_serve_config.argtypes = [P, I32]
+    L.ppb_submit.argtypes = [P, ctypes.POINTER(_TileParams), P, I32, ctypes.POINTER(ctypes.c_uint64)]
+    L.ppb_wait.argtypes = [P, ctypes.c_uint64, I32, ctypes.POINTER(_HaloBuf)]
+    L.ppb_stats_get.argtypes = [P, ctypes.POINTER(_Stats)]
+    L.ppb_stats_reset.argtypes = [P]
     for f in ("ppb_alloc_host", "ppb_alloc_device"):
         getattr(L, f).argtypes = [P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
     for f in ("ppb_free_host", "ppb_free_device"):
@@ -388,14 +401,14 @@ class Context:
         self._check(self.L.ppb_free_device(self.h, ctypes.c_void_p(ptr)))
 
     @staticmethod
-    def _params(cfg: PipelineConfig, seed: int, plain: bool) -> _TileParams:
+    def _params(cfg: PipelineConfig, seed: int, plain: bool, pk_scale: float = 1.0) -> _TileParams:
         if cfg.NonGauss not in (0,):
             raise PPBError(-6, "NonGauss modes are outside this path")
         return _TileParams(Omx=cfg.Omx, OmB=cfg.OmB, Omvac=cfg.Omvac, h=cfg.h, n=cfg.n, boxsize=cfg.boxsize,
                            nbuff=cfg.nbuff, z_out=cfg.z_out, z_max=cfg.z_max, ievol=cfg.ievol, cenx=cfg.cenx,
                            ceny=cfg.ceny, cenz=cfg.cenz, ilpt=cfg.ilpt, ioutshear=cfg.ioutshear,
                            wsmooth=cfg.wsmooth, rmax2rs=cfg.rmax2rs, seed=int(seed) & (2**64 - 1),
-                           plain=1 if plain else 0)
+                           plain=1 if plain else 0, pk_scale=float(pk_scale))
 
     def run_tile_into(self, cfg: PipelineConfig, seed: int, Rf: Sequence[float], ptr: int, capacity: int,
                       plain: bool = False):
@@ -411,16 +424,10 @@ class Context:
 
     # ---- path entry points ----
     def run_tile_arrays(self, cfg: PipelineConfig, seed: int, Rf: Sequence[float], plain: bool = False,
-                        capacity: int = 0, timed: bool = False):
+                        capacity: int = 0, timed: bool = False, pk_scale: float = 1.0):
         """run_tile with the tables already set.  Returns (records, RTHLmax,
         npeaks[, device_ms])."""
-        if cfg.NonGauss not in (0,):
-            raise PPBError(-6, "NonGauss modes are outside this path")
-        p = _TileParams(Omx=cfg.Omx, OmB=cfg.OmB, Omvac=cfg.Omvac, h=cfg.h, n=cfg.n, boxsize=cfg.boxsize,
-                        nbuff=cfg.nbuff, z_out=cfg.z_out, z_max=cfg.z_max, ievol=cfg.ievol, cenx=cfg.cenx,
-                        ceny=cfg.ceny, cenz=cfg.cenz, ilpt=cfg.ilpt, ioutshear=cfg.ioutshear,
-                        wsmooth=cfg.wsmooth, rmax2rs=cfg.rmax2rs, seed=int(seed) & (2**64 - 1),
-                        plain=1 if plain else 0)
+        p = self._params(cfg, seed, plain, pk_scale)
         rf = np.ascontiguousarray(np.asarray(Rf, dtype=np.float64))
         nf = 33 if cfg.ioutshear >= 1 else 11
         cap = capacity or max(1024, getattr(self, "_last_count", 0) * 2)
@@ -438,6 +445,46 @@ class Context:
             out = (rec[:hb.count].copy(), float(hb.RTHLmax), int(hb.npeaks))
             return out + (ms.value,) if timed else out
         raise PPBError(-7, "record capacity")
+
+    # ---- serving ----
+    def serve_config(self, slots: int):
+        """Number of execution slots of the serving loop (before the first submit)."""
+        self._check(self.L.ppb_serve_config(self.h, int(slots)))
+
+    def submit(self, cfg: PipelineConfig, seed: int, Rf: Sequence[float], pk_scale: float = 1.0,
+               plain: bool = False) -> int:
+        """Queue a tile request; returns its ticket."""
+        p = self._params(cfg, seed, plain, pk_scale)
+        rf = np.ascontiguousarray(np.asarray(Rf, dtype=np.float64))
+        t = ctypes.c_uint64()
+        self._check(self.L.ppb_submit(self.h, ctypes.byref(p), _p(rf), len(rf), ctypes.byref(t)))
+        return int(t.value)
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """Result of a submitted request: (records, RTHLmax, npeaks), or None
+        when timeout_ms ran out first."""
+        hb = _HaloBuf(records=None, capacity=0)
+        rc = self.L.ppb_wait(self.h, ctypes.c_uint64(ticket), int(timeout_ms), ctypes.byref(hb))
+        if rc == -5:
+            return None
+        if rc == -7 or (rc == 0 and hb.count == 0):
+            nf = int(hb.nfields) or 33
+            rec = np.empty((max(int(hb.count), 1), nf), dtype=np.float32)
+            if rc == -7:
+                hb2 = _HaloBuf(records=rec.ctypes.data, capacity=rec.shape[0])
+                self._check(self.L.ppb_wait(self.h, ctypes.c_uint64(ticket), -1, ctypes.byref(hb2)))
+                hb = hb2
+            return rec[:hb.count].copy(), float(hb.RTHLmax), int(hb.npeaks)
+        self._check(rc)
+        raise PPBError(-1, "unexpected ppb_wait result")
+
+    def serve_stats(self) -> dict:
+        st = _Stats()
+        self._check(self.L.ppb_stats_get(self.h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in _Stats._fields_}
+
+    def serve_stats_reset(self):
+        self._check(self.L.ppb_stats_reset(self.h))
 
     def run_tile(self, cfg: PipelineConfig, seed: int = 42, plain: bool = False, write: bool = True):
         """Pipeline.run_tile(cfg; seed): reads cfg.pkfile / filterfile /

@@ -29,7 +29,22 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert pp.load_library().ppb_abi_version() == 1
+    assert pp.load_library().ppb_abi_version() == 2
+
+
+def test_tile_params_layout_matches_the_header():
+    # ppb_tile_params: 168 bytes, pk_scale at offset 144 (after plain and reserved0)
+    assert ctypes.sizeof(pp._TileParams) == 168
+    assert pp._TileParams.pk_scale.offset == 144
+    assert ctypes.sizeof(pp._Stats) == 8 * 6 + 8 * 2 + 4 * 4
+
+
+def test_serving_entry_points_reject_bad_arguments():
+    L = pp.load_library()
+    assert L.ppb_submit(None, None, None, 0, None) == -1
+    assert L.ppb_wait(None, 1, 0, None) == -1
+    assert L.ppb_stats_get(None, None) == -1
+    assert L.ppb_serve_config(None, 4) == -1
 
 
 def test_write_pksc_through_the_abi(tmp_path):
