@@ -10,6 +10,7 @@ that tile: noise, fields, filter bank + peaks, shells, records.
 
 Usage:
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--plain]
+  python bench.py --serve      # the serving stream: 200 requests, Poisson arrivals
 Under torchrun each rank runs independent tiles on its own GPU (run_tile
 does not shard: replicas) with its own seed; the job value is the tiles of
 all ranks over the slowest rank's device time.
@@ -236,11 +237,13 @@ def run_ours(args, dist: Dist):
     l0 = ctx.launch_count()
     ctx.event_record(0)
     shell_ms, shell_visits, npk_tot, nh_tot, stage = 0.0, 0, 0, 0, None
+    gather_ms = 0.0
     for s in range(args.steps):
         cnt, rmax, npk, dms = ctx.run_tile_into(cfg, seed0, FILTERS, dev_out, cap, plain=args.plain)
         st = ctx.shell_stats()
         last_shell_stats = st
         shell_ms += st["ms"]
+        gather_ms += st["kernel_ms"]["gather"]
         shell_visits += st["visits"]
         npk_tot += npk
         nh_tot += cnt
@@ -270,11 +273,16 @@ def run_ours(args, dist: Dist):
     tiles = dist.sum(float(args.steps))
     value = tiles / (dev_ms_max / 1000.0)
     e2e = tiles / (e2e_ms_max / 1000.0)
-    # roofline of the dominant own kernel (the shell kernel): algorithmic
-    # bytes = in-bounds cell visits x 32 B gather record + 248 B result per peak
-    bytes_alg = shell_visits * 32 + npk_tot * 31 * 8
-    achieved = bytes_alg / (shell_ms / 1000.0) / 1e9 if shell_ms > 0 else 0.0
+    # roofline of the dominant own kernel (the shell gather): algorithmic
+    # bytes = in-bounds cell visits x 32 B packed record (delta, deltaT,
+    # psi1 x3, psi2 x3 as Float32)
+    bytes_alg = shell_visits * 32
+    achieved = bytes_alg / (gather_ms / 1000.0) / 1e9 if gather_ms > 0 else 0.0
     peaks = _measured_peaks()
+    extra = {}
+    if dist.rank == 0 and not args.plain and not args.no_extras:
+        extra["plain_path"] = _plain_compare(ctx, cfg, seed0, dev_out, cap, value / max(1, dist.world))
+        extra["serving_burst"] = _serving_burst(ctx)
     line = None
     if dist.rank == 0:
         line = {
@@ -292,18 +300,146 @@ def run_ours(args, dist: Dist):
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
             "gpu_launches": int(launches),
-            "roofline": {"kernel": "shell_kernel (gather + collapse walk)", "bound": "hbm",
+            "roofline": {"kernel": "gather_kernel (shell sums)", "bound": "hbm",
                          "achieved": achieved, "peak": peaks[0], "unit": "GB/s",
-                         "frac": achieved / peaks[0] if peaks[0] else None, "traffic": None,
+                         "frac": achieved / peaks[0] if peaks[0] else None, "traffic": GATHER_TRAFFIC_384,
                          "peak_source": peaks[1],
                          "alg_bytes_per_launch": bytes_alg / max(1, args.steps),
-                         "kernel_ms_per_launch": shell_ms / max(1, args.steps)},
+                         "kernel_ms_per_launch": gather_ms / max(1, args.steps),
+                         "shell_stage_ms_per_step": shell_ms / max(1, args.steps)},
             "clocks": clk,
         }
+        line.update(extra)
     ctx.free_device(dev_out)
     ctx.free_host(host_out)
     ctx.close()
     return line
+
+
+# DRAM bytes (read + write) of one gather_kernel launch on the 384^3 tile,
+# scaled from the ncu capture of the same kernel on the 256^3 tile by the cell
+# visits (profiles/gather_kernel_run_tile_256.md); None until captured
+GATHER_TRAFFIC_384 = None
+
+
+def _plain_compare(ctx, cfg, seed, dev_out, cap, opt_tiles_per_s):
+    """The plain GPU path (full spheres, FP64 shell sums, unbatched
+    transforms) on the same tile: one warm-up and one timed run."""
+    ctx.run_tile_into(cfg, seed, FILTERS, dev_out, cap, plain=True)
+    ctx.synchronize()
+    ctx.event_record(4)
+    cnt, rmax, npk, dms = ctx.run_tile_into(cfg, seed, FILTERS, dev_out, cap, plain=True)
+    ctx.event_record(5)
+    ctx.synchronize()
+    ms = ctx.event_elapsed(4, 5)
+    return {"tiles_per_s": 1000.0 / ms, "ms_per_tile": ms, "halos": cnt, "peaks": npk,
+            "optimised_over_plain": opt_tiles_per_s * ms / 1000.0}
+
+
+SERVE_SIZES = (128, 192, 256, 384)
+
+
+def _serving_request(rng):
+    import peakpatch_b200 as pp
+    n = int(rng.choice(SERVE_SIZES))
+    ievol = int(rng.integers(0, 2))
+    s8 = float(rng.uniform(0.75, 0.85))
+    box = BOX_PER_CELL * n
+    cfg = pp.PipelineConfig(Omx=0.315 - 0.049, OmB=0.049, Omvac=0.685, h=0.674, n=n, boxsize=box, nbuff=32,
+                            z_out=0.0, z_max=4.6 if ievol else 0.0, ievol=ievol, ilpt=2, ioutshear=1, wsmooth=1,
+                            rmax2rs=0.0, cenx=-box / 2 if ievol else 0.0, ceny=-box / 2 if ievol else 0.0,
+                            cenz=-box / 2 if ievol else 0.0)
+    return cfg, int(rng.integers(1, 2**31)), (s8 / 0.808) ** 2
+
+
+def _serving_burst(ctx, nreq=24, slots=4):
+    """nreq mixed requests (nmesh in {128,192,256,384}, random seeds,
+    sigma8 in 0.75-0.85, ievol 0/1) submitted at once to the serving loop,
+    against the same requests run one after another through run_tile."""
+    rng = np.random.default_rng(123)
+    reqs = [_serving_request(rng) for _ in range(nreq)]
+    for cfg, seed, sc in reqs[:4]:   # warm the plans and tables of every size once
+        ctx.run_tile_arrays(cfg, seed, FILTERS, pk_scale=sc)
+    t0 = time.perf_counter()
+    for cfg, seed, sc in reqs:
+        ctx.run_tile_arrays(cfg, seed, FILTERS, pk_scale=sc)
+    seq_s = time.perf_counter() - t0
+    ctx.serve_config(slots)
+    for cfg, seed, sc in reqs[:slots]:   # warm the slots
+        ctx.wait(ctx.submit(cfg, seed, FILTERS, pk_scale=sc))
+    ctx.serve_stats_reset()
+    t0 = time.perf_counter()
+    tickets = [ctx.submit(cfg, seed, FILTERS, pk_scale=sc) for cfg, seed, sc in reqs]
+    for t in tickets:
+        ctx.wait(t)
+    served_s = time.perf_counter() - t0
+    st = ctx.serve_stats()
+    return {"requests": nreq, "slots": slots, "sizes": list(SERVE_SIZES),
+            "served_tiles_per_s": nreq / served_s, "sequential_tiles_per_s": nreq / seq_s,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "hbm_in_use_gb": st["hbm_in_use"] / 1e9}
+
+
+def run_serve(args, dist: Dist):
+    """The serving stream: 200 requests with Poisson arrivals (mean 4/s),
+    nmesh uniform in {128,192,256,384}^3, random seeds, sigma8 uniform in
+    0.75-0.85, ievol in {0,1}; latency from arrival to result."""
+    import peakpatch_b200 as pp
+    from peakpatch_b200 import powerspec
+    if dist.rank != 0:
+        return None
+    ctx = pp.Context(dist.local)
+    k, P = powerspec.eh_table()
+    ctx.set_pk_table(k, P)
+    ctx.set_collapse_table(pp.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat")))
+    ctx.serve_config(args.slots)
+    rng = np.random.default_rng(2026)
+    reqs = [_serving_request(rng) for _ in range(args.requests)]
+    gaps = rng.exponential(1.0 / args.rate, size=args.requests)
+    for n in SERVE_SIZES:   # warm plans and tables of each size (not timed)
+        cfg, seed, sc = _serving_request(np.random.default_rng(n))
+        cfg.n, cfg.boxsize = n, BOX_PER_CELL * n
+        ctx.wait(ctx.submit(cfg, seed, FILTERS, pk_scale=sc))
+    ctx.serve_stats_reset()
+    done = []
+    lock = threading.Lock()
+    tickets = []
+
+    def collector():
+        while True:
+            with lock:
+                if len(done) == len(reqs):
+                    return
+                pending = [t for t in tickets if t not in done]
+            for t in pending:
+                if ctx.wait(t, timeout_ms=5) is not None:
+                    with lock:
+                        done.append(t)
+            time.sleep(0.001)
+
+    th = threading.Thread(target=collector)
+    t0 = time.perf_counter()
+    th.start()
+    tnext = t0
+    for (cfg, seed, sc), g in zip(reqs, gaps):
+        tnext += g
+        dt = tnext - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        t = ctx.submit(cfg, seed, FILTERS, pk_scale=sc)
+        with lock:
+            tickets.append(t)
+    th.join()
+    wall = time.perf_counter() - t0
+    st = ctx.serve_stats()
+    ctx.close()
+    return {"metric": "tiles/s (served stream)", "value": st["tiles_per_s"], "unit": "tiles/s", "n_gpus": 1,
+            "steps": args.requests, "warmup": len(SERVE_SIZES), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "data": "synthetic", "dtype": "f32 fields, compensated-f32 shell sums",
+            "config": {"workload": "serving stream: Poisson arrivals, nmesh in {128,192,256,384}^3, sigma8 0.75-0.85, "
+                                   "ievol 0/1", "requests": args.requests, "rate_per_s": args.rate,
+                       "slots": args.slots},
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "failed": st["failed"], "wall_s": wall,
+            "peaks_per_s": st["peaks_done"] / wall, "hbm_in_use_gb": st["hbm_in_use"] / 1e9}
 
 
 def _measured_peaks():
@@ -325,11 +461,21 @@ def main():
     ap.add_argument("--plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-extras", action="store_true", help="skip the plain-path and serving-burst comparisons")
+    ap.add_argument("--serve", action="store_true", help="run the serving stream instead of the tile benchmark")
+    ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--rate", type=float, default=4.0)
+    ap.add_argument("--slots", type=int, default=4)
     args = ap.parse_args()
     dist = Dist()
     try:
         if args.impl == "reference":
             run_reference(args, dist)
+            return
+        if args.serve:
+            line = run_serve(args, dist)
+            if line is not None:
+                print(json.dumps(line), flush=True)
             return
         line = run_ours(args, dist)
         if dist.rank == 0 and line is not None:

@@ -7,6 +7,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cub/cub.cuh>
+
 #include "ppb_ctx.h"
 
 using namespace ppb;
@@ -53,13 +55,15 @@ void Slot::init(int dev) {
 
 void Slot::release_buffers() {
   tile.reset();
-  for (DevBuf* b : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool})
+  for (DevBuf* b : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
+                    &okey2, &oidx, &oidx2, &otmp})
     b->release();
 }
 
 size_t Slot::bytes_held() const {
   size_t b = tile ? tile->bytes() : 0;
-  for (const DevBuf* d : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool})
+  for (const DevBuf* d : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool,
+                          &okey, &okey2, &oidx, &oidx2, &otmp})
     b += d->bytes;
   return b;
 }
@@ -249,7 +253,20 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     for (int e = 0; e < 10; e++) b.fhalf[e] = std::pow(e / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
     PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, 16, stream));
     PPB_CUDA(cudaEventRecord(sl.shell_ev[0], stream));
-    launch_shell_geo(L, b);
+    // gather in spatial order: sort the peaks of the batch by brick Morton key
+    sl.okey.ensure(nb * 4 + 16);
+    sl.okey2.ensure(nb * 4 + 16);
+    sl.oidx.ensure(nb * 4 + 16);
+    sl.oidx2.ensure(nb * 4 + 16);
+    launch_shell_geo(L, b, sl.okey.as<uint32_t>(), sl.oidx.as<int32_t>());
+    size_t tb = 0;
+    PPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, sl.okey.as<uint32_t>(), sl.okey2.as<uint32_t>(),
+                                             sl.oidx.as<int32_t>(), sl.oidx2.as<int32_t>(), (int)nb, 0, 32, stream));
+    sl.otmp.ensure(tb + 16);
+    PPB_CUDA(cub::DeviceRadixSort::SortPairs(sl.otmp.p, tb, sl.okey.as<uint32_t>(), sl.okey2.as<uint32_t>(),
+                                             sl.oidx.as<int32_t>(), sl.oidx2.as<int32_t>(), (int)nb, 0, 32, stream));
+    sl.launches++;
+    b.order = sl.oidx2.as<int32_t>();
     launch_shell_gather(L, b, comp, adaptive, gblocks);
     PPB_CUDA(cudaEventRecord(sl.shell_ev[1], stream));
     launch_shell_collapse(L, b);

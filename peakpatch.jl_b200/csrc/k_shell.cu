@@ -555,21 +555,44 @@ __global__ void __launch_bounds__(32 * kGatherWarps, PPB_GATHER_MINB) gather_ker
   double* stage = a.stage + slot * a.stage_stride;
   double* part = gsm + (size_t)wib * GATHER_WARP_DOUBLES;
   while (true) {
-    int p = 0;
-    if (lane == 0) p = atomicAdd(a.queue, 1);
-    p = __shfl_sync(FULL, p, 0);
-    if (p >= a.npk) break;
+    int q = 0;
+    if (lane == 0) q = atomicAdd(a.queue, 1);
+    q = __shfl_sync(FULL, q, 0);
+    if (q >= a.npk) break;
+    const int64_t p = a.order ? (int64_t)a.order[q] : (int64_t)q;
     gather_one<COMP, ADAPTIVE>(a, p, stage, part);
     __syncwarp();
   }
 }
 
-// per-peak geometry (thread per peak)
-__global__ void geo_kernel(ShellArgs a) {
+// interleave the low 10 bits of x, y, z (Morton order)
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+  v &= 0x3ff;
+  v = (v | (v << 16)) & 0x030000ff;
+  v = (v | (v << 8)) & 0x0300f00f;
+  v = (v | (v << 4)) & 0x030c30c3;
+  v = (v | (v << 2)) & 0x09249249;
+  return v;
+}
+
+// per-peak geometry (thread per peak) and the gather order key: the Morton
+// index of the peak's 8^3-cell brick, so that peaks whose spheres overlap
+// (of any filter) are gathered close in time and share cached records
+__global__ void geo_kernel(ShellArgs a, uint32_t* key, int32_t* idx) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.npk) return;
   const Geo g = geometry(a, a.pk.Rf[p], a.pk.ir2min[p]);
   a.geo[p] = make_int4(g.m0_init, g.mrf, g.mlow_rf, g.mupp_rf);
+  if (key) {
+    const int64_t lin = a.pk.lin[p], n = a.n, n2 = n * n;
+    uint32_t k = 0xffffffffu;   // invalid peaks last
+    if (lin >= 0 && lin < n2 * n) {
+      const uint32_t i = (uint32_t)(lin % n) >> 3, j = (uint32_t)((lin / n) % n) >> 3, kk = (uint32_t)(lin / n2) >> 3;
+      k = spread3(i) | (spread3(j) << 1) | (spread3(kk) << 2);
+    }
+    key[p] = k;
+    idx[p] = (int32_t)p;
+  }
 }
 
 // ===========================================================================
@@ -991,10 +1014,10 @@ int shell_gather_blocks_per_sm(bool comp, bool adaptive) {
   return b > 0 ? b : 1;
 }
 
-void launch_shell_geo(Launch L, const ShellArgs& a) {
+void launch_shell_geo(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx) {
   const int64_t blocks = (a.npk + 127) / 128;
   if (blocks == 0) return;
-  geo_kernel<<<(unsigned)blocks, 128, 0, L.s>>>(a);
+  geo_kernel<<<(unsigned)blocks, 128, 0, L.s>>>(a, key, idx);
   PPB_LAUNCHED(*L.count);
 }
 

@@ -52,6 +52,7 @@ struct Slot {
   DevBuf filt_Rf, filt_ir2;                         // filter bank of the run
   DevBuf g_a, g_D, g_f, chi;                        // growth / chi tables of the run
   DevBuf stage, counters, ctl, hdr, geo, pool;      // shell stage
+  DevBuf okey, okey2, oidx, oidx2, otmp;            // spatial gather order
   int gather_bps[2][2] = {{0, 0}, {0, 0}};          // gather blocks per SM by [comp][adaptive]
   double rows_per_peak[2] = {0.0, 0.0};             // pool rows per peak seen last, by adaptive
   ShellStats last_shell{};

@@ -230,6 +230,7 @@ struct ShellArgs {
   int64_t stage_stride;     // doubles per warp slot
   double fhalf[10];         // ((e/9) / 2 + 1/2)^(1/3), e = 0..9 (zvir_half radii)
   int* queue;               // work counter for the persistent gather kernel
+  const int32_t* order;     // gather order (queue position -> peak), null: list order
   unsigned long long* counters;   // [0] cell visits, [1..5] dump reasons
 };
 
@@ -283,7 +284,9 @@ void launch_peakfind(Launch L, const float* ds, const float* ls, uint8_t* mask, 
 constexpr int kGatherWarps = 4;   // warps per gather block
 int64_t shell_stage_doubles_per_warp(int nshell);
 int shell_gather_blocks_per_sm(bool comp, bool adaptive);
-void launch_shell_geo(Launch L, const ShellArgs& a);
+// per-peak geometry; with key/idx non-null also the spatial gather-order
+// keys (Morton index of the peak's 8^3 brick) and the identity permutation
+void launch_shell_geo(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx);
 void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks);
 void launch_shell_collapse(Launch L, const ShellArgs& a);
 void launch_shell_zhalf(Launch L, const ShellArgs& a);

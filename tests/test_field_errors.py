@@ -1,0 +1,103 @@
+"""Per-field error of the shell sums against the FP64 oracle.
+
+The optimised path sums the shell fields in compensated single precision
+(packed FP32x2 two-sum, chunk partials combined in double); the plain path
+sums in double precision like the reference (RadialShell.jl:324-331).  Both
+run here on the oracle's own fields and peak list (identical input), and every
+output field of analyse_peak is compared with the oracle's FP64 result: radius
+RTHL, mass (proportional to RTHL^3), the three eigenvalues of the strain at
+RTHL, the displacements Sbar (1LPT) and Sbar2 (2LPT), Fbarx, e_v, p_v, the
+gradients, Srb, zvir_half and d2F.
+
+Size and sample are set by PPB_FIELD_ERR_N (default 128) and
+PPB_FIELD_ERR_SAMPLE (peaks compared, 0 = all); PPB_FIELD_ERR_OUT names a JSON
+file that receives the table."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+import peakpatch_b200 as pp
+from conftest import filter_bank
+
+N = int(os.environ.get("PPB_FIELD_ERR_N", "128"))
+SAMPLE = int(os.environ.get("PPB_FIELD_ERR_SAMPLE", "0"))
+RTOL = 1e-4
+MISMATCH = 1e-3
+
+
+def _columns(r):
+    """The compared quantities of a (npk, 31) result array, by name."""
+    R = r[:, 0]
+    strain = r[:, 8:17].reshape(-1, 3, 3)
+    fin = np.isfinite(strain).all(axis=(1, 2))
+    lam = np.full((len(r), 3), np.nan)
+    if fin.any():
+        s = strain[fin]
+        lam[fin] = np.linalg.eigvalsh(0.5 * (s + np.transpose(s, (0, 2, 1))))
+    cols = {"RTHL": R, "mass": R ** 3, "strain_eig1": lam[:, 0], "strain_eig2": lam[:, 1],
+            "strain_eig3": lam[:, 2], "Fbarx": r[:, 23], "e_v": r[:, 24], "p_v": r[:, 25], "Srb": r[:, 1],
+            "zvir_half": r[:, 26], "d2F": r[:, 30]}
+    for name, sl in (("Sbar", 2), ("Sbar2", 5), ("gradpk", 17), ("gradpkrf", 20), ("gradpkf", 27)):
+        for c in range(3):
+            cols[f"{name}_{'xyz'[c]}"] = r[:, sl + c]
+    return cols
+
+
+def field_error_table(g, o):
+    """Mismatch fraction (collapse flag or RTHL beyond RTOL) and, over the
+    halos that agree, the max and median relative error of every field.  The
+    relative error of a field is scaled by max(|oracle value|, 1e-6 of the
+    field's largest magnitude) so that components near zero do not dominate."""
+    cg, co = g[:, 0] > 0, o[:, 0] > 0
+    both = cg & co
+    rR = np.abs(g[:, 0] - o[:, 0]) / np.maximum(np.abs(o[:, 0]), 1e-300)
+    bad = (cg != co) | (both & (rR > RTOL))
+    keep = both & ~bad
+    A, B = _columns(g[keep]), _columns(o[keep])
+    table = {}
+    for name in A:
+        a, b = A[name], B[name]
+        fin = np.isfinite(a) & np.isfinite(b)
+        if not fin.any():
+            continue
+        scale = np.maximum(np.abs(b[fin]), 1e-6 * np.abs(b[fin]).max() + 1e-300)
+        e = np.abs(a[fin] - b[fin]) / scale
+        table[name] = {"max": float(e.max()), "median": float(np.median(e))}
+    return {"halos": int(co.sum()), "compared": int(keep.sum()), "mismatch": float(bad.sum() / max(1, co.sum())),
+            "fields": table}
+
+
+def test_per_field_error_vs_fp64_oracle(ora, julia_table, eh_pk):
+    from peakpatch_b200 import powerspec   # noqa: F401  (EH table comes from the fixture)
+    k, P = eh_pk
+    T = julia_table
+    box = 2.0 * N
+    cfg = ora.Config(Omx=0.315 - 0.049, OmB=0.049, Omvac=0.685, h=0.674, n=N, boxsize=box, nbuff=min(32, N // 4),
+                     z_out=0.0, z_max=0.0, ievol=0, ilpt=2, ioutshear=1, wsmooth=1, rmax2rs=0.0)
+    st = ora.run_tile_stages(cfg, 7, k, P, filter_bank(), T, peak_sample=np.arange(0))
+    ipp = st["peaks"]["ipp"]
+    sel = np.arange(len(ipp))
+    if SAMPLE and SAMPLE < len(ipp):
+        sel = np.sort(np.random.default_rng(0).choice(len(ipp), size=SAMPLE, replace=False))
+    args = (st["fields"], ipp[sel], st["Rf"][sel], st["ir2min"][sel], st["ZZon"][sel], st["fcrit"], st["alatt"])
+    o = ora.analyse_peaks(*args, st["shells"], T, nbuff=cfg.nbuff)
+    with pp.Context(0) as ctx:
+        ctx.set_collapse_table(pp.CollapseTable(T.data, T.x1, T.x2, T.y1, T.y2, T.z1, T.z2))
+        comp = ctx.analyse_peaks(*args, st["nhunt"], plain=False)
+        fp64 = ctx.analyse_peaks(*args, st["nhunt"], plain=True)
+    res = {"nmesh": N, "peaks": int(len(sel)), "compensated_fp32": field_error_table(comp, o),
+           "fp64": field_error_table(fp64, o)}
+    out = os.environ.get("PPB_FIELD_ERR_OUT")
+    if out:
+        with open(out, "w") as f:
+            json.dump(res, f, indent=1)
+    for key in ("compensated_fp32", "fp64"):
+        t = res[key]
+        assert t["mismatch"] <= MISMATCH, (key, t["mismatch"])
+        assert t["fields"]["RTHL"]["max"] <= RTOL and t["fields"]["mass"]["max"] <= 3 * RTOL, (key, t["fields"]["RTHL"])
+    # compensated sums are as good as double-precision ones for the radius
+    assert res["compensated_fp32"]["fields"]["RTHL"]["median"] <= 1e-9
