@@ -131,6 +131,25 @@ int32_t ppb_run_tile(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, i
 int32_t ppb_run_tile_timed(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, int32_t nfilt,
                            ppb_halo_buf* out, float* device_ms);
 
+/* run_multitile(cfg; ntile, seed) (src/MultiTile.jl:108-418): fields on the
+ * full periodic grid N = nsub ntile + 2 nbuff (nsub = n - 2 nbuff,
+ * alatt = boxsize / n), the filter bank on the full grid, peaks per tile in
+ * its nsub^3 core (lightcone: fcrit at the tile centre's redshift, tiles
+ * beyond chi(z_max) dropped), shells per tile on the tile's own fields.
+ * tiles: ntiles (it, jt, kt) triples, 1-based, in the order to process; NULL
+ * (ntiles = 0) means every tile in the reference's loop order (it fastest).
+ * Records are in tile order; output as ppb_run_tile. */
+int32_t ppb_run_multitile(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, int32_t nfilt, int32_t ntile,
+                          const int32_t* tiles, int32_t ntiles, ppb_halo_buf* out);
+
+/* merge_catalog(halos) (src/Merger/Merger.jl:21-78, Exclusion.jl:198-321):
+ * Lagrangian exclusion in decreasing radius, then volume reduction of the
+ * survivors' overlaps.  records: n x nfields (11 or 33) floats, host or
+ * device; out: room for n records (host or device; may not alias records);
+ * *n_out = survivors, written in input order with the reduced RTHL. */
+int32_t ppb_merge_catalog(ppb_ctx* ctx, const float* records, int64_t n, int32_t nfields, float* out,
+                          int64_t* n_out);
+
 /* write_pksc (src/IO/Catalog.jl:53-94): Int32 N, Float32 RTHLmax, Float32 z_out,
  * then N x nfields Float32 (little endian). */
 int32_t ppb_write_pksc(const char* path, const float* records, int64_t n, int32_t nfields,

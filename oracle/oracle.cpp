@@ -1148,4 +1148,140 @@ int64_t ora_pack_records(double Om, double OB, double OL, double h, int64_t npk,
   return nh;
 }
 
+
+// ---------------------------------------------------------------------------
+// merge_catalog (src/Merger/Merger.jl:31-78, src/Merger/Exclusion.jl:29-221),
+// sequential as the reference: NC^3 linked-list hash over the padded domain,
+// halos in decreasing radius (stable), pass 1 exclusion, pass 2 volume
+// reduction with each pair counted from both sides and halved.
+// ---------------------------------------------------------------------------
+void ora_sphere_overlap(double d, double r1, double r2, double* v1, double* v2) {
+  *v1 = 0.0;
+  *v2 = 0.0;
+  if (d >= r1 + r2) return;
+  if (d <= std::fabs(r1 - r2)) return;
+  const double h1 = (r2 - r1 + d) * (r2 + r1 - d) / (2.0 * d);
+  const double h2 = (r1 - r2 + d) * (r1 + r2 - d) / (2.0 * d);
+  const double pi = 3.141592653589793;
+  *v1 = (pi / 3.0) * (h1 * h1) * (3.0 * r1 - h1);
+  *v2 = (pi / 3.0) * (h2 * h2) * (3.0 * r2 - h2);
+}
+
+// survivors (in input order) are written to out with the reduced RTHL;
+// keep (optional, n entries) receives 1 for survivors; returns their number
+int64_t ora_merge_catalog(const float* rec, int64_t n, int nf, float* out, int32_t* keep) {
+  if (n <= 0) return 0;
+  const int NC = 256;
+  std::vector<double> x(n), y(n), z(n), r(n);
+  for (int64_t i = 0; i < n; i++) {
+    x[i] = rec[i * nf + 0];
+    y[i] = rec[i * nf + 1];
+    z[i] = rec[i * nf + 2];
+    r[i] = rec[i * nf + 6];
+  }
+  std::vector<int64_t> order(n);
+  for (int64_t i = 0; i < n; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return r[a] > r[b]; });
+  const double rmax = *std::max_element(r.begin(), r.end());
+  double mn[3] = {x[0], y[0], z[0]}, mx[3] = {x[0], y[0], z[0]};
+  for (int64_t i = 1; i < n; i++) {
+    mn[0] = std::min(mn[0], x[i]); mx[0] = std::max(mx[0], x[i]);
+    mn[1] = std::min(mn[1], y[i]); mx[1] = std::max(mx[1], y[i]);
+    mn[2] = std::min(mn[2], z[i]); mx[2] = std::max(mx[2], z[i]);
+  }
+  const double pad = 2.0 * rmax;
+  double dmin[3], L = 0.0;
+  for (int d = 0; d < 3; d++) {
+    dmin[d] = mn[d] - pad;
+    L = std::max(L, (mx[d] + pad) - (mn[d] - pad));
+  }
+  const double cs = L / NC;
+  auto cidx = [&](double v, int d) {
+    int c = (int)std::floor((v - dmin[d]) / cs) + 1;
+    return c < 1 ? 1 : (c > NC ? NC : c);
+  };
+  std::vector<int32_t> hoc((size_t)NC * NC * NC, 0), ll(n, 0);   // 1-based chains, 0 = end
+  auto H = [&](int ix, int iy, int iz) -> int32_t& {
+    return hoc[(size_t)(ix - 1) + (size_t)NC * ((iy - 1) + (size_t)NC * (iz - 1))];
+  };
+  for (int64_t m = 0; m < n; m++) {
+    int32_t& h = H(cidx(x[m], 0), cidx(y[m], 1), cidx(z[m], 2));
+    ll[m] = h;
+    h = (int32_t)(m + 1);
+  }
+  std::vector<char> surv(n, 1);
+  // pass 1
+  for (int64_t rk = 0; rk < n; rk++) {
+    const int64_t i = order[rk];
+    if (!surv[i]) continue;
+    const double ri = r[i], xi = x[i], yi = y[i], zi = z[i];
+    const int dcell = (int)std::ceil(ri / cs);
+    const int ci = cidx(xi, 0), cj = cidx(yi, 1), ck = cidx(zi, 2);
+    for (int diz = -dcell; diz <= dcell; diz++)
+      for (int diy = -dcell; diy <= dcell; diy++)
+        for (int dix = -dcell; dix <= dcell; dix++) {
+          const int jx = dix + ci, jy = diy + cj, jz = diz + ck;
+          if (jx < 1 || jx > NC || jy < 1 || jy > NC || jz < 1 || jz > NC) continue;
+          int32_t j1 = H(jx, jy, jz);
+          while (j1 > 0) {
+            const int64_t j = j1 - 1;
+            if (j != i && surv[j] && ri >= r[j]) {
+              const double dx = x[j] - xi, dy = y[j] - yi, dz = z[j] - zi;
+              const double dist = std::sqrt(dx * dx + dy * dy + dz * dz);
+              if (dist < ri) surv[j] = 0;
+            }
+            j1 = ll[j];
+          }
+        }
+  }
+  // pass 2
+  std::vector<double> dV(n, 0.0);
+  const double rfirst = r[order[0]];
+  for (int64_t rk = 0; rk < n; rk++) {
+    const int64_t i = order[rk];
+    if (!surv[i]) continue;
+    const double ri = r[i], xi = x[i], yi = y[i], zi = z[i];
+    const int dcell = (int)std::ceil((ri + rfirst) / cs);
+    const int ci = cidx(xi, 0), cj = cidx(yi, 1), ck = cidx(zi, 2);
+    for (int diz = -dcell; diz <= dcell; diz++)
+      for (int diy = -dcell; diy <= dcell; diy++)
+        for (int dix = -dcell; dix <= dcell; dix++) {
+          const int jx = dix + ci, jy = diy + cj, jz = diz + ck;
+          if (jx < 1 || jx > NC || jy < 1 || jy > NC || jz < 1 || jz > NC) continue;
+          int32_t j1 = H(jx, jy, jz);
+          while (j1 > 0) {
+            const int64_t j = j1 - 1;
+            if (j != i && surv[j]) {
+              const double rj = r[j];
+              const double dx = x[j] - xi, dy = y[j] - yi, dz = z[j] - zi;
+              const double dist = std::sqrt(dx * dx + dy * dy + dz * dz);
+              if (dist < ri + rj && dist > std::fabs(ri - rj)) {
+                double v1, v2;
+                ora_sphere_overlap(dist, ri, rj, &v1, &v2);
+                dV[i] += v1;
+                dV[j] += v2;
+              }
+            }
+            j1 = ll[j];
+          }
+        }
+  }
+  const double fpt = 4.0 * 3.141592653589793 / 3.0;
+  int64_t m = 0;
+  for (int64_t i = 0; i < n; i++) {
+    double rn = 0.0;
+    if (surv[i]) {
+      const double vol_new = fpt * (r[i] * r[i] * r[i]) - dV[i] * 0.5;
+      if (vol_new <= 0.0) surv[i] = 0;
+      else rn = std::pow(vol_new / fpt, 1.0 / 3.0);
+    }
+    if (keep) keep[i] = surv[i];
+    if (!surv[i]) continue;
+    for (int f = 0; f < nf; f++) out[m * nf + f] = rec[i * nf + f];
+    out[m * nf + 6] = (float)rn;
+    m++;
+  }
+  return m;
+}
+
 }  // extern "C"

@@ -97,6 +97,9 @@ def _declare(L):
     L.ora_pack_records.argtypes = [D, D, D, D, I64, P, P, P, P, P, P, P, D, ctypes.c_int, D, D, D, D,
                                    D, ctypes.c_int, ctypes.c_int, P, P]
     L.ora_pack_records.restype = I64
+    L.ora_sphere_overlap.argtypes = [D, D, D, P, P]
+    L.ora_merge_catalog.argtypes = [P, I64, ctypes.c_int, P, P]
+    L.ora_merge_catalog.restype = I64
 
 
 def _p(a):
@@ -457,6 +460,133 @@ def run_tile_stages(cfg: Config, seed: int, pk_k, pk_p, filters, T: Table, peak_
     return dict(fields=fields, delta_k=delta_k, peaks=peaks, Rf=pRf, FcollvRf=pFc, d2FRf=pd2,
                 ir2min=ir2min, ZZon=ZZon, fcrit=fcrit_val, results=res, records=rec, shells=shells,
                 nhunt=nhunt, alatt=alatt)
+
+
+def sphere_overlap(d: float, r1: float, r2: float):
+    """sphere_overlap (src/Merger/Exclusion.jl:82-100) -> (v1, v2)."""
+    v1, v2 = np.zeros(1), np.zeros(1)
+    lib().ora_sphere_overlap(float(d), float(r1), float(r2), _p(v1), _p(v2))
+    return float(v1[0]), float(v2[0])
+
+
+def merge_catalog(rec: np.ndarray):
+    """merge_catalog (src/Merger/Merger.jl:21-78): returns (survivors with the
+    reduced RTHL, keep mask over the input)."""
+    rec = np.ascontiguousarray(rec, np.float32)
+    n, nf = rec.shape
+    out = np.empty_like(rec)
+    keep = np.zeros(n, np.int32)
+    m = lib().ora_merge_catalog(_p(rec), n, nf, _p(out), _p(keep))
+    return out[:m].copy(), keep.astype(bool)
+
+
+def tile_center(it: int, jt: int, kt: int, ntile: int, dcore: float):
+    """tile_center (src/MultiTile.jl:79-86)."""
+    cen = (ntile + 1) / 2
+    return ((it - cen) * dcore, (jt - cen) * dcore, (kt - cen) * dcore)
+
+
+def run_multitile(cfg: Config, seed: int, pk_k, pk_p, filters, T: Table, ntile: int, tiles=None):
+    """run_multitile (src/MultiTile.jl:108-418): fields on the full periodic
+    grid N = nsub ntile + 2 nbuff, the filter bank smoothed globally and the
+    peaks found per tile core, the shell analysis per tile on the extracted
+    n^3 fields; records in tile order.  `tiles` optionally lists (it, jt, kt)
+    (1-based) to process, else every tile in the reference's loop order."""
+    Om = cfg.Omx + cfg.OmB
+    filters = sorted(filters, key=lambda f: -f[2])
+    nm, nbuff = cfg.n, cfg.nbuff
+    nsub = nm - 2 * nbuff
+    N = nsub * ntile + 2 * nbuff
+    alatt = cfg.boxsize / nm
+    box = N * alatt
+    dcore = nsub * alatt
+    fcrit_val = fsc_of_z(Om, cfg.OmB, cfg.Omvac, cfg.h, cfg.z_out)
+    nhunt = min(nbuff - 1, int(np.floor(filters[0][2] * 1.75 / alatt)))
+    shells = precompute_shells(nhunt)
+    delta = generate_grf(N, pk_k, pk_p, box, seed)
+    delta_k = rfft3(delta)
+    psi = lpt1(delta_k, N, box)
+    psi2 = lpt2(delta_k, N, box) if cfg.ilpt >= 2 else [None, None, None]
+    lapd = laplacian(delta_k, N, box) if cfg.ioutshear >= 1 else None
+    if tiles is None:
+        tiles = [(it, jt, kt) for kt in range(1, ntile + 1) for jt in range(1, ntile + 1)
+                 for it in range(1, ntile + 1)]
+    obs = (cfg.cenx, cfg.ceny, cfg.cenz)
+    if cfg.ievol == 1:   # drop tiles beyond chi(z_max) (MultiTile.jl:205-216)
+        chi_max = chi(Om, cfg.Omvac, cfg.h, cfg.z_max)
+        half = dcore / 2.0
+        keep = []
+        for t in tiles:
+            c = tile_center(*t, ntile, dcore)
+            d = [max(abs(c[q] - obs[q]) - half, 0.0) for q in range(3)]
+            if np.sqrt(d[0] ** 2 + d[1] ** 2 + d[2] ** 2) <= chi_max:
+                keep.append(t)
+        tiles = keep
+    sl = lambda a, t: a[(t[2] - 1) * nsub:(t[2] - 1) * nsub + nm, (t[1] - 1) * nsub:(t[1] - 1) * nsub + nm,
+                        (t[0] - 1) * nsub:(t[0] - 1) * nsub + nm]
+    fcrit_t = []
+    for t in tiles:
+        fc = np.float32(fcrit_val)
+        if cfg.ievol == 1:   # fcrit of the tile centre's redshift (MultiTile.jl:238-243)
+            c = tile_center(*t, ntile, dcore)
+            zt = chi_to_z(Om, cfg.Omvac, cfg.h, cfg.z_max + 1.0,
+                          np.array([np.sqrt(sum((c[q] - obs[q]) ** 2 for q in range(3)))]))[0]
+            fc = np.float32(fsc_of_z(Om, cfg.OmB, cfg.Omvac, cfg.h, zt))
+        fcrit_t.append(fc)
+    masks = [np.zeros((nm, nm, nm), np.int8) for _ in tiles]
+    tp = [dict(peaks=[], Rf=[], Fc=[], d2=[]) for _ in tiles]
+    for (_, _, Rf) in filters:
+        ds = smooth_field(delta_k, N, box, Rf, cfg.wsmooth)
+        ls = smooth_field(delta_k, N, box, Rf, 3) if cfg.ioutshear >= 1 else None
+        for ti, t in enumerate(tiles):
+            dst = np.ascontiguousarray(sl(ds, t))
+            c = tile_center(*t, ntile, dcore)
+            pk = find_peaks(dst, masks[ti], c[0], c[1], c[2], alatt, nbuff, fcrit_t[ti])
+            lin = pk["ipp"] - 1
+            tp[ti]["peaks"].append(pk)
+            tp[ti]["Rf"].append(np.full(len(lin), Rf))
+            tp[ti]["Fc"].append(dst.reshape(-1)[lin])
+            tp[ti]["d2"].append(np.ascontiguousarray(sl(ls, t)).reshape(-1)[lin] if ls is not None
+                                else np.zeros(len(lin), np.float32))
+    recs, npk_tot = [], 0
+    L = lib()
+    for ti, t in enumerate(tiles):
+        peaks = {k: np.concatenate([p[k] for p in tp[ti]["peaks"]]) for k in tp[ti]["peaks"][0]}
+        pRf = np.concatenate(tp[ti]["Rf"])
+        pFc = np.concatenate(tp[ti]["Fc"]).astype(np.float32)
+        pd2 = np.concatenate(tp[ti]["d2"]).astype(np.float32)
+        npk = len(peaks["ipp"])
+        npk_tot += npk
+        if npk == 0:
+            continue
+        fields = dict(delta=np.ascontiguousarray(sl(delta, t)),
+                      etax=np.ascontiguousarray(sl(psi[0], t)), etay=np.ascontiguousarray(sl(psi[1], t)),
+                      etaz=np.ascontiguousarray(sl(psi[2], t)),
+                      eta2x=None if psi2[0] is None else np.ascontiguousarray(sl(psi2[0], t)),
+                      eta2y=None if psi2[1] is None else np.ascontiguousarray(sl(psi2[1], t)),
+                      eta2z=None if psi2[2] is None else np.ascontiguousarray(sl(psi2[2], t)),
+                      lapd=None if lapd is None else np.ascontiguousarray(sl(lapd, t)))
+        ir2min = np.minimum(np.floor((1.75 * pRf / alatt) ** 2), np.floor((40.0 / alatt - 1) ** 2)).astype(np.int64)
+        if cfg.ievol == 1:
+            dx, dy, dz = peaks["x"] - obs[0], peaks["y"] - obs[1], peaks["z"] - obs[2]
+            ZZon = 1.0 + chi_to_z(Om, cfg.Omvac, cfg.h, cfg.z_max + 1.0, np.sqrt(dx * dx + dy * dy + dz * dz))
+            fc_pp = np.array([fsc_of_z(Om, cfg.OmB, cfg.Omvac, cfg.h, z - 1.0) for z in ZZon])
+        else:
+            ZZon = np.full(npk, 1.0 + cfg.z_out)
+            fc_pp = np.full(npk, fcrit_val)
+        res = analyse_peaks(fields, peaks["ipp"], pRf, ir2min, ZZon, fc_pp, alatt, shells, T, nbuff=nbuff,
+                            rmax2rs=cfg.rmax2rs)
+        nf = 33 if cfg.ioutshear >= 1 else 11
+        rec = np.empty((npk, nf), dtype=np.float32)
+        zz = np.empty(npk)
+        nh = L.ora_pack_records(Om, cfg.OmB, cfg.Omvac, cfg.h, npk, _p(peaks["x"]), _p(peaks["y"]),
+                                _p(peaks["z"]), _p(np.ascontiguousarray(pRf)), _p(pFc), _p(pd2), _p(res),
+                                alatt, cfg.ievol, cfg.z_out, cfg.z_max, cfg.cenx, cfg.ceny, cfg.cenz,
+                                cfg.ioutshear, cfg.ilpt, _p(rec), _p(zz))
+        recs.append(rec[:nh])
+    nf = 33 if cfg.ioutshear >= 1 else 11
+    out = np.concatenate(recs) if recs else np.empty((0, nf), np.float32)
+    return out, npk_tot
 
 
 def run_tile(cfg: Config, seed: int, pk_k, pk_p, filters, T: Table) -> np.ndarray:

@@ -56,14 +56,14 @@ void Slot::init(int dev) {
 void Slot::release_buffers() {
   tile.reset();
   for (DevBuf* b : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
-                    &okey2, &oidx, &oidx2, &otmp})
+                    &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd})
     b->release();
 }
 
 size_t Slot::bytes_held() const {
   size_t b = tile ? tile->bytes() : 0;
   for (const DevBuf* d : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool,
-                          &okey, &okey2, &oidx, &oidx2, &otmp})
+                          &okey, &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd})
     b += d->bytes;
   return b;
 }
@@ -442,6 +442,56 @@ int32_t ppb_run_tile_timed(ppb_ctx* ctx, const ppb_tile_params* p, const double*
     PPB_REQUIRE(out->records != nullptr, "records buffer is null");
     copy_out(out->records, o.d_records, (size_t)o.count * o.nfields * 4, ctx->sync.stream);
   }
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_run_multitile(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, int32_t nfilt, int32_t ntile,
+                          const int32_t* tiles, int32_t ntiles, ppb_halo_buf* out) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  PPB_REQUIRE(out != nullptr, "output buffer is null");
+  PPB_REQUIRE(ntiles >= 0 && (ntiles == 0 || tiles != nullptr), "tiles must hold ntiles triples");
+  std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
+  TileOut o;
+  run_multitile_core(ctx, ctx->sync, p, Rf, nfilt, ntile, tiles, ntiles, &o);
+  out->nfields = o.nfields;
+  out->count = o.count;
+  out->npeaks = o.npeaks;
+  out->RTHLmax = o.RTHLmax;
+  if (o.count > out->capacity) return PPB_ERR_CAPACITY;
+  if (o.count > 0) {
+    PPB_REQUIRE(out->records != nullptr, "records buffer is null");
+    copy_out(out->records, o.d_records, (size_t)o.count * o.nfields * 4, ctx->sync.stream);
+  }
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_merge_catalog(ppb_ctx* ctx, const float* records, int64_t n, int32_t nfields, float* out,
+                          int64_t* n_out) {
+  if (!ctx || !n_out || n < 0 || (n > 0 && (!records || !out)) || (nfields != 11 && nfields != 33))
+    return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  *n_out = 0;
+  if (n == 0) return PPB_OK;
+  Slot& sl = ctx->sync;
+  DevBuf din, dout;
+  const size_t bytes = (size_t)n * nfields * 4;
+  const float* d_rec = (const float*)stage_in(din, records, bytes, sl.stream);
+  float* d_out = out;
+  if (!is_device_ptr(out)) {
+    dout.ensure(bytes);
+    d_out = dout.as<float>();
+  }
+  const int64_t m = merge_catalog_device(sl, d_rec, n, nfields, d_out);
+  if (m > 0 && d_out != out) copy_out(out, d_out, (size_t)m * nfields * 4, sl.stream);
+  PPB_CUDA(cudaStreamSynchronize(sl.stream));
+  *n_out = m;
   return PPB_OK;
   PPB_GUARD_END(ctx)
 }

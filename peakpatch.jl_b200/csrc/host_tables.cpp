@@ -374,6 +374,8 @@ double gk15(double Om, double OL, double a, double b, double* err) {
   *err = std::fabs((rk - rg) * hl);
   return rk * hl;
 }
+}  // namespace
+
 double chi_of_z(double Om, double OL, double h, double z) {
   if (z == 0.0) return 0.0;
   std::vector<std::pair<double, double>> st{{0.0, z}};
@@ -392,9 +394,23 @@ double chi_of_z(double Om, double OL, double h, double z) {
   }
   return (2.998e5 / 100.0) * h * tot;
 }
-}  // namespace
 
 // build_chi_to_z (Cosmology.jl:144-148): chi at npts redshifts 0..zmax
+double chi_to_z_host(const std::vector<double>& chis, double zmax, double c) {
+  const int n = (int)chis.size();
+  if (c <= chis[0]) return 0.0;
+  if (c >= chis[n - 1]) return zmax;
+  int lo = 1, hi = n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (chis[mid - 1] <= c) lo = mid; else hi = mid;
+  }
+  const double zl = zmax * (double)(lo - 1) / (double)(n - 1);
+  const double zh = zmax * (double)(hi - 1) / (double)(n - 1);
+  const double fr = (c - chis[lo - 1]) / (chis[hi - 1] - chis[lo - 1]);
+  return zl + fr * (zh - zl);
+}
+
 std::vector<double> make_chi_table(double Om, double OL, double h, double zmax, int npts) {
   std::vector<double> c(npts);
   for (int i = 0; i < npts; i++) {

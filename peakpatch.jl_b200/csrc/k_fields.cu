@@ -303,39 +303,49 @@ __global__ void hermitise_kernel(float2* __restrict__ data, int n, int nbatch) {
 // plain array so the shell gather reads one 32-byte record per cell.
 // Block: 32 x 8 threads over a 32 (a) x 32 (c) tile at fixed b.
 // ---------------------------------------------------------------------------
-__global__ void pack_kernel(float4* __restrict__ aos, const float* __restrict__ delta,
-                            const float* __restrict__ psi, const float* __restrict__ psi2, int n) {
+__global__ void pack_kernel(float4* __restrict__ aos, FieldWindow w, int n) {
   __shared__ float tile[32][33];
   const int b = blockIdx.z;
   const int a0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
-  const int64_t n2 = (int64_t)n * n, N = n2 * n;
-  // load delta(c, a, b) for c in [c0, c0+32), a in [a0, a0+32): lin = c + n a + n^2 b
+  const int64_t n2 = (int64_t)n * n;
+  auto src = [&](int x, int y, int z) { return w.off + x + w.py * y + w.pz * z; };
+  // load delta(c, a, b) for c in [c0, c0+32), a in [a0, a0+32)
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
     const int a = a0 + r, c = c0 + threadIdx.x;
-    if (a < n && c < n) tile[r][threadIdx.x] = delta[c + (int64_t)n * a + n2 * b];
+    if (a < n && c < n) tile[r][threadIdx.x] = w.delta[src(c, a, b)];
   }
   __syncthreads();
   for (int r = threadIdx.y; r < 32; r += blockDim.y) {
     const int a = a0 + threadIdx.x, c = c0 + r;
     if (a >= n || c >= n) continue;
+    const int64_t g = src(a, b, c);
     const int64_t lin = a + (int64_t)n * b + n2 * c;
     const float dT = tile[threadIdx.x][r];
     float4 v0, v1;
-    v0.x = delta[lin];
+    v0.x = w.delta[g];
     v0.y = dT;
-    v0.z = psi[lin];
-    v0.w = psi[N + lin];
-    v1.x = psi[2 * N + lin];
-    if (psi2) {
-      v1.y = psi2[lin];
-      v1.z = psi2[N + lin];
-      v1.w = psi2[2 * N + lin];
+    v0.z = w.psi[g];
+    v0.w = w.psi[w.cs + g];
+    v1.x = w.psi[2 * w.cs + g];
+    if (w.psi2) {
+      v1.y = w.psi2[g];
+      v1.z = w.psi2[w.cs + g];
+      v1.w = w.psi2[2 * w.cs + g];
     } else {
       v1.y = v1.z = v1.w = 0.f;
     }
     aos[2 * lin] = v0;
     aos[2 * lin + 1] = v1;
   }
+}
+
+// dst (n^3, local) = a cubic window of a larger array
+__global__ void extract_kernel(float* __restrict__ dst, const float* __restrict__ src, int64_t off, int64_t py,
+                               int64_t pz, int n) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y, z = blockIdx.z;
+  if (x >= n) return;
+  dst[x + (int64_t)n * (y + (int64_t)n * z)] = src[off + x + py * y + pz * z];
 }
 
 // ---------------------------------------------------------------------------
@@ -347,19 +357,18 @@ __global__ void pack_kernel(float4* __restrict__ aos, const float* __restrict__ 
 // sorting the (filter, flat index) keys.
 // ---------------------------------------------------------------------------
 __global__ void peakfind_kernel(const float* __restrict__ ds, const float* __restrict__ ls,
-                                uint8_t* __restrict__ mask, int n1, int n2, int n3, int nbuff, float fcrit,
-                                int fidx, PeakBuf pb) {
+                                uint8_t* __restrict__ mask, int n1, int n2, int n3, int64_t py, int64_t pz,
+                                int nbuff, float fcrit, unsigned long long keyhi, PeakBuf pb) {
   const int i = nbuff + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = nbuff + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = nbuff + blockIdx.z;
-  const int64_t n12 = (int64_t)n1 * n2;
   bool peak = false;
-  int64_t lin = 0;
+  int64_t g = 0;
   float ff = 0.f;
   if (i < n1 - nbuff && j < n2 - nbuff && k < n3 - nbuff) {
-    lin = i + (int64_t)n1 * j + n12 * k;
-    ff = ds[lin];
-    if (mask[lin] != 1 && !(ff < fcrit)) {
+    g = i + py * j + pz * k;
+    ff = ds[g];
+    if (mask[g] != 1 && !(ff < fcrit)) {
       peak = true;
 #pragma unroll
       for (int dk = -1; dk <= 1; dk++)
@@ -367,7 +376,7 @@ __global__ void peakfind_kernel(const float* __restrict__ ds, const float* __res
         for (int dj = -1; dj <= 1; dj++)
 #pragma unroll
           for (int di = -1; di <= 1; di++) {
-            const float v = __ldg(ds + lin + di + (int64_t)n1 * dj + n12 * dk);
+            const float v = __ldg(ds + g + di + py * dj + pz * dk);
             if (ff < v) peak = false;
           }
     }
@@ -382,13 +391,14 @@ __global__ void peakfind_kernel(const float* __restrict__ ds, const float* __res
   if (wl == leader) base = atomicAdd(pb.count, __popc(ball));
   base = __shfl_sync(full, base, leader);
   if (peak) {
-    mask[lin] = 1;
+    mask[g] = 1;
     const int slot = base + __popc(ball & ((1u << wl) - 1u));
     if (slot < pb.cap) {
-      pb.keys[slot] = ((unsigned long long)fidx << 40) | (unsigned long long)lin;
+      const int64_t lin = i + (int64_t)n1 * j + (int64_t)n1 * n2 * k;
+      pb.keys[slot] = (keyhi << 40) | (unsigned long long)lin;
       pb.vals[slot] = (uint32_t)slot;
       pb.ff[slot] = ff;
-      pb.lap[slot] = ls ? ls[lin] : 0.f;
+      pb.lap[slot] = ls ? ls[g] : 0.f;
     }
   }
 }
@@ -399,13 +409,14 @@ __global__ void peakfind_kernel(const float* __restrict__ ds, const float* __res
 // peakfind_kernel; the neighbours of a candidate are read one by one (few
 // cells reach fcrit).
 __global__ void peakfind4_kernel(const float* __restrict__ ds, const float* __restrict__ ls,
-                                 uint8_t* __restrict__ mask, int n1, int n2, int n3, int nbuff, float fcrit,
-                                 int fidx, PeakBuf pb) {
+                                 uint8_t* __restrict__ mask, int n1, int n2, int n3, int64_t py, int64_t pz,
+                                 int nbuff, float fcrit, unsigned long long keyhi, PeakBuf pb) {
   const int i0 = nbuff + 4 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int j = nbuff + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = nbuff + blockIdx.z;
-  const int64_t n12 = (int64_t)n1 * n2;
-  const int64_t lin0 = i0 + (int64_t)n1 * j + n12 * k;
+  const int64_t n12 = pz;
+  const int64_t lin0 = i0 + py * j + pz * k;
+  const int64_t loc0 = i0 + (int64_t)n1 * j + (int64_t)n1 * n2 * k;
   bool pk[4] = {false, false, false, false};
   float f[4] = {0.f, 0.f, 0.f, 0.f};
   if (i0 < n1 - nbuff && j < n2 - nbuff && k < n3 - nbuff) {
@@ -422,7 +433,7 @@ __global__ void peakfind4_kernel(const float* __restrict__ ds, const float* __re
         for (int dj = -1; dj <= 1; dj++)
 #pragma unroll
           for (int di = -1; di <= 1; di++) {
-            const float w = __ldg(ds + lin + di + (int64_t)n1 * dj + n12 * dk);
+            const float w = __ldg(ds + lin + di + py * dj + n12 * dk);
             if (f[u] < w) peak = false;
           }
       pk[u] = peak;
@@ -449,7 +460,7 @@ __global__ void peakfind4_kernel(const float* __restrict__ ds, const float* __re
     const int64_t lin = lin0 + u;
     mask[lin] = 1;
     if (slot < pb.cap) {
-      pb.keys[slot] = ((unsigned long long)fidx << 40) | (unsigned long long)lin;
+      pb.keys[slot] = (keyhi << 40) | (unsigned long long)(loc0 + u);
       pb.vals[slot] = (uint32_t)slot;
       pb.ff[slot] = f[u];
       pb.lap[slot] = ls ? ls[lin] : 0.f;
@@ -532,26 +543,32 @@ void launch_hermitise(Launch L, float2* data, int n, int nbatch) {
   PPB_LAUNCHED(*L.count);
 }
 
-void launch_pack(Launch L, float4* aos, const float* delta, const float* psi, const float* psi2, int n) {
+void launch_pack(Launch L, float4* aos, const FieldWindow& w, int n) {
   dim3 grid((n + 31) / 32, (n + 31) / 32, n);
-  pack_kernel<<<grid, dim3(32, 8), 0, L.s>>>(aos, delta, psi, psi2, n);
+  pack_kernel<<<grid, dim3(32, 8), 0, L.s>>>(aos, w, n);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_extract(Launch L, float* dst, const float* src, int64_t off, int64_t py, int64_t pz, int n) {
+  extract_kernel<<<dim3((unsigned)((n + 127) / 128), (unsigned)n, (unsigned)n), 128, 0, L.s>>>(dst, src, off, py, pz,
+                                                                                              n);
   PPB_LAUNCHED(*L.count);
 }
 
 void launch_peakfind(Launch L, const float* ds, const float* ls, uint8_t* mask, int n1, int n2, int n3,
-                     int nbuff, float fcrit, int fidx, PeakBuf pb) {
+                     int64_t py, int64_t pz, int nbuff, float fcrit, unsigned long long keyhi, PeakBuf pb) {
   const int w1 = n1 - 2 * nbuff, w2 = n2 - 2 * nbuff, w3 = n3 - 2 * nbuff;
   if (w1 <= 0 || w2 <= 0 || w3 <= 0) return;
   dim3 block(32, 4);
-  const bool vec = n1 % 4 == 0 && nbuff % 4 == 0 && reinterpret_cast<uintptr_t>(ds) % 16 == 0 &&
-                   reinterpret_cast<uintptr_t>(mask) % 4 == 0;
+  const bool vec = n1 % 4 == 0 && nbuff % 4 == 0 && py % 4 == 0 && pz % 4 == 0 &&
+                   reinterpret_cast<uintptr_t>(ds) % 16 == 0 && reinterpret_cast<uintptr_t>(mask) % 4 == 0;
   if (vec) {
     const int q1 = (w1 + 3) / 4;
     dim3 grid((q1 + 31) / 32, (w2 + 3) / 4, w3);
-    peakfind4_kernel<<<grid, block, 0, L.s>>>(ds, ls, mask, n1, n2, n3, nbuff, fcrit, fidx, pb);
+    peakfind4_kernel<<<grid, block, 0, L.s>>>(ds, ls, mask, n1, n2, n3, py, pz, nbuff, fcrit, keyhi, pb);
   } else {
     dim3 grid((w1 + 31) / 32, (w2 + 3) / 4, w3);
-    peakfind_kernel<<<grid, block, 0, L.s>>>(ds, ls, mask, n1, n2, n3, nbuff, fcrit, fidx, pb);
+    peakfind_kernel<<<grid, block, 0, L.s>>>(ds, ls, mask, n1, n2, n3, py, pz, nbuff, fcrit, keyhi, pb);
   }
   PPB_LAUNCHED(*L.count);
 }

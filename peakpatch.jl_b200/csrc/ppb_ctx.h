@@ -53,6 +53,7 @@ struct Slot {
   DevBuf g_a, g_D, g_f, chi;                        // growth / chi tables of the run
   DevBuf stage, counters, ctl, hdr, geo, pool;      // shell stage
   DevBuf okey, okey2, oidx, oidx2, otmp;            // spatial gather order
+  DevBuf tcen, tcount, t_aos, t_lapd;               // multi-tile: centres, peaks per tile, tile fields
   int gather_bps[2][2] = {{0, 0}, {0, 0}};          // gather blocks per SM by [comp][adaptive]
   double rows_per_peak[2] = {0.0, 0.0};             // pool rows per peak seen last, by adaptive
   ShellStats last_shell{};
@@ -129,6 +130,10 @@ namespace ppb {
 // device (o->d_records) until the slot's next run.  The caller holds
 // ctx->sh.mu shared.
 void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf, int nfilt, TileOut* o);
+// run_multitile (src/MultiTile.jl:108-418) on one slot; tiles = ntiles
+// (it, jt, kt) triples, 1-based, or null for every tile of the ntile^3 grid
+void run_multitile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf, int nfilt, int ntile,
+                        const int32_t* tiles, int ntiles, TileOut* o);
 void check_params(const ppb_tile_params* p, const double* Rf, int nfilt);
 // device bytes a run of this grid size holds at most (admission estimate)
 uint64_t tile_footprint(const ppb_tile_params* p);
@@ -138,6 +143,9 @@ void copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);
 bool is_device_ptr(const void* p);
 // device copy of a caller buffer (host or device); returns a device pointer
 const void* stage_in(DevBuf& buf, const void* src, size_t bytes, cudaStream_t s);
+// merge_catalog on device records (n x nf floats); writes the survivors in
+// index order to d_out (capacity n) and returns their number (k_merge.cu)
+int64_t merge_catalog_device(Slot& sl, const float* d_rec, int64_t n, int nf, float* d_out);
 // serving (serve.cu)
 void server_stop(ppb_ctx* ctx);
 }  // namespace ppb

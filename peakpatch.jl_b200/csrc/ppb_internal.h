@@ -135,6 +135,10 @@ GrowthTable make_growth_table(double Om, double OB, double OL, double h);
 void dlinear_ab(const GrowthTable& G, double ai, double* Dl, double* HD, double* Da);
 double fsc_of_z(const GrowthTable& G, double z);
 std::vector<double> make_chi_table(double Om, double OL, double h, double zmax, int npts);
+// comoving distance to z (Mpc/h) and its inverse on a make_chi_table table
+// spanning [0, zmax] (chi_to_z, Cosmology.jl:155-169)
+double chi_of_z(double Om, double OL, double h, double z);
+double chi_to_z_host(const std::vector<double>& chis, double zmax, double c);
 
 // device view of the tables used per peak (lightcone ZZon / fcrit / D(z))
 struct DevCosmo {
@@ -260,7 +264,18 @@ void launch_window_tables(Launch L, float* tab, int n, double boxsize, const dou
 void launch_window(Launch L, const float2* dk, float2* out0, float2* out1, int n, const float* tab,
                    double post_scale);
 void launch_hermitise(Launch L, float2* data, int n, int nbatch);
-void launch_pack(Launch L, float4* aos, const float* delta, const float* psi, const float* psi2, int n);
+// a cubic window of fields on a larger grid: element (x, y, z) of the window
+// is at off + x + py y + pz z; the psi components are cs apart
+struct FieldWindow {
+  const float* delta;
+  const float* psi;
+  const float* psi2;   // may be null
+  int64_t off, py, pz, cs;
+};
+// packed gather records (two float4 per cell) of an n^3 window
+void launch_pack(Launch L, float4* aos, const FieldWindow& w, int n);
+// dst (n^3) = the window of src at off with pitches py, pz
+void launch_extract(Launch L, float* dst, const float* src, int64_t off, int64_t py, int64_t pz, int n);
 
 struct PeakBuf {
   unsigned long long* keys;   // (filter << 40) | lin
@@ -270,8 +285,10 @@ struct PeakBuf {
   int* count;
   int64_t cap;
 };
+// peaks of the n1 x n2 x n3 window at ds (pitches py, pz; ls and mask share
+// them); key = keyhi << 40 | (window-local flat index)
 void launch_peakfind(Launch L, const float* ds, const float* ls, uint8_t* mask, int n1, int n2, int n3,
-                     int nbuff, float fcrit, int fidx, PeakBuf pb);
+                     int64_t py, int64_t pz, int nbuff, float fcrit, unsigned long long keyhi, PeakBuf pb);
 
 // Shell stage = five launches on one stream:
 //  geo      (one thread per peak): per-peak shell geometry

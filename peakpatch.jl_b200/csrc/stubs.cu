@@ -83,7 +83,8 @@ int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n
     DevBuf lapdummy;
     lapdummy.ensure(cap * 4);
     pb.lap = lapdummy.as<float>();
-    launch_peakfind(Launch{s, &ctx->sync.launches}, dd, nullptr, dm, n1, n2, n3, nbuff, fcrit, 0, pb);
+    launch_peakfind(Launch{s, &ctx->sync.launches}, dd, nullptr, dm, n1, n2, n3, n1, (int64_t)n1 * n2, nbuff, fcrit,
+                    0ull, pb);
     int c = 0;
     PPB_CUDA(cudaMemcpyAsync(&c, cnt.p, 4, cudaMemcpyDeviceToHost, s));
     PPB_CUDA(cudaStreamSynchronize(s));
@@ -174,7 +175,7 @@ int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, c
     }
     const float* dl = lapd ? (const float*)stage_in(st_lapd, lapd, N * 4, s) : nullptr;
     aos.ensure(N * 32);
-    launch_pack(L, aos.as<float4>(), dd, st_psi.as<float>(), dpsi2, n);
+    launch_pack(L, aos.as<float4>(), FieldWindow{dd, st_psi.as<float>(), dpsi2, 0, n, (int64_t)n * n, N}, n);
     const int64_t* dipp = (const int64_t*)stage_in(d_ipp, ipp, npk * 8, s);
     const double* dRf = (const double*)stage_in(d_Rf, Rf, npk * 8, s);
     const int64_t* dir2 = (const int64_t*)stage_in(d_ir2in, ir2min, npk * 8, s);

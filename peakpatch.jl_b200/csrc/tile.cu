@@ -86,6 +86,8 @@ struct PrepArgs {
   double z_out, fcrit0;
   double obs[3];
   DevCosmo C;
+  int fbits;                 // key = ((tile << fbits | filter) << 40) | window-local flat index
+  const double* tcen;        // 3 per tile: tile centre (null: all zero)
   int64_t* lin;
   double* Rf;
   int32_t* ir2;
@@ -101,12 +103,17 @@ __global__ void prep_kernel(PrepArgs a) {
   if (q >= a.npk) return;
   const unsigned long long key = a.keys[q];
   const uint32_t slot = a.vals[q];
-  const int f = (int)(key >> 40);
+  const unsigned long long hi = key >> 40;
+  const int f = (int)(hi & ((1ull << a.fbits) - 1));
+  const int t = (int)(hi >> a.fbits);
   const int64_t lin = (int64_t)(key & ((1ull << 40) - 1));
   const int n = a.n;
   const int i = (int)(lin % n) + 1, j = (int)((lin / n) % n) + 1, k = (int)(lin / ((int64_t)n * n)) + 1;
   const double cen = 0.5 * (n + 1);
-  const double x = a.alatt * (i - cen), y = a.alatt * (j - cen), z = a.alatt * (k - cen);
+  // x = xbx + alatt (i - (n+1)/2) (PeakFind.jl:350-425; xbx = tile centre, 0 for run_tile)
+  const double bx = a.tcen ? a.tcen[3 * t] : 0.0, by = a.tcen ? a.tcen[3 * t + 1] : 0.0,
+               bz = a.tcen ? a.tcen[3 * t + 2] : 0.0;
+  const double x = bx + a.alatt * (i - cen), y = by + a.alatt * (j - cen), z = bz + a.alatt * (k - cen);
   a.lin[q] = lin;
   a.Rf[q] = a.fRf[f];
   a.ir2[q] = a.fir2[f];
@@ -207,6 +214,11 @@ __global__ void record_kernel(RecArgs a) {
   }
 }
 
+__global__ void tile_count_kernel(const unsigned long long* keys, int npk, int shift, int* counts) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < npk) atomicAdd(counts + (int)(keys[q] >> shift), 1);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -241,7 +253,6 @@ void TileRes::setup(int nn, cudaStream_t s) {
   psi.ensure(3 * N * 4);
   psi2.ensure(3 * N * 4);
   lapd.ensure(N * 4);
-  aos.ensure(N * 32);
   kw.ensure(6 * M * 8);
   rw.ensure(6 * N * 4);
   mask.ensure(N);
@@ -316,52 +327,79 @@ uint64_t tile_footprint(const ppb_tile_params* p) {
   return fields + N * 120 + ((uint64_t)64 << 20);
 }
 
-void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf_in, int nfilt, TileOut* o) {
-  check_params(p, Rf_in, nfilt);
-  PPB_REQUIRE(ctx->sh.pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
-  PPB_REQUIRE(ctx->sh.has_tab, "collapse table not set (ppb_set_collapse_table)");
-  cudaStream_t s = sl.stream;
-  Launch L{s, &sl.launches};
-  const int n = p->n;
-  const double box = p->boxsize, alatt = box / n;
-  const double Om = p->Omx + p->OmB;
-  const int64_t N = (int64_t)n * n * n, M = (int64_t)(n / 2 + 1) * n * n;
-  const bool plain = p->plain != 0;
+namespace {
 
-  // ---- phase 0 (host) ----
-  std::vector<double> Rf(Rf_in, Rf_in + nfilt);
-  std::stable_sort(Rf.begin(), Rf.end(), [](double a, double b) { return a > b; });
-  const GrowthTable& G = ctx->growth(Om, p->OmB, p->Omvac, p->h);
-  const double fcrit_val = fsc_of_z(G, p->z_out);
-  const float fcrit = (float)fcrit_val;
-  const int nhunt = std::min(p->nbuff - 1, (int)std::floor(Rf[0] * 1.75 / alatt));
-  PPB_REQUIRE(nhunt >= 1, "nhunt = min(nbuff-1, floor(1.75 Rfmax/alatt)) must be >= 1");
-  ShellTable& shells = ctx->shell_table(nhunt, s);
+// host state of one run shared by the phases
+struct Run {
+  ppb_ctx* ctx;
+  Slot* sl;
+  const ppb_tile_params* p;
+  cudaStream_t s;
+  Launch L;
+  double Om, alatt;
+  bool plain, want_lap;
+  std::vector<double> Rf;   // descending
+  int nfilt, fbits;
+  const GrowthTable* G;
+  double fcrit_val;
+  int nhunt;
+  ShellTable* shells;
+  DevCosmo C;
+};
+
+// a peak-search window: a tile of nm^3 cells at `off` in the field grid
+struct Win {
+  int64_t off;
+  float fcrit;
+};
+
+void setup_run(Run& r, ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf_in, int nfilt,
+               double alatt) {
+  r.ctx = ctx;
+  r.sl = &sl;
+  r.p = p;
+  r.s = sl.stream;
+  r.L = Launch{sl.stream, &sl.launches};
+  r.Om = p->Omx + p->OmB;
+  r.alatt = alatt;
+  r.plain = p->plain != 0;
+  r.want_lap = p->ioutshear >= 1;
+  r.Rf.assign(Rf_in, Rf_in + nfilt);
+  std::stable_sort(r.Rf.begin(), r.Rf.end(), [](double a, double b) { return a > b; });
+  r.nfilt = nfilt;
+  r.fbits = 1;
+  while ((1 << r.fbits) < nfilt) r.fbits++;
+  r.G = &ctx->growth(r.Om, p->OmB, p->Omvac, p->h);
+  r.fcrit_val = fsc_of_z(*r.G, p->z_out);
+  r.nhunt = std::min(p->nbuff - 1, (int)std::floor(r.Rf[0] * 1.75 / alatt));
+  PPB_REQUIRE(r.nhunt >= 1, "nhunt = min(nbuff-1, floor(1.75 Rfmax/alatt)) must be >= 1");
+  r.shells = &ctx->shell_table(r.nhunt, r.s);
   std::vector<int32_t> fir2(nfilt);
   for (int f = 0; f < nfilt; f++)
-    fir2[f] = (int32_t)std::min(std::floor((1.75 * Rf[f] / alatt) * (1.75 * Rf[f] / alatt)),
+    fir2[f] = (int32_t)std::min(std::floor((1.75 * r.Rf[f] / alatt) * (1.75 * r.Rf[f] / alatt)),
                                 std::floor((40.0 / alatt - 1) * (40.0 / alatt - 1)));
-  DevCosmo C = ctx->dev_cosmo(sl, G, Om, p->Omvac, p->h, p->ievol == 1 ? p->z_max + 1.0 : 0.0, p->ievol == 1);
+  r.C = ctx->dev_cosmo(sl, *r.G, r.Om, p->Omvac, p->h, p->ievol == 1 ? p->z_max + 1.0 : 0.0, p->ievol == 1);
   sl.filt_Rf.ensure(nfilt * 8);
   sl.filt_ir2.ensure(nfilt * 4);
-  PPB_CUDA(cudaMemcpyAsync(sl.filt_Rf.p, Rf.data(), nfilt * 8, cudaMemcpyHostToDevice, s));
-  PPB_CUDA(cudaMemcpyAsync(sl.filt_ir2.p, fir2.data(), nfilt * 4, cudaMemcpyHostToDevice, s));
+  PPB_CUDA(cudaMemcpyAsync(sl.filt_Rf.p, r.Rf.data(), nfilt * 8, cudaMemcpyHostToDevice, r.s));
+  PPB_CUDA(cudaMemcpyAsync(sl.filt_ir2.p, fir2.data(), nfilt * 4, cudaMemcpyHostToDevice, r.s));
+}
 
-  TileRes& T = sl.tile_for(n);
-  T.setup(n, s);
-  if (T.cap == 0) T.ensure_peaks(std::max<int64_t>(1 << 16, std::min<int64_t>(N / 64, 1 << 22)));
-
-  cudaEvent_t* ev = sl.stage_ev;
-  PPB_CUDA(cudaEventRecord(ev[0], s));
+// phase 1 (Pipeline.jl:90-140, MultiTile.jl:157-194): Threefry noise -> R2C
+// -> sqrt(P) -> C2R = delta; delta_k = R2C(delta), projected Hermitian;
+// 1LPT, 2LPT and the Laplacian field, all on the n^3 grid of `box`
+void fields_phase(Run& r, TileRes& T, int n, double box) {
+  const ppb_tile_params* p = r.p;
+  const Launch& L = r.L;
+  const int64_t N = (int64_t)n * n * n, M = (int64_t)(n / 2 + 1) * n * n;
   const double inv_n3 = 1.0 / (double)N;
   float2* dkp = T.dk.as<float2>();
   float2* kw = T.kw.as<float2>();
   float* rw = T.rw.as<float>();
-
-  // ---- phase 1: fields ----
-  launch_noise(L, T.rw.as<float>(), n, p->seed);
-  PPB_CUFFT(cufftExecR2C(T.r2c, T.rw.as<cufftReal>(), (cufftComplex*)kw));
-  launch_convolve(L, kw, n, box, ctx->sh.pk_lk.as<double>(), ctx->sh.pk_lp.as<double>(), ctx->sh.pk_n,
+  const Shared& sh = r.ctx->sh;
+  launch_noise(L, rw, n, p->seed);
+  PPB_CUFFT(cufftExecR2C(T.r2c, rw, (cufftComplex*)kw));
+  launch_convolve(L, kw, n, box, sh.pk_lk.as<double>(), sh.pk_lp.as<double>(), sh.pk_n,
                   p->pk_scale > 0.0 ? p->pk_scale : 1.0, inv_n3);
   launch_hermitise(L, kw, n, 1);
   PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)kw, T.delta.as<cufftReal>()));
@@ -372,7 +410,7 @@ void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const doubl
   // 1LPT
   launch_lpt1(L, dkp, kw, n, box, inv_n3);
   launch_hermitise(L, kw, n, 3);
-  if (plain) {
+  if (r.plain) {
     for (int c = 0; c < 3; c++)
       PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)(kw + c * M), T.psi.as<cufftReal>() + c * N));
   } else {
@@ -382,7 +420,7 @@ void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const doubl
   if (p->ilpt >= 2) {
     launch_phi(L, dkp, kw, n, box, inv_n3);
     launch_hermitise(L, kw, n, 6);
-    if (plain) {
+    if (r.plain) {
       for (int c = 0; c < 6; c++) PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)(kw + c * M), rw + c * N));
     } else {
       PPB_CUFFT(cufftExecC2R(T.c2r6, (cufftComplex*)kw, rw));
@@ -391,7 +429,7 @@ void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const doubl
     PPB_CUFFT(cufftExecR2C(T.r2c, T.lapd.as<cufftReal>(), (cufftComplex*)kw));
     launch_lpt2(L, kw, kw + M, n, box, inv_n3);
     launch_hermitise(L, kw + M, n, 3);
-    if (plain) {
+    if (r.plain) {
       for (int c = 0; c < 3; c++)
         PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)(kw + (1 + c) * M), T.psi2.as<cufftReal>() + c * N));
     } else {
@@ -399,152 +437,367 @@ void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const doubl
     }
   }
   // Laplacian field (Pipeline.jl:35-51): irfft(k^2 delta_k) / n^3
-  const bool want_lap = p->ioutshear >= 1;
-  if (want_lap) {
+  if (r.want_lap) {
     launch_lapd(L, dkp, kw, n, box, (float)(inv_n3 * inv_n3));
     launch_hermitise(L, kw, n, 1);
     PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)kw, T.lapd.as<cufftReal>()));
   }
-  launch_pack(L, T.aos.as<float4>(), T.delta.as<float>(), T.psi.as<float>(),
-              p->ilpt >= 2 ? T.psi2.as<float>() : nullptr, n);
-  PPB_CUDA(cudaEventRecord(ev[1], s));
+}
 
-  // ---- phase 2: filter bank and peaks ----
+// phase 2 (Pipeline.jl:144-196, MultiTile.jl:218-275): per filter, largest
+// first, the smoothed field (and its k^2-weighted twin) on the n^3 grid, then
+// the peak search in every window (mask shared: windows search disjoint
+// cores).  Keys (window, filter, window-local index) restore the reference's
+// order.  Returns the number of peaks in T's peak buffers.
+int64_t peaks_phase(Run& r, TileRes& T, int n, double box, const std::vector<Win>& wins, int nm) {
+  const ppb_tile_params* p = r.p;
+  const Launch& L = r.L;
+  const int64_t N = (int64_t)n * n * n, M = (int64_t)(n / 2 + 1) * n * n;
+  const double inv_n3 = 1.0 / (double)N;
+  float2* dkp = T.dk.as<float2>();
+  float2* kw = T.kw.as<float2>();
+  float* rw = T.rw.as<float>();
   const int qn = window_table_size(n);
-  T.wtab.ensure((size_t)nfilt * 2 * qn * sizeof(float));
-  launch_window_tables(L, T.wtab.as<float>(), n, box, sl.filt_Rf.as<double>(), nfilt, p->wsmooth, want_lap);
+  T.wtab.ensure((size_t)r.nfilt * 2 * qn * sizeof(float));
+  launch_window_tables(L, T.wtab.as<float>(), n, box, r.sl->filt_Rf.as<double>(), r.nfilt, p->wsmooth, r.want_lap);
   int64_t npk = 0;
   for (int attempt = 0; attempt < 2; attempt++) {
-    PPB_CUDA(cudaMemsetAsync(T.mask.p, 0, N, s));
-    PPB_CUDA(cudaMemsetAsync(T.count.p, 0, 64, s));
+    PPB_CUDA(cudaMemsetAsync(T.mask.p, 0, N, r.s));
+    PPB_CUDA(cudaMemsetAsync(T.count.p, 0, 64, r.s));
     PeakBuf pb{T.keys.as<unsigned long long>(), T.vals.as<uint32_t>(), T.ff.as<float>(), T.lap.as<float>(),
                T.count.as<int>(), T.cap};
-    for (int f = 0; f < nfilt; f++) {
-      float2* o1 = want_lap ? kw + M : nullptr;
+    for (int f = 0; f < r.nfilt; f++) {
+      float2* o1 = r.want_lap ? kw + M : nullptr;
       launch_window(L, dkp, kw, o1, n, T.wtab.as<float>() + (size_t)f * 2 * qn, inv_n3);
-      if (want_lap && !plain) {
+      if (r.want_lap && !r.plain) {
         PPB_CUFFT(cufftExecC2R(T.c2r2, (cufftComplex*)kw, rw));
       } else {
         PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)kw, rw));
-        if (want_lap) PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)(kw + M), rw + N));
+        if (r.want_lap) PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)(kw + M), rw + N));
       }
-      launch_peakfind(L, rw, want_lap ? rw + N : nullptr, T.mask.as<uint8_t>(), n, n, n, p->nbuff, fcrit, f, pb);
+      for (size_t t = 0; t < wins.size(); t++) {
+        const Win& w = wins[t];
+        launch_peakfind(L, rw + w.off, r.want_lap ? rw + N + w.off : nullptr, T.mask.as<uint8_t>() + w.off, nm, nm,
+                        nm, n, (int64_t)n * n, p->nbuff, w.fcrit,
+                        ((unsigned long long)t << r.fbits) | (unsigned long long)f, pb);
+      }
     }
     int cnt = 0;
-    PPB_CUDA(cudaMemcpyAsync(&cnt, T.count.p, 4, cudaMemcpyDeviceToHost, s));
-    PPB_CUDA(cudaStreamSynchronize(s));
+    PPB_CUDA(cudaMemcpyAsync(&cnt, T.count.p, 4, cudaMemcpyDeviceToHost, r.s));
+    PPB_CUDA(cudaStreamSynchronize(r.s));
     npk = cnt;
     if (npk <= T.cap) break;
     PPB_REQUIRE(attempt == 0, "peak capacity exceeded twice");
     T.ensure_peaks((int64_t)(npk * 1.25) + 1024);   // grow and redo the filter bank
   }
-  PPB_CUDA(cudaEventRecord(ev[2], s));
+  return npk;
+}
 
-  // ---- sort peaks to (filter, scan order), per-peak parameters ----
-  int fbits = 1;
-  while ((1 << fbits) < nfilt) fbits++;
-  if (npk > 0) {
-    size_t tb = T.tmp.bytes;
-    PPB_CUDA(cub::DeviceRadixSort::SortPairs(T.tmp.p, tb, T.keys.as<unsigned long long>(),
-                                             T.keys_s.as<unsigned long long>(), T.vals.as<uint32_t>(),
-                                             T.vals_s.as<uint32_t>(), (int)npk, 0, 40 + fbits, s));
-    sl.launches++;
-    PrepArgs pa{};
-    pa.keys = T.keys_s.as<unsigned long long>();
-    pa.vals = T.vals_s.as<uint32_t>();
-    pa.ff = T.ff.as<float>();
-    pa.lap = T.lap.as<float>();
-    pa.npk = (int)npk;
-    pa.n = n;
-    pa.alatt = alatt;
-    pa.fRf = sl.filt_Rf.as<double>();
-    pa.fir2 = sl.filt_ir2.as<int32_t>();
-    pa.ievol = p->ievol;
-    pa.z_out = p->z_out;
-    pa.fcrit0 = fcrit_val;
-    pa.obs[0] = p->cenx; pa.obs[1] = p->ceny; pa.obs[2] = p->cenz;
-    pa.C = C;
-    pa.lin = T.p_lin.as<int64_t>();
-    pa.Rf = T.p_Rf.as<double>();
-    pa.ir2 = T.p_ir2.as<int32_t>();
-    pa.Z = T.p_Z.as<double>();
-    pa.fc = T.p_fc.as<double>();
-    pa.FcRf = T.p_FcRf.as<float>();
-    pa.d2Rf = T.p_d2Rf.as<float>();
-    pa.pos = T.p_pos.as<double>();
-    prep_kernel<<<(unsigned)((npk + 255) / 256), 256, 0, s>>>(pa);
-    PPB_LAUNCHED(sl.launches);
-  }
+// sort the peaks to (window, filter, scan order) and derive the per-peak
+// parameters; tcen (device, 3 per window) gives the window centres
+void prep_phase(Run& r, TileRes& T, int64_t npk, int nm, int nwin, const double* tcen) {
+  if (npk <= 0) return;
+  int tbits = 0;
+  while ((1 << tbits) < nwin) tbits++;
+  size_t tb = T.tmp.bytes;
+  PPB_CUDA(cub::DeviceRadixSort::SortPairs(T.tmp.p, tb, T.keys.as<unsigned long long>(),
+                                           T.keys_s.as<unsigned long long>(), T.vals.as<uint32_t>(),
+                                           T.vals_s.as<uint32_t>(), (int)npk, 0, 40 + r.fbits + tbits, r.s));
+  r.sl->launches++;
+  const ppb_tile_params* p = r.p;
+  PrepArgs pa{};
+  pa.keys = T.keys_s.as<unsigned long long>();
+  pa.vals = T.vals_s.as<uint32_t>();
+  pa.ff = T.ff.as<float>();
+  pa.lap = T.lap.as<float>();
+  pa.npk = (int)npk;
+  pa.n = nm;
+  pa.alatt = r.alatt;
+  pa.fRf = r.sl->filt_Rf.as<double>();
+  pa.fir2 = r.sl->filt_ir2.as<int32_t>();
+  pa.ievol = p->ievol;
+  pa.z_out = p->z_out;
+  pa.fcrit0 = r.fcrit_val;
+  pa.obs[0] = p->cenx; pa.obs[1] = p->ceny; pa.obs[2] = p->cenz;
+  pa.C = r.C;
+  pa.fbits = r.fbits;
+  pa.tcen = tcen;
+  pa.lin = T.p_lin.as<int64_t>();
+  pa.Rf = T.p_Rf.as<double>();
+  pa.ir2 = T.p_ir2.as<int32_t>();
+  pa.Z = T.p_Z.as<double>();
+  pa.fc = T.p_fc.as<double>();
+  pa.FcRf = T.p_FcRf.as<float>();
+  pa.d2Rf = T.p_d2Rf.as<float>();
+  pa.pos = T.p_pos.as<double>();
+  prep_kernel<<<(unsigned)((npk + 255) / 256), 256, 0, r.s>>>(pa);
+  PPB_LAUNCHED(r.sl->launches);
+}
 
-  // ---- phase 4: shells ----
+// phase 4 (Pipeline.jl:200-240) for peaks [p0, p1) on an nm^3 window whose
+// packed records are aos (and Laplacian lapd)
+void shells_phase(Run& r, TileRes& T, int64_t p0, int64_t p1, int nm, const float4* aos, const float* lapd,
+                  ShellStats* acc) {
+  if (p1 <= p0) return;
+  ShellArgs a = r.ctx->shell_args(*r.sl, *r.shells, nm, r.alatt, aos, lapd);
+  a.pk = PeakParams{T.p_lin.as<int64_t>() + p0, T.p_Rf.as<double>() + p0, T.p_ir2.as<int32_t>() + p0,
+                    T.p_Z.as<double>() + p0, T.p_fc.as<double>() + p0};
+  a.npk = p1 - p0;
+  a.out = T.res.as<double>() + p0 * RES_N;
   ShellStats st{};
-  if (npk > 0) {
-    ShellArgs a = ctx->shell_args(sl, shells, n, alatt, T.aos.as<float4>(), want_lap ? T.lapd.as<float>() : nullptr);
-    a.pk = PeakParams{T.p_lin.as<int64_t>(), T.p_Rf.as<double>(), T.p_ir2.as<int32_t>(), T.p_Z.as<double>(),
-                      T.p_fc.as<double>()};
-    a.npk = npk;
-    a.out = T.res.as<double>();
-    ctx->run_shells(sl, a, !plain, !plain, &st);
-  }
-  PPB_CUDA(cudaEventRecord(ev[3], s));
+  r.ctx->run_shells(*r.sl, a, !r.plain, !r.plain, &st);
+  acc->visits += st.visits;
+  acc->guard += st.guard;
+  acc->akk += st.akk;
+  for (int i = 0; i < 5; i++) acc->dump[i] += st.dump[i];
+  for (int i = 0; i < 16; i++) acc->raw[i] += st.raw[i];
+  acc->ms += st.ms;
+  for (int i = 0; i < 4; i++) acc->kms[i] += st.kms[i];
+  acc->pool_rows += st.pool_rows;
+  acc->batches += st.batches;
+}
 
-  // ---- records ----
+// records (Pipeline.jl:243-318): RTHL > 0 (and z <= z_max on the lightcone),
+// 11 or 33 floats in peak order, and their largest RTHL
+void records_phase(Run& r, TileRes& T, int64_t npk, int64_t* nrec_out, float* rmax_out) {
+  const ppb_tile_params* p = r.p;
   const int nf = p->ioutshear >= 1 ? 33 : 11;
   int64_t nrec = 0;
   float rmax = 0.f;
   if (npk > 0) {
-    RecArgs r{};
-    r.res = T.res.as<double>();
-    r.pos = T.p_pos.as<double>();
-    r.Rf = T.p_Rf.as<double>();
-    r.FcRf = T.p_FcRf.as<float>();
-    r.d2Rf = T.p_d2Rf.as<float>();
-    r.Z = T.p_Z.as<double>();
-    r.npk = (int)npk;
-    r.ievol = p->ievol;
-    r.z_max = p->z_max;
-    r.alatt = alatt;
-    r.Omnr = Om;
-    r.OL = p->Omvac;
-    r.ilpt = p->ilpt;
-    r.nf = nf;
-    r.C = C;
-    r.flags = T.flags.as<int>();
-    r.offs = T.offs.as<int>();
-    r.rec = T.rec.as<float>();
-    r.rthl = T.rthl.as<float>();
+    RecArgs a{};
+    a.res = T.res.as<double>();
+    a.pos = T.p_pos.as<double>();
+    a.Rf = T.p_Rf.as<double>();
+    a.FcRf = T.p_FcRf.as<float>();
+    a.d2Rf = T.p_d2Rf.as<float>();
+    a.Z = T.p_Z.as<double>();
+    a.npk = (int)npk;
+    a.ievol = p->ievol;
+    a.z_max = p->z_max;
+    a.alatt = r.alatt;
+    a.Omnr = r.Om;
+    a.OL = p->Omvac;
+    a.ilpt = p->ilpt;
+    a.nf = nf;
+    a.C = r.C;
+    a.flags = T.flags.as<int>();
+    a.offs = T.offs.as<int>();
+    a.rec = T.rec.as<float>();
+    a.rthl = T.rthl.as<float>();
     const unsigned gb = (unsigned)((npk + 255) / 256);
-    flag_kernel<<<gb, 256, 0, s>>>(r);
-    PPB_LAUNCHED(sl.launches);
-    PPB_CUDA(cudaMemsetAsync(T.flags.as<int>() + npk, 0, 4, s));
+    flag_kernel<<<gb, 256, 0, r.s>>>(a);
+    PPB_LAUNCHED(r.sl->launches);
+    PPB_CUDA(cudaMemsetAsync(T.flags.as<int>() + npk, 0, 4, r.s));
     size_t tb = T.tmp.bytes;
-    PPB_CUDA(cub::DeviceScan::ExclusiveSum(T.tmp.p, tb, T.flags.as<int>(), T.offs.as<int>(), (int)npk + 1, s));
-    sl.launches++;
-    record_kernel<<<gb, 256, 0, s>>>(r);
-    PPB_LAUNCHED(sl.launches);
+    PPB_CUDA(cub::DeviceScan::ExclusiveSum(T.tmp.p, tb, T.flags.as<int>(), T.offs.as<int>(), (int)npk + 1, r.s));
+    r.sl->launches++;
+    record_kernel<<<gb, 256, 0, r.s>>>(a);
+    PPB_LAUNCHED(r.sl->launches);
     int nr = 0;
-    PPB_CUDA(cudaMemcpyAsync(&nr, T.offs.as<int>() + npk, 4, cudaMemcpyDeviceToHost, s));
-    PPB_CUDA(cudaStreamSynchronize(s));
+    PPB_CUDA(cudaMemcpyAsync(&nr, T.offs.as<int>() + npk, 4, cudaMemcpyDeviceToHost, r.s));
+    PPB_CUDA(cudaStreamSynchronize(r.s));
     nrec = nr;
     if (nrec > 0) {
       size_t tb2 = T.tmp.bytes;
       float* dmax = T.count.as<float>() + 8;
-      PPB_CUDA(cub::DeviceReduce::Max(T.tmp.p, tb2, T.rthl.as<float>(), dmax, (int)nrec, s));
-      sl.launches++;
-      PPB_CUDA(cudaMemcpyAsync(&rmax, dmax, 4, cudaMemcpyDeviceToHost, s));
+      PPB_CUDA(cub::DeviceReduce::Max(T.tmp.p, tb2, T.rthl.as<float>(), dmax, (int)nrec, r.s));
+      r.sl->launches++;
+      PPB_CUDA(cudaMemcpyAsync(&rmax, dmax, 4, cudaMemcpyDeviceToHost, r.s));
     }
   }
-  PPB_CUDA(cudaEventRecord(ev[4], s));
-  PPB_CUDA(cudaStreamSynchronize(s));
+  PPB_CUDA(cudaStreamSynchronize(r.s));
+  *nrec_out = nrec;
+  *rmax_out = nrec > 0 ? rmax : 0.f;
+}
+
+void check_shell_stats(const ShellStats& st) {
   if (st.guard != 0)
     throw Error{PPB_ERR_CUDA, "shell truncation guard tripped: a profile read beyond the gathered shells"};
   if (st.akk != 0)
     throw Error{PPB_ERR_INVALID, "kernel_strain SPH table index out of range (the reference raises here too)"};
+}
 
-  o->nfields = nf;
+}  // namespace
+
+void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf_in, int nfilt, TileOut* o) {
+  check_params(p, Rf_in, nfilt);
+  PPB_REQUIRE(ctx->sh.pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
+  PPB_REQUIRE(ctx->sh.has_tab, "collapse table not set (ppb_set_collapse_table)");
+  const int n = p->n;
+  const double box = p->boxsize;
+  const int64_t N = (int64_t)n * n * n;
+  Run r;
+  setup_run(r, ctx, sl, p, Rf_in, nfilt, box / n);
+  TileRes& T = sl.tile_for(n);
+  T.setup(n, r.s);
+  T.aos.ensure(N * 32);
+  if (T.cap == 0) T.ensure_peaks(std::max<int64_t>(1 << 16, std::min<int64_t>(N / 64, 1 << 22)));
+  cudaEvent_t* ev = sl.stage_ev;
+  PPB_CUDA(cudaEventRecord(ev[0], r.s));
+  fields_phase(r, T, n, box);
+  launch_pack(r.L, T.aos.as<float4>(),
+              FieldWindow{T.delta.as<float>(), T.psi.as<float>(), p->ilpt >= 2 ? T.psi2.as<float>() : nullptr, 0,
+                          n, (int64_t)n * n, N},
+              n);
+  PPB_CUDA(cudaEventRecord(ev[1], r.s));
+  const int64_t npk = peaks_phase(r, T, n, box, {Win{0, (float)r.fcrit_val}}, n);
+  PPB_CUDA(cudaEventRecord(ev[2], r.s));
+  prep_phase(r, T, npk, n, 1, nullptr);
+  ShellStats st{};
+  shells_phase(r, T, 0, npk, n, T.aos.as<float4>(), r.want_lap ? T.lapd.as<float>() : nullptr, &st);
+  PPB_CUDA(cudaEventRecord(ev[3], r.s));
+  int64_t nrec = 0;
+  float rmax = 0.f;
+  records_phase(r, T, npk, &nrec, &rmax);
+  PPB_CUDA(cudaEventRecord(ev[4], r.s));
+  PPB_CUDA(cudaStreamSynchronize(r.s));
+  check_shell_stats(st);
+  sl.last_shell = st;
+  o->nfields = p->ioutshear >= 1 ? 33 : 11;
   o->count = nrec;
   o->npeaks = npk;
-  o->RTHLmax = nrec > 0 ? rmax : 0.f;
+  o->RTHLmax = rmax;
+  o->d_records = T.rec.as<float>();
+  sl.last_visits = st.visits;
+  sl.last_npk = npk;
+  float ms[4];
+  for (int i = 0; i < 4; i++) PPB_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+  std::memcpy(sl.stage_ms, ms, sizeof(ms));
+  o->device_ms = ms[0] + ms[1] + ms[2] + ms[3];
+}
+
+// run_multitile (src/MultiTile.jl:108-418): fields on the full periodic grid
+// N = nsub ntile + 2 nbuff (nsub = n - 2 nbuff, alatt = boxsize / n), the
+// filter bank on the full grid, peaks per tile in its nsub^3 core (tile
+// (it, jt, kt) starts at cell ((it-1) nsub, (jt-1) nsub, (kt-1) nsub); on the
+// lightcone with the fcrit of the tile centre's redshift and tiles beyond
+// chi(z_max) dropped), and the shell analysis per tile on the tile's own
+// n^3 fields.  Records are in tile order.
+void run_multitile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf_in, int nfilt,
+                        int ntile, const int32_t* tiles_in, int ntiles_in, TileOut* o) {
+  check_params(p, Rf_in, nfilt);
+  PPB_REQUIRE(ctx->sh.pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
+  PPB_REQUIRE(ctx->sh.has_tab, "collapse table not set (ppb_set_collapse_table)");
+  PPB_REQUIRE(ntile >= 1 && ntile <= 16, "ntile must be in [1, 16]");
+  const int nm = p->n, nbuff = p->nbuff, nsub = nm - 2 * nbuff;
+  const int64_t Ng = (int64_t)nsub * ntile + 2 * nbuff;
+  PPB_REQUIRE(Ng <= 2048, "full grid nsub ntile + 2 nbuff must be <= 2048");
+  const int n = (int)Ng;
+  const double alatt = p->boxsize / nm, box = n * alatt, dcore = nsub * alatt;
+  const int64_t N = (int64_t)n * n * n;
+  Run r;
+  setup_run(r, ctx, sl, p, Rf_in, nfilt, alatt);
+  // tiles: the given list, else every tile in (kt, jt, it) loop order
+  std::vector<std::array<int, 3>> tl;
+  if (tiles_in && ntiles_in > 0) {
+    for (int t = 0; t < ntiles_in; t++) {
+      const int it = tiles_in[3 * t], jt = tiles_in[3 * t + 1], kt = tiles_in[3 * t + 2];
+      PPB_REQUIRE(it >= 1 && it <= ntile && jt >= 1 && jt <= ntile && kt >= 1 && kt <= ntile,
+                  "tile index out of range");
+      tl.push_back({it, jt, kt});
+    }
+  } else {
+    for (int kt = 1; kt <= ntile; kt++)
+      for (int jt = 1; jt <= ntile; jt++)
+        for (int it = 1; it <= ntile; it++) tl.push_back({it, jt, kt});
+  }
+  const double cen = 0.5 * (ntile + 1);
+  auto centre = [&](const std::array<int, 3>& t, int d) { return (t[d] - cen) * dcore; };
+  const double obs[3] = {p->cenx, p->ceny, p->cenz};
+  std::vector<double> chis;
+  if (p->ievol == 1) {   // lightcone: drop tiles beyond chi(z_max) (MultiTile.jl:205-216)
+    const double chi_max = chi_of_z(r.Om, p->Omvac, p->h, p->z_max);
+    const double half = dcore / 2.0;
+    std::vector<std::array<int, 3>> keep;
+    for (const auto& t : tl) {
+      double d2 = 0.0;
+      for (int d = 0; d < 3; d++) {
+        const double e = std::max(std::fabs(centre(t, d) - obs[d]) - half, 0.0);
+        d2 += e * e;
+      }
+      if (std::sqrt(d2) <= chi_max) keep.push_back(t);
+    }
+    tl.swap(keep);
+    chis = ctx->chi_table(r.Om, p->Omvac, p->h, p->z_max + 1.0);
+  }
+  const int nwin = (int)tl.size();
+  std::vector<Win> wins(nwin);
+  std::vector<double> tcen(3 * std::max(nwin, 1), 0.0);
+  for (int t = 0; t < nwin; t++) {
+    const int64_t i1 = (int64_t)(tl[t][0] - 1) * nsub, j1 = (int64_t)(tl[t][1] - 1) * nsub,
+                  k1 = (int64_t)(tl[t][2] - 1) * nsub;
+    wins[t].off = i1 + (int64_t)n * j1 + (int64_t)n * n * k1;
+    for (int d = 0; d < 3; d++) tcen[3 * t + d] = centre(tl[t], d);
+    double fc = r.fcrit_val;
+    if (p->ievol == 1) {   // fcrit at the tile centre's redshift (MultiTile.jl:238-243)
+      double d2 = 0.0;
+      for (int d = 0; d < 3; d++) d2 += (tcen[3 * t + d] - obs[d]) * (tcen[3 * t + d] - obs[d]);
+      fc = fsc_of_z(*r.G, chi_to_z_host(chis, p->z_max + 1.0, std::sqrt(d2)));
+    }
+    wins[t].fcrit = (float)fc;
+  }
+  TileRes& T = sl.tile_for(n);
+  T.setup(n, r.s);
+  if (T.cap == 0) T.ensure_peaks(std::max<int64_t>(1 << 16, std::min<int64_t>(N / 64, 1 << 22)));
+  sl.tcen.ensure(tcen.size() * 8);
+  PPB_CUDA(cudaMemcpyAsync(sl.tcen.p, tcen.data(), tcen.size() * 8, cudaMemcpyHostToDevice, r.s));
+  cudaEvent_t* ev = sl.stage_ev;
+  PPB_CUDA(cudaEventRecord(ev[0], r.s));
+  fields_phase(r, T, n, box);
+  PPB_CUDA(cudaEventRecord(ev[1], r.s));
+  int64_t npk = 0;
+  if (nwin > 0) npk = peaks_phase(r, T, n, box, wins, nm);
+  PPB_CUDA(cudaEventRecord(ev[2], r.s));
+  prep_phase(r, T, npk, nm, nwin, sl.tcen.as<double>());
+  // peaks per tile (the sorted list is grouped by tile)
+  std::vector<int> cnt(std::max(nwin, 1), 0);
+  if (npk > 0) {
+    int tbits = 0;
+    while ((1 << tbits) < nwin) tbits++;
+    PPB_CUDA(cudaMemsetAsync(T.count.p, 0, 64, r.s));
+    sl.tcount.ensure(cnt.size() * 4);
+    PPB_CUDA(cudaMemsetAsync(sl.tcount.p, 0, cnt.size() * 4, r.s));
+    tile_count_kernel<<<(unsigned)((npk + 255) / 256), 256, 0, r.s>>>(T.keys_s.as<unsigned long long>(), (int)npk,
+                                                                      40 + r.fbits, sl.tcount.as<int>());
+    PPB_LAUNCHED(sl.launches);
+    PPB_CUDA(cudaMemcpyAsync(cnt.data(), sl.tcount.p, cnt.size() * 4, cudaMemcpyDeviceToHost, r.s));
+    PPB_CUDA(cudaStreamSynchronize(r.s));
+  }
+  // shells per tile on the tile's own fields (MultiTile.jl:286-327)
+  const int64_t Nt = (int64_t)nm * nm * nm;
+  ShellStats st{};
+  int64_t p0 = 0;
+  for (int t = 0; t < nwin; t++) {
+    const int64_t p1 = p0 + cnt[t];
+    if (p1 > p0) {
+      sl.t_aos.ensure(Nt * 32);
+      launch_pack(r.L, sl.t_aos.as<float4>(),
+                  FieldWindow{T.delta.as<float>(), T.psi.as<float>(), p->ilpt >= 2 ? T.psi2.as<float>() : nullptr,
+                              wins[t].off, n, (int64_t)n * n, N},
+                  nm);
+      const float* lapd = nullptr;
+      if (r.want_lap) {
+        sl.t_lapd.ensure(Nt * 4);
+        launch_extract(r.L, sl.t_lapd.as<float>(), T.lapd.as<float>(), wins[t].off, n, (int64_t)n * n, nm);
+        lapd = sl.t_lapd.as<float>();
+      }
+      shells_phase(r, T, p0, p1, nm, sl.t_aos.as<float4>(), lapd, &st);
+    }
+    p0 = p1;
+  }
+  PPB_CUDA(cudaEventRecord(ev[3], r.s));
+  int64_t nrec = 0;
+  float rmax = 0.f;
+  records_phase(r, T, npk, &nrec, &rmax);
+  PPB_CUDA(cudaEventRecord(ev[4], r.s));
+  PPB_CUDA(cudaStreamSynchronize(r.s));
+  check_shell_stats(st);
+  sl.last_shell = st;
+  o->nfields = p->ioutshear >= 1 ? 33 : 11;
+  o->count = nrec;
+  o->npeaks = npk;
+  o->RTHLmax = rmax;
   o->d_records = T.rec.as<float>();
   sl.last_visits = st.visits;
   sl.last_npk = npk;

@@ -96,6 +96,7 @@ EXPORTED = (
     "ppb_launch_count", "ppb_last_shell_stats", "ppb_last_stage_ms", "ppb_alloc_host", "ppb_free_host",
     "ppb_alloc_device", "ppb_free_device", "ppb_shell_counters", "ppb_find_peaks_noalloc",
     "ppb_last_shell_times", "ppb_serve_config", "ppb_submit", "ppb_wait", "ppb_stats_get", "ppb_stats_reset",
+    "ppb_run_multitile", "ppb_merge_catalog",
 )
 
 
@@ -140,6 +141,8 @@ def load_library():
     L.ppb_wait.argtypes = [P, ctypes.c_uint64, I32, ctypes.POINTER(_HaloBuf)]
     L.ppb_stats_get.argtypes = [P, ctypes.POINTER(_Stats)]
     L.ppb_stats_reset.argtypes = [P]
+    L.ppb_run_multitile.argtypes = [P, ctypes.POINTER(_TileParams), P, I32, I32, P, I32, ctypes.POINTER(_HaloBuf)]
+    L.ppb_merge_catalog.argtypes = [P, P, I64, I32, P, ctypes.POINTER(ctypes.c_int64)]
     for f in ("ppb_alloc_host", "ppb_alloc_device"):
         getattr(L, f).argtypes = [P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
     for f in ("ppb_free_host", "ppb_free_device"):
@@ -445,6 +448,38 @@ class Context:
             out = (rec[:hb.count].copy(), float(hb.RTHLmax), int(hb.npeaks))
             return out + (ms.value,) if timed else out
         raise PPBError(-7, "record capacity")
+
+    def run_multitile_arrays(self, cfg: PipelineConfig, seed: int, Rf: Sequence[float], ntile: int,
+                             tiles=None, plain: bool = False, pk_scale: float = 1.0):
+        """run_multitile(cfg; ntile, seed) with the tables set.  tiles: optional
+        list of (it, jt, kt), 1-based.  Returns (records, RTHLmax, npeaks)."""
+        p = self._params(cfg, seed, plain, pk_scale)
+        rf = np.ascontiguousarray(np.asarray(Rf, dtype=np.float64))
+        tl = None if tiles is None else np.ascontiguousarray(np.asarray(tiles, dtype=np.int32).reshape(-1, 3))
+        nt = 0 if tl is None else len(tl)
+        nf = 33 if cfg.ioutshear >= 1 else 11
+        cap = max(1024, getattr(self, "_last_count", 0) * 2)
+        for _ in range(2):
+            rec = np.empty((cap, nf), dtype=np.float32)
+            hb = _HaloBuf(records=rec.ctypes.data, capacity=cap)
+            rc = self.L.ppb_run_multitile(self.h, ctypes.byref(p), _p(rf), len(rf), int(ntile),
+                                          None if tl is None else _p(tl), nt, ctypes.byref(hb))
+            if rc == -7:
+                cap = int(hb.count) + 16
+                continue
+            self._check(rc)
+            return rec[:hb.count].copy(), float(hb.RTHLmax), int(hb.npeaks)
+        raise PPBError(-7, "record capacity")
+
+    def merge_catalog(self, records: np.ndarray) -> np.ndarray:
+        """merge_catalog(halos): exclusion and volume reduction; returns the
+        surviving records (input order) with the reduced RTHL."""
+        rec = np.ascontiguousarray(records, dtype=np.float32)
+        n, nf = rec.shape if rec.ndim == 2 else (0, 33)
+        out = np.empty((max(n, 1), nf), dtype=np.float32)
+        m = ctypes.c_int64()
+        self._check(self.L.ppb_merge_catalog(self.h, _p(rec) if n else None, n, nf, _p(out), ctypes.byref(m)))
+        return out[:m.value].copy()
 
     # ---- serving ----
     def serve_config(self, slots: int):

@@ -353,3 +353,47 @@ def test_growth_and_distance(ora):
     assert np.all(np.diff(d) > 0)
     z = ora.chi_to_z(0.315, 0.685, 0.674, 5.6, [ora.chi(0.315, 0.685, 0.674, zz) for zz in (0.5, 1.0, 3.0)])
     assert np.allclose(z, [0.5, 1.0, 3.0], rtol=1e-4)
+
+
+# ------------------------------------------------------------------ merge_catalog
+def _halos(xyz, r, nf=11):
+    rec = np.zeros((len(r), nf), np.float32)
+    rec[:, :3] = np.asarray(xyz, np.float32)
+    rec[:, 6] = np.asarray(r, np.float32)
+    rec[:, 3] = np.arange(len(r))   # tag
+    return rec
+
+
+def test_sphere_overlap_kats(ora):
+    # test/test_merger.jl:7-47
+    assert ora.sphere_overlap(10.0, 2.0, 3.0) == (0.0, 0.0)
+    assert ora.sphere_overlap(5.0, 2.0, 3.0) == (0.0, 0.0)
+    assert ora.sphere_overlap(0.5, 3.0, 1.0) == (0.0, 0.0)
+    assert ora.sphere_overlap(0.0, 2.0, 2.0) == (0.0, 0.0)
+    r = 2.0
+    v1, v2 = ora.sphere_overlap(r, r, r)
+    h = r / 2.0
+    assert v1 == pytest.approx(v2) and v1 == pytest.approx((np.pi / 3.0) * h ** 2 * (3.0 * r - h))
+    assert 0 < v1 + v2 < 4 * np.pi / 3 * r ** 3
+    v1, v2 = ora.sphere_overlap(3.0, 3.0, 1.0)
+    assert 0 < v1 < v2
+
+
+def test_merge_exclusion_kats(ora):
+    # test/test_merger.jl:71-112: A (large) kills B (inside), C far away survives
+    out, keep = ora.merge_catalog(_halos([[0, 0, 0], [0.3, 0.3, 0.3], [10, 10, 10]], [2.0, 0.5, 1.0]))
+    assert keep.tolist() == [True, False, True]
+    # equal radii: the earlier halo of the stable order wins
+    out, keep = ora.merge_catalog(_halos([[0, 0, 0], [0.5, 0, 0]], [2.0, 2.0]))
+    assert keep.tolist() == [True, False]
+
+
+def test_merge_volume_reduction_kats(ora):
+    # test/test_merger.jl:114-151: overlapping equal pair shrinks symmetrically
+    out, keep = ora.merge_catalog(_halos([[0, 0, 0], [3, 0, 0]], [2.0, 2.0]))
+    assert keep.all() and out[0, 6] < 2.0 and out[0, 6] == out[1, 6]
+    h = 2.0 - 1.5   # cap height at d = 3, r = 2
+    cap = np.pi / 3 * h * h * (3 * 2.0 - h)
+    assert out[0, 6] == pytest.approx(((4 * np.pi / 3 * 8.0 - cap) / (4 * np.pi / 3)) ** (1 / 3), rel=1e-6)
+    out, keep = ora.merge_catalog(_halos([[0, 0, 0], [100, 0, 0]], [2.0, 3.0]))
+    assert keep.all() and out[0, 6] == pytest.approx(2.0) and out[1, 6] == pytest.approx(3.0)
