@@ -11,6 +11,7 @@ that tile: noise, fields, filter bank + peaks, shells, records.
 Usage:
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--plain]
   python bench.py --serve      # the serving stream: 200 requests, Poisson arrivals
+  python bench.py --lightcone  # 4 lightcone tiles of 384^3 (run_multitile) + merge_catalog
 Under torchrun each rank runs independent tiles on its own GPU (run_tile
 does not shard: replicas) with its own seed; the job value is the tiles of
 all ranks over the slowest rank's device time.
@@ -442,6 +443,62 @@ def run_serve(args, dist: Dist):
             "peaks_per_s": st["peaks_done"] / wall, "hbm_in_use_gb": st["hbm_in_use"] / 1e9}
 
 
+def run_lightcone(args, dist: Dist):
+    """Lightcone multi-tile: run_multitile with nmesh = 384, nbuff = 32
+    (nsub = 320, full grid N = 704, alatt 2 Mpc/h), ievol = 1, z_out = 0,
+    z_max = 4.6, observer at the corner of the 2^3 cores
+    (cen = -N_core alatt / 2 = -640 Mpc/h); the 4 tiles of the (it, jt, 1)
+    layer of ntile = 2, then merge_catalog.  A step is the whole chain."""
+    import peakpatch_b200 as pp
+    from peakpatch_b200 import powerspec
+    if dist.rank != 0:
+        return None
+    n, nbuff, ntile = 384, 32, 2
+    alatt = BOX_PER_CELL
+    ncore = (n - 2 * nbuff) * ntile
+    cen = -ncore * alatt / 2
+    cfg = pp.PipelineConfig(Omx=0.315 - 0.049, OmB=0.049, Omvac=0.685, h=0.674, n=n, boxsize=alatt * n,
+                            nbuff=nbuff, z_out=0.0, z_max=4.6, ievol=1, ilpt=2, ioutshear=1, wsmooth=1,
+                            rmax2rs=0.0, cenx=cen, ceny=cen, cenz=cen)
+    tiles = [(1, 1, 1), (2, 1, 1), (1, 2, 1), (2, 2, 1)]
+    ctx = pp.Context(dist.local)
+    k, P = powerspec.eh_table()
+    ctx.set_pk_table(k, P)
+    ctx.set_collapse_table(pp.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat")))
+    for _ in range(max(1, args.warmup)):
+        rec, rmax, npk = ctx.run_multitile_arrays(cfg, SEED, FILTERS, ntile, tiles=tiles)
+        merged = ctx.merge_catalog(rec)
+    ctx.synchronize()
+    t_mt, t_mg, w_all = [], [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ctx.event_record(6)
+        rec, rmax, npk = ctx.run_multitile_arrays(cfg, SEED, FILTERS, ntile, tiles=tiles)
+        ctx.event_record(7)
+        merged = ctx.merge_catalog(rec)
+        ctx.event_record(8)
+        ctx.synchronize()
+        w_all.append(time.perf_counter() - t0)
+        t_mt.append(ctx.event_elapsed(6, 7) / 1000.0)
+        t_mg.append(ctx.event_elapsed(7, 8) / 1000.0)
+    stage = ctx.stage_ms()
+    sh = ctx.shell_stats()
+    ctx.close()
+    tm, tg = statistics.median(t_mt), statistics.median(t_mg)
+    return {"metric": "tiles/s (lightcone chain)", "value": len(tiles) / (tm + tg), "unit": "tiles/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": 1000 * (tm + tg),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+            "dtype": "f32 fields, compensated-f32 shell sums",
+            "config": {"workload": "run_multitile lightcone: 4 tiles of 384^3 (nbuff 32, N = 704), ievol 1, "
+                                   "z_max 4.6, observer at the core corner, then merge_catalog",
+                       "tiles": tiles, "seed": SEED},
+            "multitile_ms": 1000 * tm, "merge_ms": 1000 * tg, "stage_ms": stage,
+            "shell_kernel_ms": sh["kernel_ms"], "peaks": npk, "halos": len(rec), "halos_after_merge": len(merged),
+            "wall_ms_per_step": 1000 * statistics.median(w_all),
+            "note": "device time (CUDA events on the library stream) of run_multitile and merge_catalog, "
+                    "records copied to host inside it"}
+
+
 def _measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -466,11 +523,17 @@ def main():
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--lightcone", action="store_true", help="run the lightcone multi-tile chain instead")
     args = ap.parse_args()
     dist = Dist()
     try:
         if args.impl == "reference":
             run_reference(args, dist)
+            return
+        if args.lightcone:
+            line = run_lightcone(args, dist)
+            if line is not None:
+                print(json.dumps(line), flush=True)
             return
         if args.serve:
             line = run_serve(args, dist)

@@ -218,13 +218,18 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
   // profile pool: sized from the rows per peak of the previous call; peaks
   // run in batches that fit the pool budget, and a batch whose rows overflow
   // the pool runs again with a larger pool or fewer peaks
-  size_t fr = 0, tot = 0;
-  PPB_CUDA(cudaMemGetInfo(&fr, &tot));
   const size_t row_bytes = ROW * sizeof(double);
-  const int64_t budget_rows = std::max<int64_t>(
-      1 << 16, (int64_t)(std::min<size_t>((size_t)32 << 30, (fr + sl.pool.bytes) / 2) / row_bytes));
   double& rpp = sl.rows_per_peak[adaptive];
   if (rpp <= 0.0) rpp = adaptive ? 64.0 : (double)(a.mmax + 1);
+  // pool budget: half of the free memory (with the pool's own), at most 32 GB;
+  // the free-memory query runs only when the pool would have to grow
+  int64_t budget_rows = (int64_t)(sl.pool.bytes / row_bytes);
+  if ((double)a.npk * rpp * 1.25 + 4096 > (double)budget_rows) {
+    size_t fr = 0, tot = 0;
+    PPB_CUDA(cudaMemGetInfo(&fr, &tot));
+    budget_rows = std::max<int64_t>(
+        1 << 16, (int64_t)(std::min<size_t>((size_t)32 << 30, (fr + sl.pool.bytes) / 2) / row_bytes));
+  }
   ShellStats s{};
   unsigned long long before[16] = {}, c[16] = {};
   int64_t p0 = 0;
@@ -269,7 +274,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     b.order = sl.oidx2.as<int32_t>();
     launch_shell_gather(L, b, comp, adaptive, gblocks);
     PPB_CUDA(cudaEventRecord(sl.shell_ev[1], stream));
-    launch_shell_collapse(L, b);
+    launch_shell_collapse(L, b, nsm, sl.walk_per_peak);
     PPB_CUDA(cudaEventRecord(sl.shell_ev[2], stream));
     launch_shell_zhalf(L, b);
     PPB_CUDA(cudaEventRecord(sl.shell_ev[3], stream));
@@ -294,6 +299,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     s.pool_rows += used;
     s.batches++;
     if (nb == a.npk - p0 || nb >= 1024) rpp = std::max(1.0, (double)used / (double)nb);
+    if (nb >= 1024) sl.walk_per_peak = (double)(c[9] - before[9]) / (double)nb;
     std::memcpy(before, c, sizeof(c));
     p0 += nb;
   }

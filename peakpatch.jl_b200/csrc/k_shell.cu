@@ -29,9 +29,9 @@
 //    The kernel ends with the fcrit crossing m0 (RadialShell.jl:494-537) and
 //    moves the peak's rows from its staging slot to a pool.
 //
-//  collapse_kernel (one thread per peak).  kernel_strain windows, the inward
-//    collapse walk, RTHL and Sbar/Srb in double precision, in the reference's
-//    summation order.  The window weights hRinteg/(u12-u0^2)^2 depend only on
+//  collapse_kernel (four threads per peak).  kernel_strain windows, the
+//    inward collapse walk (four candidate steps per round), RTHL and Sbar/Srb
+//    in double precision, in the reference's summation order.  The window weights hRinteg/(u12-u0^2)^2 depend only on
 //    the radii and come from a host table.
 //
 //  zhalf_kernel (sixteen threads per collapsed peak, ten radii).  zvir_half.
@@ -596,7 +596,7 @@ __global__ void geo_kernel(ShellArgs a, uint32_t* key, int32_t* idx) {
 }
 
 // ===========================================================================
-// collapse kernel (one thread per peak)
+// collapse kernel (four threads per peak)
 // ===========================================================================
 struct KS {
   double E[6];   // xx yy zz xy xz yz
@@ -736,6 +736,8 @@ __device__ __forceinline__ void write_no_collapse(double* o) {
   for (int q = 0; q < RES_N; q++) o[q] = (q == 0 || q == 26) ? -1.0 : 0.0;
 }
 
+// One thread per peak: the walk one step at a time (the device is full of
+// peaks, so its latency is hidden).
 __device__ void collapse_one(const ShellArgs& a, int64_t p) {
   double* out = a.out + p * RES_N;
   const PeakHdr h = a.hdr[p];
@@ -905,9 +907,223 @@ __device__ void collapse_one(const ShellArgs& a, int64_t p) {
   for (int q = 0; q < RES_N; q++) out[q] = r[q];
 }
 
-__global__ void __launch_bounds__(128) collapse_kernel(ShellArgs a) {
+__device__ __forceinline__ KS shfl_ks(const KS& k, int src, unsigned mask) {
+  KS r;
+#pragma unroll
+  for (int q = 0; q < 6; q++) r.E[q] = __shfl_sync(mask, k.E[q], src);
+#pragma unroll
+  for (int L = 0; L < 3; L++) {
+    r.g[L] = __shfl_sync(mask, k.g[L], src);
+    r.gf[L] = __shfl_sync(mask, k.gf[L], src);
+  }
+  return r;
+}
+
+// QT threads per peak (lanes qbase .. qbase+QT-1, QT = 2 or 4): the inward
+// walk evaluates QT consecutive steps per round, thread q taking step
+// base + q (mp = m0 - step; step 0 is the m0 step, whose zvir is forced to
+// -1), and the group takes the first step that collapses; the step before it
+// comes from the thread to its left or, for q = 0, from the previous round's
+// last step.  Thread 0 then finishes the peak alone.  Several threads per
+// peak shorten the walk's latency when there are few peaks to hide it.
+template <int QT>
+__device__ void collapse_group(const ShellArgs& a, int64_t p, int q, int qbase, unsigned qmask) {
+  double* out = a.out + p * RES_N;
+  const PeakHdr h = a.hdr[p];
+  if (h.status != HS_OK) {
+    if (q == 0) write_no_collapse(out);
+    return;
+  }
+  const double* __restrict__ rad = a.rad;
+  const Rows R{a.pool + h.off * ROW, h.mdone, a.counters};
+  const double ZZon = a.pk.ZZon[p];
+  const double alatt = a.alatt;
+  const int m = a.mmax;
+  const int4 gq = a.geo[p];
+  Geo geo;
+  geo.m0_init = gq.x; geo.mrf = gq.y; geo.mlow_rf = gq.z; geo.mupp_rf = gq.w;
+  const double anor = 1.0;
+  const double aRnor = 3.0 * anor / alatt, wnor = anor / (4.0 * 3.141592653589793), wRnor = 3.0 * wnor / alatt;
+
+  // Phase 3: gradient at the filter scale (thread 0, beside its m0 step)
+  double grf[3] = {0.0, 0.0, 0.0};
+  if (q == 0) {
+    KS krf;
+    kernel_strain(a, R, geo.mrf, geo.mlow_rf, geo.mupp_rf, wRnor, aRnor, &krf);
+#pragma unroll
+    for (int L = 0; L < 3; L++) grf[L] = krf.g[L];
+  }
+
+  // Phase 5: inward walk (RadialShell.jl:566-699) from the crossing m0.  At
+  // mp = 1 the reference's running window is [2, last shell with rad < 2].
+  const int hi1 = last_lt(rad, 2, m, 2.0);
+  const int m0o = h.m0;
+  int m0 = m0o;
+  KS prev, last, carry;
+  double zcarry = -1.0, zvir1 = -1.0, zvir1p = -1.0, lastFh = 0.0;
+  bool collapsed = false;
+  long long steps = 0;
+  for (int base = 0;; base += QT) {
+    const int st = base + q, mp = m0o - st;
+    const bool act = mp >= 1;
+    KS cur = {};
+    double zv = -1.0, Fh = 0.0;
+    if (act) {
+      kernel_strain(a, R, mp, 2, mp > 1 ? m : hi1, wRnor, aRnor, &cur);
+      steps++;
+      if (st >= 1) {
+        double ev, pv;
+        ev_pv(cur.E, &Fh, &ev, &pv);
+        zv = zvir_of(a.tab, R.get(R_FBAR, mp), ev, pv);
+      }
+    }
+    const bool hit = act && st >= 1 && zv >= ZZon;
+    {
+      const unsigned bal = (__ballot_sync(qmask, hit) >> qbase) & ((1u << QT) - 1u);
+      if (bal) {
+        const int qs = __ffs(bal) - 1;
+        last = shfl_ks(cur, qbase + qs, qmask);
+        lastFh = __shfl_sync(qmask, Fh, qbase + qs);
+        zvir1p = __shfl_sync(qmask, zv, qbase + qs);
+        const int ql = qs > 0 ? qs - 1 : 0;
+        const KS left = shfl_ks(cur, qbase + ql, qmask);
+        const double zl = __shfl_sync(qmask, zv, qbase + ql);
+        prev = qs > 0 ? left : carry;
+        zvir1 = qs > 0 ? zl : zcarry;
+        m0 = m0o - (base + qs) + 1;
+        collapsed = true;
+        break;
+      }
+      if (m0o - (base + QT - 1) <= 1) break;   // walked down to mp = 1
+      carry = shfl_ks(cur, qbase + QT - 1, qmask);
+      zcarry = __shfl_sync(qmask, zv, qbase + QT - 1);
+    }
+  }
+  atomicAdd(a.counters + CNT_WALK, (unsigned long long)steps);
+  if (q != 0) return;
+  if (!collapsed) {
+    atomicAdd(a.counters + CNT_NOCOLL, 1ull);
+    write_no_collapse(out);
+    return;
+  }
+
+  // Phase 6: collapse radius (RadialShell.jl:707-754)
+  const double dZvir = zvir1p - zvir1;
+  double RTHL;
+  const double ra = __ldg(rad + m0 - 1), rb = __ldg(rad + m0);
+  const double rad3p = ra * ra * ra, rad3 = rb * rb * rb;
+  if (zvir1 > 0.0 && dZvir != 0.0) {
+    const double R3 = rad3p + (rad3 - rad3p) * (zvir1p - ZZon) / dZvir;
+    RTHL = pow(R3, 1.0 / 3.0);
+  } else {
+    RTHL = ra;
+  }
+  if (RTHL <= 0.0) {
+    atomicAdd(a.counters + CNT_RTHLNEG, 1ull);
+    write_no_collapse(out);
+    return;
+  }
+  const double RTHL3 = RTHL * RTHL * RTHL, RTHL5 = RTHL3 * RTHL * RTHL;
+  const double drad3 = rad3 - rad3p;
+  const double Fa = R.get(R_FBAR, m0 - 1), Fb = R.get(R_FBAR, m0);
+  const double dFb = Fb - Fa;
+  double Fbarx;
+  double S[6], gk[3], gkf[3];
+  if (zvir1 > 0.0 && drad3 != 0.0) {
+    const double fr = (RTHL3 - rad3p) / drad3;
+    Fbarx = Fa + fr * dFb;
+#pragma unroll
+    for (int q = 0; q < 6; q++) S[q] = last.E[q] + fr * (prev.E[q] - last.E[q]);
+#pragma unroll
+    for (int L = 0; L < 3; L++) {
+      gk[L] = last.g[L] + fr * (prev.g[L] - last.g[L]);
+      gkf[L] = last.gf[L] + fr * (prev.gf[L] - last.gf[L]);
+    }
+  } else {
+    Fbarx = Fa;
+#pragma unroll
+    for (int q = 0; q < 6; q++) S[q] = last.E[q];
+#pragma unroll
+    for (int L = 0; L < 3; L++) { gk[L] = prev.g[L]; gkf[L] = prev.gf[L]; }
+  }
+  // normalize_strain then eigenvalues (RadialShell.jl:748-752)
+  {
+    const double tr = S[0] + S[1] + S[2];
+    if (tr != 0.0) {
+      const double f = Fbarx / tr;
+#pragma unroll
+      for (int q = 0; q < 6; q++) S[q] *= f;
+    }
+  }
+  double Frhoc, e_v_f, p_v_f;
+  ev_pv(S, &Frhoc, &e_v_f, &p_v_f);
+  double smat[6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) smat[q] = last.E[q] * (Fbarx / lastFh);
+
+  // Phase 7: Sbar, Sbar2 (RadialShell.jl:758-773), Srb (:776-790)
+  double sb[6] = {0, 0, 0, 0, 0, 0};
+  long long nS = 0;
+  double srb = 0.0;
+  for (int m1 = 1; m1 <= m0 - 1; m1++) {
+    const double nn = R.get(R_N, m1);
+    if (nn > 0) {
+#pragma unroll
+      for (int L = 0; L < 3; L++) {
+        sb[L] += R.get(R_S + L, m1);
+        sb[3 + L] += R.get(R_S2 + L, m1);
+      }
+      nS += (long long)nn;
+    }
+    if (m1 >= 2) {
+      const double r5 = __ldg(a.rad5 + m1), r5p = m1 - 1 >= 2 ? __ldg(a.rad5 + m1 - 1) : 0.0;
+      srb += 0.5 * (R.get(R_FBAR, m1 - 1) + R.get(R_FBAR, m1)) * (r5 - r5p);
+    }
+  }
+  if (nS > 0) {
+#pragma unroll
+    for (int q = 0; q < 6; q++) sb[q] /= (double)nS;
+  }
+  const double rad5p = (m0 - 1 >= 2) ? __ldg(a.rad5 + m0 - 1) : 0.0;
+  if (zvir1 > 0.0 && dZvir != 0.0) srb += 0.5 * (Fa + Fbarx) * (RTHL5 - rad5p);
+  if (Fbarx * RTHL5 > 0.0) srb /= (Fbarx * RTHL5);
+
+  // results (layout in ppb.h); zvir_half (26) comes from zhalf_kernel and
+  // d2F (30) from d2f_kernel
+  double r[RES_N];
+  r[0] = RTHL;
+  r[1] = srb;
+#pragma unroll
+  for (int L = 0; L < 3; L++) {
+    r[2 + L] = sb[L];
+    r[5 + L] = sb[3 + L];
+    r[17 + L] = gk[L];
+    r[20 + L] = grf[L];
+    r[27 + L] = gkf[L];
+  }
+  r[8] = smat[0]; r[9] = smat[3]; r[10] = smat[4];
+  r[11] = smat[3]; r[12] = smat[1]; r[13] = smat[5];
+  r[14] = smat[4]; r[15] = smat[5]; r[16] = smat[2];
+  r[23] = Fbarx;
+  r[24] = e_v_f;
+  r[25] = p_v_f;
+  r[26] = -1.0;
+  r[30] = 0.0;
+#pragma unroll
+  for (int q = 0; q < RES_N; q++) out[q] = r[q];
+}
+
+__global__ void __launch_bounds__(128) collapse1_kernel(ShellArgs a) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p < a.npk) collapse_one(a, p);
+}
+
+template <int QT>
+__global__ void __launch_bounds__(128) collapse_kernel(ShellArgs a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t p = t / QT;
+  const int lane = threadIdx.x & 31, q = lane & (QT - 1), qbase = lane & ~(QT - 1);
+  if (p < a.npk) collapse_group<QT>(a, p, q, qbase, ((1u << QT) - 1u) << qbase);
 }
 
 // ===========================================================================
@@ -1031,10 +1247,18 @@ void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive,
   PPB_LAUNCHED(*L.count);
 }
 
-void launch_shell_collapse(Launch L, const ShellArgs& a) {
-  const int64_t blocks = (a.npk + 127) / 128;
+void launch_shell_collapse(Launch L, const ShellArgs& a, int nsm, double walk_steps_per_peak) {
+  // threads per peak: 4 while 4 per peak still fit about 24 warps per SM or
+  // when walks are long (more than 8 steps per peak in the previous batch:
+  // the lightcone), else 1 (the device is full and the latency is hidden)
+  const int64_t full = (int64_t)nsm * 24 * 32;
+  int lg = a.npk * 4 <= full ? 2 : (a.npk * 2 <= full ? 1 : 0);
+  if (walk_steps_per_peak > 8.0) lg = 2;
+  const int64_t blocks = ((a.npk << lg) + 127) / 128;
   if (blocks == 0) return;
-  collapse_kernel<<<(unsigned)blocks, 128, 0, L.s>>>(a);
+  if (lg == 2) collapse_kernel<4><<<(unsigned)blocks, 128, 0, L.s>>>(a);
+  else if (lg == 1) collapse_kernel<2><<<(unsigned)blocks, 128, 0, L.s>>>(a);
+  else collapse1_kernel<<<(unsigned)blocks, 128, 0, L.s>>>(a);
   PPB_LAUNCHED(*L.count);
 }
 

@@ -56,6 +56,7 @@ struct Slot {
   DevBuf tcen, tcount, t_aos, t_lapd;               // multi-tile: centres, peaks per tile, tile fields
   int gather_bps[2][2] = {{0, 0}, {0, 0}};          // gather blocks per SM by [comp][adaptive]
   double rows_per_peak[2] = {0.0, 0.0};             // pool rows per peak seen last, by adaptive
+  double walk_per_peak = 0.0;                       // collapse-walk steps per peak seen last
   ShellStats last_shell{};
   int64_t last_visits = 0, last_npk = 0;
   void init(int device);

@@ -293,7 +293,7 @@ void launch_peakfind(Launch L, const float* ds, const float* ls, uint8_t* mask, 
 // Shell stage = five launches on one stream:
 //  geo      (one thread per peak): per-peak shell geometry
 //  gather   (persistent, one warp per peak): profile rows + PeakHdr
-//  collapse (one thread per peak): results except zvir_half and d2F
+//  collapse (1 to 4 threads per peak): results except zvir_half and d2F
 //  zhalf    (sixteen threads per peak): result 26
 //  d2f      (one warp per collapsed peak): result 30
 // comp: compensated single-precision gather sums (else double); adaptive:
@@ -305,7 +305,7 @@ int shell_gather_blocks_per_sm(bool comp, bool adaptive);
 // keys (Morton index of the peak's 8^3 brick) and the identity permutation
 void launch_shell_geo(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx);
 void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks);
-void launch_shell_collapse(Launch L, const ShellArgs& a);
+void launch_shell_collapse(Launch L, const ShellArgs& a, int nsm, double walk_steps_per_peak);
 void launch_shell_zhalf(Launch L, const ShellArgs& a);
 void launch_shell_d2f(Launch L, const ShellArgs& a, int blocks);
 

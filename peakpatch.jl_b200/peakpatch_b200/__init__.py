@@ -458,7 +458,9 @@ class Context:
         tl = None if tiles is None else np.ascontiguousarray(np.asarray(tiles, dtype=np.int32).reshape(-1, 3))
         nt = 0 if tl is None else len(tl)
         nf = 33 if cfg.ioutshear >= 1 else 11
-        cap = max(1024, getattr(self, "_last_count", 0) * 2)
+        # about one halo per 60 core cells (384^3 tiles); grown and rerun when short
+        ncore = (cfg.n - 2 * cfg.nbuff) ** 3 * (ntile ** 3 if tl is None else nt)
+        cap = max(1024, getattr(self, "_last_count", 0) * 2, ncore // 40)
         for _ in range(2):
             rec = np.empty((cap, nf), dtype=np.float32)
             hb = _HaloBuf(records=rec.ctypes.data, capacity=cap)
@@ -468,6 +470,7 @@ class Context:
                 cap = int(hb.count) + 16
                 continue
             self._check(rc)
+            self._last_count = int(hb.count)
             return rec[:hb.count].copy(), float(hb.RTHLmax), int(hb.npeaks)
         raise PPBError(-7, "record capacity")
 
