@@ -116,6 +116,10 @@ int32_t ppb_set_collapse_table(ppb_ctx* ctx, const float* tab, int32_t nx, int32
 /* P(k) table (k in h/Mpc, P in the reference's file convention) for the
  * log-log interpolant of load_pk (src/InitialConditions/PowerSpectrum.jl:11-30). */
 int32_t ppb_set_pk_table(ppb_ctx* ctx, const double* k, const double* pk, int32_t n);
+/* The collapse table with Float64 nodes (same layout and ranges as
+ * ppb_set_collapse_table; replaces the resident table). */
+int32_t ppb_set_collapse_table_f64(ppb_ctx* ctx, const double* tab, int32_t nx, int32_t ny, int32_t nz, double x1,
+                                   double x2, double y1, double y2, double z1, double z2);
 
 /* ---- the drop-in for run_tile ------------------------------------------ */
 /* Pipeline.run_tile(cfg; seed) (src/Pipeline.jl:66-325): noise -> sqrt(P)
@@ -149,6 +153,14 @@ int32_t ppb_run_multitile(ppb_ctx* ctx, const ppb_tile_params* p, const double* 
  * *n_out = survivors, written in input order with the reduced RTHL. */
 int32_t ppb_merge_catalog(ppb_ctx* ctx, const float* records, int64_t n, int32_t nfields, float* out,
                           int64_t* n_out);
+
+/* The fields of run_tile's first phase for params p (src/Pipeline.jl:90-140):
+ * delta = generate_grf(n, P, boxsize, seed), psi = displacements_1lpt,
+ * psi2 = displacements_2lpt (ilpt >= 2), lapd = irfft(k^2 delta_k)/n^3
+ * (ioutshear >= 1).  Outputs are n^3 column-major Float32 (psi, psi2: three
+ * consecutive components), host or device; any may be NULL. */
+int32_t ppb_generate_fields(ppb_ctx* ctx, const ppb_tile_params* p, float* delta, float* psi, float* psi2,
+                            float* lapd);
 
 /* write_pksc (src/IO/Catalog.jl:53-94): Int32 N, Float32 RTHLmax, Float32 z_out,
  * then N x nfields Float32 (little endian). */
@@ -200,6 +212,15 @@ int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, c
                           int64_t npk, const int64_t* ipp, const double* Rf, const int64_t* ir2min,
                           const double* ZZon, const double* fcrit, double alatt, int32_t plain,
                           double* out);
+/* ppb_analyse_peaks with a shell list per peak: peak q analyses the cells
+ * with r^2 <= r2lim[q] (in cells^2; the reference's precompute_shells(R) for
+ * R^2 = r2lim[q]), clipped to nhunt^2; r2lim NULL or an entry <= 0 means the
+ * whole nhunt list. */
+int32_t ppb_analyse_peaks_lim(ppb_ctx* ctx, const float* delta, const float* etax, const float* etay,
+                              const float* etaz, const float* eta2x, const float* eta2y, const float* eta2z,
+                              const float* lapd, int32_t n, int32_t nhunt, int64_t npk, const int64_t* ipp,
+                              const double* Rf, const int64_t* ir2min, const double* ZZon, const double* fcrit,
+                              const int32_t* r2lim, double alatt, int32_t plain, double* out);
 
 /* ---- memory helpers ----------------------------------------------------- */
 /* Page-locked host memory (fast, asynchronous copies of records) and device

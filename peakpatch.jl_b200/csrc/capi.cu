@@ -56,14 +56,14 @@ void Slot::init(int dev) {
 void Slot::release_buffers() {
   tile.reset();
   for (DevBuf* b : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
-                    &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd})
+                    &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim})
     b->release();
 }
 
 size_t Slot::bytes_held() const {
   size_t b = tile ? tile->bytes() : 0;
   for (const DevBuf* d : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool,
-                          &okey, &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd})
+                          &okey, &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim})
     b += d->bytes;
   return b;
 }
@@ -214,6 +214,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
   sl.ctl.ensure(64);
   sl.hdr.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(PeakHdr));
   sl.geo.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(int4));
+  sl.mlim.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(int32_t));
   PPB_CUDA(cudaMemsetAsync(sl.counters.p, 0, 16 * 8, stream));
   // profile pool: sized from the rows per peak of the previous call; peaks
   // run in batches that fit the pool budget, and a batch whose rows overflow
@@ -248,6 +249,8 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     b.out = a.out + p0 * RES_N;
     b.hdr = sl.hdr.as<PeakHdr>() + p0;
     b.geo = sl.geo.as<int4>() + p0;
+    b.mlim = sl.mlim.as<int32_t>() + p0;
+    b.r2lim = a.r2lim ? a.r2lim + p0 : nullptr;
     b.pool = sl.pool.as<double>();
     b.pool_cap = cap;
     b.pool_ctr = reinterpret_cast<unsigned long long*>(sl.ctl.as<char>() + 8);
@@ -395,8 +398,40 @@ int32_t ppb_set_collapse_table(ppb_ctx* ctx, const float* tab, int32_t nx, int32
   const size_t bytes = (size_t)nx * ny * nz * 4;
   ctx->sh.tab.ensure(bytes);
   PPB_CUDA(cudaMemcpy(ctx->sh.tab.p, tab, bytes, cudaMemcpyDefault));
-  ctx->sh.dtab = DevTable{ctx->sh.tab.as<float>(), nx, ny, nz, x1, x2, y1, y2, z1, z2};
+  ctx->sh.dtab = DevTable{ctx->sh.tab.as<float>(), nullptr, nx, ny, nz, x1, x2, y1, y2, z1, z2};
   ctx->sh.has_tab = true;
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_set_collapse_table_f64(ppb_ctx* ctx, const double* tab, int32_t nx, int32_t ny, int32_t nz, double x1,
+                                   double x2, double y1, double y2, double z1, double z2) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  PPB_GUARD_BEGIN
+  std::unique_lock<std::shared_mutex> wl(ctx->sh.mu);   // waits for runs in flight
+  PPB_REQUIRE(tab != nullptr, "table is null");
+  PPB_REQUIRE(nx >= 2 && ny >= 2 && nz >= 2, "table needs at least 2 nodes per axis");
+  PPB_REQUIRE(x2 > x1 && y2 > y1 && z2 > z1, "table ranges must be increasing");
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  const size_t bytes = (size_t)nx * ny * nz * 8;
+  ctx->sh.tab.ensure(bytes);
+  PPB_CUDA(cudaMemcpy(ctx->sh.tab.p, tab, bytes, cudaMemcpyDefault));
+  ctx->sh.dtab = DevTable{nullptr, ctx->sh.tab.as<double>(), nx, ny, nz, x1, x2, y1, y2, z1, z2};
+  ctx->sh.has_tab = true;
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_generate_fields(ppb_ctx* ctx, const ppb_tile_params* p, float* delta, float* psi, float* psi2,
+                            float* lapd) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  PPB_REQUIRE(p != nullptr, "params is null");
+  std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
+  generate_fields_core(ctx, ctx->sync, p, delta, psi, psi2, lapd);
   return PPB_OK;
   PPB_GUARD_END(ctx)
 }

@@ -203,9 +203,10 @@ struct Geo {
   int mlow_rf, mupp_rf;
 };
 
-__device__ __forceinline__ Geo geometry(const ShellArgs& a, double Rf, int ir2min) {
+// mmax: the peak's last finalised shell (nshell_p - 1 for a shell list of
+// nshell_p distinct r^2)
+__device__ __forceinline__ Geo geometry(const ShellArgs& a, double Rf, int ir2min, int mmax) {
   Geo g;
-  const int mmax = a.mmax;
   {
     int lo = 2, hi = mmax;
     while (lo <= hi) {
@@ -220,7 +221,7 @@ __device__ __forceinline__ Geo geometry(const ShellArgs& a, double Rf, int ir2mi
   g.mrf = 1;
   {
     const double rq = (Rf / a.alatt) * (Rf / a.alatt);
-    const int K = a.nshell - 1;
+    const int K = mmax;   // nonzero distinct r^2 values of the peak's list
     int lo = 1, hi = K;
     while (lo <= hi) {
       const int mid = (lo + hi) >> 1;
@@ -342,7 +343,11 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
   const int pk = (int)(lin / n2), pj = (int)((lin / n) % n), pi = (int)(lin % n);
   const double fcrit = a.pk.fcrit[p];
   const double* __restrict__ rad = a.rad;
-  const int mmax = a.mmax;
+  const int mmax = a.mlim[p];   // the peak's last finalised shell
+  // cells past the first cell of shell mmax + 1 are not summed (a peak with a
+  // shorter list reads only its own shells; the list's last shell is never
+  // finalised, RadialShell.jl:386-390)
+  const int cell_lim = __ldg(a.sh_start + mmax);
   const int4 gq = a.geo[p];
   const int m0_init = gq.x, mrf = gq.y, mupp_rf = gq.w;
 
@@ -372,14 +377,15 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
   double dF_prev = (double)c0.x;        // shell-mean delta of shell mdone
   long long visits = 0;
   for (int g = 0; g < a.ngroups; g++) {
-    const int base = __ldg(a.grp_a + g), gend = __ldg(a.grp_b + g);
-    if (mtarget >= 0 && base > mtarget) break;
+    const int base = __ldg(a.grp_a + g);
+    if (base > mmax || (mtarget >= 0 && base > mtarget)) break;
+    const int gend = min(__ldg(a.grp_b + g), mmax);
     const int c0g = __ldg(a.grp_c + g), ncg = __ldg(a.grp_c + g + 1) - c0g;
     // (a) lane l sums chunk c0g + l into the shared partial table
     if (lane < ncg) {
       typename std::conditional<COMP, AccP, Acc<false>>::type A;
       A.zero();
-      const int s0 = __ldg(a.ck_s + c0g + lane), cnt = __ldg(a.ck_n + c0g + lane);
+      const int s0 = __ldg(a.ck_s + c0g + lane), cnt = s0 < cell_lim ? __ldg(a.ck_n + c0g + lane) : 0;
       const int nsh = sum_chunk<decltype(A), COMP>(a, s0, cnt, lin, inside, pi, pj, pk, A);
       visits += nsh;
 #pragma unroll
@@ -466,7 +472,7 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
     if (ADAPTIVE && mtarget < 0 && (state != 0 || mdone >= mmax)) {
       int M = max(max(m0_init, mrf), mupp_rf);
       if (state == 2) M = max(M, mcross);
-      mtarget = state == 0 ? mmax : __ldg(a.need + M);
+      mtarget = state == 0 ? mmax : min(__ldg(a.need + M), mmax);
     }
     __syncwarp();
   }
@@ -581,7 +587,17 @@ __device__ __forceinline__ uint32_t spread3(uint32_t v) {
 __global__ void geo_kernel(ShellArgs a, uint32_t* key, int32_t* idx) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.npk) return;
-  const Geo g = geometry(a, a.pk.Rf[p], a.pk.ir2min[p]);
+  int mmax = a.mmax;
+  if (a.r2lim && a.r2lim[p] > 0) {   // shell list r^2 <= r2lim: nshell_p distinct values
+    int lo = 1, hi = a.nshell;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(a.r2m + mid) <= a.r2lim[p]) lo = mid + 1; else hi = mid - 1;
+    }
+    mmax = max(min(hi - 1, a.mmax), 1);
+  }
+  a.mlim[p] = mmax;
+  const Geo g = geometry(a, a.pk.Rf[p], a.pk.ir2min[p], mmax);
   a.geo[p] = make_int4(g.m0_init, g.mrf, g.mlow_rf, g.mupp_rf);
   if (key) {
     const int64_t lin = a.pk.lin[p], n = a.n, n2 = n * n;
@@ -632,7 +648,8 @@ __device__ __noinline__ void eig3(const double* m, double* lam) {
   lam[0] = e1; lam[1] = e2; lam[2] = e3;
 }
 
-// trilinear lookup, outside the box -> -1 (CollapseTable.jl:128-145)
+// trilinear lookup, outside the box -> -1 (CollapseTable.jl:128-145); Float32
+// or Float64 nodes
 __device__ __noinline__ double tab_interp(const DevTable& T, double x, double y, double z) {
   if (!(x >= T.x1 && x <= T.x2 && y >= T.y1 && y <= T.y2 && z >= T.z1 && z <= T.z2)) return -1.0;
   const double px = (x - T.x1) / ((T.x2 - T.x1) / (T.nx - 1));
@@ -643,12 +660,13 @@ __device__ __noinline__ double tab_interp(const DevTable& T, double x, double y,
   iy = iy < 0 ? 0 : (iy > T.ny - 2 ? T.ny - 2 : iy);
   iz = iz < 0 ? 0 : (iz > T.nz - 2 ? T.nz - 2 : iz);
   const double wx = px - ix, wy = py - iy, wz = pz - iz;
-  const float* b = T.t + ix + (int64_t)T.nx * (iy + (int64_t)T.ny * iz);
+  const int64_t o = ix + (int64_t)T.nx * (iy + (int64_t)T.ny * iz);
   const int64_t sy = T.nx, sz = (int64_t)T.nx * T.ny;
-  const double c00 = (1 - wx) * (double)__ldg(b) + wx * (double)__ldg(b + 1);
-  const double c10 = (1 - wx) * (double)__ldg(b + sy) + wx * (double)__ldg(b + sy + 1);
-  const double c01 = (1 - wx) * (double)__ldg(b + sz) + wx * (double)__ldg(b + sz + 1);
-  const double c11 = (1 - wx) * (double)__ldg(b + sz + sy) + wx * (double)__ldg(b + sz + sy + 1);
+  auto v = [&](int64_t i) { return T.td ? __ldg(T.td + o + i) : (double)__ldg(T.t + o + i); };
+  const double c00 = (1 - wx) * v(0) + wx * v(1);
+  const double c10 = (1 - wx) * v(sy) + wx * v(sy + 1);
+  const double c01 = (1 - wx) * v(sz) + wx * v(sz + 1);
+  const double c11 = (1 - wx) * v(sz + sy) + wx * v(sz + sy + 1);
   const double c0 = (1 - wy) * c00 + wy * c10;
   const double c1 = (1 - wy) * c01 + wy * c11;
   return (1 - wz) * c0 + wz * c1;
@@ -749,7 +767,7 @@ __device__ void collapse_one(const ShellArgs& a, int64_t p) {
   const Rows R{a.pool + h.off * ROW, h.mdone, a.counters};
   const double ZZon = a.pk.ZZon[p];
   const double alatt = a.alatt;
-  const int m = a.mmax;
+  const int m = a.mlim[p];
   const int4 gq = a.geo[p];
   Geo geo;
   geo.m0_init = gq.x; geo.mrf = gq.y; geo.mlow_rf = gq.z; geo.mupp_rf = gq.w;
@@ -938,7 +956,7 @@ __device__ void collapse_group(const ShellArgs& a, int64_t p, int q, int qbase, 
   const Rows R{a.pool + h.off * ROW, h.mdone, a.counters};
   const double ZZon = a.pk.ZZon[p];
   const double alatt = a.alatt;
-  const int m = a.mmax;
+  const int m = a.mlim[p];
   const int4 gq = a.geo[p];
   Geo geo;
   geo.m0_init = gq.x; geo.mrf = gq.y; geo.mlow_rf = gq.z; geo.mupp_rf = gq.w;
@@ -1147,7 +1165,7 @@ __global__ void __launch_bounds__(128) zhalf_kernel(ShellArgs a) {
       const PeakHdr h = a.hdr[p];
       const Rows R{a.pool + h.off * ROW, h.mdone, a.counters};
       const double* __restrict__ rad = a.rad;
-      const int m = a.mmax;
+      const int m = a.mlim[p];
       const double alatt = a.alatt, anor = 1.0;
       const double aRnor = 3.0 * anor / alatt, wRnor = 3.0 * (anor / (4.0 * 3.141592653589793)) / alatt;
       const double rcur = RTHL * a.fhalf[e];

@@ -51,7 +51,7 @@ struct Slot {
   std::unique_ptr<TileRes> tile;                    // one grid size at a time
   DevBuf filt_Rf, filt_ir2;                         // filter bank of the run
   DevBuf g_a, g_D, g_f, chi;                        // growth / chi tables of the run
-  DevBuf stage, counters, ctl, hdr, geo, pool;      // shell stage
+  DevBuf stage, counters, ctl, hdr, geo, mlim, pool;   // shell stage
   DevBuf okey, okey2, oidx, oidx2, otmp;            // spatial gather order
   DevBuf tcen, tcount, t_aos, t_lapd;               // multi-tile: centres, peaks per tile, tile fields
   int gather_bps[2][2] = {{0, 0}, {0, 0}};          // gather blocks per SM by [comp][adaptive]
@@ -136,6 +136,10 @@ void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const doubl
 void run_multitile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf, int nfilt, int ntile,
                         const int32_t* tiles, int ntiles, TileOut* o);
 void check_params(const ppb_tile_params* p, const double* Rf, int nfilt);
+// the fields of run_tile's first phase, copied to the given buffers (host or
+// device, any may be null)
+void generate_fields_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, float* delta, float* psi, float* psi2,
+                          float* lapd);
 // device bytes a run of this grid size holds at most (admission estimate)
 uint64_t tile_footprint(const ppb_tile_params* p);
 // copy `bytes` from device memory to dst (host or device)

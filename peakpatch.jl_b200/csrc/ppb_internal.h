@@ -154,7 +154,8 @@ struct DevCosmo {
 
 // collapse table on the device
 struct DevTable {
-  const float* t;
+  const float* t;     // Float32 nodes (read_homeltab), or
+  const double* td;   // Float64 nodes (set when t is null)
   int nx, ny, nz;
   double x1, x2, y1, y2, z1, z2;
 };
@@ -227,6 +228,8 @@ struct ShellArgs {
   double* out;              // npk x RES_N
   PeakHdr* hdr;             // npk
   int4* geo;                // npk: (m0_init, mrf, mlow_rf, mupp_rf)
+  const int32_t* r2lim;     // npk or null: per-peak shell list r^2 <= r2lim (> 0), else the whole list
+  int32_t* mlim;            // npk: the peak's last finalised shell (written by the geometry kernel)
   double* pool;             // profile rows, pool_cap rows of ROW doubles
   int64_t pool_cap;
   unsigned long long* pool_ctr;   // rows handed out

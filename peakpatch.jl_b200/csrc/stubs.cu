@@ -133,11 +133,11 @@ int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n
   }
 }
 
-int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, const float* etay,
-                          const float* etaz, const float* eta2x, const float* eta2y, const float* eta2z,
-                          const float* lapd, int32_t n, int32_t nhunt, int64_t npk, const int64_t* ipp,
-                          const double* Rf, const int64_t* ir2min, const double* ZZon, const double* fcrit,
-                          double alatt, int32_t plain, double* out) {
+static int32_t analyse_peaks_impl(ppb_ctx* ctx, const float* delta, const float* etax, const float* etay,
+                                  const float* etaz, const float* eta2x, const float* eta2y, const float* eta2z,
+                                  const float* lapd, int32_t n, int32_t nhunt, int64_t npk, const int64_t* ipp,
+                                  const double* Rf, const int64_t* ir2min, const double* ZZon, const double* fcrit,
+                                  const int32_t* r2lim, double alatt, int32_t plain, double* out) {
   if (!ctx) return PPB_ERR_INVALID;
   std::lock_guard<std::recursive_mutex> lk(ctx->mu);
   try {
@@ -156,7 +156,7 @@ int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, c
     std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
     ShellTable& shells = ctx->shell_table(nhunt, s);
     // fields -> contiguous device staging -> packed gather records
-    DevBuf st_delta, st_psi, st_psi2, st_lapd, aos, d_ipp, d_lin, d_Rf, d_ir2in, d_ir2, d_Z, d_fc, d_out;
+    DevBuf st_delta, st_psi, st_psi2, st_lapd, aos, d_ipp, d_lin, d_Rf, d_ir2in, d_ir2, d_Z, d_fc, d_out, d_lim;
     st_psi.ensure(3 * N * 4);
     auto put = [&](DevBuf& b, size_t off, const float* src) {
       PPB_CUDA(cudaMemcpyAsync((char*)b.p + off, src, N * 4, cudaMemcpyDefault, s));
@@ -188,6 +188,7 @@ int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, c
     ShellArgs a = ctx->shell_args(ctx->sync, shells, n, alatt, aos.as<float4>(), dl);
     a.pk = PeakParams{d_lin.as<int64_t>(), dRf, d_ir2.as<int32_t>(), dZ, dfc};
     a.npk = npk;
+    a.r2lim = r2lim ? (const int32_t*)stage_in(d_lim, r2lim, npk * 4, s) : nullptr;
     double* dout = out;
     if (!is_device_ptr(out)) {
       d_out.ensure(npk * RES_N * 8);
@@ -212,6 +213,24 @@ int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, c
     ctx->set_error("unknown error");
     return PPB_ERR_INVALID;
   }
+}
+
+int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, const float* etay,
+                          const float* etaz, const float* eta2x, const float* eta2y, const float* eta2z,
+                          const float* lapd, int32_t n, int32_t nhunt, int64_t npk, const int64_t* ipp,
+                          const double* Rf, const int64_t* ir2min, const double* ZZon, const double* fcrit,
+                          double alatt, int32_t plain, double* out) {
+  return analyse_peaks_impl(ctx, delta, etax, etay, etaz, eta2x, eta2y, eta2z, lapd, n, nhunt, npk, ipp, Rf, ir2min,
+                            ZZon, fcrit, nullptr, alatt, plain, out);
+}
+
+int32_t ppb_analyse_peaks_lim(ppb_ctx* ctx, const float* delta, const float* etax, const float* etay,
+                              const float* etaz, const float* eta2x, const float* eta2y, const float* eta2z,
+                              const float* lapd, int32_t n, int32_t nhunt, int64_t npk, const int64_t* ipp,
+                              const double* Rf, const int64_t* ir2min, const double* ZZon, const double* fcrit,
+                              const int32_t* r2lim, double alatt, int32_t plain, double* out) {
+  return analyse_peaks_impl(ctx, delta, etax, etay, etaz, eta2x, eta2y, eta2z, lapd, n, nhunt, npk, ipp, Rf, ir2min,
+                            ZZon, fcrit, r2lim, alatt, plain, out);
 }
 
 // Shell-kernel statistics of the last call: cell visits and the five

@@ -620,6 +620,34 @@ void check_shell_stats(const ShellStats& st) {
 
 }  // namespace
 
+void generate_fields_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, float* delta, float* psi, float* psi2,
+                          float* lapd) {
+  PPB_REQUIRE(p->n >= 8 && p->n <= 2048, "n must be in [8, 2048]");
+  PPB_REQUIRE(p->boxsize > 0, "boxsize must be positive");
+  PPB_REQUIRE(p->ilpt == 1 || p->ilpt == 2, "ilpt must be 1 or 2");
+  PPB_REQUIRE(ctx->sh.pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
+  PPB_REQUIRE(psi2 == nullptr || p->ilpt >= 2, "psi2 needs ilpt = 2");
+  PPB_REQUIRE(lapd == nullptr || p->ioutshear >= 1, "lapd needs ioutshear >= 1");
+  const int n = p->n;
+  const int64_t N = (int64_t)n * n * n;
+  Run r{};
+  r.ctx = ctx;
+  r.sl = &sl;
+  r.p = p;
+  r.s = sl.stream;
+  r.L = Launch{sl.stream, &sl.launches};
+  r.plain = p->plain != 0;
+  r.want_lap = p->ioutshear >= 1;
+  TileRes& T = sl.tile_for(n);
+  T.setup(n, r.s);
+  fields_phase(r, T, n, p->boxsize);
+  if (delta) copy_out(delta, T.delta.p, N * 4, r.s);
+  if (psi) copy_out(psi, T.psi.p, 3 * N * 4, r.s);
+  if (psi2) copy_out(psi2, T.psi2.p, 3 * N * 4, r.s);
+  if (lapd) copy_out(lapd, T.lapd.p, N * 4, r.s);
+  PPB_CUDA(cudaStreamSynchronize(r.s));
+}
+
 void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf_in, int nfilt, TileOut* o) {
   check_params(p, Rf_in, nfilt);
   PPB_REQUIRE(ctx->sh.pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");

@@ -96,7 +96,8 @@ EXPORTED = (
     "ppb_launch_count", "ppb_last_shell_stats", "ppb_last_stage_ms", "ppb_alloc_host", "ppb_free_host",
     "ppb_alloc_device", "ppb_free_device", "ppb_shell_counters", "ppb_find_peaks_noalloc",
     "ppb_last_shell_times", "ppb_serve_config", "ppb_submit", "ppb_wait", "ppb_stats_get", "ppb_stats_reset",
-    "ppb_run_multitile", "ppb_merge_catalog",
+    "ppb_run_multitile", "ppb_merge_catalog", "ppb_set_collapse_table_f64", "ppb_generate_fields",
+    "ppb_analyse_peaks_lim",
 )
 
 
@@ -143,6 +144,9 @@ def load_library():
     L.ppb_stats_reset.argtypes = [P]
     L.ppb_run_multitile.argtypes = [P, ctypes.POINTER(_TileParams), P, I32, I32, P, I32, ctypes.POINTER(_HaloBuf)]
     L.ppb_merge_catalog.argtypes = [P, P, I64, I32, P, ctypes.POINTER(ctypes.c_int64)]
+    L.ppb_set_collapse_table_f64.argtypes = [P, P, I32, I32, I32, D, D, D, D, D, D]
+    L.ppb_generate_fields.argtypes = [P, ctypes.POINTER(_TileParams), P, P, P, P]
+    L.ppb_analyse_peaks_lim.argtypes = [P] * 9 + [I32, I32, I64, P, P, P, P, P, P, D, I32, P]
     for f in ("ppb_alloc_host", "ppb_alloc_device"):
         getattr(L, f).argtypes = [P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
     for f in ("ppb_free_host", "ppb_free_device"):
@@ -567,10 +571,12 @@ class Context:
                 "Rsmooth": np.full(m, float(Rsmooth))}
 
     def analyse_peaks(self, fields: dict, ipp, Rf, ir2min, ZZon, fcrit, alatt: float, nhunt: int,
-                      plain: bool = False) -> np.ndarray:
+                      plain: bool = False, r2lim=None) -> np.ndarray:
         """analyse_peak over a batch (rmax2rs = 0).  fields: delta, etax, etay,
-        etaz and optional eta2x/eta2y/eta2z/lapd (C-order float32, cubic).
-        Returns (npk, 31) float64 (layout RESULT_FIELDS)."""
+        etaz and optional eta2x/eta2y/eta2z/lapd (C-order float32, cubic;
+        numpy arrays or device pointers as ints).  r2lim: optional per-peak
+        shell-list limit r^2 <= r2lim (cells^2).  Returns (npk, 31) float64
+        (layout RESULT_FIELDS)."""
         d = fields["delta"]
         n = d.shape[0]
         if d.shape != (n, n, n):
@@ -582,10 +588,35 @@ class Context:
         out = np.empty((npk, 31), dtype=np.float64)
         a_ipp, a_Rf, a_ir2, a_Z, a_fc = arr(ipp, np.int64), arr(Rf, np.float64), arr(ir2min, np.int64), \
             arr(ZZon, np.float64), arr(fcrit, np.float64)
-        self._check(self.L.ppb_analyse_peaks(self.h, _p(f["delta"]), _p(f["etax"]), _p(f["etay"]), _p(f["etaz"]),
-                                             _p(f["eta2x"]), _p(f["eta2y"]), _p(f["eta2z"]), _p(f["lapd"]), n,
-                                             nhunt, npk, _p(a_ipp), _p(a_Rf), _p(a_ir2), _p(a_Z), _p(a_fc), alatt,
-                                             1 if plain else 0, _p(out)))
+        lim = None if r2lim is None else arr(r2lim, np.int32)
+        self._check(self.L.ppb_analyse_peaks_lim(self.h, _p(f["delta"]), _p(f["etax"]), _p(f["etay"]),
+                                                 _p(f["etaz"]), _p(f["eta2x"]), _p(f["eta2y"]), _p(f["eta2z"]),
+                                                 _p(f["lapd"]), n, nhunt, npk, _p(a_ipp), _p(a_Rf), _p(a_ir2),
+                                                 _p(a_Z), _p(a_fc), _p(lim), alatt, 1 if plain else 0, _p(out)))
+        return out
+
+    def set_collapse_table_f64(self, data: np.ndarray, ranges):
+        """Collapse table with Float64 nodes; data C-order (nz, ny, nx), ranges
+        (X1, X2, Y1, Y2, Z1, Z2)."""
+        d = np.ascontiguousarray(data, dtype=np.float64)
+        nz, ny, nx = d.shape
+        self._check(self.L.ppb_set_collapse_table_f64(self.h, _p(d), nx, ny, nz, *[float(v) for v in ranges]))
+        self._table_key = None
+
+    def generate_fields(self, cfg: PipelineConfig, seed: int, pk_scale: float = 1.0) -> dict:
+        """run_tile's fields (generate_grf, 1LPT, 2LPT, Laplacian) for cfg and
+        seed as C-order float32 host arrays: delta, etax/etay/etaz,
+        eta2x/eta2y/eta2z (ilpt = 2), lapd (ioutshear >= 1)."""
+        p = self._params(cfg, seed, False, pk_scale)
+        n = cfg.n
+        d = np.empty((n, n, n), np.float32)
+        psi = np.empty((3, n, n, n), np.float32)
+        psi2 = np.empty((3, n, n, n), np.float32) if cfg.ilpt >= 2 else None
+        lap = np.empty((n, n, n), np.float32) if cfg.ioutshear >= 1 else None
+        self._check(self.L.ppb_generate_fields(self.h, ctypes.byref(p), _p(d), _p(psi), _p(psi2), _p(lap)))
+        out = dict(delta=d, etax=psi[0], etay=psi[1], etaz=psi[2], lapd=lap)
+        if psi2 is not None:
+            out.update(eta2x=psi2[0], eta2y=psi2[1], eta2z=psi2[2])
         return out
 
 
