@@ -304,7 +304,7 @@ def run_ours(args, dist: Dist):
             "gpu_launches": int(launches),
             "roofline": {"kernel": "gather_kernel (shell sums)", "bound": "hbm",
                          "achieved": achieved, "peak": peaks[0], "unit": "GB/s",
-                         "frac": achieved / peaks[0] if peaks[0] else None, "traffic": GATHER_TRAFFIC_384,
+                         "frac": achieved / peaks[0] if peaks[0] else None, "traffic": GATHER_TRAFFIC_384 if n == 384 else None,
                          "peak_source": peaks[1],
                          "alg_bytes_per_launch": bytes_alg / max(1, args.steps),
                          "kernel_ms_per_launch": gather_ms / max(1, args.steps),
@@ -320,8 +320,8 @@ def run_ours(args, dist: Dist):
 
 # DRAM bytes (read + write) of one gather_kernel launch on the 384^3 tile,
 # scaled from the ncu capture of the same kernel on the 256^3 tile by the cell
-# visits (profiles/gather_kernel_run_tile_256.md); None until captured
-GATHER_TRAFFIC_384 = None
+# visits (profiles/gather_kernel_run_tile_256.md): 4.64 GB x 824.5M / 179.3M
+GATHER_TRAFFIC_384 = 21.35e9
 
 
 def _plain_compare(ctx, cfg, seed, dev_out, cap, opt_tiles_per_s):
