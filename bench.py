@@ -220,6 +220,7 @@ def run_ours(args, dist: Dist):
     n = args.n
     gpu = dist.local
     ctx = pp.Context(gpu)
+    _apply_options(ctx, args)
     k, P = powerspec.eh_table()
     T = pp.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat"))
     ctx.set_pk_table(k, P)
@@ -310,6 +311,8 @@ def run_ours(args, dist: Dist):
                          "kernel_ms_per_launch": gather_ms / max(1, args.steps),
                          "shell_stage_ms_per_step": shell_ms / max(1, args.steps)},
             "clocks": clk,
+            "graphs": ctx.graph_stats(),
+            "autotune": ctx.tune_entries(),
         }
         line.update(extra)
     ctx.free_device(dev_out)
@@ -390,6 +393,7 @@ def run_serve(args, dist: Dist):
     if dist.rank != 0:
         return None
     ctx = pp.Context(dist.local)
+    _apply_options(ctx, args)
     k, P = powerspec.eh_table()
     ctx.set_pk_table(k, P)
     ctx.set_collapse_table(pp.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat")))
@@ -463,6 +467,7 @@ def run_lightcone(args, dist: Dist):
                             rmax2rs=0.0, cenx=cen, ceny=cen, cenz=cen)
     tiles = [(1, 1, 1), (2, 1, 1), (1, 2, 1), (2, 2, 1)]
     ctx = pp.Context(dist.local)
+    _apply_options(ctx, args)
     k, P = powerspec.eh_table()
     ctx.set_pk_table(k, P)
     ctx.set_collapse_table(pp.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat")))
@@ -559,6 +564,7 @@ def run_shells_bench(args, dist: Dist):
         return None
     n, alatt, npk = args.shells_n, 2.0, args.shells_peaks
     ctx = pp.Context(dist.local)
+    _apply_options(ctx, args)
     kk = np.logspace(-5, 2, 500)
     ctx.set_pk_table(kk, kk ** -2.5)
     cfg = pp.PipelineConfig(Omx=0.315 - 0.049, OmB=0.049, Omvac=0.685, h=0.674, n=n, boxsize=alatt * n, nbuff=32,
@@ -579,8 +585,9 @@ def run_shells_bench(args, dist: Dist):
     ctx.set_collapse_table_f64(_resampled_table(T), (T.X1, T.X2, T.Y1, T.Y2, T.Z1, T.Z2))
     out = {}
     for name, plain in (("optimised", False), ("plain", True)):
-        ctx.analyse_peaks(f, ipp[:20000], Rf[:20000], ir2[:20000], 1.0, 1.686, alatt, 40, plain=plain,
-                          r2lim=r2lim[:20000])   # warm-up: tables, plans, pool
+        # warm-up on the whole batch: tables, pool, and the autotuner's
+        # timing of the order bricks and collapse widths for this batch
+        ctx.analyse_peaks(f, ipp, Rf, ir2, 1.0, 1.686, alatt, 40, plain=plain, r2lim=r2lim)
         ctx.analyse_peaks(f, ipp, Rf, ir2, 1.0, 1.686, alatt, 40, plain=plain, r2lim=r2lim)
         st = ctx.shell_stats()
         km = st["kernel_ms"]
@@ -591,6 +598,7 @@ def run_shells_bench(args, dist: Dist):
                      "halos": None}
     peaks = _measured_peaks()
     opt = out["optimised"]
+    tune = ctx.tune_entries()
     ctx.close()
     return {"metric": "shell peaks/s (batched shell analysis)", "value": opt["peaks_per_s"], "unit": "peaks/s",
             "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -598,11 +606,20 @@ def run_shells_bench(args, dist: Dist):
             "config": {"workload": f"{npk} peaks on a {n}^3 power-law (k^-2.5) field, R_p lognormal 2-40 cells, "
                                    "FP64 1000x10x10 table", "nmesh": n, "peaks": npk, "sigma_cell": sigma,
                        "pk_scale": scale},
-            "optimised": opt, "plain": out["plain"],
+            "optimised": opt, "plain": out["plain"], "autotune": tune,
+            "roofline": {"kernel": "gather_kernel (compensated)", "bound": "hbm", "achieved": opt["gather_GBps"],
+                         "peak": peaks[0], "unit": "GB/s", "frac": (opt["gather_GBps"] or 0) / peaks[0],
+                         "traffic": None, "peak_source": peaks[1]},
             "optimised_over_plain": out["plain"]["shell_stage_ms"] / opt["shell_stage_ms"],
             "roofline_plain_gather": {"bound": "hbm", "achieved": out["plain"]["gather_GBps"], "peak": peaks[0],
                                       "frac": (out["plain"]["gather_GBps"] or 0) / peaks[0], "unit": "GB/s",
                                       "alg_bytes": out["plain"]["visits"] * 32}}
+
+
+def _apply_options(ctx, args):
+    import peakpatch_b200 as pp
+    ctx.set_option(pp.OPT_GRAPHS, 0 if getattr(args, "no_graphs", False) else 1)
+    ctx.set_option(pp.OPT_AUTOTUNE, 0 if getattr(args, "no_autotune", False) else 1)
 
 
 def _measured_peaks():
@@ -633,6 +650,8 @@ def main():
     ap.add_argument("--shells", action="store_true", help="run the batched shell analysis instead")
     ap.add_argument("--shells-n", type=int, default=512)
     ap.add_argument("--shells-peaks", type=int, default=1_000_000)
+    ap.add_argument("--no-graphs", action="store_true", help="launch kernels one by one instead of as CUDA graphs")
+    ap.add_argument("--no-autotune", action="store_true", help="default shell-stage choices, no autotuning")
     args = ap.parse_args()
     dist = Dist()
     try:

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PPB_ABI_VERSION 2
+#define PPB_ABI_VERSION 3
 
 enum {
   PPB_OK = 0,
@@ -277,6 +277,58 @@ int32_t ppb_shell_counters(ppb_ctx* ctx, int64_t* out16);
  * [0] gather, [1] collapse walk, [2] zvir_half, [3] d2F; *rows = profile
  * rows written (24 doubles each), *batches = peak batches the stage ran in. */
 int32_t ppb_last_shell_times(ppb_ctx* ctx, float* ms4, int64_t* rows, int32_t* batches);
+/* ---- launch options and the autotuner ------------------------------------ */
+/* Context options (no reference counterpart).
+ *  PPB_OPT_GRAPHS     1 (default): the fields, the filter bank and each
+ *                     shell-stage sub-batch (with a multi-tile run's
+ *                     per-tile field windows) are recorded into CUDA graphs,
+ *                     updated in place from one call to the next and
+ *                     launched whole; 0: the same kernels launched one by one.
+ *  PPB_OPT_AUTOTUNE   1 (default): the first shell stage of each kind of
+ *                     batch (grid size, shell list, arithmetic, truncation,
+ *                     per-peak limits, walk length class) with at least
+ *                     PPB_OPT_TUNE_MIN_PEAKS peaks times the gather-order
+ *                     bricks (4, 8, 16, 32 cells, list order) and the
+ *                     collapse widths (1, 2, 4 threads per peak) and keeps
+ *                     the fastest; 0: defaults (8-cell bricks, width by
+ *                     batch size); setting 2 clears the table.
+ *                     Results do not depend on the choice.
+ *  PPB_OPT_TUNE_MIN_PEAKS  smallest batch that is tuned (default 16384).
+ *  PPB_OPT_BRICK_SHIFT     fixes the gather-order brick over the tuner's
+ *                     choice: 2..5 (bricks of 4..32 cells), -1 list order,
+ *                     -2 (default) the tuner's choice.
+ *  PPB_OPT_COLLAPSE_THREADS  fixes the collapse width: 1, 2 or 4, 0 (default)
+ *                     the tuner's choice.
+ * Read-only (ppb_get_option, summed over the context's slots):
+ *  PPB_OPT_GRAPH_LAUNCHES, PPB_OPT_GRAPH_INSTANTIATIONS, PPB_OPT_GRAPH_UPDATES. */
+enum {
+  PPB_OPT_GRAPHS = 1,
+  PPB_OPT_AUTOTUNE = 2,
+  PPB_OPT_TUNE_MIN_PEAKS = 3,
+  PPB_OPT_BRICK_SHIFT = 4,
+  PPB_OPT_COLLAPSE_THREADS = 5,
+  PPB_OPT_GRAPH_LAUNCHES = 16,
+  PPB_OPT_GRAPH_INSTANTIATIONS = 17,
+  PPB_OPT_GRAPH_UPDATES = 18
+};
+int32_t ppb_set_option(ppb_ctx* ctx, int32_t option, int64_t value);
+int32_t ppb_get_option(ppb_ctx* ctx, int32_t option, int64_t* value);
+
+/* One autotuned shell-stage configuration. */
+typedef struct ppb_tune_entry {
+  int32_t n, nshell;          /* grid size, distinct r^2 of the shell list */
+  int32_t comp, adaptive;     /* compensated FP32 sums, adaptive truncation */
+  int32_t limited;            /* per-peak shell limits (ppb_analyse_peaks_lim) */
+  int32_t brick_shift;        /* chosen order brick: 2^brick_shift cells, -1 = list order */
+  int32_t collapse_threads;   /* chosen collapse width, 0 = by batch size */
+  int32_t long_walk;          /* batches after ones with > 8 collapse-walk steps per peak (lightcone) */
+  int64_t npk;                /* peaks of the batch the candidates were timed on */
+  float gather_ms[5];         /* gather kernel: bricks of 4, 8, 16, 32 cells, list order */
+  float collapse_ms[3];       /* collapse kernel: 1, 2, 4 threads per peak */
+} ppb_tune_entry;
+/* Copies up to `cap` entries; *n = the number of entries held. */
+int32_t ppb_tune_entries(ppb_ctx* ctx, ppb_tune_entry* out, int32_t cap, int32_t* n);
+
 /* Per-stage device times (ms) of the last ppb_run_tile_timed call:
  * [0] fields, [1] filter bank + peaks, [2] shell analysis, [3] records. */
 int32_t ppb_last_stage_ms(ppb_ctx* ctx, float* ms4);

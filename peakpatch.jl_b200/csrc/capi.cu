@@ -58,6 +58,7 @@ void Slot::release_buffers() {
   for (DevBuf* b : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
                     &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim})
     b->release();
+  tune_save.release();
 }
 
 size_t Slot::bytes_held() const {
@@ -70,6 +71,7 @@ size_t Slot::bytes_held() const {
 
 TileRes& Slot::tile_for(int n) {
   if (!tile || tile->n != n) {
+    if (tile) PPB_CUDA(cudaStreamSynchronize(stream));   // nothing of the old size in flight
     tile.reset();   // one grid size resident per slot keeps the footprint bounded
     tile = std::make_unique<TileRes>();
   }
@@ -78,6 +80,9 @@ TileRes& Slot::tile_for(int n) {
 
 Slot::~Slot() {
   if (stream) cudaStreamSynchronize(stream);
+  for (auto& g : graphs)
+    if (g.second) cudaGraphExecDestroy(g.second);
+  graphs.clear();
   release_buffers();
   for (auto& e : stage_ev) if (e) cudaEventDestroy(e);
   for (auto& e : shell_ev) if (e) cudaEventDestroy(e);
@@ -202,7 +207,130 @@ ShellArgs ppb_ctx::shell_args(Slot& sl, ShellTable& shells, int n, double alatt,
   return a;
 }
 
-void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, ShellStats* st) {
+void ppb_ctx::captured(Slot& sl, std::map<std::pair<int, int64_t>, cudaGraphExec_t>& graphs, int site, int64_t key,
+                       const std::function<void()>& rec) {
+  if (!sh.use_graphs.load()) {
+    rec();
+    return;
+  }
+  cudaStream_t s = sl.stream;
+  // thread-local mode: other threads (other slots' workers) may allocate
+  // while this stream records
+  PPB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  cudaGraph_t g = nullptr;
+  try {
+    rec();
+  } catch (...) {
+    cudaStreamEndCapture(s, &g);
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    throw;
+  }
+  PPB_CUDA(cudaStreamEndCapture(s, &g));
+  struct Owned {
+    cudaGraph_t g;
+    ~Owned() { if (g) cudaGraphDestroy(g); }
+  } owned{g};
+  size_t nodes = 0;
+  PPB_CUDA(cudaGraphGetNodes(g, nullptr, &nodes));
+  if (nodes == 0) return;
+  cudaGraphExec_t& ex = graphs[{site, key}];
+  if (ex) {
+    cudaGraphExecUpdateResultInfo info{};
+    if (cudaGraphExecUpdate(ex, g, &info) == cudaSuccess) {
+      sl.graph_updates++;
+    } else {   // the launch sequence changed shape: instantiate anew
+      cudaGetLastError();
+      cudaGraphExecDestroy(ex);
+      ex = nullptr;
+    }
+  }
+  if (!ex) {
+    PPB_CUDA(cudaGraphInstantiate(&ex, g, 0));
+    sl.graph_instantiations++;
+  }
+  PPB_CUDA(cudaGraphLaunch(ex, s));
+  sl.graph_launches++;
+}
+
+// an event record that is also a node of the graph being captured (a
+// timing point inside the graph) when the stream is capturing
+static void record_event(cudaEvent_t e, cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  PPB_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs == cudaStreamCaptureStatusActive) PPB_CUDA(cudaEventRecordWithFlags(e, s, cudaEventRecordExternal));
+  else PPB_CUDA(cudaEventRecord(e, s));
+}
+
+// gather order: geometry for every peak and, for brick_shift >= 0, the
+// Morton sort of the peaks by brick (b.order set), else list order
+static void shell_order(Slot& sl, ShellArgs& b, int brick_shift) {
+  Launch L{sl.stream, &sl.launches};
+  if (brick_shift < 0) {
+    launch_shell_geo(L, b, nullptr, nullptr);
+    b.order = nullptr;
+    return;
+  }
+  b.brick_shift = brick_shift;
+  launch_shell_geo(L, b, sl.okey.as<uint32_t>(), sl.oidx.as<int32_t>());
+  size_t tb = sl.otmp.bytes;
+  PPB_CUDA(cub::DeviceRadixSort::SortPairs(sl.otmp.p, tb, sl.okey.as<uint32_t>(), sl.okey2.as<uint32_t>(),
+                                           sl.oidx.as<int32_t>(), sl.oidx2.as<int32_t>(), (int)b.npk, 0, 32,
+                                           sl.stream));
+  sl.launches++;
+  b.order = sl.oidx2.as<int32_t>();
+}
+
+TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool adaptive, int gblocks) {
+  cudaStream_t s = sl.stream;
+  Launch L{s, &sl.launches};
+  TuneEntry te;
+  te.npk = b0.npk;
+  sl.tune_save.ensure(16 * 8);
+  PPB_CUDA(cudaMemcpyAsync(sl.tune_save.p, sl.counters.p, 16 * 8, cudaMemcpyDeviceToDevice, s));
+  cudaEvent_t* ev = sl.shell_ev;
+  // candidates: bricks of 8 (the default, timed first), 4, 16 and 32 cells,
+  // and list order; every run leaves the same per-peak rows
+  static const int bricks[5] = {3, 2, 4, 5, -1};
+  static const int slot_of[5] = {1, 0, 2, 3, 4};
+  ShellArgs b = b0;
+  for (int c = 0; c < 5; c++) {
+    PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, 16, s));
+    shell_order(sl, b, bricks[c]);
+    PPB_CUDA(cudaEventRecord(ev[0], s));
+    launch_shell_gather(L, b, comp, adaptive, gblocks);
+    PPB_CUDA(cudaEventRecord(ev[1], s));
+    PPB_CUDA(cudaEventSynchronize(ev[1]));
+    PPB_CUDA(cudaEventElapsedTime(&te.gather_ms[slot_of[c]], ev[0], ev[1]));
+  }
+  static const int widths[3] = {1, 2, 4};
+  for (int c = 0; c < 3; c++) {
+    PPB_CUDA(cudaEventRecord(ev[0], s));
+    launch_shell_collapse(L, b, nsm, sl.walk_per_peak, widths[c]);
+    PPB_CUDA(cudaEventRecord(ev[1], s));
+    PPB_CUDA(cudaEventSynchronize(ev[1]));
+    PPB_CUDA(cudaEventElapsedTime(&te.collapse_ms[c], ev[0], ev[1]));
+  }
+  // the default wins unless another candidate is at least 3 % faster
+  int bi = 1;
+  for (int c = 0; c < 5; c++)
+    if (te.gather_ms[c] < te.gather_ms[bi]) bi = c;
+  if (!(te.gather_ms[bi] < 0.97f * te.gather_ms[1])) bi = 1;
+  static const int shift_of[5] = {2, 3, 4, 5, -1};
+  te.brick_shift = shift_of[bi];
+  const int wd = shell_collapse_width(b.npk, nsm, sl.walk_per_peak);
+  const int di = wd == 4 ? 2 : wd - 1;
+  int ci = di;
+  for (int c = 0; c < 3; c++)
+    if (te.collapse_ms[c] < te.collapse_ms[ci]) ci = c;
+  te.collapse_threads = te.collapse_ms[ci] < 0.97f * te.collapse_ms[di] ? widths[ci] : 0;
+  PPB_CUDA(cudaMemcpyAsync(sl.counters.p, sl.tune_save.p, 16 * 8, cudaMemcpyDeviceToDevice, s));
+  PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, 16, s));
+  return te;
+}
+
+void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, ShellStats* st,
+                         const std::function<void()>& pre) {
   cudaStream_t stream = sl.stream;
   Launch L{stream, &sl.launches};
   int& bps = sl.gather_bps[comp][adaptive];
@@ -233,6 +361,22 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
   }
   ShellStats s{};
   unsigned long long before[16] = {}, c[16] = {};
+  // autotuned order brick and collapse width for this kind of batch
+  // (the walk class: collapse walks of more than 8 steps per peak in the
+  // slot's previous batch, as on the lightcone, favour other widths)
+  const std::array<int64_t, 6> tkey{a.n, a.nshell, comp, adaptive, a.r2lim != nullptr, sl.walk_per_peak > 8.0};
+  TuneEntry te;
+  bool tuned = false;
+  {
+    std::lock_guard<std::mutex> lk(sh.cache_mu);
+    auto it = sh.tune.find(tkey);
+    if (it != sh.tune.end()) {
+      te = it->second;
+      tuned = true;
+    }
+  }
+  bool tune_now = !tuned && sh.autotune.load() != 0 && a.npk >= sh.tune_min_peaks.load();
+  bool first = true;
   int64_t p0 = 0;
   while (p0 < a.npk) {
     const double want = std::max(1.0, rpp * 1.25);
@@ -258,31 +402,49 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     b.stage = sl.stage.as<double>();
     b.stage_stride = stride;
     b.counters = sl.counters.as<unsigned long long>();
+    b.brick_shift = 3;
     for (int e = 0; e < 10; e++) b.fhalf[e] = std::pow(e / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
-    PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, 16, stream));
-    PPB_CUDA(cudaEventRecord(sl.shell_ev[0], stream));
-    // gather in spatial order: sort the peaks of the batch by brick Morton key
+    // buffers of the spatial order (allocated before any capture)
     sl.okey.ensure(nb * 4 + 16);
     sl.okey2.ensure(nb * 4 + 16);
     sl.oidx.ensure(nb * 4 + 16);
     sl.oidx2.ensure(nb * 4 + 16);
-    launch_shell_geo(L, b, sl.okey.as<uint32_t>(), sl.oidx.as<int32_t>());
-    size_t tb = 0;
-    PPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, sl.okey.as<uint32_t>(), sl.okey2.as<uint32_t>(),
-                                             sl.oidx.as<int32_t>(), sl.oidx2.as<int32_t>(), (int)nb, 0, 32, stream));
-    sl.otmp.ensure(tb + 16);
-    PPB_CUDA(cub::DeviceRadixSort::SortPairs(sl.otmp.p, tb, sl.okey.as<uint32_t>(), sl.okey2.as<uint32_t>(),
-                                             sl.oidx.as<int32_t>(), sl.oidx2.as<int32_t>(), (int)nb, 0, 32, stream));
-    sl.launches++;
-    b.order = sl.oidx2.as<int32_t>();
-    launch_shell_gather(L, b, comp, adaptive, gblocks);
-    PPB_CUDA(cudaEventRecord(sl.shell_ev[1], stream));
-    launch_shell_collapse(L, b, nsm, sl.walk_per_peak);
-    PPB_CUDA(cudaEventRecord(sl.shell_ev[2], stream));
-    launch_shell_zhalf(L, b);
-    PPB_CUDA(cudaEventRecord(sl.shell_ev[3], stream));
-    launch_shell_d2f(L, b, nsm * 16);
-    PPB_CUDA(cudaEventRecord(sl.shell_ev[4], stream));
+    {
+      size_t tb = 0;
+      PPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, sl.okey.as<uint32_t>(), sl.okey2.as<uint32_t>(),
+                                               sl.oidx.as<int32_t>(), sl.oidx2.as<int32_t>(), (int)nb, 0, 32,
+                                               stream));
+      sl.otmp.ensure(tb + 16);
+    }
+    if (tune_now) {
+      if (first && pre) pre();   // the tuning pass reads what `pre` writes
+      te = tune_shells(sl, b, comp, adaptive, gblocks);
+      {
+        std::lock_guard<std::mutex> lk(sh.cache_mu);
+        sh.tune[tkey] = te;
+      }
+      tune_now = false;
+    }
+    const int fb = sh.force_brick.load(), fc = sh.force_collapse.load();
+    if (fb != -2) te.brick_shift = fb;
+    if (fc != 0) te.collapse_threads = fc;
+    // the sub-batch as one graph: geometry, order, gather, collapse,
+    // zvir_half, d2F, with timing events between the kernels
+    captured(sl, sl.graphs, 2, (int64_t)a.n * 4 + (comp ? 2 : 0) + (adaptive ? 1 : 0), [&] {
+      if (first && pre) pre();
+      PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, 16, stream));
+      record_event(sl.shell_ev[0], stream);
+      shell_order(sl, b, te.brick_shift);
+      launch_shell_gather(L, b, comp, adaptive, gblocks);
+      record_event(sl.shell_ev[1], stream);
+      launch_shell_collapse(L, b, nsm, sl.walk_per_peak, te.collapse_threads);
+      record_event(sl.shell_ev[2], stream);
+      launch_shell_zhalf(L, b);
+      record_event(sl.shell_ev[3], stream);
+      launch_shell_d2f(L, b, nsm * 16);
+      record_event(sl.shell_ev[4], stream);
+    });
+    first = false;
     unsigned long long used = 0;
     PPB_CUDA(cudaMemcpyAsync(&used, b.pool_ctr, sizeof(used), cudaMemcpyDeviceToHost, stream));
     PPB_CUDA(cudaMemcpyAsync(c, sl.counters.p, sizeof(c), cudaMemcpyDeviceToHost, stream));
@@ -635,6 +797,91 @@ int32_t ppb_launch_count(ppb_ctx* ctx, int64_t* count) {
   if (!ctx || !count) return PPB_ERR_INVALID;
   *count = ctx->launches_total();
   return PPB_OK;
+}
+
+int32_t ppb_set_option(ppb_ctx* ctx, int32_t option, int64_t value) {
+  if (!ctx) return PPB_ERR_INVALID;
+  PPB_GUARD_BEGIN
+  switch (option) {
+    case PPB_OPT_GRAPHS:
+      PPB_REQUIRE(value == 0 || value == 1, "PPB_OPT_GRAPHS takes 0 or 1");
+      ctx->sh.use_graphs.store((int)value);
+      break;
+    case PPB_OPT_AUTOTUNE:
+      PPB_REQUIRE(value >= 0 && value <= 2, "PPB_OPT_AUTOTUNE takes 0, 1 or 2");
+      if (value == 2) {
+        std::lock_guard<std::mutex> lk(ctx->sh.cache_mu);
+        ctx->sh.tune.clear();
+      }
+      ctx->sh.autotune.store(value == 0 ? 0 : 1);
+      break;
+    case PPB_OPT_TUNE_MIN_PEAKS:
+      PPB_REQUIRE(value >= 1, "PPB_OPT_TUNE_MIN_PEAKS must be >= 1");
+      ctx->sh.tune_min_peaks.store(value);
+      break;
+    case PPB_OPT_BRICK_SHIFT:
+      PPB_REQUIRE(value == -2 || value == -1 || (value >= 2 && value <= 5), "PPB_OPT_BRICK_SHIFT takes -2, -1 or 2..5");
+      ctx->sh.force_brick.store((int)value);
+      break;
+    case PPB_OPT_COLLAPSE_THREADS:
+      PPB_REQUIRE(value == 0 || value == 1 || value == 2 || value == 4, "PPB_OPT_COLLAPSE_THREADS takes 0, 1, 2 or 4");
+      ctx->sh.force_collapse.store((int)value);
+      break;
+    default:
+      throw Error{PPB_ERR_INVALID, "unknown or read-only option"};
+  }
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_get_option(ppb_ctx* ctx, int32_t option, int64_t* value) {
+  if (!ctx || !value) return PPB_ERR_INVALID;
+  PPB_GUARD_BEGIN
+  switch (option) {
+    case PPB_OPT_GRAPHS: *value = ctx->sh.use_graphs.load(); break;
+    case PPB_OPT_AUTOTUNE: *value = ctx->sh.autotune.load(); break;
+    case PPB_OPT_TUNE_MIN_PEAKS: *value = ctx->sh.tune_min_peaks.load(); break;
+    case PPB_OPT_BRICK_SHIFT: *value = ctx->sh.force_brick.load(); break;
+    case PPB_OPT_COLLAPSE_THREADS: *value = ctx->sh.force_collapse.load(); break;
+    case PPB_OPT_GRAPH_LAUNCHES:
+    case PPB_OPT_GRAPH_INSTANTIATIONS:
+    case PPB_OPT_GRAPH_UPDATES: {
+      int64_t v[3];
+      graph_counts(ctx, v);
+      *value = v[option - PPB_OPT_GRAPH_LAUNCHES];
+      break;
+    }
+    default:
+      throw Error{PPB_ERR_INVALID, "unknown option"};
+  }
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_tune_entries(ppb_ctx* ctx, ppb_tune_entry* out, int32_t cap, int32_t* n) {
+  if (!ctx || !n || cap < 0 || (cap > 0 && !out)) return PPB_ERR_INVALID;
+  PPB_GUARD_BEGIN
+  std::lock_guard<std::mutex> lk(ctx->sh.cache_mu);
+  *n = (int32_t)ctx->sh.tune.size();
+  int32_t i = 0;
+  for (const auto& kv : ctx->sh.tune) {
+    if (i >= cap) break;
+    ppb_tune_entry e{};
+    e.n = (int32_t)kv.first[0];
+    e.nshell = (int32_t)kv.first[1];
+    e.comp = (int32_t)kv.first[2];
+    e.adaptive = (int32_t)kv.first[3];
+    e.limited = (int32_t)kv.first[4];
+    e.long_walk = (int32_t)kv.first[5];
+    e.brick_shift = kv.second.brick_shift;
+    e.collapse_threads = kv.second.collapse_threads;
+    e.npk = kv.second.npk;
+    std::memcpy(e.gather_ms, kv.second.gather_ms, sizeof(e.gather_ms));
+    std::memcpy(e.collapse_ms, kv.second.collapse_ms, sizeof(e.collapse_ms));
+    out[i++] = e;
+  }
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
 }
 
 int32_t ppb_last_stage_ms(ppb_ctx* ctx, float* ms4) {

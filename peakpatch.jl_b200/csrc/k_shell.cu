@@ -582,8 +582,9 @@ __device__ __forceinline__ uint32_t spread3(uint32_t v) {
 }
 
 // per-peak geometry (thread per peak) and the gather order key: the Morton
-// index of the peak's 8^3-cell brick, so that peaks whose spheres overlap
-// (of any filter) are gathered close in time and share cached records
+// index of the peak's brick (2^brick_shift cells on a side, 10 bits per
+// axis), so that peaks whose spheres overlap (of any filter) are gathered
+// close in time and share cached records
 __global__ void geo_kernel(ShellArgs a, uint32_t* key, int32_t* idx) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.npk) return;
@@ -603,7 +604,8 @@ __global__ void geo_kernel(ShellArgs a, uint32_t* key, int32_t* idx) {
     const int64_t lin = a.pk.lin[p], n = a.n, n2 = n * n;
     uint32_t k = 0xffffffffu;   // invalid peaks last
     if (lin >= 0 && lin < n2 * n) {
-      const uint32_t i = (uint32_t)(lin % n) >> 3, j = (uint32_t)((lin / n) % n) >> 3, kk = (uint32_t)(lin / n2) >> 3;
+      const int b = a.brick_shift;
+      const uint32_t i = (uint32_t)(lin % n) >> b, j = (uint32_t)((lin / n) % n) >> b, kk = (uint32_t)(lin / n2) >> b;
       k = spread3(i) | (spread3(j) << 1) | (spread3(kk) << 2);
     }
     key[p] = k;
@@ -1265,17 +1267,23 @@ void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive,
   PPB_LAUNCHED(*L.count);
 }
 
-void launch_shell_collapse(Launch L, const ShellArgs& a, int nsm, double walk_steps_per_peak) {
-  // threads per peak: 4 while 4 per peak still fit about 24 warps per SM or
+int shell_collapse_width(int64_t npk, int nsm, double walk_steps_per_peak) {
+  // 4 threads per peak while 4 per peak still fit about 24 warps per SM or
   // when walks are long (more than 8 steps per peak in the previous batch:
-  // the lightcone), else 1 (the device is full and the latency is hidden)
+  // the lightcone), else 2 or 1 (the device is full and the latency hidden)
   const int64_t full = (int64_t)nsm * 24 * 32;
-  int lg = a.npk * 4 <= full ? 2 : (a.npk * 2 <= full ? 1 : 0);
-  if (walk_steps_per_peak > 8.0) lg = 2;
+  if (walk_steps_per_peak > 8.0 || npk * 4 <= full) return 4;
+  return npk * 2 <= full ? 2 : 1;
+}
+
+void launch_shell_collapse(Launch L, const ShellArgs& a, int nsm, double walk_steps_per_peak, int threads_per_peak) {
+  int w = threads_per_peak;
+  if (w != 1 && w != 2 && w != 4) w = shell_collapse_width(a.npk, nsm, walk_steps_per_peak);
+  const int lg = w == 4 ? 2 : w - 1;
   const int64_t blocks = ((a.npk << lg) + 127) / 128;
   if (blocks == 0) return;
-  if (lg == 2) collapse_kernel<4><<<(unsigned)blocks, 128, 0, L.s>>>(a);
-  else if (lg == 1) collapse_kernel<2><<<(unsigned)blocks, 128, 0, L.s>>>(a);
+  if (w == 4) collapse_kernel<4><<<(unsigned)blocks, 128, 0, L.s>>>(a);
+  else if (w == 2) collapse_kernel<2><<<(unsigned)blocks, 128, 0, L.s>>>(a);
   else collapse1_kernel<<<(unsigned)blocks, 128, 0, L.s>>>(a);
   PPB_LAUNCHED(*L.count);
 }

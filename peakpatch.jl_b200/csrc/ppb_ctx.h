@@ -3,6 +3,7 @@
 #pragma once
 #include <array>
 #include <atomic>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -22,10 +23,23 @@ struct TileRes {
   int64_t cap = 0;
   DevBuf keys, vals, ff, lap, keys_s, vals_s, tmp;
   DevBuf p_lin, p_Rf, p_ir2, p_Z, p_fc, p_FcRf, p_d2Rf, p_pos, res, flags, offs, rec, rthl;
+  // executable graphs that hold this grid size's cuFFT plans (fields, filter
+  // bank): they live exactly as long as the plans whose kernels they launch
+  std::map<std::pair<int, int64_t>, cudaGraphExec_t> graphs;
   ~TileRes();
   void setup(int n, cudaStream_t s);
   void ensure_peaks(int64_t c);
   size_t bytes() const;
+};
+
+// one autotuned shell-stage configuration: the gather order brick and the
+// collapse threads per peak, with the timings of every candidate
+struct TuneEntry {
+  int brick_shift = 3;        // -1: list order
+  int collapse_threads = 0;   // 0: the size heuristic
+  int64_t npk = 0;            // peaks of the batch it was measured on
+  float gather_ms[5] = {};    // bricks of 4, 8, 16, 32 cells and list order
+  float collapse_ms[3] = {};  // 1, 2 and 4 threads per peak
 };
 
 struct ShellStats {
@@ -59,6 +73,12 @@ struct Slot {
   double walk_per_peak = 0.0;                       // collapse-walk steps per peak seen last
   ShellStats last_shell{};
   int64_t last_visits = 0, last_npk = 0;
+  // executable graphs of the shell stage (own and CUB kernels only) by
+  // (call site, shape key); updated in place from each new capture,
+  // re-instantiated when the launch sequence changed shape
+  std::map<std::pair<int, int64_t>, cudaGraphExec_t> graphs;
+  int64_t graph_launches = 0, graph_instantiations = 0, graph_updates = 0;
+  DevBuf tune_save;                                 // counters saved around a tuning pass
   void init(int device);
   void release_buffers();
   size_t bytes_held() const;
@@ -92,6 +112,15 @@ struct Shared {
   std::map<int, std::unique_ptr<ShellTable>> shells;                           // by nhunt
   std::map<std::array<double, 4>, std::unique_ptr<GrowthTable>> growth;        // by (Om, OB, OL, h)
   std::map<std::array<double, 4>, std::unique_ptr<std::vector<double>>> chi;   // by (Om, OL, h, zmax)
+  // autotuned shell-stage choices by (n, nshell, comp, adaptive, per-peak
+  // limits, long collapse walks)
+  std::map<std::array<int64_t, 6>, TuneEntry> tune;
+  // options (ppb_set_option)
+  std::atomic<int> use_graphs{1};
+  std::atomic<int> autotune{1};
+  std::atomic<int64_t> tune_min_peaks{16384};
+  std::atomic<int> force_brick{-2};      // -2: tuner's choice
+  std::atomic<int> force_collapse{0};    // 0: tuner's choice
 };
 
 struct Server;   // serve.cu
@@ -120,7 +149,20 @@ struct ppb_ctx {
                           bool need_chi);
   ppb::ShellArgs shell_args(ppb::Slot& sl, ppb::ShellTable& st, int n, double alatt, const float4* aos,
                             const float* lapd);
-  void run_shells(ppb::Slot& sl, ppb::ShellArgs& a, bool comp, bool adaptive, ppb::ShellStats* st);
+  // the shell stage of a peak batch: geometry, spatial order, gather,
+  // collapse, zvir_half, d2F, in pool-sized sub-batches; `pre` records
+  // launches that run ahead of the first sub-batch in the same graph
+  void run_shells(ppb::Slot& sl, ppb::ShellArgs& a, bool comp, bool adaptive, ppb::ShellStats* st,
+                  const std::function<void()>& pre = nullptr);
+  // times the order bricks and collapse widths on one sub-batch and keeps the
+  // fastest for the batch's tuning key (outputs are the same for every choice)
+  ppb::TuneEntry tune_shells(ppb::Slot& sl, const ppb::ShellArgs& b, bool comp, bool adaptive, int gblocks);
+  // records the launches of `rec` on the slot's stream into the graph for
+  // (site, key) of `graphs` and launches it; with graphs off, runs `rec`
+  // directly.  A graph that launches cuFFT kernels must be kept in the map of
+  // the TileRes that owns the plans.
+  void captured(ppb::Slot& sl, std::map<std::pair<int, int64_t>, cudaGraphExec_t>& graphs, int site, int64_t key,
+                const std::function<void()>& rec);
   int64_t launches_total() const;
   ppb_ctx();
   ~ppb_ctx();
@@ -153,4 +195,6 @@ const void* stage_in(DevBuf& buf, const void* src, size_t bytes, cudaStream_t s)
 int64_t merge_catalog_device(Slot& sl, const float* d_rec, int64_t n, int nf, float* d_out);
 // serving (serve.cu)
 void server_stop(ppb_ctx* ctx);
+// graph launches, instantiations and in-place updates over every slot
+void graph_counts(const ppb_ctx* ctx, int64_t* out3);
 }  // namespace ppb

@@ -248,6 +248,20 @@ int64_t ppb_ctx::launches_total() const {
   return t;
 }
 
+namespace ppb {
+void graph_counts(const ppb_ctx* ctx, int64_t* out3) {
+  out3[0] = ctx->sync.graph_launches;
+  out3[1] = ctx->sync.graph_instantiations;
+  out3[2] = ctx->sync.graph_updates;
+  if (ctx->server)
+    for (const auto& st : ctx->server->slots) {
+      out3[0] += st->slot->graph_launches;
+      out3[1] += st->slot->graph_instantiations;
+      out3[2] += st->slot->graph_updates;
+    }
+}
+}  // namespace ppb
+
 extern "C" {
 
 int32_t ppb_serve_config(ppb_ctx* ctx, int32_t slots) {

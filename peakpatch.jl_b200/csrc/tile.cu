@@ -232,6 +232,9 @@ static cufftHandle make_plan(int n, cufftType t, int batch) {
 }
 
 TileRes::~TileRes() {
+  for (auto& g : graphs)   // before the plans whose kernels they launch
+    if (g.second) cudaGraphExecDestroy(g.second);
+  graphs.clear();
   for (cufftHandle h : {r2c, c2r1, c2r2, c2r3, c2r6})
     if (h) cufftDestroy(h);
 }
@@ -459,29 +462,34 @@ int64_t peaks_phase(Run& r, TileRes& T, int n, double box, const std::vector<Win
   float* rw = T.rw.as<float>();
   const int qn = window_table_size(n);
   T.wtab.ensure((size_t)r.nfilt * 2 * qn * sizeof(float));
-  launch_window_tables(L, T.wtab.as<float>(), n, box, r.sl->filt_Rf.as<double>(), r.nfilt, p->wsmooth, r.want_lap);
   int64_t npk = 0;
   for (int attempt = 0; attempt < 2; attempt++) {
-    PPB_CUDA(cudaMemsetAsync(T.mask.p, 0, N, r.s));
-    PPB_CUDA(cudaMemsetAsync(T.count.p, 0, 64, r.s));
     PeakBuf pb{T.keys.as<unsigned long long>(), T.vals.as<uint32_t>(), T.ff.as<float>(), T.lap.as<float>(),
                T.count.as<int>(), T.cap};
-    for (int f = 0; f < r.nfilt; f++) {
-      float2* o1 = r.want_lap ? kw + M : nullptr;
-      launch_window(L, dkp, kw, o1, n, T.wtab.as<float>() + (size_t)f * 2 * qn, inv_n3);
-      if (r.want_lap && !r.plain) {
-        PPB_CUFFT(cufftExecC2R(T.c2r2, (cufftComplex*)kw, rw));
-      } else {
-        PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)kw, rw));
-        if (r.want_lap) PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)(kw + M), rw + N));
+    // the whole filter bank as one graph (window tables, per filter the
+    // window multiply, the inverse transforms and the peak search)
+    r.ctx->captured(*r.sl, T.graphs, 1, (int64_t)n * 4096 + (int64_t)wins.size(), [&] {
+      PPB_CUDA(cudaMemsetAsync(T.mask.p, 0, N, r.s));
+      PPB_CUDA(cudaMemsetAsync(T.count.p, 0, 64, r.s));
+      launch_window_tables(L, T.wtab.as<float>(), n, box, r.sl->filt_Rf.as<double>(), r.nfilt, p->wsmooth,
+                           r.want_lap);
+      for (int f = 0; f < r.nfilt; f++) {
+        float2* o1 = r.want_lap ? kw + M : nullptr;
+        launch_window(L, dkp, kw, o1, n, T.wtab.as<float>() + (size_t)f * 2 * qn, inv_n3);
+        if (r.want_lap && !r.plain) {
+          PPB_CUFFT(cufftExecC2R(T.c2r2, (cufftComplex*)kw, rw));
+        } else {
+          PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)kw, rw));
+          if (r.want_lap) PPB_CUFFT(cufftExecC2R(T.c2r1, (cufftComplex*)(kw + M), rw + N));
+        }
+        for (size_t t = 0; t < wins.size(); t++) {
+          const Win& w = wins[t];
+          launch_peakfind(L, rw + w.off, r.want_lap ? rw + N + w.off : nullptr, T.mask.as<uint8_t>() + w.off, nm,
+                          nm, nm, n, (int64_t)n * n, p->nbuff, w.fcrit,
+                          ((unsigned long long)t << r.fbits) | (unsigned long long)f, pb);
+        }
       }
-      for (size_t t = 0; t < wins.size(); t++) {
-        const Win& w = wins[t];
-        launch_peakfind(L, rw + w.off, r.want_lap ? rw + N + w.off : nullptr, T.mask.as<uint8_t>() + w.off, nm, nm,
-                        nm, n, (int64_t)n * n, p->nbuff, w.fcrit,
-                        ((unsigned long long)t << r.fbits) | (unsigned long long)f, pb);
-      }
-    }
+    });
     int cnt = 0;
     PPB_CUDA(cudaMemcpyAsync(&cnt, T.count.p, 4, cudaMemcpyDeviceToHost, r.s));
     PPB_CUDA(cudaStreamSynchronize(r.s));
@@ -537,7 +545,7 @@ void prep_phase(Run& r, TileRes& T, int64_t npk, int nm, int nwin, const double*
 // phase 4 (Pipeline.jl:200-240) for peaks [p0, p1) on an nm^3 window whose
 // packed records are aos (and Laplacian lapd)
 void shells_phase(Run& r, TileRes& T, int64_t p0, int64_t p1, int nm, const float4* aos, const float* lapd,
-                  ShellStats* acc) {
+                  ShellStats* acc, const std::function<void()>& pre = nullptr) {
   if (p1 <= p0) return;
   ShellArgs a = r.ctx->shell_args(*r.sl, *r.shells, nm, r.alatt, aos, lapd);
   a.pk = PeakParams{T.p_lin.as<int64_t>() + p0, T.p_Rf.as<double>() + p0, T.p_ir2.as<int32_t>() + p0,
@@ -545,7 +553,7 @@ void shells_phase(Run& r, TileRes& T, int64_t p0, int64_t p1, int nm, const floa
   a.npk = p1 - p0;
   a.out = T.res.as<double>() + p0 * RES_N;
   ShellStats st{};
-  r.ctx->run_shells(*r.sl, a, !r.plain, !r.plain, &st);
+  r.ctx->run_shells(*r.sl, a, !r.plain, !r.plain, &st, pre);
   acc->visits += st.visits;
   acc->guard += st.guard;
   acc->akk += st.akk;
@@ -663,11 +671,14 @@ void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const doubl
   if (T.cap == 0) T.ensure_peaks(std::max<int64_t>(1 << 16, std::min<int64_t>(N / 64, 1 << 22)));
   cudaEvent_t* ev = sl.stage_ev;
   PPB_CUDA(cudaEventRecord(ev[0], r.s));
-  fields_phase(r, T, n, box);
-  launch_pack(r.L, T.aos.as<float4>(),
-              FieldWindow{T.delta.as<float>(), T.psi.as<float>(), p->ilpt >= 2 ? T.psi2.as<float>() : nullptr, 0,
-                          n, (int64_t)n * n, N},
-              n);
+  // fields and the packed gather records as one graph
+  ctx->captured(sl, T.graphs, 0, n, [&] {
+    fields_phase(r, T, n, box);
+    launch_pack(r.L, T.aos.as<float4>(),
+                FieldWindow{T.delta.as<float>(), T.psi.as<float>(), p->ilpt >= 2 ? T.psi2.as<float>() : nullptr, 0,
+                            n, (int64_t)n * n, N},
+                n);
+  });
   PPB_CUDA(cudaEventRecord(ev[1], r.s));
   const int64_t npk = peaks_phase(r, T, n, box, {Win{0, (float)r.fcrit_val}}, n);
   PPB_CUDA(cudaEventRecord(ev[2], r.s));
@@ -772,7 +783,7 @@ void run_multitile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const 
   PPB_CUDA(cudaMemcpyAsync(sl.tcen.p, tcen.data(), tcen.size() * 8, cudaMemcpyHostToDevice, r.s));
   cudaEvent_t* ev = sl.stage_ev;
   PPB_CUDA(cudaEventRecord(ev[0], r.s));
-  fields_phase(r, T, n, box);
+  ctx->captured(sl, T.graphs, 0, n, [&] { fields_phase(r, T, n, box); });
   PPB_CUDA(cudaEventRecord(ev[1], r.s));
   int64_t npk = 0;
   if (nwin > 0) npk = peaks_phase(r, T, n, box, wins, nm);
@@ -799,18 +810,20 @@ void run_multitile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const 
   for (int t = 0; t < nwin; t++) {
     const int64_t p1 = p0 + cnt[t];
     if (p1 > p0) {
+      // the tile's chain: its packed records and Laplacian window, then the
+      // shell stage, captured together as one graph per sub-batch
       sl.t_aos.ensure(Nt * 32);
-      launch_pack(r.L, sl.t_aos.as<float4>(),
-                  FieldWindow{T.delta.as<float>(), T.psi.as<float>(), p->ilpt >= 2 ? T.psi2.as<float>() : nullptr,
-                              wins[t].off, n, (int64_t)n * n, N},
-                  nm);
-      const float* lapd = nullptr;
-      if (r.want_lap) {
-        sl.t_lapd.ensure(Nt * 4);
-        launch_extract(r.L, sl.t_lapd.as<float>(), T.lapd.as<float>(), wins[t].off, n, (int64_t)n * n, nm);
-        lapd = sl.t_lapd.as<float>();
-      }
-      shells_phase(r, T, p0, p1, nm, sl.t_aos.as<float4>(), lapd, &st);
+      if (r.want_lap) sl.t_lapd.ensure(Nt * 4);
+      const float* lapd = r.want_lap ? sl.t_lapd.as<float>() : nullptr;
+      const int64_t off = wins[t].off;
+      shells_phase(r, T, p0, p1, nm, sl.t_aos.as<float4>(), lapd, &st, [&] {
+        launch_pack(r.L, sl.t_aos.as<float4>(),
+                    FieldWindow{T.delta.as<float>(), T.psi.as<float>(), p->ilpt >= 2 ? T.psi2.as<float>() : nullptr,
+                                off, n, (int64_t)n * n, N},
+                    nm);
+        if (r.want_lap)
+          launch_extract(r.L, sl.t_lapd.as<float>(), T.lapd.as<float>(), off, n, (int64_t)n * n, nm);
+      });
     }
     p0 = p1;
   }

@@ -81,6 +81,18 @@ class _Stats(ctypes.Structure):
                 ("queued", ctypes.c_int32), ("slots", ctypes.c_int32), ("failed", ctypes.c_int32)]
 
 
+class _TuneEntry(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("nshell", ctypes.c_int32), ("comp", ctypes.c_int32),
+                ("adaptive", ctypes.c_int32), ("limited", ctypes.c_int32), ("brick_shift", ctypes.c_int32),
+                ("collapse_threads", ctypes.c_int32), ("long_walk", ctypes.c_int32), ("npk", ctypes.c_int64),
+                ("gather_ms", ctypes.c_float * 5), ("collapse_ms", ctypes.c_float * 3)]
+
+
+# context options (include/ppb.h)
+OPT_GRAPHS, OPT_AUTOTUNE, OPT_TUNE_MIN_PEAKS, OPT_BRICK_SHIFT, OPT_COLLAPSE_THREADS = 1, 2, 3, 4, 5
+OPT_GRAPH_LAUNCHES, OPT_GRAPH_INSTANTIATIONS, OPT_GRAPH_UPDATES = 16, 17, 18
+
+
 class _HaloBuf(ctypes.Structure):
     _fields_ = [("records", ctypes.c_void_p), ("capacity", ctypes.c_int64), ("count", ctypes.c_int64),
                 ("nfields", ctypes.c_int32), ("RTHLmax", ctypes.c_float), ("npeaks", ctypes.c_int64)]
@@ -97,7 +109,7 @@ EXPORTED = (
     "ppb_alloc_device", "ppb_free_device", "ppb_shell_counters", "ppb_find_peaks_noalloc",
     "ppb_last_shell_times", "ppb_serve_config", "ppb_submit", "ppb_wait", "ppb_stats_get", "ppb_stats_reset",
     "ppb_run_multitile", "ppb_merge_catalog", "ppb_set_collapse_table_f64", "ppb_generate_fields",
-    "ppb_analyse_peaks_lim",
+    "ppb_analyse_peaks_lim", "ppb_set_option", "ppb_get_option", "ppb_tune_entries",
 )
 
 
@@ -147,6 +159,9 @@ def load_library():
     L.ppb_set_collapse_table_f64.argtypes = [P, P, I32, I32, I32, D, D, D, D, D, D]
     L.ppb_generate_fields.argtypes = [P, ctypes.POINTER(_TileParams), P, P, P, P]
     L.ppb_analyse_peaks_lim.argtypes = [P] * 9 + [I32, I32, I64, P, P, P, P, P, P, D, I32, P]
+    L.ppb_set_option.argtypes = [P, I32, I64]
+    L.ppb_get_option.argtypes = [P, I32, ctypes.POINTER(ctypes.c_int64)]
+    L.ppb_tune_entries.argtypes = [P, ctypes.POINTER(_TuneEntry), I32, ctypes.POINTER(ctypes.c_int32)]
     for f in ("ppb_alloc_host", "ppb_alloc_device"):
         getattr(L, f).argtypes = [P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
     for f in ("ppb_free_host", "ppb_free_device"):
@@ -373,6 +388,39 @@ class Context:
                 "akk_overrun": int(raw[7]), "bad_peaks": int(raw[8]), "walk_steps": int(raw[9]),
                 "kernel_ms": dict(zip(("gather", "collapse", "zvir_half", "d2f"), kms.tolist())),
                 "pool_rows": rows.value, "batches": nb.value}
+
+    # ---- launch options and the autotuner ----
+    def set_option(self, option: int, value: int):
+        self._check(self.L.ppb_set_option(self.h, option, int(value)))
+
+    def get_option(self, option: int) -> int:
+        v = ctypes.c_int64()
+        self._check(self.L.ppb_get_option(self.h, option, ctypes.byref(v)))
+        return v.value
+
+    def graph_stats(self):
+        return {"launches": self.get_option(OPT_GRAPH_LAUNCHES),
+                "instantiations": self.get_option(OPT_GRAPH_INSTANTIATIONS),
+                "updates": self.get_option(OPT_GRAPH_UPDATES)}
+
+    def tune_entries(self):
+        """The autotuned shell-stage configurations: one dict per kind of batch
+        with the chosen gather-order brick (cells on a side, 0 = list order),
+        the collapse width and every candidate's time."""
+        n = ctypes.c_int32()
+        self._check(self.L.ppb_tune_entries(self.h, None, 0, ctypes.byref(n)))
+        buf = (_TuneEntry * max(1, n.value))()
+        self._check(self.L.ppb_tune_entries(self.h, buf, n.value, ctypes.byref(n)))
+        out = []
+        for e in buf[:n.value]:
+            out.append({"n": e.n, "nshell": e.nshell, "comp": bool(e.comp), "adaptive": bool(e.adaptive),
+                        "limited": bool(e.limited), "long_walk": bool(e.long_walk),
+                        "brick": (1 << e.brick_shift) if e.brick_shift >= 0 else 0,
+                        "collapse_threads": e.collapse_threads, "npk": e.npk,
+                        "gather_ms": dict(zip(("brick4", "brick8", "brick16", "brick32", "list"),
+                                              [round(x, 4) for x in e.gather_ms])),
+                        "collapse_ms": dict(zip(("w1", "w2", "w4"), [round(x, 4) for x in e.collapse_ms]))})
+        return out
 
     def stage_ms(self):
         a = np.zeros(4, np.float32)

@@ -1,0 +1,91 @@
+"""CUDA-graph launches and the shell-stage autotuner.  Neither may change a
+result: the records of run_tile and run_multitile are compared byte for byte
+with graphs on and off and under every gather-order brick and collapse width
+the autotuner chooses from."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+import peakpatch_b200 as pp
+from conftest import filter_bank
+from test_gpu_parity import tile_config
+
+RF = [f[2] for f in filter_bank()]
+
+
+@pytest.fixture(scope="module")
+def tctx(julia_table, eh_pk):
+    T = julia_table
+    with pp.Context(0) as c:
+        c.set_pk_table(*eh_pk)
+        c.set_collapse_table(pp.CollapseTable(T.data, T.x1, T.x2, T.y1, T.y2, T.z1, T.z2))
+        yield c
+
+
+def _defaults(c):
+    c.set_option(pp.OPT_GRAPHS, 1)
+    c.set_option(pp.OPT_AUTOTUNE, 0)
+    c.set_option(pp.OPT_BRICK_SHIFT, -2)
+    c.set_option(pp.OPT_COLLAPSE_THREADS, 0)
+    c.set_option(pp.OPT_TUNE_MIN_PEAKS, 16384)
+
+
+def test_graphs_on_and_off_give_the_same_records(tctx):
+    _defaults(tctx)
+    cfg = tile_config()
+    tctx.set_option(pp.OPT_GRAPHS, 0)
+    a, _, _ = tctx.run_tile_arrays(cfg, 31, RF)
+    g0 = tctx.graph_stats()
+    tctx.set_option(pp.OPT_GRAPHS, 1)
+    b, _, _ = tctx.run_tile_arrays(cfg, 31, RF)
+    g1 = tctx.graph_stats()
+    assert g1["launches"] >= g0["launches"] + 3   # fields, filter bank, shell stage
+    c, _, _ = tctx.run_tile_arrays(cfg, 32, RF)   # another seed: the graphs are updated in place
+    d, _, _ = tctx.run_tile_arrays(cfg, 31, RF)
+    g3 = tctx.graph_stats()
+    assert g3["updates"] >= g1["updates"] + 4
+    assert a.tobytes() == b.tobytes() == d.tobytes()
+    assert c.tobytes() != a.tobytes()
+
+
+def test_multitile_chain_graphs_on_and_off(tctx):
+    _defaults(tctx)
+    cfg = tile_config()
+    tctx.set_option(pp.OPT_GRAPHS, 0)
+    a, _, _ = tctx.run_multitile_arrays(cfg, 5, RF, ntile=2, tiles=[(1, 1, 1), (2, 2, 1)])
+    tctx.set_option(pp.OPT_GRAPHS, 1)
+    b, _, _ = tctx.run_multitile_arrays(cfg, 5, RF, ntile=2, tiles=[(1, 1, 1), (2, 2, 1)])
+    assert len(a) > 20 and a.tobytes() == b.tobytes()
+
+
+@pytest.mark.parametrize("brick", [-1, 2, 3, 4, 5])
+def test_every_order_brick_and_collapse_width_gives_the_same_records(tctx, brick):
+    _defaults(tctx)
+    cfg = tile_config()
+    ref, _, _ = tctx.run_tile_arrays(cfg, 41, RF)
+    tctx.set_option(pp.OPT_BRICK_SHIFT, brick)
+    for w in (1, 2, 4):
+        tctx.set_option(pp.OPT_COLLAPSE_THREADS, w)
+        g, _, _ = tctx.run_tile_arrays(cfg, 41, RF)
+        assert g.tobytes() == ref.tobytes(), (brick, w)
+    _defaults(tctx)
+
+
+def test_autotuner_times_every_candidate_and_keeps_the_records(tctx):
+    _defaults(tctx)
+    cfg = tile_config()
+    ref, _, _ = tctx.run_tile_arrays(cfg, 43, RF)
+    tctx.set_option(pp.OPT_TUNE_MIN_PEAKS, 1)
+    tctx.set_option(pp.OPT_AUTOTUNE, 2)   # clear the table, tune on next use
+    a, _, npk = tctx.run_tile_arrays(cfg, 43, RF)
+    ents = tctx.tune_entries()
+    assert len(ents) == 1
+    e = ents[0]
+    assert e["n"] == cfg.n and e["comp"] and e["adaptive"] and not e["limited"] and e["npk"] == npk
+    assert all(v > 0 for v in e["gather_ms"].values()) and all(v > 0 for v in e["collapse_ms"].values())
+    assert e["brick"] in (0, 4, 8, 16, 32) and e["collapse_threads"] in (0, 1, 2, 4)
+    b, _, _ = tctx.run_tile_arrays(cfg, 43, RF)   # runs with the tuned choice, no new entry
+    assert len(tctx.tune_entries()) == 1
+    assert ref.tobytes() == a.tobytes() == b.tobytes()
+    _defaults(tctx)

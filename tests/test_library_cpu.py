@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert pp.load_library().ppb_abi_version() == 2
+    assert pp.load_library().ppb_abi_version() == 3
 
 
 def test_tile_params_layout_matches_the_header():
@@ -37,6 +37,18 @@ def test_tile_params_layout_matches_the_header():
     assert ctypes.sizeof(pp._TileParams) == 168
     assert pp._TileParams.pk_scale.offset == 144
     assert ctypes.sizeof(pp._Stats) == 8 * 6 + 8 * 2 + 4 * 4
+
+
+def test_tune_entry_layout_and_option_entry_points():
+    # ppb_tune_entry: 8 int32, an int64, 5 + 3 floats
+    assert ctypes.sizeof(pp._TuneEntry) == 8 * 4 + 8 + 8 * 4
+    assert pp._TuneEntry.gather_ms.offset == 40
+    L = pp.load_library()
+    v = ctypes.c_int64()
+    n = ctypes.c_int32()
+    assert L.ppb_set_option(None, pp.OPT_GRAPHS, 1) == -1
+    assert L.ppb_get_option(None, pp.OPT_GRAPHS, ctypes.byref(v)) == -1
+    assert L.ppb_tune_entries(None, None, 0, ctypes.byref(n)) == -1
 
 
 def test_serving_entry_points_reject_bad_arguments():
