@@ -2,6 +2,7 @@
 // the context methods.  No C++ exception crosses the boundary: every entry
 // point catches ppb::Error (and anything else) and returns a status code,
 // keeping the message for ppb_last_error().
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -54,7 +55,9 @@ void Slot::init(int dev) {
 }
 
 void Slot::release_buffers() {
-  tile.reset();
+  if (stream) PPB_CUDA(cudaStreamSynchronize(stream));
+  tiles.clear();
+  tile_lru.clear();
   for (DevBuf* b : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
                     &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim})
     b->release();
@@ -62,20 +65,53 @@ void Slot::release_buffers() {
 }
 
 size_t Slot::bytes_held() const {
-  size_t b = tile ? tile->bytes() : 0;
+  size_t b = shell_bytes();
+  for (const auto& t : tiles) b += t.second->bytes();
+  return b;
+}
+
+size_t Slot::shell_bytes() const {
+  size_t b = 0;
   for (const DevBuf* d : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool,
                           &okey, &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim})
     b += d->bytes;
   return b;
 }
 
+int Slot::lru_tile(int keep) const {
+  for (int m : tile_lru)
+    if (m != keep) return m;
+  return 0;
+}
+
+uint64_t Slot::drop_tile(int n) {
+  auto it = tiles.find(n);
+  if (it == tiles.end()) return 0;
+  PPB_CUDA(cudaStreamSynchronize(stream));   // nothing of that size in flight
+  const uint64_t b = it->second->bytes();
+  tiles.erase(it);
+  tile_lru.erase(std::remove(tile_lru.begin(), tile_lru.end(), n), tile_lru.end());
+  return b;
+}
+
 TileRes& Slot::tile_for(int n) {
-  if (!tile || tile->n != n) {
-    if (tile) PPB_CUDA(cudaStreamSynchronize(stream));   // nothing of the old size in flight
-    tile.reset();   // one grid size resident per slot keeps the footprint bounded
-    tile = std::make_unique<TileRes>();
+  auto it = tiles.find(n);
+  if (it == tiles.end()) {
+    while ((int)tiles.size() >= std::max(1, max_tiles)) drop_tile(lru_tile(n));
+    if (!tiles.empty()) {   // room for the new size's buffers, else give up older sizes
+      const uint64_t need = tile_bytes_estimate(n);
+      size_t fr = 0, tot = 0;
+      PPB_CUDA(cudaMemGetInfo(&fr, &tot));
+      while (!tiles.empty() && (uint64_t)fr < need + need / 4) {
+        drop_tile(lru_tile(n));
+        PPB_CUDA(cudaMemGetInfo(&fr, &tot));
+      }
+    }
+    it = tiles.emplace(n, std::make_unique<TileRes>()).first;
   }
-  return *tile;
+  tile_lru.erase(std::remove(tile_lru.begin(), tile_lru.end(), n), tile_lru.end());
+  tile_lru.push_back(n);
+  return *it->second;
 }
 
 Slot::~Slot() {

@@ -62,7 +62,9 @@ struct Slot {
   cudaEvent_t stage_ev[5] = {};
   cudaEvent_t shell_ev[5] = {};
   float stage_ms[4] = {0, 0, 0, 0};
-  std::unique_ptr<TileRes> tile;                    // one grid size at a time
+  std::map<int, std::unique_ptr<TileRes>> tiles;    // resident grid sizes (buffers, plans, graphs)
+  std::vector<int> tile_lru;                        // resident sizes, least recently used first
+  int max_tiles = 4;                                // sizes kept resident at most
   DevBuf filt_Rf, filt_ir2;                         // filter bank of the run
   DevBuf g_a, g_D, g_f, chi;                        // growth / chi tables of the run
   DevBuf stage, counters, ctl, hdr, geo, mlim, pool;   // shell stage
@@ -82,7 +84,16 @@ struct Slot {
   void init(int device);
   void release_buffers();
   size_t bytes_held() const;
+  size_t shell_bytes() const;   // held outside the per-size buffers (shell stage and tables)
+  // the buffers of grid size n: kept from an earlier run of that size when
+  // resident, else new, after dropping least recently used sizes while more
+  // than max_tiles - 1 are resident or free memory is short of n's estimate
   TileRes& tile_for(int n);
+  bool has_tile(int n) const { return tiles.count(n) != 0; }
+  // least recently used resident size other than `keep` (0: none)
+  int lru_tile(int keep) const;
+  // frees the buffers of size n; returns the bytes freed
+  uint64_t drop_tile(int n);
   ~Slot();
 };
 
@@ -184,6 +195,9 @@ void generate_fields_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, floa
                           float* lapd);
 // device bytes a run of this grid size holds at most (admission estimate)
 uint64_t tile_footprint(const ppb_tile_params* p);
+// the part of it held per grid size (TileRes) and per slot (shell stage)
+uint64_t tile_bytes_estimate(int n);
+uint64_t shell_bytes_estimate(int n);
 // copy `bytes` from device memory to dst (host or device)
 void copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);
 // true when p points to device memory

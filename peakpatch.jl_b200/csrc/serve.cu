@@ -2,16 +2,17 @@
 // execution slots (one CUDA stream and buffer set each) as slots and HBM
 // budget free up, so that tiles of different requests overlap on the device.
 //
-// Threads: one dispatcher and one worker per slot.  The dispatcher takes the
-// oldest queued request, picks an idle slot (one whose buffers already have
-// the request's grid size first) and admits the request when the bytes
-// reserved by all slots, with this slot's reservation replaced by the
-// request's footprint, fit the context's HBM budget.  Idle slots give up
-// their cached buffers when memory is short; a request that does not fit with
-// every other slot idle and empty fails with PPB_ERR_ADMISSION.  A worker runs
-// run_tile_core on its slot, copies the records to host memory and marks the
-// request done.  Results do not depend on which slot ran a request or on what
-// ran beside it.
+// Threads: one dispatcher and one worker per slot.  Slots keep the buffers,
+// cuFFT plans and graphs of up to four grid sizes resident between requests.
+// The dispatcher takes the oldest queued request, picks an idle slot (one
+// that already holds the request's grid size first) and admits the request
+// when the bytes held by all slots, plus the request's footprint if its slot
+// does not hold that size yet, fit the context's HBM budget.  When memory is
+// short, idle slots give up their least recently used sizes (then all their
+// buffers); a request that does not fit with every other slot idle and empty
+// fails with PPB_ERR_ADMISSION.  A worker runs run_tile_core on its slot,
+// copies the records to host memory and marks the request done.  Results do
+// not depend on which slot ran a request or on what ran beside it.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -45,8 +46,8 @@ struct SlotState {
   std::unique_ptr<Slot> slot;
   std::thread th;
   std::shared_ptr<Request> job;   // the running request, null when idle
-  uint64_t reserved = 0;          // bytes charged to this slot
-  int n_cached = 0;               // grid size of its buffers (0: none)
+  uint64_t reserved = 0;          // bytes charged to this slot: what it holds, plus the
+                                  // footprint of a new grid size while that runs
 };
 
 struct Server {
@@ -93,9 +94,10 @@ void Server::dispatch_loop() {
     cv_dispatch.wait(lk, [&] { return stop || !queue.empty(); });
     if (stop) return;
     std::shared_ptr<Request> r = queue.front();
+    const int n = r->p.n;
     SlotState* pick = nullptr;
     for (auto& s : slots)
-      if (!s->job && s->n_cached == r->p.n) { pick = s.get(); break; }
+      if (!s->job && s->slot->has_tile(n)) { pick = s.get(); break; }
     if (!pick)
       for (auto& s : slots)
         if (!s->job) { pick = s.get(); break; }
@@ -103,16 +105,31 @@ void Server::dispatch_loop() {
       cv_dispatch.wait(lk);
       continue;
     }
-    uint64_t after = in_use - pick->reserved + r->footprint;
-    if (after > budget) {   // let idle slots give their cached buffers back
+    // new bytes: the grid size's buffers unless resident, and the growth of
+    // the slot's shell-stage buffers to this size's estimate
+    const uint64_t sh_now = pick->slot->shell_bytes(), sh_est = shell_bytes_estimate(n);
+    const uint64_t need = (pick->slot->has_tile(n) ? 0 : tile_bytes_estimate(n)) + (sh_est > sh_now ? sh_est - sh_now : 0);
+    uint64_t after = in_use + need;
+    // memory short: idle slots give up their least recently used grid sizes
+    // (never the picked slot's copy of this request's size), then everything
+    for (int pass = 0; pass < 2 && after > budget; pass++) {
       for (auto& s : slots) {
-        if (s->job || s.get() == pick || s->reserved == 0) continue;
-        s->slot->release_buffers();
-        in_use -= s->reserved;
-        s->reserved = 0;
-        s->n_cached = 0;
+        if (s->job || after <= budget) continue;
+        if (pass == 0) {
+          for (int m = s->slot->lru_tile(s.get() == pick ? n : 0); m != 0 && after > budget;
+               m = s->slot->lru_tile(s.get() == pick ? n : 0)) {
+            const uint64_t freed = std::min<uint64_t>(s->slot->drop_tile(m), s->reserved);
+            s->reserved -= freed;
+            in_use -= freed;
+            after -= std::min(after, freed);
+          }
+        } else if (s.get() != pick && s->reserved > 0) {
+          s->slot->release_buffers();
+          in_use -= s->reserved;
+          after -= std::min(after, s->reserved);
+          s->reserved = 0;
+        }
       }
-      after = in_use - pick->reserved + r->footprint;
     }
     if (after > budget) {
       bool busy = false;
@@ -129,12 +146,8 @@ void Server::dispatch_loop() {
       continue;
     }
     queue.pop_front();
-    if (pick->n_cached != r->p.n && pick->reserved > 0) {   // the slot switches grid size
-      pick->slot->release_buffers();
-      pick->n_cached = 0;
-    }
-    in_use = after;
-    pick->reserved = r->footprint;
+    in_use += need;
+    pick->reserved += need;
     pick->job = r;
     cv_slot.notify_all();
   }
@@ -176,19 +189,15 @@ void Server::worker_loop(SlotState* st) {
     r->nf = o.nfields;
     r->RTHLmax = o.RTHLmax;
     if (status == PPB_OK) {
-      // keep the buffers for the next request of this grid size, charging
-      // what the run actually holds when that exceeds the estimate
-      st->n_cached = r->p.n;
+      // keep the buffers for the next request of this grid size and charge
+      // what the slot actually holds now
       const uint64_t held = st->slot->bytes_held();
-      if (held > st->reserved) {
-        in_use += held - st->reserved;
-        st->reserved = held;
-      }
+      in_use = in_use - st->reserved + held;
+      st->reserved = held;
     } else {
       st->slot->release_buffers();
       in_use -= st->reserved;
       st->reserved = 0;
-      st->n_cached = 0;
     }
     st->job.reset();
     finish(r, Clock::now());

@@ -322,12 +322,22 @@ void check_params(const ppb_tile_params* p, const double* Rf, int nfilt) {
                 "(mask writes of RadialShell.jl:793-802 race with the pre-mask read at :311-316)"};
 }
 
-uint64_t tile_footprint(const ppb_tile_params* p) {
-  const uint64_t n = (uint64_t)p->n, N = n * n * n, M = (n / 2 + 1) * n * n;
+uint64_t tile_footprint(const ppb_tile_params* p) { return tile_bytes_estimate(p->n) + shell_bytes_estimate(p->n); }
+
+uint64_t tile_bytes_estimate(int nn) {
+  const uint64_t n = (uint64_t)nn, N = n * n * n, M = (n / 2 + 1) * n * n;
   // TileRes fields: delta, psi (3), psi2 (3), lapd, rw (6), mask, aos (8 floats), dk + kw (7 complex)
   const uint64_t fields = N * 4 * (1 + 3 + 3 + 1 + 6) + N + N * 32 + M * 8 * 7;
-  // peaks, results, records and the shell-stage pool: about 120 bytes per cell
-  return fields + N * 120 + ((uint64_t)64 << 20);
+  // peak, result and record buffers: about 1/64 peak per cell, 0.5 KB each;
+  // plans and their work areas
+  return fields + N * 8 + ((uint64_t)64 << 20);
+}
+
+uint64_t shell_bytes_estimate(int nn) {
+  const uint64_t n = (uint64_t)nn, N = n * n * n;
+  // the shell stage's per-warp staging rows (16 warps per SM, 600 shells of
+  // 24 doubles) and the profile pool (about 100 bytes per cell)
+  return (uint64_t)148 * 16 * 600 * 24 * 8 + N * 100;
 }
 
 namespace {

@@ -62,6 +62,25 @@ def test_each_result_is_the_same_alone_and_in_the_mix():
         assert st["slots"] == 3 and st["queued"] == 0 and st["in_flight"] == 0
 
 
+def test_tight_budget_evicts_resident_sizes_and_keeps_every_result():
+    # about 900 MB: a 128^3 request's estimate is ~0.8 GB (0.33 GB of grid-size
+    # buffers, the rest shell-stage buffers of its slot), so three slots
+    # cycling through the mix must give resident sizes back to admit the next
+    with pp.Context(0, hbm_budget=900 << 20) as ctx:
+        _tables(ctx)
+        alone = [ctx.run_tile_arrays(_cfg(n, ievol), seed, RF, pk_scale=(s8 / 0.808) ** 2)
+                 for n, seed, s8, ievol in MIX]
+        ctx.serve_config(3)
+        tickets = [ctx.submit(_cfg(n, ievol), seed, RF, pk_scale=(s8 / 0.808) ** 2) for n, seed, s8, ievol in MIX]
+        for t, (rec0, rmax0, npk0), m in zip(tickets, alone, MIX):
+            rec, rmax, npk = ctx.wait(t)
+            assert npk == npk0 and rec.tobytes() == rec0.tobytes() and rmax == rmax0, m
+        st = ctx.serve_stats()
+        assert st["failed"] == 0 and st["tiles_done"] == len(MIX)
+        # admission works on estimates; what the slots then hold may exceed them a little
+        assert st["hbm_in_use"] <= 1.25 * (900 << 20)
+
+
 def test_sigma8_rescale_changes_the_catalogue():
     with pp.Context(0) as ctx:
         _tables(ctx)
