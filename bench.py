@@ -13,6 +13,7 @@ Usage:
   python bench.py --serve      # the serving stream: 200 requests, Poisson arrivals
   python bench.py --lightcone  # 4 lightcone tiles of 384^3 (run_multitile) + merge_catalog
   python bench.py --shells     # batched shell analysis: 10^6 peaks on a 512^3 power-law field
+  python bench.py --table      # collapse-table generation (make_table, RK4) on the GPU
 Under torchrun each rank runs independent tiles on its own GPU (run_tile
 does not shard: replicas) with its own seed; the job value is the tiles of
 all ranks over the slowest rank's device time.
@@ -643,6 +644,47 @@ def run_shells_bench(args, dist: Dist):
                                       "alg_bytes": out["plain"]["visits"] * 32}}
 
 
+def run_table_bench(args, dist: Dist):
+    """Collapse-table generation: make_table with the RK4 solver and the
+    default 50 x 20 x 20 grid (log10 F in [log10 1.5, log10 8], e_v in
+    [0, 0.5], p_v/e_v in [-1, 1]) for the Planck 2018 cosmology of the tile
+    benchmark, on the GPU (one FP64 integration per node), beside the same
+    table computed by the oracle on every host core."""
+    import peakpatch_b200 as pp
+    if dist.rank != 0:
+        return None
+    cosmo = (0.315, 0.049, 0.685, 0.674)
+    ctx = pp.Context(dist.local)
+    for _ in range(max(1, args.warmup)):
+        ctx.make_table(*cosmo)
+    ms, steps = [], 0
+    for _ in range(args.steps):
+        ctx.make_table(*cosmo)
+        st = ctx.table_stats()
+        ms.append(st["ms"])
+        steps = st["rk4_steps"]
+    ctx.close()
+    t = statistics.median(ms)
+    line = {"metric": "collapse tables/s (make_table, RK4, 50x20x20)", "value": 1000.0 / t, "unit": "tables/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": t,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+            "dtype": "f64", "config": {"workload": "make_table RK4, default CollapseTableParams and EllipsoidParams, "
+                                                   "Om 0.315 Ob 0.049 OL 0.685 h 0.674", "nodes": 20000},
+            "rk4_steps_per_table": steps, "rk4_steps_per_s": steps / (t / 1000.0)}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        oracle.build()
+        cores = os.cpu_count() or 1
+        oracle.set_threads(cores)
+        t0 = time.perf_counter()
+        oracle.make_table(*cosmo)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "tables/s", "cores": cores, "kind": "port",
+                                "sample": "the whole 50x20x20 table, oracle C++/OpenMP (one node per task)"}
+    return line
+
+
 def _apply_options(ctx, args):
     import peakpatch_b200 as pp
     ctx.set_option(pp.OPT_GRAPHS, 0 if getattr(args, "no_graphs", False) else 1)
@@ -677,6 +719,7 @@ def main():
     ap.add_argument("--shells", action="store_true", help="run the batched shell analysis instead")
     ap.add_argument("--shells-n", type=int, default=512)
     ap.add_argument("--shells-peaks", type=int, default=1_000_000)
+    ap.add_argument("--table", action="store_true", help="run the collapse-table generation instead")
     ap.add_argument("--no-graphs", action="store_true", help="launch kernels one by one instead of as CUDA graphs")
     ap.add_argument("--no-autotune", action="store_true", help="default shell-stage choices, no autotuning")
     args = ap.parse_args()
@@ -687,6 +730,11 @@ def main():
             return
         if args.shells:
             line = run_shells_bench(args, dist)
+            if line is not None:
+                print(json.dumps(line), flush=True)
+            return
+        if args.table:
+            line = run_table_bench(args, dist)
             if line is not None:
                 print(json.dumps(line), flush=True)
             return

@@ -277,6 +277,34 @@ int32_t ppb_shell_counters(ppb_ctx* ctx, int64_t* out16);
  * [0] gather, [1] collapse walk, [2] zvir_half, [3] d2F; *rows = profile
  * rows written (24 doubles each), *batches = peak batches the stage ran in. */
 int32_t ppb_last_shell_times(ppb_ctx* ctx, float* ms4, int64_t* rows, int32_t* batches);
+/* ---- collapse-table generation ------------------------------------------ */
+/* make_table (src/EllipsoidalCollapse/CollapseTable.jl:33-52) with the RK4
+ * solver (EllipsoidParams(cosmo; solver = :rk4), evolve_ellipse_full,
+ * src/EllipsoidalCollapse/EllipsoidalCollapse.jl:518-624), one FP64
+ * integration per node on the GPU.  Fields mirror CosmologyParams (Om is the
+ * total matter density), CollapseTableParams and the EllipsoidParams
+ * defaults (iforce_strat 4, ivir_strat 2, fcoll 0.01 / 0.171 / 0.171,
+ * tfac 0.01, nstepmax 10000, zinit_fac 20; Carlson RD shape integrals). */
+typedef struct ppb_table_params {
+  double Om, OB, OL, h;
+  int32_t Nx, Ny, Nz;            /* nodes along log10 F, e_v, p_v / e_v (50, 20, 20) */
+  int32_t iforce_strat;          /* 0, 1, 3, 4, 5 or 6 */
+  int32_t ivir_strat;            /* 1 or 2 */
+  int32_t nstepmax;
+  double X1, X2;                 /* log10 F range (log10 1.5, log10 8) */
+  double Y1, Y2;                 /* e_v range (0, 0.5) */
+  double Z1, Z2;                 /* p_v / e_v range (-1 + 1e-4, 1 - 1e-4) */
+  double fcoll_1, fcoll_2, fcoll_3, tfac, zinit_fac;
+  int32_t reserved[4];
+} ppb_table_params;
+/* Computes the Nx x Ny x Nz table of 1 + z_vir (-1: no collapse) in double
+ * precision, column-major (i fastest), into `out` (host or device, may be
+ * null) and, with install = 1, makes it the context's collapse table rounded
+ * to Float32 (the reference's table) or, with install = 2, with Float64
+ * nodes.  ppb_last_table_stats reports the device time and the RK4 steps. */
+int32_t ppb_make_collapse_table(ppb_ctx* ctx, const ppb_table_params* p, double* out, int32_t install);
+int32_t ppb_last_table_stats(ppb_ctx* ctx, float* ms, int64_t* steps);
+
 /* ---- launch options and the autotuner ------------------------------------ */
 /* Context options (no reference counterpart).
  *  PPB_OPT_GRAPHS     1 (default): the fields, the filter bank and each

@@ -554,6 +554,204 @@ static void dlinear_ab(const OraGrowth& G, double ai, double* Dl, double* HD, do
   }
 }
 
+// ---------------------------------------------------------------------------
+// Collapse-table generation, RK4 path: make_table (CollapseTable.jl:33-52)
+// calling evolve_ellipse_full with solver = :rk4 (EllipsoidalCollapse.jl
+// :518-624): get_derivs! (:212-323), rk4_homel! (:153-179), get_b_2
+// (:113-149), Carlson's RD (:66-108), Ha_b_nr (:56-58).  The logarithm of the
+// oblate branch is the project's log (ppbm::log_pos), as on the device.
+// ---------------------------------------------------------------------------
+struct OraEll {
+  int iforce, ivir, nstepmax;
+  double fcoll1, fcoll2, fcoll3, tfac, zinit_fac;
+  double Rvac, Rcurv;
+  const OraGrowth* G;
+};
+
+static double ell_rd(double x, double y, double z) {
+  const double ERRTOL = 0.05, C1 = 3.0 / 14.0, C2 = 1.0 / 6.0, C3 = 9.0 / 22.0, C4 = 3.0 / 26.0;
+  const double C5 = 0.25 * C3, C6 = 1.5 * C4;
+  double xt = x, yt = y, zt = z, sum = 0.0, fac = 1.0, delx = 0.0, dely = 0.0, delz = 0.0, ave = 0.0;
+  for (int it = 0; it < 200; it++) {
+    const double sx = std::sqrt(xt), sy = std::sqrt(yt), sz = std::sqrt(zt);
+    const double alamb = sx * (sy + sz) + sy * sz;
+    sum += fac / (sz * (zt + alamb));
+    fac *= 0.25;
+    xt = 0.25 * (xt + alamb);
+    yt = 0.25 * (yt + alamb);
+    zt = 0.25 * (zt + alamb);
+    ave = 0.2 * (xt + yt + 3.0 * zt);
+    delx = (ave - xt) / ave;
+    dely = (ave - yt) / ave;
+    delz = (ave - zt) / ave;
+    if (std::max(std::max(std::fabs(delx), std::fabs(dely)), std::fabs(delz)) <= ERRTOL) break;
+  }
+  const double ea = delx * dely, eb = delz * delz, ec = ea - eb, ed = ea - 6.0 * eb, ee = ed + ec + ec;
+  return 3.0 * sum + fac * (1.0 + ed * (-C1 + C5 * ed - C6 * delz * ee) +
+                            delz * (C2 * ee + delz * (-C3 * ec + delz * C4 * ea))) / (ave * std::sqrt(ave));
+}
+
+static void ell_b2(double a1, double a2, double a3, double* b) {
+  const double third = 1.0 / 3.0;
+  const double r2 = a2 / a1, r3 = a3 / a1;
+  if (r3 >= r2) {
+    if (r3 >= 0.999) { b[0] = b[1] = b[2] = third; return; }
+    double b3;
+    if (r3 <= 0.001) {
+      const double ecc2 = 1.0 - r3 * r3, one_ecc2 = r3 * r3, one_ecc = 0.5 * (r3 * r3), ecc = std::sqrt(ecc2);
+      b3 = 0.5 * (one_ecc2 / ecc2 * (1.0 / one_ecc2 - ppbm::log_pos((1.0 + ecc) / one_ecc) * 0.5 / ecc));
+    } else {
+      const double ecc2 = 1.0 - r3 * r3, ecc = std::sqrt(ecc2);
+      b3 = 0.5 * ((1.0 - ecc2) / ecc2 * (1.0 / (1.0 - ecc2) - ppbm::log_pos((1.0 + ecc) / (1.0 - ecc)) * 0.5 / ecc));
+    }
+    b[0] = 1.0 - 2.0 * b3; b[1] = b3; b[2] = b3;
+    return;
+  }
+  const double r22 = r2 * r2, r32 = r3 * r3, qrat = third * r2 * r3;
+  const double b3 = qrat * ell_rd(r22, 1.0, r32), b2 = qrat * ell_rd(r32, 1.0, r22);
+  b[0] = 1.0 - (b2 + b3); b[1] = b2; b[2] = b3;
+}
+
+struct OraDeriv {
+  int lvir[3];
+  double aeq[3];           // frozen axis values (a_1eq, a_2eq, a_3eq)
+  double a3eq2, a3eq1, Ha;
+  double lam[3], F3;
+};
+
+static double ell_Ha(const OraEll& E, double a) {
+  return std::sqrt((1.0 + E.Rvac * (a * a * a) + E.Rcurv * a) / a);
+}
+
+// y = (a1, a2, a3, v1, v2, v3) 0-based; may freeze axes of y
+static void ell_derivs(const OraEll& E, OraDeriv& S, double t, double* y, double* dy) {
+  for (int i = 0; i < 6; i++) dy[i] = 0.0;
+  const double ab = t, ab3 = ab * ab * ab;
+  const double Ha = ell_Ha(E, ab);
+  S.Ha = Ha;
+  const double Hi = 1.0 / Ha;
+  if (S.lvir[2] == 0 && y[2] <= E.fcoll3 * ab) {
+    S.lvir[2] = 1;
+    S.aeq[2] = E.fcoll3 * ab;
+    if (E.ivir == 1) { S.a3eq2 = S.aeq[2] * 1.001; S.a3eq1 = S.aeq[2] * 1.0003; }
+  }
+  if (E.ivir == 2 && S.lvir[1] == 0) S.a3eq2 = E.fcoll2 * ab;
+  if (E.ivir == 2 && S.lvir[0] == 0) S.a3eq1 = E.fcoll1 * ab;
+  if (S.lvir[2] == 1 && y[1] <= S.a3eq2 && S.lvir[1] == 0) { S.lvir[1] = 1; S.aeq[1] = S.a3eq2; }
+  if (S.lvir[2] == 1 && y[0] <= S.a3eq1 && S.lvir[0] == 0) { S.lvir[0] = 1; S.aeq[0] = S.a3eq1; }
+  for (int ax = 2; ax >= 0; ax--)
+    if (S.lvir[ax] == 1) { y[ax] = S.aeq[ax]; y[ax + 3] = 0.0; dy[ax] = 0.0; dy[ax + 3] = 0.0; }
+  const double a1 = y[0], a2 = y[1], a3 = y[2];
+  const double d1e = ab3 / (a1 * a2 * a3);
+  double d0, d1i, d1x = 0.0;
+  if (E.iforce == 0) {
+    d0 = -E.Rvac * Hi;
+    d1i = 1.5 * d1e / ab3 * Hi;
+  } else {
+    d0 = (0.5 / ab3 - E.Rvac) * Hi;
+    d1i = 1.5 * (d1e - 1.0) / ab3 * Hi;
+    if (E.iforce == 4 || E.iforce == 5 || E.iforce == 6) {
+      double dl, hd, da;
+      dlinear_ab(*E.G, ab, &dl, &hd, &da);
+      d1x = 1.5 / ab3 * Hi * dl;
+    } else if (E.iforce == 3) {
+      d1x = 1.5 * 2.5 / ab3 * Hi;
+    }
+  }
+  double b[3] = {0.0, 0.0, 0.0};
+  if (E.iforce != 5 && E.iforce != 6) ell_b2(a1, a2, a3, b);
+  const double third = 1.0 / 3.0;
+  for (int ax = 2; ax >= 0; ax--) {   // axis 3, 2, 1 as the reference
+    if (S.lvir[ax] != 0) continue;
+    dy[ax] = y[ax + 3] * Hi;
+    const double ya = y[ax];
+    switch (E.iforce) {
+      case 0: dy[ax + 3] = -ya * d1i * b[ax]; break;
+      case 1: dy[ax + 3] = -ya * (d1i * b[ax] + d0); break;
+      case 3: dy[ax + 3] = -ya * (d1i * b[ax] + d0 + d1x * (b[ax] - third)); break;
+      case 5: dy[ax + 3] = -ya * d0 - d1x * ab * S.lam[ax]; break;
+      default: dy[ax + 3] = -ya * (d1i * b[ax] + d0 + d1x * (S.lam[ax] - S.F3)); break;   // 4, 6
+    }
+  }
+}
+
+static double ell_evolve(const OraEll& E, double Frho, double ev, double pv) {
+  OraDeriv S{};
+  S.lam[2] = Frho / 3.0 * (1.0 + 3.0 * ev + pv);
+  S.lam[1] = Frho / 3.0 * (1.0 - 2.0 * pv);
+  S.lam[0] = Frho / 3.0 * (1.0 - 3.0 * ev + pv);
+  S.F3 = Frho / 3.0;
+  const double zinit = E.zinit_fac * Frho;
+  const double ab = 1.0 / zinit;
+  double t = ab;
+  double dl, hd, da;
+  dlinear_ab(*E.G, ab, &dl, &hd, &da);
+  const double Ha = ell_Ha(E, ab);
+  S.Ha = Ha;
+  double y[6];
+  for (int ax = 2; ax >= 0; ax--) {
+    y[ax] = ab * (1.0 - dl * S.lam[ax]);
+  }
+  for (int ax = 2; ax >= 0; ax--) {
+    y[ax + 3] = Ha * (1.0 - (1.0 + hd) * dl * S.lam[ax]);
+  }
+  double zdyn[6] = {-1.0, -1.0, -1.0, -1.0, -1.0, -1.0};
+  int ldyn[6] = {0, 0, 0, 0, 0, 0};
+  double aturn[3] = {0.0, 0.0, 0.0};
+  double dy[6], yout[6], yt[6], dyt[6], dym[6];
+  int istep = 0;
+  while (true) {
+    istep++;
+    const double a_3 = y[2];
+    const double h = E.tfac * a_3 * std::sqrt(a_3) * S.Ha;
+    ell_derivs(E, S, t, y, dy);
+    // rk4_homel!
+    const double hh = h * 0.5, h6 = h / 6.0, xh = t + hh;
+    for (int i = 0; i < 6; i++) yt[i] = y[i] + hh * dy[i];
+    ell_derivs(E, S, xh, yt, dyt);
+    for (int i = 0; i < 6; i++) yt[i] = y[i] + hh * dyt[i];
+    ell_derivs(E, S, xh, yt, dym);
+    for (int i = 0; i < 6; i++) { yt[i] = y[i] + h * dym[i]; dym[i] = dyt[i] + dym[i]; }
+    ell_derivs(E, S, t + h, yt, dyt);
+    for (int i = 0; i < 6; i++) yout[i] = y[i] + h6 * (dy[i] + dyt[i] + 2.0 * dym[i]);
+    for (int i = 0; i < 6; i++) y[i] = yout[i];
+    t += h;
+    for (int ii = 0; ii < 3; ii++)
+      if (S.lvir[ii] != ldyn[ii]) { zdyn[ii] = 1.0 / t; ldyn[ii] = 1; }
+    for (int ii = 3; ii < 6; ii++) {
+      if (ldyn[ii] != 1) {
+        const int iax = ii - 3;
+        if (y[iax] < aturn[iax]) { zdyn[ii] = 1.0 / t; ldyn[ii] = 1; }
+        else aturn[iax] = y[iax];
+      }
+    }
+    if (S.lvir[0] == 1 || istep >= E.nstepmax || t >= 2.0) return zdyn[0];   // idynax = 1
+  }
+}
+
+// make_table with the RK4 solver: out[i + Nx (j + Ny k)] = 1 + z_vir of
+// axis 1 (-1: no collapse by a = 2), x = X1 + i dX = log10 F, y = e_v,
+// z = p_v / e_v.  prm = (X1, X2, Y1, Y2, Z1, Z2, fcoll1, fcoll2, fcoll3, tfac,
+// zinit_fac); iprm = (Nx, Ny, Nz, iforce_strat, ivir_strat, nstepmax).
+void ora_make_table(double Om, double OB, double OL, double h, const int32_t* iprm, const double* prm,
+                    double* out) {
+  OraGrowth G = growth_tables(Om, OB, OL, h);
+  OraEll E{iprm[3], iprm[4], iprm[5], prm[6], prm[7], prm[8], prm[9], prm[10], OL / Om, (1.0 - Om - OL) / Om, &G};
+  const int Nx = iprm[0], Ny = iprm[1], Nz = iprm[2];
+  const double dX = (prm[1] - prm[0]) / (Nx - 1), dY = (prm[3] - prm[2]) / (Ny - 1), dZ = (prm[5] - prm[4]) / (Nz - 1);
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+  for (int k = 0; k < Nz; k++)
+    for (int j = 0; j < Ny; j++)
+      for (int i = 0; i < Nx; i++) {
+        const double z = prm[4] + k * dZ, y = prm[2] + j * dY, x = prm[0] + i * dX;
+        const double Frho = std::pow(10.0, x);
+        out[i + (int64_t)Nx * (j + (int64_t)Ny * k)] = ell_evolve(E, Frho, y, z * y);
+      }
+}
+
+double ora_elliptic_rd(double x, double y, double z) { return ell_rd(x, y, z); }
+void ora_shape_b2(double a1, double a2, double a3, double* b) { ell_b2(a1, a2, a3, b); }
+
 // Exposed for tests: returns D(a) for each a.
 void ora_dlinear(double Om, double OB, double OL, double h, const double* a, int na, double* D) {
   OraGrowth G = growth_tables(Om, OB, OL, h);

@@ -23,6 +23,7 @@ Reference files restated (PeakPatch.jl):
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 import os
 import struct
 import subprocess
@@ -78,6 +79,10 @@ def _declare(L):
     L.ora_find_peaks.restype = I64
     L.ora_hRinteg.argtypes = [D, D]
     L.ora_hRinteg.restype = D
+    L.ora_make_table.argtypes = [D, D, D, D, P, P, P]
+    L.ora_elliptic_rd.argtypes = [D, D, D]
+    L.ora_elliptic_rd.restype = D
+    L.ora_shape_b2.argtypes = [D, D, D, P]
     L.ora_atab4.argtypes = [P]
     L.ora_shells.argtypes = [ctypes.c_int, P]
     L.ora_shells.restype = I64
@@ -309,6 +314,53 @@ def dlinear(Om, OB, OL, h, a) -> np.ndarray:
     out = np.empty_like(a)
     lib().ora_dlinear(Om, OB, OL, h, _p(a), len(a), _p(out))
     return out
+
+
+@dataclasses.dataclass
+class TableParams:
+    """CollapseTableParams (src/EllipsoidalCollapse/CollapseTable.jl:9-23) and
+    the EllipsoidParams defaults of the RK4 path (EllipsoidalCollapse.jl:25-38)."""
+    Nx: int = 50
+    Ny: int = 20
+    Nz: int = 20
+    X1: float = float(np.log10(1.5))
+    X2: float = float(np.log10(8.0))
+    Y1: float = 0.0
+    Y2: float = 0.5
+    Z1: float = -1.0 + 1e-4
+    Z2: float = 1.0 - 1e-4
+    iforce_strat: int = 4
+    ivir_strat: int = 2
+    fcoll_1: float = 0.01
+    fcoll_2: float = 0.171
+    fcoll_3: float = 0.171
+    tfac: float = 0.01
+    nstepmax: int = 10000
+    zinit_fac: float = 20.0
+
+
+def make_table(Om, OB, OL, h, tp: TableParams = None) -> np.ndarray:
+    """make_table(EllipsoidParams(cosmo; solver=:rk4), tp)
+    (src/EllipsoidalCollapse/CollapseTable.jl:33-52): the (Nz, Ny, Nx) array
+    (C order, i.e. Julia's [i, j, k]) of 1 + z_vir in double precision; the
+    reference stores it rounded to Float32."""
+    tp = tp or TableParams()
+    ip = np.array([tp.Nx, tp.Ny, tp.Nz, tp.iforce_strat, tp.ivir_strat, tp.nstepmax], np.int32)
+    dp = np.array([tp.X1, tp.X2, tp.Y1, tp.Y2, tp.Z1, tp.Z2, tp.fcoll_1, tp.fcoll_2, tp.fcoll_3, tp.tfac,
+                   tp.zinit_fac], np.float64)
+    out = np.empty((tp.Nz, tp.Ny, tp.Nx), np.float64)
+    lib().ora_make_table(Om, OB, OL, h, _p(ip), _p(dp), _p(out))
+    return out
+
+
+def elliptic_rd(x, y, z) -> float:
+    return float(lib().ora_elliptic_rd(x, y, z))
+
+
+def shape_b2(a1, a2, a3) -> np.ndarray:
+    b = np.zeros(3)
+    lib().ora_shape_b2(a1, a2, a3, _p(b))
+    return b
 
 
 def fsc_of_z(Om, OB, OL, h, z) -> float:

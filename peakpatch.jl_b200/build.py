@@ -36,9 +36,14 @@ def _headers():
         glob.glob(os.path.join(ROOT, "include", "*.h"))
 
 
+# per-file flags: the collapse-table integrations must not contract
+# multiplies and adds (bit-exact with the CPU restatement)
+FILE_FLAGS = {"k_table.cu": ["-fmad=false"]}
+
+
 def _compile(src: str, extra: list[str]) -> str:
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    cmd = [NVCC] + ARCH + FLAGS + extra + ["-c", src, "-o", obj]
+    cmd = [NVCC] + ARCH + FLAGS + FILE_FLAGS.get(os.path.basename(src), []) + extra + ["-c", src, "-o", obj]
     if src.endswith(".cpp"):
         cmd = [NVCC, "-x", "cu"] + ARCH + FLAGS + extra + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -621,6 +621,70 @@ int32_t ppb_set_collapse_table_f64(ppb_ctx* ctx, const double* tab, int32_t nx, 
   PPB_GUARD_END(ctx)
 }
 
+int32_t ppb_make_collapse_table(ppb_ctx* ctx, const ppb_table_params* p, double* out, int32_t install) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  PPB_GUARD_BEGIN
+  PPB_REQUIRE(p != nullptr, "params is null");
+  PPB_REQUIRE(p->Om > 0 && p->OB >= 0 && p->OB <= p->Om && p->OL >= 0 && p->h > 0, "bad cosmology");
+  PPB_REQUIRE(p->Nx >= 2 && p->Ny >= 2 && p->Nz >= 2, "table needs at least 2 nodes per axis");
+  PPB_REQUIRE((int64_t)p->Nx * p->Ny * p->Nz <= ((int64_t)1 << 26), "table larger than 2^26 nodes");
+  PPB_REQUIRE(p->X2 > p->X1 && p->Y2 > p->Y1 && p->Z2 > p->Z1, "table ranges must be increasing");
+  const int f = p->iforce_strat;
+  PPB_REQUIRE(f == 0 || f == 1 || f == 3 || f == 4 || f == 5 || f == 6, "iforce_strat must be 0, 1, 3, 4, 5 or 6");
+  PPB_REQUIRE(p->ivir_strat == 1 || p->ivir_strat == 2, "ivir_strat must be 1 or 2");
+  PPB_REQUIRE(p->nstepmax >= 1 && p->nstepmax <= 100000000, "nstepmax must be in [1, 1e8]");
+  PPB_REQUIRE(p->fcoll_1 > 0 && p->fcoll_2 > 0 && p->fcoll_3 > 0 && p->tfac > 0 && p->zinit_fac > 0,
+              "fcoll, tfac and zinit_fac must be positive");
+  PPB_REQUIRE(install >= 0 && install <= 2, "install must be 0, 1 or 2");
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  Slot& sl = ctx->sync;
+  const GrowthTable& G = ctx->growth(p->Om, p->OB, p->OL, p->h);
+  // F = 10^x on the host (make_table's Frho = 10.0^logF)
+  std::vector<double> F(p->Nx);
+  const double dX = (p->X2 - p->X1) / (p->Nx - 1);
+  for (int i = 0; i < p->Nx; i++) F[i] = std::pow(10.0, p->X1 + i * dX);
+  const int64_t nn = (int64_t)p->Nx * p->Ny * p->Nz;
+  DevBuf dF, dout, dsteps;
+  dF.ensure(F.size() * 8);
+  dout.ensure((size_t)nn * 8);
+  dsteps.ensure(8);
+  PPB_CUDA(cudaMemcpyAsync(dF.p, F.data(), F.size() * 8, cudaMemcpyHostToDevice, sl.stream));
+  PPB_CUDA(cudaMemsetAsync(dsteps.p, 0, 8, sl.stream));
+  PPB_CUDA(cudaEventRecord(sl.stage_ev[0], sl.stream));
+  make_table_device(sl, G, p, dF.as<double>(), dout.as<double>(), dsteps.as<unsigned long long>());
+  PPB_CUDA(cudaEventRecord(sl.stage_ev[1], sl.stream));
+  unsigned long long steps = 0;
+  PPB_CUDA(cudaMemcpyAsync(&steps, dsteps.p, 8, cudaMemcpyDeviceToHost, sl.stream));
+  PPB_CUDA(cudaStreamSynchronize(sl.stream));
+  PPB_CUDA(cudaEventElapsedTime(&ctx->table_ms, sl.stage_ev[0], sl.stage_ev[1]));
+  ctx->table_steps = (int64_t)steps;
+  if (out) copy_out(out, dout.p, (size_t)nn * 8, sl.stream);
+  if (install == 2) {
+    const int32_t rc = ppb_set_collapse_table_f64(ctx, dout.as<double>(), p->Nx, p->Ny, p->Nz, p->X1, p->X2, p->Y1,
+                                                  p->Y2, p->Z1, p->Z2);
+    if (rc != PPB_OK) return rc;
+  } else if (install == 1) {   // Float32 nodes, as make_table stores them
+    std::vector<double> h((size_t)nn);
+    PPB_CUDA(cudaMemcpy(h.data(), dout.p, (size_t)nn * 8, cudaMemcpyDeviceToHost));
+    std::vector<float> t32((size_t)nn);
+    for (int64_t q = 0; q < nn; q++) t32[q] = (float)h[q];
+    const int32_t rc = ppb_set_collapse_table(ctx, t32.data(), p->Nx, p->Ny, p->Nz, p->X1, p->X2, p->Y1, p->Y2,
+                                              p->Z1, p->Z2);
+    if (rc != PPB_OK) return rc;
+  }
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_last_table_stats(ppb_ctx* ctx, float* ms, int64_t* steps) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  if (ms) *ms = ctx->table_ms;
+  if (steps) *steps = ctx->table_steps;
+  return PPB_OK;
+}
+
 int32_t ppb_generate_fields(ppb_ctx* ctx, const ppb_tile_params* p, float* delta, float* psi, float* psi2,
                             float* lapd) {
   if (!ctx) return PPB_ERR_INVALID;

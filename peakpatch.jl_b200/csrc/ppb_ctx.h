@@ -150,6 +150,8 @@ struct ppb_ctx {
   ppb::Slot sync;            // the slot of the synchronous entry points
   std::unique_ptr<ppb::Server> server;
   int serve_slots = 4;
+  float table_ms = 0.f;        // last ppb_make_collapse_table: device time
+  int64_t table_steps = 0;     // and RK4 steps over all nodes
 
   void set_error(const std::string& m);
   const ppb::GrowthTable& growth(double Om, double OB, double OL, double h);
@@ -211,4 +213,9 @@ int64_t merge_catalog_device(Slot& sl, const float* d_rec, int64_t n, int nf, fl
 void server_stop(ppb_ctx* ctx);
 // graph launches, instantiations and in-place updates over every slot
 void graph_counts(const ppb_ctx* ctx, int64_t* out3);
+// make_table's RK4 integrations on the device (k_table.cu): d_Frho holds
+// 10^x of the Nx log10 F nodes; d_out the Nx Ny Nz node values; d_steps
+// accumulates the RK4 steps taken
+void make_table_device(Slot& sl, const GrowthTable& G, const ppb_table_params* p, const double* d_Frho, double* d_out,
+                       unsigned long long* d_steps);
 }  // namespace ppb

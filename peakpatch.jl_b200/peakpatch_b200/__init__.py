@@ -23,6 +23,7 @@ or a GPU the calls raise.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 import os
 import struct
 from dataclasses import dataclass, field, fields, replace
@@ -93,6 +94,40 @@ OPT_GRAPHS, OPT_AUTOTUNE, OPT_TUNE_MIN_PEAKS, OPT_BRICK_SHIFT, OPT_COLLAPSE_THRE
 OPT_GRAPH_LAUNCHES, OPT_GRAPH_INSTANTIATIONS, OPT_GRAPH_UPDATES = 16, 17, 18
 
 
+class _TableParams(ctypes.Structure):
+    _fields_ = [("Om", ctypes.c_double), ("OB", ctypes.c_double), ("OL", ctypes.c_double), ("h", ctypes.c_double),
+                ("Nx", ctypes.c_int32), ("Ny", ctypes.c_int32), ("Nz", ctypes.c_int32),
+                ("iforce_strat", ctypes.c_int32), ("ivir_strat", ctypes.c_int32), ("nstepmax", ctypes.c_int32),
+                ("X1", ctypes.c_double), ("X2", ctypes.c_double), ("Y1", ctypes.c_double), ("Y2", ctypes.c_double),
+                ("Z1", ctypes.c_double), ("Z2", ctypes.c_double), ("fcoll_1", ctypes.c_double),
+                ("fcoll_2", ctypes.c_double), ("fcoll_3", ctypes.c_double), ("tfac", ctypes.c_double),
+                ("zinit_fac", ctypes.c_double), ("reserved", ctypes.c_int32 * 4)]
+
+
+@dataclasses.dataclass
+class CollapseTableParams:
+    """CollapseTableParams (src/EllipsoidalCollapse/CollapseTable.jl:9-23)
+    with the EllipsoidParams settings of the RK4 path
+    (src/EllipsoidalCollapse/EllipsoidalCollapse.jl:25-38), defaults as there."""
+    Nx: int = 50
+    Ny: int = 20
+    Nz: int = 20
+    X1: float = float(np.log10(1.5))
+    X2: float = float(np.log10(8.0))
+    Y1: float = 0.0
+    Y2: float = 0.5
+    Z1: float = -1.0 + 1e-4
+    Z2: float = 1.0 - 1e-4
+    iforce_strat: int = 4
+    ivir_strat: int = 2
+    fcoll_1: float = 0.01
+    fcoll_2: float = 0.171
+    fcoll_3: float = 0.171
+    tfac: float = 0.01
+    nstepmax: int = 10000
+    zinit_fac: float = 20.0
+
+
 class _HaloBuf(ctypes.Structure):
     _fields_ = [("records", ctypes.c_void_p), ("capacity", ctypes.c_int64), ("count", ctypes.c_int64),
                 ("nfields", ctypes.c_int32), ("RTHLmax", ctypes.c_float), ("npeaks", ctypes.c_int64)]
@@ -109,7 +144,8 @@ EXPORTED = (
     "ppb_alloc_device", "ppb_free_device", "ppb_shell_counters", "ppb_find_peaks_noalloc",
     "ppb_last_shell_times", "ppb_serve_config", "ppb_submit", "ppb_wait", "ppb_stats_get", "ppb_stats_reset",
     "ppb_run_multitile", "ppb_merge_catalog", "ppb_set_collapse_table_f64", "ppb_generate_fields",
-    "ppb_analyse_peaks_lim", "ppb_set_option", "ppb_get_option", "ppb_tune_entries",
+    "ppb_analyse_peaks_lim", "ppb_set_option", "ppb_get_option", "ppb_tune_entries", "ppb_make_collapse_table",
+    "ppb_last_table_stats",
 )
 
 
@@ -159,6 +195,8 @@ def load_library():
     L.ppb_set_collapse_table_f64.argtypes = [P, P, I32, I32, I32, D, D, D, D, D, D]
     L.ppb_generate_fields.argtypes = [P, ctypes.POINTER(_TileParams), P, P, P, P]
     L.ppb_analyse_peaks_lim.argtypes = [P] * 9 + [I32, I32, I64, P, P, P, P, P, P, D, I32, P]
+    L.ppb_make_collapse_table.argtypes = [P, ctypes.POINTER(_TableParams), P, I32]
+    L.ppb_last_table_stats.argtypes = [P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int64)]
     L.ppb_set_option.argtypes = [P, I32, I64]
     L.ppb_get_option.argtypes = [P, I32, ctypes.POINTER(ctypes.c_int64)]
     L.ppb_tune_entries.argtypes = [P, ctypes.POINTER(_TuneEntry), I32, ctypes.POINTER(ctypes.c_int32)]
@@ -388,6 +426,32 @@ class Context:
                 "akk_overrun": int(raw[7]), "bad_peaks": int(raw[8]), "walk_steps": int(raw[9]),
                 "kernel_ms": dict(zip(("gather", "collapse", "zvir_half", "d2f"), kms.tolist())),
                 "pool_rows": rows.value, "batches": nb.value}
+
+    # ---- collapse-table generation ----
+    def make_table(self, Om: float, OB: float, OL: float, h: float, tp: "CollapseTableParams" = None,
+                   install: int = 0) -> np.ndarray:
+        """make_table(EllipsoidParams(cosmo; solver=:rk4), tp) on the GPU
+        (src/EllipsoidalCollapse/CollapseTable.jl:33-52): the (Nz, Ny, Nx)
+        array (Julia's [i, j, k]) of 1 + z_vir in double precision (the
+        reference rounds it to Float32).  Om is the total matter density.
+        install = 1 makes it the context's collapse table with Float32 nodes,
+        2 with Float64 nodes."""
+        tp = tp or CollapseTableParams()
+        p = _TableParams(Om=Om, OB=OB, OL=OL, h=h, Nx=tp.Nx, Ny=tp.Ny, Nz=tp.Nz, iforce_strat=tp.iforce_strat,
+                         ivir_strat=tp.ivir_strat, nstepmax=tp.nstepmax, X1=tp.X1, X2=tp.X2, Y1=tp.Y1, Y2=tp.Y2,
+                         Z1=tp.Z1, Z2=tp.Z2, fcoll_1=tp.fcoll_1, fcoll_2=tp.fcoll_2, fcoll_3=tp.fcoll_3,
+                         tfac=tp.tfac, zinit_fac=tp.zinit_fac)
+        out = np.empty((tp.Nz, tp.Ny, tp.Nx), np.float64)
+        self._check(self.L.ppb_make_collapse_table(self.h, ctypes.byref(p), _p(out), int(install)))
+        if install:
+            self._table_key = None
+        return out
+
+    def table_stats(self):
+        ms = ctypes.c_float()
+        st = ctypes.c_int64()
+        self._check(self.L.ppb_last_table_stats(self.h, ctypes.byref(ms), ctypes.byref(st)))
+        return {"ms": ms.value, "rk4_steps": st.value}
 
     # ---- launch options and the autotuner ----
     def set_option(self, option: int, value: int):

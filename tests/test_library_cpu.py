@@ -51,6 +51,14 @@ def test_tune_entry_layout_and_option_entry_points():
     assert L.ppb_tune_entries(None, None, 0, ctypes.byref(n)) == -1
 
 
+def test_table_params_layout_matches_the_header():
+    # ppb_table_params: 4 doubles, 6 int32, 11 doubles, 4 int32 = 160 bytes
+    assert ctypes.sizeof(pp._TableParams) == 160
+    assert pp._TableParams.X1.offset == 56 and pp._TableParams.zinit_fac.offset == 136
+    L = pp.load_library()
+    assert L.ppb_make_collapse_table(None, None, None, 0) == -1
+
+
 def test_serving_entry_points_reject_bad_arguments():
     L = pp.load_library()
     assert L.ppb_submit(None, None, None, 0, None) == -1

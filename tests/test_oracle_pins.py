@@ -397,3 +397,42 @@ def test_merge_volume_reduction_kats(ora):
     assert out[0, 6] == pytest.approx(((4 * np.pi / 3 * 8.0 - cap) / (4 * np.pi / 3)) ** (1 / 3), rel=1e-6)
     out, keep = ora.merge_catalog(_halos([[0, 0, 0], [100, 0, 0]], [2.0, 3.0]))
     assert keep.all() and out[0, 6] == pytest.approx(2.0) and out[1, 6] == pytest.approx(3.0)
+
+
+# ---------------------------------------------------------------------------
+# collapse-table generation (RK4 path of make_table)
+# ---------------------------------------------------------------------------
+def test_elliptic_rd_and_shape_integrals(ora):
+    # test/test_ellipsoidalcollapse.jl:8-38: RD(x,x,x) = x^-3/2; b sums to 1;
+    # (1,1,1) is spherical
+    for x in (1.0, 2.0, 0.5, 10.0):
+        assert ora.elliptic_rd(x, x, x) == pytest.approx(x ** -1.5, rel=1e-10)
+    assert ora.elliptic_rd(1.0, 2.0, 3.0) > 0
+    assert np.allclose(ora.shape_b2(1.0, 1.0, 1.0), 1.0 / 3.0, rtol=1e-10)
+    for a in [(0.5, 0.8, 1.2), (0.3, 0.7, 1.5), (0.9, 0.95, 1.0), (1.2, 0.8, 0.5)]:
+        assert ora.shape_b2(*a).sum() == pytest.approx(1.0, rel=1e-10)
+
+
+def test_single_ellipsoids(ora):
+    # test/test_ellipsoidalcollapse.jl:71-98 and :183-186 (RK4): overdensities
+    # collapse, more overdense earlier, Frho = 0.5 never (-1)
+    tp = ora.TableParams(Nx=2, Ny=2, Nz=2, X1=np.log10(3.0), X2=np.log10(5.0), Y1=0.0, Y2=0.3, Z1=0.0, Z2=0.5)
+    t = ora.make_table(0.315, 0.049, 0.685, 0.674, tp)
+    assert (t > 0).all()                       # (3, 0.3, 0) and (5, 0, 0) collapse
+    assert (t[:, :, 1] > t[:, :, 0]).all()     # higher F, earlier (larger 1 + z)
+    sph = ora.make_table(0.315, 0.049, 0.685, 0.674, ora.TableParams(Nx=2, Ny=2, Nz=2, X1=np.log10(1.5),
+                                                                     X2=np.log10(1.686), Y2=1e-9, Z1=0.0, Z2=0.1))
+    assert sph[0, 0, 1] > 0 and sph[0, 0, 1] > sph[0, 0, 0]   # Frho = 1.686 collapses (zvir > 0)
+    low = ora.make_table(0.315, 0.049, 0.685, 0.674, ora.TableParams(Nx=2, Ny=2, Nz=2, X1=np.log10(0.4),
+                                                                     X2=np.log10(0.5), Y2=0.1, Z1=0.0, Z2=0.1))
+    assert (low == -1.0).all()
+
+
+def test_make_table_reproduces_the_reference_table(ora, julia_table):
+    # tests/golden/HomelTab_julia.dat is the reference's make_table output
+    # (RK4 path, default CollapseTableParams) for the Websky cosmology of
+    # validation/websky_multitile (Om 0.3138, OB 0.0493, OL 0.6862, h 0.6735):
+    # the restatement reproduces every one of its 20,000 Float32 nodes
+    t = ora.make_table(0.3138, 0.0493, 0.6862, 0.6735)
+    assert t.shape == julia_table.data.shape
+    assert np.array_equal(t.astype(np.float32), julia_table.data)
