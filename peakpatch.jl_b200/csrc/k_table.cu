@@ -43,17 +43,20 @@ struct TabArgs {
   unsigned long long* steps;   // total RK4 steps (statistics)
 };
 
-// Dlinear_ab: bisection hunt, 4-point (2-point at the ends) Lagrange
-// interpolation of D(a)/a and dlnD/dlna; returns D(a) and dlnD/dlna
-__device__ void dlin(const TabArgs& A, double ai, double* Dl, double* HD) {
+// Dlinear_ab: the table position, 4-point (2-point at the ends) Lagrange
+// interpolation of D(a)/a and dlnD/dlna; returns D(a) and dlnD/dlna.  The
+// reference's bisection returns the number of table entries below ai (the
+// table increases strictly); the integration's a only moves forward, so that
+// count is kept in *pos and walked from the previous call (the same index,
+// a few cached loads instead of a dozen dependent ones).
+__device__ void dlin(const TabArgs& A, double ai, double* Dl, double* HD, int* pos) {
   const int ntab = A.ng;
   if (ai > A.amin && ai < A.amax) {
-    int jlo = 0, jhi = ntab + 1;
-    while (jhi - jlo > 1) {
-      const int jm = (jhi + jlo) / 2;
-      if (ai > __ldg(A.ga + jm - 1)) jlo = jm; else jhi = jm;
-    }
-    const int kk = jlo;
+    int j = *pos;
+    while (j < ntab && ai > __ldg(A.ga + j)) j++;
+    while (j > 0 && !(ai > __ldg(A.ga + j - 1))) j--;
+    *pos = j;
+    const int kk = j;
     int nl, kkl;
     if (kk < 2 || kk >= ntab) { nl = 2; kkl = kk - 1 > 1 ? kk - 1 : 1; } else { nl = 4; kkl = kk - 2; }
     const double* xa = A.ga + kkl - 1;
@@ -85,29 +88,58 @@ __device__ void dlin(const TabArgs& A, double ai, double* Dl, double* HD) {
   }
 }
 
-// Carlson's RD(x, y, z) by duplication until the relative spread is below
-// 0.05, then the fifth-order series (at most 200 duplications)
-__device__ double rd(double x, double y, double z) {
+// Carlson's RD by duplication until the relative spread is below 0.05, then
+// the fifth-order series (at most 200 duplications).  RD(x, y, z) and
+// RD(u, y, w) are evaluated together: the two duplication sequences advance in
+// one loop (two independent chains of square roots and divisions in flight
+// instead of one), each stopping at its own tolerance test, so each result is
+// the one a separate evaluation gives
+__device__ void rd2(double x, double y, double z, double u, double w, double* r1, double* r2) {
   const double ERRTOL = 0.05, C1 = 3.0 / 14.0, C2 = 1.0 / 6.0, C3 = 9.0 / 22.0, C4 = 3.0 / 26.0;
   const double C5 = 0.25 * C3, C6 = 1.5 * C4;
   double xt = x, yt = y, zt = z, sum = 0.0, fac = 1.0, dx = 0.0, dy = 0.0, dz = 0.0, ave = 0.0;
-  for (int it = 0; it < 200; it++) {
-    const double sx = sqrt(xt), sy = sqrt(yt), sz = sqrt(zt);
-    const double al = sx * (sy + sz) + sy * sz;
-    sum += fac / (sz * (zt + al));
-    fac *= 0.25;
-    xt = 0.25 * (xt + al);
-    yt = 0.25 * (yt + al);
-    zt = 0.25 * (zt + al);
-    ave = 0.2 * (xt + yt + 3.0 * zt);
-    dx = (ave - xt) / ave;
-    dy = (ave - yt) / ave;
-    dz = (ave - zt) / ave;
-    if (fmax(fmax(fabs(dx), fabs(dy)), fabs(dz)) <= ERRTOL) break;
+  double ut = u, vt = y, wt = w, sum2 = 0.0, fac2 = 1.0, du = 0.0, dv = 0.0, dw = 0.0, ave2 = 0.0;
+  bool go1 = true, go2 = true;
+  for (int it = 0; it < 200 && (go1 || go2); it++) {
+    if (go1) {
+      const double sx = sqrt(xt), sy = sqrt(yt), sz = sqrt(zt);
+      const double al = sx * (sy + sz) + sy * sz;
+      sum += fac / (sz * (zt + al));
+      fac *= 0.25;
+      xt = 0.25 * (xt + al);
+      yt = 0.25 * (yt + al);
+      zt = 0.25 * (zt + al);
+      ave = 0.2 * (xt + yt + 3.0 * zt);
+      dx = (ave - xt) / ave;
+      dy = (ave - yt) / ave;
+      dz = (ave - zt) / ave;
+      go1 = !(fmax(fmax(fabs(dx), fabs(dy)), fabs(dz)) <= ERRTOL);
+    }
+    if (go2) {
+      const double su = sqrt(ut), sv = sqrt(vt), sw = sqrt(wt);
+      const double al = su * (sv + sw) + sv * sw;
+      sum2 += fac2 / (sw * (wt + al));
+      fac2 *= 0.25;
+      ut = 0.25 * (ut + al);
+      vt = 0.25 * (vt + al);
+      wt = 0.25 * (wt + al);
+      ave2 = 0.2 * (ut + vt + 3.0 * wt);
+      du = (ave2 - ut) / ave2;
+      dv = (ave2 - vt) / ave2;
+      dw = (ave2 - wt) / ave2;
+      go2 = !(fmax(fmax(fabs(du), fabs(dv)), fabs(dw)) <= ERRTOL);
+    }
   }
-  const double ea = dx * dy, eb = dz * dz, ec = ea - eb, ed = ea - 6.0 * eb, ee = ed + ec + ec;
-  return 3.0 * sum + fac * (1.0 + ed * (-C1 + C5 * ed - C6 * dz * ee) + dz * (C2 * ee + dz * (-C3 * ec + dz * C4 * ea))) /
-                         (ave * sqrt(ave));
+  {
+    const double ea = dx * dy, eb = dz * dz, ec = ea - eb, ed = ea - 6.0 * eb, ee = ed + ec + ec;
+    *r1 = 3.0 * sum + fac * (1.0 + ed * (-C1 + C5 * ed - C6 * dz * ee) + dz * (C2 * ee + dz * (-C3 * ec + dz * C4 * ea))) /
+                          (ave * sqrt(ave));
+  }
+  {
+    const double ea = du * dv, eb = dw * dw, ec = ea - eb, ed = ea - 6.0 * eb, ee = ed + ec + ec;
+    *r2 = 3.0 * sum2 + fac2 * (1.0 + ed * (-C1 + C5 * ed - C6 * dw * ee) + dw * (C2 * ee + dw * (-C3 * ec + dw * C4 * ea))) /
+                           (ave2 * sqrt(ave2));
+  }
 }
 
 // shape integrals b_1..b_3 of axes a1, a2, a3
@@ -131,11 +163,14 @@ __device__ void shape_b(double a1, double a2, double a3, double* b) {
     return;
   }
   const double r22 = r2 * r2, r32 = r3 * r3, q = third * r2 * r3;
-  const double b3 = q * rd(r22, 1.0, r32), b2 = q * rd(r32, 1.0, r22);
+  double rd3, rd2v;
+  rd2(r22, 1.0, r32, r32, r22, &rd3, &rd2v);   // RD(r2^2, 1, r3^2) and RD(r3^2, 1, r2^2)
+  const double b3 = q * rd3, b2 = q * rd2v;
   b[0] = 1.0 - (b2 + b3); b[1] = b2; b[2] = b3;
 }
 
 struct Ell {
+  int pos;                   // growth-table position of the last lookup
   int lv0, lv1, lv2;         // axis virialised
   double eq0, eq1, eq2;      // frozen axis values
   double a3eq2, a3eq1, Ha;
@@ -191,7 +226,7 @@ __device__ void derivs(const TabArgs& A, Ell& S, double t, double* y, double* dy
     d1i = 1.5 * (d1e - 1.0) / ab3 * Hi;
     if (A.iforce == 4 || A.iforce == 5 || A.iforce == 6) {
       double dl, hd;
-      dlin(A, ab, &dl, &hd);
+      dlin(A, ab, &dl, &hd, &S.pos);
       d1x = 1.5 / ab3 * Hi * dl;
     } else if (A.iforce == 3) {
       d1x = 1.5 * 2.5 / ab3 * Hi;
@@ -220,7 +255,8 @@ __global__ void __launch_bounds__(64) table_kernel(TabArgs A) {
   const double ab = 1.0 / zinit;
   double t = ab;
   double dl, hd;
-  dlin(A, ab, &dl, &hd);
+  S.pos = 0;
+  dlin(A, ab, &dl, &hd, &S.pos);
   const double Ha = hubble(A, ab);
   S.Ha = Ha;
   double y[6], dy[6], yt[6], dyt[6], dym[6];
