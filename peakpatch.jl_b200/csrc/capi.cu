@@ -163,21 +163,6 @@ ShellTable& ppb_ctx::shell_table(int nhunt, cudaStream_t s) {
   return *e;
 }
 
-const float4* ppb_ctx::cellf(ShellTable& st, int n, cudaStream_t s) {
-  std::lock_guard<std::mutex> lk(sh.cache_mu);
-  auto& e = st.cellf[n];
-  if (!e) {
-    std::vector<float4> f;
-    build_cellf(st, n, f);
-    auto b = std::make_unique<DevBuf>();
-    b->ensure(f.size() * sizeof(float4));
-    PPB_CUDA(cudaMemcpyAsync(b->p, f.data(), f.size() * sizeof(float4), cudaMemcpyHostToDevice, s));
-    PPB_CUDA(cudaStreamSynchronize(s));
-    e = std::move(b);
-  }
-  return e->as<float4>();
-}
-
 // device copies of the run's growth (and chi) tables on the slot; the host
 // tables are cache entries that outlive the asynchronous copies
 DevCosmo ppb_ctx::dev_cosmo(Slot& sl, const GrowthTable& G, double Om, double OL, double h, double zmax,
@@ -215,7 +200,8 @@ ShellArgs ppb_ctx::shell_args(Slot& sl, ShellTable& shells, int n, double alatt,
   a.alatt = alatt;
   PPB_REQUIRE(n <= 4096, "grid size above 4096");
   a.cell8 = shells.d_cell8.as<int32_t>();
-  a.cellf = cellf(shells, n, sl.stream);
+  a.ck_p = shells.d_ck_p.as<int32_t>();
+  a.ck_cells = shells.d_ck_cells.as<int4>();
   a.sh_start = shells.d_start.as<int32_t>();
   a.sh_count = shells.d_count.as<int32_t>();
   a.rad = shells.d_rad.as<double>();

@@ -129,20 +129,16 @@ void build_shell_table(ShellTable& st, int nhunt) {
   }
   st.ngroups = (int)st.grp_a.size();
   st.grp_c.push_back((int32_t)st.ck_s.size());
+  // chunk-major packed offsets, each chunk padded to a multiple of 4 cells
+  st.ck_p.clear();
+  st.ck_cells.clear();
+  for (size_t c = 0; c < st.ck_s.size(); c++) {
+    st.ck_p.push_back((int32_t)(st.ck_cells.size() / 4));
+    for (int i = 0; i < st.ck_n[c]; i++) st.ck_cells.push_back(st.cell8[st.ck_s[c] + i]);
+    while (st.ck_cells.size() % 4) st.ck_cells.push_back(0);
+  }
   st.nhunt = nhunt;
   st.d_cell8.release();   // force re-upload
-  st.cellf.clear();
-}
-
-void build_cellf(const ShellTable& st, int n, std::vector<float4>& out) {
-  out.resize(st.cells.size());
-  for (size_t i = 0; i < st.cells.size(); i++) {
-    const int4 c = st.cells[i];
-    const int32_t off = c.x + n * (c.y + n * c.z);
-    float w;
-    std::memcpy(&w, &off, 4);
-    out[i] = make_float4((float)c.x, (float)c.y, (float)c.z, w);
-  }
 }
 
 // hRinteg (src/HaloFinder/RadialShell.jl:100-127)
@@ -213,6 +209,8 @@ void upload_shell_table(ShellTable& st, cudaStream_t s) {
   up(st.d_ck_n, st.ck_n.data(), st.ck_n.size() * 4);
   up(st.d_sh_c0, st.sh_c0.data(), st.sh_c0.size() * 4);
   up(st.d_sh_nc, st.sh_nc.data(), st.sh_nc.size() * 4);
+  up(st.d_ck_p, st.ck_p.data(), st.ck_p.size() * 4);
+  up(st.d_ck_cells, st.ck_cells.data(), st.ck_cells.size() * 4);
   PPB_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -12,8 +12,9 @@
 //    splits the shells (distinct r^2 of the sorted cell list; shell 1 is the
 //    peak cell) into chunks of at most 24 cells and packs 32 chunks per
 //    group, groups ending on shell boundaries.  Lane l sums chunk l of the
-//    group (four cells per step, so that eight 16-byte record loads are in
-//    flight per lane), lane l then finalises shell l of the group from the
+//    group (four cells per step: the four cells' packed offsets in one
+//    16-byte load, four 32-byte records in flight per lane, each one 256-bit
+//    load), lane l then finalises shell l of the group from the
 //    chunk partials, and the cumulative profile Fbar comes from a warp scan
 //    of r^3 Fbar.  Sums are compensated single precision (two-sum, error-free
 //    per addend) on the optimised path and double precision on the plain
@@ -261,65 +262,66 @@ __device__ __forceinline__ void unpack_cell(int w, int& di, int& dj, int& dk) {
   dk = (w << 8) >> 24;
 }
 
-// Build-time tuning of the gather (measured on B200 at 384^3: 4 cells per
-// step, no entry prefetch and a 128-register cap, i.e. 16 warps per SM, are
-// fastest; 2- and 8-cell steps, prefetching and other caps are slower).
-#ifndef PPB_GATHER_BATCH
-#define PPB_GATHER_BATCH 4
-#endif
-#ifndef PPB_GATHER_PREFETCH
-#define PPB_GATHER_PREFETCH 0
-#endif
-constexpr int GB = PPB_GATHER_BATCH;   // cells per lane per step
 // shared memory of one gather warp, in doubles: the chunk partials
 constexpr int GATHER_WARP_DOUBLES = (NACC + 1) * 32;
 
-// Sum one chunk (cells s0 .. s0+cnt-1 of the sorted list) into A, GB cells
-// per step: the 2 GB record loads of a step are issued together, and the
-// cell-table entries of the next step are loaded before the current step is
-// summed.  Returns the number of in-grid cells.
+// One cell's 32-byte record with one 256-bit load (Blackwell's
+// ld.global.v8): one L1 tag lookup per cell instead of two 16-byte loads.
+// The records are 32-byte aligned (cell index x 32 bytes from a 256-byte
+// aligned buffer).
+__device__ __forceinline__ void ldg_record(const float4* p, float4& a, float4& b) {
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+
+// exact float of a small integer (|d| < 2^22) on the FMA pipe: the bits of
+// 1.5 * 2^23 plus d are the float 1.5 * 2^23 + d (ulp 1 there); subtracting
+// 1.5 * 2^23 is exact
+__device__ __forceinline__ float small_int_float(int d) {
+  return __fsub_rn(__int_as_float(0x4B400000 + d), 12582912.0f);
+}
+
+// Sum one chunk (ck_n cells of chunk ck of the schedule) into A, four cells
+// per step: the offsets of the four cells come packed in one 16-byte load of
+// the chunk-major cell list (loaded one step ahead), the four 32-byte records
+// are issued together.  Returns the number of in-grid cells.
 template <class AccT, bool COMP>
-__device__ __forceinline__ int sum_chunk(const ShellArgs& a, int s0, int cnt, int64_t lin, bool inside, int pi,
+__device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, int64_t lin, bool inside, int pi,
                                          int pj, int pk, AccT& A) {
-  const int n = a.n;
+  const int n = a.n, n2 = a.n * a.n;   // n <= 4096: every offset fits 32 bits
   const float4* __restrict__ aos = a.aos;
-  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  float4 cfn[GB];
-#pragma unroll
-  for (int u = 0; u < GB; u++) cfn[u] = u < cnt ? __ldg(a.cellf + s0 + u) : zero4;
+  const int4* __restrict__ cp = a.ck_cells + __ldg(a.ck_p + ck);
+  int4 wn = cnt > 0 ? __ldg(cp) : make_int4(0, 0, 0, 0);
   int nsh = 0;
-  for (int c = 0; c < cnt; c += GB) {
-    float4 ra[GB], rb[GB], cf[GB];
-    bool ok[GB];
+  for (int c = 0; c < cnt; c += 4) {
+    const int w[4] = {wn.x, wn.y, wn.z, wn.w};
+    float4 ra[4], rb[4];
+    int d[4][3];
+    bool ok[4];
 #pragma unroll
-    for (int u = 0; u < GB; u++) {
-      cf[u] = cfn[u];
+    for (int u = 0; u < 4; u++) {
+      d[u][0] = (w[u] << 24) >> 24;
+      d[u][1] = (w[u] << 16) >> 24;
+      d[u][2] = (w[u] << 8) >> 24;
       bool in = c + u < cnt;
-      if (!inside) {
-        const int iv1 = pi + (int)cf[u].x, iv2 = pj + (int)cf[u].y, iv3 = pk + (int)cf[u].z;
-        in = in && iv1 >= 0 && iv1 < n && iv2 >= 0 && iv2 < n && iv3 >= 0 && iv3 < n;
-      }
+      if (!inside)
+        in = in && (unsigned)(pi + d[u][0]) < (unsigned)n && (unsigned)(pj + d[u][1]) < (unsigned)n &&
+             (unsigned)(pk + d[u][2]) < (unsigned)n;
       ok[u] = in;
       // cells past the chunk or off the grid read the peak cell and are skipped
-      const int64_t li = lin + (ok[u] ? __float_as_int(cf[u].w) : 0);
-      ra[u] = __ldg(aos + 2 * li);
-      rb[u] = __ldg(aos + 2 * li + 1);
+      const int off = d[u][0] + n * d[u][1] + n2 * d[u][2];
+      ldg_record(aos + 2 * (lin + (in ? off : 0)), ra[u], rb[u]);
     }
-    if (PPB_GATHER_PREFETCH) {
+    if (c + 4 < cnt) wn = __ldg(cp + (c >> 2) + 1);
 #pragma unroll
-      for (int u = 0; u < GB; u++) cfn[u] = c + GB + u < cnt ? __ldg(a.cellf + s0 + c + GB + u) : zero4;
-    }
-#pragma unroll
-    for (int u = 0; u < GB; u++) {
+    for (int u = 0; u < 4; u++) {
       if (ok[u]) {
         nsh++;
-        if constexpr (COMP) accumulate_cell_packed(A, ra[u], rb[u], cf[u].x, cf[u].y, cf[u].z);
-        else accumulate_cell<false>(A, ra[u], rb[u], cf[u].x, cf[u].y, cf[u].z);
+        const float fi = small_int_float(d[u][0]), fj = small_int_float(d[u][1]), fk = small_int_float(d[u][2]);
+        if constexpr (COMP) accumulate_cell_packed(A, ra[u], rb[u], fi, fj, fk);
+        else accumulate_cell<false>(A, ra[u], rb[u], fi, fj, fk);
       }
-    }
-    if (!PPB_GATHER_PREFETCH) {
-#pragma unroll
-      for (int u = 0; u < GB; u++) cfn[u] = c + GB + u < cnt ? __ldg(a.cellf + s0 + c + GB + u) : zero4;
     }
   }
   return nsh;
@@ -353,7 +355,8 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
 
   // ---- the peak cell (shell 1) ------------------------------------------
   const float4* __restrict__ aos = a.aos;
-  const float4 c0 = __ldg(aos + 2 * lin), c1 = __ldg(aos + 2 * lin + 1);
+  float4 c0, c1;
+  ldg_record(aos + 2 * lin, c0, c1);
   if (lane < ROW) {
     double v = 0.0;
     if (lane == R_FBAR) v = (double)c0.x;
@@ -386,7 +389,7 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
       typename std::conditional<COMP, AccP, Acc<false>>::type A;
       A.zero();
       const int s0 = __ldg(a.ck_s + c0g + lane), cnt = s0 < cell_lim ? __ldg(a.ck_n + c0g + lane) : 0;
-      const int nsh = sum_chunk<decltype(A), COMP>(a, s0, cnt, lin, inside, pi, pj, pk, A);
+      const int nsh = sum_chunk<decltype(A), COMP>(a, c0g + lane, cnt, lin, inside, pi, pj, pk, A);
       visits += nsh;
 #pragma unroll
       for (int v = 0; v < NACC; v++) part[v * 32 + lane] = A.get(v);

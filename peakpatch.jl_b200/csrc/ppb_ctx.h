@@ -157,7 +157,6 @@ struct ppb_ctx {
   const ppb::GrowthTable& growth(double Om, double OB, double OL, double h);
   const std::vector<double>& chi_table(double Om, double OL, double h, double zmax);
   ppb::ShellTable& shell_table(int nhunt, cudaStream_t s);
-  const float4* cellf(ppb::ShellTable& st, int n, cudaStream_t s);
   ppb::DevCosmo dev_cosmo(ppb::Slot& sl, const ppb::GrowthTable& G, double Om, double OL, double h, double zmax,
                           bool need_chi);
   ppb::ShellArgs shell_args(ppb::Slot& sl, ppb::ShellTable& st, int n, double alatt, const float4* aos,

@@ -112,17 +112,18 @@ struct ShellTable {
   // cell offsets packed one per 32-bit word: bytes 0..2 = di, dj, dk as
   // signed 8-bit values (|d| <= nhunt <= 64)
   std::vector<int32_t> cell8;
-  // per grid size n: (di, dj, dk, linear offset di + n dj + n^2 dk as int
-  // bits) as one 16-byte load per cell for the gather
-  std::map<int, std::unique_ptr<DevBuf>> cellf;
+  // the packed offsets again, chunk by chunk, each chunk starting on a
+  // 16-byte boundary (zero padding), so that a gather lane reads the offsets
+  // of four consecutive cells of its chunk with one 16-byte load; chunk c
+  // starts at ck_cells[4 ck_p[c]]
+  std::vector<int32_t> ck_p, ck_cells;
   DevBuf d_cell8, d_start, d_count, d_r2m, d_rad, d_wlo, d_whi, d_woff, d_wts, d_w1, d_need, d_rad5;
-  DevBuf d_grp_a, d_grp_b, d_grp_c, d_ck_s, d_ck_n, d_sh_c0, d_sh_nc;
+  DevBuf d_grp_a, d_grp_b, d_grp_c, d_ck_s, d_ck_n, d_sh_c0, d_sh_nc, d_ck_p, d_ck_cells;
 };
 void build_shell_table(ShellTable& st, int nhunt);
 double hRinteg(double u0, double u12);
 std::vector<double> make_atab4();
 void upload_shell_table(ShellTable& st, cudaStream_t s);
-void build_cellf(const ShellTable& st, int n, std::vector<float4>& out);
 
 // ---------------------------------------------------------------------------
 // linear-growth and chi->z tables (host, double precision)
@@ -204,7 +205,8 @@ struct ShellArgs {
   double alatt;
   // shell geometry
   const int32_t* cell8;     // packed cell offsets (ShellTable::cell8)
-  const float4* cellf;      // cell offsets for grid size n (ShellTable::d_cellf)
+  const int32_t* ck_p;      // chunk starts in ck_cells, in 16-byte units
+  const int4* ck_cells;     // packed cell offsets, chunk-major (ShellTable::ck_cells)
   const int32_t* sh_start;
   const int32_t* sh_count;
   const double* rad;        // rad[m], m = 0..nshell (index 0 unused); rad[1] = 0
