@@ -317,7 +317,8 @@ int32_t ppb_last_table_stats(ppb_ctx* ctx, float* ms, int64_t* steps);
  *                     per-peak limits, walk length class) with at least
  *                     PPB_OPT_TUNE_MIN_PEAKS peaks times the gather-order
  *                     bricks (4, 8, 16, 32 cells, list order) and the
- *                     collapse widths (1, 2, 4 threads per peak) and keeps
+ *                     collapse kernels (1, 2, 4 threads per peak, lane
+ *                     queues) and keeps
  *                     the fastest; 0: defaults (8-cell bricks, width by
  *                     batch size); setting 2 clears the table.
  *                     Results do not depend on the choice.
@@ -325,8 +326,9 @@ int32_t ppb_last_table_stats(ppb_ctx* ctx, float* ms, int64_t* steps);
  *  PPB_OPT_BRICK_SHIFT     fixes the gather-order brick over the tuner's
  *                     choice: 2..5 (bricks of 4..32 cells), -1 list order,
  *                     -2 (default) the tuner's choice.
- *  PPB_OPT_COLLAPSE_THREADS  fixes the collapse width: 1, 2 or 4, 0 (default)
- *                     the tuner's choice.
+ *  PPB_OPT_COLLAPSE_THREADS  fixes the collapse kernel: 1, 2 or 4 threads
+ *                     per peak, 8 one thread per peak with lane work queues,
+ *                     0 (default) the tuner's choice.
  * Read-only (ppb_get_option, summed over the context's slots):
  *  PPB_OPT_GRAPH_LAUNCHES, PPB_OPT_GRAPH_INSTANTIATIONS, PPB_OPT_GRAPH_UPDATES. */
 enum {
@@ -352,7 +354,7 @@ typedef struct ppb_tune_entry {
   int32_t long_walk;          /* batches after ones with > 8 collapse-walk steps per peak (lightcone) */
   int64_t npk;                /* peaks of the batch the candidates were timed on */
   float gather_ms[5];         /* gather kernel: bricks of 4, 8, 16, 32 cells, list order */
-  float collapse_ms[3];       /* collapse kernel: 1, 2, 4 threads per peak */
+  float collapse_ms[4];       /* collapse kernel: 1, 2, 4 threads per peak, lane work queues (8) */
 } ppb_tune_entry;
 /* Copies up to `cap` entries; *n = the number of entries held. */
 int32_t ppb_tune_entries(ppb_ctx* ctx, ppb_tune_entry* out, int32_t cap, int32_t* n);

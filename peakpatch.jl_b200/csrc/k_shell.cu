@@ -39,6 +39,7 @@
 //
 //  d2f_kernel (one warp per collapsed peak).  Mean Laplacian over the cells
 //    within RTHL in list order, stopping at the first out-of-grid cell.
+#include <algorithm>
 #include <type_traits>
 
 #include "ppb_internal.h"
@@ -734,6 +735,8 @@ __device__ __noinline__ void kernel_strain(const ShellArgs& a, const Rows& R, in
     atomicAdd(R.counters + CNT_GUARD, 1ull);
     hi = R.mdone;
   }
+  // four rows' loads in flight per thread (the sum stays in m1 order)
+#pragma unroll 4
   for (int m1 = lo; m1 <= hi; m1++) {
     const double wt = __ldg(w + m1);
     if (mp == 1 && isnan(wt)) atomicAdd(R.counters + CNT_AKK, 1ull);
@@ -759,71 +762,13 @@ __device__ __forceinline__ void write_no_collapse(double* o) {
   for (int q = 0; q < RES_N; q++) o[q] = (q == 0 || q == 26) ? -1.0 : 0.0;
 }
 
-// One thread per peak: the walk one step at a time (the device is full of
-// peaks, so its latency is hidden).
-__device__ void collapse_one(const ShellArgs& a, int64_t p) {
-  double* out = a.out + p * RES_N;
-  const PeakHdr h = a.hdr[p];
-  if (h.status != HS_OK) {
-    write_no_collapse(out);
-    return;
-  }
+// Phases 6-7 of a collapsed peak (RadialShell.jl:707-790) and its result
+// row: m0 is the shell above the first collapsing step, last / prev the
+// kernel_strain values of that step and of the step before it (zvir1p /
+// zvir1 their zvir), lastFh the trace at the collapsing step.
+__device__ void collapse_finish(const ShellArgs& a, const Rows& R, double ZZon, int m0, double zvir1, double zvir1p,
+                                const KS& prev, const KS& last, double lastFh, const double* grf, double* out) {
   const double* __restrict__ rad = a.rad;
-  const Rows R{a.pool + h.off * ROW, h.mdone, a.counters};
-  const double ZZon = a.pk.ZZon[p];
-  const double alatt = a.alatt;
-  const int m = a.mlim[p];
-  const int4 gq = a.geo[p];
-  Geo geo;
-  geo.m0_init = gq.x; geo.mrf = gq.y; geo.mlow_rf = gq.z; geo.mupp_rf = gq.w;
-  const double anor = 1.0;
-  const double aRnor = 3.0 * anor / alatt, wnor = anor / (4.0 * 3.141592653589793), wRnor = 3.0 * wnor / alatt;
-
-  // Phase 3: gradient at the filter scale
-  double grf[3];
-  {
-    KS krf;
-    kernel_strain(a, R, geo.mrf, geo.mlow_rf, geo.mupp_rf, wRnor, aRnor, &krf);
-#pragma unroll
-    for (int L = 0; L < 3; L++) grf[L] = krf.g[L];
-  }
-
-  // Phase 5: inward walk (RadialShell.jl:566-699) from the crossing m0; the
-  // m0 step's zvir is forced to -1.  At mp = 1 the reference's running window
-  // is [2, last shell with rad < 2].
-  const int hi1 = last_lt(rad, 2, m, 2.0);
-  int m0 = h.m0;
-  KS prev, last;
-  kernel_strain(a, R, m0, 2, m0 > 1 ? m : hi1, wRnor, aRnor, &prev);
-  double zprev = -1.0, zvir1 = -1.0, zvir1p = -1.0, lastFh = 0.0;
-  bool collapsed = false;
-  long long steps = 1;
-  for (int mp = m0 - 1; mp >= 1; mp--) {
-    KS cur;
-    kernel_strain(a, R, mp, 2, mp > 1 ? m : hi1, wRnor, aRnor, &cur);
-    steps++;
-    double Fh, ev, pv;
-    ev_pv(cur.E, &Fh, &ev, &pv);
-    const double zv = zvir_of(a.tab, R.get(R_FBAR, mp), ev, pv);
-    if (zv >= ZZon) {
-      last = cur;
-      lastFh = Fh;
-      zvir1p = zv;
-      zvir1 = zprev;
-      m0 = mp + 1;
-      collapsed = true;
-      break;
-    }
-    prev = cur;
-    zprev = zv;
-  }
-  atomicAdd(a.counters + CNT_WALK, (unsigned long long)steps);
-  if (!collapsed) {
-    atomicAdd(a.counters + CNT_NOCOLL, 1ull);
-    write_no_collapse(out);
-    return;
-  }
-
   // Phase 6: collapse radius (RadialShell.jl:707-754)
   const double dZvir = zvir1p - zvir1;
   double RTHL;
@@ -928,6 +873,74 @@ __device__ void collapse_one(const ShellArgs& a, int64_t p) {
   r[30] = 0.0;
 #pragma unroll
   for (int q = 0; q < RES_N; q++) out[q] = r[q];
+}
+
+// One thread per peak: the walk one step at a time (the device is full of
+// peaks, so its latency is hidden).
+__device__ void collapse_one(const ShellArgs& a, int64_t p) {
+  double* out = a.out + p * RES_N;
+  const PeakHdr h = a.hdr[p];
+  if (h.status != HS_OK) {
+    write_no_collapse(out);
+    return;
+  }
+  const double* __restrict__ rad = a.rad;
+  const Rows R{a.pool + h.off * ROW, h.mdone, a.counters};
+  const double ZZon = a.pk.ZZon[p];
+  const double alatt = a.alatt;
+  const int m = a.mlim[p];
+  const int4 gq = a.geo[p];
+  Geo geo;
+  geo.m0_init = gq.x; geo.mrf = gq.y; geo.mlow_rf = gq.z; geo.mupp_rf = gq.w;
+  const double anor = 1.0;
+  const double aRnor = 3.0 * anor / alatt, wnor = anor / (4.0 * 3.141592653589793), wRnor = 3.0 * wnor / alatt;
+
+  // Phase 3: gradient at the filter scale
+  double grf[3];
+  {
+    KS krf;
+    kernel_strain(a, R, geo.mrf, geo.mlow_rf, geo.mupp_rf, wRnor, aRnor, &krf);
+#pragma unroll
+    for (int L = 0; L < 3; L++) grf[L] = krf.g[L];
+  }
+
+  // Phase 5: inward walk (RadialShell.jl:566-699) from the crossing m0; the
+  // m0 step's zvir is forced to -1.  At mp = 1 the reference's running window
+  // is [2, last shell with rad < 2].
+  const int hi1 = last_lt(rad, 2, m, 2.0);
+  int m0 = h.m0;
+  KS prev, last;
+  kernel_strain(a, R, m0, 2, m0 > 1 ? m : hi1, wRnor, aRnor, &prev);
+  double zprev = -1.0, zvir1 = -1.0, zvir1p = -1.0, lastFh = 0.0;
+  bool collapsed = false;
+  long long steps = 1;
+  for (int mp = m0 - 1; mp >= 1; mp--) {
+    KS cur;
+    kernel_strain(a, R, mp, 2, mp > 1 ? m : hi1, wRnor, aRnor, &cur);
+    steps++;
+    double Fh, ev, pv;
+    ev_pv(cur.E, &Fh, &ev, &pv);
+    const double zv = zvir_of(a.tab, R.get(R_FBAR, mp), ev, pv);
+    if (zv >= ZZon) {
+      last = cur;
+      lastFh = Fh;
+      zvir1p = zv;
+      zvir1 = zprev;
+      m0 = mp + 1;
+      collapsed = true;
+      break;
+    }
+    prev = cur;
+    zprev = zv;
+  }
+  atomicAdd(a.counters + CNT_WALK, (unsigned long long)steps);
+  if (!collapsed) {
+    atomicAdd(a.counters + CNT_NOCOLL, 1ull);
+    write_no_collapse(out);
+    return;
+  }
+
+  collapse_finish(a, R, ZZon, m0, zvir1, zvir1p, prev, last, lastFh, grf, out);
 }
 
 __device__ __forceinline__ KS shfl_ks(const KS& k, int src, unsigned mask) {
@@ -1030,110 +1043,7 @@ __device__ void collapse_group(const ShellArgs& a, int64_t p, int q, int qbase, 
     return;
   }
 
-  // Phase 6: collapse radius (RadialShell.jl:707-754)
-  const double dZvir = zvir1p - zvir1;
-  double RTHL;
-  const double ra = __ldg(rad + m0 - 1), rb = __ldg(rad + m0);
-  const double rad3p = ra * ra * ra, rad3 = rb * rb * rb;
-  if (zvir1 > 0.0 && dZvir != 0.0) {
-    const double R3 = rad3p + (rad3 - rad3p) * (zvir1p - ZZon) / dZvir;
-    RTHL = pow(R3, 1.0 / 3.0);
-  } else {
-    RTHL = ra;
-  }
-  if (RTHL <= 0.0) {
-    atomicAdd(a.counters + CNT_RTHLNEG, 1ull);
-    write_no_collapse(out);
-    return;
-  }
-  const double RTHL3 = RTHL * RTHL * RTHL, RTHL5 = RTHL3 * RTHL * RTHL;
-  const double drad3 = rad3 - rad3p;
-  const double Fa = R.get(R_FBAR, m0 - 1), Fb = R.get(R_FBAR, m0);
-  const double dFb = Fb - Fa;
-  double Fbarx;
-  double S[6], gk[3], gkf[3];
-  if (zvir1 > 0.0 && drad3 != 0.0) {
-    const double fr = (RTHL3 - rad3p) / drad3;
-    Fbarx = Fa + fr * dFb;
-#pragma unroll
-    for (int q = 0; q < 6; q++) S[q] = last.E[q] + fr * (prev.E[q] - last.E[q]);
-#pragma unroll
-    for (int L = 0; L < 3; L++) {
-      gk[L] = last.g[L] + fr * (prev.g[L] - last.g[L]);
-      gkf[L] = last.gf[L] + fr * (prev.gf[L] - last.gf[L]);
-    }
-  } else {
-    Fbarx = Fa;
-#pragma unroll
-    for (int q = 0; q < 6; q++) S[q] = last.E[q];
-#pragma unroll
-    for (int L = 0; L < 3; L++) { gk[L] = prev.g[L]; gkf[L] = prev.gf[L]; }
-  }
-  // normalize_strain then eigenvalues (RadialShell.jl:748-752)
-  {
-    const double tr = S[0] + S[1] + S[2];
-    if (tr != 0.0) {
-      const double f = Fbarx / tr;
-#pragma unroll
-      for (int q = 0; q < 6; q++) S[q] *= f;
-    }
-  }
-  double Frhoc, e_v_f, p_v_f;
-  ev_pv(S, &Frhoc, &e_v_f, &p_v_f);
-  double smat[6];
-#pragma unroll
-  for (int q = 0; q < 6; q++) smat[q] = last.E[q] * (Fbarx / lastFh);
-
-  // Phase 7: Sbar, Sbar2 (RadialShell.jl:758-773), Srb (:776-790)
-  double sb[6] = {0, 0, 0, 0, 0, 0};
-  long long nS = 0;
-  double srb = 0.0;
-  for (int m1 = 1; m1 <= m0 - 1; m1++) {
-    const double nn = R.get(R_N, m1);
-    if (nn > 0) {
-#pragma unroll
-      for (int L = 0; L < 3; L++) {
-        sb[L] += R.get(R_S + L, m1);
-        sb[3 + L] += R.get(R_S2 + L, m1);
-      }
-      nS += (long long)nn;
-    }
-    if (m1 >= 2) {
-      const double r5 = __ldg(a.rad5 + m1), r5p = m1 - 1 >= 2 ? __ldg(a.rad5 + m1 - 1) : 0.0;
-      srb += 0.5 * (R.get(R_FBAR, m1 - 1) + R.get(R_FBAR, m1)) * (r5 - r5p);
-    }
-  }
-  if (nS > 0) {
-#pragma unroll
-    for (int q = 0; q < 6; q++) sb[q] /= (double)nS;
-  }
-  const double rad5p = (m0 - 1 >= 2) ? __ldg(a.rad5 + m0 - 1) : 0.0;
-  if (zvir1 > 0.0 && dZvir != 0.0) srb += 0.5 * (Fa + Fbarx) * (RTHL5 - rad5p);
-  if (Fbarx * RTHL5 > 0.0) srb /= (Fbarx * RTHL5);
-
-  // results (layout in ppb.h); zvir_half (26) comes from zhalf_kernel and
-  // d2F (30) from d2f_kernel
-  double r[RES_N];
-  r[0] = RTHL;
-  r[1] = srb;
-#pragma unroll
-  for (int L = 0; L < 3; L++) {
-    r[2 + L] = sb[L];
-    r[5 + L] = sb[3 + L];
-    r[17 + L] = gk[L];
-    r[20 + L] = grf[L];
-    r[27 + L] = gkf[L];
-  }
-  r[8] = smat[0]; r[9] = smat[3]; r[10] = smat[4];
-  r[11] = smat[3]; r[12] = smat[1]; r[13] = smat[5];
-  r[14] = smat[4]; r[15] = smat[5]; r[16] = smat[2];
-  r[23] = Fbarx;
-  r[24] = e_v_f;
-  r[25] = p_v_f;
-  r[26] = -1.0;
-  r[30] = 0.0;
-#pragma unroll
-  for (int q = 0; q < RES_N; q++) out[q] = r[q];
+  collapse_finish(a, R, ZZon, m0, zvir1, zvir1p, prev, last, lastFh, grf, out);
 }
 
 __global__ void __launch_bounds__(128) collapse1_kernel(ShellArgs a) {
@@ -1147,6 +1057,105 @@ __global__ void __launch_bounds__(128) collapse_kernel(ShellArgs a) {
   const int64_t p = t / QT;
   const int lane = threadIdx.x & 31, q = lane & (QT - 1), qbase = lane & ~(QT - 1);
   if (p < a.npk) collapse_group<QT>(a, p, q, qbase, ((1u << QT) - 1u) << qbase);
+}
+
+// One thread per peak with a work queue per lane: a lane takes its next peak
+// from the batch as soon as its walk ends (the warp's idle lanes take theirs
+// with one atomic), so that short and long walks share warps instead of
+// lanes idling behind the longest walk of their warp.  Every loop round each
+// busy lane evaluates exactly one kernel_strain, at one program point: the
+// filter-scale window of phase 3, the crossing shell m0, or the next step of
+// the inward walk; the rest of a round is the step's small bookkeeping.
+// Per peak the arithmetic is collapse_one's, in the same order.
+__global__ void __launch_bounds__(128) collapseq_kernel(ShellArgs a) {
+  const int lane = threadIdx.x & 31;
+  const double anor = 1.0;
+  const double aRnor = 3.0 * anor / a.alatt, wnor = anor / (4.0 * 3.141592653589793), wRnor = 3.0 * wnor / a.alatt;
+  const double* __restrict__ rad = a.rad;
+  int state = 0;   // 0 idle, 1 filter-scale strain next, 2 crossing-shell strain next, 3 walking
+  bool retired = false;
+  int64_t p = 0;
+  Rows R{a.pool, 0, a.counters};
+  double ZZon = 0.0;
+  int m = 1, hi1 = 1, m0 = 1, mp = 1, mrf = 1, mlo = 1, mup = 1;
+  long long steps = 0;
+  double grf[3] = {0.0, 0.0, 0.0}, zprev = -1.0;
+  KS prev = {};
+  while (true) {
+    const bool want = state == 0 && !retired;
+    const unsigned wb = __ballot_sync(FULL, want);
+    if (wb) {
+      const int leader = __ffs(wb) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(a.cqueue, __popc(wb));
+      base = __shfl_sync(FULL, base, leader);
+      if (want) {
+        const int q = base + __popc(wb & ((1u << lane) - 1u));
+        if (q >= a.npk) {
+          retired = true;
+        } else {
+          p = q;
+          const PeakHdr h = a.hdr[p];
+          if (h.status != HS_OK) {
+            write_no_collapse(a.out + p * RES_N);   // state stays 0: the lane takes another peak
+          } else {
+            R = Rows{a.pool + h.off * ROW, h.mdone, a.counters};
+            ZZon = a.pk.ZZon[p];
+            m = a.mlim[p];
+            const int4 gq = a.geo[p];
+            mrf = gq.y; mlo = gq.z; mup = gq.w;
+            hi1 = last_lt(rad, 2, m, 2.0);
+            m0 = h.m0;
+            state = 1;
+          }
+        }
+      }
+    }
+    if (__ballot_sync(FULL, state != 0 || !retired) == 0) break;
+    if (state == 0) continue;
+    int c, lo, hi;
+    if (state == 1) { c = mrf; lo = mlo; hi = mup; }
+    else if (state == 2) { c = m0; lo = 2; hi = m0 > 1 ? m : hi1; }
+    else { c = mp; lo = 2; hi = mp > 1 ? m : hi1; }
+    KS cur;
+    kernel_strain(a, R, c, lo, hi, wRnor, aRnor, &cur);
+    if (state == 1) {          // Phase 3: gradient at the filter scale
+#pragma unroll
+      for (int L = 0; L < 3; L++) grf[L] = cur.g[L];
+      state = 2;
+    } else if (state == 2) {   // the crossing shell's strain; the walk starts below it
+      prev = cur;
+      zprev = -1.0;
+      steps = 1;
+      mp = m0 - 1;
+      state = 3;
+      if (mp < 1) {
+        atomicAdd(a.counters + CNT_WALK, (unsigned long long)steps);
+        atomicAdd(a.counters + CNT_NOCOLL, 1ull);
+        write_no_collapse(a.out + p * RES_N);
+        state = 0;
+      }
+    } else {                   // Phase 5: one inward step
+      steps++;
+      double Fh, ev, pv;
+      ev_pv(cur.E, &Fh, &ev, &pv);
+      const double zv = zvir_of(a.tab, R.get(R_FBAR, mp), ev, pv);
+      if (zv >= ZZon) {
+        atomicAdd(a.counters + CNT_WALK, (unsigned long long)steps);
+        collapse_finish(a, R, ZZon, mp + 1, zprev, zv, prev, cur, Fh, grf, a.out + p * RES_N);
+        state = 0;
+      } else if (mp == 1) {
+        atomicAdd(a.counters + CNT_WALK, (unsigned long long)steps);
+        atomicAdd(a.counters + CNT_NOCOLL, 1ull);
+        write_no_collapse(a.out + p * RES_N);
+        state = 0;
+      } else {
+        prev = cur;
+        zprev = zv;
+        mp--;
+      }
+    }
+  }
 }
 
 // ===========================================================================
@@ -1270,6 +1279,16 @@ void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive,
   PPB_LAUNCHED(*L.count);
 }
 
+int shell_collapseq_blocks(int nsm) {
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    int b = 0;
+    PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, collapseq_kernel, 128, 0));
+    per_sm = b > 0 ? b : 1;
+  }
+  return nsm * per_sm;
+}
+
 int shell_collapse_width(int64_t npk, int nsm, double walk_steps_per_peak) {
   // 4 threads per peak while 4 per peak still fit about 24 warps per SM or
   // when walks are long (more than 8 steps per peak in the previous batch:
@@ -1281,6 +1300,14 @@ int shell_collapse_width(int64_t npk, int nsm, double walk_steps_per_peak) {
 
 void launch_shell_collapse(Launch L, const ShellArgs& a, int nsm, double walk_steps_per_peak, int threads_per_peak) {
   int w = threads_per_peak;
+  if (w == 8) {   // one thread per peak, lane work queues (persistent grid)
+    if (a.npk == 0) return;
+    PPB_CUDA(cudaMemsetAsync(a.cqueue, 0, sizeof(int), L.s));
+    const int64_t blocks = std::min<int64_t>(shell_collapseq_blocks(nsm), (a.npk + 127) / 128);
+    collapseq_kernel<<<(unsigned)blocks, 128, 0, L.s>>>(a);
+    PPB_LAUNCHED(*L.count);
+    return;
+  }
   if (w != 1 && w != 2 && w != 4) w = shell_collapse_width(a.npk, nsm, walk_steps_per_peak);
   const int lg = w == 4 ? 2 : w - 1;
   const int64_t blocks = ((a.npk << lg) + 127) / 128;

@@ -39,7 +39,7 @@ struct TuneEntry {
   int collapse_threads = 0;   // 0: the size heuristic
   int64_t npk = 0;            // peaks of the batch it was measured on
   float gather_ms[5] = {};    // bricks of 4, 8, 16, 32 cells and list order
-  float collapse_ms[3] = {};  // 1, 2 and 4 threads per peak
+  float collapse_ms[4] = {};  // 1, 2 and 4 threads per peak, lane queues
 };
 
 struct ShellStats {

@@ -239,6 +239,7 @@ struct ShellArgs {
   int64_t stage_stride;     // doubles per warp slot
   double fhalf[10];         // ((e/9) / 2 + 1/2)^(1/3), e = 0..9 (zvir_half radii)
   int* queue;               // work counter for the persistent gather kernel
+  int* cqueue;              // work counter of the collapse lane queues
   const int32_t* order;     // gather order (queue position -> peak), null: list order
   int brick_shift;          // gather order key: Morton index of the peak's 2^brick_shift-cell brick
   unsigned long long* counters;   // [0] cell visits, [1..5] dump reasons
@@ -313,7 +314,8 @@ void launch_shell_geo(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx)
 void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks);
 // collapse threads per peak picked by batch size and walk length
 int shell_collapse_width(int64_t npk, int nsm, double walk_steps_per_peak);
-// threads_per_peak 1, 2 or 4; 0 picks by shell_collapse_width
+// threads_per_peak 1, 2 or 4 (thread groups per peak), 8 (one thread per
+// peak with lane work queues); 0 picks by shell_collapse_width
 void launch_shell_collapse(Launch L, const ShellArgs& a, int nsm, double walk_steps_per_peak, int threads_per_peak);
 void launch_shell_zhalf(Launch L, const ShellArgs& a);
 void launch_shell_d2f(Launch L, const ShellArgs& a, int blocks);

@@ -86,7 +86,7 @@ class _TuneEntry(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int32), ("nshell", ctypes.c_int32), ("comp", ctypes.c_int32),
                 ("adaptive", ctypes.c_int32), ("limited", ctypes.c_int32), ("brick_shift", ctypes.c_int32),
                 ("collapse_threads", ctypes.c_int32), ("long_walk", ctypes.c_int32), ("npk", ctypes.c_int64),
-                ("gather_ms", ctypes.c_float * 5), ("collapse_ms", ctypes.c_float * 3)]
+                ("gather_ms", ctypes.c_float * 5), ("collapse_ms", ctypes.c_float * 4)]
 
 
 # context options (include/ppb.h)
@@ -483,7 +483,7 @@ class Context:
                         "collapse_threads": e.collapse_threads, "npk": e.npk,
                         "gather_ms": dict(zip(("brick4", "brick8", "brick16", "brick32", "list"),
                                               [round(x, 4) for x in e.gather_ms])),
-                        "collapse_ms": dict(zip(("w1", "w2", "w4"), [round(x, 4) for x in e.collapse_ms]))})
+                        "collapse_ms": dict(zip(("w1", "w2", "w4", "queue"), [round(x, 4) for x in e.collapse_ms]))})
         return out
 
     def stage_ms(self):

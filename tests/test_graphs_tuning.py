@@ -65,7 +65,7 @@ def test_every_order_brick_and_collapse_width_gives_the_same_records(tctx, brick
     cfg = tile_config()
     ref, _, _ = tctx.run_tile_arrays(cfg, 41, RF)
     tctx.set_option(pp.OPT_BRICK_SHIFT, brick)
-    for w in (1, 2, 4):
+    for w in (1, 2, 4, 8):
         tctx.set_option(pp.OPT_COLLAPSE_THREADS, w)
         g, _, _ = tctx.run_tile_arrays(cfg, 41, RF)
         assert g.tobytes() == ref.tobytes(), (brick, w)
@@ -84,7 +84,7 @@ def test_autotuner_times_every_candidate_and_keeps_the_records(tctx):
     e = ents[0]
     assert e["n"] == cfg.n and e["comp"] and e["adaptive"] and not e["limited"] and e["npk"] == npk
     assert all(v > 0 for v in e["gather_ms"].values()) and all(v > 0 for v in e["collapse_ms"].values())
-    assert e["brick"] in (0, 4, 8, 16, 32) and e["collapse_threads"] in (0, 1, 2, 4)
+    assert e["brick"] in (0, 4, 8, 16, 32) and e["collapse_threads"] in (0, 1, 2, 4, 8)
     b, _, _ = tctx.run_tile_arrays(cfg, 43, RF)   # runs with the tuned choice, no new entry
     assert len(tctx.tune_entries()) == 1
     assert ref.tobytes() == a.tobytes() == b.tobytes()

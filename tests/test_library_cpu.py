@@ -40,8 +40,8 @@ def test_tile_params_layout_matches_the_header():
 
 
 def test_tune_entry_layout_and_option_entry_points():
-    # ppb_tune_entry: 8 int32, an int64, 5 + 3 floats
-    assert ctypes.sizeof(pp._TuneEntry) == 8 * 4 + 8 + 8 * 4
+    # ppb_tune_entry: 8 int32, an int64, 5 + 4 floats (padded to 8 bytes)
+    assert ctypes.sizeof(pp._TuneEntry) == 8 * 4 + 8 + 9 * 4 + 4
     assert pp._TuneEntry.gather_ms.offset == 40
     L = pp.load_library()
     v = ctypes.c_int64()
