@@ -628,7 +628,7 @@ struct KS {
 // Symmetric 3x3 eigenvalues, ascending: the trigonometric solution of the
 // characteristic cubic (O. K. Smith, "Eigenvalues of a symmetric 3 x 3
 // matrix", Comm. ACM 4 (1961) 168).  m = (xx, yy, zz, xy, xz, yz).
-__device__ __noinline__ void eig3(const double* m, double* lam) {
+__device__ __forceinline__ void eig3(const double* m, double* lam) {
   const double a00 = m[0], a11 = m[1], a22 = m[2], a01 = m[3], a02 = m[4], a12 = m[5];
   const double p1 = a01 * a01 + a02 * a02 + a12 * a12;
   double e1, e2, e3;
@@ -656,7 +656,7 @@ __device__ __noinline__ void eig3(const double* m, double* lam) {
 
 // trilinear lookup, outside the box -> -1 (CollapseTable.jl:128-145); Float32
 // or Float64 nodes
-__device__ __noinline__ double tab_interp(const DevTable& T, double x, double y, double z) {
+__device__ __forceinline__ double tab_interp(const DevTable& T, double x, double y, double z) {
   if (!(x >= T.x1 && x <= T.x2 && y >= T.y1 && y <= T.y2 && z >= T.z1 && z <= T.z2)) return -1.0;
   const double px = (x - T.x1) / ((T.x2 - T.x1) / (T.nx - 1));
   const double py = (y - T.y1) / ((T.y2 - T.y1) / (T.ny - 1));
@@ -716,7 +716,7 @@ struct Rows {
 // [lo, hi], summed in m1 order.  For mp > 1 only the shells with
 // (rad[mp] - rad[m1])^2 < 4 contribute (the table window); for mp == 1 the
 // SPH table weights apply to every m1 of [lo, hi].
-__device__ __noinline__ void kernel_strain(const ShellArgs& a, const Rows& R, int mp, int lo, int hi,
+__device__ __forceinline__ void kernel_strain(const ShellArgs& a, const Rows& R, int mp, int lo, int hi,
                                            double wRnor, double aRnor, KS* out) {
   double E[6] = {0, 0, 0, 0, 0, 0}, g[3] = {0, 0, 0}, gf[3] = {0, 0, 0};
   const double* w;
