@@ -412,6 +412,7 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
         for (int v = 0; v <= NACC; v++) t[v] += part[v * 32 + k];
       }
       const double r = __ldg(rad + m);
+      const double ir = 1.0 / r;   // one division; the products differ from t / r by at most an ulp
       const double nsh = t[NACC];
       my_dF = nsh > 0 ? t[0] / nsh : 0.0;
       double row[ROW];
@@ -422,15 +423,15 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
       for (int L = 0; L < 3; L++) {
         row[R_S + L] = t[1 + L];
         row[R_S2 + L] = t[4 + L];
-        row[R_G + L] = t[7 + L] / r;
-        row[R_GF + L] = t[10 + L] / r;
+        row[R_G + L] = t[7 + L] * ir;
+        row[R_GF + L] = t[10 + L] * ir;
       }
-      row[R_Q + 0] = (2.0 * t[13]) / r;
-      row[R_Q + 1] = (2.0 * t[14]) / r;
-      row[R_Q + 2] = (2.0 * t[15]) / r;
-      row[R_Q + 3] = t[16] / r;
-      row[R_Q + 4] = t[17] / r;
-      row[R_Q + 5] = t[18] / r;
+      row[R_Q + 0] = (2.0 * t[13]) * ir;
+      row[R_Q + 1] = (2.0 * t[14]) * ir;
+      row[R_Q + 2] = (2.0 * t[15]) * ir;
+      row[R_Q + 3] = t[16] * ir;
+      row[R_Q + 4] = t[17] * ir;
+      row[R_Q + 5] = t[18] * ir;
       double2* dst = reinterpret_cast<double2*>(stage + (int64_t)m * ROW);
 #pragma unroll
       for (int v = 1; v < ROW / 2; v++) dst[v] = make_double2(row[2 * v], row[2 * v + 1]);
