@@ -324,8 +324,8 @@ def run_ours(args, dist: Dist):
 
 # DRAM bytes (read + write) of one gather_kernel launch on the 384^3 tile,
 # scaled from the ncu capture of the same kernel on the 256^3 tile by the cell
-# visits (profiles/gather_kernel_run_tile_256.md): 4.64 GB x 824.5M / 179.3M
-GATHER_TRAFFIC_384 = 21.35e9
+# visits (profiles/gather_kernel_run_tile_256.md): 1.713 GB x 824.5M / 179.3M
+GATHER_TRAFFIC_384 = 7.88e9
 
 
 def _plain_compare(ctx, cfg, seed, dev_out, cap, opt_tiles_per_s):
