@@ -222,6 +222,70 @@ int32_t ppb_analyse_peaks_lim(ppb_ctx* ctx, const float* delta, const float* eta
                               const double* Rf, const int64_t* ir2min, const double* ZZon, const double* fcrit,
                               const int32_t* r2lim, double alatt, int32_t plain, double* out);
 
+/* ---- multi-resolution tile fields ---------------------------------------
+ * The MUSIC-style split of run_multitile_split (src/MultiResolution.jl:523-
+ * 1236): a coarse M^3 periodic grid for the long modes plus, per tile, an
+ * isolated zero-padded convolution of the Hoffman–Ribak residual noise.
+ * Global fine grid N^3 with N % M == 0 (block = N / M <= 1024); tiles are
+ * numbered (it, jt, kt) from 1 and cover nmesh^3 cells starting at global
+ * cell (t - 1) nsub - (nmesh - nsub) / 2 (0-based, periodic in N).  P(k) is
+ * the table of ppb_set_pk_table.  Fields are column-major Float32, host or
+ * device. */
+
+/* _downsample_noise (src/MultiResolution.jl:68-89): coarse cell (I, J, K) =
+ * sum of the block^3 Float64 Threefry deviates of its fine cells (noise of
+ * fill_noise_threefry! on the N^3 grid) in the reference's order, divided by
+ * sqrt(block^3), rounded to Float32.  Bit-identical to the reference.
+ * out: M^3. */
+int32_t ppb_downsample_noise(ppb_ctx* ctx, int64_t N, int32_t M, uint64_t seed, float* out);
+
+/* _generate_extended_residual (src/MultiResolution.jl:197-236): fine noise
+ * minus coarse[cell's block] * Float32(1/sqrt(block^3)) on the tile's region
+ * extended by nshell cells per side.  Bit-identical.
+ * out: (nmesh + 2 nshell)^3. */
+int32_t ppb_extended_residual(ppb_ctx* ctx, const float* coarse, int32_t M, int32_t it, int32_t jt, int32_t kt,
+                              int32_t nsub, int32_t nmesh, int64_t N, uint64_t seed, int32_t nshell, float* out);
+
+/* isolated_convolve_gpu_multi (stub src/PeakPatch.jl:280-298; CPU
+ * _isolated_convolve, src/MultiResolution.jl:246-283): zero-pad the n_input^3
+ * noise to (2 n_input)^3, one rfft, then per kernel multiply by
+ * sqrt(P(k) dk^3 n2^3) times the kernel (DC := 0, dk = 2 pi / (n2 dx),
+ * dx = boxsize_local / n), irfft, keep the n^3 region starting at nshell.
+ * kernels: nkern triples (kernel_fn_id, dim1, dim2) with the ids of
+ * isolated_convolve_gpu: 0 sqrt(P), 1 i k_dim1/k^2, 2 -i k_dim1/k^2,
+ * 3 -k_dim1 k_dim2/k^2, 4 k^2.  out: nkern consecutive n^3 fields.
+ * n_input <= 640 and nshell + n <= 2 n_input. */
+int32_t ppb_isolated_convolve(ppb_ctx* ctx, const float* noise, int32_t n_input, double boxsize_local, int32_t n,
+                              const int32_t* kernels, int32_t nkern, int32_t nshell, float* out);
+
+/* interpolate_to_tile_gpu (stub src/PeakPatch.jl:329-339; CPU
+ * _interpolate_to_tile / _tricubic, src/MultiResolution.jl:95-122, 156-189):
+ * Catmull-Rom tricubic interpolation of the periodic M^3 coarse field at the
+ * tile's fine cells.  Bit-identical.  out: nmesh^3. */
+int32_t ppb_interpolate_to_tile(ppb_ctx* ctx, const float* coarse, int32_t it, int32_t jt, int32_t kt, int32_t nsub,
+                                int32_t nmesh, int64_t N, int32_t M, float* out);
+
+/* compute_2lpt_gpu (stub src/PeakPatch.jl:300-316; CPU block
+ * src/MultiResolution.jl:804-831): tile-local periodic 2LPT of delta_tile,
+ * src2 = delta^2/2 - sum_a phi_aa^2/2 - sum_{a<b} phi_ab^2, psi2_d =
+ * irfft(-i k_d/k^2 rfft(src2)), with _apply_kernel_inplace!'s zeroing of the
+ * DC mode and the Nyquist planes.  psi2: 3 consecutive n^3 fields. */
+int32_t ppb_compute_2lpt(ppb_ctx* ctx, const float* delta_tile, int32_t n, double boxsize_local, float* psi2);
+
+/* compute_laplacian_gpu (stub src/PeakPatch.jl:318-327; CPU
+ * src/MultiResolution.jl:835-846): irfft(k^2 rfft(delta_tile)) with the same
+ * zeroing (no extra 1/n^3, unlike run_tile's lapd).  lapd: n^3. */
+int32_t ppb_compute_laplacian(ppb_ctx* ctx, const float* delta_tile, int32_t n, double boxsize_local, float* lapd);
+
+/* The coarse phase of run_multitile_split (src/MultiResolution.jl:617-667)
+ * on the M^3 coarse noise, each field an irfft of _periodic_convolve!
+ * (:286-309) of its rfft in a box of side boxsize_full: delta (M^3), psi
+ * (3 M^3, 1LPT kernels), psi2 (3 M^3, ilpt >= 2: the trace-identity source
+ * convolved with sqrt(P) and the 2LPT kernel, as the reference does) and
+ * lapd (M^3, ioutshear >= 1).  Any output may be NULL. */
+int32_t ppb_coarse_fields(ppb_ctx* ctx, const float* coarse_noise, int32_t M, double boxsize_full, int32_t ilpt,
+                          int32_t ioutshear, float* delta, float* psi, float* psi2, float* lapd);
+
 /* ---- memory helpers ----------------------------------------------------- */
 /* Page-locked host memory (fast, asynchronous copies of records) and device
  * memory on the context's GPU, for callers that have no CUDA runtime of

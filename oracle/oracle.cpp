@@ -1482,4 +1482,150 @@ int64_t ora_merge_catalog(const float* rec, int64_t n, int nf, float* out, int32
   return m;
 }
 
+
+// ---------------------------------------------------------------------------
+// Multi-resolution (MUSIC-style) per-tile building blocks,
+// src/MultiResolution.jl: _downsample_noise (:68-89), _generate_extended_residual
+// (:197-236), _tricubic / _catmull_rom (:156-189), _interpolate_to_tile (:95-122),
+// the transfer multiply of _isolated_convolve (:246-283) and
+// _apply_kernel_inplace! (:1239-1255).  Indices 0-based here; the reference's
+// 1-based (it, jt, kt) tile numbers are kept.
+// ---------------------------------------------------------------------------
+void ora_mr_coarse_noise(int64_t N, int64_t M, uint64_t seed, float* out) {
+  const int64_t block = N / M;
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+  for (int64_t K = 0; K < M; K++)
+    for (int64_t J = 0; J < M; J++)
+      for (int64_t I = 0; I < M; I++) {
+        double val = 0.0;
+        for (int64_t dk = 0; dk < block; dk++)
+          for (int64_t dj = 0; dj < block; dj++)
+            for (int64_t di = 0; di < block; di++) {
+              const int64_t gi = I * block + di, gj = J * block + dj, gk = K * block + dk;
+              val += ppbm::noise_cell_d(seed, (uint64_t)(gi + N * (gj + N * gk)));   // Float64 deviate
+            }
+        const double b = (double)block;
+        out[I + M * (J + M * K)] = (float)(val / std::sqrt(b * b * b));
+      }
+}
+
+static inline int64_t mod0(int64_t i, int64_t n) { int64_t r = i % n; return r < 0 ? r + n : r; }
+
+void ora_mr_residual(const float* coarse, int64_t M, int64_t it, int64_t jt, int64_t kt, int64_t nsub, int64_t nmesh,
+                     int64_t N, uint64_t seed, int64_t nshell, float* out) {
+  const int64_t block = N / M, nbuff = (nmesh - nsub) / 2, next = nmesh + 2 * nshell;
+  const double b = (double)block;
+  const float inv = (float)(1.0 / std::sqrt(b * b * b));
+  // 0-based origin of the extended region in global cells
+  const int64_t i0 = (it - 1) * nsub - nbuff - nshell, j0 = (jt - 1) * nsub - nbuff - nshell,
+                k0 = (kt - 1) * nsub - nbuff - nshell;
+#pragma omp parallel for schedule(static)
+  for (int64_t lk = 0; lk < next; lk++)
+    for (int64_t lj = 0; lj < next; lj++)
+      for (int64_t li = 0; li < next; li++) {
+        const int64_t gi = mod0(i0 + li, N), gj = mod0(j0 + lj, N), gk = mod0(k0 + lk, N);
+        const float fine = ppbm::noise_cell(seed, (uint64_t)(gi + N * (gj + N * gk)));
+        const float bm = coarse[gi / block + M * (gj / block + M * (gk / block))] * inv;
+        out[li + next * (lj + next * lk)] = fine - bm;
+      }
+}
+
+static inline void catmull_rom(float t, float* w) {
+  const float t2 = t * t, t3 = t2 * t;
+  w[0] = -0.5f * t3 + t2 - 0.5f * t;
+  w[1] = 1.5f * t3 - 2.5f * t2 + 1.0f;
+  w[2] = -1.5f * t3 + 2.0f * t2 + 0.5f * t;
+  w[3] = 0.5f * t3 - 0.5f * t2;
+}
+
+void ora_mr_tricubic(const float* coarse, int64_t M, int64_t it, int64_t jt, int64_t kt, int64_t nsub, int64_t nmesh,
+                     int64_t N, float* out) {
+  const int64_t block = N / M, nbuff = (nmesh - nsub) / 2;
+  const int64_t i0 = (it - 1) * nsub - nbuff, j0 = (jt - 1) * nsub - nbuff, k0 = (kt - 1) * nsub - nbuff;
+#pragma omp parallel for schedule(static)
+  for (int64_t lk = 0; lk < nmesh; lk++)
+    for (int64_t lj = 0; lj < nmesh; lj++)
+      for (int64_t li = 0; li < nmesh; li++) {
+        // 1-based global cell gi (as the reference) -> fractional coarse coordinate
+        const int64_t g[3] = {mod0(i0 + li, N) + 1, mod0(j0 + lj, N) + 1, mod0(k0 + lk, N) + 1};
+        int64_t ic[3];
+        float w[3][4];
+        for (int d = 0; d < 3; d++) {
+          const double f = ((double)g[d] - 0.5) / (double)block + 0.5;
+          ic[d] = (int64_t)std::floor(f);
+          catmull_rom((float)(f - (double)ic[d]), w[d]);
+        }
+        float val = 0.0f;
+        for (int a = 0; a < 4; a++) {
+          const int64_t kk = mod0(ic[2] - 1 + a - 1, M);   // mod1(iz + dkk, M) - 1
+          for (int bq = 0; bq < 4; bq++) {
+            const int64_t jj = mod0(ic[1] - 1 + bq - 1, M);
+            for (int c = 0; c < 4; c++) {
+              const int64_t ii = mod0(ic[0] - 1 + c - 1, M);
+              val += w[0][c] * w[1][bq] * w[2][a] * coarse[ii + M * (jj + M * kk)];
+            }
+          }
+        }
+        out[li + nmesh * (lj + nmesh * lk)] = val;
+      }
+}
+
+// kernel kinds (the reference's kernel_fn ids): 0 none, 1 i k_d1/k^2 (1LPT),
+// 2 -i k_d1/k^2 (2LPT), 3 -k_d1 k_d2/k^2 (phi_ij), 4 k^2 (Laplacian); d1, d2
+// in 1..3.  v *= mult * kernel, rounded once to complex64.
+static inline c64 apply_kind(c64 v, double mult, int kind, int d1, int d2, double kx, double ky, double kz,
+                             double k2) {
+  const double kv[3] = {kx, ky, kz};
+  const double a = (double)v.real(), b = (double)v.imag();
+  switch (kind) {
+    case 0: return c64((float)(a * mult), (float)(b * mult));
+    case 1: { const double c = mult * (kv[d1 - 1] / k2); return c64((float)(-b * c), (float)(a * c)); }
+    case 2: { const double c = mult * (-kv[d1 - 1] / k2); return c64((float)(-b * c), (float)(a * c)); }
+    case 3: { const double c = mult * (-kv[d1 - 1] * kv[d2 - 1] / k2); return c64((float)(a * c), (float)(b * c)); }
+    default: { const double c = mult * k2; return c64((float)(a * c), (float)(b * c)); }
+  }
+}
+
+// the transfer multiply of _isolated_convolve (on the rfft of the padded
+// n2^3 box, box = n2 * dx) and of _periodic_convolve! (:286-309, box =
+// boxsize): sqrt(P(k) dk^3 n2^3) times the kernel, dk = 2 pi / box, DC := 0
+void ora_mr_transfer(c64* arr, int64_t n2, double box, const double* k, const double* pk, int np, int kind, int d1,
+                     int d2) {
+  std::vector<double> lk(np), lp(np);
+  for (int i = 0; i < np; i++) { lk[i] = std::log(k[i]); lp[i] = std::log(pk[i]); }
+  const double dk = 2.0 * PI / box;
+  const double mult = ((double)n2 * dk) / (double)n2;
+  const int64_t nh = n2 / 2 + 1;
+  const double nd = (double)n2;
+#pragma omp parallel for schedule(static)
+  for (int64_t iz = 0; iz < n2; iz++)
+    for (int64_t iy = 0; iy < n2; iy++)
+      for (int64_t ix = 0; ix < nh; ix++) {
+        const double kx = (double)ix * mult, ky = freq(iy, n2, mult), kz = freq(iz, n2, mult);
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        c64& v = arr[ix + nh * (iy + n2 * iz)];
+        if (k2 == 0.0) { v = c64(0.f, 0.f); continue; }
+        const double amp = std::sqrt(pk_eval(lk.data(), lp.data(), np, std::sqrt(k2)) * (dk * dk * dk) * (nd * nd * nd));
+        v = apply_kind(v, amp, kind, d1, d2, kx, ky, kz, k2);
+      }
+}
+
+// _apply_kernel_inplace!: periodic n^3 box; DC, ix = n/2, iy = n/2 and
+// iz = n/2 zeroed
+void ora_mr_apply_kernel(c64* arr, int64_t n, double boxsize, int kind, int d1, int d2) {
+  const double dk = 2.0 * PI / boxsize;
+  const double mult = ((double)n * dk) / (double)n;
+  const int64_t nh = n / 2 + 1, nyq = n / 2;
+#pragma omp parallel for schedule(static)
+  for (int64_t iz = 0; iz < n; iz++)
+    for (int64_t iy = 0; iy < n; iy++)
+      for (int64_t ix = 0; ix < nh; ix++) {
+        const double kx = (double)ix * mult, ky = freq(iy, n, mult), kz = freq(iz, n, mult);
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        c64& v = arr[ix + nh * (iy + n * iz)];
+        if (k2 == 0.0 || ix == nh - 1 || iy == nyq || iz == nyq) { v = c64(0.f, 0.f); continue; }
+        v = apply_kind(v, 1.0, kind, d1, d2, kx, ky, kz, k2);
+      }
+}
+
 }  // extern "C"

@@ -80,6 +80,11 @@ def _declare(L):
     L.ora_hRinteg.argtypes = [D, D]
     L.ora_hRinteg.restype = D
     L.ora_make_table.argtypes = [D, D, D, D, P, P, P]
+    L.ora_mr_coarse_noise.argtypes = [I64, I64, ctypes.c_uint64, P]
+    L.ora_mr_residual.argtypes = [P, I64, I64, I64, I64, I64, I64, I64, ctypes.c_uint64, I64, P]
+    L.ora_mr_tricubic.argtypes = [P, I64, I64, I64, I64, I64, I64, I64, P]
+    L.ora_mr_transfer.argtypes = [P, I64, D, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.ora_mr_apply_kernel.argtypes = [P, I64, D, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     L.ora_elliptic_rd.argtypes = [D, D, D]
     L.ora_elliptic_rd.restype = D
     L.ora_shape_b2.argtypes = [D, D, D, P]
@@ -643,3 +648,173 @@ def run_multitile(cfg: Config, seed: int, pk_k, pk_p, filters, T: Table, ntile: 
 
 def run_tile(cfg: Config, seed: int, pk_k, pk_p, filters, T: Table) -> np.ndarray:
     return run_tile_stages(cfg, seed, pk_k, pk_p, filters, T)["records"]
+
+
+# --------------------------------------------------------------------------
+# Multi-resolution (MUSIC-style) per-tile building blocks
+# (src/MultiResolution.jl).  Arrays C-order [k][j][i] (Julia [i, j, k]); tile
+# numbers (it, jt, kt) 1-based as the reference.
+# Kernel kinds: 0 delta, 1 1LPT (i k_d1 / k^2), 2 2LPT (-i k_d1 / k^2),
+# 3 phi_ij (-k_d1 k_d2 / k^2), 4 Laplacian (k^2).
+# --------------------------------------------------------------------------
+def mr_coarse_noise(N: int, M: int, seed: int) -> np.ndarray:
+    """_downsample_noise (:68-89): block means of the global Threefry noise,
+    summed in double, scaled to unit variance."""
+    out = np.empty((M, M, M), np.float32)
+    lib().ora_mr_coarse_noise(N, M, seed, _p(out))
+    return out
+
+
+def mr_residual(coarse, M, it, jt, kt, nsub, nmesh, N, seed, nshell=0) -> np.ndarray:
+    """_generate_extended_residual (:197-236): fine noise minus its coarse
+    cell's block mean on the tile's (nmesh + 2 nshell)^3 region."""
+    c = np.ascontiguousarray(coarse, np.float32)
+    ne = nmesh + 2 * nshell
+    out = np.empty((ne, ne, ne), np.float32)
+    lib().ora_mr_residual(_p(c), M, it, jt, kt, nsub, nmesh, N, seed, nshell, _p(out))
+    return out
+
+
+def mr_tricubic(coarse, M, it, jt, kt, nsub, nmesh, N) -> np.ndarray:
+    """_interpolate_to_tile (:95-122): Catmull-Rom tricubic interpolation of
+    the periodic coarse grid at the tile's fine cells."""
+    c = np.ascontiguousarray(coarse, np.float32)
+    out = np.empty((nmesh, nmesh, nmesh), np.float32)
+    lib().ora_mr_tricubic(_p(c), M, it, jt, kt, nsub, nmesh, N, _p(out))
+    return out
+
+
+def isolated_convolve(noise, pk_k, pk_p, boxsize_local, n, kind=0, d1=0, d2=0, nshell=0) -> np.ndarray:
+    """_isolated_convolve (:246-283): zero-pad to twice the input size, rfft,
+    multiply by sqrt(P(k) dk^3 n2^3) and the kernel, irfft, keep the n^3 tile
+    region (offset nshell)."""
+    noise = np.ascontiguousarray(noise, np.float32)
+    ni = noise.shape[0]
+    n2 = 2 * ni
+    padded = np.zeros((n2, n2, n2), np.float32)
+    padded[:ni, :ni, :ni] = noise
+    pk = np.ascontiguousarray(rfft3(padded))
+    kk = np.ascontiguousarray(pk_k, np.float64)
+    pp = np.ascontiguousarray(pk_p, np.float64)
+    dx = float(boxsize_local) / n
+    lib().ora_mr_transfer(_p(pk), n2, n2 * dx, _p(kk), _p(pp), len(kk), kind, d1, d2)
+    res = irfft3(pk, n2)
+    return np.ascontiguousarray(res[nshell:nshell + n, nshell:nshell + n, nshell:nshell + n])
+
+
+def mr_apply_kernel(arr_k, n, boxsize, kind, d1=0, d2=0) -> np.ndarray:
+    a = np.ascontiguousarray(arr_k, np.complex64).copy()
+    lib().ora_mr_apply_kernel(_p(a), n, float(boxsize), kind, d1, d2)
+    return a
+
+
+def tile_2lpt_laplacian(delta_tile, n, boxsize, ilpt=2, want_lap=True):
+    """The tile-local 2LPT and Laplacian of run_multitile_split
+    (src/MultiResolution.jl:804-847): src2 = delta^2/2 - sum_d phi_dd^2/2 -
+    sum_{i<j} phi_ij^2, psi2_d = irfft(-i k_d/k^2 src2_k), lapd =
+    irfft(k^2 delta_k), with the kernel applied by _apply_kernel_inplace!.
+    Returns (psi2 (3, n, n, n) or None, lapd or None)."""
+    d = np.ascontiguousarray(delta_tile, np.float32)
+    dk = rfft3(d)
+    psi2 = None
+    if ilpt >= 2:
+        h = np.float32(0.5)
+        src2 = np.zeros_like(d)
+        src2 = src2 + (d * d) * h
+        for a in (1, 2, 3):
+            r = irfft3(mr_apply_kernel(dk, n, boxsize, 3, a, a), n)
+            src2 = src2 - (r * r) * h
+        for a, b in ((1, 2), (1, 3), (2, 3)):
+            r = irfft3(mr_apply_kernel(dk, n, boxsize, 3, a, b), n)
+            src2 = src2 - r * r
+        s2k = rfft3(src2)
+        psi2 = np.stack([irfft3(mr_apply_kernel(s2k, n, boxsize, 2, a), n) for a in (1, 2, 3)])
+    lap = irfft3(mr_apply_kernel(dk, n, boxsize, 4), n) if want_lap else None
+    return psi2, lap
+
+
+def periodic_convolve(arr_k, pk_k, pk_p, n, boxsize, kind=0, d1=0, d2=0) -> np.ndarray:
+    """_periodic_convolve! (:286-309) on a copy of the rfft arr_k of a
+    periodic n^3 box of side boxsize."""
+    a = np.ascontiguousarray(arr_k, np.complex64).copy()
+    kk = np.ascontiguousarray(pk_k, np.float64)
+    pp = np.ascontiguousarray(pk_p, np.float64)
+    lib().ora_mr_transfer(_p(a), n, float(boxsize), _p(kk), _p(pp), len(kk), kind, d1, d2)
+    return a
+
+
+def coarse_fields(coarse_noise, pk_k, pk_p, boxsize_full, ilpt=2, ioutshear=1):
+    """Phase 1a of run_multitile_split (:617-667) on the M^3 coarse noise:
+    delta_coarse, psi_coarse (3, M, M, M), psi2_coarse (ilpt >= 2, the
+    reference's P(k)-weighted 2LPT multiplier) and lapd_coarse (ioutshear >=
+    1), each an irfft of a _periodic_convolve! of the coarse rfft."""
+    c = np.ascontiguousarray(coarse_noise, np.float32)
+    M = c.shape[0]
+    ck = rfft3(c)
+    pc = lambda a, kind, d1=0, d2=0: irfft3(periodic_convolve(a, pk_k, pk_p, M, boxsize_full, kind, d1, d2), M)
+    delta = pc(ck, 0)
+    psi = np.stack([pc(ck, 1, a) for a in (1, 2, 3)])
+    psi2 = None
+    if ilpt >= 2:
+        h = np.float32(0.5)
+        src2 = np.zeros_like(c)
+        src2 = src2 + (delta * delta) * h
+        for a in (1, 2, 3):
+            r = pc(ck, 3, a, a)
+            src2 = src2 - (r * r) * h
+        for a, b in ((1, 2), (1, 3), (2, 3)):
+            r = pc(ck, 3, a, b)
+            src2 = src2 - r * r
+        s2k = rfft3(src2)
+        psi2 = np.stack([pc(s2k, 2, a) for a in (1, 2, 3)])
+    lap = pc(ck, 4) if ioutshear >= 1 else None
+    return delta, psi, psi2, lap
+
+
+def _correlation(a, b):
+    da = a - a.sum() / a.size
+    db = b - b.sum() / b.size
+    return float((da * db).sum() / np.sqrt((da ** 2).sum() * (db ** 2).sum()))
+
+
+def _rms_frac(a, b):
+    ra = np.sqrt((a ** 2).sum() / a.size)
+    return float(np.sqrt(((a - b) ** 2).sum() / a.size) / ra) if ra > 0 else 0.0
+
+
+def compare_fields_split(pk_k, pk_p, N, boxsize, seed, ntile, coarse_factor, nbuff=8, coarse_grid=0):
+    """compare_fields_split (src/MultiResolution.jl:1266-1353): per tile, the
+    split delta and psi_x (isolated convolution of the residual plus the
+    tricubic coarse field) against the global-FFT fields on the tile core.
+    Returns [(tile, corr_delta, rms_delta, corr_psi1, rms_psi1)]."""
+    nsub = (N - 2 * nbuff) // ntile
+    nmesh = nsub + 2 * nbuff
+    assert nsub * ntile + 2 * nbuff == N
+    M = coarse_grid if coarse_grid > 0 else ntile * coarse_factor
+    assert N % M == 0
+    alatt = boxsize / N
+    dg = generate_grf(N, pk_k, pk_p, boxsize, seed)
+    psig = lpt1(rfft3(dg), N, boxsize)[0]
+    cn = mr_coarse_noise(N, M, seed)
+    ck = rfft3(cn)
+    dc = irfft3(periodic_convolve(ck, pk_k, pk_p, M, boxsize, 0), M)
+    pc = irfft3(periodic_convolve(ck, pk_k, pk_p, M, boxsize, 1, 1), M)
+    box_tile = nmesh * alatt
+    out = []
+    for kt in range(1, ntile + 1):
+        for jt in range(1, ntile + 1):
+            for it in range(1, ntile + 1):
+                sl = lambda t: slice((t - 1) * nsub, t * nsub)
+                core = slice(nbuff, nbuff + nsub)
+                ref_d = dg[sl(kt), sl(jt), sl(it)].astype(np.float64)
+                ref_p = psig[sl(kt), sl(jt), sl(it)].astype(np.float64)
+                res = mr_residual(cn, M, it, jt, kt, nsub, nmesh, N, seed, 0)
+                d = isolated_convolve(res, pk_k, pk_p, box_tile, nmesh, 0) + mr_tricubic(dc, M, it, jt, kt, nsub,
+                                                                                          nmesh, N)
+                p = isolated_convolve(res, pk_k, pk_p, box_tile, nmesh, 1, 1) + mr_tricubic(pc, M, it, jt, kt, nsub,
+                                                                                             nmesh, N)
+                d = d[core, core, core].astype(np.float64)
+                p = p[core, core, core].astype(np.float64)
+                out.append(((it, jt, kt), _correlation(ref_d, d), _rms_frac(ref_d, d), _correlation(ref_p, p),
+                            _rms_frac(ref_p, p)))
+    return out

@@ -38,7 +38,7 @@ def _headers():
 
 # per-file flags: the collapse-table integrations must not contract
 # multiplies and adds (bit-exact with the CPU restatement)
-FILE_FLAGS = {"k_table.cu": ["-fmad=false"]}
+FILE_FLAGS = {"k_table.cu": ["-fmad=false"], "k_multires.cu": ["-fmad=false"]}
 
 
 def _compile(src: str, extra: list[str]) -> str:

@@ -59,9 +59,10 @@ void Slot::release_buffers() {
   tiles.clear();
   tile_lru.clear();
   for (DevBuf* b : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
-                    &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim})
+                    &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &mr_in, &mr_out, &mr_aux})
     b->release();
   tune_save.release();
+  iso.reset();
 }
 
 size_t Slot::bytes_held() const {
@@ -73,8 +74,10 @@ size_t Slot::bytes_held() const {
 size_t Slot::shell_bytes() const {
   size_t b = 0;
   for (const DevBuf* d : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool,
-                          &okey, &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim})
+                          &okey, &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &mr_in,
+                          &mr_out, &mr_aux})
     b += d->bytes;
+  if (iso) b += iso->bytes();
   return b;
 }
 

@@ -11,6 +11,7 @@
 // following inverse transform (cuFFT's C2R is unnormalised, Julia's irfft is
 // normalised), passed as `post_scale`.
 #include "ppb_internal.h"
+#include "ppb_kspace.cuh"
 #include "ppb_math.h"
 
 namespace ppb {
@@ -18,13 +19,8 @@ namespace ppb {
 namespace {
 
 constexpr double kPi = 3.141592653589793;
-
-// AbstractFFTs frequency of 0-based index idx: fftfreq keeps idx < ceil(n/2)
-// non-negative, the rest wrap to idx - n; rfftfreq is idx itself.
-__device__ __forceinline__ double fftfreq(int idx, int n, double mult) {
-  const int v = idx < (n + 1) / 2 ? idx : idx - n;
-  return (double)v * mult;
-}
+using ks::fftfreq;
+using ks::pk_eval;
 
 // mode decomposition for a (nh x n) plane per blockIdx.y = iz
 struct Mode {
@@ -65,27 +61,6 @@ __global__ void noise_kernel(float* __restrict__ out, int64_t ncell, uint64_t se
       out[c] = (float)g1;
     }
   }
-}
-
-// ---------------------------------------------------------------------------
-// P(k): log-log linear interpolation with linear extrapolation
-// (PowerSpectrum.jl:11-30)
-// ---------------------------------------------------------------------------
-__device__ double pk_eval(const double* __restrict__ lk, const double* __restrict__ lp, int np, double k) {
-  const double x = log(k);
-  int i;
-  if (x <= lk[0]) i = 0;
-  else if (x >= lk[np - 1]) i = np - 2;
-  else {
-    int lo = 0, hi = np - 1;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (lk[mid] <= x) lo = mid; else hi = mid;
-    }
-    i = lo;
-  }
-  const double t = (x - lk[i]) / (lk[i + 1] - lk[i]);
-  return exp(lp[i] * (1.0 - t) + lp[i + 1] * t);
 }
 
 // noise_k *= sqrt(P(k) dk^3 n^3), DC := 0  (RandomField.jl:136-168)

@@ -1,0 +1,356 @@
+// multires.cu — C-ABI entry points of the multi-resolution (MUSIC-style)
+// tile fields of run_multitile_split (src/MultiResolution.jl), the drop-in
+// for the reference's GPU plug-in functions isolated_convolve_gpu(_multi),
+// interpolate_to_tile_gpu, compute_2lpt_gpu and compute_laplacian_gpu
+// (stubs src/PeakPatch.jl:255-339) and for the CPU steps around them
+// (_downsample_noise, _generate_extended_residual, the coarse phase).
+//
+// All of them run on the context's synchronous slot; buffers stay resident
+// between calls (the isolated convolution keeps its plans for the last padded
+// size, the periodic kernels use the slot's per-size tile buffers).
+#include <algorithm>
+#include <cmath>
+
+#include "ppb_ctx.h"
+
+using namespace ppb;
+
+namespace ppb {
+
+// ---------------------------------------------------------------------------
+// isolated-convolution resources
+// ---------------------------------------------------------------------------
+static cufftHandle plan_inplace(int n, cufftType t, size_t* ws) {
+  cufftHandle h;
+  PPB_CUFFT(cufftCreate(&h));
+  PPB_CUFFT(cufftSetAutoAllocation(h, 0));
+  long long dims[3] = {n, n, n};
+  const long long nh = n / 2 + 1;
+  long long cemb[3] = {n, n, nh}, remb[3] = {n, n, 2 * nh};
+  const long long cdist = (long long)n * n * nh, rdist = 2 * cdist;
+  if (t == CUFFT_R2C)
+    PPB_CUFFT(cufftMakePlanMany64(h, 3, dims, remb, 1, rdist, cemb, 1, cdist, t, 1, ws));
+  else
+    PPB_CUFFT(cufftMakePlanMany64(h, 3, dims, cemb, 1, cdist, remb, 1, rdist, t, 1, ws));
+  return h;
+}
+
+IsoRes::~IsoRes() {
+  if (r2c) cufftDestroy(r2c);
+  if (c2r) cufftDestroy(c2r);
+}
+
+void IsoRes::setup(int nn, int nb, cudaStream_t s) {
+  const int64_t modes = (int64_t)(nn / 2 + 1) * nn * nn;
+  if (nn != n2) {
+    if (r2c) { cufftDestroy(r2c); r2c = 0; }
+    if (c2r) { cufftDestroy(c2r); c2r = 0; }
+    n2 = 0;
+    size_t w1 = 0, w2 = 0;
+    r2c = plan_inplace(nn, CUFFT_R2C, &w1);
+    c2r = plan_inplace(nn, CUFFT_C2R, &w2);
+    ws.ensure(std::max<size_t>(std::max(w1, w2), 256));
+    PPB_CUFFT(cufftSetWorkArea(r2c, ws.p));
+    PPB_CUFFT(cufftSetWorkArea(c2r, ws.p));
+    spec.ensure(modes * 8);
+    n2 = nn;
+  }
+  PPB_CUFFT(cufftSetStream(r2c, s));
+  PPB_CUFFT(cufftSetStream(c2r, s));
+  work.ensure((size_t)nb * modes * 8);
+  batch = (int)(work.bytes / ((size_t)modes * 8));
+}
+
+}  // namespace ppb
+
+namespace {
+
+// the reference's frequency kernels (kernel_fn_id, dim1, dim2) accepted by
+// isolated_convolve_gpu (src/PeakPatch.jl:261-272)
+void check_kernel(int kind, int d1, int d2) {
+  PPB_REQUIRE(kind >= 0 && kind <= 4, "kernel_fn_id must be 0..4");
+  if (kind == 1 || kind == 2 || kind == 3) PPB_REQUIRE(d1 >= 1 && d1 <= 3, "dim1 must be 1..3");
+  if (kind == 3) PPB_REQUIRE(d2 >= 1 && d2 <= 3, "dim2 must be 1..3");
+}
+
+void check_coarse(int64_t N, int M) {
+  PPB_REQUIRE(N >= 1 && M >= 1 && N % M == 0, "N must be a positive multiple of M");
+  PPB_REQUIRE(N / M <= 1024, "block N/M above 1024");
+  PPB_REQUIRE(N <= (1ll << 20), "N above 2^20");
+  PPB_REQUIRE((int64_t)M * M * M <= (1ll << 30), "M^3 above 2^30");
+}
+
+void check_tile(int it, int jt, int kt, int nsub, int nmesh) {
+  PPB_REQUIRE(it >= 1 && jt >= 1 && kt >= 1, "tile numbers are 1-based");
+  PPB_REQUIRE(nmesh >= 1 && nsub >= 1 && nsub <= nmesh, "need 1 <= nsub <= nmesh");
+  PPB_REQUIRE(nmesh <= 2048, "nmesh above 2048");
+}
+
+// 0-based global origin of a tile's region extended by `ext` cells
+// (src/MultiResolution.jl:207-209, 1-based there)
+int64_t origin(int t, int nsub, int nmesh, int ext) { return (int64_t)(t - 1) * nsub - (nmesh - nsub) / 2 - ext; }
+
+template <class F>
+int32_t guarded(ppb_ctx* ctx, F&& body) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  try {
+    PPB_CUDA(cudaSetDevice(ctx->device));
+    body();
+    return PPB_OK;
+  } catch (const ppb::Error& e) {
+    ctx->set_error(e.msg);
+    return e.code;
+  } catch (...) {
+    ctx->set_error("unknown error");
+    return PPB_ERR_INVALID;
+  }
+}
+
+// device buffer for a result of `bytes`: the caller's own when it is device
+// memory, else the staging buffer (copied out by finish_out)
+float* out_buffer(float* dst, DevBuf& stage, size_t bytes) {
+  if (is_device_ptr(dst)) return dst;
+  stage.ensure(bytes);
+  return stage.as<float>();
+}
+
+void finish_out(float* dst, const float* dev, size_t bytes, cudaStream_t s) {
+  if (dst != dev) PPB_CUDA(cudaMemcpyAsync(dst, dev, bytes, cudaMemcpyDeviceToHost, s));
+}
+
+// the periodic n^3 kernels of run_multitile_split's tile stage on the slot's
+// tile buffers: rfft of delta_tile into tr.dk (delta_tile copied to tr.delta)
+TileRes& periodic_setup(ppb_ctx* ctx, const float* delta_tile, int n) {
+  Slot& sl = ctx->sync;
+  TileRes& tr = sl.tile_for(n);
+  tr.setup(n, sl.stream);
+  const int64_t N = (int64_t)n * n * n;
+  PPB_CUDA(cudaMemcpyAsync(tr.delta.p, delta_tile, N * 4, cudaMemcpyDefault, sl.stream));
+  PPB_CUFFT(cufftExecR2C(tr.r2c, tr.delta.as<float>(), tr.dk.as<cufftComplex>()));
+  sl.launches++;
+  return tr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t ppb_downsample_noise(ppb_ctx* ctx, int64_t N, int32_t M, uint64_t seed, float* out) {
+  return guarded(ctx, [&] {
+    PPB_REQUIRE(out, "null argument");
+    check_coarse(N, M);
+    Slot& sl = ctx->sync;
+    const size_t bytes = (size_t)M * M * M * 4;
+    float* d = out_buffer(out, sl.mr_out, bytes);
+    launch_coarse_noise(Launch{sl.stream, &sl.launches}, d, N, M, seed);
+    finish_out(out, d, bytes, sl.stream);
+    PPB_CUDA(cudaStreamSynchronize(sl.stream));
+  });
+}
+
+int32_t ppb_extended_residual(ppb_ctx* ctx, const float* coarse, int32_t M, int32_t it, int32_t jt, int32_t kt,
+                              int32_t nsub, int32_t nmesh, int64_t N, uint64_t seed, int32_t nshell, float* out) {
+  return guarded(ctx, [&] {
+    PPB_REQUIRE(coarse && out, "null argument");
+    check_coarse(N, M);
+    check_tile(it, jt, kt, nsub, nmesh);
+    PPB_REQUIRE(nshell >= 0 && nmesh + 2 * (int64_t)nshell <= 4096, "nshell out of range");
+    Slot& sl = ctx->sync;
+    const int next = nmesh + 2 * nshell;
+    const size_t bytes = (size_t)next * next * next * 4;
+    const float* c = (const float*)stage_in(sl.mr_in, coarse, (size_t)M * M * M * 4, sl.stream);
+    float* d = out_buffer(out, sl.mr_out, bytes);
+    launch_residual(Launch{sl.stream, &sl.launches}, c, d, M, N, origin(it, nsub, nmesh, nshell),
+                    origin(jt, nsub, nmesh, nshell), origin(kt, nsub, nmesh, nshell), next, seed);
+    finish_out(out, d, bytes, sl.stream);
+    PPB_CUDA(cudaStreamSynchronize(sl.stream));
+  });
+}
+
+int32_t ppb_interpolate_to_tile(ppb_ctx* ctx, const float* coarse, int32_t it, int32_t jt, int32_t kt, int32_t nsub,
+                                int32_t nmesh, int64_t N, int32_t M, float* out) {
+  return guarded(ctx, [&] {
+    PPB_REQUIRE(coarse && out, "null argument");
+    check_coarse(N, M);
+    check_tile(it, jt, kt, nsub, nmesh);
+    Slot& sl = ctx->sync;
+    const size_t bytes = (size_t)nmesh * nmesh * nmesh * 4;
+    const float* c = (const float*)stage_in(sl.mr_in, coarse, (size_t)M * M * M * 4, sl.stream);
+    float* d = out_buffer(out, sl.mr_out, bytes);
+    launch_tricubic(Launch{sl.stream, &sl.launches}, c, d, M, N, origin(it, nsub, nmesh, 0), origin(jt, nsub, nmesh, 0),
+                    origin(kt, nsub, nmesh, 0), nmesh);
+    finish_out(out, d, bytes, sl.stream);
+    PPB_CUDA(cudaStreamSynchronize(sl.stream));
+  });
+}
+
+int32_t ppb_isolated_convolve(ppb_ctx* ctx, const float* noise, int32_t n_input, double boxsize_local, int32_t n,
+                              const int32_t* kernels, int32_t nkern, int32_t nshell, float* out) {
+  return guarded(ctx, [&] {
+    PPB_REQUIRE(noise && out && kernels, "null argument");
+    PPB_REQUIRE(n_input >= 1 && n_input <= 640, "n_input must be 1..640");
+    PPB_REQUIRE(n >= 1 && nshell >= 0 && (int64_t)nshell + n <= 2 * (int64_t)n_input,
+                "the tile region [nshell, nshell + n) must lie inside the padded box");
+    PPB_REQUIRE(nkern >= 1 && nkern <= 64, "nkern must be 1..64");
+    PPB_REQUIRE(boxsize_local > 0.0, "boxsize_local must be > 0");
+    for (int b = 0; b < nkern; b++) check_kernel(kernels[3 * b], kernels[3 * b + 1], kernels[3 * b + 2]);
+    std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
+    PPB_REQUIRE(ctx->sh.pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
+    Slot& sl = ctx->sync;
+    cudaStream_t s = sl.stream;
+    Launch L{s, &sl.launches};
+    const int n2 = 2 * n_input, nh2 = n2 / 2 + 1;
+    const int64_t modes = (int64_t)nh2 * n2 * n2, px = 2 * (int64_t)nh2;
+    // kernels per transfer pass: all of them (up to 4) unless memory is short
+    int batch = std::min(nkern, 4);
+    if (!sl.iso) sl.iso.reset(new IsoRes());
+    IsoRes& iso = *sl.iso;
+    if (iso.n2 != n2 || iso.batch < batch) {
+      size_t fr = 0, tot = 0;
+      PPB_CUDA(cudaMemGetInfo(&fr, &tot));
+      const size_t have = fr + iso.work.bytes + iso.spec.bytes;
+      while (batch > 1 && (size_t)(batch + 2) * modes * 8 > have) batch--;
+    }
+    iso.setup(n2, batch, s);
+    batch = std::min(iso.batch, std::min(nkern, kMaxKSpecs));
+    const int64_t Nt = (int64_t)n * n * n;
+    const float* src = (const float*)stage_in(sl.mr_in, noise, (size_t)n_input * n_input * n_input * 4, s);
+    float* dout = out_buffer(out, sl.mr_out, (size_t)nkern * Nt * 4);
+    launch_pad(L, src, iso.spec.as<float>(), n_input, n2, px);
+    PPB_CUFFT(cufftExecR2C(iso.r2c, iso.spec.as<float>(), iso.spec.as<cufftComplex>()));
+    sl.launches++;
+    // dx = boxsize_local / n; the padded box is n2 * dx (src/MultiResolution.jl:249-259)
+    const double box = (double)n2 * (boxsize_local / (double)n);
+    const double post = 1.0 / ((double)n2 * (double)n2 * (double)n2);
+    for (int b0 = 0; b0 < nkern; b0 += batch) {
+      const int g = std::min(batch, nkern - b0);
+      int kind[kMaxKSpecs], d1[kMaxKSpecs], d2[kMaxKSpecs];
+      for (int q = 0; q < g; q++) {
+        kind[q] = kernels[3 * (b0 + q)];
+        d1[q] = kernels[3 * (b0 + q) + 1];
+        d2[q] = kernels[3 * (b0 + q) + 2];
+      }
+      launch_kspace(L, true, iso.spec.as<float2>(), iso.work.as<float2>(), modes, n2, box, ctx->sh.pk_lk.as<double>(),
+                    ctx->sh.pk_lp.as<double>(), ctx->sh.pk_n, kind, d1, d2, g, post);
+      for (int q = 0; q < g; q++) {
+        float2* w = iso.work.as<float2>() + q * modes;
+        PPB_CUFFT(cufftExecC2R(iso.c2r, reinterpret_cast<cufftComplex*>(w), reinterpret_cast<float*>(w)));
+        sl.launches++;
+        launch_extract(L, dout + (b0 + q) * Nt, reinterpret_cast<const float*>(w),
+                       (int64_t)nshell * (1 + px + px * n2), px, px * n2, n);
+      }
+    }
+    finish_out(out, dout, (size_t)nkern * Nt * 4, s);
+    PPB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int32_t ppb_compute_2lpt(ppb_ctx* ctx, const float* delta_tile, int32_t n, double boxsize_local, float* psi2) {
+  return guarded(ctx, [&] {
+    PPB_REQUIRE(delta_tile && psi2, "null argument");
+    PPB_REQUIRE(n >= 2 && n <= 1024, "n must be 2..1024");
+    PPB_REQUIRE(boxsize_local > 0.0, "boxsize_local must be > 0");
+    Slot& sl = ctx->sync;
+    cudaStream_t s = sl.stream;
+    Launch L{s, &sl.launches};
+    const int64_t N = (int64_t)n * n * n, Mk = (int64_t)(n / 2 + 1) * n * n;
+    TileRes& tr = periodic_setup(ctx, delta_tile, n);
+    const double post = 1.0 / ((double)n * (double)n * (double)n);
+    // phi_11, phi_22, phi_33, phi_12, phi_13, phi_23 (:812-821)
+    const int pk6[6] = {3, 3, 3, 3, 3, 3}, pa[6] = {1, 2, 3, 1, 1, 2}, pb[6] = {1, 2, 3, 2, 3, 3};
+    launch_kspace(L, false, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, n, boxsize_local, nullptr, nullptr, 0, pk6, pa,
+                  pb, 6, post);
+    PPB_CUFFT(cufftExecC2R(tr.c2r6, tr.kw.as<cufftComplex>(), tr.rw.as<float>()));
+    sl.launches++;
+    launch_src2_trace(L, tr.delta.as<float>(), tr.rw.as<float>(), tr.rw.as<float>(), n, n, (int64_t)n * n, N);
+    PPB_CUFFT(cufftExecR2C(tr.r2c, tr.rw.as<float>(), tr.dk.as<cufftComplex>()));
+    sl.launches++;
+    const int k2[3] = {2, 2, 2}, da[3] = {1, 2, 3}, db[3] = {0, 0, 0};
+    launch_kspace(L, false, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, n, boxsize_local, nullptr, nullptr, 0, k2, da,
+                  db, 3, post);
+    float* d = out_buffer(psi2, sl.mr_out, (size_t)3 * N * 4);
+    PPB_CUFFT(cufftExecC2R(tr.c2r3, tr.kw.as<cufftComplex>(), d));
+    sl.launches++;
+    finish_out(psi2, d, (size_t)3 * N * 4, s);
+    PPB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int32_t ppb_compute_laplacian(ppb_ctx* ctx, const float* delta_tile, int32_t n, double boxsize_local, float* lapd) {
+  return guarded(ctx, [&] {
+    PPB_REQUIRE(delta_tile && lapd, "null argument");
+    PPB_REQUIRE(n >= 2 && n <= 1024, "n must be 2..1024");
+    PPB_REQUIRE(boxsize_local > 0.0, "boxsize_local must be > 0");
+    Slot& sl = ctx->sync;
+    cudaStream_t s = sl.stream;
+    Launch L{s, &sl.launches};
+    const int64_t N = (int64_t)n * n * n, Mk = (int64_t)(n / 2 + 1) * n * n;
+    TileRes& tr = periodic_setup(ctx, delta_tile, n);
+    const double post = 1.0 / ((double)n * (double)n * (double)n);
+    const int k4[1] = {4}, z[1] = {0};
+    launch_kspace(L, false, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, n, boxsize_local, nullptr, nullptr, 0, k4, z, z,
+                  1, post);
+    float* d = out_buffer(lapd, sl.mr_out, (size_t)N * 4);
+    PPB_CUFFT(cufftExecC2R(tr.c2r1, tr.kw.as<cufftComplex>(), d));
+    sl.launches++;
+    finish_out(lapd, d, (size_t)N * 4, s);
+    PPB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int32_t ppb_coarse_fields(ppb_ctx* ctx, const float* coarse_noise, int32_t M, double boxsize_full, int32_t ilpt,
+                          int32_t ioutshear, float* delta, float* psi, float* psi2, float* lapd) {
+  return guarded(ctx, [&] {
+    PPB_REQUIRE(coarse_noise, "null argument");
+    PPB_REQUIRE(M >= 2 && M <= 1024, "M must be 2..1024");
+    PPB_REQUIRE(boxsize_full > 0.0, "boxsize_full must be > 0");
+    std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
+    PPB_REQUIRE(ctx->sh.pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
+    const double* lk = ctx->sh.pk_lk.as<double>();
+    const double* lp = ctx->sh.pk_lp.as<double>();
+    const int np = ctx->sh.pk_n;
+    Slot& sl = ctx->sync;
+    cudaStream_t s = sl.stream;
+    Launch L{s, &sl.launches};
+    const int64_t N = (int64_t)M * M * M, Mk = (int64_t)(M / 2 + 1) * M * M;
+    TileRes& tr = periodic_setup(ctx, coarse_noise, M);
+    const double post = 1.0 / ((double)M * (double)M * (double)M);
+    // outputs: delta, psi (3), psi2 (3), lapd
+    sl.mr_aux.ensure(8 * N * 4);
+    float* o = sl.mr_aux.as<float>();
+    auto c2r_into = [&](int q, float* dst) {
+      PPB_CUFFT(cufftExecC2R(tr.c2r1, tr.kw.as<cufftComplex>() + q * Mk, dst));
+      sl.launches++;
+    };
+    {  // delta and psi_d (:621-632), lapd (:662-667)
+      int kind[5] = {0, 1, 1, 1, 4}, a[5] = {0, 1, 2, 3, 0}, b[5] = {0, 0, 0, 0, 0};
+      const int g = ioutshear >= 1 ? 5 : 4;
+      launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, kind, a, b, g,
+                    post);
+      for (int q = 0; q < 4; q++) c2r_into(q, o + q * N);
+      if (g == 5) c2r_into(4, o + 7 * N);
+    }
+    if (ilpt >= 2) {  // the 2LPT source and displacements (:635-659)
+      const int pk6[6] = {3, 3, 3, 3, 3, 3}, pa[6] = {1, 2, 3, 1, 1, 2}, pb[6] = {1, 2, 3, 2, 3, 3};
+      launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, pk6, pa, pb, 6,
+                    post);
+      PPB_CUFFT(cufftExecC2R(tr.c2r6, tr.kw.as<cufftComplex>(), tr.rw.as<float>()));
+      sl.launches++;
+      launch_src2_trace(L, o, tr.rw.as<float>(), tr.rw.as<float>(), M, M, (int64_t)M * M, N);
+      PPB_CUFFT(cufftExecR2C(tr.r2c, tr.rw.as<float>(), tr.dk.as<cufftComplex>()));
+      sl.launches++;
+      const int k2[3] = {2, 2, 2}, da[3] = {1, 2, 3}, db[3] = {0, 0, 0};
+      launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, k2, da, db, 3,
+                    post);
+      for (int q = 0; q < 3; q++) c2r_into(q, o + (4 + q) * N);
+    }
+    if (delta) copy_out(delta, o, N * 4, s);
+    if (psi) copy_out(psi, o + N, 3 * N * 4, s);
+    if (psi2 && ilpt >= 2) copy_out(psi2, o + 4 * N, 3 * N * 4, s);
+    if (lapd && ioutshear >= 1) copy_out(lapd, o + 7 * N, N * 4, s);
+    PPB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+}  // extern "C"

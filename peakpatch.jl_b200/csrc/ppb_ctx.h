@@ -32,6 +32,20 @@ struct TileRes {
   size_t bytes() const;
 };
 
+// the zero-padded isolated convolution of one padded size n2 (multires.cu):
+// in-place transforms over one cuFFT work area
+struct IsoRes {
+  int n2 = 0, batch = 0;
+  cufftHandle r2c = 0, c2r = 0;   // n2^3, in place, one transform each
+  DevBuf spec;   // the padded input (row pitch 2 (n2/2+1) floats), then its half-spectrum
+  DevBuf work;   // `batch` half-spectra, each then transformed back in place
+  DevBuf ws;     // cuFFT work area of both plans
+  ~IsoRes();
+  // plans and buffers for padded size n2 and up to `batch` kernels per pass
+  void setup(int n2, int batch, cudaStream_t s);
+  size_t bytes() const { return spec.bytes + work.bytes + ws.bytes; }
+};
+
 // one autotuned shell-stage configuration: the gather order brick and the
 // collapse threads per peak, with the timings of every candidate
 struct TuneEntry {
@@ -70,6 +84,8 @@ struct Slot {
   DevBuf stage, counters, ctl, hdr, geo, mlim, pool;   // shell stage
   DevBuf okey, okey2, oidx, oidx2, otmp;            // spatial gather order
   DevBuf tcen, tcount, t_aos, t_lapd;               // multi-tile: centres, peaks per tile, tile fields
+  std::unique_ptr<IsoRes> iso;                      // multi-resolution: isolated convolution
+  DevBuf mr_in, mr_out, mr_aux;                     // multi-resolution: staged inputs and outputs
   int gather_bps[2][2] = {{0, 0}, {0, 0}};          // gather blocks per SM by [comp][adaptive]
   double rows_per_peak[2] = {0.0, 0.0};             // pool rows per peak seen last, by adaptive
   double walk_per_peak = 0.0;                       // collapse-walk steps per peak seen last

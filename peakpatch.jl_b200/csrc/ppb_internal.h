@@ -320,4 +320,24 @@ void launch_shell_collapse(Launch L, const ShellArgs& a, int nsm, double walk_st
 void launch_shell_zhalf(Launch L, const ShellArgs& a);
 void launch_shell_d2f(Launch L, const ShellArgs& a, int blocks);
 
+// multi-resolution tile fields (k_multires.cu).  Origins (i0, j0, k0) are
+// 0-based global cells, periodic in N; coarse grids are M^3 with N % M == 0.
+constexpr int kMaxKSpecs = 6;   // kernels per k-space launch
+void launch_coarse_noise(Launch L, float* out, int64_t N, int M, uint64_t seed);
+void launch_residual(Launch L, const float* coarse, float* out, int M, int64_t N, int64_t i0, int64_t j0, int64_t k0,
+                     int next, uint64_t seed);
+void launch_pad(Launch L, const float* in, float* out, int nin, int n2, int64_t px);
+// transfer (P(k) amplitude, isolated / periodic convolution) or apply
+// (kernel only, Nyquist planes zeroed) of nspec kernels (kind, d1, d2) from
+// the half-spectrum `in` of an n^3 box of side `box` into nspec half-spectra
+// odist float2 apart, times post; Hermitian projection fused
+void launch_kspace(Launch L, bool transfer, const float2* in, float2* out, int64_t odist, int n, double box,
+                   const double* lk, const double* lp, int np, const int* kind, const int* d1, const int* d2,
+                   int nspec, double post);
+void launch_src2_trace(Launch L, const float* delta, const float* phi, float* out, int n, int64_t px, int64_t pz,
+                       int64_t pd);
+void launch_tricubic(Launch L, const float* coarse, float* out, int M, int64_t N, int64_t i0, int64_t j0, int64_t k0,
+                     int n);
+void launch_add(Launch L, float* dst, const float* a, const float* b, int64_t N);
+
 }  // namespace ppb

@@ -211,13 +211,15 @@ PPB_HD void threefry_gaussian_pair(uint64_t seed, uint64_t pair, double* g1, dou
   *g2 = dmul(r, sn);
 }
 
-// Noise value of the cell with 0-based column-major linear index `lin`
+// Float64 deviate of the cell with 0-based column-major linear index `lin`
 // (lin = i + n*j + n*n*k, i fastest): pair lin>>1, first deviate when lin is
 // even, second when odd (RandomField.jl:75-78).
-PPB_HD float noise_cell(uint64_t seed, uint64_t lin) {
+PPB_HD double noise_cell_d(uint64_t seed, uint64_t lin) {
   double g1, g2;
   threefry_gaussian_pair(seed, lin >> 1, &g1, &g2);
-  return (float)((lin & 1ULL) ? g2 : g1);
+  return (lin & 1ULL) ? g2 : g1;
 }
+// the deviate rounded to Float32, the value stored in a noise field
+PPB_HD float noise_cell(uint64_t seed, uint64_t lin) { return (float)noise_cell_d(seed, lin); }
 
 }  // namespace ppbm

@@ -145,7 +145,8 @@ EXPORTED = (
     "ppb_last_shell_times", "ppb_serve_config", "ppb_submit", "ppb_wait", "ppb_stats_get", "ppb_stats_reset",
     "ppb_run_multitile", "ppb_merge_catalog", "ppb_set_collapse_table_f64", "ppb_generate_fields",
     "ppb_analyse_peaks_lim", "ppb_set_option", "ppb_get_option", "ppb_tune_entries", "ppb_make_collapse_table",
-    "ppb_last_table_stats",
+    "ppb_last_table_stats", "ppb_downsample_noise", "ppb_extended_residual", "ppb_isolated_convolve",
+    "ppb_interpolate_to_tile", "ppb_compute_2lpt", "ppb_compute_laplacian", "ppb_coarse_fields",
 )
 
 
@@ -200,6 +201,14 @@ def load_library():
     L.ppb_set_option.argtypes = [P, I32, I64]
     L.ppb_get_option.argtypes = [P, I32, ctypes.POINTER(ctypes.c_int64)]
     L.ppb_tune_entries.argtypes = [P, ctypes.POINTER(_TuneEntry), I32, ctypes.POINTER(ctypes.c_int32)]
+    U64 = ctypes.c_uint64
+    L.ppb_downsample_noise.argtypes = [P, I64, I32, U64, P]
+    L.ppb_extended_residual.argtypes = [P, P, I32, I32, I32, I32, I32, I32, I64, U64, I32, P]
+    L.ppb_isolated_convolve.argtypes = [P, P, I32, D, I32, P, I32, I32, P]
+    L.ppb_interpolate_to_tile.argtypes = [P, P, I32, I32, I32, I32, I32, I64, I32, P]
+    L.ppb_compute_2lpt.argtypes = [P, P, I32, D, P]
+    L.ppb_compute_laplacian.argtypes = [P, P, I32, D, P]
+    L.ppb_coarse_fields.argtypes = [P, P, I32, D, I32, I32, P, P, P, P]
     for f in ("ppb_alloc_host", "ppb_alloc_device"):
         getattr(L, f).argtypes = [P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
     for f in ("ppb_free_host", "ppb_free_device"):
@@ -730,6 +739,98 @@ class Context:
         if psi2 is not None:
             out.update(eta2x=psi2[0], eta2y=psi2[1], eta2z=psi2[2])
         return out
+
+    # ---- multi-resolution tile fields (src/MultiResolution.jl) -------------
+    # Arrays are C-order float32 (k, j, i) = Julia's column-major [i, j, k];
+    # tiles (it, jt, kt) are 1-based.  P(k) is the resident table: pass
+    # pk=(k, P) to install one first, or None to use the installed one.
+    def _pk(self, pk):
+        if pk is not None:
+            self.set_pk_table(np.asarray(pk[0], np.float64), np.asarray(pk[1], np.float64))
+
+    @staticmethod
+    def _f32(a, name):
+        a = np.ascontiguousarray(a, np.float32)
+        if a.ndim != 3 or not a.shape[0] == a.shape[1] == a.shape[2]:
+            raise ValueError(f"{name} must be a cubic 3-D array")
+        return a
+
+    def downsample_noise(self, N: int, M: int, seed: int) -> np.ndarray:
+        """_downsample_noise(N, M, seed) (src/MultiResolution.jl:68-89)."""
+        out = np.empty((M, M, M), np.float32)
+        self._check(self.L.ppb_downsample_noise(self.h, N, M, int(seed) & (2**64 - 1), _p(out)))
+        return out
+
+    def generate_extended_residual(self, it: int, jt: int, kt: int, nsub: int, nmesh: int, N: int, seed: int,
+                                   coarse_noise: np.ndarray, M: int, nshell: int = 0) -> np.ndarray:
+        """_generate_extended_residual (src/MultiResolution.jl:197-236)."""
+        c = self._f32(coarse_noise, "coarse_noise")
+        if c.shape[0] != M:
+            raise ValueError("coarse_noise must be M^3")
+        ne = nmesh + 2 * nshell
+        out = np.empty((ne, ne, ne), np.float32)
+        self._check(self.L.ppb_extended_residual(self.h, _p(c), M, it, jt, kt, nsub, nmesh, N,
+                                                 int(seed) & (2**64 - 1), nshell, _p(out)))
+        return out
+
+    def isolated_convolve_gpu_multi(self, noise: np.ndarray, pk, boxsize_local: float, n: int,
+                                    kernels=((0, 0, 0), (1, 1, 0), (1, 2, 0), (1, 3, 0)), nshell: int = 0):
+        """isolated_convolve_gpu_multi (src/PeakPatch.jl:280-298): one
+        zero-padded rfft of the noise, then per (kernel_fn_id, dim1, dim2)
+        the transfer multiply and irfft; returns one n^3 array per kernel."""
+        self._pk(pk)
+        x = self._f32(noise, "noise")
+        ks = np.ascontiguousarray(np.asarray(kernels, np.int32).reshape(-1, 3))
+        out = np.empty((len(ks), n, n, n), np.float32)
+        self._check(self.L.ppb_isolated_convolve(self.h, _p(x), x.shape[0], float(boxsize_local), n, _p(ks), len(ks),
+                                                 nshell, _p(out)))
+        return [out[i] for i in range(len(ks))]
+
+    def isolated_convolve_gpu(self, noise: np.ndarray, pk, boxsize_local: float, n: int, kernel_fn_id: int = 0,
+                              dim1: int = 0, dim2: int = 0, nshell: int = 0) -> np.ndarray:
+        """isolated_convolve_gpu (src/PeakPatch.jl:255-278)."""
+        return self.isolated_convolve_gpu_multi(noise, pk, boxsize_local, n, ((kernel_fn_id, dim1, dim2),),
+                                                nshell)[0]
+
+    def interpolate_to_tile_gpu(self, coarse: np.ndarray, it: int, jt: int, kt: int, nsub: int, nmesh: int, N: int,
+                                M: int) -> np.ndarray:
+        """interpolate_to_tile_gpu (src/PeakPatch.jl:329-339)."""
+        c = self._f32(coarse, "coarse")
+        if c.shape[0] != M:
+            raise ValueError("coarse must be M^3")
+        out = np.empty((nmesh, nmesh, nmesh), np.float32)
+        self._check(self.L.ppb_interpolate_to_tile(self.h, _p(c), it, jt, kt, nsub, nmesh, N, M, _p(out)))
+        return out
+
+    def compute_2lpt_gpu(self, delta_tile: np.ndarray, nmesh: int, boxsize_local: float):
+        """compute_2lpt_gpu (src/PeakPatch.jl:300-316): [psi2_x, psi2_y, psi2_z]."""
+        d = self._f32(delta_tile, "delta_tile")
+        out = np.empty((3, nmesh, nmesh, nmesh), np.float32)
+        self._check(self.L.ppb_compute_2lpt(self.h, _p(d), nmesh, float(boxsize_local), _p(out)))
+        return [out[0], out[1], out[2]]
+
+    def compute_laplacian_gpu(self, delta_tile: np.ndarray, nmesh: int, boxsize_local: float) -> np.ndarray:
+        """compute_laplacian_gpu (src/PeakPatch.jl:318-327)."""
+        d = self._f32(delta_tile, "delta_tile")
+        out = np.empty((nmesh, nmesh, nmesh), np.float32)
+        self._check(self.L.ppb_compute_laplacian(self.h, _p(d), nmesh, float(boxsize_local), _p(out)))
+        return out
+
+    def coarse_fields(self, coarse_noise: np.ndarray, pk, boxsize_full: float, ilpt: int = 2,
+                      ioutshear: int = 1) -> dict:
+        """The coarse phase of run_multitile_split (src/MultiResolution.jl:
+        617-667): delta, psi (3, M, M, M), psi2 (ilpt >= 2), lapd
+        (ioutshear >= 1)."""
+        self._pk(pk)
+        c = self._f32(coarse_noise, "coarse_noise")
+        M = c.shape[0]
+        d = np.empty((M, M, M), np.float32)
+        psi = np.empty((3, M, M, M), np.float32)
+        psi2 = np.empty((3, M, M, M), np.float32) if ilpt >= 2 else None
+        lap = np.empty((M, M, M), np.float32) if ioutshear >= 1 else None
+        self._check(self.L.ppb_coarse_fields(self.h, _p(c), M, float(boxsize_full), ilpt, ioutshear, _p(d), _p(psi),
+                                             _p(psi2), _p(lap)))
+        return dict(delta=d, psi=psi, psi2=psi2, lapd=lap)
 
 
 _default_ctx: Optional[Context] = None
