@@ -316,8 +316,10 @@ int32_t ppb_coarse_fields(ppb_ctx* ctx, const float* coarse_noise, int32_t M, do
     const int64_t N = (int64_t)M * M * M, Mk = (int64_t)(M / 2 + 1) * M * M;
     TileRes& tr = periodic_setup(ctx, coarse_noise, M);
     const double post = 1.0 / ((double)M * (double)M * (double)M);
-    // outputs: delta, psi (3), psi2 (3), lapd
-    sl.mr_aux.ensure(8 * N * 4);
+    // outputs: delta, psi (3), psi2 (3), lapd, each starting on a 16-byte
+    // boundary (cuFFT's real output must be aligned to its complex type)
+    const int64_t fs = (N + 3) & ~(int64_t)3;
+    sl.mr_aux.ensure(8 * fs * 4);
     float* o = sl.mr_aux.as<float>();
     auto c2r_into = [&](int q, float* dst) {
       PPB_CUFFT(cufftExecC2R(tr.c2r1, tr.kw.as<cufftComplex>() + q * Mk, dst));
@@ -328,8 +330,8 @@ int32_t ppb_coarse_fields(ppb_ctx* ctx, const float* coarse_noise, int32_t M, do
       const int g = ioutshear >= 1 ? 5 : 4;
       launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, kind, a, b, g,
                     post);
-      for (int q = 0; q < 4; q++) c2r_into(q, o + q * N);
-      if (g == 5) c2r_into(4, o + 7 * N);
+      for (int q = 0; q < 4; q++) c2r_into(q, o + q * fs);
+      if (g == 5) c2r_into(4, o + 7 * fs);
     }
     if (ilpt >= 2) {  // the 2LPT source and displacements (:635-659)
       const int pk6[6] = {3, 3, 3, 3, 3, 3}, pa[6] = {1, 2, 3, 1, 1, 2}, pb[6] = {1, 2, 3, 2, 3, 3};
@@ -343,12 +345,14 @@ int32_t ppb_coarse_fields(ppb_ctx* ctx, const float* coarse_noise, int32_t M, do
       const int k2[3] = {2, 2, 2}, da[3] = {1, 2, 3}, db[3] = {0, 0, 0};
       launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, k2, da, db, 3,
                     post);
-      for (int q = 0; q < 3; q++) c2r_into(q, o + (4 + q) * N);
+      for (int q = 0; q < 3; q++) c2r_into(q, o + (4 + q) * fs);
     }
     if (delta) copy_out(delta, o, N * 4, s);
-    if (psi) copy_out(psi, o + N, 3 * N * 4, s);
-    if (psi2 && ilpt >= 2) copy_out(psi2, o + 4 * N, 3 * N * 4, s);
-    if (lapd && ioutshear >= 1) copy_out(lapd, o + 7 * N, N * 4, s);
+    for (int q = 0; q < 3; q++) {
+      if (psi) copy_out(psi + q * N, o + (1 + q) * fs, N * 4, s);
+      if (psi2 && ilpt >= 2) copy_out(psi2 + q * N, o + (4 + q) * fs, N * 4, s);
+    }
+    if (lapd && ioutshear >= 1) copy_out(lapd, o + 7 * fs, N * 4, s);
     PPB_CUDA(cudaStreamSynchronize(s));
   });
 }
