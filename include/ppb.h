@@ -286,6 +286,28 @@ int32_t ppb_compute_laplacian(ppb_ctx* ctx, const float* delta_tile, int32_t n, 
 int32_t ppb_coarse_fields(ppb_ctx* ctx, const float* coarse_noise, int32_t M, double boxsize_full, int32_t ilpt,
                           int32_t ioutshear, float* delta, float* psi, float* psi2, float* lapd);
 
+/* run_multitile_split(cfg; ntile, seed, coarse_factor, coarse_grid,
+ * use_gpu=true) (src/MultiResolution.jl:523-1236): N = nsub ntile + 2 nbuff
+ * (nsub = n - 2 nbuff, alatt = boxsize / n); coarse grid M as
+ * ppb_split_coarse_grid; coarse noise and coarse delta / psi on M^3; per tile
+ * the split fields (ppb_extended_residual -> ppb_isolated_convolve with
+ * kernels delta, psi_x, psi_y, psi_z -> plus ppb_interpolate_to_tile of the
+ * coarse fields; ppb_compute_2lpt and ppb_compute_laplacian of the tile's
+ * delta), then the filter bank, peaks, shells and records on the tile's own
+ * n^3 grid as run_tile does, with the tile centre's position and (ievol = 1)
+ * the fcrit of its redshift; tiles beyond chi(z_max) dropped.  tiles as
+ * ppb_run_multitile.  Records in tile order (no merge), output as
+ * ppb_run_tile.  n <= 640. */
+int32_t ppb_run_multitile_split(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, int32_t nfilt,
+                                int32_t ntile, int32_t coarse_factor, int32_t coarse_grid, const int32_t* tiles,
+                                int32_t ntiles, ppb_halo_buf* out);
+
+/* The coarse grid M of run_multitile_split (src/MultiResolution.jl:592-612):
+ * coarse_grid when > 0, else ntile coarse_factor when > 0, else the divisor m
+ * of N in [2, N/2] whose block N/m is closest to n/3 (the smallest such m).
+ * Returns M (0 when no divisor exists) or PPB_ERR_INVALID. */
+int32_t ppb_split_coarse_grid(int32_t n, int32_t nbuff, int32_t ntile, int32_t coarse_factor, int32_t coarse_grid);
+
 /* ---- memory helpers ----------------------------------------------------- */
 /* Page-locked host memory (fast, asynchronous copies of records) and device
  * memory on the context's GPU, for callers that have no CUDA runtime of

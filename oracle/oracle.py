@@ -818,3 +818,113 @@ def compare_fields_split(pk_k, pk_p, N, boxsize, seed, ntile, coarse_factor, nbu
                 out.append(((it, jt, kt), _correlation(ref_d, d), _rms_frac(ref_d, d), _correlation(ref_p, p),
                             _rms_frac(ref_p, p)))
     return out
+
+
+def split_coarse_grid(N, nmesh, ntile, coarse_factor=0, coarse_grid=0) -> int:
+    """The coarse grid M of run_multitile_split (src/MultiResolution.jl:592-612)."""
+    if coarse_grid > 0:
+        return coarse_grid
+    if coarse_factor > 0:
+        return ntile * coarse_factor
+    target, best, best_dist = nmesh // 3, 0, N
+    for m in range(2, N // 2 + 1):
+        if N % m == 0 and abs(N // m - target) < best_dist:
+            best, best_dist = m, abs(N // m - target)
+    return best
+
+
+def run_multitile_split(cfg: Config, seed: int, pk_k, pk_p, filters, T: Table, ntile: int, coarse_factor=0,
+                        coarse_grid=0, tiles=None):
+    """run_multitile_split (src/MultiResolution.jl:523-1236): coarse delta and
+    psi on M^3, per tile the split fields (isolated convolution of the
+    residual + tricubic coarse field, tile 2LPT and Laplacian), the filter
+    bank and peaks on the tile's grid with the tile centre's position (and
+    fcrit of its redshift on the lightcone), shells and records; records in
+    tile order.  Returns (records, total peaks)."""
+    Om = cfg.Omx + cfg.OmB
+    filters = sorted(filters, key=lambda f: -f[2])
+    nm, nbuff = cfg.n, cfg.nbuff
+    nsub = nm - 2 * nbuff
+    N = nsub * ntile + 2 * nbuff
+    alatt = cfg.boxsize / nm
+    box_full, box_local, dcore = N * alatt, nm * alatt, nsub * alatt
+    M = split_coarse_grid(N, nm, ntile, coarse_factor, coarse_grid)
+    assert M > 0 and N % M == 0
+    fcrit_val = fsc_of_z(Om, cfg.OmB, cfg.Omvac, cfg.h, cfg.z_out)
+    nhunt = min(nbuff - 1, int(np.floor(filters[0][2] * 1.75 / alatt)))
+    shells = precompute_shells(nhunt)
+    cn = mr_coarse_noise(N, M, seed)
+    ck = rfft3(cn)
+    dc = irfft3(periodic_convolve(ck, pk_k, pk_p, M, box_full, 0), M)
+    pc = [irfft3(periodic_convolve(ck, pk_k, pk_p, M, box_full, 1, a), M) for a in (1, 2, 3)]
+    if tiles is None:
+        tiles = [(it, jt, kt) for kt in range(1, ntile + 1) for jt in range(1, ntile + 1)
+                 for it in range(1, ntile + 1)]
+    obs = (cfg.cenx, cfg.ceny, cfg.cenz)
+    if cfg.ievol == 1:   # drop tiles beyond chi(z_max) (:680-692)
+        chi_max = chi(Om, cfg.Omvac, cfg.h, cfg.z_max)
+        keep = []
+        for t in tiles:
+            c = tile_center(*t, ntile, dcore)
+            d = [max(abs(c[q] - obs[q]) - dcore / 2.0, 0.0) for q in range(3)]
+            if np.sqrt(d[0] ** 2 + d[1] ** 2 + d[2] ** 2) <= chi_max:
+                keep.append(t)
+        tiles = keep
+    nf = 33 if cfg.ioutshear >= 1 else 11
+    recs, npk_tot = [], 0
+    L = lib()
+    for t in tiles:
+        it, jt, kt = t
+        c = tile_center(*t, ntile, dcore)
+        fc_t = np.float32(fcrit_val)
+        if cfg.ievol == 1:   # fcrit at the tile centre's redshift (:864-871)
+            zt = chi_to_z(Om, cfg.Omvac, cfg.h, cfg.z_max + 1.0,
+                          np.array([np.sqrt(sum((c[q] - obs[q]) ** 2 for q in range(3)))]))[0]
+            fc_t = np.float32(fsc_of_z(Om, cfg.OmB, cfg.Omvac, cfg.h, zt))
+        res = mr_residual(cn, M, it, jt, kt, nsub, nm, N, seed, 0)
+        d = isolated_convolve(res, pk_k, pk_p, box_local, nm, 0) + mr_tricubic(dc, M, it, jt, kt, nsub, nm, N)
+        psi = [isolated_convolve(res, pk_k, pk_p, box_local, nm, 1, a) + mr_tricubic(pc[a - 1], M, it, jt, kt, nsub,
+                                                                                      nm, N) for a in (1, 2, 3)]
+        psi2, lap = tile_2lpt_laplacian(d, nm, box_local, cfg.ilpt, cfg.ioutshear >= 1)
+        dk = rfft3(d)
+        mask = np.zeros((nm, nm, nm), np.int8)
+        plist, pRf, pFc, pd2 = [], [], [], []
+        for (_, _, Rf) in filters:
+            ds = smooth_field(dk, nm, box_local, Rf, cfg.wsmooth)
+            ls = smooth_field(dk, nm, box_local, Rf, 3) if cfg.ioutshear >= 1 else None
+            pk = find_peaks(ds, mask, c[0], c[1], c[2], alatt, nbuff, fc_t)
+            lin = pk["ipp"] - 1
+            plist.append(pk)
+            pRf.append(np.full(len(lin), Rf))
+            pFc.append(ds.reshape(-1)[lin])
+            pd2.append(ls.reshape(-1)[lin] if ls is not None else np.zeros(len(lin), np.float32))
+        peaks = {k: np.concatenate([p[k] for p in plist]) for k in plist[0]}
+        pRf = np.concatenate(pRf)
+        pFc = np.concatenate(pFc).astype(np.float32)
+        pd2 = np.concatenate(pd2).astype(np.float32)
+        npk = len(peaks["ipp"])
+        npk_tot += npk
+        if npk == 0:
+            continue
+        fields = dict(delta=d, etax=psi[0], etay=psi[1], etaz=psi[2],
+                      eta2x=None if psi2 is None else psi2[0], eta2y=None if psi2 is None else psi2[1],
+                      eta2z=None if psi2 is None else psi2[2], lapd=lap)
+        ir2min = np.minimum(np.floor((1.75 * pRf / alatt) ** 2), np.floor((40.0 / alatt - 1) ** 2)).astype(np.int64)
+        if cfg.ievol == 1:
+            dx, dy, dz = peaks["x"] - obs[0], peaks["y"] - obs[1], peaks["z"] - obs[2]
+            ZZon = 1.0 + chi_to_z(Om, cfg.Omvac, cfg.h, cfg.z_max + 1.0, np.sqrt(dx * dx + dy * dy + dz * dz))
+            fc_pp = np.array([fsc_of_z(Om, cfg.OmB, cfg.Omvac, cfg.h, z - 1.0) for z in ZZon])
+        else:
+            ZZon = np.full(npk, 1.0 + cfg.z_out)
+            fc_pp = np.full(npk, fcrit_val)
+        r = analyse_peaks(fields, peaks["ipp"], pRf, ir2min, ZZon, fc_pp, alatt, shells, T, nbuff=nbuff,
+                          rmax2rs=cfg.rmax2rs)
+        rec = np.empty((npk, nf), dtype=np.float32)
+        zz = np.empty(npk)
+        nh = L.ora_pack_records(Om, cfg.OmB, cfg.Omvac, cfg.h, npk, _p(peaks["x"]), _p(peaks["y"]),
+                                _p(peaks["z"]), _p(np.ascontiguousarray(pRf)), _p(pFc), _p(pd2), _p(r),
+                                alatt, cfg.ievol, cfg.z_out, cfg.z_max, cfg.cenx, cfg.ceny, cfg.cenz,
+                                cfg.ioutshear, cfg.ilpt, _p(rec), _p(zz))
+        recs.append(rec[:nh])
+    out = np.concatenate(recs) if recs else np.empty((0, nf), np.float32)
+    return out, npk_tot

@@ -59,7 +59,8 @@ void Slot::release_buffers() {
   tiles.clear();
   tile_lru.clear();
   for (DevBuf* b : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
-                    &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &mr_in, &mr_out, &mr_aux})
+                    &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &mr_in, &mr_out, &mr_aux,
+                    &mr_rec})
     b->release();
   tune_save.release();
   iso.reset();
@@ -75,7 +76,7 @@ size_t Slot::shell_bytes() const {
   size_t b = 0;
   for (const DevBuf* d : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool,
                           &okey, &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &mr_in,
-                          &mr_out, &mr_aux})
+                          &mr_out, &mr_aux, &mr_rec})
     b += d->bytes;
   if (iso) b += iso->bytes();
   return b;
@@ -771,6 +772,37 @@ int32_t ppb_run_multitile(ppb_ctx* ctx, const ppb_tile_params* p, const double* 
   }
   return PPB_OK;
   PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_run_multitile_split(ppb_ctx* ctx, const ppb_tile_params* p, const double* Rf, int32_t nfilt,
+                                int32_t ntile, int32_t coarse_factor, int32_t coarse_grid, const int32_t* tiles,
+                                int32_t ntiles, ppb_halo_buf* out) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  PPB_REQUIRE(out != nullptr, "output buffer is null");
+  PPB_REQUIRE(ntiles >= 0 && (ntiles == 0 || tiles != nullptr), "tiles must hold ntiles triples");
+  std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
+  TileOut o;
+  run_multitile_split_core(ctx, ctx->sync, p, Rf, nfilt, ntile, coarse_factor, coarse_grid, tiles, ntiles, &o);
+  out->nfields = o.nfields;
+  out->count = o.count;
+  out->npeaks = o.npeaks;
+  out->RTHLmax = o.RTHLmax;
+  if (o.count > out->capacity) return PPB_ERR_CAPACITY;
+  if (o.count > 0) {
+    PPB_REQUIRE(out->records != nullptr, "records buffer is null");
+    copy_out(out->records, o.d_records, (size_t)o.count * o.nfields * 4, ctx->sync.stream);
+  }
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_split_coarse_grid(int32_t n, int32_t nbuff, int32_t ntile, int32_t coarse_factor, int32_t coarse_grid) {
+  const int64_t nsub = (int64_t)n - 2 * nbuff;
+  if (n < 1 || nbuff < 0 || nsub < 1 || ntile < 1) return PPB_ERR_INVALID;
+  return split_coarse_grid(nsub * ntile + 2 * nbuff, n, ntile, coarse_factor, coarse_grid);
 }
 
 int32_t ppb_merge_catalog(ppb_ctx* ctx, const float* records, int64_t n, int32_t nfields, float* out,

@@ -259,8 +259,10 @@ __device__ __forceinline__ void catmull_rom(float t, float* w) {
   w[3] = __fsub_rn(__fmul_rn(0.5f, t3), __fmul_rn(0.5f, t2));
 }
 
-__global__ void tricubic_kernel(const float* __restrict__ coarse, float* __restrict__ out, int M, int block,
-                                int64_t N, int64_t i0, int64_t j0, int64_t k0, int n, int64_t ostride) {
+// out = val, or base + val (the combined field delta_self .+ delta_long of
+// :779-795; base may be out itself)
+__global__ void tricubic_kernel(const float* __restrict__ coarse, float* out, const float* base, int M, int block,
+                                int64_t N, int64_t i0, int64_t j0, int64_t k0, int n) {
   const int li = blockIdx.x * blockDim.x + threadIdx.x;
   const int lj = blockIdx.y, lk = blockIdx.z;
   if (li >= n) return;
@@ -289,15 +291,8 @@ __global__ void tricubic_kernel(const float* __restrict__ coarse, float* __restr
       }
     }
   }
-  out[li + ostride * (lj + (int64_t)n * lk)] = val;
-}
-
-// dst = a + b (Float32), n^3 dense; the combined tile field of
-// run_multitile_split (:779-795)
-__global__ void add_kernel(float* __restrict__ dst, const float* __restrict__ a, const float* __restrict__ b,
-                           int64_t N) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
-    dst[i] = __fadd_rn(a[i], b[i]);
+  const int64_t o = li + (int64_t)n * (lj + (int64_t)n * lk);
+  out[o] = base ? __fadd_rn(base[o], val) : val;
 }
 
 }  // namespace
@@ -365,16 +360,10 @@ void launch_src2_trace(Launch L, const float* delta, const float* phi, float* ou
 }
 
 void launch_tricubic(Launch L, const float* coarse, float* out, int M, int64_t N, int64_t i0, int64_t j0, int64_t k0,
-                     int n) {
+                     int n, const float* base) {
   const int block = (int)(N / M);
   dim3 grid((unsigned)((n + 127) / 128), (unsigned)n, (unsigned)n);
-  tricubic_kernel<<<grid, 128, 0, L.s>>>(coarse, out, M, block, N, i0, j0, k0, n, n);
-  PPB_LAUNCHED(*L.count);
-}
-
-void launch_add(Launch L, float* dst, const float* a, const float* b, int64_t N) {
-  const int64_t blocks = std::min<int64_t>((N + 255) / 256, 148 * 16);
-  add_kernel<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, L.s>>>(dst, a, b, N);
+  tricubic_kernel<<<grid, 128, 0, L.s>>>(coarse, out, base, M, block, N, i0, j0, k0, n);
   PPB_LAUNCHED(*L.count);
 }
 

@@ -10,6 +10,7 @@
 // size, the periodic kernels use the slot's per-size tile buffers).
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "ppb_ctx.h"
 
@@ -59,6 +60,129 @@ void IsoRes::setup(int nn, int nb, cudaStream_t s) {
   PPB_CUFFT(cufftSetStream(c2r, s));
   work.ensure((size_t)nb * modes * 8);
   batch = (int)(work.bytes / ((size_t)modes * 8));
+}
+
+
+// ---------------------------------------------------------------------------
+// device-level stages (shared by the entry points below and the split driver)
+// ---------------------------------------------------------------------------
+void mr_isolated_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int n_input, double boxsize_local, int n,
+                        const int32_t* kernels, int nk, int nshell, float* const* outs) {
+  cudaStream_t s = sl.stream;
+  Launch L{s, &sl.launches};
+  const int n2 = 2 * n_input, nh2 = n2 / 2 + 1;
+  const int64_t modes = (int64_t)nh2 * n2 * n2, px = 2 * (int64_t)nh2;
+  // kernels per transfer pass: all of them (up to 4) unless memory is short
+  int batch = std::min(nk, 4);
+  if (!sl.iso) sl.iso.reset(new IsoRes());
+  IsoRes& iso = *sl.iso;
+  if (iso.n2 != n2 || iso.batch < batch) {
+    size_t fr = 0, tot = 0;
+    PPB_CUDA(cudaMemGetInfo(&fr, &tot));
+    const size_t have = fr + iso.work.bytes + iso.spec.bytes;
+    while (batch > 1 && (size_t)(batch + 2) * modes * 8 > have) batch--;
+  }
+  iso.setup(n2, batch, s);
+  batch = std::min(iso.batch, std::min(nk, kMaxKSpecs));
+  launch_pad(L, d_noise, iso.spec.as<float>(), n_input, n2, px);
+  PPB_CUFFT(cufftExecR2C(iso.r2c, iso.spec.as<float>(), iso.spec.as<cufftComplex>()));
+  sl.launches++;
+  // dx = boxsize_local / n; the padded box is n2 * dx (src/MultiResolution.jl:249-259)
+  const double box = (double)n2 * (boxsize_local / (double)n);
+  const double post = 1.0 / ((double)n2 * (double)n2 * (double)n2);
+  for (int b0 = 0; b0 < nk; b0 += batch) {
+    const int g = std::min(batch, nk - b0);
+    int kind[kMaxKSpecs], d1[kMaxKSpecs], d2[kMaxKSpecs];
+    for (int q = 0; q < g; q++) {
+      kind[q] = kernels[3 * (b0 + q)];
+      d1[q] = kernels[3 * (b0 + q) + 1];
+      d2[q] = kernels[3 * (b0 + q) + 2];
+    }
+    launch_kspace(L, true, iso.spec.as<float2>(), iso.work.as<float2>(), modes, n2, box, ctx->sh.pk_lk.as<double>(),
+                  ctx->sh.pk_lp.as<double>(), ctx->sh.pk_n, kind, d1, d2, g, post);
+    for (int q = 0; q < g; q++) {
+      float2* w = iso.work.as<float2>() + q * modes;
+      PPB_CUFFT(cufftExecC2R(iso.c2r, reinterpret_cast<cufftComplex*>(w), reinterpret_cast<float*>(w)));
+      sl.launches++;
+      launch_extract(L, outs[b0 + q], reinterpret_cast<const float*>(w), (int64_t)nshell * (1 + px + px * n2), px,
+                     px * n2, n);
+    }
+  }
+}
+
+void mr_tile_2lpt_lap(ppb_ctx* ctx, Slot& sl, TileRes& T, int n, double box, float* psi2, float* lapd) {
+  (void)ctx;
+  Launch L{sl.stream, &sl.launches};
+  const int64_t N = (int64_t)n * n * n, Mk = (int64_t)(n / 2 + 1) * n * n;
+  const double post = 1.0 / ((double)n * (double)n * (double)n);
+  auto forward = [&](float* src) {
+    PPB_CUFFT(cufftExecR2C(T.r2c, src, T.dk.as<cufftComplex>()));
+    sl.launches++;
+  };
+  forward(T.delta.as<float>());
+  if (psi2) {
+    // phi_11, phi_22, phi_33, phi_12, phi_13, phi_23 (:812-821)
+    const int pk6[6] = {3, 3, 3, 3, 3, 3}, pa[6] = {1, 2, 3, 1, 1, 2}, pb[6] = {1, 2, 3, 2, 3, 3};
+    launch_kspace(L, false, T.dk.as<float2>(), T.kw.as<float2>(), Mk, n, box, nullptr, nullptr, 0, pk6, pa, pb, 6,
+                  post);
+    PPB_CUFFT(cufftExecC2R(T.c2r6, T.kw.as<cufftComplex>(), T.rw.as<float>()));
+    sl.launches++;
+    launch_src2_trace(L, T.delta.as<float>(), T.rw.as<float>(), T.rw.as<float>(), n, n, (int64_t)n * n, N);
+    forward(T.rw.as<float>());
+    const int k2[3] = {2, 2, 2}, da[3] = {1, 2, 3}, db[3] = {0, 0, 0};
+    launch_kspace(L, false, T.dk.as<float2>(), T.kw.as<float2>(), Mk, n, box, nullptr, nullptr, 0, k2, da, db, 3,
+                  post);
+    PPB_CUFFT(cufftExecC2R(T.c2r3, T.kw.as<cufftComplex>(), psi2));
+    sl.launches++;
+    forward(T.delta.as<float>());   // T.dk back to rfft(delta)
+  }
+  if (lapd) {
+    const int k4[1] = {4}, z[1] = {0};
+    launch_kspace(L, false, T.dk.as<float2>(), T.kw.as<float2>(), Mk, n, box, nullptr, nullptr, 0, k4, z, z, 1, post);
+    PPB_CUFFT(cufftExecC2R(T.c2r1, T.kw.as<cufftComplex>(), lapd));
+    sl.launches++;
+  }
+}
+
+void mr_coarse_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int M, double boxsize_full, int ilpt,
+                      int ioutshear, float* o, int64_t fs) {
+  const double* lk = ctx->sh.pk_lk.as<double>();
+  const double* lp = ctx->sh.pk_lp.as<double>();
+  const int np = ctx->sh.pk_n;
+  Launch L{sl.stream, &sl.launches};
+  const int64_t N = (int64_t)M * M * M, Mk = (int64_t)(M / 2 + 1) * M * M;
+  TileRes& tr = sl.tile_for(M);
+  tr.setup(M, sl.stream);
+  PPB_CUDA(cudaMemcpyAsync(tr.delta.p, d_noise, N * 4, cudaMemcpyDeviceToDevice, sl.stream));
+  PPB_CUFFT(cufftExecR2C(tr.r2c, tr.delta.as<float>(), tr.dk.as<cufftComplex>()));
+  sl.launches++;
+  const double post = 1.0 / ((double)M * (double)M * (double)M);
+  auto c2r_into = [&](int q, float* dst) {
+    PPB_CUFFT(cufftExecC2R(tr.c2r1, tr.kw.as<cufftComplex>() + q * Mk, dst));
+    sl.launches++;
+  };
+  {  // delta and psi_d (:621-632), lapd (:662-667)
+    int kind[5] = {0, 1, 1, 1, 4}, a[5] = {0, 1, 2, 3, 0}, b[5] = {0, 0, 0, 0, 0};
+    const int g = ioutshear >= 1 ? 5 : 4;
+    launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, kind, a, b, g,
+                  post);
+    for (int q = 0; q < 4; q++) c2r_into(q, o + q * fs);
+    if (g == 5) c2r_into(4, o + 7 * fs);
+  }
+  if (ilpt >= 2) {  // the 2LPT source and displacements (:635-659)
+    const int pk6[6] = {3, 3, 3, 3, 3, 3}, pa[6] = {1, 2, 3, 1, 1, 2}, pb[6] = {1, 2, 3, 2, 3, 3};
+    launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, pk6, pa, pb, 6,
+                  post);
+    PPB_CUFFT(cufftExecC2R(tr.c2r6, tr.kw.as<cufftComplex>(), tr.rw.as<float>()));
+    sl.launches++;
+    launch_src2_trace(L, o, tr.rw.as<float>(), tr.rw.as<float>(), M, M, (int64_t)M * M, N);
+    PPB_CUFFT(cufftExecR2C(tr.r2c, tr.rw.as<float>(), tr.dk.as<cufftComplex>()));
+    sl.launches++;
+    const int k2[3] = {2, 2, 2}, da[3] = {1, 2, 3}, db[3] = {0, 0, 0};
+    launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, k2, da, db, 3,
+                  post);
+    for (int q = 0; q < 3; q++) c2r_into(q, o + (4 + q) * fs);
+  }
 }
 
 }  // namespace ppb
@@ -119,16 +243,13 @@ void finish_out(float* dst, const float* dev, size_t bytes, cudaStream_t s) {
   if (dst != dev) PPB_CUDA(cudaMemcpyAsync(dst, dev, bytes, cudaMemcpyDeviceToHost, s));
 }
 
-// the periodic n^3 kernels of run_multitile_split's tile stage on the slot's
-// tile buffers: rfft of delta_tile into tr.dk (delta_tile copied to tr.delta)
+// the caller's field copied into the slot's tile buffers of size n
 TileRes& periodic_setup(ppb_ctx* ctx, const float* delta_tile, int n) {
   Slot& sl = ctx->sync;
   TileRes& tr = sl.tile_for(n);
   tr.setup(n, sl.stream);
   const int64_t N = (int64_t)n * n * n;
   PPB_CUDA(cudaMemcpyAsync(tr.delta.p, delta_tile, N * 4, cudaMemcpyDefault, sl.stream));
-  PPB_CUFFT(cufftExecR2C(tr.r2c, tr.delta.as<float>(), tr.dk.as<cufftComplex>()));
-  sl.launches++;
   return tr;
 }
 
@@ -199,48 +320,12 @@ int32_t ppb_isolated_convolve(ppb_ctx* ctx, const float* noise, int32_t n_input,
     PPB_REQUIRE(ctx->sh.pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
     Slot& sl = ctx->sync;
     cudaStream_t s = sl.stream;
-    Launch L{s, &sl.launches};
-    const int n2 = 2 * n_input, nh2 = n2 / 2 + 1;
-    const int64_t modes = (int64_t)nh2 * n2 * n2, px = 2 * (int64_t)nh2;
-    // kernels per transfer pass: all of them (up to 4) unless memory is short
-    int batch = std::min(nkern, 4);
-    if (!sl.iso) sl.iso.reset(new IsoRes());
-    IsoRes& iso = *sl.iso;
-    if (iso.n2 != n2 || iso.batch < batch) {
-      size_t fr = 0, tot = 0;
-      PPB_CUDA(cudaMemGetInfo(&fr, &tot));
-      const size_t have = fr + iso.work.bytes + iso.spec.bytes;
-      while (batch > 1 && (size_t)(batch + 2) * modes * 8 > have) batch--;
-    }
-    iso.setup(n2, batch, s);
-    batch = std::min(iso.batch, std::min(nkern, kMaxKSpecs));
     const int64_t Nt = (int64_t)n * n * n;
     const float* src = (const float*)stage_in(sl.mr_in, noise, (size_t)n_input * n_input * n_input * 4, s);
     float* dout = out_buffer(out, sl.mr_out, (size_t)nkern * Nt * 4);
-    launch_pad(L, src, iso.spec.as<float>(), n_input, n2, px);
-    PPB_CUFFT(cufftExecR2C(iso.r2c, iso.spec.as<float>(), iso.spec.as<cufftComplex>()));
-    sl.launches++;
-    // dx = boxsize_local / n; the padded box is n2 * dx (src/MultiResolution.jl:249-259)
-    const double box = (double)n2 * (boxsize_local / (double)n);
-    const double post = 1.0 / ((double)n2 * (double)n2 * (double)n2);
-    for (int b0 = 0; b0 < nkern; b0 += batch) {
-      const int g = std::min(batch, nkern - b0);
-      int kind[kMaxKSpecs], d1[kMaxKSpecs], d2[kMaxKSpecs];
-      for (int q = 0; q < g; q++) {
-        kind[q] = kernels[3 * (b0 + q)];
-        d1[q] = kernels[3 * (b0 + q) + 1];
-        d2[q] = kernels[3 * (b0 + q) + 2];
-      }
-      launch_kspace(L, true, iso.spec.as<float2>(), iso.work.as<float2>(), modes, n2, box, ctx->sh.pk_lk.as<double>(),
-                    ctx->sh.pk_lp.as<double>(), ctx->sh.pk_n, kind, d1, d2, g, post);
-      for (int q = 0; q < g; q++) {
-        float2* w = iso.work.as<float2>() + q * modes;
-        PPB_CUFFT(cufftExecC2R(iso.c2r, reinterpret_cast<cufftComplex*>(w), reinterpret_cast<float*>(w)));
-        sl.launches++;
-        launch_extract(L, dout + (b0 + q) * Nt, reinterpret_cast<const float*>(w),
-                       (int64_t)nshell * (1 + px + px * n2), px, px * n2, n);
-      }
-    }
+    std::vector<float*> outs(nkern);
+    for (int b = 0; b < nkern; b++) outs[b] = dout + b * Nt;
+    mr_isolated_device(ctx, sl, src, n_input, boxsize_local, n, kernels, nkern, nshell, outs.data());
     finish_out(out, dout, (size_t)nkern * Nt * 4, s);
     PPB_CUDA(cudaStreamSynchronize(s));
   });
@@ -252,28 +337,12 @@ int32_t ppb_compute_2lpt(ppb_ctx* ctx, const float* delta_tile, int32_t n, doubl
     PPB_REQUIRE(n >= 2 && n <= 1024, "n must be 2..1024");
     PPB_REQUIRE(boxsize_local > 0.0, "boxsize_local must be > 0");
     Slot& sl = ctx->sync;
-    cudaStream_t s = sl.stream;
-    Launch L{s, &sl.launches};
-    const int64_t N = (int64_t)n * n * n, Mk = (int64_t)(n / 2 + 1) * n * n;
+    const int64_t N = (int64_t)n * n * n;
     TileRes& tr = periodic_setup(ctx, delta_tile, n);
-    const double post = 1.0 / ((double)n * (double)n * (double)n);
-    // phi_11, phi_22, phi_33, phi_12, phi_13, phi_23 (:812-821)
-    const int pk6[6] = {3, 3, 3, 3, 3, 3}, pa[6] = {1, 2, 3, 1, 1, 2}, pb[6] = {1, 2, 3, 2, 3, 3};
-    launch_kspace(L, false, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, n, boxsize_local, nullptr, nullptr, 0, pk6, pa,
-                  pb, 6, post);
-    PPB_CUFFT(cufftExecC2R(tr.c2r6, tr.kw.as<cufftComplex>(), tr.rw.as<float>()));
-    sl.launches++;
-    launch_src2_trace(L, tr.delta.as<float>(), tr.rw.as<float>(), tr.rw.as<float>(), n, n, (int64_t)n * n, N);
-    PPB_CUFFT(cufftExecR2C(tr.r2c, tr.rw.as<float>(), tr.dk.as<cufftComplex>()));
-    sl.launches++;
-    const int k2[3] = {2, 2, 2}, da[3] = {1, 2, 3}, db[3] = {0, 0, 0};
-    launch_kspace(L, false, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, n, boxsize_local, nullptr, nullptr, 0, k2, da,
-                  db, 3, post);
     float* d = out_buffer(psi2, sl.mr_out, (size_t)3 * N * 4);
-    PPB_CUFFT(cufftExecC2R(tr.c2r3, tr.kw.as<cufftComplex>(), d));
-    sl.launches++;
-    finish_out(psi2, d, (size_t)3 * N * 4, s);
-    PPB_CUDA(cudaStreamSynchronize(s));
+    mr_tile_2lpt_lap(ctx, sl, tr, n, boxsize_local, d, nullptr);
+    finish_out(psi2, d, (size_t)3 * N * 4, sl.stream);
+    PPB_CUDA(cudaStreamSynchronize(sl.stream));
   });
 }
 
@@ -283,19 +352,12 @@ int32_t ppb_compute_laplacian(ppb_ctx* ctx, const float* delta_tile, int32_t n, 
     PPB_REQUIRE(n >= 2 && n <= 1024, "n must be 2..1024");
     PPB_REQUIRE(boxsize_local > 0.0, "boxsize_local must be > 0");
     Slot& sl = ctx->sync;
-    cudaStream_t s = sl.stream;
-    Launch L{s, &sl.launches};
-    const int64_t N = (int64_t)n * n * n, Mk = (int64_t)(n / 2 + 1) * n * n;
+    const int64_t N = (int64_t)n * n * n;
     TileRes& tr = periodic_setup(ctx, delta_tile, n);
-    const double post = 1.0 / ((double)n * (double)n * (double)n);
-    const int k4[1] = {4}, z[1] = {0};
-    launch_kspace(L, false, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, n, boxsize_local, nullptr, nullptr, 0, k4, z, z,
-                  1, post);
     float* d = out_buffer(lapd, sl.mr_out, (size_t)N * 4);
-    PPB_CUFFT(cufftExecC2R(tr.c2r1, tr.kw.as<cufftComplex>(), d));
-    sl.launches++;
-    finish_out(lapd, d, (size_t)N * 4, s);
-    PPB_CUDA(cudaStreamSynchronize(s));
+    mr_tile_2lpt_lap(ctx, sl, tr, n, boxsize_local, nullptr, d);
+    finish_out(lapd, d, (size_t)N * 4, sl.stream);
+    PPB_CUDA(cudaStreamSynchronize(sl.stream));
   });
 }
 
@@ -307,46 +369,16 @@ int32_t ppb_coarse_fields(ppb_ctx* ctx, const float* coarse_noise, int32_t M, do
     PPB_REQUIRE(boxsize_full > 0.0, "boxsize_full must be > 0");
     std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
     PPB_REQUIRE(ctx->sh.pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
-    const double* lk = ctx->sh.pk_lk.as<double>();
-    const double* lp = ctx->sh.pk_lp.as<double>();
-    const int np = ctx->sh.pk_n;
     Slot& sl = ctx->sync;
     cudaStream_t s = sl.stream;
-    Launch L{s, &sl.launches};
-    const int64_t N = (int64_t)M * M * M, Mk = (int64_t)(M / 2 + 1) * M * M;
-    TileRes& tr = periodic_setup(ctx, coarse_noise, M);
-    const double post = 1.0 / ((double)M * (double)M * (double)M);
+    const int64_t N = (int64_t)M * M * M;
+    const float* src = (const float*)stage_in(sl.mr_in, coarse_noise, (size_t)N * 4, s);
     // outputs: delta, psi (3), psi2 (3), lapd, each starting on a 16-byte
     // boundary (cuFFT's real output must be aligned to its complex type)
     const int64_t fs = (N + 3) & ~(int64_t)3;
     sl.mr_aux.ensure(8 * fs * 4);
     float* o = sl.mr_aux.as<float>();
-    auto c2r_into = [&](int q, float* dst) {
-      PPB_CUFFT(cufftExecC2R(tr.c2r1, tr.kw.as<cufftComplex>() + q * Mk, dst));
-      sl.launches++;
-    };
-    {  // delta and psi_d (:621-632), lapd (:662-667)
-      int kind[5] = {0, 1, 1, 1, 4}, a[5] = {0, 1, 2, 3, 0}, b[5] = {0, 0, 0, 0, 0};
-      const int g = ioutshear >= 1 ? 5 : 4;
-      launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, kind, a, b, g,
-                    post);
-      for (int q = 0; q < 4; q++) c2r_into(q, o + q * fs);
-      if (g == 5) c2r_into(4, o + 7 * fs);
-    }
-    if (ilpt >= 2) {  // the 2LPT source and displacements (:635-659)
-      const int pk6[6] = {3, 3, 3, 3, 3, 3}, pa[6] = {1, 2, 3, 1, 1, 2}, pb[6] = {1, 2, 3, 2, 3, 3};
-      launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, pk6, pa, pb, 6,
-                    post);
-      PPB_CUFFT(cufftExecC2R(tr.c2r6, tr.kw.as<cufftComplex>(), tr.rw.as<float>()));
-      sl.launches++;
-      launch_src2_trace(L, o, tr.rw.as<float>(), tr.rw.as<float>(), M, M, (int64_t)M * M, N);
-      PPB_CUFFT(cufftExecR2C(tr.r2c, tr.rw.as<float>(), tr.dk.as<cufftComplex>()));
-      sl.launches++;
-      const int k2[3] = {2, 2, 2}, da[3] = {1, 2, 3}, db[3] = {0, 0, 0};
-      launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, k2, da, db, 3,
-                    post);
-      for (int q = 0; q < 3; q++) c2r_into(q, o + (4 + q) * fs);
-    }
+    mr_coarse_device(ctx, sl, src, M, boxsize_full, ilpt, ioutshear, o, fs);
     if (delta) copy_out(delta, o, N * 4, s);
     for (int q = 0; q < 3; q++) {
       if (psi) copy_out(psi + q * N, o + (1 + q) * fs, N * 4, s);

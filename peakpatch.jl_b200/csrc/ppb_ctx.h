@@ -85,7 +85,7 @@ struct Slot {
   DevBuf okey, okey2, oidx, oidx2, otmp;            // spatial gather order
   DevBuf tcen, tcount, t_aos, t_lapd;               // multi-tile: centres, peaks per tile, tile fields
   std::unique_ptr<IsoRes> iso;                      // multi-resolution: isolated convolution
-  DevBuf mr_in, mr_out, mr_aux;                     // multi-resolution: staged inputs and outputs
+  DevBuf mr_in, mr_out, mr_aux, mr_rec;             // multi-resolution: staged inputs, outputs, records
   int gather_bps[2][2] = {{0, 0}, {0, 0}};          // gather blocks per SM by [comp][adaptive]
   double rows_per_peak[2] = {0.0, 0.0};             // pool rows per peak seen last, by adaptive
   double walk_per_peak = 0.0;                       // collapse-walk steps per peak seen last
@@ -205,6 +205,16 @@ void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const doubl
 // (it, jt, kt) triples, 1-based, or null for every tile of the ntile^3 grid
 void run_multitile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf, int nfilt, int ntile,
                         const int32_t* tiles, int ntiles, TileOut* o);
+// run_multitile_split (src/MultiResolution.jl:523-1236) on one slot: fields
+// by the multi-resolution split per tile, analysed on the tile's own grid;
+// records in tile order (o->d_records stays valid until the slot's next
+// split run)
+void run_multitile_split_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf, int nfilt,
+                              int ntile, int coarse_factor, int coarse_grid, const int32_t* tiles, int ntiles,
+                              TileOut* o);
+// the coarse grid M the split uses (coarse_grid, ntile coarse_factor, or the
+// automatic choice of src/MultiResolution.jl:592-612)
+int split_coarse_grid(int64_t N, int nmesh, int ntile, int coarse_factor, int coarse_grid);
 void check_params(const ppb_tile_params* p, const double* Rf, int nfilt);
 // the fields of run_tile's first phase, copied to the given buffers (host or
 // device, any may be null)
@@ -233,4 +243,16 @@ void graph_counts(const ppb_ctx* ctx, int64_t* out3);
 // accumulates the RK4 steps taken
 void make_table_device(Slot& sl, const GrowthTable& G, const ppb_table_params* p, const double* d_Frho, double* d_out,
                        unsigned long long* d_steps);
+// multi-resolution stages on device buffers (multires.cu).  The coarse phase
+// writes delta, psi (3), psi2 (3, ilpt >= 2) and lapd (ioutshear >= 1) of the
+// M^3 coarse noise to o, fields fs floats apart (fs a multiple of 4).
+void mr_coarse_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int M, double boxsize_full, int ilpt,
+                      int ioutshear, float* o, int64_t fs);
+// isolated convolution of the n_input^3 noise for nk (kind, d1, d2) kernels,
+// the n^3 region at nshell into outs[b]; the caller holds ctx->sh.mu shared
+void mr_isolated_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int n_input, double boxsize_local, int n,
+                        const int32_t* kernels, int nk, int nshell, float* const* outs);
+// tile-local 2LPT (psi2: 3 fields n^3 apart) and/or Laplacian of T.delta;
+// leaves T.dk = rfft(T.delta)
+void mr_tile_2lpt_lap(ppb_ctx* ctx, Slot& sl, TileRes& T, int n, double box, float* psi2, float* lapd);
 }  // namespace ppb

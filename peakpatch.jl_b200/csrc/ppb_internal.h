@@ -336,8 +336,8 @@ void launch_kspace(Launch L, bool transfer, const float2* in, float2* out, int64
                    int nspec, double post);
 void launch_src2_trace(Launch L, const float* delta, const float* phi, float* out, int n, int64_t px, int64_t pz,
                        int64_t pd);
+// out (n^3) = tricubic interpolation, plus base[i] when base is not null
 void launch_tricubic(Launch L, const float* coarse, float* out, int M, int64_t N, int64_t i0, int64_t j0, int64_t k0,
-                     int n);
-void launch_add(Launch L, float* dst, const float* a, const float* b, int64_t N);
+                     int n, const float* base = nullptr);
 
 }  // namespace ppb

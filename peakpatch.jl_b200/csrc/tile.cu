@@ -858,4 +858,194 @@ void run_multitile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const 
   o->device_ms = ms[0] + ms[1] + ms[2] + ms[3];
 }
 
+// the coarse grid of run_multitile_split (src/MultiResolution.jl:592-612):
+// coarse_grid, else ntile coarse_factor, else the divisor m of N (2 <= m <=
+// N/2) whose block N/m is closest to nmesh/3 (the first such m)
+int split_coarse_grid(int64_t N, int nmesh, int ntile, int coarse_factor, int coarse_grid) {
+  if (coarse_grid > 0) return coarse_grid;
+  if (coarse_factor > 0) return ntile * coarse_factor;
+  const int64_t target = nmesh / 3;
+  int64_t best = 0, best_dist = N;
+  for (int64_t m = 2; m <= N / 2; m++) {
+    if (N % m != 0) continue;
+    const int64_t dist = std::llabs(N / m - target);
+    if (dist < best_dist) {
+      best_dist = dist;
+      best = m;
+    }
+  }
+  return (int)best;
+}
+
+namespace {
+
+// dst (device, `used` bytes kept) grown to hold `more` bytes beyond used
+void grow_keep(DevBuf& dst, size_t used, size_t more, cudaStream_t s) {
+  if (used + more <= dst.bytes) return;
+  const size_t nb = std::max(used + more, 2 * dst.bytes);
+  void* np = nullptr;
+  PPB_CUDA(cudaMalloc(&np, nb));
+  if (used) PPB_CUDA(cudaMemcpyAsync(np, dst.p, used, cudaMemcpyDeviceToDevice, s));
+  PPB_CUDA(cudaStreamSynchronize(s));
+  dst.release();
+  dst.p = np;
+  dst.bytes = nb;
+}
+
+}  // namespace
+
+// run_multitile_split (src/MultiResolution.jl:523-1236) with use_gpu: the
+// coarse noise and coarse delta / psi on M^3 once, then per tile the fields
+// by the split (isolated convolution of the Hoffman-Ribak residual plus the
+// tricubic coarse field; tile-local 2LPT and Laplacian), the filter bank and
+// peak search on the tile's own nmesh^3 grid (fcrit of the tile centre on
+// the lightcone), the shell analysis and the records, in tile order.
+void run_multitile_split_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const double* Rf_in, int nfilt,
+                              int ntile, int coarse_factor, int coarse_grid, const int32_t* tiles_in, int ntiles_in,
+                              TileOut* o) {
+  check_params(p, Rf_in, nfilt);
+  PPB_REQUIRE(ctx->sh.pk_n >= 2, "P(k) table not set (ppb_set_pk_table)");
+  PPB_REQUIRE(ctx->sh.has_tab, "collapse table not set (ppb_set_collapse_table)");
+  PPB_REQUIRE(ntile >= 1 && ntile <= 64, "ntile must be in [1, 64]");
+  const int nm = p->n, nbuff = p->nbuff, nsub = nm - 2 * nbuff;
+  PPB_REQUIRE(nm <= 640, "nmesh must be <= 640 (isolated convolution box (2 nmesh)^3)");
+  const int64_t N = (int64_t)nsub * ntile + 2 * nbuff;
+  const int M = split_coarse_grid(N, nm, ntile, coarse_factor, coarse_grid);
+  PPB_REQUIRE(M >= 1 && N % M == 0, "N = nsub ntile + 2 nbuff must be divisible by the coarse grid M");
+  PPB_REQUIRE(N / M <= 1024 && M <= 1024 && N <= (1 << 20), "coarse grid out of range");
+  const double alatt = p->boxsize / nm, box_full = (double)N * alatt, box_local = nm * alatt, dcore = nsub * alatt;
+  const int64_t Nt = (int64_t)nm * nm * nm;
+  Run r;
+  setup_run(r, ctx, sl, p, Rf_in, nfilt, alatt);
+  // tiles: the given list, else every tile in (kt, jt, it) loop order
+  std::vector<std::array<int, 3>> tl;
+  if (tiles_in && ntiles_in > 0) {
+    for (int t = 0; t < ntiles_in; t++) {
+      const int it = tiles_in[3 * t], jt = tiles_in[3 * t + 1], kt = tiles_in[3 * t + 2];
+      PPB_REQUIRE(it >= 1 && it <= ntile && jt >= 1 && jt <= ntile && kt >= 1 && kt <= ntile,
+                  "tile index out of range");
+      tl.push_back({it, jt, kt});
+    }
+  } else {
+    for (int kt = 1; kt <= ntile; kt++)
+      for (int jt = 1; jt <= ntile; jt++)
+        for (int it = 1; it <= ntile; it++) tl.push_back({it, jt, kt});
+  }
+  const double cen = 0.5 * (ntile + 1);
+  auto centre = [&](const std::array<int, 3>& t, int d) { return (t[d] - cen) * dcore; };
+  const double obs[3] = {p->cenx, p->ceny, p->cenz};
+  std::vector<double> chis;
+  if (p->ievol == 1) {   // lightcone: drop tiles beyond chi(z_max) (:680-692)
+    const double chi_max = chi_of_z(r.Om, p->Omvac, p->h, p->z_max);
+    const double half = dcore / 2.0;
+    std::vector<std::array<int, 3>> keep;
+    for (const auto& t : tl) {
+      double d2 = 0.0;
+      for (int d = 0; d < 3; d++) {
+        const double e = std::max(std::fabs(centre(t, d) - obs[d]) - half, 0.0);
+        d2 += e * e;
+      }
+      if (std::sqrt(d2) <= chi_max) keep.push_back(t);
+    }
+    tl.swap(keep);
+    chis = ctx->chi_table(r.Om, p->Omvac, p->h, p->z_max + 1.0);
+  }
+  const int nt = (int)tl.size();
+  std::vector<double> tcen(3 * std::max(nt, 1), 0.0);
+  std::vector<float> fcrit_t(std::max(nt, 1), (float)r.fcrit_val);
+  for (int t = 0; t < nt; t++) {
+    for (int d = 0; d < 3; d++) tcen[3 * t + d] = centre(tl[t], d);
+    if (p->ievol == 1) {   // fcrit at the tile centre's redshift (:864-871)
+      double d2 = 0.0;
+      for (int d = 0; d < 3; d++) d2 += (tcen[3 * t + d] - obs[d]) * (tcen[3 * t + d] - obs[d]);
+      fcrit_t[t] = (float)fsc_of_z(*r.G, chi_to_z_host(chis, p->z_max + 1.0, std::sqrt(d2)));
+    }
+  }
+  sl.tcen.ensure(tcen.size() * 8);
+  PPB_CUDA(cudaMemcpyAsync(sl.tcen.p, tcen.data(), tcen.size() * 8, cudaMemcpyHostToDevice, r.s));
+  // phase 0 / 1a: coarse noise, coarse delta and psi (:596-632; the coarse
+  // 2LPT and Laplacian of :635-667 are never read afterwards)
+  const int64_t Mc = (int64_t)M * M * M, fs = (Mc + 3) & ~(int64_t)3;
+  sl.mr_in.ensure(Mc * 4);
+  sl.mr_aux.ensure(4 * fs * 4);
+  float* cnoise = sl.mr_in.as<float>();
+  float* cf = sl.mr_aux.as<float>();
+  cudaEvent_t* ev = sl.stage_ev;
+  PPB_CUDA(cudaEventRecord(ev[0], r.s));
+  launch_coarse_noise(r.L, cnoise, N, M, p->seed);
+  mr_coarse_device(ctx, sl, cnoise, M, box_full, 1, 0, cf, fs);
+  TileRes& T = sl.tile_for(nm);
+  T.setup(nm, r.s);
+  T.aos.ensure(Nt * 32);
+  if (T.cap == 0) T.ensure_peaks(std::max<int64_t>(1 << 16, std::min<int64_t>(Nt / 64, 1 << 22)));
+  sl.mr_out.ensure(Nt * 4);
+  float* resid = sl.mr_out.as<float>();
+  const int nf = p->ioutshear >= 1 ? 33 : 11;
+  const int32_t kern4[12] = {0, 0, 0, 1, 1, 0, 1, 2, 0, 1, 3, 0};
+  float* outs[4] = {T.delta.as<float>(), T.psi.as<float>(), T.psi.as<float>() + Nt, T.psi.as<float>() + 2 * Nt};
+  size_t used = 0;
+  int64_t nrec_tot = 0, npk_tot = 0;
+  float rmax_tot = 0.f;
+  float ms[4] = {0.f, 0.f, 0.f, 0.f};
+  ShellStats st{};
+  PPB_CUDA(cudaEventRecord(ev[1], r.s));
+  PPB_CUDA(cudaEventSynchronize(ev[1]));
+  PPB_CUDA(cudaEventElapsedTime(&ms[0], ev[0], ev[1]));
+  for (int t = 0; t < nt; t++) {
+    const int64_t i0 = (int64_t)(tl[t][0] - 1) * nsub - nbuff, j0 = (int64_t)(tl[t][1] - 1) * nsub - nbuff,
+                  k0 = (int64_t)(tl[t][2] - 1) * nsub - nbuff;
+    PPB_CUDA(cudaEventRecord(ev[0], r.s));
+    // fields (:728-847)
+    launch_residual(r.L, cnoise, resid, M, N, i0, j0, k0, nm, p->seed);
+    mr_isolated_device(ctx, sl, resid, nm, box_local, nm, kern4, 4, 0, outs);
+    launch_tricubic(r.L, cf, outs[0], M, N, i0, j0, k0, nm, outs[0]);
+    for (int c = 0; c < 3; c++) launch_tricubic(r.L, cf + (1 + c) * fs, outs[1 + c], M, N, i0, j0, k0, nm, outs[1 + c]);
+    mr_tile_2lpt_lap(ctx, sl, T, nm, box_local, p->ilpt >= 2 ? T.psi2.as<float>() : nullptr,
+                     r.want_lap ? T.lapd.as<float>() : nullptr);
+    launch_hermitise(r.L, T.dk.as<float2>(), nm, 1);
+    launch_pack(r.L, T.aos.as<float4>(),
+                FieldWindow{T.delta.as<float>(), T.psi.as<float>(), p->ilpt >= 2 ? T.psi2.as<float>() : nullptr, 0,
+                            nm, (int64_t)nm * nm, Nt},
+                nm);
+    PPB_CUDA(cudaEventRecord(ev[1], r.s));
+    // peaks on the tile's grid (:856-906), shells (:908-1021), records
+    const int64_t npk = peaks_phase(r, T, nm, box_local, {Win{0, fcrit_t[t]}}, nm);
+    PPB_CUDA(cudaEventRecord(ev[2], r.s));
+    prep_phase(r, T, npk, nm, 1, sl.tcen.as<double>() + 3 * t);
+    shells_phase(r, T, 0, npk, nm, T.aos.as<float4>(), r.want_lap ? T.lapd.as<float>() : nullptr, &st);
+    PPB_CUDA(cudaEventRecord(ev[3], r.s));
+    int64_t nrec = 0;
+    float rmax = 0.f;
+    records_phase(r, T, npk, &nrec, &rmax);
+    if (nrec > 0) {
+      const size_t bytes = (size_t)nrec * nf * 4;
+      grow_keep(sl.mr_rec, used, bytes, r.s);
+      PPB_CUDA(cudaMemcpyAsync((char*)sl.mr_rec.p + used, T.rec.p, bytes, cudaMemcpyDeviceToDevice, r.s));
+      used += bytes;
+    }
+    PPB_CUDA(cudaEventRecord(ev[4], r.s));
+    PPB_CUDA(cudaEventSynchronize(ev[4]));
+    float e[4];
+    for (int i = 0; i < 4; i++) PPB_CUDA(cudaEventElapsedTime(&e[i], ev[i], ev[i + 1]));
+    ms[0] += e[0];
+    ms[1] += e[1];
+    ms[2] += e[2];
+    ms[3] += e[3];
+    nrec_tot += nrec;
+    npk_tot += npk;
+    rmax_tot = std::max(rmax_tot, rmax);
+  }
+  check_shell_stats(st);
+  sl.last_shell = st;
+  o->nfields = nf;
+  o->count = nrec_tot;
+  o->npeaks = npk_tot;
+  o->RTHLmax = nrec_tot > 0 ? rmax_tot : 0.f;
+  o->d_records = sl.mr_rec.as<float>();
+  sl.last_visits = st.visits;
+  sl.last_npk = npk_tot;
+  std::memcpy(sl.stage_ms, ms, sizeof(ms));
+  o->device_ms = ms[0] + ms[1] + ms[2] + ms[3];
+}
+
 }  // namespace ppb

@@ -147,6 +147,7 @@ EXPORTED = (
     "ppb_analyse_peaks_lim", "ppb_set_option", "ppb_get_option", "ppb_tune_entries", "ppb_make_collapse_table",
     "ppb_last_table_stats", "ppb_downsample_noise", "ppb_extended_residual", "ppb_isolated_convolve",
     "ppb_interpolate_to_tile", "ppb_compute_2lpt", "ppb_compute_laplacian", "ppb_coarse_fields",
+    "ppb_run_multitile_split", "ppb_split_coarse_grid",
 )
 
 
@@ -209,6 +210,9 @@ def load_library():
     L.ppb_compute_2lpt.argtypes = [P, P, I32, D, P]
     L.ppb_compute_laplacian.argtypes = [P, P, I32, D, P]
     L.ppb_coarse_fields.argtypes = [P, P, I32, D, I32, I32, P, P, P, P]
+    L.ppb_run_multitile_split.argtypes = [P, ctypes.POINTER(_TileParams), P, I32, I32, I32, I32, P, I32,
+                                          ctypes.POINTER(_HaloBuf)]
+    L.ppb_split_coarse_grid.argtypes = [I32, I32, I32, I32, I32]
     for f in ("ppb_alloc_host", "ppb_alloc_device"):
         getattr(L, f).argtypes = [P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
     for f in ("ppb_free_host", "ppb_free_device"):
@@ -591,6 +595,33 @@ class Context:
             hb = _HaloBuf(records=rec.ctypes.data, capacity=cap)
             rc = self.L.ppb_run_multitile(self.h, ctypes.byref(p), _p(rf), len(rf), int(ntile),
                                           None if tl is None else _p(tl), nt, ctypes.byref(hb))
+            if rc == -7:
+                cap = int(hb.count) + 16
+                continue
+            self._check(rc)
+            self._last_count = int(hb.count)
+            return rec[:hb.count].copy(), float(hb.RTHLmax), int(hb.npeaks)
+        raise PPBError(-7, "record capacity")
+
+    def run_multitile_split_arrays(self, cfg: PipelineConfig, seed: int, Rf: Sequence[float], ntile: int,
+                                   coarse_factor: int = 0, coarse_grid: int = 0, tiles=None):
+        """run_multitile_split(cfg; ntile, seed, coarse_factor, coarse_grid)
+        with the tables set (src/MultiResolution.jl:523-1236).  tiles:
+        optional list of (it, jt, kt), 1-based.  Returns (records, RTHLmax,
+        npeaks), records in tile order."""
+        p = self._params(cfg, seed, False)
+        rf = np.ascontiguousarray(np.asarray(Rf, dtype=np.float64))
+        tl = None if tiles is None else np.ascontiguousarray(np.asarray(tiles, dtype=np.int32).reshape(-1, 3))
+        nt = 0 if tl is None else len(tl)
+        nf = 33 if cfg.ioutshear >= 1 else 11
+        ncore = (cfg.n - 2 * cfg.nbuff) ** 3 * (ntile ** 3 if tl is None else nt)
+        cap = max(1024, getattr(self, "_last_count", 0) * 2, ncore // 30)
+        for _ in range(2):
+            rec = np.empty((cap, nf), dtype=np.float32)
+            hb = _HaloBuf(records=rec.ctypes.data, capacity=cap)
+            rc = self.L.ppb_run_multitile_split(self.h, ctypes.byref(p), _p(rf), len(rf), int(ntile),
+                                                int(coarse_factor), int(coarse_grid), None if tl is None else _p(tl),
+                                                nt, ctypes.byref(hb))
             if rc == -7:
                 cap = int(hb.count) + 16
                 continue

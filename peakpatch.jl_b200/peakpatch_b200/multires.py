@@ -78,3 +78,83 @@ def compare_fields_split(ctx: Context, pk, N: int, boxsize: float, seed: int, nt
                                 corr_psi1=_correlation(ref_p, p), rms_psi1=_rms_frac(ref_p, p),
                                 std_global_delta=float(np.sqrt((ref_d ** 2).mean()))))
     return out
+
+
+def coarse_grid_size(n: int, nbuff: int, ntile: int, coarse_factor: int = 0, coarse_grid: int = 0) -> int:
+    """The coarse grid M run_multitile_split uses for tile size n (src/
+    MultiResolution.jl:592-612)."""
+    from . import load_library
+    m = load_library().ppb_split_coarse_grid(n, nbuff, ntile, coarse_factor, coarse_grid)
+    if m < 0:
+        raise ValueError("invalid tile geometry")
+    return m
+
+
+def run_multitile_split(cfg: PipelineConfig, ntile: int, seed: int = 42, verbose: bool = False,
+                        coarse_factor: int = 0, coarse_grid: int = 0, use_gpu: bool = True, devices=None,
+                        profile: bool = False, ctx: Context = None, Rf=None, pk=None, table=None):
+    """Drop-in for run_multitile_split(cfg; ntile, seed, verbose,
+    coarse_factor, coarse_grid, use_gpu, devices, profile)
+    (src/MultiResolution.jl:523-1236); returns the records array (11 or 33
+    Float32 fields per halo).
+
+    Every stage runs on the GPU whatever `use_gpu` says (this library has no
+    CPU path).  devices=[d0, d1, ...] splits the tiles round-robin over one
+    worker per device (tile i to worker (i mod n_workers)) and concatenates
+    the workers' records in worker order, as the reference does
+    (:1183-1213); otherwise one context (ctx, or a new one on device 0)
+    processes the tiles in order.  pk = (k, P), table (a CollapseTable) and
+    Rf (filter radii) are installed when given; otherwise a new context reads
+    them from cfg's pkfile, tabfile and filterfile, and a given ctx keeps the
+    tables it holds."""
+    import threading
+    import time
+    from . import read_filterbank, read_homeltab, read_pk_table
+
+    def setup(c: Context, fresh: bool):
+        if pk is not None:
+            c.set_pk_table(np.asarray(pk[0], np.float64), np.asarray(pk[1], np.float64))
+        elif fresh:
+            c.set_pk_table(*read_pk_table(cfg.pkfile))
+        if table is not None:
+            c.set_collapse_table(table)
+        elif fresh:
+            c.set_collapse_table(read_homeltab(cfg.tabfile))
+        return list(Rf) if Rf is not None else [f[2] for f in read_filterbank(cfg.filterfile)]
+
+    t0 = time.perf_counter()
+    tile_ids = [(it, jt, kt) for kt in range(1, ntile + 1) for jt in range(1, ntile + 1) for it in range(1, ntile + 1)]
+    if devices:
+        nw = len(devices)
+        parts = [None] * nw
+        errs = []
+
+        def work(w):
+            try:
+                mine = [t for i, t in enumerate(tile_ids) if i % nw == w]
+                if not mine:
+                    parts[w] = np.zeros((0, 33 if cfg.ioutshear >= 1 else 11), np.float32)
+                    return
+                with Context(int(devices[w])) as c:
+                    rf = setup(c, True)
+                    parts[w] = c.run_multitile_split_arrays(cfg, seed, rf, ntile, coarse_factor, coarse_grid,
+                                                            tiles=mine)[0]
+            except Exception as e:   # surfaced after join
+                errs.append(e)
+
+        th = [threading.Thread(target=work, args=(w,)) for w in range(nw)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        if errs:
+            raise errs[0]
+        rec = np.concatenate(parts, axis=0)
+    else:
+        c = ctx if ctx is not None else Context(0)
+        rf = setup(c, ctx is None)
+        rec = c.run_multitile_split_arrays(cfg, seed, rf, ntile, coarse_factor, coarse_grid)[0]
+    if verbose or profile:
+        print(f"run_multitile_split: {len(rec)} halos, ntile={ntile}, nmesh={cfg.n}, "
+              f"{time.perf_counter() - t0:.2f} s")
+    return rec

@@ -71,3 +71,43 @@ def test_tricubic_reproduces_constant_and_coarse_nodes(ora):
     c = rng.standard_normal((8, 8, 8)).astype(np.float32)
     t = ora.mr_tricubic(c, 8, 1, 1, 1, 8, 8, 8)
     assert t.tobytes() == c.tobytes()
+
+
+def _ref_config(ora, ilpt):
+    # _make_config(n=68, boxsize=226.67, z=0, ilpt, nbuff=8) of
+    # test/test_multiresolution.jl:10-46
+    return ora.Config(Omx=0.261, OmB=0.049, Omvac=0.69, h=0.68, n=68, boxsize=226.67, nbuff=8, z_out=0.0, z_max=0.0,
+                      ievol=0, ilpt=ilpt, ioutshear=0, wsmooth=1, rmax2rs=0.0)
+
+
+@pytest.fixture(scope="module")
+def ref_table(ora):
+    # make_table for CosmologyParams(0.31, 0.049, 0.69, 0.68) with the default
+    # table parameters, stored as Float32 like write_homeltab
+    tp = ora.TableParams()
+    d = ora.make_table(0.31, 0.049, 0.69, 0.68, tp).astype(np.float32)
+    return ora.Table(d, tp.Nx, tp.Ny, tp.Nz, tp.X1, tp.X2, tp.Y1, tp.Y2, tp.Z1, tp.Z2)
+
+
+REF_FILTERS = [(1, 1.686, 8.0), (2, 1.686, 5.0), (3, 1.686, 3.0)]
+
+
+@pytest.mark.parametrize("ilpt", [1, 2])
+def test_split_halo_count_tracks_global(ora, ref_table, ilpt):
+    # "Halo count comparison (ntile=2, 1LPT / 2LPT)"
+    # (test/test_multiresolution.jl:123-170): split vs global FFT within 5 %
+    cfg = _ref_config(ora, ilpt)
+    k, p = _pk()
+    g, _ = ora.run_multitile(cfg, 42, k, p, REF_FILTERS, ref_table, ntile=2)
+    s, _ = ora.run_multitile_split(cfg, 42, k, p, REF_FILTERS, ref_table, ntile=2, coarse_factor=5)
+    assert len(g) > 50
+    assert abs(len(s) - len(g)) / len(g) < 0.05 or abs(len(s) - len(g)) <= 3, (len(s), len(g))
+
+
+def test_split_coarse_grid_choice(ora):
+    # coarse_grid wins, then ntile coarse_factor, then the divisor whose block
+    # is closest to nmesh/3 (src/MultiResolution.jl:592-612)
+    assert ora.split_coarse_grid(120, 68, 2, 5, 0) == 10
+    assert ora.split_coarse_grid(120, 68, 2, 5, 24) == 24
+    assert ora.split_coarse_grid(120, 68, 2) == 5        # block 24 ~ 68 // 3 = 22 (block 20 ties later)
+    assert 120 % ora.split_coarse_grid(120, 60, 3) == 0
