@@ -14,6 +14,7 @@ Usage:
   python bench.py --lightcone  # 4 lightcone tiles of 384^3 (run_multitile) + merge_catalog
   python bench.py --shells     # batched shell analysis: 10^6 peaks on a 512^3 power-law field
   python bench.py --table      # collapse-table generation (make_table, RK4) on the GPU
+  python bench.py --split      # run_multitile_split, 8 tiles of nmesh 192 (--split-n 128..384)
 Under torchrun each rank runs independent tiles on its own GPU (run_tile
 does not shard: replicas) with its own seed; the job value is the tiles of
 all ranks over the slowest rank's device time.
@@ -547,6 +548,89 @@ def run_lightcone(args, dist: Dist):
                     "ranks is in wall_ms_per_step only"}
 
 
+# the multi-resolution sweep of the reference (run_multitile_split, GPU,
+# RTX A5000): per-tile wall time and halo count at nmesh 128..384
+SPLIT_PUBLISHED = {128: (0.818, 4982), 192: (2.550, 20467), 256: (6.667, 54057), 320: (12.312, 112271),
+                   384: (20.605, 198049)}
+
+
+def run_split_bench(args, dist: Dist):
+    """run_multitile_split on the reference's GPU scaling-sweep workload:
+    ntile 2 (8 tiles), nbuff 8, nmesh = --split-n (N = 2 (nmesh - 16) + 16,
+    isolated boxes (2 nmesh)^3), boxsize = N * 226.67/68 Mpc/h (as the
+    sweep sets it: the driver's cell is boxsize / nmesh), ilpt 2, ioutshear 0,
+    the automatic coarse grid, P(k) = 1e4 k^-1.5 tabulated at 200
+    log-spaced k in [1e-4, 10], filters 8 / 5 / 3 Mpc/h, the collapse table of
+    make_table for (Om 0.31, Ob 0.049, OL 0.69, h 0.68), seed 42.  A step is
+    the whole run: coarse phase, then per tile the split fields, peaks,
+    shells and records, copied to the host.  Under torchrun the tiles are
+    shared round-robin between the ranks (the reference's devices= dispatch)
+    and rank 0 gathers the records."""
+    import peakpatch_b200 as pp
+    from peakpatch_b200 import distributed as D
+    nm, nbuff, ntile = args.split_n, 8, 2
+    nsub = nm - 2 * nbuff
+    N = nsub * ntile + 2 * nbuff
+    box = N * 226.67 / 68.0
+    cfg = pp.PipelineConfig(Omx=0.261, OmB=0.049, Omvac=0.69, h=0.68, n=nm, boxsize=box, nbuff=nbuff,
+                            z_out=0.0, z_max=0.0, ievol=0, ilpt=2, ioutshear=0, wsmooth=1, rmax2rs=0.0)
+    rf = [8.0, 5.0, 3.0]
+    tiles = [(it, jt, kt) for kt in (1, 2) for jt in (1, 2) for it in (1, 2)]
+    mine = D.shard_tiles(tiles, dist.rank, dist.world)
+    ctx = pp.Context(dist.local)
+    _apply_options(ctx, args)
+    k = 10.0 ** np.linspace(-4, 1, 200)
+    ctx.set_pk_table(k, 1e4 * k ** -1.5)
+    ctx.make_table(0.31, 0.049, 0.69, 0.68, install=1)
+    from peakpatch_b200 import multires
+    M = multires.coarse_grid_size(nm, nbuff, ntile)
+    empty = np.zeros((0, 11), np.float32)
+
+    def run():
+        ctx.event_record(6)
+        rec, _, npk = ctx.run_multitile_split_arrays(cfg, 42, rf, ntile, tiles=mine) if mine else (empty, 0.0, 0)
+        ctx.event_record(7)
+        ctx.synchronize()
+        return ctx.event_elapsed(6, 7) / 1000.0, rec, npk
+
+    for _ in range(max(1, args.warmup)):
+        run()
+    t_dev, t_wall = [], []
+    for _ in range(args.steps):
+        dist.barrier()
+        t0 = time.perf_counter()
+        a, rec, npk = run()
+        dist.barrier()
+        t_wall.append(dist.max(time.perf_counter() - t0))
+        t_dev.append(dist.max(a))
+    stage = ctx.stage_ms()
+    nh = dist.sum(float(len(rec)))
+    npk_all = dist.sum(float(npk))
+    ctx.close()
+    if dist.rank != 0:
+        return None
+    td, tw = statistics.median(t_dev), statistics.median(t_wall)
+    pub = SPLIT_PUBLISHED.get(nm)
+    line = {"metric": "tiles/s (run_multitile_split)", "value": len(tiles) / td, "unit": "tiles/s",
+            "n_gpus": dist.world, "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": 1000 * td,
+            "higher_is_better": True, "scaling": "strong" if dist.world > 1 else "weak",
+            "vs_baseline": (len(tiles) / td) / (1.0 / pub[0]) if pub else None, "data": "synthetic",
+            "dtype": "f32 fields, compensated-f32 shell sums",
+            "config": {"workload": f"run_multitile_split, ntile 2, nmesh {nm} (N {N}, coarse grid {M}^3, isolated "
+                                   f"boxes {2 * nm}^3), nbuff 8, boxsize {box:.2f} Mpc/h, ilpt 2, ioutshear 0, "
+                                   "P(k) = 1e4 k^-1.5, filters 8/5/3 Mpc/h, seed 42",
+                       "parallelism": f"tiles round-robin over {dist.world} ranks" if dist.world > 1 else "1 GPU"},
+            "e2e": {"value": len(tiles) / tw, "unit": "tiles/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(nh) * 11 * 4},
+            "halos": int(nh), "peaks": int(npk_all), "stage_ms_rank0_last_run": stage,
+            "note": "value: device time (CUDA events on the library stream) of the slowest rank's run; e2e: wall "
+                    "clock of the Python call, records copied to the host"}
+    if pub:
+        line["reference_published"] = {"per_tile_s": pub[0], "tiles_per_s": 1.0 / pub[0], "halos": pub[1],
+                                       "hardware": "RTX A5000 (the reference's GPU scaling sweep)"}
+    return line
+
+
 def _threefry2x64_20(k0, k1, c0, c1):
     """Threefry-2x64 with 20 rounds (Salmon et al., SC'11; Random123), on
     uint64 numpy arrays."""
@@ -734,6 +818,8 @@ def main():
     ap.add_argument("--shells-n", type=int, default=512)
     ap.add_argument("--shells-peaks", type=int, default=1_000_000)
     ap.add_argument("--table", action="store_true", help="run the collapse-table generation instead")
+    ap.add_argument("--split", action="store_true", help="run the multi-resolution run_multitile_split instead")
+    ap.add_argument("--split-n", type=int, default=192, help="nmesh of the --split workload")
     ap.add_argument("--no-graphs", action="store_true", help="launch kernels one by one instead of as CUDA graphs")
     ap.add_argument("--no-autotune", action="store_true", help="default shell-stage choices, no autotuning")
     args = ap.parse_args()
@@ -749,6 +835,11 @@ def main():
             return
         if args.table:
             line = run_table_bench(args, dist)
+            if line is not None:
+                print(json.dumps(line), flush=True)
+            return
+        if args.split:
+            line = run_split_bench(args, dist)
             if line is not None:
                 print(json.dumps(line), flush=True)
             return

@@ -60,7 +60,7 @@ void Slot::release_buffers() {
   tile_lru.clear();
   for (DevBuf* b : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
                     &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &mr_in, &mr_out, &mr_aux,
-                    &mr_rec})
+                    &mr_rec, &mr_axis, &mr_amp})
     b->release();
   tune_save.release();
   iso.reset();
@@ -76,7 +76,7 @@ size_t Slot::shell_bytes() const {
   size_t b = 0;
   for (const DevBuf* d : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool,
                           &okey, &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &mr_in,
-                          &mr_out, &mr_aux, &mr_rec})
+                          &mr_out, &mr_aux, &mr_rec, &mr_axis, &mr_amp})
     b += d->bytes;
   if (iso) b += iso->bytes();
   return b;
@@ -718,6 +718,7 @@ int32_t ppb_set_pk_table(ppb_ctx* ctx, const double* k, const double* pk, int32_
   PPB_CUDA(cudaMemcpy(ctx->sh.pk_lk.p, lk.data(), n * 8, cudaMemcpyHostToDevice));
   PPB_CUDA(cudaMemcpy(ctx->sh.pk_lp.p, lp.data(), n * 8, cudaMemcpyHostToDevice));
   ctx->sh.pk_n = n;
+  ctx->sh.pk_version++;
   return PPB_OK;
   PPB_GUARD_END(ctx)
 }

@@ -81,11 +81,13 @@ __global__ void coarse_noise_kernel(float* __restrict__ out, int64_t N, int M, i
 // _generate_extended_residual (src/MultiResolution.jl:197-236): Float32 fine
 // noise minus its coarse cell's value times 1/sqrt(block^3), on the
 // (nmesh + 2 nshell)^3 region whose 0-based global origin is (i0, j0, k0),
-// periodic in N.  A thread takes two x-neighbours (one Threefry call when
-// they form a pair).
+// periodic in N, written with row pitch opx and plane pitch opz (a dense
+// array, or the corner of a zero-padded box).  A thread takes two
+// x-neighbours (one Threefry call when they form a pair).
 // ---------------------------------------------------------------------------
 __global__ void residual_kernel(const float* __restrict__ coarse, float* __restrict__ out, int M, int block,
-                                int64_t N, int64_t i0, int64_t j0, int64_t k0, int next, uint64_t seed, float inv) {
+                                int64_t N, int64_t i0, int64_t j0, int64_t k0, int next, uint64_t seed, float inv,
+                                int64_t opx, int64_t opz) {
   const int li = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   const int lj = blockIdx.y, lk = blockIdx.z;
   if (li >= next) return;
@@ -93,7 +95,7 @@ __global__ void residual_kernel(const float* __restrict__ coarse, float* __restr
   const int64_t gi = mod0(i0 + li, N);
   const int64_t row = N * (gj + N * gk);
   const int64_t cj = gj / block, ck = gk / block;
-  const int64_t o = li + (int64_t)next * (lj + (int64_t)next * lk);
+  const int64_t o = li + opx * lj + opz * lk;
   const uint64_t l0 = (uint64_t)(gi + row);
   if (li + 1 < next) {
     const int64_t gi1 = mod0(i0 + li + 1, N);
@@ -136,9 +138,12 @@ __global__ void pad_kernel(const float* __restrict__ in, float* __restrict__ out
 // the planes ix = n/2 + 1 - 1, iy = n/2, iz = n/2 (0-based) := 0.  Kernel
 // kinds (the reference's kernel_fn ids): 0 none, 1 i k_d1/k^2, 2 -i k_d1/k^2,
 // 3 -k_d1 k_d2/k^2, 4 k^2; the amplitude times `post` (the 1/n^3 of the
-// inverse transform) times the kernel is formed in Float64 and the product
-// rounded once to Float32.  `out` must not overlap `in`.
+// inverse transform) times the kernel is formed in Float64 (1/k^2 taken once
+// per mode) and the product rounded once to Float32.  `out` must not overlap
+// `in`.
 //
+// The TRANSFER amplitude comes from a table over the integer |freq|^2
+// (amp_table_kernel): one load per mode instead of a P(k) interpolation.
 // One thread per mode, all kernels of `sp` from one read of the input.  On
 // the ix = 0 plane and (even n) the ix = n/2 plane the thread also forms the
 // mirror mode (-iy, -iz) and writes the Hermitian projection
@@ -152,28 +157,30 @@ struct KSpecs {
 };
 
 __device__ __forceinline__ float2 kmul(float2 v, double amp, int kind, int d1, int d2, double kx, double ky,
-                                       double kz, double k2) {
+                                       double kz, double k2, double inv_k2) {
   const double a = (double)v.x, b = (double)v.y;
   const double ka = d1 == 1 ? kx : d1 == 2 ? ky : kz;
   const double kb = d2 == 1 ? kx : d2 == 2 ? ky : kz;
   float re, im;
   switch (kind) {
     case 0: re = (float)(a * amp); im = (float)(b * amp); break;
-    case 1: { const double c = amp * (ka / k2); re = (float)(-b * c); im = (float)(a * c); break; }
-    case 2: { const double c = amp * (-ka / k2); re = (float)(-b * c); im = (float)(a * c); break; }
-    case 3: { const double c = amp * (-ka * kb / k2); re = (float)(a * c); im = (float)(b * c); break; }
+    case 1: { const double c = amp * (ka * inv_k2); re = (float)(-b * c); im = (float)(a * c); break; }
+    case 2: { const double c = amp * (-ka * inv_k2); re = (float)(-b * c); im = (float)(a * c); break; }
+    case 3: { const double c = amp * ((-ka * kb) * inv_k2); re = (float)(a * c); im = (float)(b * c); break; }
     default: { const double c = amp * k2; re = (float)(a * c); im = (float)(b * c); break; }
   }
   return make_float2(re, im);
 }
 
+__device__ __forceinline__ int ifreq(int idx, int n) { return idx < (n + 1) / 2 ? idx : idx - n; }
+
 template <bool TRANSFER>
 __device__ __forceinline__ void kmode(const float2* __restrict__ in, int n, int nh, int ix, int iy, int iz,
-                                      double mult, double dk3n3, const double* __restrict__ lk,
-                                      const double* __restrict__ lp, int np, const KSpecs& sp, double post,
+                                      double mult, const double* __restrict__ amp_tab, const KSpecs& sp, double post,
                                       float2* t) {
   const float2 v = __ldg(in + ix + (int64_t)nh * (iy + (int64_t)n * iz));
-  const double kx = (double)ix * mult, ky = ks::fftfreq(iy, n, mult), kz = ks::fftfreq(iz, n, mult);
+  const int fy = ifreq(iy, n), fz = ifreq(iz, n);
+  const double kx = (double)ix * mult, ky = (double)fy * mult, kz = (double)fz * mult;
   const double k2 = kx * kx + ky * ky + kz * kz;
   bool zero = k2 == 0.0;
   if (!TRANSFER) zero = zero || ix == nh - 1 || iy == n / 2 || iz == n / 2;
@@ -182,26 +189,26 @@ __device__ __forceinline__ void kmode(const float2* __restrict__ in, int n, int 
     for (int s = 0; s < kMaxKSpecs; s++) t[s] = make_float2(0.f, 0.f);
     return;
   }
-  const double amp = TRANSFER ? sqrt(ks::pk_eval(lk, lp, np, sqrt(k2)) * dk3n3) * post : post;
+  const double amp = TRANSFER ? __ldg(amp_tab + (ix * ix + fy * fy + fz * fz)) : post;
+  const double inv_k2 = 1.0 / k2;   // one division per mode (k_a / k^2 as k_a * (1 / k^2))
 #pragma unroll
   for (int s = 0; s < kMaxKSpecs; s++)
-    if (s < sp.n) t[s] = kmul(v, amp, sp.kind[s], sp.d1[s], sp.d2[s], kx, ky, kz, k2);
+    if (s < sp.n) t[s] = kmul(v, amp, sp.kind[s], sp.d1[s], sp.d2[s], kx, ky, kz, k2, inv_k2);
 }
 
 template <bool TRANSFER>
 __global__ void __launch_bounds__(256) kspace_kernel(const float2* __restrict__ in, float2* __restrict__ out,
-                                                     int64_t odist, int n, double mult, double dk3n3,
-                                                     const double* __restrict__ lk, const double* __restrict__ lp,
-                                                     int np, KSpecs sp, double post) {
+                                                     int64_t odist, int n, double mult,
+                                                     const double* __restrict__ amp_tab, KSpecs sp, double post) {
   const int nh = n / 2 + 1;
-  const int64_t plane = (int64_t)nh * n;
-  const int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (id >= plane * n) return;
-  const int iz = (int)(id / plane);
-  const int r = (int)(id - (int64_t)iz * plane);
+  const int plane = nh * n;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= plane) return;
+  const int iz = blockIdx.y;
   const int iy = r / nh, ix = r - iy * nh;
+  const int64_t id = (int64_t)iz * plane + r;
   float2 t[kMaxKSpecs];
-  kmode<TRANSFER>(in, n, nh, ix, iy, iz, mult, dk3n3, lk, lp, np, sp, post, t);
+  kmode<TRANSFER>(in, n, nh, ix, iy, iz, mult, amp_tab, sp, post, t);
   if (ix == 0 || (n % 2 == 0 && ix == n / 2)) {
     const int jy = (n - iy) % n, jz = (n - iz) % n;
     if (jy == iy && jz == iz) {
@@ -209,7 +216,7 @@ __global__ void __launch_bounds__(256) kspace_kernel(const float2* __restrict__ 
       for (int s = 0; s < kMaxKSpecs; s++) t[s].y = 0.f;
     } else {
       float2 u[kMaxKSpecs];
-      kmode<TRANSFER>(in, n, nh, ix, jy, jz, mult, dk3n3, lk, lp, np, sp, post, u);
+      kmode<TRANSFER>(in, n, nh, ix, jy, jz, mult, amp_tab, sp, post, u);
 #pragma unroll
       for (int s = 0; s < kMaxKSpecs; s++) t[s] = make_float2(0.5f * (t[s].x + u[s].x), 0.5f * (t[s].y - u[s].y));
     }
@@ -259,40 +266,123 @@ __device__ __forceinline__ void catmull_rom(float t, float* w) {
   w[3] = __fsub_rn(__fmul_rn(0.5f, t3), __fmul_rn(0.5f, t2));
 }
 
-// out = val, or base + val (the combined field delta_self .+ delta_long of
-// :779-795; base may be out itself)
-__global__ void tricubic_kernel(const float* __restrict__ coarse, float* out, const float* base, int M, int block,
-                                int64_t N, int64_t i0, int64_t j0, int64_t k0, int n) {
+// Per axis d and tile coordinate l (3n entries, d major): the four wrapped
+// coarse indices and Catmull-Rom weights of _tricubic for the fine cell at
+// global (1-based) g = mod1(o_d + l + 1, N): f = (g - 0.5)/block + 0.5 in
+// Float64, ix = floor(f), t = Float32(f - ix).  The weights of a cell are the
+// product of its three axes' entries, so the per-cell work is only the
+// 64-term sum.
+__global__ void axis_weights_kernel(int4* __restrict__ idx, float4* __restrict__ wt, int M, int block, int64_t N,
+                                    int64_t o0, int64_t o1, int64_t o2, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3 * n) return;
+  const int d = t / n, l = t - d * n;
+  const int64_t o = d == 0 ? o0 : d == 1 ? o1 : o2;
+  const int64_t g = mod0(o + l, N) + 1;
+  const double f = __dadd_rn(__ddiv_rn(__dsub_rn((double)g, 0.5), (double)block), 0.5);
+  const double fl = floor(f);
+  const int64_t ic = (int64_t)fl;
+  float w[4];
+  catmull_rom((float)__dsub_rn(f, fl), w);
+  idx[t] = make_int4((int)mod0(ic - 2, M), (int)mod0(ic - 1, M), (int)mod0(ic, M), (int)mod0(ic + 1, M));
+  wt[t] = make_float4(w[0], w[1], w[2], w[3]);
+}
+
+__device__ __forceinline__ int comp(const int4& v, int c) { return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w; }
+__device__ __forceinline__ float comp(const float4& v, int c) {
+  return c == 0 ? v.x : c == 1 ? v.y : c == 2 ? v.z : v.w;
+}
+
+// _interpolate_to_tile / _tricubic / _catmull_rom (src/MultiResolution.jl:
+// 95-122, 156-189): the 64-term Catmull-Rom sum over the periodic M^3 coarse
+// field, terms ((wi * wj) * wk) * field added in the reference's order
+// (dkk outer, dii inner), for NF fields sharing one set of weights (NF = 4:
+// the fields interleaved as float4, one load per term).  Field f of cell
+// (li, lj, lk) goes to out[f][li + n lj + n^2 lk] as val, or as base[f] + val
+// when base is given (the combined field delta_self .+ delta_long of
+// :779-795); base[f] is read at bofs + li + bpy lj + bpz lk, so it may be a
+// zero-padded transform's output.
+template <int NF>
+struct TriArgs {
+  const float* coarse;     // NF == 1: the field; NF == 4: float4-interleaved fields
+  float* out[NF];
+  const float* base[NF];
+  int64_t bofs, bpy, bpz;
+};
+
+template <int NF>
+__device__ __forceinline__ void tri_load(const float* c, int q, float* v) {
+  if (NF == 1) {
+    v[0] = __ldg(c + q);
+  } else {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(c) + q);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  }
+}
+
+template <int NF>
+__global__ void __launch_bounds__(128) tricubic_kernel(TriArgs<NF> A, const int4* __restrict__ aidx,
+                                                       const float4* __restrict__ awt, int M, int n) {
   const int li = blockIdx.x * blockDim.x + threadIdx.x;
   const int lj = blockIdx.y, lk = blockIdx.z;
   if (li >= n) return;
-  const int64_t g[3] = {mod0(i0 + li, N) + 1, mod0(j0 + lj, N) + 1, mod0(k0 + lk, N) + 1};
-  int ic[3];
-  float w[3][4];
+  const int4 ix = __ldg(aidx + li), iy = __ldg(aidx + n + lj), iz = __ldg(aidx + 2 * n + lk);
+  const float4 wx = __ldg(awt + li), wy = __ldg(awt + n + lj), wz = __ldg(awt + 2 * n + lk);
+  // wi * wj for every (dii, djj): the first product of ((wi * wj) * wk) * f
+  float wij[4][4];
 #pragma unroll
-  for (int d = 0; d < 3; d++) {
-    const double f = __dadd_rn(__ddiv_rn(__dsub_rn((double)g[d], 0.5), (double)block), 0.5);
-    const double fl = floor(f);
-    ic[d] = (int)fl;
-    catmull_rom((float)__dsub_rn(f, fl), w[d]);
-  }
-  float val = 0.0f;
+  for (int b = 0; b < 4; b++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) wij[b][c] = __fmul_rn(comp(wx, c), comp(wy, b));
+  float val[NF];
+#pragma unroll
+  for (int f = 0; f < NF; f++) val[f] = 0.0f;
+#pragma unroll
   for (int a = 0; a < 4; a++) {
-    const int kk = (int)mod0(ic[2] - 2 + a, M);
+    const int kk = comp(iz, a);
+    const float wk = comp(wz, a);
+#pragma unroll
     for (int b = 0; b < 4; b++) {
-      const int jj = (int)mod0(ic[1] - 2 + b, M);
-      const float* row = coarse + (int64_t)M * (jj + (int64_t)M * kk);
+      const int row = M * (comp(iy, b) + M * kk);
 #pragma unroll
       for (int c = 0; c < 4; c++) {
-        const int ii = (int)mod0(ic[0] - 2 + c, M);
-        // ((wi * wj) * wk) * field, as Julia evaluates wi * wj * wk * f
-        const float term = __fmul_rn(__fmul_rn(__fmul_rn(w[0][c], w[1][b]), w[2][a]), __ldg(row + ii));
-        val = __fadd_rn(val, term);
+        const float w3 = __fmul_rn(wij[b][c], wk);
+        float v[NF];
+        tri_load<NF>(A.coarse, row + comp(ix, c), v);
+#pragma unroll
+        for (int f = 0; f < NF; f++) val[f] = __fadd_rn(val[f], __fmul_rn(w3, v[f]));
       }
     }
   }
   const int64_t o = li + (int64_t)n * (lj + (int64_t)n * lk);
-  out[o] = base ? __fadd_rn(base[o], val) : val;
+  const int64_t ob = A.bofs + li + A.bpy * lj + A.bpz * lk;
+#pragma unroll
+  for (int f = 0; f < NF; f++) A.out[f][o] = A.base[f] ? __fadd_rn(A.base[f][ob], val[f]) : val[f];
+}
+
+// four M^3 fields a apart interleaved as float4 (the tricubic input of the
+// split's coarse delta and psi)
+__global__ void interleave4_kernel(float4* __restrict__ dst, const float* __restrict__ src, int64_t fs, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  dst[i] = make_float4(src[i], src[fs + i], src[2 * fs + i], src[3 * fs + i]);
+}
+
+// the amplitude of the transfer multiply by integer |freq|^2 q on an n^3 box:
+// tab[q] = sqrt(P(sqrt(q) dk) dk^3 n^3) * post (tab[0] = 0)
+__global__ void amp_table_kernel(double* __restrict__ tab, int qmax, double mult, double dk3n3,
+                                 const double* __restrict__ lk, const double* __restrict__ lp, int np, double post) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q > qmax) return;
+  if (q == 0) {
+    tab[0] = 0.0;
+    return;
+  }
+  const double k2 = (double)q * (mult * mult);
+  tab[q] = sqrt(ks::pk_eval(lk, lp, np, sqrt(k2)) * dk3n3) * post;
 }
 
 }  // namespace
@@ -312,13 +402,15 @@ void launch_coarse_noise(Launch L, float* out, int64_t N, int M, uint64_t seed) 
 }
 
 void launch_residual(Launch L, const float* coarse, float* out, int M, int64_t N, int64_t i0, int64_t j0, int64_t k0,
-                     int next, uint64_t seed) {
+                     int next, uint64_t seed, int64_t opx, int64_t opz) {
   const int block = (int)(N / M);
   const double b = (double)block;
   const float inv = (float)(1.0 / std::sqrt(b * b * b));
   const int pairs = (next + 1) / 2;
+  if (opx <= 0) opx = next;
+  if (opz <= 0) opz = (int64_t)next * next;
   dim3 grid((unsigned)((pairs + 127) / 128), (unsigned)next, (unsigned)next);
-  residual_kernel<<<grid, 128, 0, L.s>>>(coarse, out, M, block, N, i0, j0, k0, next, seed, inv);
+  residual_kernel<<<grid, 128, 0, L.s>>>(coarse, out, M, block, N, i0, j0, k0, next, seed, inv, opx, opz);
   PPB_LAUNCHED(*L.count);
 }
 
@@ -328,10 +420,22 @@ void launch_pad(Launch L, const float* in, float* out, int nin, int n2, int64_t 
   PPB_LAUNCHED(*L.count);
 }
 
-void launch_kspace(Launch L, bool transfer, const float2* in, float2* out, int64_t odist, int n, double box,
-                   const double* lk, const double* lp, int np, const int* kind, const int* d1, const int* d2,
-                   int nspec, double post) {
-  if (nspec < 1 || nspec > kMaxKSpecs) throw Error{PPB_ERR_INVALID, "kspace: 1..8 kernels per launch"};
+int64_t amp_table_size(int n) { return 3 * (int64_t)(n / 2 + 1) * (n / 2 + 1) + 1; }
+
+void launch_amp_table(Launch L, double* tab, int n, double box, const double* lk, const double* lp, int np,
+                      double post) {
+  const double dk = 2.0 * 3.141592653589793 / box;
+  const double mult = ((double)n * dk) / (double)n;
+  const double nd = (double)n;
+  const double dk3n3 = (dk * dk * dk) * (nd * nd * nd);
+  const int qmax = (int)(amp_table_size(n) - 1);
+  amp_table_kernel<<<(qmax + 256) / 256, 256, 0, L.s>>>(tab, qmax, mult, dk3n3, lk, lp, np, post);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_kspace(Launch L, const double* amp_tab, const float2* in, float2* out, int64_t odist, int n, double box,
+                   const int* kind, const int* d1, const int* d2, int nspec, double post) {
+  if (nspec < 1 || nspec > kMaxKSpecs) throw Error{PPB_ERR_INVALID, "kspace: 1..6 kernels per launch"};
   KSpecs sp{};
   sp.n = nspec;
   for (int s = 0; s < nspec; s++) {
@@ -341,14 +445,11 @@ void launch_kspace(Launch L, bool transfer, const float2* in, float2* out, int64
   }
   const double dk = 2.0 * 3.141592653589793 / box;
   const double mult = ((double)n * dk) / (double)n;
-  const double nd = (double)n;
-  const double dk3n3 = (dk * dk * dk) * (nd * nd * nd);
-  const int64_t modes = (int64_t)(n / 2 + 1) * n * n;
-  const unsigned blocks = (unsigned)((modes + 255) / 256);
-  if (transfer)
-    kspace_kernel<true><<<blocks, 256, 0, L.s>>>(in, out, odist, n, mult, dk3n3, lk, lp, np, sp, post);
+  const dim3 grid((unsigned)(((n / 2 + 1) * n + 255) / 256), (unsigned)n);
+  if (amp_tab)
+    kspace_kernel<true><<<grid, 256, 0, L.s>>>(in, out, odist, n, mult, amp_tab, sp, post);
   else
-    kspace_kernel<false><<<blocks, 256, 0, L.s>>>(in, out, odist, n, mult, dk3n3, lk, lp, np, sp, post);
+    kspace_kernel<false><<<grid, 256, 0, L.s>>>(in, out, odist, n, mult, nullptr, sp, post);
   PPB_LAUNCHED(*L.count);
 }
 
@@ -359,11 +460,34 @@ void launch_src2_trace(Launch L, const float* delta, const float* phi, float* ou
   PPB_LAUNCHED(*L.count);
 }
 
-void launch_tricubic(Launch L, const float* coarse, float* out, int M, int64_t N, int64_t i0, int64_t j0, int64_t k0,
-                     int n, const float* base) {
+void launch_axis_weights(Launch L, int4* idx, float4* wt, int M, int64_t N, int64_t i0, int64_t j0, int64_t k0,
+                         int n) {
   const int block = (int)(N / M);
+  axis_weights_kernel<<<(3 * n + 127) / 128, 128, 0, L.s>>>(idx, wt, M, block, N, i0, j0, k0, n);
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_tricubic(Launch L, const int4* idx, const float4* wt, int M, int n, int nf, const float* coarse,
+                     float* const* out, const float* const* base, int64_t bofs, int64_t bpy, int64_t bpz) {
   dim3 grid((unsigned)((n + 127) / 128), (unsigned)n, (unsigned)n);
-  tricubic_kernel<<<grid, 128, 0, L.s>>>(coarse, out, base, M, block, N, i0, j0, k0, n);
+  if (nf == 1) {
+    TriArgs<1> A{coarse, {out[0]}, {base ? base[0] : nullptr}, bofs, bpy, bpz};
+    tricubic_kernel<1><<<grid, 128, 0, L.s>>>(A, idx, wt, M, n);
+  } else if (nf == 4) {
+    TriArgs<4> A{coarse,
+                 {out[0], out[1], out[2], out[3]},
+                 {base ? base[0] : nullptr, base ? base[1] : nullptr, base ? base[2] : nullptr,
+                  base ? base[3] : nullptr},
+                 bofs, bpy, bpz};
+    tricubic_kernel<4><<<grid, 128, 0, L.s>>>(A, idx, wt, M, n);
+  } else {
+    throw Error{PPB_ERR_INVALID, "tricubic: 1 or 4 fields per launch"};
+  }
+  PPB_LAUNCHED(*L.count);
+}
+
+void launch_interleave4(Launch L, float4* dst, const float* src, int64_t fs, int64_t n) {
+  interleave4_kernel<<<(unsigned)((n + 255) / 256), 256, 0, L.s>>>(dst, src, fs, n);
   PPB_LAUNCHED(*L.count);
 }
 

@@ -21,7 +21,9 @@ namespace ppb {
 // ---------------------------------------------------------------------------
 // isolated-convolution resources
 // ---------------------------------------------------------------------------
-static cufftHandle plan_inplace(int n, cufftType t, size_t* ws) {
+// an in-place n^3 real<->complex plan over `batch` consecutive boxes, its
+// work area supplied by the caller (the size is returned in *ws)
+static cufftHandle plan_inplace(int n, cufftType t, int batch, size_t* ws) {
   cufftHandle h;
   PPB_CUFFT(cufftCreate(&h));
   PPB_CUFFT(cufftSetAutoAllocation(h, 0));
@@ -30,36 +32,62 @@ static cufftHandle plan_inplace(int n, cufftType t, size_t* ws) {
   long long cemb[3] = {n, n, nh}, remb[3] = {n, n, 2 * nh};
   const long long cdist = (long long)n * n * nh, rdist = 2 * cdist;
   if (t == CUFFT_R2C)
-    PPB_CUFFT(cufftMakePlanMany64(h, 3, dims, remb, 1, rdist, cemb, 1, cdist, t, 1, ws));
+    PPB_CUFFT(cufftMakePlanMany64(h, 3, dims, remb, 1, rdist, cemb, 1, cdist, t, batch, ws));
   else
-    PPB_CUFFT(cufftMakePlanMany64(h, 3, dims, cemb, 1, cdist, remb, 1, rdist, t, 1, ws));
+    PPB_CUFFT(cufftMakePlanMany64(h, 3, dims, cemb, 1, cdist, remb, 1, rdist, t, batch, ws));
   return h;
 }
 
 IsoRes::~IsoRes() {
-  if (r2c) cufftDestroy(r2c);
-  if (c2r) cufftDestroy(c2r);
+  for (cufftHandle h : {r2c, c2r, c2r4})
+    if (h) cufftDestroy(h);
 }
 
 void IsoRes::setup(int nn, int nb, cudaStream_t s) {
   const int64_t modes = (int64_t)(nn / 2 + 1) * nn * nn;
   if (nn != n2) {
-    if (r2c) { cufftDestroy(r2c); r2c = 0; }
-    if (c2r) { cufftDestroy(c2r); c2r = 0; }
+    for (cufftHandle* h : {&r2c, &c2r, &c2r4})
+      if (*h) { cufftDestroy(*h); *h = 0; }
     n2 = 0;
     size_t w1 = 0, w2 = 0;
-    r2c = plan_inplace(nn, CUFFT_R2C, &w1);
-    c2r = plan_inplace(nn, CUFFT_C2R, &w2);
+    r2c = plan_inplace(nn, CUFFT_R2C, 1, &w1);
+    c2r = plan_inplace(nn, CUFFT_C2R, 1, &w2);
     ws.ensure(std::max<size_t>(std::max(w1, w2), 256));
     PPB_CUFFT(cufftSetWorkArea(r2c, ws.p));
     PPB_CUFFT(cufftSetWorkArea(c2r, ws.p));
     spec.ensure(modes * 8);
+    amp.ensure(amp_table_size(nn) * 8);
+    amp_box = 0.0;
     n2 = nn;
   }
   PPB_CUFFT(cufftSetStream(r2c, s));
   PPB_CUFFT(cufftSetStream(c2r, s));
+  if (nb >= 4 && !c2r4) {   // the four inverse transforms of the split as one batched plan
+    size_t w4 = 0;
+    c2r4 = plan_inplace(nn, CUFFT_C2R, 4, &w4);
+    if (w4 > ws.bytes) {
+      ws.ensure(w4);
+      PPB_CUFFT(cufftSetWorkArea(r2c, ws.p));
+      PPB_CUFFT(cufftSetWorkArea(c2r, ws.p));
+    }
+    PPB_CUFFT(cufftSetWorkArea(c2r4, ws.p));
+  }
+  if (c2r4) PPB_CUFFT(cufftSetStream(c2r4, s));
   work.ensure((size_t)nb * modes * 8);
   batch = (int)(work.bytes / ((size_t)modes * 8));
+}
+
+// the amplitude table of the padded box of side `box` (rebuilt when the box
+// or the P(k) table changed)
+static const double* iso_amp(ppb_ctx* ctx, Slot& sl, IsoRes& iso, double box) {
+  if (iso.amp_box != box || iso.amp_pk != ctx->sh.pk_version) {
+    const double post = 1.0 / ((double)iso.n2 * (double)iso.n2 * (double)iso.n2);
+    launch_amp_table(Launch{sl.stream, &sl.launches}, iso.amp.as<double>(), iso.n2, box, ctx->sh.pk_lk.as<double>(),
+                     ctx->sh.pk_lp.as<double>(), ctx->sh.pk_n, post);
+    iso.amp_box = box;
+    iso.amp_pk = ctx->sh.pk_version;
+  }
+  return iso.amp.as<double>();
 }
 
 
@@ -90,6 +118,7 @@ void mr_isolated_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int n_inpu
   // dx = boxsize_local / n; the padded box is n2 * dx (src/MultiResolution.jl:249-259)
   const double box = (double)n2 * (boxsize_local / (double)n);
   const double post = 1.0 / ((double)n2 * (double)n2 * (double)n2);
+  const double* amp = iso_amp(ctx, sl, iso, box);
   for (int b0 = 0; b0 < nk; b0 += batch) {
     const int g = std::min(batch, nk - b0);
     int kind[kMaxKSpecs], d1[kMaxKSpecs], d2[kMaxKSpecs];
@@ -98,8 +127,7 @@ void mr_isolated_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int n_inpu
       d1[q] = kernels[3 * (b0 + q) + 1];
       d2[q] = kernels[3 * (b0 + q) + 2];
     }
-    launch_kspace(L, true, iso.spec.as<float2>(), iso.work.as<float2>(), modes, n2, box, ctx->sh.pk_lk.as<double>(),
-                  ctx->sh.pk_lp.as<double>(), ctx->sh.pk_n, kind, d1, d2, g, post);
+    launch_kspace(L, amp, iso.spec.as<float2>(), iso.work.as<float2>(), modes, n2, box, kind, d1, d2, g, post);
     for (int q = 0; q < g; q++) {
       float2* w = iso.work.as<float2>() + q * modes;
       PPB_CUFFT(cufftExecC2R(iso.c2r, reinterpret_cast<cufftComplex*>(w), reinterpret_cast<float*>(w)));
@@ -123,25 +151,58 @@ void mr_tile_2lpt_lap(ppb_ctx* ctx, Slot& sl, TileRes& T, int n, double box, flo
   if (psi2) {
     // phi_11, phi_22, phi_33, phi_12, phi_13, phi_23 (:812-821)
     const int pk6[6] = {3, 3, 3, 3, 3, 3}, pa[6] = {1, 2, 3, 1, 1, 2}, pb[6] = {1, 2, 3, 2, 3, 3};
-    launch_kspace(L, false, T.dk.as<float2>(), T.kw.as<float2>(), Mk, n, box, nullptr, nullptr, 0, pk6, pa, pb, 6,
-                  post);
+    launch_kspace(L, nullptr, T.dk.as<float2>(), T.kw.as<float2>(), Mk, n, box, pk6, pa, pb, 6, post);
     PPB_CUFFT(cufftExecC2R(T.c2r6, T.kw.as<cufftComplex>(), T.rw.as<float>()));
     sl.launches++;
     launch_src2_trace(L, T.delta.as<float>(), T.rw.as<float>(), T.rw.as<float>(), n, n, (int64_t)n * n, N);
-    forward(T.rw.as<float>());
-    const int k2[3] = {2, 2, 2}, da[3] = {1, 2, 3}, db[3] = {0, 0, 0};
-    launch_kspace(L, false, T.dk.as<float2>(), T.kw.as<float2>(), Mk, n, box, nullptr, nullptr, 0, k2, da, db, 3,
-                  post);
-    PPB_CUFFT(cufftExecC2R(T.c2r3, T.kw.as<cufftComplex>(), psi2));
+    // rfft(src2) into the first phi slot (its transform has consumed it), so
+    // T.dk keeps rfft(delta)
+    PPB_CUFFT(cufftExecR2C(T.r2c, T.rw.as<float>(), T.kw.as<cufftComplex>()));
     sl.launches++;
-    forward(T.delta.as<float>());   // T.dk back to rfft(delta)
+    const int k2[3] = {2, 2, 2}, da[3] = {1, 2, 3}, db[3] = {0, 0, 0};
+    launch_kspace(L, nullptr, T.kw.as<float2>(), T.kw.as<float2>() + Mk, Mk, n, box, k2, da, db, 3, post);
+    PPB_CUFFT(cufftExecC2R(T.c2r3, T.kw.as<cufftComplex>() + Mk, psi2));
+    sl.launches++;
   }
   if (lapd) {
     const int k4[1] = {4}, z[1] = {0};
-    launch_kspace(L, false, T.dk.as<float2>(), T.kw.as<float2>(), Mk, n, box, nullptr, nullptr, 0, k4, z, z, 1, post);
+    launch_kspace(L, nullptr, T.dk.as<float2>(), T.kw.as<float2>(), Mk, n, box, k4, z, z, 1, post);
     PPB_CUFFT(cufftExecC2R(T.c2r1, T.kw.as<cufftComplex>(), lapd));
     sl.launches++;
   }
+}
+
+void mr_split_tile_fields(ppb_ctx* ctx, Slot& sl, TileRes& T, const float* cnoise, const float* cf4, int M, int64_t N,
+                          int64_t i0, int64_t j0, int64_t k0, int nm, double box_local, uint64_t seed) {
+  cudaStream_t s = sl.stream;
+  Launch L{s, &sl.launches};
+  const int n2 = 2 * nm, nh2 = n2 / 2 + 1;
+  const int64_t modes = (int64_t)nh2 * n2 * n2, px = 2 * (int64_t)nh2, Nt = (int64_t)nm * nm * nm;
+  if (!sl.iso) sl.iso.reset(new IsoRes());
+  IsoRes& iso = *sl.iso;
+  iso.setup(n2, 4, s);
+  // the residual written straight into the zero-padded box (:731-733, 254-255)
+  PPB_CUDA(cudaMemsetAsync(iso.spec.p, 0, (size_t)modes * 8, s));
+  launch_residual(L, cnoise, iso.spec.as<float>(), M, N, i0, j0, k0, nm, seed, px, px * n2);
+  PPB_CUFFT(cufftExecR2C(iso.r2c, iso.spec.as<float>(), iso.spec.as<cufftComplex>()));
+  sl.launches++;
+  // delta, psi_x, psi_y, psi_z of the isolated convolution (:740-752)
+  const double box = (double)n2 * (box_local / (double)nm);
+  const int kind[4] = {0, 1, 1, 1}, d1[4] = {0, 1, 2, 3}, d2[4] = {0, 0, 0, 0};
+  launch_kspace(L, iso_amp(ctx, sl, iso, box), iso.spec.as<float2>(), iso.work.as<float2>(), modes, n2, box, kind, d1,
+                d2, 4, 1.0 / ((double)n2 * (double)n2 * (double)n2));
+  PPB_CUFFT(cufftExecC2R(iso.c2r4, iso.work.as<cufftComplex>(), iso.work.as<float>()));
+  sl.launches++;
+  // plus the tricubic coarse fields, read from the transforms in place
+  // (:764-795): one pass writes the four tile fields
+  sl.mr_axis.ensure((size_t)3 * nm * 32);
+  int4* aidx = sl.mr_axis.as<int4>();
+  float4* awt = reinterpret_cast<float4*>(aidx + 3 * nm);
+  launch_axis_weights(L, aidx, awt, M, N, i0, j0, k0, nm);
+  float* out[4] = {T.delta.as<float>(), T.psi.as<float>(), T.psi.as<float>() + Nt, T.psi.as<float>() + 2 * Nt};
+  const float* w = iso.work.as<float>();
+  const float* base[4] = {w, w + 2 * modes, w + 4 * modes, w + 6 * modes};
+  launch_tricubic(L, aidx, awt, M, nm, 4, cf4, out, base, 0, px, px * n2);
 }
 
 void mr_coarse_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int M, double boxsize_full, int ilpt,
@@ -157,6 +218,9 @@ void mr_coarse_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int M, doubl
   PPB_CUFFT(cufftExecR2C(tr.r2c, tr.delta.as<float>(), tr.dk.as<cufftComplex>()));
   sl.launches++;
   const double post = 1.0 / ((double)M * (double)M * (double)M);
+  sl.mr_amp.ensure(amp_table_size(M) * 8);
+  const double* amp = sl.mr_amp.as<double>();
+  launch_amp_table(L, sl.mr_amp.as<double>(), M, boxsize_full, lk, lp, np, post);
   auto c2r_into = [&](int q, float* dst) {
     PPB_CUFFT(cufftExecC2R(tr.c2r1, tr.kw.as<cufftComplex>() + q * Mk, dst));
     sl.launches++;
@@ -164,23 +228,20 @@ void mr_coarse_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int M, doubl
   {  // delta and psi_d (:621-632), lapd (:662-667)
     int kind[5] = {0, 1, 1, 1, 4}, a[5] = {0, 1, 2, 3, 0}, b[5] = {0, 0, 0, 0, 0};
     const int g = ioutshear >= 1 ? 5 : 4;
-    launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, kind, a, b, g,
-                  post);
+    launch_kspace(L, amp, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, kind, a, b, g, post);
     for (int q = 0; q < 4; q++) c2r_into(q, o + q * fs);
     if (g == 5) c2r_into(4, o + 7 * fs);
   }
   if (ilpt >= 2) {  // the 2LPT source and displacements (:635-659)
     const int pk6[6] = {3, 3, 3, 3, 3, 3}, pa[6] = {1, 2, 3, 1, 1, 2}, pb[6] = {1, 2, 3, 2, 3, 3};
-    launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, pk6, pa, pb, 6,
-                  post);
+    launch_kspace(L, amp, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, pk6, pa, pb, 6, post);
     PPB_CUFFT(cufftExecC2R(tr.c2r6, tr.kw.as<cufftComplex>(), tr.rw.as<float>()));
     sl.launches++;
     launch_src2_trace(L, o, tr.rw.as<float>(), tr.rw.as<float>(), M, M, (int64_t)M * M, N);
     PPB_CUFFT(cufftExecR2C(tr.r2c, tr.rw.as<float>(), tr.dk.as<cufftComplex>()));
     sl.launches++;
     const int k2[3] = {2, 2, 2}, da[3] = {1, 2, 3}, db[3] = {0, 0, 0};
-    launch_kspace(L, true, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, lk, lp, np, k2, da, db, 3,
-                  post);
+    launch_kspace(L, amp, tr.dk.as<float2>(), tr.kw.as<float2>(), Mk, M, boxsize_full, k2, da, db, 3, post);
     for (int q = 0; q < 3; q++) c2r_into(q, o + (4 + q) * fs);
   }
 }
@@ -299,8 +360,13 @@ int32_t ppb_interpolate_to_tile(ppb_ctx* ctx, const float* coarse, int32_t it, i
     const size_t bytes = (size_t)nmesh * nmesh * nmesh * 4;
     const float* c = (const float*)stage_in(sl.mr_in, coarse, (size_t)M * M * M * 4, sl.stream);
     float* d = out_buffer(out, sl.mr_out, bytes);
-    launch_tricubic(Launch{sl.stream, &sl.launches}, c, d, M, N, origin(it, nsub, nmesh, 0), origin(jt, nsub, nmesh, 0),
-                    origin(kt, nsub, nmesh, 0), nmesh);
+    Launch L{sl.stream, &sl.launches};
+    sl.mr_axis.ensure((size_t)3 * nmesh * 32);
+    int4* aidx = sl.mr_axis.as<int4>();
+    float4* awt = reinterpret_cast<float4*>(aidx + 3 * nmesh);
+    launch_axis_weights(L, aidx, awt, M, N, origin(it, nsub, nmesh, 0), origin(jt, nsub, nmesh, 0),
+                        origin(kt, nsub, nmesh, 0), nmesh);
+    launch_tricubic(L, aidx, awt, M, nmesh, 1, c, &d, nullptr, 0, 0, 0);
     finish_out(out, d, bytes, sl.stream);
     PPB_CUDA(cudaStreamSynchronize(sl.stream));
   });

@@ -37,13 +37,17 @@ struct TileRes {
 struct IsoRes {
   int n2 = 0, batch = 0;
   cufftHandle r2c = 0, c2r = 0;   // n2^3, in place, one transform each
+  cufftHandle c2r4 = 0;           // four consecutive boxes of `work` (batch >= 4)
   DevBuf spec;   // the padded input (row pitch 2 (n2/2+1) floats), then its half-spectrum
   DevBuf work;   // `batch` half-spectra, each then transformed back in place
-  DevBuf ws;     // cuFFT work area of both plans
+  DevBuf ws;     // cuFFT work area of the plans
+  DevBuf amp;    // transfer amplitude by integer |freq|^2 for box amp_box and P(k) version amp_pk
+  double amp_box = 0.0;
+  int64_t amp_pk = -1;
   ~IsoRes();
   // plans and buffers for padded size n2 and up to `batch` kernels per pass
   void setup(int n2, int batch, cudaStream_t s);
-  size_t bytes() const { return spec.bytes + work.bytes + ws.bytes; }
+  size_t bytes() const { return spec.bytes + work.bytes + ws.bytes + amp.bytes; }
 };
 
 // one autotuned shell-stage configuration: the gather order brick and the
@@ -86,6 +90,7 @@ struct Slot {
   DevBuf tcen, tcount, t_aos, t_lapd;               // multi-tile: centres, peaks per tile, tile fields
   std::unique_ptr<IsoRes> iso;                      // multi-resolution: isolated convolution
   DevBuf mr_in, mr_out, mr_aux, mr_rec;             // multi-resolution: staged inputs, outputs, records
+  DevBuf mr_axis, mr_amp;                           // multi-resolution: tricubic axis tables, coarse amplitudes
   int gather_bps[2][2] = {{0, 0}, {0, 0}};          // gather blocks per SM by [comp][adaptive]
   double rows_per_peak[2] = {0.0, 0.0};             // pool rows per peak seen last, by adaptive
   double walk_per_peak = 0.0;                       // collapse-walk steps per peak seen last
@@ -131,6 +136,7 @@ struct Shared {
   std::shared_mutex mu;
   DevBuf pk_lk, pk_lp;
   int pk_n = 0;
+  int64_t pk_version = 0;   // incremented by every P(k) upload
   DevBuf tab;
   bool has_tab = false;
   DevTable dtab{};
@@ -252,6 +258,13 @@ void mr_coarse_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int M, doubl
 // the n^3 region at nshell into outs[b]; the caller holds ctx->sh.mu shared
 void mr_isolated_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int n_input, double boxsize_local, int n,
                         const int32_t* kernels, int nk, int nshell, float* const* outs);
+// the split's tile fields into T.delta and T.psi: residual of the tile at
+// origin (i0, j0, k0) straight into the padded box, one forward transform,
+// the delta and psi kernels, one batched inverse transform, plus the
+// tricubic coarse fields cf4 (delta, psi x3 interleaved as float4) in one
+// pass; the caller holds ctx->sh.mu shared
+void mr_split_tile_fields(ppb_ctx* ctx, Slot& sl, TileRes& T, const float* cnoise, const float* cf4, int M, int64_t N,
+                          int64_t i0, int64_t j0, int64_t k0, int nm, double box_local, uint64_t seed);
 // tile-local 2LPT (psi2: 3 fields n^3 apart) and/or Laplacian of T.delta;
 // leaves T.dk = rfft(T.delta)
 void mr_tile_2lpt_lap(ppb_ctx* ctx, Slot& sl, TileRes& T, int n, double box, float* psi2, float* lapd);

@@ -324,20 +324,33 @@ void launch_shell_d2f(Launch L, const ShellArgs& a, int blocks);
 // 0-based global cells, periodic in N; coarse grids are M^3 with N % M == 0.
 constexpr int kMaxKSpecs = 6;   // kernels per k-space launch
 void launch_coarse_noise(Launch L, float* out, int64_t N, int M, uint64_t seed);
+// the residual on the (next)^3 region at origin (i0, j0, k0), written with
+// row pitch opx and plane pitch opz (<= 0: dense next^3)
 void launch_residual(Launch L, const float* coarse, float* out, int M, int64_t N, int64_t i0, int64_t j0, int64_t k0,
-                     int next, uint64_t seed);
+                     int next, uint64_t seed, int64_t opx = 0, int64_t opz = 0);
 void launch_pad(Launch L, const float* in, float* out, int nin, int n2, int64_t px);
-// transfer (P(k) amplitude, isolated / periodic convolution) or apply
-// (kernel only, Nyquist planes zeroed) of nspec kernels (kind, d1, d2) from
-// the half-spectrum `in` of an n^3 box of side `box` into nspec half-spectra
-// odist float2 apart, times post; Hermitian projection fused
-void launch_kspace(Launch L, bool transfer, const float2* in, float2* out, int64_t odist, int n, double box,
-                   const double* lk, const double* lp, int np, const int* kind, const int* d1, const int* d2,
-                   int nspec, double post);
+// the transfer amplitude by integer |freq|^2 on an n^3 box of side box
+// (amp_table_size(n) doubles), times post
+int64_t amp_table_size(int n);
+void launch_amp_table(Launch L, double* tab, int n, double box, const double* lk, const double* lp, int np,
+                      double post);
+// nspec kernels (kind, d1, d2) from the half-spectrum `in` of an n^3 box of
+// side `box` into nspec half-spectra odist float2 apart: transfer (amplitude
+// from amp_tab, DC zeroed) or, with amp_tab null, apply (amplitude post, DC
+// and Nyquist planes zeroed); Hermitian projection fused
+void launch_kspace(Launch L, const double* amp_tab, const float2* in, float2* out, int64_t odist, int n, double box,
+                   const int* kind, const int* d1, const int* d2, int nspec, double post);
 void launch_src2_trace(Launch L, const float* delta, const float* phi, float* out, int n, int64_t px, int64_t pz,
                        int64_t pd);
-// out (n^3) = tricubic interpolation, plus base[i] when base is not null
-void launch_tricubic(Launch L, const float* coarse, float* out, int M, int64_t N, int64_t i0, int64_t j0, int64_t k0,
-                     int n, const float* base = nullptr);
+// per-axis tricubic indices and weights (3n entries) of the n^3 tile at
+// origin (i0, j0, k0), then the interpolation of nf coarse fields sharing
+// them (nf 1: one field; nf 4: four fields interleaved as float4 by
+// launch_interleave4): out[f] (n^3) = value, or base[f] (at bofs + x + bpy y +
+// bpz z) + value
+void launch_axis_weights(Launch L, int4* idx, float4* wt, int M, int64_t N, int64_t i0, int64_t j0, int64_t k0,
+                         int n);
+void launch_tricubic(Launch L, const int4* idx, const float4* wt, int M, int n, int nf, const float* coarse,
+                     float* const* out, const float* const* base, int64_t bofs, int64_t bpy, int64_t bpz);
+void launch_interleave4(Launch L, float4* dst, const float* src, int64_t fs, int64_t n);
 
 }  // namespace ppb

@@ -967,22 +967,20 @@ void run_multitile_split_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, 
   // 2LPT and Laplacian of :635-667 are never read afterwards)
   const int64_t Mc = (int64_t)M * M * M, fs = (Mc + 3) & ~(int64_t)3;
   sl.mr_in.ensure(Mc * 4);
-  sl.mr_aux.ensure(4 * fs * 4);
+  sl.mr_aux.ensure(4 * fs * 4 + Mc * 16);
   float* cnoise = sl.mr_in.as<float>();
   float* cf = sl.mr_aux.as<float>();
+  float4* cf4 = reinterpret_cast<float4*>(cf + 4 * fs);   // 16-byte aligned: fs is a multiple of 4
   cudaEvent_t* ev = sl.stage_ev;
   PPB_CUDA(cudaEventRecord(ev[0], r.s));
   launch_coarse_noise(r.L, cnoise, N, M, p->seed);
   mr_coarse_device(ctx, sl, cnoise, M, box_full, 1, 0, cf, fs);
+  launch_interleave4(r.L, cf4, cf, fs, Mc);
   TileRes& T = sl.tile_for(nm);
   T.setup(nm, r.s);
   T.aos.ensure(Nt * 32);
   if (T.cap == 0) T.ensure_peaks(std::max<int64_t>(1 << 16, std::min<int64_t>(Nt / 64, 1 << 22)));
-  sl.mr_out.ensure(Nt * 4);
-  float* resid = sl.mr_out.as<float>();
   const int nf = p->ioutshear >= 1 ? 33 : 11;
-  const int32_t kern4[12] = {0, 0, 0, 1, 1, 0, 1, 2, 0, 1, 3, 0};
-  float* outs[4] = {T.delta.as<float>(), T.psi.as<float>(), T.psi.as<float>() + Nt, T.psi.as<float>() + 2 * Nt};
   size_t used = 0;
   int64_t nrec_tot = 0, npk_tot = 0;
   float rmax_tot = 0.f;
@@ -996,10 +994,8 @@ void run_multitile_split_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, 
                   k0 = (int64_t)(tl[t][2] - 1) * nsub - nbuff;
     PPB_CUDA(cudaEventRecord(ev[0], r.s));
     // fields (:728-847)
-    launch_residual(r.L, cnoise, resid, M, N, i0, j0, k0, nm, p->seed);
-    mr_isolated_device(ctx, sl, resid, nm, box_local, nm, kern4, 4, 0, outs);
-    launch_tricubic(r.L, cf, outs[0], M, N, i0, j0, k0, nm, outs[0]);
-    for (int c = 0; c < 3; c++) launch_tricubic(r.L, cf + (1 + c) * fs, outs[1 + c], M, N, i0, j0, k0, nm, outs[1 + c]);
+    mr_split_tile_fields(ctx, sl, T, cnoise, reinterpret_cast<const float*>(cf4), M, N, i0, j0, k0, nm, box_local,
+                         p->seed);
     mr_tile_2lpt_lap(ctx, sl, T, nm, box_local, p->ilpt >= 2 ? T.psi2.as<float>() : nullptr,
                      r.want_lap ? T.lapd.as<float>() : nullptr);
     launch_hermitise(r.L, T.dk.as<float2>(), nm, 1);
