@@ -120,12 +120,14 @@ __global__ void residual_kernel(const float* __restrict__ coarse, float* __restr
 // ---------------------------------------------------------------------------
 // zero padding of _isolated_convolve (:254-255): the n_in^3 input in the
 // corner of an n2^3 box stored with row pitch `px` floats (the layout of an
-// in-place real-to-complex transform)
+// in-place real-to-complex transform).  The row padding is zeroed too: the
+// pruned forward transform reads the planes it does not transform as
+// complex data, whose last element per row is that padding.
 // ---------------------------------------------------------------------------
 __global__ void pad_kernel(const float* __restrict__ in, float* __restrict__ out, int nin, int n2, int64_t px) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
-  if (x >= n2) return;
+  if (x >= px) return;
   float v = 0.f;
   if (x < nin && y < nin && z < nin) v = __ldg(in + x + (int64_t)nin * (y + (int64_t)nin * z));
   out[x + px * (y + (int64_t)n2 * z)] = v;
@@ -415,7 +417,7 @@ void launch_residual(Launch L, const float* coarse, float* out, int M, int64_t N
 }
 
 void launch_pad(Launch L, const float* in, float* out, int nin, int n2, int64_t px) {
-  dim3 grid((unsigned)((n2 + 127) / 128), (unsigned)n2, (unsigned)n2);
+  dim3 grid((unsigned)((px + 127) / 128), (unsigned)n2, (unsigned)n2);
   pad_kernel<<<grid, 128, 0, L.s>>>(in, out, nin, n2, px);
   PPB_LAUNCHED(*L.count);
 }

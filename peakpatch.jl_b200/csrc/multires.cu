@@ -21,60 +21,85 @@ namespace ppb {
 // ---------------------------------------------------------------------------
 // isolated-convolution resources
 // ---------------------------------------------------------------------------
-// an in-place n^3 real<->complex plan over `batch` consecutive boxes, its
-// work area supplied by the caller (the size is returned in *ws)
-static cufftHandle plan_inplace(int n, cufftType t, int batch, size_t* ws) {
+// the pruned transforms of a zero-padded box: 2-D (y, x) real<->complex
+// transforms over `planes` consecutive z-planes, and the 1-D complex
+// transform along z of every (y, x) column, all in place
+static cufftHandle plan_planes(int n, cufftType t, int planes, size_t* ws) {
   cufftHandle h;
   PPB_CUFFT(cufftCreate(&h));
   PPB_CUFFT(cufftSetAutoAllocation(h, 0));
-  long long dims[3] = {n, n, n};
+  long long dims[2] = {n, n};
   const long long nh = n / 2 + 1;
-  long long cemb[3] = {n, n, nh}, remb[3] = {n, n, 2 * nh};
-  const long long cdist = (long long)n * n * nh, rdist = 2 * cdist;
+  long long cemb[2] = {n, nh}, remb[2] = {n, 2 * nh};
+  const long long cdist = (long long)n * nh, rdist = 2 * cdist;
   if (t == CUFFT_R2C)
-    PPB_CUFFT(cufftMakePlanMany64(h, 3, dims, remb, 1, rdist, cemb, 1, cdist, t, batch, ws));
+    PPB_CUFFT(cufftMakePlanMany64(h, 2, dims, remb, 1, rdist, cemb, 1, cdist, t, planes, ws));
   else
-    PPB_CUFFT(cufftMakePlanMany64(h, 3, dims, cemb, 1, cdist, remb, 1, rdist, t, batch, ws));
+    PPB_CUFFT(cufftMakePlanMany64(h, 2, dims, cemb, 1, cdist, remb, 1, rdist, t, planes, ws));
+  return h;
+}
+
+static cufftHandle plan_columns(int n, size_t* ws) {
+  cufftHandle h;
+  PPB_CUFFT(cufftCreate(&h));
+  PPB_CUFFT(cufftSetAutoAllocation(h, 0));
+  long long dims[1] = {n};
+  const long long plane = (long long)n * (n / 2 + 1);
+  long long emb[1] = {n};
+  PPB_CUFFT(cufftMakePlanMany64(h, 1, dims, emb, plane, 1, emb, plane, 1, CUFFT_C2C, plane, ws));
   return h;
 }
 
 IsoRes::~IsoRes() {
-  for (cufftHandle h : {r2c, c2r, c2r4})
+  for (cufftHandle h : {f2d, i2d, col})
     if (h) cufftDestroy(h);
 }
 
 void IsoRes::setup(int nn, int nb, cudaStream_t s) {
   const int64_t modes = (int64_t)(nn / 2 + 1) * nn * nn;
   if (nn != n2) {
-    for (cufftHandle* h : {&r2c, &c2r, &c2r4})
+    for (cufftHandle* h : {&f2d, &i2d, &col})
       if (*h) { cufftDestroy(*h); *h = 0; }
     n2 = 0;
-    size_t w1 = 0, w2 = 0;
-    r2c = plan_inplace(nn, CUFFT_R2C, 1, &w1);
-    c2r = plan_inplace(nn, CUFFT_C2R, 1, &w2);
-    ws.ensure(std::max<size_t>(std::max(w1, w2), 256));
-    PPB_CUFFT(cufftSetWorkArea(r2c, ws.p));
-    PPB_CUFFT(cufftSetWorkArea(c2r, ws.p));
+    size_t w[3] = {0, 0, 0};
+    f2d = plan_planes(nn, CUFFT_R2C, nn / 2, &w[0]);
+    i2d = plan_planes(nn, CUFFT_C2R, nn / 2, &w[1]);
+    col = plan_columns(nn, &w[2]);
+    ws.ensure(std::max<size_t>(std::max(w[0], std::max(w[1], w[2])), 256));
+    for (cufftHandle h : {f2d, i2d, col}) PPB_CUFFT(cufftSetWorkArea(h, ws.p));
     spec.ensure(modes * 8);
     amp.ensure(amp_table_size(nn) * 8);
     amp_box = 0.0;
     n2 = nn;
   }
-  PPB_CUFFT(cufftSetStream(r2c, s));
-  PPB_CUFFT(cufftSetStream(c2r, s));
-  if (nb >= 4 && !c2r4) {   // the four inverse transforms of the split as one batched plan
-    size_t w4 = 0;
-    c2r4 = plan_inplace(nn, CUFFT_C2R, 4, &w4);
-    if (w4 > ws.bytes) {
-      ws.ensure(w4);
-      PPB_CUFFT(cufftSetWorkArea(r2c, ws.p));
-      PPB_CUFFT(cufftSetWorkArea(c2r, ws.p));
-    }
-    PPB_CUFFT(cufftSetWorkArea(c2r4, ws.p));
-  }
-  if (c2r4) PPB_CUFFT(cufftSetStream(c2r4, s));
+  for (cufftHandle h : {f2d, i2d, col}) PPB_CUFFT(cufftSetStream(h, s));
   work.ensure((size_t)nb * modes * 8);
   batch = (int)(work.bytes / ((size_t)modes * 8));
+}
+
+// forward transform of the zero-padded box in spec (input nonzero on planes
+// z < n2/2 only): the 2-D transform of those planes, then every z-column
+static void iso_forward(Slot& sl, IsoRes& iso) {
+  PPB_CUFFT(cufftExecR2C(iso.f2d, iso.spec.as<float>(), iso.spec.as<cufftComplex>()));
+  PPB_CUFFT(cufftExecC2C(iso.col, iso.spec.as<cufftComplex>(), iso.spec.as<cufftComplex>(), CUFFT_FORWARD));
+  sl.launches += 2;
+}
+
+// inverse transform of the half-spectrum at w, valid on the z-planes
+// [z0, z0 + nz): every z-column, then the 2-D transform of n2/2 planes that
+// cover them (of all planes when nz > n2/2)
+static void iso_inverse(Slot& sl, IsoRes& iso, float2* w, int z0, int nz) {
+  const int half = iso.n2 / 2;
+  const int64_t plane = (int64_t)iso.n2 * (half + 1);
+  cufftComplex* c = reinterpret_cast<cufftComplex*>(w);
+  PPB_CUFFT(cufftExecC2C(iso.col, c, c, CUFFT_INVERSE));
+  sl.launches++;
+  const int starts[2] = {nz > half ? 0 : std::min(z0, iso.n2 - half), half};
+  for (int h = 0; h < (nz > half ? 2 : 1); h++) {
+    cufftComplex* p = c + starts[h] * plane;
+    PPB_CUFFT(cufftExecC2R(iso.i2d, p, reinterpret_cast<float*>(p)));
+    sl.launches++;
+  }
 }
 
 // the amplitude table of the padded box of side `box` (rebuilt when the box
@@ -113,8 +138,7 @@ void mr_isolated_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int n_inpu
   iso.setup(n2, batch, s);
   batch = std::min(iso.batch, std::min(nk, kMaxKSpecs));
   launch_pad(L, d_noise, iso.spec.as<float>(), n_input, n2, px);
-  PPB_CUFFT(cufftExecR2C(iso.r2c, iso.spec.as<float>(), iso.spec.as<cufftComplex>()));
-  sl.launches++;
+  iso_forward(sl, iso);
   // dx = boxsize_local / n; the padded box is n2 * dx (src/MultiResolution.jl:249-259)
   const double box = (double)n2 * (boxsize_local / (double)n);
   const double post = 1.0 / ((double)n2 * (double)n2 * (double)n2);
@@ -130,8 +154,7 @@ void mr_isolated_device(ppb_ctx* ctx, Slot& sl, const float* d_noise, int n_inpu
     launch_kspace(L, amp, iso.spec.as<float2>(), iso.work.as<float2>(), modes, n2, box, kind, d1, d2, g, post);
     for (int q = 0; q < g; q++) {
       float2* w = iso.work.as<float2>() + q * modes;
-      PPB_CUFFT(cufftExecC2R(iso.c2r, reinterpret_cast<cufftComplex*>(w), reinterpret_cast<float*>(w)));
-      sl.launches++;
+      iso_inverse(sl, iso, w, nshell, n);
       launch_extract(L, outs[b0 + q], reinterpret_cast<const float*>(w), (int64_t)nshell * (1 + px + px * n2), px,
                      px * n2, n);
     }
@@ -184,15 +207,13 @@ void mr_split_tile_fields(ppb_ctx* ctx, Slot& sl, TileRes& T, const float* cnois
   // the residual written straight into the zero-padded box (:731-733, 254-255)
   PPB_CUDA(cudaMemsetAsync(iso.spec.p, 0, (size_t)modes * 8, s));
   launch_residual(L, cnoise, iso.spec.as<float>(), M, N, i0, j0, k0, nm, seed, px, px * n2);
-  PPB_CUFFT(cufftExecR2C(iso.r2c, iso.spec.as<float>(), iso.spec.as<cufftComplex>()));
-  sl.launches++;
+  iso_forward(sl, iso);
   // delta, psi_x, psi_y, psi_z of the isolated convolution (:740-752)
   const double box = (double)n2 * (box_local / (double)nm);
   const int kind[4] = {0, 1, 1, 1}, d1[4] = {0, 1, 2, 3}, d2[4] = {0, 0, 0, 0};
   launch_kspace(L, iso_amp(ctx, sl, iso, box), iso.spec.as<float2>(), iso.work.as<float2>(), modes, n2, box, kind, d1,
                 d2, 4, 1.0 / ((double)n2 * (double)n2 * (double)n2));
-  PPB_CUFFT(cufftExecC2R(iso.c2r4, iso.work.as<cufftComplex>(), iso.work.as<float>()));
-  sl.launches++;
+  for (int q = 0; q < 4; q++) iso_inverse(sl, iso, iso.work.as<float2>() + q * modes, 0, nm);
   // plus the tricubic coarse fields, read from the transforms in place
   // (:764-795): one pass writes the four tile fields
   sl.mr_axis.ensure((size_t)3 * nm * 32);

@@ -36,8 +36,10 @@ struct TileRes {
 // in-place transforms over one cuFFT work area
 struct IsoRes {
   int n2 = 0, batch = 0;
-  cufftHandle r2c = 0, c2r = 0;   // n2^3, in place, one transform each
-  cufftHandle c2r4 = 0;           // four consecutive boxes of `work` (batch >= 4)
+  // pruned in-place transforms: 2-D (y, x) over n2/2 z-planes (forward: the
+  // planes holding the input; inverse: the planes holding the wanted output)
+  // and the 1-D z transform of every column
+  cufftHandle f2d = 0, i2d = 0, col = 0;
   DevBuf spec;   // the padded input (row pitch 2 (n2/2+1) floats), then its half-spectrum
   DevBuf work;   // `batch` half-spectra, each then transformed back in place
   DevBuf ws;     // cuFFT work area of the plans

@@ -98,6 +98,17 @@ def test_isolated_convolve_vs_oracle(mctx, ora, eh_pk, nmesh, nshell):
         _close(g, o)
 
 
+def test_isolated_convolve_region_wider_than_input(mctx, ora, eh_pk):
+    # the kept region may reach into the zero padding (n + nshell up to
+    # 2 n_input): the pruned inverse then transforms every plane
+    rng = np.random.default_rng(5)
+    noise = rng.standard_normal((12, 12, 12)).astype(np.float32)
+    for n, nshell in ((20, 2), (12, 0), (5, 9)):
+        g = mctx.isolated_convolve_gpu_multi(noise, None, 40.0, n, [(0, 0, 0), (1, 3, 0)], nshell)
+        for (kind, d1, d2), x in zip([(0, 0, 0), (1, 3, 0)], g):
+            _close(x, ora.isolated_convolve(noise, *eh_pk, 40.0, n, kind, d1, d2, nshell))
+
+
 def test_isolated_convolve_multi_equals_single(mctx, ora):
     # kernels grouped into passes of up to four give the same bits as one
     # kernel per call
