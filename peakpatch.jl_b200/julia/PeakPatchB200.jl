@@ -166,4 +166,92 @@ function find_peaks(delta::Array{Float32,3}, mask::Array{Int8,3}, xbx, ybx, zbx,
             for q in 1:np[]]
 end
 
+# ---- multi-resolution split (src/MultiResolution.jl) ---------------------
+# Methods for the reference's GPU plug-in stubs of run_multitile_split
+# (src/PeakPatch.jl:255-339) and the driver itself.  `pk` is a P(k) file path
+# (or nothing to keep the context's table); kernels are (kernel_fn_id, dim1,
+# dim2) tuples with the ids of isolated_convolve_gpu.
+
+"""GPU isolated_convolve_gpu_multi: one zero-padded rfft, then per kernel the
+transfer multiply and irfft; one n^3 array per kernel."""
+function isolated_convolve_gpu_multi(noise::Array{Float32,3}, pk, boxsize_local, n::Integer;
+                                     kernels=[(0, 0, 0), (1, 1, 0), (1, 2, 0), (1, 3, 0)], nshell::Integer=0,
+                                     ctx::Context=default_context())
+    pk === nothing || set_pk_table!(ctx, pk)
+    ks = Int32[k[j] for k in kernels for j in 1:3]
+    out = Array{Float32,4}(undef, n, n, n, length(kernels))
+    check(ctx, ccall((:ppb_isolated_convolve, libppb), Int32,
+                     (Ptr{Cvoid}, Ptr{Float32}, Int32, Float64, Int32, Ptr{Int32}, Int32, Int32, Ptr{Float32}),
+                     ctx.h, noise, size(noise, 1), boxsize_local, n, ks, length(kernels), nshell, out))
+    return [out[:, :, :, q] for q in 1:length(kernels)]
+end
+
+isolated_convolve_gpu(noise, pk, boxsize_local, n; kernel_fn_id=0, dim1=0, dim2=0, nshell=0,
+                      ctx::Context=default_context()) =
+    isolated_convolve_gpu_multi(noise, pk, boxsize_local, n; kernels=[(kernel_fn_id, dim1, dim2)], nshell=nshell,
+                                ctx=ctx)[1]
+
+"""GPU interpolate_to_tile_gpu: Catmull-Rom tricubic interpolation of the
+periodic M^3 coarse field at the tile's cells (bit-identical)."""
+function interpolate_to_tile_gpu(coarse::Array{Float32,3}, it, jt, kt, nsub, nmesh, N, M;
+                                 ctx::Context=default_context())
+    out = Array{Float32,3}(undef, nmesh, nmesh, nmesh)
+    check(ctx, ccall((:ppb_interpolate_to_tile, libppb), Int32,
+                     (Ptr{Cvoid}, Ptr{Float32}, Int32, Int32, Int32, Int32, Int32, Int64, Int32, Ptr{Float32}),
+                     ctx.h, coarse, it, jt, kt, nsub, nmesh, N, M, out))
+    return out
+end
+
+"""GPU compute_2lpt_gpu: tile-local 2LPT displacements [psi2_x, psi2_y, psi2_z]."""
+function compute_2lpt_gpu(delta_tile::Array{Float32,3}, nmesh, boxsize_local; ctx::Context=default_context())
+    out = Array{Float32,4}(undef, nmesh, nmesh, nmesh, 3)
+    check(ctx, ccall((:ppb_compute_2lpt, libppb), Int32, (Ptr{Cvoid}, Ptr{Float32}, Int32, Float64, Ptr{Float32}),
+                     ctx.h, delta_tile, nmesh, boxsize_local, out))
+    return [out[:, :, :, d] for d in 1:3]
+end
+
+"""GPU compute_laplacian_gpu: irfft(k^2 rfft(delta_tile)) with the Nyquist zeroing."""
+function compute_laplacian_gpu(delta_tile::Array{Float32,3}, nmesh, boxsize_local; ctx::Context=default_context())
+    out = Array{Float32,3}(undef, nmesh, nmesh, nmesh)
+    check(ctx, ccall((:ppb_compute_laplacian, libppb), Int32, (Ptr{Cvoid}, Ptr{Float32}, Int32, Float64, Ptr{Float32}),
+                     ctx.h, delta_tile, nmesh, boxsize_local, out))
+    return out
+end
+
+"""
+    run_multitile_split(cfg; ntile, seed=42, coarse_factor=0, coarse_grid=0) -> halos
+
+Drop-in for MultiResolution.run_multitile_split(cfg; ntile, seed, coarse_factor,
+coarse_grid, use_gpu=true): every stage on the GPU, records in tile order.
+"""
+function run_multitile_split(cfg; ntile::Integer, seed::Integer=42, verbose::Bool=false, coarse_factor::Integer=0,
+                             coarse_grid::Integer=0, ctx::Context=default_context())
+    PP = Base.root_module(Base.__toplevel__, :PeakPatch)
+    table, tp = PP.read_homeltab(cfg.tabfile)
+    set_collapse_table!(ctx, table, tp)
+    set_pk_table!(ctx, cfg.pkfile)
+    Rf = Float64[f[3] for f in PP.read_filterbank(cfg.filterfile)]
+    params = Ref(tile_params(cfg, seed))
+    nf = cfg.ioutshear >= 1 ? 33 : 11
+    cap = 1 << 20
+    while true
+        buf = Vector{Float32}(undef, nf * cap)
+        hb = Ref(HaloBuf(pointer(buf), cap, 0, 0, 0f0, 0))
+        rc = GC.@preserve buf ccall((:ppb_run_multitile_split, libppb), Int32,
+                                    (Ptr{Cvoid}, Ref{TileParams}, Ptr{Float64}, Int32, Int32, Int32, Int32,
+                                     Ptr{Int32}, Int32, Ref{HaloBuf}),
+                                    ctx.h, params, Rf, length(Rf), ntile, coarse_factor, coarse_grid, C_NULL, 0, hb)
+        if rc == PPB_ERR_CAPACITY
+            cap = Int(hb[].count) + 16
+            continue
+        end
+        check(ctx, rc)
+        n = Int(hb[].count)
+        recs = reshape(buf[1:nf * n], nf, n)
+        verbose && @info "run_multitile_split (B200): $(n) halos"
+        return nf == 33 ? [PP.ExtHaloRecord(recs[:, i]...) for i in 1:n] :
+                          [PP.HaloRecord(recs[:, i]...) for i in 1:n]
+    end
+end
+
 end # module PeakPatchB200
