@@ -31,11 +31,18 @@ __device__ __forceinline__ int64_t mod0(int64_t i, int64_t n) {
 // ---------------------------------------------------------------------------
 // _downsample_noise (src/MultiResolution.jl:68-89): coarse cell (I, J, K)
 // sums the Float64 deviates of its block^3 fine cells in the order dk, dj, di
-// (di fastest).  One warp per coarse cell: the lanes evaluate 64 consecutive
-// cells of that order (two per lane, one Threefry call when the two form a
-// pair) and every lane adds the 64 values in order, so the sum is the
-// sequential one bit for bit.
+// (di fastest).  One warp per coarse cell: per step the lanes evaluate 256
+// consecutive cells of that order (eight per lane as four Threefry pairs,
+// independent chains that hide each other's latency) and every lane adds the
+// 256 values in order, so the sum is the sequential one bit for bit.
 // ---------------------------------------------------------------------------
+constexpr int kNoisePairsPerLane = 4;
+
+__device__ __forceinline__ uint64_t block_cell_lin(int t, int block, int64_t gi0, int64_t gj0, int64_t gk0, int64_t N) {
+  const int di = t % block, dj = (t / block) % block, dk = t / (block * block);
+  return (uint64_t)((gi0 + di) + N * ((gj0 + dj) + N * (gk0 + dk)));
+}
+
 __global__ void coarse_noise_kernel(float* __restrict__ out, int64_t N, int M, int block, uint64_t seed,
                                     double denom) {
   const int lane = threadIdx.x & 31;
@@ -45,33 +52,38 @@ __global__ void coarse_noise_kernel(float* __restrict__ out, int64_t N, int M, i
   const int64_t I = cell % M, J = (cell / M) % M, K = cell / ((int64_t)M * M);
   const int total = block * block * block;
   const int64_t gi0 = I * block, gj0 = J * block, gk0 = K * block;
+  constexpr int kPer = 2 * kNoisePairsPerLane, kStep = 32 * kPer;
   double val = 0.0;
-  for (int base = 0; base < total; base += 64) {
-    const int t0 = base + 2 * lane;
-    double v0 = 0.0, v1 = 0.0;
-    if (t0 < total) {
-      const int di = t0 % block, dj = (t0 / block) % block, dk = t0 / (block * block);
-      const uint64_t l0 = (uint64_t)((gi0 + di) + N * ((gj0 + dj) + N * (gk0 + dk)));
-      if (t0 + 1 < total) {
-        const int t1 = t0 + 1;
-        const int ei = t1 % block, ej = (t1 / block) % block, ek = t1 / (block * block);
-        const uint64_t l1 = (uint64_t)((gi0 + ei) + N * ((gj0 + ej) + N * (gk0 + ek)));
-        if ((l0 & 1ull) == 0 && l1 == l0 + 1) {
-          ppbm::threefry_gaussian_pair(seed, l0 >> 1, &v0, &v1);
+  for (int base = 0; base < total; base += kStep) {
+    double v[kPer];
+#pragma unroll
+    for (int q = 0; q < kNoisePairsPerLane; q++) {
+      const int t0 = base + kPer * lane + 2 * q;
+      double a = 0.0, b = 0.0;
+      if (t0 < total) {
+        const uint64_t l0 = block_cell_lin(t0, block, gi0, gj0, gk0, N);
+        if (t0 + 1 < total) {
+          const uint64_t l1 = block_cell_lin(t0 + 1, block, gi0, gj0, gk0, N);
+          if ((l0 & 1ull) == 0 && l1 == l0 + 1) {
+            ppbm::threefry_gaussian_pair(seed, l0 >> 1, &a, &b);
+          } else {
+            a = ppbm::noise_cell_d(seed, l0);
+            b = ppbm::noise_cell_d(seed, l1);
+          }
         } else {
-          v0 = ppbm::noise_cell_d(seed, l0);
-          v1 = ppbm::noise_cell_d(seed, l1);
+          a = ppbm::noise_cell_d(seed, l0);
         }
-      } else {
-        v0 = ppbm::noise_cell_d(seed, l0);
       }
+      v[2 * q] = a;
+      v[2 * q + 1] = b;
     }
-    const int cnt = min(64, total - base);
-#pragma unroll 8
+    const int cnt = min(kStep, total - base);
     for (int j = 0; j < 32; j++) {
-      const double a = __shfl_sync(kFull, v0, j), b = __shfl_sync(kFull, v1, j);
-      if (2 * j < cnt) val = __dadd_rn(val, a);
-      if (2 * j + 1 < cnt) val = __dadd_rn(val, b);
+#pragma unroll
+      for (int q = 0; q < kPer; q++) {
+        const double x = __shfl_sync(kFull, v[q], j);
+        if (kPer * j + q < cnt) val = __dadd_rn(val, x);
+      }
     }
   }
   if (lane == 0) out[cell] = (float)__ddiv_rn(val, denom);
@@ -203,12 +215,11 @@ __global__ void __launch_bounds__(256) kspace_kernel(const float2* __restrict__ 
                                                      int64_t odist, int n, double mult,
                                                      const double* __restrict__ amp_tab, KSpecs sp, double post) {
   const int nh = n / 2 + 1;
-  const int plane = nh * n;
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= plane) return;
-  const int iz = blockIdx.y;
-  const int iy = r / nh, ix = r - iy * nh;
-  const int64_t id = (int64_t)iz * plane + r;
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iz = blockIdx.z;
+  if (ix >= nh || iy >= n) return;
+  const int64_t id = ix + (int64_t)nh * (iy + (int64_t)n * iz);
   float2 t[kMaxKSpecs];
   kmode<TRANSFER>(in, n, nh, ix, iy, iz, mult, amp_tab, sp, post, t);
   if (ix == 0 || (n % 2 == 0 && ix == n / 2)) {
@@ -447,11 +458,13 @@ void launch_kspace(Launch L, const double* amp_tab, const float2* in, float2* ou
   }
   const double dk = 2.0 * 3.141592653589793 / box;
   const double mult = ((double)n * dk) / (double)n;
-  const dim3 grid((unsigned)(((n / 2 + 1) * n + 255) / 256), (unsigned)n);
+  // threads along ix (32 per warp), 8 rows of iy per block, one iz per grid z
+  const dim3 block(32, 8);
+  const dim3 grid((unsigned)((n / 2 + 1 + 31) / 32), (unsigned)((n + 7) / 8), (unsigned)n);
   if (amp_tab)
-    kspace_kernel<true><<<grid, 256, 0, L.s>>>(in, out, odist, n, mult, amp_tab, sp, post);
+    kspace_kernel<true><<<grid, block, 0, L.s>>>(in, out, odist, n, mult, amp_tab, sp, post);
   else
-    kspace_kernel<false><<<grid, 256, 0, L.s>>>(in, out, odist, n, mult, nullptr, sp, post);
+    kspace_kernel<false><<<grid, block, 0, L.s>>>(in, out, odist, n, mult, nullptr, sp, post);
   PPB_LAUNCHED(*L.count);
 }
 
