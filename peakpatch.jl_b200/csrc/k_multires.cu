@@ -21,7 +21,6 @@ namespace ppb {
 
 namespace {
 
-constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ int64_t mod0(int64_t i, int64_t n) {
   const int64_t r = i % n;
@@ -31,62 +30,68 @@ __device__ __forceinline__ int64_t mod0(int64_t i, int64_t n) {
 // ---------------------------------------------------------------------------
 // _downsample_noise (src/MultiResolution.jl:68-89): coarse cell (I, J, K)
 // sums the Float64 deviates of its block^3 fine cells in the order dk, dj, di
-// (di fastest).  One warp per coarse cell: per step the lanes evaluate 256
-// consecutive cells of that order (eight per lane as four Threefry pairs,
-// independent chains that hide each other's latency) and every lane adds the
-// 256 values in order, so the sum is the sequential one bit for bit.
+// (di fastest).  One block per coarse cell: per chunk, warps 1..7 evaluate
+// 1792 consecutive cells of that order into shared memory (eight per lane as
+// four Threefry pairs) while thread 0 adds the previous chunk's values in
+// order, so the sum is the sequential one bit for bit and the addition chain
+// is the only serial part.
 // ---------------------------------------------------------------------------
-constexpr int kNoisePairsPerLane = 4;
+constexpr int kNoiseThreads = 256;
+constexpr int kNoiseGenWarps = kNoiseThreads / 32 - 1;
+constexpr int kNoisePer = 8;                                   // cells per generating lane
+constexpr int kNoiseChunk = kNoiseGenWarps * 32 * kNoisePer;   // 1792 cells
 
 __device__ __forceinline__ uint64_t block_cell_lin(int t, int block, int64_t gi0, int64_t gj0, int64_t gk0, int64_t N) {
   const int di = t % block, dj = (t / block) % block, dk = t / (block * block);
   return (uint64_t)((gi0 + di) + N * ((gj0 + dj) + N * (gk0 + dk)));
 }
 
-__global__ void coarse_noise_kernel(float* __restrict__ out, int64_t N, int M, int block, uint64_t seed,
-                                    double denom) {
-  const int lane = threadIdx.x & 31;
-  const int64_t cell = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t M3 = (int64_t)M * M * M;
-  if (cell >= M3) return;   // uniform over the warp
+__global__ void __launch_bounds__(kNoiseThreads) coarse_noise_kernel(float* __restrict__ out, int64_t N, int M,
+                                                                       int block, uint64_t seed, double denom) {
+  __shared__ double buf[2][kNoiseChunk];
+  const int64_t cell = blockIdx.x;
   const int64_t I = cell % M, J = (cell / M) % M, K = cell / ((int64_t)M * M);
   const int total = block * block * block;
   const int64_t gi0 = I * block, gj0 = J * block, gk0 = K * block;
-  constexpr int kPer = 2 * kNoisePairsPerLane, kStep = 32 * kPer;
+  const int nchunk = (total + kNoiseChunk - 1) / kNoiseChunk;
+  const int warp = threadIdx.x >> 5;
   double val = 0.0;
-  for (int base = 0; base < total; base += kStep) {
-    double v[kPer];
+  for (int c = 0; c <= nchunk; c++) {
+    if (warp > 0 && c < nchunk) {   // generate chunk c
+      double* dst = buf[c & 1] + ((warp - 1) * 32 + (threadIdx.x & 31)) * kNoisePer;
+      const int tb = c * kNoiseChunk + ((warp - 1) * 32 + (threadIdx.x & 31)) * kNoisePer;
 #pragma unroll
-    for (int q = 0; q < kNoisePairsPerLane; q++) {
-      const int t0 = base + kPer * lane + 2 * q;
-      double a = 0.0, b = 0.0;
-      if (t0 < total) {
-        const uint64_t l0 = block_cell_lin(t0, block, gi0, gj0, gk0, N);
-        if (t0 + 1 < total) {
-          const uint64_t l1 = block_cell_lin(t0 + 1, block, gi0, gj0, gk0, N);
-          if ((l0 & 1ull) == 0 && l1 == l0 + 1) {
-            ppbm::threefry_gaussian_pair(seed, l0 >> 1, &a, &b);
+      for (int q = 0; q < kNoisePer; q += 2) {
+        const int t0 = tb + q;
+        double a = 0.0, b = 0.0;
+        if (t0 < total) {
+          const uint64_t l0 = block_cell_lin(t0, block, gi0, gj0, gk0, N);
+          if (t0 + 1 < total) {
+            const uint64_t l1 = block_cell_lin(t0 + 1, block, gi0, gj0, gk0, N);
+            if ((l0 & 1ull) == 0 && l1 == l0 + 1) {
+              ppbm::threefry_gaussian_pair(seed, l0 >> 1, &a, &b);
+            } else {
+              a = ppbm::noise_cell_d(seed, l0);
+              b = ppbm::noise_cell_d(seed, l1);
+            }
           } else {
             a = ppbm::noise_cell_d(seed, l0);
-            b = ppbm::noise_cell_d(seed, l1);
           }
-        } else {
-          a = ppbm::noise_cell_d(seed, l0);
         }
-      }
-      v[2 * q] = a;
-      v[2 * q + 1] = b;
-    }
-    const int cnt = min(kStep, total - base);
-    for (int j = 0; j < 32; j++) {
-#pragma unroll
-      for (int q = 0; q < kPer; q++) {
-        const double x = __shfl_sync(kFull, v[q], j);
-        if (kPer * j + q < cnt) val = __dadd_rn(val, x);
+        dst[q] = a;
+        dst[q + 1] = b;
       }
     }
+    if (threadIdx.x == 0 && c > 0) {   // add chunk c - 1 in order
+      const double* src = buf[(c - 1) & 1];
+      const int cnt = min(kNoiseChunk, total - (c - 1) * kNoiseChunk);
+      for (int i = 0; i < cnt; i++) val = __dadd_rn(val, src[i]);
+    }
+    // chunk c is written and chunk c - 1 consumed before buffer (c + 1) & 1
+    // (= (c - 1) & 1) is written again
+    __syncthreads();
   }
-  if (lane == 0) out[cell] = (float)__ddiv_rn(val, denom);
+  if (threadIdx.x == 0) out[cell] = (float)__ddiv_rn(val, denom);
 }
 
 // ---------------------------------------------------------------------------
@@ -407,10 +412,8 @@ void launch_coarse_noise(Launch L, float* out, int64_t N, int M, uint64_t seed) 
   const int block = (int)(N / M);
   const double b = (double)block;
   const double denom = std::sqrt(b * b * b);
-  const int64_t warps = (int64_t)M * M * M;
-  const int threads = 128;
-  const int64_t blocks = (warps * 32 + threads - 1) / threads;
-  coarse_noise_kernel<<<(unsigned)blocks, threads, 0, L.s>>>(out, N, M, block, seed, denom);
+  const int64_t cells = (int64_t)M * M * M;
+  coarse_noise_kernel<<<(unsigned)cells, kNoiseThreads, 0, L.s>>>(out, N, M, block, seed, denom);
   PPB_LAUNCHED(*L.count);
 }
 
