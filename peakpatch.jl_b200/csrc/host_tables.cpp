@@ -105,9 +105,15 @@ void build_shell_table(ShellTable& st, int nhunt) {
   st.sh_c0.assign(st.nshell + 1, 0);
   st.sh_nc.assign(st.nshell + 1, 0);
   int in_group = 0;
+  // chunk size: kChunkCells, smaller (down to 4 cells) when the whole list
+  // would leave most of the 32 lanes of one group idle (small nhunt: few,
+  // small shells), so that the lanes split the cells of each shell
+  int total = 0;
+  for (int m = 2; m <= mmax; m++) total += st.shell_count[m - 1];
+  const int csize = std::min(kChunkCells, std::max(4, 4 * ((total + 127) / 128)));
   for (int m = 2; m <= mmax; m++) {
     const int cnt = st.shell_count[m - 1], s0 = st.shell_start[m - 1];
-    int nck = (cnt + kChunkCells - 1) / kChunkCells;
+    int nck = (cnt + csize - 1) / csize;
     if (nck > 32) nck = 32;
     if (nck < 1) nck = 1;
     if (in_group + nck > 32 || st.grp_a.empty()) {   // open a new group

@@ -77,7 +77,7 @@ struct DevBuf {
 // ---------------------------------------------------------------------------
 // geometry of the sorted shell-cell list (precompute_shells)
 // ---------------------------------------------------------------------------
-constexpr int kChunkCells = 24;   // gather chunk size (cells per lane per group)
+constexpr int kChunkCells = 24;   // gather chunk size (cells per lane per group; smaller for short lists)
 
 struct ShellTable {
   int nhunt = -1;

@@ -174,6 +174,24 @@ def test_analyse_peaks_vs_oracle(ctx, shell_case, julia_table, plain):
     assert st["visits"] > 0
 
 
+@pytest.mark.parametrize("nhunt", [2, 3, 5])
+def test_analyse_peaks_short_shell_lists(ctx, ora, shell_case, julia_table, nhunt):
+    # short shell lists (cells 1.5-5 Mpc/h wide against the filter radii, as in
+    # the reference's multi-resolution sweep) get smaller gather chunks
+    c = shell_case
+    ctx.set_collapse_table(pp.CollapseTable(julia_table.data, julia_table.x1, julia_table.x2, julia_table.y1,
+                                            julia_table.y2, julia_table.z1, julia_table.z2))
+    o = ora.analyse_peaks(c["fields"], c["ipp"], c["Rf"], c["ir2"], 1.0, c["fcrit"], c["alatt"],
+                          ora.precompute_shells(nhunt), julia_table)
+    assert (o[:, 0] > 0).sum() > 20
+    for plain in (False, True):
+        g = ctx.analyse_peaks(c["fields"], c["ipp"], c["Rf"], c["ir2"], 1.0, c["fcrit"], c["alatt"], nhunt,
+                              plain=plain)
+        frac, errs = compare_results(g, o)
+        assert frac <= MISMATCH, (nhunt, plain, frac, errs)
+        assert errs["RTHL"] < RTOL
+
+
 def test_adaptive_truncation_reads_fewer_cells(ctx, shell_case, julia_table):
     c = shell_case
     ctx.set_collapse_table(pp.CollapseTable(julia_table.data, julia_table.x1, julia_table.x2, julia_table.y1,
