@@ -43,6 +43,17 @@ def test_split_vs_oracle(sctx, ora, julia_table, eh_pk, ilpt, ioutshear):
     _check(rg, ro, 33 if ioutshear else 11)
 
 
+@pytest.mark.parametrize("n,nbuff,ntile", [(64, 16, 1), (63, 15, 2)])
+def test_split_geometries_vs_oracle(sctx, ora, julia_table, eh_pk, n, nbuff, ntile):
+    # one tile (N = nmesh), and an odd tile size (odd periodic grids, padded
+    # boxes of 2 n)
+    cfg = tile_config(n=n, box=2.0 * n, nbuff=nbuff)
+    rg, _, npk = sctx.run_multitile_split_arrays(cfg, 8, RF, ntile=ntile)
+    ro, npk_o = ora.run_multitile_split(ora_config(ora, cfg), 8, *eh_pk, filter_bank(), julia_table, ntile=ntile)
+    assert abs(npk - npk_o) <= max(3, 0.002 * npk_o)
+    _check(rg, ro)
+
+
 def test_split_lightcone_vs_oracle(sctx, ora, julia_table, eh_pk):
     # ievol = 1: fcrit of each tile centre's redshift, per-peak redshifts
     cfg = tile_config(ievol=1, z_out=0.0, z_max=0.3)
