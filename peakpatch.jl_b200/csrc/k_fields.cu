@@ -211,9 +211,8 @@ __global__ void window_table_kernel(float* __restrict__ tab, int qn, double dkk,
     w0 = (float)window_w(fkR, k, wsmooth);
     if (want_lap) w1 = (float)window_w(fkR, k, 3);
   }
-  float* t = tab + (int64_t)f * 2 * qn;
-  t[q] = w0;
-  t[qn + q] = w1;
+  // (W_wsmooth, W_3 k^2) side by side: one 8-byte load per mode serves both
+  reinterpret_cast<float2*>(tab + (int64_t)f * 2 * qn)[q] = make_float2(w0, w1);
 }
 
 // four modes per thread (r, r + 256, r + 512, r + 768 of one kz plane): four
@@ -246,10 +245,11 @@ __global__ void __launch_bounds__(256) window_kernel(const float2* __restrict__ 
   for (int u = 0; u < kWinPerThread; u++) {
     if (q[u] < 0) continue;
     const int64_t id = base + r0 + 256 * u;
-    const float w0 = __ldg(tab + q[u]);
+    const float2 w = __ldg(reinterpret_cast<const float2*>(tab) + q[u]);
+    const float w0 = w.x;
     out0[id] = make_float2(__fmul_rn(__fmul_rn(d[u].x, w0), ps), __fmul_rn(__fmul_rn(d[u].y, w0), ps));
     if (out1) {
-      const float w1 = __ldg(tab + qn + q[u]);
+      const float w1 = w.y;
       out1[id] = make_float2(__fmul_rn(__fmul_rn(d[u].x, w1), ps), __fmul_rn(__fmul_rn(d[u].y, w1), ps));
     }
   }

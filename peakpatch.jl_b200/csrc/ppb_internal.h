@@ -262,9 +262,9 @@ void launch_phi(Launch L, const float2* dk, float2* out, int n, double boxsize, 
 void launch_src2(Launch L, const float* phi, float* out, int64_t N);
 void launch_lpt2(Launch L, const float2* s2k, float2* out, int n, double boxsize, double post_scale);
 void launch_lapd(Launch L, const float2* dk, float2* out, int n, double boxsize, float post_scale);
-// window tables: per filter f, 2 * window_table_size(n) floats at
-// tab + f * 2 * window_table_size(n) (W_wsmooth, then the k^2-weighted
-// Gaussian of the Laplacian diagnostic); Rf is a device array of nfilt radii
+// window tables: per filter f, window_table_size(n) float pairs (W_wsmooth,
+// the k^2-weighted Gaussian of the Laplacian diagnostic) by integer |k|^2 at
+// tab + f * 2 * window_table_size(n); Rf is a device array of nfilt radii
 int window_table_size(int n);
 void launch_window_tables(Launch L, float* tab, int n, double boxsize, const double* Rf, int nfilt, int wsmooth,
                           bool want_lap);
