@@ -604,11 +604,16 @@ def run_split_bench(args, dist: Dist):
         t_wall.append(dist.max(time.perf_counter() - t0))
         t_dev.append(dist.max(a))
     stage = ctx.stage_ms()
-    nh = dist.sum(float(len(rec)))
+    full = rec
+    if dist.world > 1:   # rank 0 gathers the last run's records in tile order
+        dcore = nsub * (box / nm)
+        parts = dict(zip(mine, D.split_by_tile(rec, mine, ntile, dcore)))
+        full = D.gather_tile_records(parts, tiles, 11)
     npk_all = dist.sum(float(npk))
     ctx.close()
     if dist.rank != 0:
         return None
+    nh = len(full)
     td, tw = statistics.median(t_dev), statistics.median(t_wall)
     pub = SPLIT_PUBLISHED.get(nm)
     line = {"metric": "tiles/s (run_multitile_split)", "value": len(tiles) / td, "unit": "tiles/s",
@@ -624,7 +629,8 @@ def run_split_bench(args, dist: Dist):
                     "d2h_bytes_per_step": int(nh) * 11 * 4},
             "halos": int(nh), "peaks": int(npk_all), "stage_ms_rank0_last_run": stage,
             "note": "value: device time (CUDA events on the library stream) of the slowest rank's run; e2e: wall "
-                    "clock of the Python call, records copied to the host"}
+                    "clock of the Python call, records copied to the host (the records gather between ranks "
+                    "follows the timed runs)"}
     if pub:
         line["reference_published"] = {"per_tile_s": pub[0], "tiles_per_s": 1.0 / pub[0], "halos": pub[1],
                                        "hardware": "RTX A5000 (the reference's GPU scaling sweep)"}
