@@ -365,6 +365,15 @@ TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool ad
   return te;
 }
 
+// grow b to at least `need` bytes with 50 % headroom (at most `limit`):
+// buffers sized by the peak count of a request then rarely grow again in a
+// stream of requests whose counts vary, and every growth's cudaFree waits
+// for all work on the device, other slots' included
+static void grow(DevBuf& b, size_t need, size_t limit = ~(size_t)0) {
+  if (need <= b.bytes) return;
+  b.ensure(std::max(need, std::min(need + need / 2, limit)));
+}
+
 void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, ShellStats* st,
                          const std::function<void()>& pre) {
   cudaStream_t stream = sl.stream;
@@ -376,9 +385,9 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
   sl.stage.ensure((size_t)((int64_t)gblocks * kGatherWarps * stride * 8));
   sl.counters.ensure(16 * 8);
   sl.ctl.ensure(64);
-  sl.hdr.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(PeakHdr));
-  sl.geo.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(int4));
-  sl.mlim.ensure(std::max<size_t>(1, (size_t)a.npk) * sizeof(int32_t));
+  grow(sl.hdr, std::max<size_t>(1, (size_t)a.npk) * sizeof(PeakHdr));
+  grow(sl.geo, std::max<size_t>(1, (size_t)a.npk) * sizeof(int4));
+  grow(sl.mlim, std::max<size_t>(1, (size_t)a.npk) * sizeof(int32_t));
   PPB_CUDA(cudaMemsetAsync(sl.counters.p, 0, 16 * 8, stream));
   // profile pool: sized from the rows per peak of the previous call; peaks
   // run in batches that fit the pool budget, and a batch whose rows overflow
@@ -418,7 +427,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     const double want = std::max(1.0, rpp * 1.25);
     int64_t nb = std::min<int64_t>(a.npk - p0, std::max<int64_t>(1, (int64_t)((double)budget_rows / want)));
     const int64_t cap = std::min<int64_t>(budget_rows, (int64_t)((double)nb * want) + 4096);
-    sl.pool.ensure((size_t)cap * row_bytes);
+    grow(sl.pool, (size_t)cap * row_bytes, (size_t)budget_rows * row_bytes);
     ShellArgs b = a;
     b.pk.lin = a.pk.lin + p0;
     b.pk.Rf = a.pk.Rf + p0;
@@ -442,16 +451,16 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     b.brick_shift = 3;
     for (int e = 0; e < 10; e++) b.fhalf[e] = std::pow(e / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
     // buffers of the spatial order (allocated before any capture)
-    sl.okey.ensure(nb * 4 + 16);
-    sl.okey2.ensure(nb * 4 + 16);
-    sl.oidx.ensure(nb * 4 + 16);
-    sl.oidx2.ensure(nb * 4 + 16);
+    grow(sl.okey, nb * 4 + 16);
+    grow(sl.okey2, nb * 4 + 16);
+    grow(sl.oidx, nb * 4 + 16);
+    grow(sl.oidx2, nb * 4 + 16);
     {
       size_t tb = 0;
       PPB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, sl.okey.as<uint32_t>(), sl.okey2.as<uint32_t>(),
                                                sl.oidx.as<int32_t>(), sl.oidx2.as<int32_t>(), (int)nb, 0, 32,
                                                stream));
-      sl.otmp.ensure(tb + 16);
+      grow(sl.otmp, tb + 16);
     }
     if (tune_now) {
       if (first && pre) pre();   // the tuning pass reads what `pre` writes

@@ -232,6 +232,8 @@ void generate_fields_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, floa
 uint64_t tile_footprint(const ppb_tile_params* p);
 // the part of it held per grid size (TileRes) and per slot (shell stage)
 uint64_t tile_bytes_estimate(int n);
+// peak-buffer capacity given to a grid of N cells on its first run
+int64_t initial_peak_capacity(int64_t N);
 uint64_t shell_bytes_estimate(int n);
 // copy `bytes` from device memory to dst (host or device)
 void copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);

@@ -324,13 +324,20 @@ void check_params(const ppb_tile_params* p, const double* Rf, int nfilt) {
 
 uint64_t tile_footprint(const ppb_tile_params* p) { return tile_bytes_estimate(p->n) + shell_bytes_estimate(p->n); }
 
+// Peak buffers of a grid of N cells before the first run: one peak per 40
+// cells.  The 384^3 benchmark tile has one per 66 cells at sigma8 0.808 and
+// about 10 % more at 0.85; starting with room for them means a served stream
+// of varying sigma8 does not grow the buffers (every cudaFree of a growth
+// waits for all slots' work on the device).  A larger count still grows them.
+int64_t initial_peak_capacity(int64_t N) { return std::max<int64_t>(1 << 16, std::min<int64_t>(N / 40, 1 << 22)); }
+
 uint64_t tile_bytes_estimate(int nn) {
   const uint64_t n = (uint64_t)nn, N = n * n * n, M = (n / 2 + 1) * n * n;
   // TileRes fields: delta, psi (3), psi2 (3), lapd, rw (6), mask, aos (8 floats), dk + kw (7 complex)
   const uint64_t fields = N * 4 * (1 + 3 + 3 + 1 + 6) + N + N * 32 + M * 8 * 7;
-  // peak, result and record buffers: about 1/64 peak per cell, 0.5 KB each;
-  // plans and their work areas
-  return fields + N * 8 + ((uint64_t)64 << 20);
+  // peak, result and record buffers: initial_peak_capacity (1/40 peak per
+  // cell), 0.5 KB each; plans and their work areas
+  return fields + N * 13 + ((uint64_t)64 << 20);
 }
 
 uint64_t shell_bytes_estimate(int nn) {
@@ -678,7 +685,7 @@ void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const doubl
   TileRes& T = sl.tile_for(n);
   T.setup(n, r.s);
   T.aos.ensure(N * 32);
-  if (T.cap == 0) T.ensure_peaks(std::max<int64_t>(1 << 16, std::min<int64_t>(N / 64, 1 << 22)));
+  if (T.cap == 0) T.ensure_peaks(initial_peak_capacity(N));
   cudaEvent_t* ev = sl.stage_ev;
   PPB_CUDA(cudaEventRecord(ev[0], r.s));
   // fields and the packed gather records as one graph
@@ -788,7 +795,7 @@ void run_multitile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const 
   }
   TileRes& T = sl.tile_for(n);
   T.setup(n, r.s);
-  if (T.cap == 0) T.ensure_peaks(std::max<int64_t>(1 << 16, std::min<int64_t>(N / 64, 1 << 22)));
+  if (T.cap == 0) T.ensure_peaks(initial_peak_capacity(N));
   sl.tcen.ensure(tcen.size() * 8);
   PPB_CUDA(cudaMemcpyAsync(sl.tcen.p, tcen.data(), tcen.size() * 8, cudaMemcpyHostToDevice, r.s));
   cudaEvent_t* ev = sl.stage_ev;
@@ -979,7 +986,7 @@ void run_multitile_split_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, 
   TileRes& T = sl.tile_for(nm);
   T.setup(nm, r.s);
   T.aos.ensure(Nt * 32);
-  if (T.cap == 0) T.ensure_peaks(std::max<int64_t>(1 << 16, std::min<int64_t>(Nt / 64, 1 << 22)));
+  if (T.cap == 0) T.ensure_peaks(initial_peak_capacity(Nt));
   const int nf = p->ioutshear >= 1 ? 33 : 11;
   size_t used = 0;
   int64_t nrec_tot = 0, npk_tot = 0;
