@@ -18,7 +18,12 @@ namespace ppb {
 struct TileRes {
   int n = 0;
   cufftHandle r2c = 0, c2r1 = 0, c2r2 = 0, c2r3 = 0, c2r6 = 0;
+  // in-place inverse C2C of contiguous n x n (kz, ky) planes, batched over
+  // the n/2+1 kx of one field (yz1) or of two fields back to back (yz2): the
+  // filter bank's transforms before the fused x pass (0 where unsupported)
+  cufftHandle yz1 = 0, yz2 = 0;
   DevBuf delta, dk, psi, psi2, lapd, aos, kw, rw, mask, count, wtab;
+  DevBuf xtw;   // exp(2 pi i k / n), k < n: the fused x pass's twiddles
   // peaks
   int64_t cap = 0;
   DevBuf keys, vals, ff, lap, keys_s, vals_s, tmp;

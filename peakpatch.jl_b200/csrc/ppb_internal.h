@@ -296,6 +296,19 @@ struct PeakBuf {
 // them); key = keyhi << 40 | (window-local flat index)
 void launch_peakfind(Launch L, const float* ds, const float* ls, uint8_t* mask, int n1, int n2, int n3,
                      int64_t py, int64_t pz, int nbuff, float fcrit, unsigned long long keyhi, PeakBuf pb);
+// the filter bank's x pass fused with the peak search (k_xpeak.cu): ds (and
+// ls) hold half spectra in [kx][z][y] order (window_t output) already
+// transformed back along z and y; one window over the whole n^3 grid.
+// Supported for n = 64 J, J = 1..8, nbuff >= 1.
+bool xpeak_supported(int n, int nbuff);
+void xpeak_prepare(int n);
+void launch_window_t(Launch L, const float2* dk, float2* out0, float2* out1, int n, const float* tab,
+                     double post_scale);
+// tw[k] = exp(2 pi i k / n), k < n (the fused x pass's twiddles)
+void launch_twiddles(Launch L, float2* tw, int n);
+// first: device word the launch resets and lowers to the first slot it appends
+void launch_xpeak(Launch L, const float2* ds, const float2* ls, const float2* tw, uint8_t* mask, unsigned* first,
+                  int n, int nbuff, float fcrit, unsigned long long keyhi, PeakBuf pb);
 
 // Shell stage = five launches on one stream:
 //  geo      (one thread per peak): per-peak shell geometry

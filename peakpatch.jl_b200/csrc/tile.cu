@@ -235,13 +235,13 @@ TileRes::~TileRes() {
   for (auto& g : graphs)   // before the plans whose kernels they launch
     if (g.second) cudaGraphExecDestroy(g.second);
   graphs.clear();
-  for (cufftHandle h : {r2c, c2r1, c2r2, c2r3, c2r6})
+  for (cufftHandle h : {r2c, c2r1, c2r2, c2r3, c2r6, yz1, yz2})
     if (h) cufftDestroy(h);
 }
 
 void TileRes::setup(int nn, cudaStream_t s) {
   if (n == nn) return;
-  for (cufftHandle* h : {&r2c, &c2r1, &c2r2, &c2r3, &c2r6})
+  for (cufftHandle* h : {&r2c, &c2r1, &c2r2, &c2r3, &c2r6, &yz1, &yz2})
     if (*h) { cufftDestroy(*h); *h = 0; }
   n = nn;
   const int64_t N = (int64_t)n * n * n, M = (int64_t)(n / 2 + 1) * n * n;
@@ -251,6 +251,15 @@ void TileRes::setup(int nn, cudaStream_t s) {
   c2r3 = make_plan(n, CUFFT_C2R, 3);
   c2r6 = make_plan(n, CUFFT_C2R, 6);
   for (cufftHandle h : {r2c, c2r1, c2r2, c2r3, c2r6}) PPB_CUFFT(cufftSetStream(h, s));
+  if (xpeak_supported(n, 1)) {
+    int dims[2] = {n, n};
+    const int nh = n / 2 + 1;
+    PPB_CUFFT(cufftPlanMany(&yz1, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, nh));
+    PPB_CUFFT(cufftPlanMany(&yz2, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, 2 * nh));
+    for (cufftHandle h : {yz1, yz2}) PPB_CUFFT(cufftSetStream(h, s));
+    xpeak_prepare(n);
+    xtw.ensure((size_t)n * sizeof(float2));
+  }
   delta.ensure(N * 4);
   dk.ensure(M * 8);
   psi.ensure(3 * N * 4);
@@ -479,6 +488,10 @@ int64_t peaks_phase(Run& r, TileRes& T, int n, double box, const std::vector<Win
   float* rw = T.rw.as<float>();
   const int qn = window_table_size(n);
   T.wtab.ensure((size_t)r.nfilt * 2 * qn * sizeof(float));
+  // one window over the whole grid (every caller) and a supported size: the
+  // x pass of each filter's transform runs fused with the peak search
+  const bool fused = !r.plain && T.yz1 && xpeak_supported(n, p->nbuff) && wins.size() == 1 && wins[0].off == 0 &&
+                     nm == n;
   int64_t npk = 0;
   for (int attempt = 0; attempt < 2; attempt++) {
     PeakBuf pb{T.keys.as<unsigned long long>(), T.vals.as<uint32_t>(), T.ff.as<float>(), T.lap.as<float>(),
@@ -490,8 +503,18 @@ int64_t peaks_phase(Run& r, TileRes& T, int n, double box, const std::vector<Win
       PPB_CUDA(cudaMemsetAsync(T.count.p, 0, 64, r.s));
       launch_window_tables(L, T.wtab.as<float>(), n, box, r.sl->filt_Rf.as<double>(), r.nfilt, p->wsmooth,
                            r.want_lap);
+      if (fused) launch_twiddles(L, T.xtw.as<float2>(), n);
       for (int f = 0; f < r.nfilt; f++) {
         float2* o1 = r.want_lap ? kw + M : nullptr;
+        if (fused) {
+          // window multiply into [kx][kz][ky], z and y by cuFFT (both fields
+          // in one call), then x and the peak search in one kernel
+          launch_window_t(L, dkp, kw, o1, n, T.wtab.as<float>() + (size_t)f * 2 * qn, inv_n3);
+          PPB_CUFFT(cufftExecC2C(o1 ? T.yz2 : T.yz1, (cufftComplex*)kw, (cufftComplex*)kw, CUFFT_INVERSE));
+          launch_xpeak(L, kw, o1, T.xtw.as<float2>(), T.mask.as<uint8_t>(), T.count.as<unsigned>() + 2, n,
+                       p->nbuff, wins[0].fcrit, (unsigned long long)f, pb);
+          continue;
+        }
         launch_window(L, dkp, kw, o1, n, T.wtab.as<float>() + (size_t)f * 2 * qn, inv_n3);
         if (r.want_lap && !r.plain) {
           PPB_CUFFT(cufftExecC2R(T.c2r2, (cufftComplex*)kw, rw));

@@ -368,3 +368,26 @@ def test_run_tile_file_api(ctx, tmp_path, eh_pk):
     r2, rthl, zo = pp.read_pksc(cfg.fileout)
     assert rec.tobytes() == r2.tobytes() and zo == 0.0   # bit for bit, NaN fields included
     assert rthl == pytest.approx(rec[:, 6].max()) if len(rec) else rthl == 0.0
+
+
+@pytest.mark.parametrize("n,nbuff,ioutshear,seed", [(128, 5, 1, 3), (192, 12, 1, 8), (256, 32, 0, 11)])
+def test_fused_filter_bank_matches_full_transforms(ctx, eh_pk, julia_table, n, nbuff, ioutshear, seed):
+    """The filter bank with cuFFT's z/y passes and the fused x pass + peak
+    search (grid sizes 64 J) against the path with full 3-D C2R transforms and
+    the separate peak search: the same peaks up to single-precision FFT
+    rounding, the same halos within the oracle bars."""
+    cfg = tile_config(n=n, box=2.0 * n, nbuff=nbuff, ioutshear=ioutshear)
+    filters = filter_bank()
+    T = julia_table
+    ctx.set_pk_table(*eh_pk)
+    ctx.set_collapse_table(pp.CollapseTable(T.data, T.x1, T.x2, T.y1, T.y2, T.z1, T.z2))
+    rf = [f[2] for f in filters]
+    fused, rmax_f, npk_f = ctx.run_tile_arrays(cfg, seed, rf, plain=False)
+    full, rmax_p, npk_p = ctx.run_tile_arrays(cfg, seed, rf, plain=True)
+    nf = 33 if ioutshear else 11
+    assert fused.shape[1] == nf and len(full) > 100
+    assert abs(npk_f - npk_p) <= max(2, 0.002 * npk_p), (npk_f, npk_p)
+    frac, errs = match_records(fused, full, nf)
+    assert frac <= MISMATCH * 3, (frac, errs)
+    assert errs["RTHL"] < RTOL, errs
+    assert rmax_f == pytest.approx(rmax_p, rel=RTOL)
