@@ -43,7 +43,9 @@ struct RowConsts {
   float2 pre[J];   // w^(l + 32 j), w = exp(2 pi i / n)
   float2 wj[J];    // exp(2 pi i m / J) = w^(64 m)
   float2 mid[J];   // exp(2 pi i l q / H) = w^(2 l q)
-  float2 st[4];    // stage twiddles exp(2 pi i (l mod h) / (2 h)) = w^(n (l mod h) / (2 h)), h = 16, 8, 4, 2
+  float2 st[4];    // stage twiddles: exp(2 pi i (l mod h) / (2 h)) = w^(n (l mod h) / (2 h)) on the
+                   // upper lane of each pair (l & h), 1 on the lower, h = 16, 8, 4, 2
+  float sg[5];     // -1 on the upper lane of stage h = 16 >> s, +1 on the lower
 };
 
 // tw[k] = w^k, k < n (twiddle_kernel)
@@ -57,9 +59,87 @@ __device__ __forceinline__ void row_consts(RowConsts<J>& c, int l, const float2*
     c.mid[j] = __ldg(tw + (2 * l * j) % n);
   }
 #pragma unroll
-  for (int s = 0; s < 4; s++) {
+  for (int s = 0; s < 5; s++) {
     const int h = 16 >> s;
-    c.st[s] = __ldg(tw + (n / (2 * h)) * (l % h));
+    const bool up = (l & h) != 0;
+    if (s < 4) c.st[s] = up ? __ldg(tw + (n / (2 * h)) * (l % h)) : make_float2(1.f, 0.f);
+    c.sg[s] = up ? -1.f : 1.f;
+  }
+}
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul_i(float2 a) { return make_float2(-a.y, a.x); }   // i a
+
+constexpr float kHalfSqrt3 = 0.8660254037844386f;   // sin(pi/3)
+constexpr float kHalfSqrt2 = 0.7071067811865476f;   // cos(pi/4)
+
+// A[q] = sum_j z[j] exp(2 pi i j q / J): butterflies for J = 1, 2, 3, 4, 6, 8
+// (6 = 2 x 3 and 8 = 2 x 4 by one radix-2 step), the direct sum with table
+// twiddles wj otherwise
+__device__ __forceinline__ void dft3(const float2 a0, const float2 a1, const float2 a2, float2& o0, float2& o1,
+                                     float2& o2) {
+  const float2 t = cadd(a1, a2);
+  const float2 m = make_float2(fmaf(-0.5f, t.x, a0.x), fmaf(-0.5f, t.y, a0.y));
+  const float2 d = csub(a1, a2);
+  const float2 isd = make_float2(-kHalfSqrt3 * d.y, kHalfSqrt3 * d.x);
+  o0 = cadd(a0, t);
+  o1 = cadd(m, isd);
+  o2 = csub(m, isd);
+}
+
+__device__ __forceinline__ void dft4(const float2 a0, const float2 a1, const float2 a2, const float2 a3, float2& o0,
+                                     float2& o1, float2& o2, float2& o3) {
+  const float2 s02 = cadd(a0, a2), d02 = csub(a0, a2), s13 = cadd(a1, a3), d13 = cmul_i(csub(a1, a3));
+  o0 = cadd(s02, s13);
+  o2 = csub(s02, s13);
+  o1 = cadd(d02, d13);
+  o3 = csub(d02, d13);
+}
+
+template <int J>
+__device__ __forceinline__ void dft_small(const float2 (&z)[J], float2 (&A)[J], const float2 (&wj)[J]) {
+  if constexpr (J == 1) {
+    A[0] = z[0];
+  } else if constexpr (J == 2) {
+    A[0] = cadd(z[0], z[1]);
+    A[1] = csub(z[0], z[1]);
+  } else if constexpr (J == 3) {
+    dft3(z[0], z[1], z[2], A[0], A[1], A[2]);
+  } else if constexpr (J == 4) {
+    dft4(z[0], z[1], z[2], z[3], A[0], A[1], A[2], A[3]);
+  } else if constexpr (J == 6) {
+    float2 e[3], o[3];
+    dft3(z[0], z[2], z[4], e[0], e[1], e[2]);
+    dft3(z[1], z[3], z[5], o[0], o[1], o[2]);
+    const float2 w1 = make_float2(0.5f, kHalfSqrt3), w2 = make_float2(-0.5f, kHalfSqrt3);   // exp(i pi q / 3)
+    const float2 t1 = cmul(o[1], w1), t2 = cmul(o[2], w2);
+    A[0] = cadd(e[0], o[0]); A[3] = csub(e[0], o[0]);
+    A[1] = cadd(e[1], t1);   A[4] = csub(e[1], t1);
+    A[2] = cadd(e[2], t2);   A[5] = csub(e[2], t2);
+  } else if constexpr (J == 8) {
+    float2 e[4], o[4];
+    dft4(z[0], z[2], z[4], z[6], e[0], e[1], e[2], e[3]);
+    dft4(z[1], z[3], z[5], z[7], o[0], o[1], o[2], o[3]);
+    const float2 t1 = make_float2(kHalfSqrt2 * (o[1].x - o[1].y), kHalfSqrt2 * (o[1].x + o[1].y));    // exp(i pi/4) o1
+    const float2 t2 = cmul_i(o[2]);
+    const float2 t3 = make_float2(-kHalfSqrt2 * (o[3].x + o[3].y), kHalfSqrt2 * (o[3].x - o[3].y));   // exp(3 i pi/4) o3
+    A[0] = cadd(e[0], o[0]); A[4] = csub(e[0], o[0]);
+    A[1] = cadd(e[1], t1);   A[5] = csub(e[1], t1);
+    A[2] = cadd(e[2], t2);   A[6] = csub(e[2], t2);
+    A[3] = cadd(e[3], t3);   A[7] = csub(e[3], t3);
+  } else {
+#pragma unroll
+    for (int q = 0; q < J; q++) {
+      float2 acc = z[0];
+#pragma unroll
+      for (int j = 1; j < J; j++) {
+        const float2 w = wj[(j * q) % J];
+        acc.x = fmaf(z[j].x, w.x, fmaf(-z[j].y, w.y, acc.x));
+        acc.y = fmaf(z[j].x, w.y, fmaf(z[j].y, w.x, acc.y));
+      }
+      A[q] = acc;
+    }
   }
 }
 
@@ -93,32 +173,21 @@ __device__ __forceinline__ void row_irfft(const RowConsts<J>& c, int l, const fl
     z[j] = make_float2(e.x - o.y, e.y + o.x);             // e + i o
   }
   float2 b[J];
+  dft_small<J>(z, b, c.wj);
 #pragma unroll
-  for (int q = 0; q < J; q++) {
-    float2 acc = z[0];
-#pragma unroll
-    for (int j = 1; j < J; j++) {
-      const float2 w = c.wj[(j * q) % J];
-      acc.x = fmaf(z[j].x, w.x, fmaf(-z[j].y, w.y, acc.x));
-      acc.y = fmaf(z[j].x, w.y, fmaf(z[j].y, w.x, acc.y));
-    }
-    b[q] = q == 0 ? acc : cmul(acc, c.mid[q]);
-  }
+  for (int q = 1; q < J; q++) b[q] = cmul(b[q], c.mid[q]);
+  // radix-2 steps across lanes: the lower lane of a pair keeps a + b, the
+  // upper (a - b) times its twiddle, a being the lower lane's value
 #pragma unroll
   for (int s = 0; s < 5; s++) {
     const int h = 16 >> s;
-    const bool up = (l & h) != 0;
 #pragma unroll
     for (int q = 0; q < J; q++) {
       float2 p;
       p.x = __shfl_xor_sync(full, b[q].x, h);
       p.y = __shfl_xor_sync(full, b[q].y, h);
-      if (up) {
-        const float2 t = make_float2(p.x - b[q].x, p.y - b[q].y);
-        b[q] = s < 4 ? cmul(t, c.st[s]) : t;
-      } else {
-        b[q] = make_float2(b[q].x + p.x, b[q].y + p.y);
-      }
+      const float2 t = make_float2(fmaf(c.sg[s], b[q].x, p.x), fmaf(c.sg[s], b[q].y, p.y));
+      b[q] = s < 4 ? cmul(t, c.st[s]) : t;
     }
   }
   const int p = __brev(l) >> 27;
@@ -147,8 +216,8 @@ __global__ void __launch_bounds__(kXpThreads, 1) xpeak_kernel(XpArgs a) {
   float* ring = reinterpret_cast<float*>(smem);                                    // [4][kXpRows][n]
   long long* lloc = reinterpret_cast<long long*>(smem + 4 * kXpRows * n * 4);      // [16][kXpList]
   float* lf = reinterpret_cast<float*>(lloc + 16 * kXpList);                        // [16][kXpList]
-  float2* stg = reinterpret_cast<float2*>(lf + 16 * kXpList);                       // [nh][kXpPad]
-  uint8_t* mbuf = reinterpret_cast<uint8_t*>(stg + nh * kXpPad);                    // [2][kXpInner][n]
+  float2* stg = reinterpret_cast<float2*>(lf + 16 * kXpList);                       // [2][nh][kXpPad]
+  uint8_t* mbuf = reinterpret_cast<uint8_t*>(stg + 2 * nh * kXpPad);                // [2][kXpInner][n]
   const int tid = threadIdx.x, l = tid & 31, warp = tid >> 5;
   const int nb = a.nbuff, hi = n - nb;
   const int y0 = nb + blockIdx.x * kXpInner;
@@ -162,7 +231,7 @@ __global__ void __launch_bounds__(kXpThreads, 1) xpeak_kernel(XpArgs a) {
   row_consts<J>(c, l, a.tw);
   // rows y0 - 1 .. y0 - 2 + R of plane z: per kx one contiguous run of R
   // float2, two kx per warp step (half-warps)
-  auto stage_plane = [&](int z) {
+  auto stage_plane = [&](float2* stg, int z) {
     const float2* src = a.ds + (int64_t)n * z + (y0 - 1);
     const int r = l & 15;
     for (int kx = 2 * warp + (l >> 4); kx < nh; kx += 2 * (kXpThreads / 32)) {
@@ -209,56 +278,58 @@ __global__ void __launch_bounds__(kXpThreads, 1) xpeak_kernel(XpArgs a) {
     __syncwarp();
     wn = 0;
   };
-  stage_plane(z0 - 1);
+  // iteration i: ring plane i (z = z0 - 1 + i) is transformed from staging
+  // buffer i & 1 into ring slot i & 3 while plane i - 2 is searched between
+  // slots i - 3 and i - 1; one barrier per iteration.  Staging buffer
+  // (i + 1) & 1 and mask buffer (i + 1) & 1 are filled during iteration i.
+  stage_plane(stg, z0 - 1);
   asm volatile("cp.async.commit_group;\n" ::);
-  for (int i = 0; i < NP; i++) {
+  const int W = hi - nb, nxc = (W + 31) / 32, nchunk = yi * nxc;
+  for (int i = 0; i <= NP; i++) {
     asm volatile("cp.async.wait_all;\n" ::);
-    __syncthreads();   // plane i staged, the mask of the plane searched below staged
-    float* slot = ring + (i & 3) * kXpRows * n;
-    if (warp < R) {
-      float2 x[J], xh;
-      row_load<J>(stg, warp, l, x, xh);
-      row_irfft<J>(c, l, x, xh, slot + warp * n);
-    }
-    __syncthreads();   // ring slot i complete; the staging buffer is free
-    if (i + 1 < NP) stage_plane(z0 + i);
-    if (i + 1 >= 2 && i + 1 < NP) stage_mask(mbuf + ((i + 1) & 1) * kXpInner * n, z0 - 1 + i);
+    __syncthreads();
+    if (i + 1 < NP) stage_plane(stg + ((i + 1) & 1) * nh * kXpPad, z0 + i);
+    if (i + 1 >= 3 && i + 1 <= NP) stage_mask(mbuf + ((i + 1) & 1) * kXpInner * n, z0 - 2 + i);
     asm volatile("cp.async.commit_group;\n" ::);
-    if (i < 2) continue;
-    // search plane z = z0 - 2 + i (ring slot i - 1) between slots i - 2 and i
-    const int z = z0 - 2 + i;
-    const float* s0 = ring + ((i - 2) & 3) * kXpRows * n;
-    const float* s1 = ring + ((i - 1) & 3) * kXpRows * n;
-    const float* s2 = slot;
+    if (i < NP && warp < R) {
+      float2 x[J], xh;
+      row_load<J>(stg + (i & 1) * nh * kXpPad, warp, l, x, xh);
+      row_irfft<J>(c, l, x, xh, ring + (i & 3) * kXpRows * n + warp * n);
+    }
+    if (i < 3) continue;
+    const int z = z0 - 3 + i;
+    const float* s0 = ring + ((i - 3) & 3) * kXpRows * n;
+    const float* s1 = ring + ((i - 2) & 3) * kXpRows * n;
+    const float* s2 = ring + ((i - 1) & 3) * kXpRows * n;
     const uint8_t* mk = mbuf + (i & 1) * kXpInner * n;
-    for (int ri = 1 + warp; ri <= yi; ri += kXpThreads / 32) {
+    // chunks of 32 cells of one row, spread over all warps
+    for (int ch = warp; ch < nchunk; ch += kXpThreads / 32) {
+      const int ri = 1 + ch / nxc;
+      const int x = nb + 32 * (ch % nxc) + l;
       const int y = y0 - 1 + ri;
-      for (int xb = nb; xb < hi; xb += 32) {
-        const int x = xb + l;
-        bool peak = false;
-        float f = 0.f;
-        if (x < hi) {
-          f = s1[ri * n + x];
-          if (!(f < a.fcrit) && mk[(ri - 1) * n + x] != 1) {
-            peak = true;
-            for (int q = 0; q < 9; q++) {
-              const int o = (ri + q / 3 - 1) * n + x + q % 3 - 1;
-              if (f < s0[o] || f < s1[o] || f < s2[o]) { peak = false; break; }
-            }
+      bool peak = false;
+      float f = 0.f;
+      if (x < hi) {
+        f = s1[ri * n + x];
+        if (!(f < a.fcrit) && mk[(ri - 1) * n + x] != 1) {
+          peak = true;
+          for (int q = 0; q < 9; q++) {
+            const int o = (ri + q / 3 - 1) * n + x + q % 3 - 1;
+            if (f < s0[o] || f < s1[o] || f < s2[o]) { peak = false; break; }
           }
         }
-        const unsigned ball = __ballot_sync(full, peak);
-        if (ball == 0) continue;
-        if (peak) {
-          const long long loc = x + (long long)n * y + nn * z;
-          const int e = wn + __popc(ball & ((1u << l) - 1u));
-          a.mask[loc] = 1;
-          myloc[e] = loc;
-          myf[e] = f;
-        }
-        wn += __popc(ball);
-        if (wn > kXpList - 32) flush();
       }
+      const unsigned ball = __ballot_sync(full, peak);
+      if (ball == 0) continue;
+      if (peak) {
+        const long long loc = x + (long long)n * y + nn * z;
+        const int e = wn + __popc(ball & ((1u << l) - 1u));
+        a.mask[loc] = 1;
+        myloc[e] = loc;
+        myf[e] = f;
+      }
+      wn += __popc(ball);
+      if (wn > kXpList - 32) flush();
     }
   }
   if (wn > 0) flush();
@@ -317,18 +388,26 @@ __global__ void __launch_bounds__(256) window_t_kernel(const float2* __restrict_
   const int fz = kz <= nyq ? kz : kz - n;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int kx = kx0 + tx;
-  for (int r = ty; r < 32; r += 8) {
-    const int ky = ky0 + r;
-    if (kx < nh) {
+  if (kx < nh) {
+    // the four loads and table lookups of this thread in flight together
+    float2 d[4], w[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int ky = ky0 + ty + 8 * u;
       const int fy = ky <= nyq ? ky : ky - n;
-      const int q = kx * kx + fy * fy + fz * fz;
-      const float2 d = dk[((int64_t)kz * n + ky) * nh + kx];
-      const float2 w = __ldg(reinterpret_cast<const float2*>(tab) + q);
-      t0[r][tx] = make_float2(__fmul_rn(__fmul_rn(d.x, w.x), ps), __fmul_rn(__fmul_rn(d.y, w.x), ps));
-      if (out1) t1[r][tx] = make_float2(__fmul_rn(__fmul_rn(d.x, w.y), ps), __fmul_rn(__fmul_rn(d.y, w.y), ps));
+      d[u] = __ldg(dk + ((int64_t)kz * n + ky) * nh + kx);
+      w[u] = __ldg(reinterpret_cast<const float2*>(tab) + (kx * kx + fy * fy + fz * fz));
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int r = ty + 8 * u;
+      t0[r][tx] = make_float2(__fmul_rn(__fmul_rn(d[u].x, w[u].x), ps), __fmul_rn(__fmul_rn(d[u].y, w[u].x), ps));
+      if (out1)
+        t1[r][tx] = make_float2(__fmul_rn(__fmul_rn(d[u].x, w[u].y), ps), __fmul_rn(__fmul_rn(d[u].y, w[u].y), ps));
     }
   }
   __syncthreads();
+#pragma unroll
   for (int cx = ty; cx < 32; cx += 8) {
     const int k = kx0 + cx;
     if (k >= nh) break;
@@ -340,7 +419,7 @@ __global__ void __launch_bounds__(256) window_t_kernel(const float2* __restrict_
 
 template <int J>
 constexpr size_t xpeak_smem() {
-  return (size_t)4 * kXpRows * 64 * J * 4 + (size_t)16 * kXpList * 12 + (size_t)(32 * J + 1) * kXpPad * 8 +
+  return (size_t)4 * kXpRows * 64 * J * 4 + (size_t)16 * kXpList * 12 + (size_t)2 * (32 * J + 1) * kXpPad * 8 +
          (size_t)2 * kXpInner * 64 * J;
 }
 
