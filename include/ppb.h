@@ -415,6 +415,11 @@ int32_t ppb_last_table_stats(ppb_ctx* ctx, float* ms, int64_t* steps);
  *  PPB_OPT_COLLAPSE_THREADS  fixes the collapse kernel: 1, 2 or 4 threads
  *                     per peak, 8 one thread per peak with lane work queues,
  *                     0 (default) the tuner's choice.
+ *  PPB_OPT_FUSED_X    the filter bank's x pass fused with the peak search
+ *                     (grid sizes 64 J, J <= 8, one window over the grid):
+ *                     -1 (default) for grid sizes >= 192, 1 wherever
+ *                     supported, 0 never (full 3-D C2R + separate search).
+ *                     The peaks agree up to FP32 transform rounding.
  * Read-only (ppb_get_option, summed over the context's slots):
  *  PPB_OPT_GRAPH_LAUNCHES, PPB_OPT_GRAPH_INSTANTIATIONS, PPB_OPT_GRAPH_UPDATES. */
 enum {
@@ -423,6 +428,7 @@ enum {
   PPB_OPT_TUNE_MIN_PEAKS = 3,
   PPB_OPT_BRICK_SHIFT = 4,
   PPB_OPT_COLLAPSE_THREADS = 5,
+  PPB_OPT_FUSED_X = 6,
   PPB_OPT_GRAPH_LAUNCHES = 16,
   PPB_OPT_GRAPH_INSTANTIATIONS = 17,
   PPB_OPT_GRAPH_UPDATES = 18

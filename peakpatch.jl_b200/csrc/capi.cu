@@ -970,6 +970,10 @@ int32_t ppb_set_option(ppb_ctx* ctx, int32_t option, int64_t value) {
                   "PPB_OPT_COLLAPSE_THREADS takes 0, 1, 2, 4 or 8");
       ctx->sh.force_collapse.store((int)value);
       break;
+    case PPB_OPT_FUSED_X:
+      PPB_REQUIRE(value >= -1 && value <= 1, "PPB_OPT_FUSED_X takes -1, 0 or 1");
+      ctx->sh.fused_x.store((int)value);
+      break;
     default:
       throw Error{PPB_ERR_INVALID, "unknown or read-only option"};
   }
@@ -986,6 +990,7 @@ int32_t ppb_get_option(ppb_ctx* ctx, int32_t option, int64_t* value) {
     case PPB_OPT_TUNE_MIN_PEAKS: *value = ctx->sh.tune_min_peaks.load(); break;
     case PPB_OPT_BRICK_SHIFT: *value = ctx->sh.force_brick.load(); break;
     case PPB_OPT_COLLAPSE_THREADS: *value = ctx->sh.force_collapse.load(); break;
+    case PPB_OPT_FUSED_X: *value = ctx->sh.fused_x.load(); break;
     case PPB_OPT_GRAPH_LAUNCHES:
     case PPB_OPT_GRAPH_INSTANTIATIONS:
     case PPB_OPT_GRAPH_UPDATES: {

@@ -158,6 +158,7 @@ struct Shared {
   // options (ppb_set_option)
   std::atomic<int> use_graphs{1};
   std::atomic<int> autotune{1};
+  std::atomic<int> fused_x{-1};   // PPB_OPT_FUSED_X
   std::atomic<int64_t> tune_min_peaks{16384};
   std::atomic<int> force_brick{-2};      // -2: tuner's choice
   std::atomic<int> force_collapse{0};    // 0: tuner's choice

@@ -488,10 +488,14 @@ int64_t peaks_phase(Run& r, TileRes& T, int n, double box, const std::vector<Win
   float* rw = T.rw.as<float>();
   const int qn = window_table_size(n);
   T.wtab.ensure((size_t)r.nfilt * 2 * qn * sizeof(float));
-  // one window over the whole grid (every caller) and a supported size: the
-  // x pass of each filter's transform runs fused with the peak search
-  const bool fused = !r.plain && T.yz1 && xpeak_supported(n, p->nbuff) && wins.size() == 1 && wins[0].off == 0 &&
-                     nm == n;
+  // one window over the whole grid (run_tile and the split's tiles; the
+  // multi-tile run searches several windows of one global grid) and a
+  // supported size: the x pass of each filter's transform runs fused with the
+  // peak search (by default from n = 192 up; below that its z halo and the
+  // per-filter launches cost more than the pass it saves)
+  const int fx = r.ctx->sh.fused_x.load();
+  const bool fused = !r.plain && (fx == 1 || (fx == -1 && n >= 192)) && T.yz1 && xpeak_supported(n, p->nbuff) &&
+                     wins.size() == 1 && wins[0].off == 0 && nm == n;
   int64_t npk = 0;
   for (int attempt = 0; attempt < 2; attempt++) {
     PeakBuf pb{T.keys.as<unsigned long long>(), T.vals.as<uint32_t>(), T.ff.as<float>(), T.lap.as<float>(),

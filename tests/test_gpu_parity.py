@@ -269,13 +269,19 @@ def tile64(ora, eh_pk, julia_table):
     return cfg, filters, st
 
 
-@pytest.mark.parametrize("plain", [False, True])
-def test_run_tile_vs_oracle(ctx, tile64, eh_pk, julia_table, plain):
+@pytest.mark.parametrize("mode", ["auto", "fused", "plain"])
+def test_run_tile_vs_oracle(ctx, tile64, eh_pk, julia_table, mode):
+    # fused: the filter bank's x pass fused with the peak search forced on at
+    # 64^3 (by default it starts at 192^3)
     cfg, filters, st = tile64
     T = julia_table
     ctx.set_pk_table(*eh_pk)
     ctx.set_collapse_table(pp.CollapseTable(T.data, T.x1, T.x2, T.y1, T.y2, T.z1, T.z2))
-    rec, rthlmax, npk = ctx.run_tile_arrays(cfg, 42, [f[2] for f in filters], plain=plain)
+    ctx.set_option(pp.OPT_FUSED_X, 1 if mode == "fused" else -1)
+    try:
+        rec, rthlmax, npk = ctx.run_tile_arrays(cfg, 42, [f[2] for f in filters], plain=mode == "plain")
+    finally:
+        ctx.set_option(pp.OPT_FUSED_X, -1)
     ro = st["records"]
     assert rec.shape[1] == 33 and len(ro) > 200
     assert abs(npk - len(st["peaks"]["ipp"])) <= max(2, 0.002 * npk)
@@ -373,17 +379,23 @@ def test_run_tile_file_api(ctx, tmp_path, eh_pk):
 @pytest.mark.parametrize("n,nbuff,ioutshear,seed", [(128, 5, 1, 3), (192, 12, 1, 8), (256, 32, 0, 11)])
 def test_fused_filter_bank_matches_full_transforms(ctx, eh_pk, julia_table, n, nbuff, ioutshear, seed):
     """The filter bank with cuFFT's z/y passes and the fused x pass + peak
-    search (grid sizes 64 J) against the path with full 3-D C2R transforms and
-    the separate peak search: the same peaks up to single-precision FFT
-    rounding, the same halos within the oracle bars."""
+    search (grid sizes 64 J; PPB_OPT_FUSED_X 1) against the same optimised
+    run with full 3-D C2R transforms and the separate peak search
+    (PPB_OPT_FUSED_X 0): the same peaks up to single-precision FFT rounding,
+    the same halos within the oracle bars."""
     cfg = tile_config(n=n, box=2.0 * n, nbuff=nbuff, ioutshear=ioutshear)
     filters = filter_bank()
     T = julia_table
     ctx.set_pk_table(*eh_pk)
     ctx.set_collapse_table(pp.CollapseTable(T.data, T.x1, T.x2, T.y1, T.y2, T.z1, T.z2))
     rf = [f[2] for f in filters]
-    fused, rmax_f, npk_f = ctx.run_tile_arrays(cfg, seed, rf, plain=False)
-    full, rmax_p, npk_p = ctx.run_tile_arrays(cfg, seed, rf, plain=True)
+    ctx.set_option(pp.OPT_FUSED_X, 1)
+    try:
+        fused, rmax_f, npk_f = ctx.run_tile_arrays(cfg, seed, rf, plain=False)
+        ctx.set_option(pp.OPT_FUSED_X, 0)
+        full, rmax_p, npk_p = ctx.run_tile_arrays(cfg, seed, rf, plain=False)
+    finally:
+        ctx.set_option(pp.OPT_FUSED_X, -1)
     nf = 33 if ioutshear else 11
     assert fused.shape[1] == nf and len(full) > 100
     assert abs(npk_f - npk_p) <= max(2, 0.002 * npk_p), (npk_f, npk_p)
