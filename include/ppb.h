@@ -417,8 +417,10 @@ int32_t ppb_last_table_stats(ppb_ctx* ctx, float* ms, int64_t* steps);
  *                     0 (default) the tuner's choice.
  *  PPB_OPT_FUSED_X    the filter bank's x pass fused with the peak search
  *                     (grid sizes 64 J, J <= 8, one window over the grid):
- *                     -1 (default) for grid sizes >= 192, 1 wherever
- *                     supported, 0 never (full 3-D C2R + separate search).
+ *                     -1 (default) with the k^2-weighted twin (ioutshear)
+ *                     for J = 3, 5, 6, 7 (where the 3-D C2R is slowest),
+ *                     1 wherever supported, 0 never (full 3-D C2R +
+ *                     separate search).
  *                     The peaks agree up to FP32 transform rounding.
  * Read-only (ppb_get_option, summed over the context's slots):
  *  PPB_OPT_GRAPH_LAUNCHES, PPB_OPT_GRAPH_INSTANTIATIONS, PPB_OPT_GRAPH_UPDATES. */

@@ -491,11 +491,15 @@ int64_t peaks_phase(Run& r, TileRes& T, int n, double box, const std::vector<Win
   // one window over the whole grid (run_tile and the split's tiles; the
   // multi-tile run searches several windows of one global grid) and a
   // supported size: the x pass of each filter's transform runs fused with the
-  // peak search (by default from n = 192 up; below that its z halo and the
-  // per-filter launches cost more than the pass it saves)
+  // peak search.  By default only with the k^2-weighted twin (two fields)
+  // and n = 64 J, J = 3, 5, 6, 7: there cuFFT's 3-D C2R is the slow part
+  // (peaks stage 384^3 26.8 -> 20.5 ms, 448^3 49.7 -> 40.0, 320^3 14.7 ->
+  // 12.1); for J a power of two (256^3 4.78 / 4.75, 512^3 46.4 / 50.4) and
+  // for one field (the split's tiles) the full transforms are as fast or faster
   const int fx = r.ctx->sh.fused_x.load();
-  const bool fused = !r.plain && (fx == 1 || (fx == -1 && n >= 192)) && T.yz1 && xpeak_supported(n, p->nbuff) &&
-                     wins.size() == 1 && wins[0].off == 0 && nm == n;
+  const int J = n / 64;
+  const bool fused = !r.plain && (fx == 1 || (fx == -1 && r.want_lap && (J & (J - 1)) != 0)) && T.yz1 &&
+                     xpeak_supported(n, p->nbuff) && wins.size() == 1 && wins[0].off == 0 && nm == n;
   int64_t npk = 0;
   for (int attempt = 0; attempt < 2; attempt++) {
     PeakBuf pb{T.keys.as<unsigned long long>(), T.vals.as<uint32_t>(), T.ff.as<float>(), T.lap.as<float>(),

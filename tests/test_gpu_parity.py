@@ -272,7 +272,7 @@ def tile64(ora, eh_pk, julia_table):
 @pytest.mark.parametrize("mode", ["auto", "fused", "plain"])
 def test_run_tile_vs_oracle(ctx, tile64, eh_pk, julia_table, mode):
     # fused: the filter bank's x pass fused with the peak search forced on at
-    # 64^3 (by default it starts at 192^3)
+    # 64^3 (by default it runs for 192, 320, 384 and 448^3 with ioutshear)
     cfg, filters, st = tile64
     T = julia_table
     ctx.set_pk_table(*eh_pk)
