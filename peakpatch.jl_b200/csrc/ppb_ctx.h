@@ -33,6 +33,9 @@ struct TileRes {
   std::map<std::pair<int, int64_t>, cudaGraphExec_t> graphs;
   ~TileRes();
   void setup(int n, cudaStream_t s);
+  // the fused filter bank's plans, twiddle buffer and kernel attribute, made
+  // the first time a filter bank of this size takes that path (outside capture)
+  void setup_fused(cudaStream_t s);
   void ensure_peaks(int64_t c);
   size_t bytes() const;
 };

@@ -251,15 +251,7 @@ void TileRes::setup(int nn, cudaStream_t s) {
   c2r3 = make_plan(n, CUFFT_C2R, 3);
   c2r6 = make_plan(n, CUFFT_C2R, 6);
   for (cufftHandle h : {r2c, c2r1, c2r2, c2r3, c2r6}) PPB_CUFFT(cufftSetStream(h, s));
-  if (xpeak_supported(n, 1)) {
-    int dims[2] = {n, n};
-    const int nh = n / 2 + 1;
-    PPB_CUFFT(cufftPlanMany(&yz1, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, nh));
-    PPB_CUFFT(cufftPlanMany(&yz2, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, 2 * nh));
-    for (cufftHandle h : {yz1, yz2}) PPB_CUFFT(cufftSetStream(h, s));
-    xpeak_prepare(n);
-    xtw.ensure((size_t)n * sizeof(float2));
-  }
+
   delta.ensure(N * 4);
   dk.ensure(M * 8);
   psi.ensure(3 * N * 4);
@@ -275,9 +267,20 @@ size_t TileRes::bytes() const {
   size_t b = 0;
   for (const DevBuf* d : {&delta, &dk, &psi, &psi2, &lapd, &aos, &kw, &rw, &mask, &count, &wtab, &keys, &vals, &ff,
                           &lap, &keys_s, &vals_s, &tmp, &p_lin, &p_Rf, &p_ir2, &p_Z, &p_fc, &p_FcRf, &p_d2Rf,
-                          &p_pos, &res, &flags, &offs, &rec, &rthl})
+                          &p_pos, &res, &flags, &offs, &rec, &rthl, &xtw})
     b += d->bytes;
   return b;
+}
+
+void TileRes::setup_fused(cudaStream_t s) {
+  if (yz1) return;
+  int dims[2] = {n, n};
+  const int nh = n / 2 + 1;
+  PPB_CUFFT(cufftPlanMany(&yz1, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, nh));
+  PPB_CUFFT(cufftPlanMany(&yz2, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, 2 * nh));
+  for (cufftHandle h : {yz1, yz2}) PPB_CUFFT(cufftSetStream(h, s));
+  xpeak_prepare(n);
+  xtw.ensure((size_t)n * sizeof(float2));
 }
 
 void TileRes::ensure_peaks(int64_t c) {
@@ -498,8 +501,9 @@ int64_t peaks_phase(Run& r, TileRes& T, int n, double box, const std::vector<Win
   // for one field (the split's tiles) the full transforms are as fast or faster
   const int fx = r.ctx->sh.fused_x.load();
   const int J = n / 64;
-  const bool fused = !r.plain && (fx == 1 || (fx == -1 && r.want_lap && (J & (J - 1)) != 0)) && T.yz1 &&
+  const bool fused = !r.plain && (fx == 1 || (fx == -1 && r.want_lap && (J & (J - 1)) != 0)) &&
                      xpeak_supported(n, p->nbuff) && wins.size() == 1 && wins[0].off == 0 && nm == n;
+  if (fused) T.setup_fused(r.s);
   int64_t npk = 0;
   for (int attempt = 0; attempt < 2; attempt++) {
     PeakBuf pb{T.keys.as<unsigned long long>(), T.vals.as<uint32_t>(), T.ff.as<float>(), T.lap.as<float>(),
