@@ -59,6 +59,9 @@ typedef struct ppb_tile_params {
   int32_t ilpt;
   int32_t ioutshear;
   int32_t wsmooth;
+  /* rmax2rs > 0 (the reference's default 1.0): a peak of filter radius Rf
+   * uses the first min(floor(4/3 pi (rmax2rs Rf / alatt)^3), npartmax) cells
+   * of the shell list (RadialShell.jl:288-295); 0 uses the whole list */
   double rmax2rs;
   uint64_t seed;
   /* path selection: 0 = optimised path (adaptive shell truncation,
@@ -172,20 +175,45 @@ int32_t ppb_write_pksc(const char* path, const float* records, int64_t n, int32_
  * Gaussian white noise, n^3 Float32, column-major. */
 int32_t ppb_noise_threefry(ppb_ctx* ctx, float* out, int32_t n, uint64_t seed);
 
-/* find_peaks (src/HaloFinder/PeakFind.jl:123-186) on one field; mask (Int8,
+/* find_peaks (src/HaloFinder/PeakFind.jl:15-79) on one field; mask (Int8,
  * n^3) is read and updated.  Peaks are returned in the reference's scan order
- * (k, then j, then i).  Outputs (capacity max_peaks): 1-based i, j, k, ipp
- * (int64) and delta (Float32); *npeaks receives the count. */
+ * (k, then j, then i).  As the reference, the scan stops after
+ * max(max_peaks, 1) peaks (it tests the count after each push, :66-71), so
+ * later cells are neither reported nor masked.  Outputs (capacity
+ * max(max_peaks, 1)): 1-based i, j, k, ipp (int64) and delta (Float32);
+ * *npeaks receives the count. */
 int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n1, int32_t n2,
                        int32_t n3, int32_t nbuff, float fcrit, int64_t max_peaks, int64_t* pi,
                        int64_t* pj, int64_t* pk, int64_t* ipp, float* pdelta, int64_t* npeaks);
+
+/* peak_find_tile_gpu(delta_tile, filters, fcrits, tile_masks_in, xbx, ybx,
+ * zbx, alatt, nbuff, wsmooth, ioutshear) (src/PeakPatch.jl:341-366; method
+ * ext/CUDAExt.jl:3068-3197): rfft(delta) once on the tile's periodic box
+ * (boxsize n alatt), then for each filter in the given order smooth_field
+ * with window wsmooth (0 Gaussian, 1 top-hat, 3 k^2-weighted Gaussian) and
+ * find_peaks with fcrit[f] and the mask carried across filters; with
+ * ioutshear >= 1 the k^2-weighted (wsmooth 3) field is sampled at each peak.
+ * delta_tile: n^3 Float32 column-major; mask: n^3 Int8, read and updated.
+ * Peaks come in (filter, scan order k, j, i) order, the order of the CPU
+ * loop over smooth_field + find_peaks.  Outputs, capacity entries each, host
+ * or device, any may be NULL: 1-based i, j, k; ipp; x = xbx + alatt (i -
+ * (n+1)/2) etc.; FcRf = the smoothed delta at the peak (PeakCandidate.delta);
+ * Rf of the peak's filter; d2Rf (0 without ioutshear); the 1-based filter
+ * number.  *npeaks receives the count; when it exceeds capacity the call
+ * returns PPB_ERR_CAPACITY and leaves the mask as it was. */
+int32_t ppb_peak_find_tile(ppb_ctx* ctx, const float* delta_tile, int32_t n, const double* Rf, const double* fcrit,
+                           int32_t nfilt, int8_t* mask, double xbx, double ybx, double zbx, double alatt,
+                           int32_t nbuff, int32_t wsmooth, int32_t ioutshear, int64_t capacity, int32_t* pi,
+                           int32_t* pj, int32_t* pk, int64_t* ipp, double* x, double* y, double* z, float* FcRf,
+                           double* Rf_out, float* d2Rf, int32_t* filter, int64_t* npeaks);
 
 /* ppb_find_peaks for callers that cannot allocate device memory at call time
  * (memory owned by another runtime's pool, or a fixed-footprint service loop
  * where cudaMalloc/cudaFree are not allowed).  No counterpart in the
  * reference: it is an addition of this library.  Same results as
- * ppb_find_peaks, but every array argument must be device memory owned by the
- * caller (npeaks is a host pointer) and the call allocates nothing: its
+ * ppb_find_peaks, but every array argument must be device memory of the
+ * context's GPU, owned by the caller (npeaks is a host pointer; a buffer on
+ * another GPU returns PPB_ERR_INVALID), and the call allocates nothing: its
  * scratch is a 2 MiB array built into the library, which limits the inner
  * cube to 268,435,456 cells (larger inputs return PPB_ERR_INVALID).  All
  * calls on a device share that array, so calls that overlap on the GPU race

@@ -266,7 +266,7 @@ void ora_smooth_k(const c64* dkf, c64* out, int64_t n, double boxsize, double Rf
 }
 
 // ---------------------------------------------------------------------------
-// Peak finding.  PeakFind.jl:123-186.  Indices returned 1-based.
+// Peak finding.  PeakFind.jl:15-79.  Indices returned 1-based.
 // Returns the number of peaks written (<= max_peaks).
 // ---------------------------------------------------------------------------
 int64_t ora_find_peaks(const float* delta, int8_t* mask, int64_t n1, int64_t n2, int64_t n3,

@@ -270,7 +270,7 @@ def window(kR: float, k: float, wsmooth: int) -> float:
 
 
 def find_peaks(delta, mask, xbx, ybx, zbx, alatt, nbuff, fcrit, max_peaks=2000000):
-    """PeakFind.jl:123-186.  delta: C-order (n3,n2,n1) float32; mask int8
+    """PeakFind.jl:15-79.  delta: C-order (n3,n2,n1) float32; mask int8
     (mutated).  Returns dict of arrays; i, j, k, ipp are 1-based."""
     n3, n2, n1 = delta.shape
     cap = int(min(max_peaks, delta.size))
@@ -504,19 +504,29 @@ def run_tile_stages(cfg: Config, seed: int, pk_k, pk_p, filters, T: Table, peak_
     t3 = time.perf_counter()
     tm["shells_s"] = t3 - t2
     tm["n_analysed"] = int(len(sel))
+    st = dict(fields=fields, delta_k=delta_k, peaks=peaks, Rf=pRf, FcollvRf=pFc, d2FRf=pd2,
+              ir2min=ir2min, ZZon=ZZon, fcrit=fcrit_val, results=res, shells=shells, nhunt=nhunt, alatt=alatt)
+    st["records"] = pack_records(cfg, st, res)
+    tm["total_s"] = time.perf_counter() - t0
+    return st
+
+
+def pack_records(cfg: Config, st: dict, res: np.ndarray) -> np.ndarray:
+    """Record packing of run_tile (Pipeline.jl:243-308) for the peaks of a
+    run_tile_stages result and per-peak analyse_peak results `res`: RTHL > 0
+    (and z <= z_max on the lightcone), 11 or 33 Float32 fields, peak order."""
+    peaks = st["peaks"]
+    npk = len(peaks["ipp"])
+    Om = cfg.Omx + cfg.OmB
     nf = 33 if cfg.ioutshear >= 1 else 11
     rec = np.empty((max(npk, 1), nf), dtype=np.float32)
     zz = np.empty(max(npk, 1))
-    L = lib()
-    nh = L.ora_pack_records(Om, cfg.OmB, cfg.Omvac, cfg.h, npk, _p(peaks["x"]), _p(peaks["y"]),
-                            _p(peaks["z"]), _p(np.ascontiguousarray(pRf)), _p(pFc), _p(pd2), _p(res),
-                            alatt, cfg.ievol, cfg.z_out, cfg.z_max, cfg.cenx, cfg.ceny, cfg.cenz,
-                            cfg.ioutshear, cfg.ilpt, _p(rec), _p(zz))
-    rec = rec[:nh].copy()
-    tm["total_s"] = time.perf_counter() - t0
-    return dict(fields=fields, delta_k=delta_k, peaks=peaks, Rf=pRf, FcollvRf=pFc, d2FRf=pd2,
-                ir2min=ir2min, ZZon=ZZon, fcrit=fcrit_val, results=res, records=rec, shells=shells,
-                nhunt=nhunt, alatt=alatt)
+    res = np.ascontiguousarray(res, dtype=np.float64)
+    nh = lib().ora_pack_records(Om, cfg.OmB, cfg.Omvac, cfg.h, npk, _p(peaks["x"]), _p(peaks["y"]),
+                                _p(peaks["z"]), _p(np.ascontiguousarray(st["Rf"])), _p(st["FcollvRf"]),
+                                _p(st["d2FRf"]), _p(res), st["alatt"], cfg.ievol, cfg.z_out, cfg.z_max, cfg.cenx,
+                                cfg.ceny, cfg.cenz, cfg.ioutshear, cfg.ilpt, _p(rec), _p(zz))
+    return rec[:nh].copy()
 
 
 def sphere_overlap(d: float, r1: float, r2: float):

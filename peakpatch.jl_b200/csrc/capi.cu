@@ -58,9 +58,9 @@ void Slot::release_buffers() {
   if (stream) PPB_CUDA(cudaStreamSynchronize(stream));
   tiles.clear();
   tile_lru.clear();
-  for (DevBuf* b : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
+  for (DevBuf* b : {&filt_Rf, &filt_ir2, &filt_np, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
                     &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &mr_in, &mr_out, &mr_aux,
-                    &mr_rec, &mr_axis, &mr_amp})
+                    &mr_rec, &mr_axis, &mr_amp, &pft})
     b->release();
   tune_save.release();
   iso.reset();
@@ -74,9 +74,9 @@ size_t Slot::bytes_held() const {
 
 size_t Slot::shell_bytes() const {
   size_t b = 0;
-  for (const DevBuf* d : {&filt_Rf, &filt_ir2, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool,
+  for (const DevBuf* d : {&filt_Rf, &filt_ir2, &filt_np, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool,
                           &okey, &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &mr_in,
-                          &mr_out, &mr_aux, &mr_rec, &mr_axis, &mr_amp})
+                          &mr_out, &mr_aux, &mr_rec, &mr_axis, &mr_amp, &pft})
     b += d->bytes;
   if (iso) b += iso->bytes();
   return b;
@@ -409,7 +409,8 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
   // autotuned order brick and collapse width for this kind of batch
   // (the walk class: collapse walks of more than 8 steps per peak in the
   // slot's previous batch, as on the lightcone, favour other widths)
-  const std::array<int64_t, 6> tkey{a.n, a.nshell, comp, adaptive, a.r2lim != nullptr, sl.walk_per_peak > 8.0};
+  const std::array<int64_t, 6> tkey{a.n, a.nshell, comp, adaptive, (a.r2lim != nullptr) | (a.npcap != nullptr) << 1,
+                                    sl.walk_per_peak > 8.0};
   TuneEntry te;
   bool tuned = false;
   {
@@ -440,6 +441,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     b.geo = sl.geo.as<int4>() + p0;
     b.mlim = sl.mlim.as<int32_t>() + p0;
     b.r2lim = a.r2lim ? a.r2lim + p0 : nullptr;
+    b.npcap = a.npcap ? a.npcap + p0 : nullptr;
     b.pool = sl.pool.as<double>();
     b.pool_cap = cap;
     b.pool_ctr = reinterpret_cast<unsigned long long*>(sl.ctl.as<char>() + 8);
@@ -704,6 +706,36 @@ int32_t ppb_generate_fields(ppb_ctx* ctx, const ppb_tile_params* p, float* delta
   PPB_REQUIRE(p != nullptr, "params is null");
   std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
   generate_fields_core(ctx, ctx->sync, p, delta, psi, psi2, lapd);
+  return PPB_OK;
+  PPB_GUARD_END(ctx)
+}
+
+int32_t ppb_peak_find_tile(ppb_ctx* ctx, const float* delta_tile, int32_t n, const double* Rf, const double* fcrit,
+                           int32_t nfilt, int8_t* mask, double xbx, double ybx, double zbx, double alatt,
+                           int32_t nbuff, int32_t wsmooth, int32_t ioutshear, int64_t capacity, int32_t* pi,
+                           int32_t* pj, int32_t* pk, int64_t* ipp, double* x, double* y, double* z, float* FcRf,
+                           double* Rf_out, float* d2Rf, int32_t* filter, int64_t* npeaks) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  PPB_GUARD_BEGIN
+  PPB_CUDA(cudaSetDevice(ctx->device));
+  std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
+  PeakTileOut o;
+  o.capacity = capacity;
+  o.pi = pi;
+  o.pj = pj;
+  o.pk = pk;
+  o.ipp = ipp;
+  o.x = x;
+  o.y = y;
+  o.z = z;
+  o.FcRf = FcRf;
+  o.Rf = Rf_out;
+  o.d2Rf = d2Rf;
+  o.filter = filter;
+  o.npeaks = npeaks;
+  peak_find_tile_core(ctx, ctx->sync, delta_tile, n, Rf, fcrit, nfilt, mask, xbx, ybx, zbx, alatt, nbuff, wsmooth,
+                      ioutshear, o);
   return PPB_OK;
   PPB_GUARD_END(ctx)
 }

@@ -345,7 +345,7 @@ __global__ void extract_kernel(float* __restrict__ dst, const float* __restrict_
 }
 
 // ---------------------------------------------------------------------------
-// peak finder for one filter (PeakFind.jl:123-186).  A cell of the inner cube
+// peak finder for one filter (PeakFind.jl:15-79).  A cell of the inner cube
 // (nbuff < i <= n - nbuff, 1-based) is a peak when it is not masked, is not
 // below fcrit, and no neighbour of the 3x3x3 block is strictly larger.  The
 // cell's mask is set; within one filter only a peak's own cell is written,

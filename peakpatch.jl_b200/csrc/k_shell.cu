@@ -602,6 +602,19 @@ __global__ void geo_kernel(ShellArgs a, uint32_t* key, int32_t* idx) {
     }
     mmax = max(min(hi - 1, a.mmax), 1);
   }
+  if (a.npcap) {   // cells 1..npart of the list: the shells closed before cell npart + 1
+    // distinct r^2 value g holds cells sh_start[g] ..; the cap's last cell
+    // (0-based npart - 1) lies in the largest g with sh_start[g] <= npart - 1,
+    // and shells 1..g (profile numbering, shell 1 = the centre) are the ones
+    // the reference finalises inside its loop over jp = 2..npart
+    const int last = a.npcap[p] - 1;
+    int lo = 0, hi = a.nshell - 1;
+    while (lo <= hi) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(a.sh_start + mid) <= last) lo = mid + 1; else hi = mid - 1;
+    }
+    mmax = max(min(hi, mmax), 1);
+  }
   a.mlim[p] = mmax;
   const Geo g = geometry(a, a.pk.Rf[p], a.pk.ir2min[p], mmax);
   a.geo[p] = make_int4(g.m0_init, g.mrf, g.mlow_rf, g.mupp_rf);
@@ -1223,7 +1236,8 @@ __global__ void __launch_bounds__(128) d2f_kernel(ShellArgs a) {
     const int64_t lin = a.pk.lin[p];
     const int pk = (int)(lin / n2), pj = (int)((lin / n) % n), pi = (int)(lin % n);
     const int mR = first_gt(a.rad, 1, a.nshell, RTHL);   // 1-based shell; distinct r2 index mR - 1
-    const int64_t cend = mR <= a.nshell ? (int64_t)__ldg(a.sh_start + mR - 1) : a.npart;
+    int64_t cend = mR <= a.nshell ? (int64_t)__ldg(a.sh_start + mR - 1) : a.npart;
+    if (a.npcap) cend = min(cend, (int64_t)a.npcap[p]);   // jp = 2..npart (RadialShell.jl:805-819)
     double acc = 0.0;
     long long navg = 0;
     for (int64_t c0 = 1; c0 < cend; c0 += 32) {

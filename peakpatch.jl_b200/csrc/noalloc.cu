@@ -23,9 +23,11 @@
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress); make that first call before any stream capture.
 //
-// Semantics are those of find_peaks (src/HaloFinder/PeakFind.jl:123-186) and
-// of ppb_find_peaks: scan order k, j, i; the first max_peaks peaks are
-// reported and masked, later ones are neither.
+// Semantics are those of find_peaks (src/HaloFinder/PeakFind.jl:15-79) and
+// of ppb_find_peaks: scan order k, j, i; the first max(max_peaks, 1) peaks
+// are reported and masked, later ones are neither (the reference pushes a
+// peak before it compares the count with max_peaks, :66-71).  Every buffer
+// must be device memory of the context's own GPU.
 #include <mutex>
 
 #include "ppb_ctx.h"
@@ -182,11 +184,16 @@ extern "C" int32_t ppb_find_peaks_noalloc(ppb_ctx* ctx, const float* delta, int8
   try {
     PPB_REQUIRE(delta && mask && pi && pj && pk && ipp && pdelta && npeaks, "null argument");
     PPB_REQUIRE(n1 >= 3 && n2 >= 3 && n3 >= 3 && nbuff >= 1, "grid must be >= 3 cells with nbuff >= 1");
-    PPB_REQUIRE(max_peaks >= 0, "max_peaks must be >= 0");
     PPB_CUDA(cudaSetDevice(ctx->device));
     for (const void* p : {(const void*)delta, (const void*)mask, (const void*)pi, (const void*)pj, (const void*)pk,
-                          (const void*)ipp, (const void*)pdelta})
+                          (const void*)ipp, (const void*)pdelta}) {
       PPB_REQUIRE(is_device_ptr(p), "ppb_find_peaks_noalloc needs device pointers for fields and outputs");
+      cudaPointerAttributes at;
+      PPB_CUDA(cudaPointerGetAttributes(&at, p));
+      PPB_REQUIRE(at.type == cudaMemoryTypeManaged || at.device == ctx->device,
+                  "ppb_find_peaks_noalloc: a buffer lives on another GPU than the context's");
+    }
+    const int64_t keep = max_peaks > 1 ? max_peaks : 1;   // at least the first peak (PeakFind.jl:66-71)
     const int w1 = n1 - 2 * nbuff, w2 = n2 - 2 * nbuff, w3 = n3 - 2 * nbuff;
     *npeaks = 0;
     if (w1 <= 0 || w2 <= 0 || w3 <= 0) return PPB_OK;
@@ -212,13 +219,13 @@ extern "C" int32_t ppb_find_peaks_noalloc(ppb_ctx* ctx, const float* delta, int8
     PPB_LAUNCHED(ctx->sync.launches);
     scan_kernel<<<1, kThreads, 0, s>>>(scratch, (int)nblocks);
     PPB_LAUNCHED(ctx->sync.launches);
-    write_kernel<<<(unsigned)nblocks, kThreads, 0, s>>>(delta, mask, g, fcrit, ninner, max_peaks, scratch, pi, pj,
-                                                       pk, ipp, pdelta);
+    write_kernel<<<(unsigned)nblocks, kThreads, 0, s>>>(delta, mask, g, fcrit, ninner, keep, scratch, pi, pj, pk,
+                                                       ipp, pdelta);
     PPB_LAUNCHED(ctx->sync.launches);
     unsigned int total = 0;
     PPB_CUDA(cudaMemcpyAsync(&total, scratch + 2 * kMaxBlocks, sizeof(total), cudaMemcpyDeviceToHost, s));
     PPB_CUDA(cudaStreamSynchronize(s));
-    *npeaks = (int64_t)total < max_peaks ? (int64_t)total : max_peaks;
+    *npeaks = (int64_t)total < keep ? (int64_t)total : keep;
     return PPB_OK;
   } catch (const ppb::Error& e) {
     ctx->set_error(e.msg);

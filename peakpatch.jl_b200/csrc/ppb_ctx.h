@@ -27,7 +27,7 @@ struct TileRes {
   // peaks
   int64_t cap = 0;
   DevBuf keys, vals, ff, lap, keys_s, vals_s, tmp;
-  DevBuf p_lin, p_Rf, p_ir2, p_Z, p_fc, p_FcRf, p_d2Rf, p_pos, res, flags, offs, rec, rthl;
+  DevBuf p_lin, p_Rf, p_ir2, p_np, p_Z, p_fc, p_FcRf, p_d2Rf, p_pos, res, flags, offs, rec, rthl;
   // executable graphs that hold this grid size's cuFFT plans (fields, filter
   // bank): they live exactly as long as the plans whose kernels they launch
   std::map<std::pair<int, int64_t>, cudaGraphExec_t> graphs;
@@ -93,7 +93,7 @@ struct Slot {
   std::map<int, std::unique_ptr<TileRes>> tiles;    // resident grid sizes (buffers, plans, graphs)
   std::vector<int> tile_lru;                        // resident sizes, least recently used first
   int max_tiles = 4;                                // sizes kept resident at most
-  DevBuf filt_Rf, filt_ir2;                         // filter bank of the run
+  DevBuf filt_Rf, filt_ir2, filt_np;                // filter bank of the run
   DevBuf g_a, g_D, g_f, chi;                        // growth / chi tables of the run
   DevBuf stage, counters, ctl, hdr, geo, mlim, pool;   // shell stage
   DevBuf okey, okey2, oidx, oidx2, otmp;            // spatial gather order
@@ -101,6 +101,7 @@ struct Slot {
   std::unique_ptr<IsoRes> iso;                      // multi-resolution: isolated convolution
   DevBuf mr_in, mr_out, mr_aux, mr_rec;             // multi-resolution: staged inputs, outputs, records
   DevBuf mr_axis, mr_amp;                           // multi-resolution: tricubic axis tables, coarse amplitudes
+  DevBuf pft;                                       // ppb_peak_find_tile: unpacked (i, j, k), ipp, filter
   int gather_bps[2][2] = {{0, 0}, {0, 0}};          // gather blocks per SM by [comp][adaptive]
   double rows_per_peak[2] = {0.0, 0.0};             // pool rows per peak seen last, by adaptive
   double walk_per_peak = 0.0;                       // collapse-walk steps per peak seen last
@@ -126,6 +127,20 @@ struct Slot {
   // frees the buffers of size n; returns the bytes freed
   uint64_t drop_tile(int n);
   ~Slot();
+};
+
+// outputs of ppb_peak_find_tile (host or device pointers; any may be null
+// except npeaks): capacity entries each
+struct PeakTileOut {
+  int64_t capacity = 0;
+  int32_t *pi = nullptr, *pj = nullptr, *pk = nullptr;
+  int64_t* ipp = nullptr;
+  double *x = nullptr, *y = nullptr, *z = nullptr;
+  float* FcRf = nullptr;
+  double* Rf = nullptr;
+  float* d2Rf = nullptr;
+  int32_t* filter = nullptr;
+  int64_t* npeaks = nullptr;
 };
 
 // the record buffer of a finished run, still on the device
@@ -233,6 +248,14 @@ void run_multitile_split_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, 
 // automatic choice of src/MultiResolution.jl:592-612)
 int split_coarse_grid(int64_t N, int nmesh, int ntile, int coarse_factor, int coarse_grid);
 void check_params(const ppb_tile_params* p, const double* Rf, int nfilt);
+// peak_find_tile_gpu (src/PeakPatch.jl:341-366): rfft of the caller's field,
+// then per filter (in the given order) the window, the inverse transform and
+// the peak search with per-filter fcrit and the caller's mask (read and
+// updated); peaks in (filter, scan) order.  *o.npeaks receives the count;
+// PPB_ERR_CAPACITY (mask untouched) when it exceeds o.capacity.
+void peak_find_tile_core(ppb_ctx* ctx, Slot& sl, const float* delta, int n, const double* Rf, const double* fcrit,
+                         int nfilt, int8_t* mask, double xbx, double ybx, double zbx, double alatt, int nbuff,
+                         int wsmooth, int ioutshear, const PeakTileOut& o);
 // the fields of run_tile's first phase, copied to the given buffers (host or
 // device, any may be null)
 void generate_fields_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, float* delta, float* psi, float* psi2,

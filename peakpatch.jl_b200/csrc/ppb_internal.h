@@ -231,6 +231,7 @@ struct ShellArgs {
   PeakHdr* hdr;             // npk
   int4* geo;                // npk: (m0_init, mrf, mlow_rf, mupp_rf)
   const int32_t* r2lim;     // npk or null: per-peak shell list r^2 <= r2lim (> 0), else the whole list
+  const int32_t* npcap;     // npk or null: per-peak cell count npart (the rmax2rs cap of RadialShell.jl:288-295)
   int32_t* mlim;            // npk: the peak's last finalised shell (written by the geometry kernel)
   double* pool;             // profile rows, pool_cap rows of ROW doubles
   int64_t pool_cap;

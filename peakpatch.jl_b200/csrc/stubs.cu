@@ -49,7 +49,6 @@ int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n
   try {
     PPB_REQUIRE(delta && mask && pi && pj && pk && ipp && pdelta && npeaks, "null argument");
     PPB_REQUIRE(n1 >= 3 && n2 >= 3 && n3 >= 3 && nbuff >= 1, "grid must be >= 3 cells with nbuff >= 1");
-    PPB_REQUIRE(max_peaks >= 0, "max_peaks must be >= 0");
     PPB_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->sync.stream;
     const int64_t N = (int64_t)n1 * n2 * n3;
@@ -99,13 +98,15 @@ int32_t ppb_find_peaks(ppb_ctx* ctx, const float* delta, int8_t* mask, int32_t n
       PPB_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tb, keys.as<unsigned long long>(), keys_s.as<unsigned long long>(),
                                                vals.as<uint32_t>(), vals_s.as<uint32_t>(), (int)np, 0, 40, s));
       ctx->sync.launches++;
-      // the reference stops scanning after max_peaks (PeakFind.jl:178-180):
+      // the reference stops scanning once max_peaks are found, testing the
+      // count after each push (PeakFind.jl:66-71, so at least one peak):
       // later cells are neither reported nor masked
-      if (np > max_peaks) {
-        const int from = (int)max_peaks, to = (int)np;
+      const int64_t keep = max_peaks > 1 ? max_peaks : 1;
+      if (np > keep) {
+        const int from = (int)keep, to = (int)np;
         unmask_kernel<<<(to - from + 255) / 256, 256, 0, s>>>(keys_s.as<unsigned long long>(), from, to, dm);
         PPB_LAUNCHED(ctx->sync.launches);
-        np = max_peaks;
+        np = keep;
       }
       if (np > 0) {
         o_i.ensure(np * 8); o_j.ensure(np * 8); o_k.ensure(np * 8); o_ipp.ensure(np * 8); o_d.ensure(np * 4);

@@ -82,6 +82,7 @@ struct PrepArgs {
   double alatt;
   const double* fRf;
   const int32_t* fir2;
+  const int32_t* fnp;        // per filter npart (rmax2rs > 0), else null
   int ievol;
   double z_out, fcrit0;
   double obs[3];
@@ -91,6 +92,7 @@ struct PrepArgs {
   int64_t* lin;
   double* Rf;
   int32_t* ir2;
+  int32_t* np;
   double* Z;
   double* fc;
   float* FcRf;
@@ -110,13 +112,14 @@ __global__ void prep_kernel(PrepArgs a) {
   const int n = a.n;
   const int i = (int)(lin % n) + 1, j = (int)((lin / n) % n) + 1, k = (int)(lin / ((int64_t)n * n)) + 1;
   const double cen = 0.5 * (n + 1);
-  // x = xbx + alatt (i - (n+1)/2) (PeakFind.jl:350-425; xbx = tile centre, 0 for run_tile)
+  // x = xbx + alatt (i - (n+1)/2) (PeakFind.jl:15-79; xbx = tile centre, 0 for run_tile)
   const double bx = a.tcen ? a.tcen[3 * t] : 0.0, by = a.tcen ? a.tcen[3 * t + 1] : 0.0,
                bz = a.tcen ? a.tcen[3 * t + 2] : 0.0;
   const double x = bx + a.alatt * (i - cen), y = by + a.alatt * (j - cen), z = bz + a.alatt * (k - cen);
   a.lin[q] = lin;
   a.Rf[q] = a.fRf[f];
   a.ir2[q] = a.fir2[f];
+  if (a.fnp) a.np[q] = a.fnp[f];
   a.FcRf[q] = a.ff[slot];
   a.d2Rf[q] = a.lap[slot];
   a.pos[q] = x;
@@ -214,6 +217,20 @@ __global__ void record_kernel(RecArgs a) {
   }
 }
 
+// sorted peak keys -> 1-based (i, j, k), ipp and filter number
+__global__ void unpack_peaks_kernel(const unsigned long long* keys, int npk, int n, int fbits, int32_t* ijk,
+                                    int64_t* ipp, int32_t* filt) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npk) return;
+  const unsigned long long key = keys[q];
+  const int64_t lin = (int64_t)(key & ((1ull << 40) - 1));
+  ijk[q] = (int32_t)(lin % n) + 1;
+  ijk[npk + q] = (int32_t)((lin / n) % n) + 1;
+  ijk[2 * npk + q] = (int32_t)(lin / ((int64_t)n * n)) + 1;
+  ipp[q] = lin + 1;
+  filt[q] = (int32_t)((key >> 40) & ((1ull << fbits) - 1)) + 1;
+}
+
 __global__ void tile_count_kernel(const unsigned long long* keys, int npk, int shift, int* counts) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q < npk) atomicAdd(counts + (int)(keys[q] >> shift), 1);
@@ -266,7 +283,7 @@ void TileRes::setup(int nn, cudaStream_t s) {
 size_t TileRes::bytes() const {
   size_t b = 0;
   for (const DevBuf* d : {&delta, &dk, &psi, &psi2, &lapd, &aos, &kw, &rw, &mask, &count, &wtab, &keys, &vals, &ff,
-                          &lap, &keys_s, &vals_s, &tmp, &p_lin, &p_Rf, &p_ir2, &p_Z, &p_fc, &p_FcRf, &p_d2Rf,
+                          &lap, &keys_s, &vals_s, &tmp, &p_lin, &p_Rf, &p_ir2, &p_np, &p_Z, &p_fc, &p_FcRf, &p_d2Rf,
                           &p_pos, &res, &flags, &offs, &rec, &rthl, &xtw})
     b += d->bytes;
   return b;
@@ -295,6 +312,7 @@ void TileRes::ensure_peaks(int64_t c) {
   p_lin.ensure(cap * 8);
   p_Rf.ensure(cap * 8);
   p_ir2.ensure(cap * 4);
+  p_np.ensure(cap * 4);
   p_Z.ensure(cap * 8);
   p_fc.ensure(cap * 8);
   p_FcRf.ensure(cap * 4);
@@ -328,10 +346,7 @@ void check_params(const ppb_tile_params* p, const double* Rf, int nfilt) {
   PPB_REQUIRE(p->wsmooth == 0 || p->wsmooth == 1 || p->wsmooth == 3, "wsmooth must be 0, 1 or 3");
   PPB_REQUIRE(p->ievol == 0 || p->ievol == 1, "ievol must be 0 or 1");
   PPB_REQUIRE(p->pk_scale >= 0.0, "pk_scale must be >= 0 (0 means 1)");
-  if (p->rmax2rs != 0.0)
-    throw Error{PPB_ERR_UNSUPPORTED,
-                "rmax2rs > 0 is not supported: the reference's result then depends on thread scheduling "
-                "(mask writes of RadialShell.jl:793-802 race with the pre-mask read at :311-316)"};
+  PPB_REQUIRE(p->rmax2rs >= 0.0 && p->rmax2rs <= 1e6, "rmax2rs must be in [0, 1e6]");
 }
 
 uint64_t tile_footprint(const ppb_tile_params* p) { return tile_bytes_estimate(p->n) + shell_bytes_estimate(p->n); }
@@ -377,6 +392,12 @@ struct Run {
   int nhunt;
   ShellTable* shells;
   DevCosmo C;
+  bool npcap;   // rmax2rs > 0: per-peak cell caps (filt_np, p_np)
+  // peak search of a caller's field (ppb_peak_find_tile): fcrit per filter
+  // (empty: the window's), and the mask as the caller gave it (else zeroed)
+  std::vector<float> ffc;
+  bool keep_mask = false;
+  const void* mask_src = nullptr;   // keep_mask: the caller's mask (host or device), copied in per attempt
 };
 
 // a peak-search window: a tile of nm^3 cells at `off` in the field grid
@@ -406,6 +427,26 @@ void setup_run(Run& r, ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const d
   r.nhunt = std::min(p->nbuff - 1, (int)std::floor(r.Rf[0] * 1.75 / alatt));
   PPB_REQUIRE(r.nhunt >= 1, "nhunt = min(nbuff-1, floor(1.75 Rfmax/alatt)) must be >= 1");
   r.shells = &ctx->shell_table(r.nhunt, r.s);
+  // rmax2rs > 0 (RadialShell.jl:288-295): a peak of filter radius Rf uses the
+  // first npart = min(floor(4/3 pi (rmax2rs Rf / alatt)^3), npartmax) cells
+  // of the shell list.  The pre-mask test of :310-316 needs no counterpart:
+  // it can only skip a peak whose filter has floor(rmax2rs Rf / alatt) = 0,
+  // i.e. npart <= 4 cells, which closes no shell beyond the centre (the six
+  // r^2 = 1 cells end at cell 7), so the peak reaches m0 = 1 and returns
+  // no_collapse (:650-653) whether or not it is skipped.  The result is then
+  // independent of the order in which peaks write and read the mask.
+  r.npcap = p->rmax2rs > 0.0;
+  if (r.npcap) {
+    const double f3p = 4.0 / 3.0 * 3.141592653589793;
+    std::vector<int32_t> fnp(nfilt);
+    for (int f = 0; f < nfilt; f++) {
+      const double x = p->rmax2rs * r.Rf[f] / alatt;
+      const double v = f3p * (x * x * x);
+      fnp[f] = v >= (double)r.shells->ncells ? (int32_t)r.shells->ncells : (int32_t)std::floor(v);
+    }
+    sl.filt_np.ensure(nfilt * 4);
+    PPB_CUDA(cudaMemcpyAsync(sl.filt_np.p, fnp.data(), nfilt * 4, cudaMemcpyHostToDevice, r.s));
+  }
   std::vector<int32_t> fir2(nfilt);
   for (int f = 0; f < nfilt; f++)
     fir2[f] = (int32_t)std::min(std::floor((1.75 * r.Rf[f] / alatt) * (1.75 * r.Rf[f] / alatt)),
@@ -508,10 +549,11 @@ int64_t peaks_phase(Run& r, TileRes& T, int n, double box, const std::vector<Win
   for (int attempt = 0; attempt < 2; attempt++) {
     PeakBuf pb{T.keys.as<unsigned long long>(), T.vals.as<uint32_t>(), T.ff.as<float>(), T.lap.as<float>(),
                T.count.as<int>(), T.cap};
+    if (r.keep_mask) PPB_CUDA(cudaMemcpyAsync(T.mask.p, r.mask_src, N, cudaMemcpyDefault, r.s));
     // the whole filter bank as one graph (window tables, per filter the
     // window multiply, the inverse transforms and the peak search)
-    r.ctx->captured(*r.sl, T.graphs, 1, (int64_t)n * 4096 + (int64_t)wins.size(), [&] {
-      PPB_CUDA(cudaMemsetAsync(T.mask.p, 0, N, r.s));
+    r.ctx->captured(*r.sl, T.graphs, r.keep_mask ? 3 : 1, (int64_t)n * 4096 + (int64_t)wins.size(), [&] {
+      if (!r.keep_mask) PPB_CUDA(cudaMemsetAsync(T.mask.p, 0, N, r.s));
       PPB_CUDA(cudaMemsetAsync(T.count.p, 0, 64, r.s));
       launch_window_tables(L, T.wtab.as<float>(), n, box, r.sl->filt_Rf.as<double>(), r.nfilt, p->wsmooth,
                            r.want_lap);
@@ -524,7 +566,7 @@ int64_t peaks_phase(Run& r, TileRes& T, int n, double box, const std::vector<Win
           launch_window_t(L, dkp, kw, o1, n, T.wtab.as<float>() + (size_t)f * 2 * qn, inv_n3);
           PPB_CUFFT(cufftExecC2C(o1 ? T.yz2 : T.yz1, (cufftComplex*)kw, (cufftComplex*)kw, CUFFT_INVERSE));
           launch_xpeak(L, kw, o1, T.xtw.as<float2>(), T.mask.as<uint8_t>(), T.count.as<unsigned>() + 2, n,
-                       p->nbuff, wins[0].fcrit, (unsigned long long)f, pb);
+                       p->nbuff, r.ffc.empty() ? wins[0].fcrit : r.ffc[f], (unsigned long long)f, pb);
           continue;
         }
         launch_window(L, dkp, kw, o1, n, T.wtab.as<float>() + (size_t)f * 2 * qn, inv_n3);
@@ -537,7 +579,7 @@ int64_t peaks_phase(Run& r, TileRes& T, int n, double box, const std::vector<Win
         for (size_t t = 0; t < wins.size(); t++) {
           const Win& w = wins[t];
           launch_peakfind(L, rw + w.off, r.want_lap ? rw + N + w.off : nullptr, T.mask.as<uint8_t>() + w.off, nm,
-                          nm, nm, n, (int64_t)n * n, p->nbuff, w.fcrit,
+                          nm, nm, n, (int64_t)n * n, p->nbuff, r.ffc.empty() ? w.fcrit : r.ffc[f],
                           ((unsigned long long)t << r.fbits) | (unsigned long long)f, pb);
         }
       }
@@ -585,6 +627,8 @@ void prep_phase(Run& r, TileRes& T, int64_t npk, int nm, int nwin, const double*
   pa.lin = T.p_lin.as<int64_t>();
   pa.Rf = T.p_Rf.as<double>();
   pa.ir2 = T.p_ir2.as<int32_t>();
+  pa.fnp = r.npcap ? r.sl->filt_np.as<int32_t>() : nullptr;
+  pa.np = T.p_np.as<int32_t>();
   pa.Z = T.p_Z.as<double>();
   pa.fc = T.p_fc.as<double>();
   pa.FcRf = T.p_FcRf.as<float>();
@@ -603,6 +647,7 @@ void shells_phase(Run& r, TileRes& T, int64_t p0, int64_t p1, int nm, const floa
   a.pk = PeakParams{T.p_lin.as<int64_t>() + p0, T.p_Rf.as<double>() + p0, T.p_ir2.as<int32_t>() + p0,
                     T.p_Z.as<double>() + p0, T.p_fc.as<double>() + p0};
   a.npk = p1 - p0;
+  a.npcap = r.npcap ? T.p_np.as<int32_t>() + p0 : nullptr;
   a.out = T.res.as<double>() + p0 * RES_N;
   ShellStats st{};
   r.ctx->run_shells(*r.sl, a, !r.plain, !r.plain, &st, pre);
@@ -679,6 +724,94 @@ void check_shell_stats(const ShellStats& st) {
 }
 
 }  // namespace
+
+void peak_find_tile_core(ppb_ctx* ctx, Slot& sl, const float* delta, int n, const double* Rf, const double* fcrit,
+                         int nfilt, int8_t* mask, double xbx, double ybx, double zbx, double alatt, int nbuff,
+                         int wsmooth, int ioutshear, const PeakTileOut& o) {
+  PPB_REQUIRE(delta && Rf && fcrit && mask && o.npeaks, "null argument");
+  PPB_REQUIRE(n >= 8 && n <= 2048, "n must be in [8, 2048]");
+  PPB_REQUIRE(alatt > 0.0, "alatt must be positive");
+  PPB_REQUIRE(nbuff >= 1 && 2 * nbuff < n, "nbuff must satisfy 1 <= nbuff and 2 nbuff < n");
+  PPB_REQUIRE(nfilt >= 1 && nfilt <= 4096, "need 1..4096 filters");
+  for (int f = 0; f < nfilt; f++) PPB_REQUIRE(Rf[f] > 0.0, "filter radii must be positive");
+  PPB_REQUIRE(wsmooth == 0 || wsmooth == 1 || wsmooth == 3, "wsmooth must be 0, 1 or 3");
+  PPB_REQUIRE(o.capacity >= 0, "capacity must be >= 0");
+  const int64_t N = (int64_t)n * n * n;
+  // the tile's own periodic box, boxsize_local = n alatt (ext/CUDAExt.jl:3081)
+  ppb_tile_params p{};
+  p.n = n;
+  p.boxsize = n * alatt;
+  p.nbuff = nbuff;
+  p.wsmooth = wsmooth;
+  p.ioutshear = ioutshear;
+  p.ilpt = 1;
+  Run r{};
+  r.ctx = ctx;
+  r.sl = &sl;
+  r.p = &p;
+  r.s = sl.stream;
+  r.L = Launch{sl.stream, &sl.launches};
+  r.alatt = alatt;
+  r.plain = false;
+  r.want_lap = ioutshear >= 1;
+  r.Rf.assign(Rf, Rf + nfilt);   // the caller's order (the filter loop of ext/CUDAExt.jl:3118)
+  r.nfilt = nfilt;
+  r.fbits = 1;
+  while ((1 << r.fbits) < nfilt) r.fbits++;
+  r.ffc.resize(nfilt);
+  for (int f = 0; f < nfilt; f++) r.ffc[f] = (float)fcrit[f];   // find_peaks compares in Float32
+  r.keep_mask = true;
+  r.mask_src = mask;
+  r.npcap = false;
+  sl.filt_Rf.ensure(nfilt * 8);
+  sl.filt_ir2.ensure(nfilt * 4);
+  PPB_CUDA(cudaMemcpyAsync(sl.filt_Rf.p, r.Rf.data(), nfilt * 8, cudaMemcpyHostToDevice, r.s));
+  PPB_CUDA(cudaMemsetAsync(sl.filt_ir2.p, 0, nfilt * 4, r.s));
+  TileRes& T = sl.tile_for(n);
+  T.setup(n, r.s);
+  if (T.cap == 0) T.ensure_peaks(initial_peak_capacity(N));
+  // rfft(delta) once, projected Hermitian as run_tile's delta_k
+  PPB_CUDA(cudaMemcpyAsync(T.delta.p, delta, N * 4, cudaMemcpyDefault, r.s));
+  PPB_CUFFT(cufftExecR2C(T.r2c, T.delta.as<cufftReal>(), T.dk.as<cufftComplex>()));
+  launch_hermitise(r.L, T.dk.as<float2>(), n, 1);
+  const int64_t npk = peaks_phase(r, T, n, p.boxsize, {Win{0, 0.f}}, n);
+  *o.npeaks = npk;
+  if (npk > o.capacity) {
+    PPB_CUDA(cudaStreamSynchronize(r.s));
+    throw Error{PPB_ERR_CAPACITY, "peak output capacity too small; *npeaks holds the count needed"};
+  }
+  sl.tcen.ensure(3 * 8);
+  const double cen[3] = {xbx, ybx, zbx};
+  PPB_CUDA(cudaMemcpyAsync(sl.tcen.p, cen, 24, cudaMemcpyHostToDevice, r.s));
+  if (npk > 0) {
+    prep_phase(r, T, npk, n, 1, sl.tcen.as<double>());
+    sl.pft.ensure((size_t)npk * 24);
+    int32_t* ijk = sl.pft.as<int32_t>();
+    int64_t* ipp = reinterpret_cast<int64_t*>(sl.pft.as<char>() + (size_t)npk * 16);
+    int32_t* filt = ijk + 3 * npk;
+    unpack_peaks_kernel<<<(unsigned)((npk + 255) / 256), 256, 0, r.s>>>(T.keys_s.as<unsigned long long>(), (int)npk,
+                                                                        n, r.fbits, ijk, ipp, filt);
+    PPB_LAUNCHED(sl.launches);
+    const size_t b4 = (size_t)npk * 4, b8 = (size_t)npk * 8;
+    if (o.pi) PPB_CUDA(cudaMemcpyAsync(o.pi, ijk, b4, cudaMemcpyDefault, r.s));
+    if (o.pj) PPB_CUDA(cudaMemcpyAsync(o.pj, ijk + npk, b4, cudaMemcpyDefault, r.s));
+    if (o.pk) PPB_CUDA(cudaMemcpyAsync(o.pk, ijk + 2 * npk, b4, cudaMemcpyDefault, r.s));
+    if (o.ipp) PPB_CUDA(cudaMemcpyAsync(o.ipp, ipp, b8, cudaMemcpyDefault, r.s));
+    if (o.filter) PPB_CUDA(cudaMemcpyAsync(o.filter, filt, b4, cudaMemcpyDefault, r.s));
+    if (o.x) PPB_CUDA(cudaMemcpyAsync(o.x, T.p_pos.as<double>(), b8, cudaMemcpyDefault, r.s));
+    if (o.y) PPB_CUDA(cudaMemcpyAsync(o.y, T.p_pos.as<double>() + npk, b8, cudaMemcpyDefault, r.s));
+    if (o.z) PPB_CUDA(cudaMemcpyAsync(o.z, T.p_pos.as<double>() + 2 * npk, b8, cudaMemcpyDefault, r.s));
+    if (o.Rf) PPB_CUDA(cudaMemcpyAsync(o.Rf, T.p_Rf.as<double>(), b8, cudaMemcpyDefault, r.s));
+    if (o.FcRf) PPB_CUDA(cudaMemcpyAsync(o.FcRf, T.p_FcRf.as<float>(), b4, cudaMemcpyDefault, r.s));
+    if (o.d2Rf) {
+      // 0.0f0 without ioutshear (ext/CUDAExt.jl:3192)
+      if (!r.want_lap) PPB_CUDA(cudaMemsetAsync(T.p_d2Rf.p, 0, b4, r.s));
+      PPB_CUDA(cudaMemcpyAsync(o.d2Rf, T.p_d2Rf.as<float>(), b4, cudaMemcpyDefault, r.s));
+    }
+  }
+  PPB_CUDA(cudaMemcpyAsync(mask, T.mask.p, N, cudaMemcpyDefault, r.s));
+  PPB_CUDA(cudaStreamSynchronize(r.s));
+}
 
 void generate_fields_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, float* delta, float* psi, float* psi2,
                           float* lapd) {

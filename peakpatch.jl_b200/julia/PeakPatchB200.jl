@@ -6,7 +6,7 @@ halo-finding path.  It supplies a drop-in `run_tile(cfg; seed)` with the
 signature and behaviour of `PeakPatch.Pipeline.run_tile` (src/Pipeline.jl:66)
 and GPU methods for the stub-level entry points `fill_noise_threefry!`
 (src/InitialConditions/RandomField.jl:70), `find_peaks`
-(src/HaloFinder/PeakFind.jl:123) and a batched `analyse_peak`
+(src/HaloFinder/PeakFind.jl:15-79) and a batched `analyse_peak`
 (src/HaloFinder/RadialShell.jl:282), all through `ccall` into the C ABI
 declared in include/ppb.h.  Errors become Julia exceptions carrying the
 library's message.

@@ -7,7 +7,7 @@ Names, argument meanings and error behaviour follow the reference
   PipelineConfig            src/IO/Parameters.jl:17-125 (kwdef + TOML)
   run_tile(cfg; seed)       src/Pipeline.jl:66-325
   fill_noise_threefry!      src/InitialConditions/RandomField.jl:70-83
-  find_peaks                src/HaloFinder/PeakFind.jl:123-186
+  find_peaks                src/HaloFinder/PeakFind.jl:15-79
   analyse_peak (batched)    src/HaloFinder/RadialShell.jl:282-891
   read_homeltab             src/EllipsoidalCollapse/CollapseTable.jl:102-122
   read_filterbank           src/HaloFinder/Filters.jl:46-58
@@ -148,7 +148,7 @@ EXPORTED = (
     "ppb_analyse_peaks_lim", "ppb_set_option", "ppb_get_option", "ppb_tune_entries", "ppb_make_collapse_table",
     "ppb_last_table_stats", "ppb_downsample_noise", "ppb_extended_residual", "ppb_isolated_convolve",
     "ppb_interpolate_to_tile", "ppb_compute_2lpt", "ppb_compute_laplacian", "ppb_coarse_fields",
-    "ppb_run_multitile_split", "ppb_split_coarse_grid",
+    "ppb_run_multitile_split", "ppb_split_coarse_grid", "ppb_peak_find_tile",
 )
 
 
@@ -214,6 +214,8 @@ def load_library():
     L.ppb_run_multitile_split.argtypes = [P, ctypes.POINTER(_TileParams), P, I32, I32, I32, I32, P, I32,
                                           ctypes.POINTER(_HaloBuf)]
     L.ppb_split_coarse_grid.argtypes = [I32, I32, I32, I32, I32]
+    L.ppb_peak_find_tile.argtypes = [P, P, I32, P, P, I32, P, D, D, D, D, I32, I32, I32, I64] + [P] * 11 + \
+        [ctypes.POINTER(ctypes.c_int64)]
     for f in ("ppb_alloc_host", "ppb_alloc_device"):
         getattr(L, f).argtypes = [P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
     for f in ("ppb_free_host", "ppb_free_device"):
@@ -722,6 +724,47 @@ class Context:
         return {"i": i, "j": j, "k": k, "ipp": bp[:m].copy(), "x": xbx + alatt * (i - cen(n1)),
                 "y": ybx + alatt * (j - cen(n2)), "z": zbx + alatt * (k - cen(n3)), "delta": bd[:m].copy(),
                 "Rsmooth": np.full(m, float(Rsmooth))}
+
+    def peak_find_tile(self, delta_tile: np.ndarray, filters, fcrits, tile_masks_in: np.ndarray, xbx: float,
+                       ybx: float, zbx: float, alatt: float, nbuff: int, wsmooth: int, ioutshear: int):
+        """peak_find_tile_gpu (src/PeakPatch.jl:341-366): the filter loop of
+        smooth_field + find_peaks on a tile's own periodic grid.  filters:
+        radii (Mpc/h) or (id, fcrit, Rf) tuples, processed in the given
+        order; fcrits: one per filter.  tile_masks_in (int8, the field's
+        shape) is updated in place.  Returns (peaks, Rf, FcRf, d2Rf, mask),
+        peaks a dict of arrays (i, j, k, ipp, x, y, z, delta, Rsmooth,
+        filter) in (filter, scan) order."""
+        d = np.ascontiguousarray(delta_tile, dtype=np.float32)
+        n = d.shape[0]
+        if d.shape != (n, n, n):
+            raise ValueError("peak_find_tile needs a cubic field")
+        m = tile_masks_in
+        if m.dtype != np.int8 or not m.flags.c_contiguous or m.shape != d.shape:
+            raise ValueError("tile_masks_in must be a C-contiguous int8 array of the field's shape")
+        Rf = np.ascontiguousarray([f[2] if isinstance(f, (tuple, list)) else f for f in filters], dtype=np.float64)
+        fc = np.ascontiguousarray(np.broadcast_to(np.asarray(fcrits, dtype=np.float64), Rf.shape))
+        cap = max(1, n ** 3 // 40)
+        while True:
+            o32 = [np.empty(cap, np.int32) for _ in range(4)]
+            o64 = np.empty(cap, np.int64)
+            od = [np.empty(cap, np.float64) for _ in range(4)]
+            of = [np.empty(cap, np.float32) for _ in range(2)]
+            npk = ctypes.c_int64()
+            rc = self.L.ppb_peak_find_tile(self.h, _p(d), n, _p(Rf), _p(fc), len(Rf), _p(m), xbx, ybx, zbx, alatt,
+                                           nbuff, wsmooth, ioutshear, cap, _p(o32[0]), _p(o32[1]), _p(o32[2]),
+                                           _p(o64), _p(od[0]), _p(od[1]), _p(od[2]), _p(of[0]), _p(od[3]),
+                                           _p(of[1]), _p(o32[3]), ctypes.byref(npk))
+            if rc == -7:
+                cap = npk.value
+                continue
+            self._check(rc)
+            break
+        c = npk.value
+        peaks = {"i": o32[0][:c].astype(np.int64), "j": o32[1][:c].astype(np.int64),
+                 "k": o32[2][:c].astype(np.int64), "ipp": o64[:c].copy(), "x": od[0][:c].copy(),
+                 "y": od[1][:c].copy(), "z": od[2][:c].copy(), "delta": of[0][:c].copy(),
+                 "Rsmooth": od[3][:c].copy(), "filter": o32[3][:c].copy()}
+        return peaks, peaks["Rsmooth"].copy(), peaks["delta"].copy(), of[1][:c].copy(), m
 
     def analyse_peaks(self, fields: dict, ipp, Rf, ir2min, ZZon, fcrit, alatt: float, nhunt: int,
                       plain: bool = False, r2lim=None) -> np.ndarray:

@@ -436,3 +436,38 @@ def test_make_table_reproduces_the_reference_table(ora, julia_table):
     t = ora.make_table(0.3138, 0.0493, 0.6862, 0.6735)
     assert t.shape == julia_table.data.shape
     assert np.array_equal(t.astype(np.float32), julia_table.data)
+
+
+def test_rmax2rs_result_does_not_depend_on_peak_order(ora, eh_pk, julia_table):
+    """With rmax2rs > 0 the reference analyses peaks under Threads.@threads
+    while each collapsed halo writes the mask (RadialShell.jl:793-802) and
+    each peak may read it first (:310-316).  That read can only skip a peak
+    with floor(Rf/alatt rmax2rs) = 0, whose cell cap npart (:288-295) is then
+    at most floor(4/3 pi) = 4 cells: no shell beyond the centre closes, so
+    such a peak returns no_collapse at m0 = 1 (:650-653) whether skipped or
+    not.  The oracle shows it: peaks in list order on one thread, and in
+    reverse order, and on all threads, give the same results bit for bit,
+    and every peak the mask could skip has no halo."""
+    n, box, nbuff = 48, 96.0, 12
+    cfg = ora.Config(Omx=0.315 - 0.049, OmB=0.049, Omvac=0.685, h=0.674, n=n, boxsize=box, nbuff=nbuff,
+                     ilpt=2, ioutshear=1, wsmooth=1, rmax2rs=1.0)
+    from conftest import filter_bank
+    st = ora.run_tile_stages(cfg, 5, *eh_pk, filter_bank(), julia_table, peak_sample=np.arange(0))
+    ipp, Rf, ir2, Z = st["peaks"]["ipp"], st["Rf"], st["ir2min"], st["ZZon"]
+    alatt = st["alatt"]
+    skippable = np.floor(Rf / alatt * 1.0) == 0
+    assert skippable.sum() > 10 and (~skippable).sum() > 100
+    runs = []
+    for order, serial in ((np.arange(len(ipp)), True), (np.arange(len(ipp))[::-1], True),
+                          (np.arange(len(ipp)), False)):
+        mask = np.zeros((n, n, n), np.int8)
+        r = ora.analyse_peaks(st["fields"], ipp[order], Rf[order], ir2[order], Z[order], st["fcrit"], alatt,
+                              st["shells"], julia_table, nbuff=nbuff, rmax2rs=1.0, mask=mask, serial_mask=serial)
+        out = np.empty_like(r)
+        out[order] = r
+        runs.append((out, mask))
+    for out, mask in runs[1:]:
+        assert np.array_equal(out.view(np.uint64), runs[0][0].view(np.uint64))
+        assert np.array_equal(mask, runs[0][1])
+    assert np.all(runs[0][0][skippable, 0] == -1.0)
+    assert (runs[0][0][:, 0] > 0).sum() > 50

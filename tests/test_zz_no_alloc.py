@@ -64,10 +64,14 @@ def _noalloc(ctx, d_delta, d_mask, shape, nbuff, fcrit, max_peaks, cap):
     return res
 
 
-@pytest.mark.parametrize("max_peaks", [2_000_000, 37])
+# max_peaks 0 keeps the first peak, as the reference (it tests the count
+# after each push); on the 80^3 grid (72^3 inner cells, 365 blocks of the
+# ordered compaction, 6707 peaks of which 4736 lie in blocks 0-255) 5500 ends
+# the scan inside the second 256-block chunk of the block-offset scan
+@pytest.mark.parametrize("max_peaks", [2_000_000, 37, 5500, 0])
 def test_noalloc_matches_find_peaks_on_two_consecutive_calls(max_peaks):
     with pp.Context(0) as ctx:
-        for call, (n, nbuff, seed) in enumerate([(64, 4, 1), (57, 3, 2)]):
+        for call, (n, nbuff, seed) in enumerate([(64, 4, 1), (57, 3, 2), (80, 4, 3)]):
             f = _field(n, seed)
             mask0 = np.zeros(f.shape, np.int8)
             mask0[::7, ::5, ::3] = 1            # a partly masked grid, as across filters
@@ -75,7 +79,7 @@ def test_noalloc_matches_find_peaks_on_two_consecutive_calls(max_peaks):
             # reference: the allocating entry point on host copies
             m_ref = mask0.copy()
             ref = ctx.find_peaks(f, m_ref, 0.0, 0.0, 0.0, 1.0, nbuff, fcrit, max_peaks=max_peaks)
-            assert len(ref["i"]) > 30
+            assert len(ref["i"]) == 1 if max_peaks == 0 else len(ref["i"]) > 30
             # the no-allocation entry point on caller-owned device buffers
             d_f = _h2d(ctx, f)
             d_m = _h2d(ctx, mask0)
