@@ -232,8 +232,8 @@ int32_t ppb_find_peaks_noalloc(ppb_ctx* ctx, const float* delta, int8_t* mask, i
  *   0 RTHL, 1 Srb, 2-4 Sbar, 5-7 Sbar2, 8-16 strain (column-major 3x3),
  *   17-19 gradpk, 20-22 gradpkrf, 23 Fbarx, 24 e_v, 25 p_v, 26 zvir_half,
  *   27-29 gradpkf, 30 d2F.
- * rmax2rs > 0 is rejected with PPB_ERR_UNSUPPORTED (the reference's result
- * then depends on thread scheduling). */
+ * The whole list is analysed (rmax2rs = 0); ppb_analyse_peaks_multirf takes
+ * rmax2rs and a mask. */
 int32_t ppb_analyse_peaks(ppb_ctx* ctx, const float* delta, const float* etax, const float* etay,
                           const float* etaz, const float* eta2x, const float* eta2y,
                           const float* eta2z, const float* lapd, int32_t n, int32_t nhunt,
@@ -249,6 +249,36 @@ int32_t ppb_analyse_peaks_lim(ppb_ctx* ctx, const float* delta, const float* eta
                               const float* lapd, int32_t n, int32_t nhunt, int64_t npk, const int64_t* ipp,
                               const double* Rf, const int64_t* ir2min, const double* ZZon, const double* fcrit,
                               const int32_t* r2lim, double alatt, int32_t plain, double* out);
+
+/* analyse_peaks_gpu_cuda_multirf(delta, etax, etay, etaz, eta2x, eta2y,
+ * eta2z, batches, stab, ct_table, X1, X2, Y1, Y2, Z1, Z2, alatt, ZZon; lapd,
+ * mask, nbuff, growth_tables, rmax2rs, fcrit_override) (src/PeakPatch.jl:
+ * 231-253; batch tuple ext/CUDAExt.jl:2327-2334): analyse_peak
+ * (RadialShell.jl:282-891) over nbatch batches of peaks, one filter scale
+ * each.  Batch b holds peaks boff[b] .. boff[b+1]-1 with 1-based pi, pj, pk,
+ * the batch's Rf[b] (Mpc/h) and ir2min[b]; ZZon_pp / fcrit_pp give per-peak
+ * redshift and fcrit (the 7-tuple batches of the lightcone) or are both NULL
+ * for the scalars ZZon and fcrit (the caller resolves fcrit_override /
+ * fsc_of_z(ZZon - 1) / 1.686 as the reference does).  The shell list is
+ * precompute_shells(nhunt) (stab); the collapse table is the resident one
+ * (ppb_set_collapse_table with the X1..Z2 ranges).  rmax2rs > 0 caps each
+ * peak's list at npart = min(floor(4/3 pi (rmax2rs Rf/alatt)^3), npartmax)
+ * cells.  mask (n^3 Int8, or NULL) is read and updated batch by batch: a
+ * peak of batch b is skipped (no collapse) when rmax2rs > 0 and its cell's
+ * mask value, as it stood before batch b, exceeds floor(Rf/alatt rmax2rs);
+ * after batch b every halo of the batch sets mask = 1 over its cells within
+ * RTHL in the interior nbuff+1 .. n-nbuff (the reference's GPU method reads
+ * and writes the mask from concurrent threads inside a batch).  Fields and
+ * per-peak arrays may be host or device memory; boff, Rf and ir2min are host
+ * arrays.  out: boff[nbatch] x 31 doubles in the layout of
+ * ppb_analyse_peaks. */
+int32_t ppb_analyse_peaks_multirf(ppb_ctx* ctx, const float* delta, const float* etax, const float* etay,
+                                  const float* etaz, const float* eta2x, const float* eta2y, const float* eta2z,
+                                  const float* lapd, int32_t n, int32_t nhunt, int32_t nbatch, const int64_t* boff,
+                                  const int32_t* pi, const int32_t* pj, const int32_t* pk, const double* Rf,
+                                  const int64_t* ir2min, const double* ZZon_pp, const double* fcrit_pp, double ZZon,
+                                  double fcrit, double alatt, int8_t* mask, int32_t nbuff, double rmax2rs,
+                                  int32_t plain, double* out);
 
 /* ---- multi-resolution tile fields ---------------------------------------
  * The MUSIC-style split of run_multitile_split (src/MultiResolution.jl:523-

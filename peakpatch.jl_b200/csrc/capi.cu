@@ -228,6 +228,9 @@ ShellArgs ppb_ctx::shell_args(Slot& sl, ShellTable& shells, int n, double alatt,
   a.nshell = shells.nshell;
   a.mmax = std::max(shells.nshell - 1, 1);
   a.npart = shells.ncells;
+  a.ch_max = shells.ch_max;
+  a.d_max = shells.nhunt;
+  a.fmax = pack_fmax(const_cast<float4*>(aos), n);
   a.tab = sh.dtab;
   a.akk = sh.akk.as<double>();
   return a;
@@ -327,7 +330,7 @@ TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool ad
   for (int c = 0; c < 4; c++) te.collapse_ms[c] = 1e30f;
   for (int round = 0; round < 2; round++) {
     for (int c = 0; c < 5; c++) {
-      PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, 16, s));
+      PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, kCtlBytes, s));
       shell_order(sl, b, bricks[c]);
       PPB_CUDA(cudaEventRecord(ev[0], s));
       launch_shell_gather(L, b, comp, adaptive, gblocks);
@@ -361,7 +364,7 @@ TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool ad
     if (te.collapse_ms[c] < te.collapse_ms[ci]) ci = c;
   te.collapse_threads = te.collapse_ms[ci] < 0.97f * te.collapse_ms[di] ? widths[ci] : 0;
   PPB_CUDA(cudaMemcpyAsync(sl.counters.p, sl.tune_save.p, 16 * 8, cudaMemcpyDeviceToDevice, s));
-  PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, 16, s));
+  PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, kCtlBytes, s));
   return te;
 }
 
@@ -384,7 +387,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
   const int64_t stride = shell_stage_doubles_per_warp(a.nshell);
   sl.stage.ensure((size_t)((int64_t)gblocks * kGatherWarps * stride * 8));
   sl.counters.ensure(16 * 8);
-  sl.ctl.ensure(64);
+  sl.ctl.ensure(kCtlBytes);
   grow(sl.hdr, std::max<size_t>(1, (size_t)a.npk) * sizeof(PeakHdr));
   grow(sl.geo, std::max<size_t>(1, (size_t)a.npk) * sizeof(int4));
   grow(sl.mlim, std::max<size_t>(1, (size_t)a.npk) * sizeof(int32_t));
@@ -480,7 +483,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     // zvir_half, d2F, with timing events between the kernels
     captured(sl, sl.graphs, 2, (int64_t)a.n * 4 + (comp ? 2 : 0) + (adaptive ? 1 : 0), [&] {
       if (first && pre) pre();
-      PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, 16, stream));
+      PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, kCtlBytes, stream));
       record_event(sl.shell_ev[0], stream);
       shell_order(sl, b, te.brick_shift);
       launch_shell_gather(L, b, comp, adaptive, gblocks);

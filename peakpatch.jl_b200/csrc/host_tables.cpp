@@ -102,6 +102,7 @@ void build_shell_table(ShellTable& st, int nhunt) {
   // gather schedule (shells 2..mmax; shell m is distinct value m-1)
   st.grp_a.clear(); st.grp_b.clear(); st.grp_c.clear();
   st.ck_s.clear(); st.ck_n.clear();
+  st.ch_max = 0;
   st.sh_c0.assign(st.nshell + 1, 0);
   st.sh_nc.assign(st.nshell + 1, 0);
   int in_group = 0;
@@ -129,6 +130,7 @@ void build_shell_table(ShellTable& st, int nhunt) {
       const int a = (int)((int64_t)cnt * c / nck), b = (int)((int64_t)cnt * (c + 1) / nck);
       st.ck_s.push_back(s0 + a);
       st.ck_n.push_back(b - a);
+      st.ch_max = std::max(st.ch_max, b - a);
     }
     in_group += nck;
     st.grp_b.back() = m;

@@ -293,14 +293,18 @@ __global__ void hermitise_kernel(float2* __restrict__ data, int n, int nbatch) {
 }
 
 // ---------------------------------------------------------------------------
-// gather-field pack: per cell two float4 = (delta, deltaT, psi_x, psi_y),
-// (psi_z, psi2_x, psi2_y, psi2_z).  deltaT at (a,b,c) is delta(c,a,b): the
+// gather-field pack: per cell two float4 = (delta, deltaT, psi_z, psi2_x),
+// (psi_x, psi_y, psi2_y, psi2_z), the pairing of the shell gather's packed
+// FP32x2 sums.  deltaT at (a,b,c) is delta(c,a,b): the
 // transposed read delta[iv3, iv1, iv2] of RadialShell.jl:448, made into a
 // plain array so the shell gather reads one 32-byte record per cell.
 // Block: 32 x 8 threads over a 32 (a) x 32 (c) tile at fixed b.
 // ---------------------------------------------------------------------------
 __global__ void pack_kernel(float4* __restrict__ aos, FieldWindow w, int n) {
   __shared__ float tile[32][33];
+  __shared__ float wmax[8][7];
+  // largest |value| per field seen by this thread: delta, psi x, y, z, psi2 x, y, z
+  float fm[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   const int b = blockIdx.z;
   const int a0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
   const int64_t n2 = (int64_t)n * n;
@@ -320,18 +324,42 @@ __global__ void pack_kernel(float4* __restrict__ aos, FieldWindow w, int n) {
     float4 v0, v1;
     v0.x = w.delta[g];
     v0.y = dT;
-    v0.z = w.psi[g];
-    v0.w = w.psi[w.cs + g];
-    v1.x = w.psi[2 * w.cs + g];
+    v0.z = w.psi[2 * w.cs + g];
+    v1.x = w.psi[g];
+    v1.y = w.psi[w.cs + g];
     if (w.psi2) {
-      v1.y = w.psi2[g];
+      v0.w = w.psi2[g];
       v1.z = w.psi2[w.cs + g];
       v1.w = w.psi2[2 * w.cs + g];
     } else {
-      v1.y = v1.z = v1.w = 0.f;
+      v0.w = v1.z = v1.w = 0.f;
     }
     aos[2 * lin] = v0;
     aos[2 * lin + 1] = v1;
+    fm[0] = fmaxf(fm[0], fabsf(v0.x));
+    fm[1] = fmaxf(fm[1], fabsf(v1.x));
+    fm[2] = fmaxf(fm[2], fabsf(v1.y));
+    fm[3] = fmaxf(fm[3], fabsf(v0.z));
+    fm[4] = fmaxf(fm[4], fabsf(v0.w));
+    fm[5] = fmaxf(fm[5], fabsf(v1.z));
+    fm[6] = fmaxf(fm[6], fabsf(v1.w));
+  }
+  // the block's field maxima into one of kFmaxSlots slots (spreads the
+  // atomics over addresses); non-negative floats order as their bit patterns
+#pragma unroll
+  for (int f = 0; f < 7; f++)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) fm[f] = fmaxf(fm[f], __shfl_xor_sync(0xffffffffu, fm[f], o));
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int f = 0; f < 7; f++) wmax[threadIdx.y][f] = fm[f];
+  __syncthreads();
+  const int t = threadIdx.y * 32 + threadIdx.x;
+  if (t < 7) {
+    float m = 0.f;
+    for (int y = 0; y < (int)blockDim.y; y++) m = fmaxf(m, wmax[y][t]);
+    const unsigned slot = (blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)) % kFmaxSlots;
+    atomicMax(pack_fmax(aos, n) + t * kFmaxSlots + slot, __float_as_uint(m));
   }
 }
 
@@ -542,6 +570,7 @@ void launch_hermitise(Launch L, float2* data, int n, int nbatch) {
 }
 
 void launch_pack(Launch L, float4* aos, const FieldWindow& w, int n) {
+  PPB_CUDA(cudaMemsetAsync(pack_fmax(aos, n), 0, 7 * kFmaxSlots * sizeof(unsigned), L.s));
   dim3 grid((n + 31) / 32, (n + 31) / 32, n);
   pack_kernel<<<grid, dim3(32, 8), 0, L.s>>>(aos, w, n);
   PPB_LAUNCHED(*L.count);

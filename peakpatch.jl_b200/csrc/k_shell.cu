@@ -16,10 +16,11 @@
 //    16-byte load, four 32-byte records in flight per lane, each one 256-bit
 //    load), lane l then finalises shell l of the group from the
 //    chunk partials, and the cumulative profile Fbar comes from a warp scan
-//    of r^3 Fbar.  Sums are compensated single precision (two-sum, error-free
-//    per addend) on the optimised path and double precision on the plain
-//    path; in both the addends are the single-precision products the
-//    reference forms (Float32 field times Int32 offset).
+//    of r^3 Fbar.  Sums are compensated single precision (anchored Fast2Sum:
+//    each rounding error is captured exactly and summed apart) on the
+//    optimised path and double precision on the plain path; in both the
+//    addends are the single-precision products the reference forms (Float32
+//    field times Int32 offset).
 //    Adaptive truncation (optimised path): the warp stops gathering once
 //    every shell later read is in, i.e. all shells up to rad[M] + 2 with
 //    M = max(crossing shell, first shell beyond ir2min, Rf window):
@@ -48,7 +49,7 @@ namespace ppb {
 
 namespace {
 
-constexpr int NACC = 19;   // gather accumulators: F, S3, S2_3, G3, Gf3, Q6 (xx yy zz xy xz yz)
+constexpr int NACC = 19;   // gather sums: F, S3, S2_3, G3, Gf3, Q6 (xx yy zz xy xz yz)
 constexpr unsigned FULL = 0xffffffffu;
 
 // counters layout
@@ -70,101 +71,76 @@ template <> struct Acc<false> {      // double precision (the reference's Float6
   __device__ __forceinline__ double get(int i) const { return s[i]; }
 };
 
-// Compensated single precision (optimised path).  The 22 addends of a cell
-// go to 11 packed FP32x2 accumulators plus one scalar, pairing values that
-// arrive in adjacent registers of the two 16-byte record loads, so that one
-// instruction serves two sums.  Each component keeps (s, c) with the
-// two-sum (Knuth) t = s + x, b' = t - s, e = (s - (t - b')) + (x - b'), so
-// that t + e == s + x exactly; c collects the e.  Component map:
-//   P0 = (delta, deltaT)  P1 = (psi_x, psi_y)  P2 = (psi_z, psi2_x)  P3 = (psi2_y, psi2_z)
-//   P4..P6 = (delta, deltaT) * d_i, d_j, d_k
-//   P7 = (psi_x d_i, psi_y d_j)  P8 = (psi_x d_j, psi_y d_i)
-//   P9 = (psi_x d_k, psi_y d_k)  P10 = (psi_z d_i, psi_z d_j)  scalar = psi_z d_k
-// (the deltaT sum of P0.y is not used).
+// Compensated single precision (optimised path): NP packed FP32x2 sums,
+// anchored.  Component i starts at a power of two K_i (per warp, in shared
+// memory) with |x| <= K_i / (2 CH) for each of its addends x, CH the longest
+// chunk, so its running sum s stays in [K_i/2, 3K_i/2]: |s| >= |x| at every
+// addition, and Fast2Sum (t = s + x, e = x - (t - s)) gives the exact
+// rounding error e of t in three operations; c collects the e.  The chunk's
+// sum is (s - K_i) + c, where s - K_i is exact (Sterbenz).  One FP32x2
+// instruction serves two sums.
 __device__ __forceinline__ float2 fsub2(float2 a, float2 b) {   // a - b, rounded once
   return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
 }
-struct AccP {
-  float2 s[11], c[11];
-  float s1, c1;
+template <int NP> struct AccH {
+  float2 s[NP], c[NP];
+  const float2* K;   // the anchors (shared memory)
   __device__ __forceinline__ void zero() {
 #pragma unroll
-    for (int i = 0; i < 11; i++) { s[i] = make_float2(0.f, 0.f); c[i] = make_float2(0.f, 0.f); }
-    s1 = 0.f;
-    c1 = 0.f;
+    for (int i = 0; i < NP; i++) { s[i] = K[i]; c[i] = make_float2(0.f, 0.f); }
   }
   __device__ __forceinline__ void add(int i, float2 x) {
     const float2 t = __fadd2_rn(s[i], x);
-    const float2 bp = fsub2(t, s[i]);
-    const float2 e = __fadd2_rn(fsub2(s[i], fsub2(t, bp)), fsub2(x, bp));
+    c[i] = __fadd2_rn(c[i], fsub2(x, fsub2(t, s[i])));
     s[i] = t;
-    c[i] = __fadd2_rn(c[i], e);
   }
-  __device__ __forceinline__ void add1(float x) {
-    const float t = __fadd_rn(s1, x);
-    const float bp = __fsub_rn(t, s1);
-    const float e = __fadd_rn(__fsub_rn(s1, __fsub_rn(t, bp)), __fsub_rn(x, bp));
-    s1 = t;
-    c1 = __fadd_rn(c1, e);
-  }
-  __device__ __forceinline__ double X(int i) const { return (double)s[i].x + (double)c[i].x; }
-  __device__ __forceinline__ double Y(int i) const { return (double)s[i].y + (double)c[i].y; }
-  // the 19 sums in the order of accumulate_cell
-  __device__ __forceinline__ double get(int v) const {
-    switch (v) {
-      case 0: return X(0);
-      case 1: return X(1);
-      case 2: return Y(1);
-      case 3: return X(2);
-      case 4: return Y(2);
-      case 5: return X(3);
-      case 6: return Y(3);
-      case 7: return X(4);
-      case 8: return X(5);
-      case 9: return X(6);
-      case 10: return Y(4);
-      case 11: return Y(5);
-      case 12: return Y(6);
-      case 13: return X(7);
-      case 14: return Y(7);
-      case 15: return (double)s1 + (double)c1;
-      case 16: return X(8) + Y(8);
-      case 17: return X(9) + X(10);
-      default: return Y(9) + Y(10);
-    }
-  }
+  __device__ __forceinline__ double X(int i) const { return (double)__fsub_rn(s[i].x, K[i].x) + (double)c[i].x; }
+  __device__ __forceinline__ double Y(int i) const { return (double)__fsub_rn(s[i].y, K[i].y) + (double)c[i].y; }
 };
 
-__device__ __forceinline__ void accumulate_cell_packed(AccP& A, const float4 a, const float4 b, float di, float dj,
-                                                       float dk) {
-  const float2 p0 = make_float2(a.x, a.y), p1 = make_float2(a.z, a.w);
-  A.add(0, p0);
-  A.add(1, p1);
-  A.add(2, make_float2(b.x, b.y));
-  A.add(3, make_float2(b.z, b.w));
-  A.add(4, __fmul2_rn(p0, make_float2(di, di)));
-  A.add(5, __fmul2_rn(p0, make_float2(dj, dj)));
-  A.add(6, __fmul2_rn(p0, make_float2(dk, dk)));
-  A.add(7, __fmul2_rn(p1, make_float2(di, dj)));
-  A.add(8, __fmul2_rn(p1, make_float2(dj, di)));
-  A.add(9, __fmul2_rn(p1, make_float2(dk, dk)));
-  A.add(10, __fmul2_rn(make_float2(b.x, b.x), make_float2(di, dj)));
-  A.add1(__fmul_rn(b.x, dk));
+// smallest power of two >= v (v >= 0 finite; 0 stays 0)
+__device__ __forceinline__ float pow2_ceil(float v) {
+  unsigned u = __float_as_uint(v);
+  if (u & 0x7fffffu) u = (u + 0x800000u) & 0xff800000u;
+  return __uint_as_float(u);
 }
 
-template <bool COMP>
-__device__ __forceinline__ void accumulate_cell(Acc<COMP>& A, const float4 a, const float4 b, float di,
-                                                float dj, float dk) {
-  // a = (delta, deltaT, psi_x, psi_y), b = (psi_z, psi2_x, psi2_y, psi2_z)
-  A.add(0, a.x);
-  A.add(1, a.z); A.add(2, a.w); A.add(3, b.x);
-  A.add(4, b.y); A.add(5, b.z); A.add(6, b.w);
-  A.add(7, __fmul_rn(a.x, di)); A.add(8, __fmul_rn(a.x, dj)); A.add(9, __fmul_rn(a.x, dk));
-  A.add(10, __fmul_rn(a.y, di)); A.add(11, __fmul_rn(a.y, dj)); A.add(12, __fmul_rn(a.y, dk));
-  A.add(13, __fmul_rn(a.z, di)); A.add(14, __fmul_rn(a.w, dj)); A.add(15, __fmul_rn(b.x, dk));
-  A.add(16, __fmul_rn(a.z, dj)); A.add(16, __fmul_rn(a.w, di));
-  A.add(17, __fmul_rn(a.z, dk)); A.add(17, __fmul_rn(b.x, di));
-  A.add(18, __fmul_rn(a.w, dk)); A.add(18, __fmul_rn(b.x, dj));
+// The packed record of a cell is two float4 halves,
+//   h0 = (delta, deltaT, psi_z, psi2_x),  h1 = (psi_x, psi_y, psi2_y, psi2_z),
+// read with one 256-bit load.  The 22 addends of a cell (11 packed sums):
+//   P0 (delta, psi_z d_k)  P1 (psi_x, psi_y)  P2 (psi_z, psi2_x)  P3 (psi2_y, psi2_z)
+//   P4..P6 (delta, deltaT) * d_i, d_j, d_k
+//   P7 (psi_x d_i, psi_y d_j)  P8 (psi_x d_j, psi_y d_i)  P9 (psi_x d_k, psi_y d_k)
+//   P10 (psi_z d_i, psi_z d_j)
+__device__ __forceinline__ void accumulate_cell_comp(AccH<11>& A, const float4 h0, const float4 h1, float di,
+                                                     float dj, float dk) {
+  const float2 dd = make_float2(h0.x, h0.y), pxy = make_float2(h1.x, h1.y);
+  A.add(0, make_float2(h0.x, __fmul_rn(h0.z, dk)));
+  A.add(1, pxy);
+  A.add(2, make_float2(h0.z, h0.w));
+  A.add(3, make_float2(h1.z, h1.w));
+  A.add(4, __fmul2_rn(dd, make_float2(di, di)));
+  A.add(5, __fmul2_rn(dd, make_float2(dj, dj)));
+  A.add(6, __fmul2_rn(dd, make_float2(dk, dk)));
+  A.add(7, __fmul2_rn(pxy, make_float2(di, dj)));
+  A.add(8, __fmul2_rn(pxy, make_float2(dj, di)));
+  A.add(9, __fmul2_rn(pxy, make_float2(dk, dk)));
+  A.add(10, __fmul2_rn(make_float2(h0.z, h0.z), make_float2(di, dj)));
+}
+
+// one cell of the plain path: both halves, 19 double sums
+__device__ __forceinline__ void accumulate_cell(Acc<false>& A, const float4 h0, const float4 h1, float di, float dj,
+                                                float dk) {
+  const float delta = h0.x, deltaT = h0.y, px = h1.x, py = h1.y, pz = h0.z;
+  A.add(0, delta);
+  A.add(1, px); A.add(2, py); A.add(3, pz);
+  A.add(4, h0.w); A.add(5, h1.z); A.add(6, h1.w);
+  A.add(7, __fmul_rn(delta, di)); A.add(8, __fmul_rn(delta, dj)); A.add(9, __fmul_rn(delta, dk));
+  A.add(10, __fmul_rn(deltaT, di)); A.add(11, __fmul_rn(deltaT, dj)); A.add(12, __fmul_rn(deltaT, dk));
+  A.add(13, __fmul_rn(px, di)); A.add(14, __fmul_rn(py, dj)); A.add(15, __fmul_rn(pz, dk));
+  A.add(16, __fmul_rn(px, dj)); A.add(16, __fmul_rn(py, di));
+  A.add(17, __fmul_rn(px, dk)); A.add(17, __fmul_rn(pz, di));
+  A.add(18, __fmul_rn(py, dk)); A.add(18, __fmul_rn(pz, dj));
 }
 
 // ---------------------------------------------------------------------------
@@ -264,7 +240,36 @@ __device__ __forceinline__ void unpack_cell(int w, int& di, int& dj, int& dk) {
 }
 
 // shared memory of one gather warp, in doubles: the chunk partials
-constexpr int GATHER_WARP_DOUBLES = (NACC + 1) * 32;
+constexpr int GATHER_WARP_DOUBLES = (NACC + 1) * 32 + 12;   // + the anchors (12 float2)
+
+// The anchors of one warp's compensated sums from the field maxima the pack
+// kernel left after the records.  K = 2^ceil(log2(2 CH M)) with M the
+// largest magnitude of the component's addends (a field maximum, times
+// d_max for the products with an offset), so |x| <= K / (2 CH).
+__device__ __forceinline__ void set_anchors(const ShellArgs& a, float2* K) {
+  const int lane = threadIdx.x & 31;
+  float M[7];   // delta, psi x, y, z, psi2 x, y, z
+#pragma unroll
+  for (int f = 0; f < 7; f++) {
+    float m = 0.f;
+    for (int q = lane; q < kFmaxSlots; q += 32) m = fmaxf(m, __uint_as_float(__ldg(a.fmax + f * kFmaxSlots + q)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+    M[f] = m;
+  }
+  if (lane == 0) {
+    const float w = 2.0f * (float)a.ch_max, wd = w * (float)a.d_max;
+    auto k = [](float m, float scale) { return pow2_ceil(m * scale); };
+    K[0] = make_float2(k(M[0], w), k(M[3], wd));
+    K[1] = make_float2(k(M[1], w), k(M[2], w));
+    K[2] = make_float2(k(M[3], w), k(M[4], w));
+    K[3] = make_float2(k(M[5], w), k(M[6], w));
+    for (int i = 4; i < 7; i++) K[i] = make_float2(k(M[0], wd), k(M[0], wd));
+    for (int i = 7; i < 10; i++) K[i] = make_float2(k(M[1], wd), k(M[2], wd));
+    K[10] = make_float2(k(M[3], wd), k(M[3], wd));
+  }
+  __syncwarp();
+}
 
 // One cell's 32-byte record with one 256-bit load (Blackwell's
 // ld.global.v8): one L1 tag lookup per cell instead of two 16-byte loads.
@@ -283,13 +288,14 @@ __device__ __forceinline__ float small_int_float(int d) {
   return __fsub_rn(__int_as_float(0x4B400000 + d), 12582912.0f);
 }
 
-// Sum one chunk (ck_n cells of chunk ck of the schedule) into A, four cells
-// per step: the offsets of the four cells come packed in one 16-byte load of
-// the chunk-major cell list (loaded one step ahead), the four 32-byte records
-// are issued together.  Returns the number of in-grid cells.
-template <class AccT, bool COMP>
-__device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, int64_t lin, bool inside, int pi,
-                                         int pj, int pk, AccT& A) {
+// Visit the cells of one chunk (ck_n cells of chunk ck of the schedule),
+// four at a time: the offsets of four cells come packed in one 16-byte load
+// of the chunk-major cell list (loaded one step ahead) and their 32-byte
+// records are in flight together.  cell(h0, h1, di, dj, dk) receives each
+// in-grid cell; returns their number.
+template <class F>
+__device__ __forceinline__ int visit_chunk(const ShellArgs& a, int ck, int cnt, int64_t lin, bool inside, int pi,
+                                           int pj, int pk, F&& cell) {
   const int n = a.n, n2 = a.n * a.n;   // n <= 4096: every offset fits 32 bits
   const float4* __restrict__ aos = a.aos;
   const int4* __restrict__ cp = a.ck_cells + __ldg(a.ck_p + ck);
@@ -319,12 +325,58 @@ __device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, in
     for (int u = 0; u < 4; u++) {
       if (ok[u]) {
         nsh++;
-        const float fi = small_int_float(d[u][0]), fj = small_int_float(d[u][1]), fk = small_int_float(d[u][2]);
-        if constexpr (COMP) accumulate_cell_packed(A, ra[u], rb[u], fi, fj, fk);
-        else accumulate_cell<false>(A, ra[u], rb[u], fi, fj, fk);
+        cell(ra[u], rb[u], small_int_float(d[u][0]), small_int_float(d[u][1]), small_int_float(d[u][2]));
       }
     }
   }
+  return nsh;
+}
+
+// the chunk's 19 sums (and its in-grid cell count) into column `col` of the
+// warp's partial table
+template <bool COMP>
+__device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, int64_t lin, bool inside, int pi,
+                                         int pj, int pk, double* part, int col) {
+  int nsh;
+  const float2* K = reinterpret_cast<const float2*>(part + (NACC + 1) * 32);
+  if constexpr (COMP) {
+    AccH<11> A;
+    A.K = K;
+    A.zero();
+    nsh = visit_chunk(a, ck, cnt, lin, inside, pi, pj, pk,
+                         [&](const float4& h0, const float4& h1, float di, float dj, float dk) {
+                           accumulate_cell_comp(A, h0, h1, di, dj, dk);
+                         });
+    part[0 * 32 + col] = A.X(0);
+    part[1 * 32 + col] = A.X(1);
+    part[2 * 32 + col] = A.Y(1);
+    part[3 * 32 + col] = A.X(2);
+    part[4 * 32 + col] = A.Y(2);
+    part[5 * 32 + col] = A.X(3);
+    part[6 * 32 + col] = A.Y(3);
+    part[7 * 32 + col] = A.X(4);
+    part[8 * 32 + col] = A.X(5);
+    part[9 * 32 + col] = A.X(6);
+    part[10 * 32 + col] = A.Y(4);
+    part[11 * 32 + col] = A.Y(5);
+    part[12 * 32 + col] = A.Y(6);
+    part[13 * 32 + col] = A.X(7);
+    part[14 * 32 + col] = A.Y(7);
+    part[15 * 32 + col] = A.Y(0);
+    part[16 * 32 + col] = A.X(8) + A.Y(8);    // psi_x d_j + psi_y d_i
+    part[17 * 32 + col] = A.X(9) + A.X(10);   // psi_x d_k + psi_z d_i
+    part[18 * 32 + col] = A.Y(9) + A.Y(10);   // psi_y d_k + psi_z d_j
+  } else {
+    Acc<false> A;
+    A.zero();
+    nsh = visit_chunk(a, ck, cnt, lin, inside, pi, pj, pk,
+                         [&](const float4& h0, const float4& h1, float di, float dj, float dk) {
+                           accumulate_cell(A, h0, h1, di, dj, dk);
+                         });
+#pragma unroll
+    for (int v = 0; v < NACC; v++) part[v * 32 + col] = A.get(v);
+  }
+  part[NACC * 32 + col] = (double)nsh;
   return nsh;
 }
 
@@ -358,14 +410,14 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
   const float4* __restrict__ aos = a.aos;
   float4 c0, c1;
   ldg_record(aos + 2 * lin, c0, c1);
-  if (lane < ROW) {
+  if (lane < ROW) {   // c0 = (delta, deltaT, psi_z, psi2_x), c1 = (psi_x, psi_y, psi2_y, psi2_z)
     double v = 0.0;
     if (lane == R_FBAR) v = (double)c0.x;
     else if (lane == R_N) v = 1.0;
-    else if (lane == R_S) v = (double)c0.z;
-    else if (lane == R_S + 1) v = (double)c0.w;
-    else if (lane == R_S + 2) v = (double)c1.x;
-    else if (lane == R_S2) v = (double)c1.y;
+    else if (lane == R_S) v = (double)c1.x;
+    else if (lane == R_S + 1) v = (double)c1.y;
+    else if (lane == R_S + 2) v = (double)c0.z;
+    else if (lane == R_S2) v = (double)c0.w;
     else if (lane == R_S2 + 1) v = (double)c1.z;
     else if (lane == R_S2 + 2) v = (double)c1.w;
     stage[ROW + lane] = v;
@@ -387,14 +439,8 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
     const int c0g = __ldg(a.grp_c + g), ncg = __ldg(a.grp_c + g + 1) - c0g;
     // (a) lane l sums chunk c0g + l into the shared partial table
     if (lane < ncg) {
-      typename std::conditional<COMP, AccP, Acc<false>>::type A;
-      A.zero();
       const int s0 = __ldg(a.ck_s + c0g + lane), cnt = s0 < cell_lim ? __ldg(a.ck_n + c0g + lane) : 0;
-      const int nsh = sum_chunk<decltype(A), COMP>(a, c0g + lane, cnt, lin, inside, pi, pj, pk, A);
-      visits += nsh;
-#pragma unroll
-      for (int v = 0; v < NACC; v++) part[v * 32 + lane] = A.get(v);
-      part[NACC * 32 + lane] = (double)nsh;
+      visits += sum_chunk<COMP>(a, c0g + lane, cnt, lin, inside, pi, pj, pk, part, lane);
     }
     __syncwarp();
     // (b) lane l finalises shell base + l from its chunks (double-precision
@@ -565,6 +611,7 @@ __global__ void __launch_bounds__(32 * kGatherWarps, PPB_GATHER_MINB) gather_ker
   const int64_t slot = (int64_t)blockIdx.x * kGatherWarps + wib;
   double* stage = a.stage + slot * a.stage_stride;
   double* part = gsm + (size_t)wib * GATHER_WARP_DOUBLES;
+  if (COMP) set_anchors(a, reinterpret_cast<float2*>(part + (NACC + 1) * 32));
   while (true) {
     int q = 0;
     if (lane == 0) q = atomicAdd(a.queue, 1);
@@ -1262,7 +1309,43 @@ __global__ void __launch_bounds__(128) d2f_kernel(ShellArgs a) {
   }
 }
 
+// ===========================================================================
+// mask writes (one warp per collapsed peak, grid-stride)
+// ===========================================================================
+// mask := 1 at the cells of the list (cells 1..npart) with sqrt(r2) <= RTHL
+// that lie in the interior nbuff+1 .. n-nbuff on every axis
+// (RadialShell.jl:793-802); the cells within RTHL are a prefix of the list.
+__global__ void __launch_bounds__(128) mask_kernel(ShellArgs a, uint8_t* mask, int nbuff) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int n = a.n;
+  const int64_t n2 = (int64_t)n * n;
+  for (int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); p < a.npk; p += nwarps) {
+    const double RTHL = a.out[p * RES_N];
+    if (!(RTHL > 0.0)) continue;
+    const int64_t lin = a.pk.lin[p];
+    const int pk = (int)(lin / n2), pj = (int)((lin / n) % n), pi = (int)(lin % n);
+    const int mR = first_gt(a.rad, 1, a.nshell, RTHL);
+    int64_t cend = mR <= a.nshell ? (int64_t)__ldg(a.sh_start + mR - 1) : a.npart;
+    if (a.npcap) cend = min(cend, (int64_t)a.npcap[p]);
+    for (int64_t c = lane; c < cend; c += 32) {
+      int di, dj, dk;
+      unpack_cell(__ldg(a.cell8 + c), di, dj, dk);
+      const int iv1 = pi + di, iv2 = pj + dj, iv3 = pk + dk;
+      if (iv1 < nbuff || iv1 >= n - nbuff || iv2 < nbuff || iv2 >= n - nbuff || iv3 < nbuff || iv3 >= n - nbuff)
+        continue;
+      mask[iv1 + (int64_t)n * iv2 + n2 * iv3] = 1;
+    }
+  }
+}
+
 }  // namespace
+
+void launch_shell_mask(Launch L, const ShellArgs& a, uint8_t* mask, int nbuff, int blocks) {
+  if (a.npk == 0) return;
+  mask_kernel<<<blocks, 128, 0, L.s>>>(a, mask, nbuff);
+  PPB_LAUNCHED(*L.count);
+}
 
 int64_t shell_stage_doubles_per_warp(int nshell) { return (int64_t)ROW * (nshell + 1); }
 

@@ -109,6 +109,7 @@ struct ShellTable {
   // ck_n[c] cells from ck_s[c]; shell m's chunks start at sh_c0[m] (sh_nc[m]).
   std::vector<int32_t> grp_a, grp_b, grp_c, ck_s, ck_n, sh_c0, sh_nc;
   int ngroups = 0;
+  int ch_max = 0;                     // longest chunk (cells)
   // cell offsets packed one per 32-bit word: bytes 0..2 = di, dj, dk as
   // signed 8-bit values (|d| <= nhunt <= 64)
   std::vector<int32_t> cell8;
@@ -178,6 +179,8 @@ struct PeakParams {          // SoA, length npk
 // kernel, read by the collapse kernel).  The first 16 values are what a
 // kernel_strain window reads, the rest what Sbar/Srb read.
 constexpr int ROW = 24;
+// the shell stage's control words (ShellArgs::queue, cqueue, pool_ctr)
+constexpr size_t kCtlBytes = 64;
 enum {
   R_FBAR = 0,   // cumulative mean overdensity Fbar (RadialShell.jl:386-390)
   R_G = 1,      // sum delta * d / r            (3)
@@ -199,7 +202,7 @@ struct PeakHdr {
 };
 
 struct ShellArgs {
-  const float4* aos;        // 2 float4 per cell: (delta, deltaT, psi1x, psi1y), (psi1z, psi2x, psi2y, psi2z)
+  const float4* aos;        // 2 float4 per cell: (delta, deltaT, psi1z, psi2x), (psi1x, psi1y, psi2y, psi2z)
   const float* lapd;        // may be null
   int n;
   double alatt;
@@ -223,6 +226,9 @@ struct ShellArgs {
   int nshell;               // distinct r2 values in the list (incl. 0)
   int mmax;                 // finalised shells: nshell - 1
   int64_t npart;            // cells used (full list here)
+  int ch_max;               // longest chunk of the schedule (cells)
+  int d_max;                // largest |offset component| of the list (nhunt)
+  const unsigned* fmax;     // the field maxima after the records (pack_fmax)
   DevTable tab;
   const double* akk;        // 1101-entry SPH kernel table
   PeakParams pk;
@@ -281,6 +287,15 @@ struct FieldWindow {
   int64_t off, py, pz, cs;
 };
 // packed gather records (two float4 per cell) of an n^3 window
+// The packed records of an n^3 window (two float4 halves per cell) are
+// followed by the largest magnitude of each field (delta, psi x, y, z, psi2
+// x, y, z) as float bits, kFmaxSlots slots per field (the maximum over the
+// slots is the field's): pack_bytes(n) bytes in all.
+constexpr int kFmaxSlots = 64;
+inline int64_t pack_bytes(int64_t n) { return n * n * n * 32 + 7 * kFmaxSlots * 4; }
+inline __host__ __device__ unsigned* pack_fmax(float4* aos, int64_t n) {
+  return reinterpret_cast<unsigned*>(aos + 2 * n * n * n);
+}
 void launch_pack(Launch L, float4* aos, const FieldWindow& w, int n);
 // dst (n^3) = the window of src at off with pitches py, pz
 void launch_extract(Launch L, float* dst, const float* src, int64_t off, int64_t py, int64_t pz, int n);
@@ -333,6 +348,9 @@ int shell_collapse_width(int64_t npk, int nsm, double walk_steps_per_peak);
 void launch_shell_collapse(Launch L, const ShellArgs& a, int nsm, double walk_steps_per_peak, int threads_per_peak);
 void launch_shell_zhalf(Launch L, const ShellArgs& a);
 void launch_shell_d2f(Launch L, const ShellArgs& a, int blocks);
+// mask := 1 over each collapsed peak's cells within RTHL, in the interior
+// (analyse_peak's mask writes)
+void launch_shell_mask(Launch L, const ShellArgs& a, uint8_t* mask, int nbuff, int blocks);
 
 // multi-resolution tile fields (k_multires.cu).  Origins (i0, j0, k0) are
 // 0-based global cells, periodic in N; coarse grids are M^3 with N % M == 0.

@@ -37,6 +37,46 @@ __global__ void ipp_to_lin(const int64_t* ipp, int64_t* lin, const int64_t* ir2,
   ir2o[q] = (int32_t)ir2[q];
 }
 
+// per-peak parameters of one batch of analyse_peaks_gpu_cuda_multirf: the
+// 1-based (i, j, k) to a flat index, the batch's Rf, ir2min and npart, the
+// per-peak ZZon / fcrit or the scalars
+__global__ void multirf_prep_kernel(const int32_t* pi, const int32_t* pj, const int32_t* pk, int64_t q0, int64_t nq,
+                                    int n, double Rf, int ir2, int np, const double* Zpp, const double* fpp, double Z,
+                                    double fc, int64_t* lin, double* oRf, int32_t* oir2, int32_t* onp, double* oZ,
+                                    double* ofc) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nq) return;
+  const int64_t q = q0 + t;
+  const int i = pi[q], j = pj[q], k = pk[q];
+  const bool ok = i >= 1 && i <= n && j >= 1 && j <= n && k >= 1 && k <= n;
+  lin[q] = ok ? (int64_t)(i - 1) + (int64_t)n * (j - 1) + (int64_t)n * n * (k - 1) : -1;   // -1: invalid peak
+  oRf[q] = Rf;
+  oir2[q] = ir2;
+  onp[q] = np;
+  oZ[q] = Zpp ? Zpp[q] : Z;
+  ofc[q] = fpp ? fpp[q] : fc;
+}
+
+// the rmax2rs pre-mask test (RadialShell.jl:310-316) against the mask as it
+// stands before the batch: skip[q] = 1 for a masked peak
+__global__ void premask_kernel(const int64_t* lin, int64_t q0, int64_t nq, const uint8_t* mask, int thr,
+                               int32_t* skip) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nq) return;
+  const int64_t l = lin[q0 + t];
+  skip[t] = (l >= 0 && (int)mask[l] > thr) ? 1 : 0;
+}
+
+// no_collapse() (RadialShell.jl:90-94) for the skipped peaks
+__global__ void skip_out_kernel(const int32_t* skip, int64_t nq, double* out) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nq || !skip[t]) return;
+  double* o = out + t * RES_N;
+  for (int v = 0; v < RES_N; v++) o[v] = 0.0;
+  o[0] = -1.0;
+  o[26] = -1.0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -175,7 +215,7 @@ static int32_t analyse_peaks_impl(ppb_ctx* ctx, const float* delta, const float*
       dpsi2 = st_psi2.as<float>();
     }
     const float* dl = lapd ? (const float*)stage_in(st_lapd, lapd, N * 4, s) : nullptr;
-    aos.ensure(N * 32);
+    aos.ensure(pack_bytes(n));
     launch_pack(L, aos.as<float4>(), FieldWindow{dd, st_psi.as<float>(), dpsi2, 0, n, (int64_t)n * n, N}, n);
     const int64_t* dipp = (const int64_t*)stage_in(d_ipp, ipp, npk * 8, s);
     const double* dRf = (const double*)stage_in(d_Rf, Rf, npk * 8, s);
@@ -232,6 +272,134 @@ int32_t ppb_analyse_peaks_lim(ppb_ctx* ctx, const float* delta, const float* eta
                               const int32_t* r2lim, double alatt, int32_t plain, double* out) {
   return analyse_peaks_impl(ctx, delta, etax, etay, etaz, eta2x, eta2y, eta2z, lapd, n, nhunt, npk, ipp, Rf, ir2min,
                             ZZon, fcrit, r2lim, alatt, plain, out);
+}
+
+int32_t ppb_analyse_peaks_multirf(ppb_ctx* ctx, const float* delta, const float* etax, const float* etay,
+                                  const float* etaz, const float* eta2x, const float* eta2y, const float* eta2z,
+                                  const float* lapd, int32_t n, int32_t nhunt, int32_t nbatch, const int64_t* boff,
+                                  const int32_t* pi, const int32_t* pj, const int32_t* pk, const double* Rf,
+                                  const int64_t* ir2min, const double* ZZon_pp, const double* fcrit_pp, double ZZon,
+                                  double fcrit, double alatt, int8_t* mask, int32_t nbuff, double rmax2rs,
+                                  int32_t plain, double* out) {
+  if (!ctx) return PPB_ERR_INVALID;
+  std::lock_guard<std::recursive_mutex> lk(ctx->mu);
+  try {
+    PPB_REQUIRE(delta && etax && etay && etaz && boff && pi && pj && pk && Rf && ir2min && out, "null argument");
+    PPB_REQUIRE((eta2x == nullptr) == (eta2y == nullptr) && (eta2y == nullptr) == (eta2z == nullptr),
+                "eta2x/eta2y/eta2z must be all given or all null");
+    PPB_REQUIRE(n >= 2 && n <= 4096, "n out of range");
+    PPB_REQUIRE(nbatch >= 0 && nbatch <= 1 << 20, "nbatch out of range");
+    PPB_REQUIRE(alatt > 0, "alatt must be positive");
+    PPB_REQUIRE(nbuff >= 0 && 2 * nbuff < n, "nbuff must satisfy 0 <= nbuff and 2 nbuff < n");
+    PPB_REQUIRE(rmax2rs >= 0.0 && rmax2rs <= 1e6, "rmax2rs must be in [0, 1e6]");
+    PPB_REQUIRE((ZZon_pp == nullptr) == (fcrit_pp == nullptr), "ZZon_pp and fcrit_pp must be both given or both null");
+    PPB_REQUIRE(ctx->sh.has_tab, "collapse table not set (ppb_set_collapse_table)");
+    PPB_REQUIRE(boff[0] == 0, "boff[0] must be 0");
+    for (int b = 0; b < nbatch; b++) {
+      PPB_REQUIRE(boff[b + 1] >= boff[b], "boff must not decrease");
+      PPB_REQUIRE(Rf[b] > 0.0, "Rf must be positive");
+    }
+    const int64_t npk = boff[nbatch];
+    PPB_REQUIRE(npk < (1ll << 31), "too many peaks");
+    PPB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->sync.stream;
+    Launch L{s, &ctx->sync.launches};
+    const int64_t N = (int64_t)n * n * n;
+    std::shared_lock<std::shared_mutex> rl(ctx->sh.mu);
+    ShellTable& shells = ctx->shell_table(nhunt, s);
+    DevBuf st_delta, st_psi, st_psi2, st_lapd, aos, d_pi, d_pj, d_pk, d_Zpp, d_fpp, d_mask, d_out;
+    DevBuf p_lin, p_Rf, p_ir2, p_np, p_Z, p_fc, p_skip;
+    st_psi.ensure(3 * N * 4);
+    auto put = [&](DevBuf& b, size_t off, const float* src) {
+      PPB_CUDA(cudaMemcpyAsync((char*)b.p + off, src, N * 4, cudaMemcpyDefault, s));
+    };
+    const float* dd = (const float*)stage_in(st_delta, delta, N * 4, s);
+    put(st_psi, 0, etax);
+    put(st_psi, N * 4, etay);
+    put(st_psi, 2 * N * 4, etaz);
+    const float* dpsi2 = nullptr;
+    if (eta2x) {
+      st_psi2.ensure(3 * N * 4);
+      put(st_psi2, 0, eta2x);
+      put(st_psi2, N * 4, eta2y);
+      put(st_psi2, 2 * N * 4, eta2z);
+      dpsi2 = st_psi2.as<float>();
+    }
+    const float* dl = lapd ? (const float*)stage_in(st_lapd, lapd, N * 4, s) : nullptr;
+    uint8_t* dm = nullptr;
+    if (mask) {
+      d_mask.ensure(N);
+      PPB_CUDA(cudaMemcpyAsync(d_mask.p, mask, N, cudaMemcpyDefault, s));
+      dm = d_mask.as<uint8_t>();
+    }
+    aos.ensure(pack_bytes(n));
+    launch_pack(L, aos.as<float4>(), FieldWindow{dd, st_psi.as<float>(), dpsi2, 0, n, (int64_t)n * n, N}, n);
+    if (npk > 0) {
+      const int32_t* dpi = (const int32_t*)stage_in(d_pi, pi, npk * 4, s);
+      const int32_t* dpj = (const int32_t*)stage_in(d_pj, pj, npk * 4, s);
+      const int32_t* dpk = (const int32_t*)stage_in(d_pk, pk, npk * 4, s);
+      const double* dZpp = (const double*)stage_in(d_Zpp, ZZon_pp, npk * 8, s);
+      const double* dfpp = (const double*)stage_in(d_fpp, fcrit_pp, npk * 8, s);
+      for (DevBuf* b : {&p_lin, &p_Rf, &p_Z, &p_fc}) b->ensure(npk * 8);
+      for (DevBuf* b : {&p_ir2, &p_np, &p_skip}) b->ensure(npk * 4);
+      double* dout = out;
+      if (!is_device_ptr(out)) {
+        d_out.ensure(npk * RES_N * 8);
+        dout = d_out.as<double>();
+      }
+      const double f3p = 4.0 / 3.0 * 3.141592653589793;
+      for (int b = 0; b < nbatch; b++) {
+        const int64_t q0 = boff[b], nq = boff[b + 1] - boff[b];
+        if (nq == 0) continue;
+        // npart of the batch (RadialShell.jl:288-295); the whole list without rmax2rs
+        int np = (int)shells.ncells;
+        if (rmax2rs > 0.0) {
+          const double x = rmax2rs * Rf[b] / alatt, v = f3p * (x * x * x);
+          np = v >= (double)shells.ncells ? (int)shells.ncells : (int)std::floor(v);
+        }
+        const unsigned g = (unsigned)((nq + 255) / 256);
+        multirf_prep_kernel<<<g, 256, 0, s>>>(dpi, dpj, dpk, q0, nq, n, Rf[b], (int)ir2min[b], np, dZpp, dfpp, ZZon,
+                                              fcrit, p_lin.as<int64_t>(), p_Rf.as<double>(), p_ir2.as<int32_t>(),
+                                              p_np.as<int32_t>(), p_Z.as<double>(), p_fc.as<double>());
+        PPB_LAUNCHED(ctx->sync.launches);
+        const bool premask = rmax2rs > 0.0 && dm;
+        if (premask) {
+          const int thr = (int)std::floor(Rf[b] / alatt * rmax2rs);
+          premask_kernel<<<g, 256, 0, s>>>(p_lin.as<int64_t>(), q0, nq, dm, thr, p_skip.as<int32_t>());
+          PPB_LAUNCHED(ctx->sync.launches);
+        }
+        ShellArgs a = ctx->shell_args(ctx->sync, shells, n, alatt, aos.as<float4>(), dl);
+        a.pk = PeakParams{p_lin.as<int64_t>() + q0, p_Rf.as<double>() + q0, p_ir2.as<int32_t>() + q0,
+                          p_Z.as<double>() + q0, p_fc.as<double>() + q0};
+        a.npk = nq;
+        a.npcap = rmax2rs > 0.0 ? p_np.as<int32_t>() + q0 : nullptr;
+        a.out = dout + q0 * RES_N;
+        ShellStats stt{};
+        ctx->run_shells(ctx->sync, a, plain == 0, plain == 0, &stt);
+        if (stt.guard != 0)
+          throw Error{PPB_ERR_CUDA, "shell truncation guard tripped: a profile read beyond the gathered shells"};
+        if (stt.akk != 0)
+          throw Error{PPB_ERR_INVALID, "kernel_strain SPH table index out of range (the reference raises here too)"};
+        if (stt.raw[8] != 0) throw Error{PPB_ERR_INVALID, "peak index outside the grid"};
+        if (premask) {
+          skip_out_kernel<<<g, 256, 0, s>>>(p_skip.as<int32_t>(), nq, a.out);
+          PPB_LAUNCHED(ctx->sync.launches);
+        }
+        // this batch's halos mask their cells before the next batch reads the mask
+        if (dm) launch_shell_mask(L, a, dm, nbuff, ctx->nsm * 16);
+      }
+      if (dout != out) PPB_CUDA(cudaMemcpyAsync(out, dout, npk * RES_N * 8, cudaMemcpyDefault, s));
+    }
+    if (mask) PPB_CUDA(cudaMemcpyAsync(mask, d_mask.p, N, cudaMemcpyDefault, s));
+    PPB_CUDA(cudaStreamSynchronize(s));
+    return PPB_OK;
+  } catch (const ppb::Error& e) {
+    ctx->set_error(e.msg);
+    return e.code;
+  } catch (...) {
+    ctx->set_error("unknown error");
+    return PPB_ERR_INVALID;
+  }
 }
 
 // Shell-kernel statistics of the last call: cell visits and the five

@@ -852,7 +852,7 @@ void run_tile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const doubl
   setup_run(r, ctx, sl, p, Rf_in, nfilt, box / n);
   TileRes& T = sl.tile_for(n);
   T.setup(n, r.s);
-  T.aos.ensure(N * 32);
+  T.aos.ensure(pack_bytes(n));
   if (T.cap == 0) T.ensure_peaks(initial_peak_capacity(N));
   cudaEvent_t* ev = sl.stage_ev;
   PPB_CUDA(cudaEventRecord(ev[0], r.s));
@@ -997,7 +997,7 @@ void run_multitile_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, const 
     if (p1 > p0) {
       // the tile's chain: its packed records and Laplacian window, then the
       // shell stage, captured together as one graph per sub-batch
-      sl.t_aos.ensure(Nt * 32);
+      sl.t_aos.ensure(pack_bytes(nm));
       if (r.want_lap) sl.t_lapd.ensure(Nt * 4);
       const float* lapd = r.want_lap ? sl.t_lapd.as<float>() : nullptr;
       const int64_t off = wins[t].off;
@@ -1153,7 +1153,7 @@ void run_multitile_split_core(ppb_ctx* ctx, Slot& sl, const ppb_tile_params* p, 
   launch_interleave4(r.L, cf4, cf, fs, Mc);
   TileRes& T = sl.tile_for(nm);
   T.setup(nm, r.s);
-  T.aos.ensure(Nt * 32);
+  T.aos.ensure(pack_bytes(nm));
   if (T.cap == 0) T.ensure_peaks(initial_peak_capacity(Nt));
   const int nf = p->ioutshear >= 1 ? 33 : 11;
   size_t used = 0;

@@ -148,7 +148,7 @@ EXPORTED = (
     "ppb_analyse_peaks_lim", "ppb_set_option", "ppb_get_option", "ppb_tune_entries", "ppb_make_collapse_table",
     "ppb_last_table_stats", "ppb_downsample_noise", "ppb_extended_residual", "ppb_isolated_convolve",
     "ppb_interpolate_to_tile", "ppb_compute_2lpt", "ppb_compute_laplacian", "ppb_coarse_fields",
-    "ppb_run_multitile_split", "ppb_split_coarse_grid", "ppb_peak_find_tile",
+    "ppb_run_multitile_split", "ppb_split_coarse_grid", "ppb_peak_find_tile", "ppb_analyse_peaks_multirf",
 )
 
 
@@ -214,6 +214,8 @@ def load_library():
     L.ppb_run_multitile_split.argtypes = [P, ctypes.POINTER(_TileParams), P, I32, I32, I32, I32, P, I32,
                                           ctypes.POINTER(_HaloBuf)]
     L.ppb_split_coarse_grid.argtypes = [I32, I32, I32, I32, I32]
+    L.ppb_analyse_peaks_multirf.argtypes = [P] * 9 + [I32, I32, I32, P, P, P, P, P, P, P, P, D, D, D, P, I32, D, I32,
+                                                       P]
     L.ppb_peak_find_tile.argtypes = [P, P, I32, P, P, I32, P, D, D, D, D, I32, I32, I32, I64] + [P] * 11 + \
         [ctypes.POINTER(ctypes.c_int64)]
     for f in ("ppb_alloc_host", "ppb_alloc_device"):
@@ -765,6 +767,39 @@ class Context:
                  "y": od[1][:c].copy(), "z": od[2][:c].copy(), "delta": of[0][:c].copy(),
                  "Rsmooth": od[3][:c].copy(), "filter": o32[3][:c].copy()}
         return peaks, peaks["Rsmooth"].copy(), peaks["delta"].copy(), of[1][:c].copy(), m
+
+    def analyse_peaks_multirf(self, fields: dict, batches, nhunt: int, alatt: float, ZZon: float = 1.0,
+                              fcrit: float = 1.686, mask: np.ndarray = None, nbuff: int = 0, rmax2rs: float = 0.0,
+                              plain: bool = False):
+        """analyse_peaks_gpu_cuda_multirf (src/PeakPatch.jl:231-253): batches
+        of (pi, pj, pk, Rf, ir2min[, ZZon_pp, fcrit_pp]) tuples, 1-based
+        indices, one filter scale per batch.  mask (int8, the fields' shape)
+        is read and updated in place.  Returns (list of (npk_b, 31) result
+        arrays, mask)."""
+        d = fields["delta"]
+        n = d.shape[0]
+        if d.shape != (n, n, n):
+            raise ValueError("analyse_peaks_multirf needs a cubic grid")
+        if mask is not None and (mask.dtype != np.int8 or not mask.flags.c_contiguous or mask.shape != d.shape):
+            raise ValueError("mask must be a C-contiguous int8 array of the fields' shape")
+        g = lambda key: None if fields.get(key) is None else np.ascontiguousarray(fields[key], np.float32)
+        f = {k: g(k) for k in ("delta", "etax", "etay", "etaz", "eta2x", "eta2y", "eta2z", "lapd")}
+        pp_ = len(batches) > 0 and len(batches[0]) >= 7
+        cat = lambda i, t: np.ascontiguousarray(np.concatenate([np.asarray(b[i], t) for b in batches])
+                                                if batches else np.zeros(0, t))
+        boff = np.zeros(len(batches) + 1, np.int64)
+        boff[1:] = np.cumsum([len(b[0]) for b in batches])
+        pi, pj, pk = cat(0, np.int32), cat(1, np.int32), cat(2, np.int32)
+        Rf = np.ascontiguousarray([float(b[3]) for b in batches], np.float64)
+        ir2 = np.ascontiguousarray([int(b[4]) for b in batches], np.int64)
+        Zpp = cat(5, np.float64) if pp_ else None
+        fpp = cat(6, np.float64) if pp_ else None
+        out = np.empty((max(int(boff[-1]), 1), 31), np.float64)
+        self._check(self.L.ppb_analyse_peaks_multirf(
+            self.h, _p(f["delta"]), _p(f["etax"]), _p(f["etay"]), _p(f["etaz"]), _p(f["eta2x"]), _p(f["eta2y"]),
+            _p(f["eta2z"]), _p(f["lapd"]), n, nhunt, len(batches), _p(boff), _p(pi), _p(pj), _p(pk), _p(Rf),
+            _p(ir2), _p(Zpp), _p(fpp), ZZon, fcrit, alatt, _p(mask), nbuff, rmax2rs, 1 if plain else 0, _p(out)))
+        return [out[boff[b]:boff[b + 1]].copy() for b in range(len(batches))], mask
 
     def analyse_peaks(self, fields: dict, ipp, Rf, ir2min, ZZon, fcrit, alatt: float, nhunt: int,
                       plain: bool = False, r2lim=None) -> np.ndarray:
