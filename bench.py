@@ -152,64 +152,129 @@ class ClockSampler:
 # CPU baseline: the oracle (a C++/OpenMP restatement of the reference's CPU
 # run_tile) on a bounded sample of the same workload
 # ---------------------------------------------------------------------------
+def config_dict(n: int, path: str = "optimised") -> dict:
+    """The workload's config, the same in both arms."""
+    return {"workload": workload_name(n), "nmesh": n, "boxsize": BOX_PER_CELL * n, "filters": 20, "nbuff": 32,
+            "ilpt": 2, "ioutshear": 1, "seed": SEED, "path": path,
+            "l2": "inputs larger than L2 (each field 226 MB at 384^3)"}
+
+
+class CpuTile:
+    """The oracle's run_tile on one tile: fields and the 20-filter peak search
+    at full size once, then the shell analysis timed on random samples of the
+    tile's peaks and extrapolated to all of them.  Two shell figures: the
+    reference's own loop (every peak gathers its whole shell list), and the
+    same loop stopping once the shells the later phases read are in (the
+    truncation the GPU path uses; the same results)."""
+
+    def __init__(self, n: int):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        from peakpatch_b200 import powerspec
+        oracle.build()
+        self.ora = oracle
+        self.cores = os.cpu_count() or 1
+        oracle.set_threads(self.cores)
+        k, P = powerspec.eh_table()
+        self.T = oracle.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat"))
+        cfg = tile_config(n)
+        ocfg = oracle.Config(**{f: getattr(cfg, f) for f in oracle.Config.__dataclass_fields__})
+        filters = [(i + 1, 1.686, R) for i, R in enumerate(FILTERS)]
+        self.tm = {}
+        self.st = oracle.run_tile_stages(ocfg, SEED, k, P, filters, self.T, peak_sample=np.arange(0), timings=self.tm)
+        self.npk = len(self.st["peaks"]["ipp"])
+        self.n = n
+        self.rng = np.random.default_rng(0)
+        self.pp = {False: [], True: []}    # per-peak seconds of each timed sub-batch, by truncation
+        self.peaks = {False: 0, True: 0}
+        self.secs = {False: 0.0, True: 0.0}
+        self.est = {False: None, True: None}
+
+    def _run(self, size: int, truncate: bool) -> float:
+        st = self.st
+        sub = np.sort(self.rng.choice(self.npk, size=min(self.npk, max(1, size)), replace=False))
+        t0 = time.perf_counter()
+        self.ora.analyse_peaks(st["fields"], st["peaks"]["ipp"][sub], st["Rf"][sub], st["ir2min"][sub],
+                               st["ZZon"][sub], st["fcrit"], st["alatt"], st["shells"], self.T, nbuff=32,
+                               truncate=truncate)
+        return time.perf_counter() - t0, len(sub)
+
+    def sample(self, budget_s: float, truncate: bool, parts: int = 4):
+        """Times `parts` random sub-batches of about budget_s seconds in all."""
+        if self.npk == 0:
+            return
+        if self.est[truncate] is None:   # per-peak cost from a small probe (not counted)
+            dt, k = self._run(max(64, 8 * self.cores), truncate)
+            self.est[truncate] = dt / k
+        size = int(budget_s / parts / max(self.est[truncate], 1e-7))
+        for _ in range(parts):
+            dt, k = self._run(size, truncate)
+            self.pp[truncate].append(dt / k)
+            self.peaks[truncate] += k
+            self.secs[truncate] += dt
+
+    def figure(self, truncate: bool) -> dict:
+        v = self.pp[truncate]
+        mean = statistics.fmean(v)
+        se = statistics.stdev(v) / np.sqrt(len(v)) / mean if len(v) > 1 else None
+        shells_s = mean * self.npk
+        tile_s = self.tm["fields_s"] + self.tm["peaks_s"] + shells_s
+        return {"tiles_per_s": 1.0 / tile_s, "tile_s": tile_s, "shells_s_extrapolated": shells_s,
+                "sampled_peaks": self.peaks[truncate], "sampled_s": self.secs[truncate],
+                "rel_std_error": se}
+
+    def baseline(self) -> dict:
+        full, trunc = self.figure(False), self.figure(True)
+        return {"value": full["tiles_per_s"], "unit": METRIC, "cores": self.cores, "kind": "port",
+                "sample": (f"{workload_name(self.n)}: the oracle (C++/OpenMP + threaded pocketfft) runs the fields "
+                           f"and the 20-filter peak search at full size ({self.tm['fields_s'] + self.tm['peaks_s']:.1f}"
+                           f" s), then analyse_peak on {full['sampled_peaks']} random peaks of {self.npk} "
+                           f"({full['sampled_s']:.1f} s, whole shell lists as the reference), extrapolated to all "
+                           f"peaks (relative standard error {full['rel_std_error'] or 0:.3f})"),
+                "stages_s": {"fields": self.tm["fields_s"], "peaks": self.tm["peaks_s"],
+                             "shells_extrapolated": full["shells_s_extrapolated"]},
+                "npeaks": self.npk,
+                "truncated_shells": {**trunc, "note": "the same oracle loop stopping each peak's gather once the "
+                                                      "shells its later phases read are in (the GPU's truncation; "
+                                                      "identical results): separates the algorithmic gain from "
+                                                      "the kernels'"}}
+
+
 def cpu_baseline(n: int, budget_s: float = 20.0):
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    from peakpatch_b200 import powerspec
-    oracle.build()
-    cores = os.cpu_count() or 1
-    oracle.set_threads(cores)
-    k, P = powerspec.eh_table()
-    T = oracle.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat"))
-    cfg = tile_config(n)
-    ocfg = oracle.Config(**{f: getattr(cfg, f) for f in oracle.Config.__dataclass_fields__})
-    filters = [(i + 1, 1.686, R) for i, R in enumerate(FILTERS)]
-    # sample: fields + filter bank + peaks at full size, the shell analysis on
-    # a random subset of the peaks sized to the time budget, extrapolated
-    tm = {}
-    probe = oracle.run_tile_stages(ocfg, SEED, k, P, filters, T, peak_sample=np.arange(0), timings=tm)
-    npk = len(probe["peaks"]["ipp"])
-    rng = np.random.default_rng(0)
-    sub = np.sort(rng.choice(npk, size=min(npk, 200), replace=False)) if npk else np.arange(0)
-    t0 = time.perf_counter()
-    if len(sub):
-        oracle.analyse_peaks(probe["fields"], probe["peaks"]["ipp"][sub], probe["Rf"][sub], probe["ir2min"][sub],
-                             probe["ZZon"][sub], probe["fcrit"], probe["alatt"], probe["shells"], T, nbuff=32)
-    per_peak = (time.perf_counter() - t0) / max(1, len(sub))
-    want = int(min(npk, max(len(sub), budget_s / max(per_peak, 1e-9))))
-    sub2 = np.sort(rng.choice(npk, size=want, replace=False)) if npk else np.arange(0)
-    t0 = time.perf_counter()
-    if len(sub2):
-        oracle.analyse_peaks(probe["fields"], probe["peaks"]["ipp"][sub2], probe["Rf"][sub2], probe["ir2min"][sub2],
-                             probe["ZZon"][sub2], probe["fcrit"], probe["alatt"], probe["shells"], T, nbuff=32)
-    shells_s = (time.perf_counter() - t0) * npk / max(1, len(sub2))
-    tile_s = tm["fields_s"] + tm["peaks_s"] + shells_s
-    return {"value": 1.0 / tile_s, "unit": METRIC, "cores": cores, "kind": "port",
-            "sample": (f"{workload_name(n)}: fields + 20-filter peak finding at full size "
-                       f"({tm['fields_s'] + tm['peaks_s']:.1f} s), shell analysis on {len(sub2)} of {npk} peaks "
-                       f"extrapolated ({shells_s:.1f} s); oracle C++/OpenMP + threaded pocketfft"),
-            "stages_s": {"fields": tm["fields_s"], "peaks": tm["peaks_s"], "shells_extrapolated": shells_s},
-            "npeaks": npk}
+    c = CpuTile(n)
+    c.sample(0.75 * budget_s, False)
+    c.sample(0.25 * budget_s, True)
+    return c.baseline()
 
 
 def run_reference(args, dist: Dist):
+    """The reference arm: the oracle's CPU run_tile on the host cores, each
+    step a bounded sample of the tile (fields and peaks are timed once at
+    full size; every step times the shell analysis of fresh random peaks)."""
     if dist.rank != 0:
         return
     n = args.n
-    vals = []
+    c = CpuTile(n)
+    per_step = max(1.0, min(6.0, args.cpu_budget / 4))
     for _ in range(args.warmup):
-        pass   # the oracle has no warm-up state beyond its first build
-    res = None
+        c.sample(0.5, False, parts=1)
+    vals = []
     for _ in range(args.steps):
-        res = cpu_baseline(n, budget_s=args.cpu_budget)
-        vals.append(res["value"])
-    v = statistics.median(vals)
+        k0 = len(c.pp[False])
+        c.sample(0.75 * per_step, False, parts=2)
+        c.sample(0.25 * per_step, True, parts=1)
+        step_pp = statistics.fmean(c.pp[False][k0:])
+        vals.append(1.0 / (c.tm["fields_s"] + c.tm["peaks_s"] + step_pp * c.npk))
+    base = c.baseline()
+    v = base["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 shell sums", "data": "synthetic",
-            "config": {"workload": workload_name(n), "nmesh": n, "filters": 20, "seed": SEED},
-            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": config_dict(n),
+            "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "step_values": vals, "stages_s": base["stages_s"], "truncated_shells": base["truncated_shells"],
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "ms_per_step is the extrapolated time of one whole tile; each timed step runs a sample of it"}
     print(json.dumps(line), flush=True)
 
 
@@ -295,9 +360,8 @@ def run_ours(args, dist: Dist):
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, compensated-f32 shell sums, f64 collapse walk",
             "data": "synthetic (seeded Threefry noise, EH P(k))",
-            "config": {"workload": workload_name(n), "nmesh": n, "boxsize": BOX_PER_CELL * n, "filters": 20,
-                       "nbuff": 32, "ilpt": 2, "ioutshear": 1, "seed": SEED, "path": "plain" if args.plain else "optimised",
-                       "l2": "inputs larger than L2 (each field 226 MB at 384^3)", "parallelism": f"replicas x{dist.world}"},
+            "config": {**config_dict(n, "plain" if args.plain else "optimised"),
+                       "parallelism": f"replicas x{dist.world}"},
             "peaks_per_s": npk_tot / (dev_ms / 1000.0), "halos_per_tile": nh_tot / args.steps,
             "peaks_per_tile": npk_tot / args.steps,
             "stage_ms_last_step": stage,
@@ -789,6 +853,25 @@ def run_table_bench(args, dist: Dist):
     return line
 
 
+def _default_extras(args, dist: Dist) -> dict:
+    """The batched shell kernel of 10^6 peaks on a 512^3 field and a shortened
+    serving stream (60 Poisson requests at 4/s), run after the tile benchmark
+    in the default invocation so that one line carries their numbers."""
+    out = {}
+    a = argparse.Namespace(**vars(args))
+    sh = run_shells_bench(a, dist)
+    out["shells_batched"] = {k: sh[k] for k in ("metric", "value", "unit", "config", "roofline",
+                                                "optimised_over_plain")}
+    out["shells_batched"]["kernel_ms"] = sh["optimised"]["kernel_ms"]
+    out["shells_batched"]["visits"] = sh["optimised"]["visits"]
+    out["shells_batched"]["plain_peaks_per_s"] = sh["plain"]["peaks_per_s"]
+    a.requests, a.rate = 60, 4.0
+    sv = run_serve(a, dist)
+    out["serving_stream"] = {k: sv[k] for k in ("metric", "value", "unit", "config", "p50_ms", "p99_ms", "failed",
+                                                "wall_s", "peaks_per_s")}
+    return out
+
+
 def _apply_options(ctx, args):
     import peakpatch_b200 as pp
     ctx.set_option(pp.OPT_GRAPHS, 0 if getattr(args, "no_graphs", False) else 1)
@@ -860,10 +943,13 @@ def main():
                 print(json.dumps(line), flush=True)
             return
         line = run_ours(args, dist)
+        if dist.rank == 0 and line is not None and dist.world == 1 and not args.no_extras and not args.plain:
+            line.update(_default_extras(args, dist))
         if dist.rank == 0 and line is not None:
             if dist.world == 1 and not args.no_cpu_baseline:
                 cb = cpu_baseline(args.n, budget_s=args.cpu_budget)
-                line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+                line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                           "stages_s", "truncated_shells")}
             print(json.dumps(line), flush=True)
     finally:
         dist.close()

@@ -165,6 +165,19 @@ int32_t ppb_merge_catalog(ppb_ctx* ctx, const float* records, int64_t n, int32_t
 int32_t ppb_generate_fields(ppb_ctx* ctx, const ppb_tile_params* p, float* delta, float* psi, float* psi2,
                             float* lapd);
 
+/* write_catalog_hdf5(path, halos, cosmo; z_max) (ext/HDF5Ext.jl:47-104;
+ * stub src/PeakPatch.jl:67): the catalogue of n records (11 or 33 floats,
+ * host or device) as one-dimensional Float32 datasets in the root group of
+ * an HDF5 file: x, y, z, ra, dec, redshift, chi, M200m, RTHL, vx, vy, vz
+ * (+ vx2, vy2, vz2, overdensity, e_v, p_v, Rf, zform for 33-field records),
+ * with chi = |x| (Mpc/h), redshift from the chi -> z table up to z_max,
+ * M200m = 4/3 pi 2.775e11 Om h^2 RTHL^3 (Om the total matter density),
+ * (ra, dec) in radians.  Written without libhdf5 in the format's original
+ * layout (superblock 0, one symbol table, contiguous storage); n = 0 writes
+ * an empty file with an empty root group. */
+int32_t ppb_write_catalog_hdf5(const char* path, const float* records, int64_t n, int32_t nfields, double Om,
+                               double OL, double h, double z_max);
+
 /* write_pksc (src/IO/Catalog.jl:53-94): Int32 N, Float32 RTHLmax, Float32 z_out,
  * then N x nfields Float32 (little endian). */
 int32_t ppb_write_pksc(const char* path, const float* records, int64_t n, int32_t nfields,

@@ -850,6 +850,12 @@ struct PeakCtx {
   const int32_t* shells; int64_t nshells;
   const double* akk;
   OraTable T;
+  int64_t ndistinct;   // distinct r^2 values of the list: profile arrays need ndistinct + 3 entries
+  // truncated gather (CPU timing leg only, not the reference's algorithm):
+  // stop reading cells once every shell the later phases read is in
+  int truncate;
+  const double* srad;  // srad[m], m = 1..ndistinct: shell radii (shell 1 = the centre)
+  const int* need;     // need[m]: shells to gather when shell m is the outermost one read
 };
 
 static void no_collapse(double* r) {
@@ -928,7 +934,8 @@ static void analyse_peak(const PeakCtx& P, int64_t ipp, double alatt, int64_t ir
       g_dump[0]++; no_collapse(out); return;
     }
   }
-  const int64_t maxm = npart + 3;
+  // profile index m counts distinct r^2 (the reference sizes them npart + 2)
+  const int64_t maxm = std::min<int64_t>(npart, P.ndistinct) + 3;
   std::vector<double> rad(maxm, 0.0), Fbar(maxm, 0.0);
   std::vector<int64_t> nshell(maxm, 0);
   std::vector<double> S[3], S2[3], G[3], Gf[3], SR[3][3];
@@ -952,9 +959,31 @@ static void analyse_peak(const PeakCtx& P, int64_t ipp, double alatt, int64_t ir
   double rupp_init = std::sqrt((double)ir2min) + 2.0 * hlatt;
   int ifcrit = 1;
   int64_t mupp = 1;
+  // truncated gather: the shells any later phase reads end at need[M], M the
+  // outermost of the first shell beyond ir2min, the Rf window and (outward)
+  // the fcrit crossing; an inward crossing is seen at that first shell
+  int64_t mlast = 0, tM = 0, tstate = 0, mtarget = -1;
+  if (P.truncate) {
+    for (int64_t jp = 2; jp <= npart; jp++)
+      if (sh[4 * (jp - 1) + 3] != sh[4 * (jp - 2) + 3]) mlast++;
+    mlast = std::max<int64_t>(mlast, 1);   // shells finalised inside the loop (the centre is shell 1)
+    // Rf window of phase 3 (depends on the radii only)
+    double rm = 10.0;
+    int64_t mr = 1, mri = 1, i2p = npart >= 2 ? sh[7] : 0;
+    const double rq0 = (Rfclvi / alatt) * (Rfclvi / alatt);
+    for (int64_t jp = 2; jp <= npart; jp++) {
+      const int64_t i2 = sh[4 * (jp - 1) + 3];
+      if (std::fabs((double)i2 - rq0) < rm) { mr = mri; rm = std::min(rm, std::fabs((double)i2 - rq0)); }
+      if (i2 != i2p) { mri++; i2p = i2; }
+    }
+    int64_t mur = mr;
+    for (int64_t m1 = mr + 1; m1 <= mlast; m1++) if (P.srad[m1] < P.srad[mr] + 2.0) mur = m1;
+    tM = std::max(mr, mur);
+  }
   for (int64_t jp = 2; jp <= npart; jp++) {
     const int32_t* c = sh + 4 * (jp - 1);
     const int64_t ir2 = c[3];
+    if (P.truncate && mtarget >= 0 && m >= mtarget) break;
     if (ir2 != ir2p) {
       m += 1;
       rad[m] = std::sqrt((double)ir2p);
@@ -969,6 +998,12 @@ static void analyse_peak(const PeakCtx& P, int64_t ipp, double alatt, int64_t ir
         if (ir2p > ir2min) { rupp_init = rad[m0] + 2.0 * hlatt; ifcrit = 0; mupp = m; }
       } else {
         if (rad[m] < rupp_init) mupp = m;
+      }
+      if (P.truncate && mtarget < 0) {
+        // the crossing state in shell order, as the GPU gather decides it
+        if (tstate == 0 && ifcrit == 0 && m == m0) tstate = Fbar[m] < fcrit ? 1 : 0;
+        else if (tstate == 0 && ifcrit == 0 && m > m0 && Fbar[m] < fcrit) { tstate = 2; tM = std::max(tM, m); }
+        if (tstate != 0) mtarget = std::min<int64_t>(P.need[std::max(tM, m0)], mlast);
       }
       ir2p = ir2;
       Fshell = 0.0; nsh = 0;
@@ -1000,6 +1035,12 @@ static void analyse_peak(const PeakCtx& P, int64_t ipp, double alatt, int64_t ir
     }
   }
 
+  if (P.truncate && m < mlast) {
+    // shells beyond the gathered ones are never read below; their radii are
+    // the list's (the loops over rad[] run to the last shell as in the full sum)
+    for (int64_t mm = m + 1; mm <= mlast; mm++) rad[mm] = P.srad[mm];
+    m = mlast;
+  }
   // Phase 3: gradient at Rf
   double rmrf = 10.0;
   int64_t mrf = 1, mrfi = 1;
@@ -1268,11 +1309,27 @@ void ora_analyse_peaks(const float* delta, const float* ex, const float* ey, con
                        double y2, double z1, double z2,
                        int64_t npk, const int64_t* ipp, const double* Rf, const int64_t* ir2min,
                        const double* ZZon, const double* fcrit, double alatt, int64_t nbuff,
-                       double rmax2rs, int serial_mask, double* out) {
+                       double rmax2rs, int serial_mask, int truncate, double* out) {
   std::vector<double> akk(1101);
   ora_atab4(akk.data());
+  // distinct r^2 values, their radii (shell m = value m - 1) and, for the
+  // truncated gather, need[m] = min(mmax, l + 2) with l the outermost shell
+  // within rad[m] + 2 (mmax: the shells finalised over the whole list)
+  std::vector<double> srad(1, 0.0);
+  for (int64_t jp = 1; jp <= nshells; jp++)
+    if (jp == 1 || shells[4 * (jp - 1) + 3] != shells[4 * (jp - 2) + 3])
+      srad.push_back(std::sqrt((double)shells[4 * (jp - 1) + 3]));
+  const int64_t nd = (int64_t)srad.size() - 1;
+  const int64_t mmax = std::max<int64_t>(nd - 1, 1);
+  std::vector<int> need(nd + 2, (int)mmax);
+  for (int64_t mm = 1; mm <= mmax; mm++) {
+    int64_t l = mm;
+    while (l + 1 <= mmax && srad[l + 1] <= srad[mm] + 2.0) l++;
+    need[mm] = (int)std::min<int64_t>(mmax, l + 2);
+  }
+  srad.push_back(0.0);
   PeakCtx P{delta, ex, ey, ez, e2x, e2y, e2z, lapd, mask, n1, n2, n3, shells, nshells, akk.data(),
-            OraTable{tab, nx, ny, nz, x1, x2, y1, y2, z1, z2}};
+            OraTable{tab, nx, ny, nz, x1, x2, y1, y2, z1, z2}, nd, truncate, srad.data(), need.data()};
   if (serial_mask) {
     for (int64_t p = 0; p < npk; p++)
       analyse_peak(P, ipp[p], alatt, ir2min[p], ZZon[p], Rf[p], nbuff, rmax2rs, fcrit[p], out + R_N * p);

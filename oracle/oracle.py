@@ -102,7 +102,7 @@ def _declare(L):
     L.ora_chi2z.argtypes = [D, D, D, D, P, ctypes.c_int, P]
     L.ora_analyse_peaks.argtypes = [P] * 9 + [I64, I64, I64, P, I64, P, ctypes.c_int, ctypes.c_int,
                                               ctypes.c_int, D, D, D, D, D, D, I64, P, P, P, P, P, D,
-                                              I64, D, ctypes.c_int, P]
+                                              I64, D, ctypes.c_int, ctypes.c_int, P]
     L.ora_dump_counts.argtypes = [P]
     L.ora_pack_records.argtypes = [D, D, D, D, I64, P, P, P, P, P, P, P, D, ctypes.c_int, D, D, D, D,
                                    D, ctypes.c_int, ctypes.c_int, P, P]
@@ -384,9 +384,11 @@ def chi_to_z(Om, OL, h, zmax, chis) -> np.ndarray:
 
 
 def analyse_peaks(fields, ipp, Rf, ir2min, ZZon, fcrit, alatt, shells, T: Table, nbuff=0,
-                  rmax2rs=0.0, mask=None, serial_mask=False) -> np.ndarray:
+                  rmax2rs=0.0, mask=None, serial_mask=False, truncate=False) -> np.ndarray:
     """RadialShell.jl:282-891 for a batch of peaks.  fields: dict with delta,
     etax, etay, etaz and optional eta2x/eta2y/eta2z/lapd (C-order float32).
+    truncate: stop each peak's gather once the shells the later phases read
+    are in (the same results; a CPU timing leg, not the reference's loop).
     Returns (npk, 31) float64 results."""
     d = fields["delta"]
     n3, n2, n1 = d.shape
@@ -401,7 +403,7 @@ def analyse_peaks(fields, ipp, Rf, ir2min, ZZon, fcrit, alatt, shells, T: Table,
                             _p(g("eta2y")), _p(g("eta2z")), _p(g("lapd")), _p(mask), n1, n2, n3,
                             _p(sh), sh.shape[0], _p(T.data), T.nx, T.ny, T.nz, T.x1, T.x2, T.y1, T.y2,
                             T.z1, T.z2, npk, _p(ipp_a), _p(Rf_a), _p(ir_a), _p(Z_a), _p(fc_a), alatt,
-                            nbuff, rmax2rs, int(bool(serial_mask)), _p(out))
+                            nbuff, rmax2rs, int(bool(serial_mask)), int(bool(truncate)), _p(out))
     return out
 
 

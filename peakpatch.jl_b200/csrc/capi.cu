@@ -889,6 +889,23 @@ int32_t ppb_write_pksc(const char* path, const float* records, int64_t n, int32_
   return ok ? PPB_OK : PPB_ERR_INVALID;
 }
 
+int32_t ppb_write_catalog_hdf5(const char* path, const float* records, int64_t n, int32_t nfields, double Om,
+                               double OL, double h, double z_max) {
+  PPB_GUARD_BEGIN
+  PPB_REQUIRE(path && n >= 0 && (n == 0 || records) && (nfields == 11 || nfields == 33), "bad arguments");
+  PPB_REQUIRE(Om > 0.0 && h > 0.0 && z_max > 0.0, "Om, h and z_max must be positive");
+  std::vector<float> host;
+  const float* rec = records;
+  if (n > 0 && is_device_ptr(records)) {
+    host.resize((size_t)n * nfields);
+    PPB_CUDA(cudaMemcpy(host.data(), records, host.size() * 4, cudaMemcpyDeviceToHost));
+    rec = host.data();
+  }
+  write_catalog_hdf5_host(path, rec, n, nfields, Om, OL, h, z_max);
+  return PPB_OK;
+  PPB_GUARD_END((ppb_ctx*)nullptr)
+}
+
 int32_t ppb_noise_threefry(ppb_ctx* ctx, float* out, int32_t n, uint64_t seed) {
   if (!ctx) return PPB_ERR_INVALID;
   std::lock_guard<std::recursive_mutex> lk(ctx->mu);

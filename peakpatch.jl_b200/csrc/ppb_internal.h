@@ -137,6 +137,9 @@ GrowthTable make_growth_table(double Om, double OB, double OL, double h);
 void dlinear_ab(const GrowthTable& G, double ai, double* Dl, double* HD, double* Da);
 double fsc_of_z(const GrowthTable& G, double z);
 std::vector<double> make_chi_table(double Om, double OL, double h, double zmax, int npts);
+// write_catalog_hdf5 of n host records (11 or 33 floats each) to path
+void write_catalog_hdf5_host(const std::string& path, const float* rec, int64_t n, int nf, double Om, double OL,
+                             double h, double z_max);
 // comoving distance to z (Mpc/h) and its inverse on a make_chi_table table
 // spanning [0, zmax] (chi_to_z, Cosmology.jl:155-169)
 double chi_of_z(double Om, double OL, double h, double z);

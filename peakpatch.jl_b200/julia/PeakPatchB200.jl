@@ -323,6 +323,25 @@ function analyse_peaks_gpu_cuda_multirf(delta, etax, etay, etaz, eta2x, eta2y, e
     return (results=results, mask=m === C_NULL ? nothing : m)
 end
 
+"""
+    write_catalog_hdf5(path, halos, cosmo; z_max=10.0)
+
+Method for the HDF5 plug-in stub (src/PeakPatch.jl:67; ext/HDF5Ext.jl:47-104)
+without libhdf5: the columns x, y, z, ra, dec, redshift, chi, M200m, RTHL,
+vx, vy, vz (+ vx2, vy2, vz2, overdensity, e_v, p_v, Rf, zform for
+ExtHaloRecord) as Float32 datasets; cosmo supplies Om (total matter), OL, h.
+"""
+function write_catalog_hdf5(path::AbstractString, halos::AbstractVector, cosmo; z_max::Float64=10.0)
+    PP = Base.root_module(Base.__toplevel__, :PeakPatch)
+    nf = eltype(halos) <: PP.ExtHaloRecord ? 33 : 11
+    rec = isempty(halos) ? Float32[] : collect(reinterpret(Float32, collect(halos)))
+    rc = ccall((:ppb_write_catalog_hdf5, libppb), Int32,
+               (Cstring, Ptr{Float32}, Int64, Int32, Float64, Float64, Float64, Float64),
+               path, rec, length(halos), nf, cosmo.Om, cosmo.OL, cosmo.h, z_max)
+    rc == PPB_OK || error("ppb_write_catalog_hdf5 failed ($rc) for $path")
+    return nothing
+end
+
 # ---- multi-resolution split (src/MultiResolution.jl) ---------------------
 # Methods for the reference's GPU plug-in stubs of run_multitile_split
 # (src/PeakPatch.jl:255-339) and the driver itself.  `pk` is a P(k) file path

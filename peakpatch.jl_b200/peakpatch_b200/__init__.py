@@ -148,7 +148,7 @@ EXPORTED = (
     "ppb_analyse_peaks_lim", "ppb_set_option", "ppb_get_option", "ppb_tune_entries", "ppb_make_collapse_table",
     "ppb_last_table_stats", "ppb_downsample_noise", "ppb_extended_residual", "ppb_isolated_convolve",
     "ppb_interpolate_to_tile", "ppb_compute_2lpt", "ppb_compute_laplacian", "ppb_coarse_fields",
-    "ppb_run_multitile_split", "ppb_split_coarse_grid", "ppb_peak_find_tile", "ppb_analyse_peaks_multirf",
+    "ppb_run_multitile_split", "ppb_split_coarse_grid", "ppb_peak_find_tile", "ppb_analyse_peaks_multirf", "ppb_write_catalog_hdf5",
 )
 
 
@@ -214,6 +214,7 @@ def load_library():
     L.ppb_run_multitile_split.argtypes = [P, ctypes.POINTER(_TileParams), P, I32, I32, I32, I32, P, I32,
                                           ctypes.POINTER(_HaloBuf)]
     L.ppb_split_coarse_grid.argtypes = [I32, I32, I32, I32, I32]
+    L.ppb_write_catalog_hdf5.argtypes = [ctypes.c_char_p, P, I64, I32, D, D, D, D]
     L.ppb_analyse_peaks_multirf.argtypes = [P] * 9 + [I32, I32, I32, P, P, P, P, P, P, P, P, D, D, D, P, I32, D, I32,
                                                        P]
     L.ppb_peak_find_tile.argtypes = [P, P, I32, P, P, I32, P, D, D, D, D, I32, I32, I32, I64] + [P] * 11 + \

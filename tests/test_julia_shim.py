@@ -79,6 +79,7 @@ def _c_prototypes():
 # C parameter type -> Julia ccall argument types that pass it correctly
 _SCALAR = {"int32_t": "Int32", "int64_t": "Int64", "uint64_t": "UInt64", "double": "Float64", "float": "Float32",
            "size_t": "Csize_t", "int8_t": "Int8", "char": "UInt8"}
+_STRING = {"Cstring", "Ptr{UInt8}"}
 
 
 def _compatible(cparam, jtype):
@@ -86,6 +87,8 @@ def _compatible(cparam, jtype):
     if "*" in ctype:
         inner = ctype.split("*")[0].strip()
         if jtype == "Ptr{Cvoid}":
+            return True
+        if inner == "char" and jtype in _STRING:
             return True
         if inner in _SCALAR:
             return jtype in (f"Ptr{{{_SCALAR[inner]}}}", f"Ref{{{_SCALAR[inner]}}}")

@@ -471,3 +471,22 @@ def test_rmax2rs_result_does_not_depend_on_peak_order(ora, eh_pk, julia_table):
         assert np.array_equal(mask, runs[0][1])
     assert np.all(runs[0][0][skippable, 0] == -1.0)
     assert (runs[0][0][:, 0] > 0).sum() > 50
+
+
+def test_truncated_gather_leg_gives_the_full_results(ora, eh_pk, julia_table):
+    """The oracle's truncated gather (each peak stops reading cells once the
+    shells its later phases read are in: the first shell beyond ir2min, the
+    Rf window and an outward fcrit crossing, plus two cells of radius) gives
+    the full-sphere results bit for bit.  The same rule truncates the GPU
+    gather; the CPU leg times the reference's algorithm with it."""
+    from conftest import filter_bank
+    for rmax2rs in (0.0, 1.0):
+        cfg = ora.Config(Omx=0.315 - 0.049, OmB=0.049, Omvac=0.685, h=0.674, n=64, boxsize=128.0, nbuff=16,
+                         ilpt=2, ioutshear=1, wsmooth=1, rmax2rs=rmax2rs)
+        st = ora.run_tile_stages(cfg, 3, *eh_pk, filter_bank(), julia_table, peak_sample=np.arange(0))
+        args = (st["fields"], st["peaks"]["ipp"], st["Rf"], st["ir2min"], st["ZZon"], st["fcrit"], st["alatt"],
+                st["shells"], julia_table)
+        full = ora.analyse_peaks(*args, nbuff=16, rmax2rs=rmax2rs)
+        trunc = ora.analyse_peaks(*args, nbuff=16, rmax2rs=rmax2rs, truncate=True)
+        assert (full[:, 0] > 0).sum() > 100
+        assert np.array_equal(full.view(np.uint64), trunc.view(np.uint64)), rmax2rs
