@@ -213,6 +213,11 @@ class CpuTile:
             self.peaks[truncate] += k
             self.secs[truncate] += dt
 
+    def reset_samples(self):
+        self.pp = {False: [], True: []}
+        self.peaks = {False: 0, True: 0}
+        self.secs = {False: 0.0, True: 0.0}
+
     def figure(self, truncate: bool) -> dict:
         v = self.pp[truncate]
         mean = statistics.fmean(v)
@@ -258,23 +263,30 @@ def run_reference(args, dist: Dist):
     per_step = max(1.0, min(6.0, args.cpu_budget / 4))
     for _ in range(args.warmup):
         c.sample(0.5, False, parts=1)
-    vals = []
+        c.sample(0.2, True, parts=1)
+    c.reset_samples()   # warm-up samples do not count
+    vals, walls = [], []
     for _ in range(args.steps):
         k0 = len(c.pp[False])
+        t0 = time.perf_counter()
         c.sample(0.75 * per_step, False, parts=2)
         c.sample(0.25 * per_step, True, parts=1)
+        walls.append(time.perf_counter() - t0)
         step_pp = statistics.fmean(c.pp[False][k0:])
         vals.append(1.0 / (c.tm["fields_s"] + c.tm["peaks_s"] + step_pp * c.npk))
     base = c.baseline()
     v = base["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.fmean(walls),
+            "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 shell sums", "data": "synthetic",
             "config": config_dict(n),
             "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "step_values": vals, "stages_s": base["stages_s"], "truncated_shells": base["truncated_shells"],
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "ms_per_step is the extrapolated time of one whole tile; each timed step runs a sample of it"}
+            "tile_s_extrapolated": 1.0 / v,
+            "note": "each timed step runs a sample of the tile (ms_per_step is its wall time); value is the tile "
+                    "rate extrapolated from all steps' samples with the full-size fields and peak search"}
     print(json.dumps(line), flush=True)
 
 
@@ -371,7 +383,10 @@ def run_ours(args, dist: Dist):
             "gpu_launches": int(launches),
             "roofline": {"kernel": "gather_kernel (shell sums)", "bound": "hbm",
                          "achieved": achieved, "peak": peaks[0], "unit": "GB/s",
-                         "frac": achieved / peaks[0] if peaks[0] else None, "traffic": GATHER_TRAFFIC_384 if n == 384 else None,
+                         "frac": achieved / peaks[0] if peaks[0] else None,
+                         "traffic": gather_traffic(last_shell_stats["visits"], last_shell_stats["pool_rows"]),
+                         "traffic_model": "dram read 2.35 B per cell visit + dram write 218 B per profile row "
+                                          "(ncu capture of the 384^3 launch)",
                          "peak_source": peaks[1],
                          "alg_bytes_per_launch": bytes_alg / max(1, args.steps),
                          "kernel_ms_per_launch": gather_ms / max(1, args.steps),
@@ -387,10 +402,19 @@ def run_ours(args, dist: Dist):
     return line
 
 
-# DRAM bytes (read + write) of one gather_kernel launch on the 384^3 tile,
-# scaled from the ncu capture of the same kernel on the 256^3 tile by the cell
-# visits (profiles/gather_kernel_run_tile_256.md): 1.713 GB x 824.5M / 179.3M
-GATHER_TRAFFIC_384 = 7.88e9
+# DRAM traffic of the gather kernel: reads per cell visit (records the L2
+# does not hold) and writes per profile row (the 24-double rows of the pool
+# and the staging slots that reach DRAM), from the ncu capture of one launch
+# on the 384^3 benchmark tile (dram__bytes_read.sum 1.94 GB and
+# dram__bytes_write.sum 6.11 GB for 824,483,046 visits and 27,993,492 rows;
+# the 256^3 tile's launch, 0.403 + 1.30 GB for 179,268,416 visits and
+# 6,073,951 rows, is within 3 % of the same model)
+GATHER_DRAM_READ_PER_VISIT = 1.94e9 / 824_483_046
+GATHER_DRAM_WRITE_PER_ROW = 6.11e9 / 27_993_492
+
+
+def gather_traffic(visits: float, rows: float) -> float:
+    return GATHER_DRAM_READ_PER_VISIT * visits + GATHER_DRAM_WRITE_PER_ROW * rows
 
 
 def _plain_compare(ctx, cfg, seed, dev_out, cap, opt_tiles_per_s):
@@ -788,7 +812,7 @@ def run_shells_bench(args, dist: Dist):
         st = ctx.shell_stats()
         km = st["kernel_ms"]
         gather_s = km["gather"] / 1000.0
-        out[name] = {"shell_stage_ms": st["ms"], "kernel_ms": km, "visits": st["visits"],
+        out[name] = {"shell_stage_ms": st["ms"], "kernel_ms": km, "visits": st["visits"], "pool_rows": st["pool_rows"],
                      "peaks_per_s": npk / (st["ms"] / 1000.0), "batches": st["batches"],
                      "gather_GBps": st["visits"] * 32 / gather_s / 1e9 if gather_s > 0 else None,
                      "halos": None}
@@ -805,7 +829,9 @@ def run_shells_bench(args, dist: Dist):
             "optimised": opt, "plain": out["plain"], "autotune": tune,
             "roofline": {"kernel": "gather_kernel (compensated)", "bound": "hbm", "achieved": opt["gather_GBps"],
                          "peak": peaks[0], "unit": "GB/s", "frac": (opt["gather_GBps"] or 0) / peaks[0],
-                         "traffic": None, "peak_source": peaks[1]},
+                         "traffic": gather_traffic(opt["visits"], opt["pool_rows"]), "peak_source": peaks[1],
+                         "traffic_model": "dram read 2.35 B per cell visit + dram write 218 B per profile row "
+                                          "(ncu capture of the 384^3 tile's launch)"},
             "optimised_over_plain": out["plain"]["shell_stage_ms"] / opt["shell_stage_ms"],
             "roofline_plain_gather": {"bound": "hbm", "achieved": out["plain"]["gather_GBps"], "peak": peaks[0],
                                       "frac": (out["plain"]["gather_GBps"] or 0) / peaks[0], "unit": "GB/s",
