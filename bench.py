@@ -902,6 +902,8 @@ def _apply_options(ctx, args):
     import peakpatch_b200 as pp
     ctx.set_option(pp.OPT_GRAPHS, 0 if getattr(args, "no_graphs", False) else 1)
     ctx.set_option(pp.OPT_AUTOTUNE, 0 if getattr(args, "no_autotune", False) else 1)
+    if getattr(args, "collapse", 0):
+        ctx.set_option(pp.OPT_COLLAPSE_THREADS, args.collapse)
 
 
 def _measured_peaks():
@@ -937,6 +939,8 @@ def main():
     ap.add_argument("--split-n", type=int, default=192, help="nmesh of the --split workload")
     ap.add_argument("--no-graphs", action="store_true", help="launch kernels one by one instead of as CUDA graphs")
     ap.add_argument("--no-autotune", action="store_true", help="default shell-stage choices, no autotuning")
+    ap.add_argument("--collapse", type=int, default=0,
+                    help="fix the collapse kernel (PPB_OPT_COLLAPSE_THREADS: 1, 2, 4, 8; 0 the tuner's choice)")
     args = ap.parse_args()
     dist = Dist()
     try:

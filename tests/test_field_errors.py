@@ -9,9 +9,10 @@ RTHL, mass (proportional to RTHL^3), the three eigenvalues of the strain at
 RTHL, the displacements Sbar (1LPT) and Sbar2 (2LPT), Fbarx, e_v, p_v, the
 gradients, Srb, zvir_half and d2F.
 
-Size and sample are set by PPB_FIELD_ERR_N (default 128) and
-PPB_FIELD_ERR_SAMPLE (peaks compared, 0 = all); PPB_FIELD_ERR_OUT names a JSON
-file that receives the table."""
+Two cases by default: 128^3 with every peak, and the 384^3 benchmark tile on
+a fixed sample of 20,000 peaks.  PPB_FIELD_ERR_N and PPB_FIELD_ERR_SAMPLE
+(peaks compared, 0 = all) replace them by one case; PPB_FIELD_ERR_OUT names a
+JSON file that receives the table of the last case."""
 import json
 import os
 
@@ -23,8 +24,10 @@ pytestmark = pytest.mark.gpu
 import peakpatch_b200 as pp
 from conftest import filter_bank
 
-N = int(os.environ.get("PPB_FIELD_ERR_N", "128"))
-SAMPLE = int(os.environ.get("PPB_FIELD_ERR_SAMPLE", "0"))
+if os.environ.get("PPB_FIELD_ERR_N"):
+    CASES = [(int(os.environ["PPB_FIELD_ERR_N"]), int(os.environ.get("PPB_FIELD_ERR_SAMPLE", "0")))]
+else:
+    CASES = [(128, 0), (384, 20000)]
 RTOL = 1e-4
 MISMATCH = 1e-3
 
@@ -71,7 +74,8 @@ def field_error_table(g, o):
             "fields": table}
 
 
-def test_per_field_error_vs_fp64_oracle(ora, julia_table, eh_pk):
+@pytest.mark.parametrize("N,SAMPLE", CASES)
+def test_per_field_error_vs_fp64_oracle(ora, julia_table, eh_pk, N, SAMPLE):
     from peakpatch_b200 import powerspec   # noqa: F401  (EH table comes from the fixture)
     k, P = eh_pk
     T = julia_table
@@ -91,6 +95,10 @@ def test_per_field_error_vs_fp64_oracle(ora, julia_table, eh_pk):
         fp64 = ctx.analyse_peaks(*args, st["nhunt"], plain=True)
     res = {"nmesh": N, "peaks": int(len(sel)), "compensated_fp32": field_error_table(comp, o),
            "fp64": field_error_table(fp64, o)}
+    for key in ("compensated_fp32", "fp64"):
+        t = res[key]
+        print(f"{N}^3 {key}: {t['compared']} of {t['halos']} halos compared, mismatch {t['mismatch']:.1e}; max rel "
+              + ", ".join(f"{k} {v['max']:.1e}" for k, v in t["fields"].items()))
     out = os.environ.get("PPB_FIELD_ERR_OUT")
     if out:
         with open(out, "w") as f:
