@@ -904,6 +904,8 @@ def _apply_options(ctx, args):
     ctx.set_option(pp.OPT_AUTOTUNE, 0 if getattr(args, "no_autotune", False) else 1)
     if getattr(args, "collapse", 0):
         ctx.set_option(pp.OPT_COLLAPSE_THREADS, args.collapse)
+    if getattr(args, "gather_ring", -1) >= 0:
+        ctx.set_option(pp.OPT_GATHER_RING, args.gather_ring)
 
 
 def _measured_peaks():
@@ -939,6 +941,8 @@ def main():
     ap.add_argument("--split-n", type=int, default=192, help="nmesh of the --split workload")
     ap.add_argument("--no-graphs", action="store_true", help="launch kernels one by one instead of as CUDA graphs")
     ap.add_argument("--no-autotune", action="store_true", help="default shell-stage choices, no autotuning")
+    ap.add_argument("--gather-ring", type=int, default=-1,
+                    help="1: gather records through TMA-staged shared-memory rings, 0: plain loads (default: library)")
     ap.add_argument("--collapse", type=int, default=0,
                     help="fix the collapse kernel (PPB_OPT_COLLAPSE_THREADS: 1, 2, 4, 8; 0 the tuner's choice)")
     args = ap.parse_args()

@@ -486,6 +486,13 @@ int32_t ppb_last_table_stats(ppb_ctx* ctx, float* ms, int64_t* steps);
  *  PPB_OPT_COLLAPSE_THREADS  fixes the collapse kernel: 1, 2 or 4 threads
  *                     per peak, 8 one thread per peak with lane work queues,
  *                     0 (default) the tuner's choice.
+ *  PPB_OPT_GATHER_RING  1: the shell gather stages its records through
+ *                     per-lane shared-memory rings filled by TMA
+ *                     (tile::gather4 bulk tensor copies, two stages, bounded
+ *                     mbarrier waits); 0 (default): 256-bit loads straight
+ *                     from global memory.  Same records either way; the
+ *                     staged form is slower on B200 (the TMA unit serialises
+ *                     the 128-byte gathers) and is kept for comparison.
  *  PPB_OPT_FUSED_X    the filter bank's x pass fused with the peak search
  *                     (grid sizes 64 J, J <= 8, one window over the grid):
  *                     -1 (default) with the k^2-weighted twin (ioutshear)
@@ -502,6 +509,7 @@ enum {
   PPB_OPT_BRICK_SHIFT = 4,
   PPB_OPT_COLLAPSE_THREADS = 5,
   PPB_OPT_FUSED_X = 6,
+  PPB_OPT_GATHER_RING = 7,
   PPB_OPT_GRAPH_LAUNCHES = 16,
   PPB_OPT_GRAPH_INSTANTIATIONS = 17,
   PPB_OPT_GRAPH_UPDATES = 18

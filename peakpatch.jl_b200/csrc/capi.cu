@@ -310,7 +310,8 @@ static void shell_order(Slot& sl, ShellArgs& b, int brick_shift) {
   b.order = sl.oidx2.as<int32_t>();
 }
 
-TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool adaptive, int gblocks) {
+TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool adaptive, int gblocks,
+                                const void* rmap) {
   cudaStream_t s = sl.stream;
   Launch L{s, &sl.launches};
   TuneEntry te;
@@ -333,7 +334,7 @@ TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool ad
       PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, kCtlBytes, s));
       shell_order(sl, b, bricks[c]);
       PPB_CUDA(cudaEventRecord(ev[0], s));
-      launch_shell_gather(L, b, comp, adaptive, gblocks);
+      launch_shell_gather(L, b, comp, adaptive, gblocks, rmap);
       PPB_CUDA(cudaEventRecord(ev[1], s));
       PPB_CUDA(cudaEventSynchronize(ev[1]));
       float ms = 0.f;
@@ -381,15 +382,20 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
                          const std::function<void()>& pre) {
   cudaStream_t stream = sl.stream;
   Launch L{stream, &sl.launches};
-  int& bps = sl.gather_bps[comp][adaptive];
-  if (bps == 0) bps = shell_gather_blocks_per_sm(comp, adaptive);
+  // the TMA-staged gather (records through per-lane shared-memory rings)
+  // when the option asks for it and the records fit a tensor map
+  alignas(64) unsigned char ring_map[128];
+  const bool ring = sh.gather_ring.load() != 0 && record_ring_map(a.aos, a.n, ring_map);
+  int& bps = sl.gather_bps[comp][adaptive][ring];
+  if (bps == 0) bps = ring ? shell_gather_ring_blocks_per_sm(comp, adaptive) : shell_gather_blocks_per_sm(comp, adaptive);
   const int gblocks = nsm * bps;
+  const void* rmap = ring ? ring_map : nullptr;
   const int64_t stride = shell_stage_doubles_per_warp(a.nshell);
   sl.stage.ensure((size_t)((int64_t)gblocks * kGatherWarps * stride * 8));
   sl.counters.ensure(16 * 8);
   sl.ctl.ensure(kCtlBytes);
   grow(sl.hdr, std::max<size_t>(1, (size_t)a.npk) * sizeof(PeakHdr));
-  grow(sl.geo, std::max<size_t>(1, (size_t)a.npk) * sizeof(int4));
+  grow(sl.geo, std::max<size_t>(1, (size_t)a.npk) * 2 * sizeof(int4));
   grow(sl.mlim, std::max<size_t>(1, (size_t)a.npk) * sizeof(int32_t));
   PPB_CUDA(cudaMemsetAsync(sl.counters.p, 0, 16 * 8, stream));
   // profile pool: sized from the rows per peak of the previous call; peaks
@@ -441,7 +447,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     b.npk = nb;
     b.out = a.out + p0 * RES_N;
     b.hdr = sl.hdr.as<PeakHdr>() + p0;
-    b.geo = sl.geo.as<int4>() + p0;
+    b.geo = sl.geo.as<int4>() + 2 * p0;
     b.mlim = sl.mlim.as<int32_t>() + p0;
     b.r2lim = a.r2lim ? a.r2lim + p0 : nullptr;
     b.npcap = a.npcap ? a.npcap + p0 : nullptr;
@@ -469,7 +475,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     }
     if (tune_now) {
       if (first && pre) pre();   // the tuning pass reads what `pre` writes
-      te = tune_shells(sl, b, comp, adaptive, gblocks);
+      te = tune_shells(sl, b, comp, adaptive, gblocks, rmap);
       {
         std::lock_guard<std::mutex> lk(sh.cache_mu);
         sh.tune[tkey] = te;
@@ -486,7 +492,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
       PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, kCtlBytes, stream));
       record_event(sl.shell_ev[0], stream);
       shell_order(sl, b, te.brick_shift);
-      launch_shell_gather(L, b, comp, adaptive, gblocks);
+      launch_shell_gather(L, b, comp, adaptive, gblocks, rmap);
       record_event(sl.shell_ev[1], stream);
       launch_shell_collapse(L, b, nsm, sl.walk_per_peak, te.collapse_threads);
       record_event(sl.shell_ev[2], stream);
@@ -526,6 +532,8 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
   for (int i = 0; i < 16; i++) s.raw[i] = c[i];
   sl.last_shell = s;
   if (st) *st = s;
+  if (c[10] != 0)
+    throw Error{PPB_ERR_CUDA, "gather: a staged record copy did not complete within the wait bound"};
 }
 
 // ---------------------------------------------------------------------------
@@ -1026,6 +1034,10 @@ int32_t ppb_set_option(ppb_ctx* ctx, int32_t option, int64_t value) {
       PPB_REQUIRE(value >= -1 && value <= 1, "PPB_OPT_FUSED_X takes -1, 0 or 1");
       ctx->sh.fused_x.store((int)value);
       break;
+    case PPB_OPT_GATHER_RING:
+      PPB_REQUIRE(value == 0 || value == 1, "PPB_OPT_GATHER_RING takes 0 or 1");
+      ctx->sh.gather_ring.store((int)value);
+      break;
     default:
       throw Error{PPB_ERR_INVALID, "unknown or read-only option"};
   }
@@ -1043,6 +1055,7 @@ int32_t ppb_get_option(ppb_ctx* ctx, int32_t option, int64_t* value) {
     case PPB_OPT_BRICK_SHIFT: *value = ctx->sh.force_brick.load(); break;
     case PPB_OPT_COLLAPSE_THREADS: *value = ctx->sh.force_collapse.load(); break;
     case PPB_OPT_FUSED_X: *value = ctx->sh.fused_x.load(); break;
+    case PPB_OPT_GATHER_RING: *value = ctx->sh.gather_ring.load(); break;
     case PPB_OPT_GRAPH_LAUNCHES:
     case PPB_OPT_GRAPH_INSTANTIATIONS:
     case PPB_OPT_GRAPH_UPDATES: {

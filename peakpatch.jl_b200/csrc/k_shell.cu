@@ -40,6 +40,8 @@
 //
 //  d2f_kernel (one warp per collapsed peak).  Mean Laplacian over the cells
 //    within RTHL in list order, stopping at the first out-of-grid cell.
+#include <cuda.h>   // CUtensorMap
+
 #include <algorithm>
 #include <type_traits>
 
@@ -54,7 +56,7 @@ constexpr unsigned FULL = 0xffffffffu;
 
 // counters layout
 enum { CNT_VISITS = 0, CNT_PREMASK = 1, CNT_NOFCRIT = 2, CNT_M0ONE = 3, CNT_NOCOLL = 4, CNT_RTHLNEG = 5,
-       CNT_GUARD = 6, CNT_AKK = 7, CNT_BADPEAK = 8, CNT_WALK = 9 };
+       CNT_GUARD = 6, CNT_AKK = 7, CNT_BADPEAK = 8, CNT_WALK = 9, CNT_RING = 10 };
 
 // ---------------------------------------------------------------------------
 // accumulators
@@ -332,21 +334,215 @@ __device__ __forceinline__ int visit_chunk(const ShellArgs& a, int ck, int cnt, 
   return nsh;
 }
 
+// ---------------------------------------------------------------------------
+// TMA-staged records.  Each lane owns a two-stage ring in shared memory: a
+// stage is one tile::gather4 bulk tensor copy of the four records of one
+// step (four rows of the record array viewed as an n^3 x 8 float tensor,
+// box 8 x 1) completing on the lane's own mbarrier.  While the lane sums the
+// four cells of step s from shared memory, the copy of step s + 1 is in
+// flight, so the record latency is hidden without holding the records in
+// registers.  Slot j of a stage holds cell (j - lane) & 3 of the step, so
+// that the lanes of a shared-memory phase read different banks.  Every wait
+// is bounded in time (kRingWaitNs on the global timer): a wait that gives up
+// counts CNT_RING (the host then fails the call) and retires the lane's
+// ring, which then issues no copy and waits no more, and the lane goes on
+// with stale slots; before the kernel ends a lane waits (bounded again) for
+// every copy it still has in flight.
+// ---------------------------------------------------------------------------
+constexpr int kRingStages = 2;
+constexpr int kRingSlot = 128;   // bytes per lane and stage: four records
+constexpr int kRingWarpBytes = kRingStages * 32 * (kRingSlot + 8);
+constexpr unsigned long long kRingWaitNs = 200000000ull;   // 0.2 s
+
+struct Ring {
+  uint32_t slot;    // shared address of the lane's stage-0 slot
+  uint32_t bar;     // shared address of the lane's stage-0 mbarrier
+  uint32_t phase;   // bit st: the parity the next wait on stage st expects
+  uint32_t pend;    // bit st: a copy into stage st is in flight
+  bool dead;        // a wait gave up: no more copies or waits
+  uint64_t tm;      // generic address of the tensor map (kernel parameter)
+  unsigned long long* counters;
+  __device__ __forceinline__ uint32_t slot_at(int st) const { return slot + st * 32 * kRingSlot; }
+  __device__ __forceinline__ uint32_t bar_at(int st) const { return bar + st * 32 * 8; }
+};
+
+__device__ __forceinline__ void ring_init(Ring& R) {
+#pragma unroll
+  for (int st = 0; st < kRingStages; st++)
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(R.bar_at(st)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncwarp();
+}
+
+// rows r0..r3 (cells of the step in slot order) into stage st
+__device__ __forceinline__ void ring_issue(Ring& R, int st, int r0, int r1, int r2, int r3) {
+  if (R.dead) return;
+  const uint32_t bar = R.bar_at(st), dst = R.slot_at(st);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kRingSlot) : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+      "l"(R.tm), "r"(0), "r"(r0), "r"(r1), "r"(r2), "r"(r3), "r"(bar)
+      : "memory");
+  R.pend |= 1u << st;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// wait for stage st's copy for at most kRingWaitNs; true when it completed
+__device__ __forceinline__ bool ring_wait_bounded(Ring& R, int st) {
+  const uint32_t bar = R.bar_at(st), par = (R.phase >> st) & 1u;
+  uint32_t done = 0;
+  const unsigned long long t0 = global_ns();
+  while (true) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(bar), "r"(par)
+        : "memory");
+    if (done || global_ns() - t0 > kRingWaitNs) break;
+  }
+  if (done) {
+    R.phase ^= 1u << st;
+    R.pend &= ~(1u << st);
+  }
+  return done != 0;
+}
+
+__device__ __forceinline__ void ring_wait(Ring& R, int st) {
+  if (R.dead) return;
+  if (!ring_wait_bounded(R, st)) {
+    atomicAdd(R.counters + CNT_RING, 1ull);
+    R.dead = true;
+  }
+}
+
+// before the kernel ends: no copy of this lane may still be in flight
+__device__ __forceinline__ void ring_drain(Ring& R) {
+#pragma unroll
+  for (int st = 0; st < kRingStages; st++)
+    if (R.pend & (1u << st)) ring_wait_bounded(R, st);
+}
+
+__device__ __forceinline__ void lds_record(uint32_t addr, float4& a, float4& b) {
+  asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+               : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w)
+               : "r"(addr));
+  asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+               : "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+               : "r"(addr + 16));
+}
+
+// the rows (cell indices, the peak cell for cells past the chunk or off the
+// grid) and the in-grid mask of step s of a chunk
+__device__ __forceinline__ unsigned step_rows(const int4 w4, int c, int cnt, int lin, bool inside, int pi, int pj,
+                                              int pk, int n, int n2, int* row) {
+  const int w[4] = {w4.x, w4.y, w4.z, w4.w};
+  unsigned ok = 0;
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int di = (w[u] << 24) >> 24, dj = (w[u] << 16) >> 24, dk = (w[u] << 8) >> 24;
+    bool in = c + u < cnt;
+    if (!inside)
+      in = in && (unsigned)(pi + di) < (unsigned)n && (unsigned)(pj + dj) < (unsigned)n &&
+           (unsigned)(pk + dk) < (unsigned)n;
+    ok |= (in ? 1u : 0u) << u;
+    row[u] = lin + (in ? di + n * dj + n2 * dk : 0);
+  }
+  return ok;
+}
+
+__device__ __forceinline__ void ring_issue_step(Ring& R, int st, const int* row, int rot) {
+  // slot j <- cell (j - rot) & 3
+  int r[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int q = (j - rot) & 3;
+    r[j] = q == 0 ? row[0] : q == 1 ? row[1] : q == 2 ? row[2] : row[3];
+  }
+  ring_issue(R, st, r[0], r[1], r[2], r[3]);
+}
+
+// visit_chunk with the records staged by the ring (same cells, same order
+// of the callbacks)
+template <class F>
+__device__ __forceinline__ int visit_chunk_ring(const ShellArgs& a, Ring& R, int ck, int cnt, int lin, bool inside,
+                                                int pi, int pj, int pk, F&& cell) {
+  const int n = a.n, n2 = a.n * a.n;
+  const int4* __restrict__ cp = a.ck_cells + __ldg(a.ck_p + ck);
+  const int nst = (cnt + 3) >> 2;
+  const int rot = threadIdx.x & 3;
+  int4 w0 = make_int4(0, 0, 0, 0), w1 = w0;
+  unsigned ok0 = 0, ok1 = 0;
+  int row[4];
+  if (nst > 0) {
+    w0 = __ldg(cp);
+    ok0 = step_rows(w0, 0, cnt, lin, inside, pi, pj, pk, n, n2, row);
+    ring_issue_step(R, 0, row, rot);
+  }
+  if (nst > 1) {
+    w1 = __ldg(cp + 1);
+    ok1 = step_rows(w1, 4, cnt, lin, inside, pi, pj, pk, n, n2, row);
+    ring_issue_step(R, 1, row, rot);
+  }
+  int nsh = 0;
+  auto consume = [&](int st, const int4 w4, unsigned ok) {
+    ring_wait(R, st);
+    const int w[4] = {w4.x, w4.y, w4.z, w4.w};
+    const uint32_t base = R.slot_at(st);
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      if (ok & (1u << u)) {
+        float4 h0, h1;
+        lds_record(base + ((u + rot) & 3) * 32, h0, h1);
+        nsh++;
+        cell(h0, h1, small_int_float((w[u] << 24) >> 24), small_int_float((w[u] << 16) >> 24),
+             small_int_float((w[u] << 8) >> 24));
+      }
+    }
+    // the slot's reads come before the next copy into it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  };
+  for (int s = 0; s < nst; s += 2) {
+    consume(0, w0, ok0);
+    if (s + 2 < nst) {
+      w0 = __ldg(cp + s + 2);
+      ok0 = step_rows(w0, 4 * (s + 2), cnt, lin, inside, pi, pj, pk, n, n2, row);
+      ring_issue_step(R, 0, row, rot);
+    }
+    if (s + 1 < nst) {
+      consume(1, w1, ok1);
+      if (s + 3 < nst) {
+        w1 = __ldg(cp + s + 3);
+        ok1 = step_rows(w1, 4 * (s + 3), cnt, lin, inside, pi, pj, pk, n, n2, row);
+        ring_issue_step(R, 1, row, rot);
+      }
+    }
+  }
+  return nsh;
+}
+
 // the chunk's 19 sums (and its in-grid cell count) into column `col` of the
 // warp's partial table
-template <bool COMP>
+template <bool COMP, bool RING>
 __device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, int64_t lin, bool inside, int pi,
-                                         int pj, int pk, double* part, int col) {
+                                         int pj, int pk, double* part, int col, Ring* ring) {
   int nsh;
   const float2* K = reinterpret_cast<const float2*>(part + (NACC + 1) * 32);
   if constexpr (COMP) {
     AccH<11> A;
     A.K = K;
     A.zero();
-    nsh = visit_chunk(a, ck, cnt, lin, inside, pi, pj, pk,
-                         [&](const float4& h0, const float4& h1, float di, float dj, float dk) {
-                           accumulate_cell_comp(A, h0, h1, di, dj, dk);
-                         });
+    auto f = [&](const float4& h0, const float4& h1, float di, float dj, float dk) {
+      accumulate_cell_comp(A, h0, h1, di, dj, dk);
+    };
+    if constexpr (RING) nsh = visit_chunk_ring(a, *ring, ck, cnt, (int)lin, inside, pi, pj, pk, f);
+    else nsh = visit_chunk(a, ck, cnt, lin, inside, pi, pj, pk, f);
     part[0 * 32 + col] = A.X(0);
     part[1 * 32 + col] = A.X(1);
     part[2 * 32 + col] = A.Y(1);
@@ -369,10 +565,11 @@ __device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, in
   } else {
     Acc<false> A;
     A.zero();
-    nsh = visit_chunk(a, ck, cnt, lin, inside, pi, pj, pk,
-                         [&](const float4& h0, const float4& h1, float di, float dj, float dk) {
-                           accumulate_cell(A, h0, h1, di, dj, dk);
-                         });
+    auto f = [&](const float4& h0, const float4& h1, float di, float dj, float dk) {
+      accumulate_cell(A, h0, h1, di, dj, dk);
+    };
+    if constexpr (RING) nsh = visit_chunk_ring(a, *ring, ck, cnt, (int)lin, inside, pi, pj, pk, f);
+    else nsh = visit_chunk(a, ck, cnt, lin, inside, pi, pj, pk, f);
 #pragma unroll
     for (int v = 0; v < NACC; v++) part[v * 32 + col] = A.get(v);
   }
@@ -380,22 +577,27 @@ __device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, in
   return nsh;
 }
 
-template <bool COMP, bool ADAPTIVE>
-__device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double* part) {
+template <bool COMP, bool ADAPTIVE, bool RING>
+__device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double* part, Ring* ring) {
   const int lane = threadIdx.x & 31;
   PeakHdr* hdr = a.hdr + p;
-  const int n = a.n;
-  const int64_t n2 = (int64_t)n * n;
-  const int64_t lin = a.pk.lin[p];
-  const double ZZon = a.pk.ZZon[p];
-  if (lin < 0 || lin >= n2 * n || !(ZZon > -1.0)) {   // invalid peak index or redshift from the caller
+  int4 gq, pc;   // geometry, and the peak's cell with its flags (geometry kernel)
+  {
+    const float4* g2 = reinterpret_cast<const float4*>(a.geo + 2 * p);
+    float4 u, v;
+    ldg_record(g2, u, v);
+    gq = make_int4(__float_as_int(u.x), __float_as_int(u.y), __float_as_int(u.z), __float_as_int(u.w));
+    pc = make_int4(__float_as_int(v.x), __float_as_int(v.y), __float_as_int(v.z), __float_as_int(v.w));
+  }
+  if (!(pc.w & 1)) {   // invalid peak index or redshift from the caller
     if (lane == 0) {
       atomicAdd(a.counters + CNT_BADPEAK, 1ull);
       hdr->status = HS_BAD;
     }
     return;
   }
-  const int pk = (int)(lin / n2), pj = (int)((lin / n) % n), pi = (int)(lin % n);
+  const int64_t lin = a.pk.lin[p];
+  const int pi = pc.x, pj = pc.y, pk = pc.z;
   const double fcrit = a.pk.fcrit[p];
   const double* __restrict__ rad = a.rad;
   const int mmax = a.mlim[p];   // the peak's last finalised shell
@@ -403,7 +605,6 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
   // shorter list reads only its own shells; the list's last shell is never
   // finalised, RadialShell.jl:386-390)
   const int cell_lim = __ldg(a.sh_start + mmax);
-  const int4 gq = a.geo[p];
   const int m0_init = gq.x, mrf = gq.y, mupp_rf = gq.w;
 
   // ---- the peak cell (shell 1) ------------------------------------------
@@ -422,9 +623,7 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
     else if (lane == R_S2 + 2) v = (double)c1.w;
     stage[ROW + lane] = v;
   }
-  const int rext = (int)ceil(__ldg(rad + mmax)) + 1;
-  const bool inside = pi - rext >= 0 && pj - rext >= 0 && pk - rext >= 0 && pi + rext < n && pj + rext < n &&
-                      pk + rext < n;
+  const bool inside = (pc.w & 2) != 0;
   int state = 0;          // 0 unknown, 1 inward, 2 crossing found
   int mcross = 0;
   int mtarget = ADAPTIVE ? -1 : mmax;   // last shell to gather (-1: not known yet)
@@ -440,7 +639,7 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
     // (a) lane l sums chunk c0g + l into the shared partial table
     if (lane < ncg) {
       const int s0 = __ldg(a.ck_s + c0g + lane), cnt = s0 < cell_lim ? __ldg(a.ck_n + c0g + lane) : 0;
-      visits += sum_chunk<COMP>(a, c0g + lane, cnt, lin, inside, pi, pj, pk, part, lane);
+      visits += sum_chunk<COMP, RING>(a, c0g + lane, cnt, lin, inside, pi, pj, pk, part, lane, ring);
     }
     __syncwarp();
     // (b) lane l finalises shell base + l from its chunks (double-precision
@@ -618,9 +817,44 @@ __global__ void __launch_bounds__(32 * kGatherWarps, PPB_GATHER_MINB) gather_ker
     q = __shfl_sync(FULL, q, 0);
     if (q >= a.npk) break;
     const int64_t p = a.order ? (int64_t)a.order[q] : (int64_t)q;
-    gather_one<COMP, ADAPTIVE>(a, p, stage, part);
+    gather_one<COMP, ADAPTIVE, false>(a, p, stage, part, nullptr);
     __syncwarp();
   }
+}
+
+// The same with the records staged through each lane's TMA ring (tm: the
+// record array as an n^3 x 8 float tensor, box 8 x 1; n^3 < 2^31).  Shared
+// memory: the warps' rings, then their partial tables.
+template <bool COMP, bool ADAPTIVE>
+__global__ void __launch_bounds__(32 * kGatherWarps, PPB_GATHER_MINB)
+    gather_ring_kernel(ShellArgs a, const __grid_constant__ CUtensorMap tm) {
+  extern __shared__ __align__(128) unsigned char rsm[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int64_t slot = (int64_t)blockIdx.x * kGatherWarps + wib;
+  double* stage = a.stage + slot * a.stage_stride;
+  unsigned char* ring_mem = rsm + (size_t)wib * kRingWarpBytes;
+  double* part = reinterpret_cast<double*>(rsm + (size_t)kGatherWarps * kRingWarpBytes) + (size_t)wib * GATHER_WARP_DOUBLES;
+  Ring R;
+  R.slot = (uint32_t)__cvta_generic_to_shared(ring_mem) + lane * kRingSlot;
+  R.bar = (uint32_t)__cvta_generic_to_shared(ring_mem + kRingStages * 32 * kRingSlot) + lane * 8;
+  R.phase = 0;
+  R.pend = 0;
+  R.dead = false;
+  R.tm = reinterpret_cast<uint64_t>(&tm);
+  R.counters = a.counters;
+  ring_init(R);
+  if (COMP) set_anchors(a, reinterpret_cast<float2*>(part + (NACC + 1) * 32));
+  while (true) {
+    int q = 0;
+    if (lane == 0) q = atomicAdd(a.queue, 1);
+    q = __shfl_sync(FULL, q, 0);
+    if (q >= a.npk) break;
+    const int64_t p = a.order ? (int64_t)a.order[q] : (int64_t)q;
+    gather_one<COMP, ADAPTIVE, true>(a, p, stage, part, &R);
+    __syncwarp();
+  }
+  ring_drain(R);
 }
 
 // interleave the low 10 bits of x, y, z (Morton order)
@@ -664,14 +898,28 @@ __global__ void geo_kernel(ShellArgs a, uint32_t* key, int32_t* idx) {
   }
   a.mlim[p] = mmax;
   const Geo g = geometry(a, a.pk.Rf[p], a.pk.ir2min[p], mmax);
-  a.geo[p] = make_int4(g.m0_init, g.mrf, g.mlow_rf, g.mupp_rf);
+  a.geo[2 * p] = make_int4(g.m0_init, g.mrf, g.mlow_rf, g.mupp_rf);
+  // the peak's cell and flags for the gather: bit 0 a valid peak (index on
+  // the grid, redshift > -1), bit 1 every cell of its shells up to mmax
+  // (radius < rad[mmax] + 1) on the grid
+  const int64_t lin = a.pk.lin[p], n = a.n, n2 = n * n;
+  const bool valid = lin >= 0 && lin < n2 * n && a.pk.ZZon[p] > -1.0;
+  int pi = 0, pj = 0, pk = 0, flags = 0;
+  if (valid) {
+    pk = (int)(lin / n2);
+    pj = (int)((lin / n) % n);
+    pi = (int)(lin % n);
+    const int rext = (int)ceil(__ldg(a.rad + mmax)) + 1;
+    const bool inside = pi - rext >= 0 && pj - rext >= 0 && pk - rext >= 0 && pi + rext < n && pj + rext < n &&
+                        pk + rext < n;
+    flags = 1 | (inside ? 2 : 0);
+  }
+  a.geo[2 * p + 1] = make_int4(pi, pj, pk, flags);
   if (key) {
-    const int64_t lin = a.pk.lin[p], n = a.n, n2 = n * n;
     uint32_t k = 0xffffffffu;   // invalid peaks last
     if (lin >= 0 && lin < n2 * n) {
       const int b = a.brick_shift;
-      const uint32_t i = (uint32_t)(lin % n) >> b, j = (uint32_t)((lin / n) % n) >> b, kk = (uint32_t)(lin / n2) >> b;
-      k = spread3(i) | (spread3(j) << 1) | (spread3(kk) << 2);
+      k = spread3((uint32_t)pi >> b) | (spread3((uint32_t)pj >> b) << 1) | (spread3((uint32_t)pk >> b) << 2);
     }
     key[p] = k;
     idx[p] = (int32_t)p;
@@ -950,7 +1198,7 @@ __device__ void collapse_one(const ShellArgs& a, int64_t p) {
   const double ZZon = a.pk.ZZon[p];
   const double alatt = a.alatt;
   const int m = a.mlim[p];
-  const int4 gq = a.geo[p];
+  const int4 gq = a.geo[2 * p];
   Geo geo;
   geo.m0_init = gq.x; geo.mrf = gq.y; geo.mlow_rf = gq.z; geo.mupp_rf = gq.w;
   const double anor = 1.0;
@@ -1036,7 +1284,7 @@ __device__ void collapse_group(const ShellArgs& a, int64_t p, int q, int qbase, 
   const double ZZon = a.pk.ZZon[p];
   const double alatt = a.alatt;
   const int m = a.mlim[p];
-  const int4 gq = a.geo[p];
+  const int4 gq = a.geo[2 * p];
   Geo geo;
   geo.m0_init = gq.x; geo.mrf = gq.y; geo.mlow_rf = gq.z; geo.mupp_rf = gq.w;
   const double anor = 1.0;
@@ -1163,7 +1411,7 @@ __global__ void __launch_bounds__(128) collapseq_kernel(ShellArgs a) {
             R = Rows{a.pool + h.off * ROW, h.mdone, a.counters};
             ZZon = a.pk.ZZon[p];
             m = a.mlim[p];
-            const int4 gq = a.geo[p];
+            const int4 gq = a.geo[2 * p];
             mrf = gq.y; mlo = gq.z; mup = gq.w;
             hi1 = last_lt(rad, 2, m, 2.0);
             m0 = h.m0;
@@ -1367,14 +1615,66 @@ void launch_shell_geo(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx)
   PPB_LAUNCHED(*L.count);
 }
 
-void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks) {
+constexpr size_t kGatherRingSmem = (size_t)kGatherWarps * kRingWarpBytes + kGatherSmem;
+
+int shell_gather_ring_blocks_per_sm(bool comp, bool adaptive) {
+  const void* f = comp ? (adaptive ? (const void*)gather_ring_kernel<true, true>
+                                   : (const void*)gather_ring_kernel<true, false>)
+                       : (adaptive ? (const void*)gather_ring_kernel<false, true>
+                                   : (const void*)gather_ring_kernel<false, false>);
+  PPB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherRingSmem));
+  int b = 0;
+  PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, 32 * kGatherWarps, kGatherRingSmem));
+  return b > 0 ? b : 1;
+}
+
+void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks, const void* ring_map) {
   const dim3 grid(blocks), block(32 * kGatherWarps);
+  if (ring_map) {
+    const CUtensorMap& tm = *static_cast<const CUtensorMap*>(ring_map);
+    const size_t rs = kGatherRingSmem;
+    if (comp && adaptive) gather_ring_kernel<true, true><<<grid, block, rs, L.s>>>(a, tm);
+    else if (comp) gather_ring_kernel<true, false><<<grid, block, rs, L.s>>>(a, tm);
+    else if (adaptive) gather_ring_kernel<false, true><<<grid, block, rs, L.s>>>(a, tm);
+    else gather_ring_kernel<false, false><<<grid, block, rs, L.s>>>(a, tm);
+    PPB_LAUNCHED(*L.count);
+    return;
+  }
   const size_t sm = kGatherSmem;
   if (comp && adaptive) gather_kernel<true, true><<<grid, block, sm, L.s>>>(a);
   else if (comp) gather_kernel<true, false><<<grid, block, sm, L.s>>>(a);
   else if (adaptive) gather_kernel<false, true><<<grid, block, sm, L.s>>>(a);
   else gather_kernel<false, false><<<grid, block, sm, L.s>>>(a);
   PPB_LAUNCHED(*L.count);
+}
+
+bool record_ring_map(const float4* aos, int n, void* map128) {
+  const uint64_t cells = (uint64_t)n * n * n;
+  if (n <= 0 || cells >= (1ull << 31)) return false;
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  static Encode encode = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    looked = true;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<Encode>(fn);
+    cudaGetLastError();
+  }
+  if (!encode) return false;
+  // rows of 8 floats (one 32-byte record), one row per box
+  const cuuint64_t dims[2] = {8, cells};
+  const cuuint64_t strides[1] = {32};
+  const cuuint32_t box[2] = {8, 1};
+  const cuuint32_t estr[2] = {1, 1};
+  return encode(static_cast<CUtensorMap*>(map128), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float4*>(aos), dims,
+                strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 int shell_collapseq_blocks(int nsm) {

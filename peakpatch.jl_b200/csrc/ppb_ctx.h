@@ -102,7 +102,7 @@ struct Slot {
   DevBuf mr_in, mr_out, mr_aux, mr_rec;             // multi-resolution: staged inputs, outputs, records
   DevBuf mr_axis, mr_amp;                           // multi-resolution: tricubic axis tables, coarse amplitudes
   DevBuf pft;                                       // ppb_peak_find_tile: unpacked (i, j, k), ipp, filter
-  int gather_bps[2][2] = {{0, 0}, {0, 0}};          // gather blocks per SM by [comp][adaptive]
+  int gather_bps[2][2][2] = {};                      // gather blocks per SM by [comp][adaptive][ring]
   double rows_per_peak[2] = {0.0, 0.0};             // pool rows per peak seen last, by adaptive
   double walk_per_peak = 0.0;                       // collapse-walk steps per peak seen last
   ShellStats last_shell{};
@@ -177,6 +177,7 @@ struct Shared {
   std::atomic<int> use_graphs{1};
   std::atomic<int> autotune{1};
   std::atomic<int> fused_x{-1};   // PPB_OPT_FUSED_X
+  std::atomic<int> gather_ring{0};   // PPB_OPT_GATHER_RING
   std::atomic<int64_t> tune_min_peaks{16384};
   std::atomic<int> force_brick{-2};      // -2: tuner's choice
   std::atomic<int> force_collapse{0};    // 0: tuner's choice
@@ -216,7 +217,8 @@ struct ppb_ctx {
                   const std::function<void()>& pre = nullptr);
   // times the order bricks and collapse widths on one sub-batch and keeps the
   // fastest for the batch's tuning key (outputs are the same for every choice)
-  ppb::TuneEntry tune_shells(ppb::Slot& sl, const ppb::ShellArgs& b, bool comp, bool adaptive, int gblocks);
+  ppb::TuneEntry tune_shells(ppb::Slot& sl, const ppb::ShellArgs& b, bool comp, bool adaptive, int gblocks,
+                            const void* ring_map);
   // records the launches of `rec` on the slot's stream into the graph for
   // (site, key) of `graphs` and launches it; with graphs off, runs `rec`
   // directly.  A graph that launches cuFFT kernels must be kept in the map of

@@ -238,7 +238,7 @@ struct ShellArgs {
   int64_t npk;
   double* out;              // npk x RES_N
   PeakHdr* hdr;             // npk
-  int4* geo;                // npk: (m0_init, mrf, mlow_rf, mupp_rf)
+  int4* geo;                // 2 npk: (m0_init, mrf, mlow_rf, mupp_rf), (i, j, k of the peak cell, flags)
   const int32_t* r2lim;     // npk or null: per-peak shell list r^2 <= r2lim (> 0), else the whole list
   const int32_t* npcap;     // npk or null: per-peak cell count npart (the rmax2rs cap of RadialShell.jl:288-295)
   int32_t* mlim;            // npk: the peak's last finalised shell (written by the geometry kernel)
@@ -343,7 +343,14 @@ int shell_gather_blocks_per_sm(bool comp, bool adaptive);
 // per-peak geometry; with key/idx non-null also the spatial gather-order
 // keys (Morton index of the peak's 8^3 brick) and the identity permutation
 void launch_shell_geo(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx);
-void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks);
+// ring_map: null for the plain-load gather, else a CUtensorMap of the
+// records (record_ring_map) for the TMA-staged gather
+void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks,
+                         const void* ring_map = nullptr);
+int shell_gather_ring_blocks_per_sm(bool comp, bool adaptive);
+// the records of an n^3 grid (32 bytes per cell) as the tensor map the
+// TMA-staged gather reads: false when n^3 >= 2^31 or the driver refuses
+bool record_ring_map(const float4* aos, int n, void* map128);
 // collapse threads per peak picked by batch size and walk length
 int shell_collapse_width(int64_t npk, int nsm, double walk_steps_per_peak);
 // threads_per_peak 1, 2 or 4 (thread groups per peak), 8 (one thread per

@@ -92,6 +92,7 @@ class _TuneEntry(ctypes.Structure):
 # context options (include/ppb.h)
 OPT_GRAPHS, OPT_AUTOTUNE, OPT_TUNE_MIN_PEAKS, OPT_BRICK_SHIFT, OPT_COLLAPSE_THREADS = 1, 2, 3, 4, 5
 OPT_FUSED_X = 6
+OPT_GATHER_RING = 7
 OPT_GRAPH_LAUNCHES, OPT_GRAPH_INSTANTIATIONS, OPT_GRAPH_UPDATES = 16, 17, 18
 
 

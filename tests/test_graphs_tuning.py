@@ -89,3 +89,25 @@ def test_autotuner_times_every_candidate_and_keeps_the_records(tctx):
     assert len(tctx.tune_entries()) == 1
     assert ref.tobytes() == a.tobytes() == b.tobytes()
     _defaults(tctx)
+
+
+@pytest.mark.parametrize("plain", [False, True])
+def test_tma_staged_gather_gives_the_same_records(tctx, plain):
+    """Records gathered through the per-lane TMA rings (tile::gather4 copies
+    into shared memory) equal those of plain loads byte for byte: the same
+    cells in the same order reach the same sums.  Also for a multi-tile run
+    (the tile's own record array) and with the compensated sums off."""
+    _defaults(tctx)
+    cfg = tile_config()
+    try:
+        tctx.set_option(pp.OPT_GATHER_RING, 0)
+        a, _, _ = tctx.run_tile_arrays(cfg, 51, RF, plain=plain)
+        m0, _, _ = tctx.run_multitile_arrays(cfg, 5, RF, ntile=2, tiles=[(1, 1, 1), (2, 2, 1)])
+        tctx.set_option(pp.OPT_GATHER_RING, 1)
+        b, _, _ = tctx.run_tile_arrays(cfg, 51, RF, plain=plain)
+        m1, _, _ = tctx.run_multitile_arrays(cfg, 5, RF, ntile=2, tiles=[(1, 1, 1), (2, 2, 1)])
+        assert tctx.get_option(pp.OPT_GATHER_RING) == 1
+    finally:
+        tctx.set_option(pp.OPT_GATHER_RING, 0)
+    assert len(a) > 100 and a.tobytes() == b.tobytes()
+    assert m0.tobytes() == m1.tobytes()
