@@ -916,6 +916,8 @@ def _apply_options(ctx, args):
         ctx.set_option(pp.OPT_COLLAPSE_THREADS, args.collapse)
     if getattr(args, "gather_ring", -1) >= 0:
         ctx.set_option(pp.OPT_GATHER_RING, args.gather_ring)
+    if getattr(args, "collapse_order", -1) >= 0:
+        ctx.set_option(pp.OPT_COLLAPSE_ORDER, args.collapse_order)
 
 
 def _measured_peaks():
@@ -953,6 +955,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="default shell-stage choices, no autotuning")
     ap.add_argument("--gather-ring", type=int, default=-1,
                     help="1: gather records through TMA-staged shared-memory rings, 0: plain loads (default: library)")
+    ap.add_argument("--collapse-order", type=int, default=-1,
+                    help="1: collapse peaks by descending crossing shell, 0: in gather-list order (default: library)")
     ap.add_argument("--collapse", type=int, default=0,
                     help="fix the collapse kernel (PPB_OPT_COLLAPSE_THREADS: 1, 2, 4, 8; 0 the tuner's choice)")
     args = ap.parse_args()

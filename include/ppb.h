@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PPB_ABI_VERSION 3
+#define PPB_ABI_VERSION 4
 
 enum {
   PPB_OK = 0,
@@ -486,6 +486,12 @@ int32_t ppb_last_table_stats(ppb_ctx* ctx, float* ms, int64_t* steps);
  *  PPB_OPT_COLLAPSE_THREADS  fixes the collapse kernel: 1, 2 or 4 threads
  *                     per peak, 8 one thread per peak with lane work queues,
  *                     0 (default) the tuner's choice.
+ *  PPB_OPT_COLLAPSE_ORDER  the order the collapse kernels take the peaks
+ *                     in: 1 by descending crossing shell m0 (similar walks
+ *                     share a warp, the longest start first; a key kernel
+ *                     and a radix sort after the gather), 0 list order, -1
+ *                     (default) the tuner's choice (list order for batches
+ *                     below PPB_OPT_TUNE_MIN_PEAKS).  Same records.
  *  PPB_OPT_GATHER_RING  1: the shell gather stages its records through
  *                     per-lane shared-memory rings filled by TMA
  *                     (tile::gather4 bulk tensor copies, two stages, bounded
@@ -510,6 +516,7 @@ enum {
   PPB_OPT_COLLAPSE_THREADS = 5,
   PPB_OPT_FUSED_X = 6,
   PPB_OPT_GATHER_RING = 7,
+  PPB_OPT_COLLAPSE_ORDER = 8,
   PPB_OPT_GRAPH_LAUNCHES = 16,
   PPB_OPT_GRAPH_INSTANTIATIONS = 17,
   PPB_OPT_GRAPH_UPDATES = 18
@@ -528,6 +535,8 @@ typedef struct ppb_tune_entry {
   int64_t npk;                /* peaks of the batch the candidates were timed on */
   float gather_ms[5];         /* gather kernel: bricks of 4, 8, 16, 32 cells, list order */
   float collapse_ms[4];       /* collapse kernel: 1, 2, 4 threads per peak, lane work queues (8) */
+  int32_t collapse_order;     /* chosen: 1 = peaks by descending crossing shell, 0 = list order */
+  float collapse_ordered_ms[4];   /* the collapse widths with that order */
 } ppb_tune_entry;
 /* Copies up to `cap` entries; *n = the number of entries held. */
 int32_t ppb_tune_entries(ppb_ctx* ctx, ppb_tune_entry* out, int32_t cap, int32_t* n);

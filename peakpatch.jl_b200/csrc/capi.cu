@@ -310,6 +310,21 @@ static void shell_order(Slot& sl, ShellArgs& b, int brick_shift) {
   b.order = sl.oidx2.as<int32_t>();
 }
 
+// collapse order (after the gather, which it reuses the order buffers of):
+// the collapse kernels take the peaks by descending crossing shell
+static void collapse_order(Slot& sl, ShellArgs& b, bool on) {
+  b.corder = nullptr;
+  if (!on || b.npk < 2) return;
+  Launch L{sl.stream, &sl.launches};
+  launch_collapse_order_keys(L, b, sl.okey.as<uint32_t>(), sl.oidx.as<int32_t>());
+  size_t tb = sl.otmp.bytes;
+  PPB_CUDA(cub::DeviceRadixSort::SortPairs(sl.otmp.p, tb, sl.okey.as<uint32_t>(), sl.okey2.as<uint32_t>(),
+                                           sl.oidx.as<int32_t>(), sl.oidx2.as<int32_t>(), (int)b.npk, 0, 17,
+                                           sl.stream));
+  sl.launches++;
+  b.corder = sl.oidx2.as<int32_t>();
+}
+
 TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool adaptive, int gblocks,
                                 const void* rmap) {
   cudaStream_t s = sl.stream;
@@ -328,7 +343,7 @@ TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool ad
   // two rounds over the candidates, keeping each one's faster time, so that
   // the first launches' warm-up (caches, TLB) does not count against one
   for (int c = 0; c < 5; c++) te.gather_ms[c] = 1e30f;
-  for (int c = 0; c < 4; c++) te.collapse_ms[c] = 1e30f;
+  for (int c = 0; c < 4; c++) te.collapse_ms[c] = te.collapse_ordered_ms[c] = 1e30f;
   for (int round = 0; round < 2; round++) {
     for (int c = 0; c < 5; c++) {
       PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, kCtlBytes, s));
@@ -341,14 +356,18 @@ TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool ad
       PPB_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
       te.gather_ms[slot_of[c]] = std::min(te.gather_ms[slot_of[c]], ms);
     }
-    for (int c = 0; c < 4; c++) {
-      PPB_CUDA(cudaEventRecord(ev[0], s));
-      launch_shell_collapse(L, b, nsm, sl.walk_per_peak, widths[c]);
-      PPB_CUDA(cudaEventRecord(ev[1], s));
-      PPB_CUDA(cudaEventSynchronize(ev[1]));
-      float ms = 0.f;
-      PPB_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
-      te.collapse_ms[c] = std::min(te.collapse_ms[c], ms);
+    for (int o = 0; o < 2; o++) {   // list order, then by descending crossing shell
+      for (int c = 0; c < 4; c++) {
+        PPB_CUDA(cudaEventRecord(ev[0], s));
+        collapse_order(sl, b, o == 1);
+        launch_shell_collapse(L, b, nsm, sl.walk_per_peak, widths[c]);
+        PPB_CUDA(cudaEventRecord(ev[1], s));
+        PPB_CUDA(cudaEventSynchronize(ev[1]));
+        float ms = 0.f;
+        PPB_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+        float& t = o ? te.collapse_ordered_ms[c] : te.collapse_ms[c];
+        t = std::min(t, ms);
+      }
     }
   }
   // the default wins unless another candidate is at least 3 % faster
@@ -358,12 +377,24 @@ TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool ad
   if (!(te.gather_ms[bi] < 0.97f * te.gather_ms[1])) bi = 1;
   static const int shift_of[5] = {2, 3, 4, 5, -1};
   te.brick_shift = shift_of[bi];
+  // collapse: the size heuristic's width in list order unless another
+  // (width, order) is at least 3 % faster
   const int wd = shell_collapse_width(b.npk, nsm, sl.walk_per_peak);
   const int di = wd == 4 ? 2 : wd - 1;
-  int ci = di;
-  for (int c = 0; c < 4; c++)
-    if (te.collapse_ms[c] < te.collapse_ms[ci]) ci = c;
-  te.collapse_threads = te.collapse_ms[ci] < 0.97f * te.collapse_ms[di] ? widths[ci] : 0;
+  int ci = di, co = 0;
+  for (int o = 0; o < 2; o++)
+    for (int c = 0; c < 4; c++) {
+      const float t = o ? te.collapse_ordered_ms[c] : te.collapse_ms[c];
+      if (t < (co ? te.collapse_ordered_ms[ci] : te.collapse_ms[ci])) { ci = c; co = o; }
+    }
+  const float best = co ? te.collapse_ordered_ms[ci] : te.collapse_ms[ci];
+  if (best < 0.97f * te.collapse_ms[di]) {
+    te.collapse_threads = widths[ci];
+    te.collapse_order = co == 1;
+  } else {
+    te.collapse_threads = 0;
+    te.collapse_order = false;
+  }
   PPB_CUDA(cudaMemcpyAsync(sl.counters.p, sl.tune_save.p, 16 * 8, cudaMemcpyDeviceToDevice, s));
   PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, kCtlBytes, s));
   return te;
@@ -483,6 +514,8 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
       tune_now = false;
     }
     const int fb = sh.force_brick.load(), fc = sh.force_collapse.load();
+    const int fo = sh.collapse_order.load();
+    const bool corder_on = fo == 1 || (fo == -1 && te.collapse_order);
     if (fb != -2) te.brick_shift = fb;
     if (fc != 0) te.collapse_threads = fc;
     // the sub-batch as one graph: geometry, order, gather, collapse,
@@ -494,6 +527,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
       shell_order(sl, b, te.brick_shift);
       launch_shell_gather(L, b, comp, adaptive, gblocks, rmap);
       record_event(sl.shell_ev[1], stream);
+      collapse_order(sl, b, corder_on);
       launch_shell_collapse(L, b, nsm, sl.walk_per_peak, te.collapse_threads);
       record_event(sl.shell_ev[2], stream);
       launch_shell_zhalf(L, b);
@@ -1038,6 +1072,10 @@ int32_t ppb_set_option(ppb_ctx* ctx, int32_t option, int64_t value) {
       PPB_REQUIRE(value == 0 || value == 1, "PPB_OPT_GATHER_RING takes 0 or 1");
       ctx->sh.gather_ring.store((int)value);
       break;
+    case PPB_OPT_COLLAPSE_ORDER:
+      PPB_REQUIRE(value >= -1 && value <= 1, "PPB_OPT_COLLAPSE_ORDER takes -1, 0 or 1");
+      ctx->sh.collapse_order.store((int)value);
+      break;
     default:
       throw Error{PPB_ERR_INVALID, "unknown or read-only option"};
   }
@@ -1056,6 +1094,7 @@ int32_t ppb_get_option(ppb_ctx* ctx, int32_t option, int64_t* value) {
     case PPB_OPT_COLLAPSE_THREADS: *value = ctx->sh.force_collapse.load(); break;
     case PPB_OPT_FUSED_X: *value = ctx->sh.fused_x.load(); break;
     case PPB_OPT_GATHER_RING: *value = ctx->sh.gather_ring.load(); break;
+    case PPB_OPT_COLLAPSE_ORDER: *value = ctx->sh.collapse_order.load(); break;
     case PPB_OPT_GRAPH_LAUNCHES:
     case PPB_OPT_GRAPH_INSTANTIATIONS:
     case PPB_OPT_GRAPH_UPDATES: {
@@ -1091,6 +1130,8 @@ int32_t ppb_tune_entries(ppb_ctx* ctx, ppb_tune_entry* out, int32_t cap, int32_t
     e.npk = kv.second.npk;
     std::memcpy(e.gather_ms, kv.second.gather_ms, sizeof(e.gather_ms));
     std::memcpy(e.collapse_ms, kv.second.collapse_ms, sizeof(e.collapse_ms));
+    e.collapse_order = kv.second.collapse_order ? 1 : 0;
+    std::memcpy(e.collapse_ordered_ms, kv.second.collapse_ordered_ms, sizeof(e.collapse_ordered_ms));
     out[i++] = e;
   }
   return PPB_OK;

@@ -1355,17 +1355,33 @@ __device__ void collapse_group(const ShellArgs& a, int64_t p, int q, int qbase, 
   collapse_finish(a, R, ZZon, m0, zvir1, zvir1p, prev, last, lastFh, grf, out);
 }
 
+// the peak of collapse slot i: i itself, or its place in the collapse order
+__device__ __forceinline__ int64_t collapse_peak(const ShellArgs& a, int64_t i) {
+  return a.corder ? (int64_t)__ldg(a.corder + i) : i;
+}
+
 __global__ void __launch_bounds__(128) collapse1_kernel(ShellArgs a) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < a.npk) collapse_one(a, p);
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < a.npk) collapse_one(a, collapse_peak(a, i));
 }
 
 template <int QT>
 __global__ void __launch_bounds__(128) collapse_kernel(ShellArgs a) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t p = t / QT;
+  const int64_t i = t / QT;
   const int lane = threadIdx.x & 31, q = lane & (QT - 1), qbase = lane & ~(QT - 1);
-  if (p < a.npk) collapse_group<QT>(a, p, q, qbase, ((1u << QT) - 1u) << qbase);
+  if (i < a.npk) collapse_group<QT>(a, collapse_peak(a, i), q, qbase, ((1u << QT) - 1u) << qbase);
+}
+
+// collapse order key (thread per peak): peaks that reach the walk by
+// descending crossing shell m0 — the longest windows and walks first, and
+// peaks of similar walks side by side in a warp — the rest last
+__global__ void corder_kernel(ShellArgs a, uint32_t* key, int32_t* idx) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.npk) return;
+  const PeakHdr h = a.hdr[p];
+  key[p] = h.status == HS_OK ? 0xffffu - (uint32_t)min(max(h.m0, 0), 0xffff) : 0x1ffffu;
+  idx[p] = (int32_t)p;
 }
 
 // One thread per peak with a work queue per lane: a lane takes its next peak
@@ -1403,7 +1419,7 @@ __global__ void __launch_bounds__(128) collapseq_kernel(ShellArgs a) {
         if (q >= a.npk) {
           retired = true;
         } else {
-          p = q;
+          p = collapse_peak(a, q);
           const PeakHdr h = a.hdr[p];
           if (h.status != HS_OK) {
             write_no_collapse(a.out + p * RES_N);   // state stays 0: the lane takes another peak
@@ -1606,6 +1622,13 @@ int shell_gather_blocks_per_sm(bool comp, bool adaptive) {
   int b = 0;
   PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, 32 * kGatherWarps, kGatherSmem));
   return b > 0 ? b : 1;
+}
+
+void launch_collapse_order_keys(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx) {
+  const int64_t blocks = (a.npk + 127) / 128;
+  if (blocks == 0) return;
+  corder_kernel<<<(unsigned)blocks, 128, 0, L.s>>>(a, key, idx);
+  PPB_LAUNCHED(*L.count);
 }
 
 void launch_shell_geo(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx) {

@@ -68,6 +68,8 @@ struct TuneEntry {
   int64_t npk = 0;            // peaks of the batch it was measured on
   float gather_ms[5] = {};    // bricks of 4, 8, 16, 32 cells and list order
   float collapse_ms[4] = {};  // 1, 2 and 4 threads per peak, lane queues
+  bool collapse_order = false;            // peaks by descending crossing shell
+  float collapse_ordered_ms[4] = {};      // the same widths with that order
 };
 
 struct ShellStats {
@@ -178,6 +180,7 @@ struct Shared {
   std::atomic<int> autotune{1};
   std::atomic<int> fused_x{-1};   // PPB_OPT_FUSED_X
   std::atomic<int> gather_ring{0};   // PPB_OPT_GATHER_RING
+  std::atomic<int> collapse_order{-1};   // PPB_OPT_COLLAPSE_ORDER (-1: tuner's choice)
   std::atomic<int64_t> tune_min_peaks{16384};
   std::atomic<int> force_brick{-2};      // -2: tuner's choice
   std::atomic<int> force_collapse{0};    // 0: tuner's choice

@@ -238,6 +238,7 @@ struct ShellArgs {
   int64_t npk;
   double* out;              // npk x RES_N
   PeakHdr* hdr;             // npk
+  const int32_t* corder;    // npk or null: the order the collapse kernels take the peaks in
   int4* geo;                // 2 npk: (m0_init, mrf, mlow_rf, mupp_rf), (i, j, k of the peak cell, flags)
   const int32_t* r2lim;     // npk or null: per-peak shell list r^2 <= r2lim (> 0), else the whole list
   const int32_t* npcap;     // npk or null: per-peak cell count npart (the rmax2rs cap of RadialShell.jl:288-295)
@@ -343,6 +344,8 @@ int shell_gather_blocks_per_sm(bool comp, bool adaptive);
 // per-peak geometry; with key/idx non-null also the spatial gather-order
 // keys (Morton index of the peak's 8^3 brick) and the identity permutation
 void launch_shell_geo(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx);
+// keys (17 bits) and identity indices of the collapse order
+void launch_collapse_order_keys(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx);
 // ring_map: null for the plain-load gather, else a CUtensorMap of the
 // records (record_ring_map) for the TMA-staged gather
 void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive, int blocks,

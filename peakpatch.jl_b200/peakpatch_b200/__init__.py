@@ -86,13 +86,15 @@ class _TuneEntry(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int32), ("nshell", ctypes.c_int32), ("comp", ctypes.c_int32),
                 ("adaptive", ctypes.c_int32), ("limited", ctypes.c_int32), ("brick_shift", ctypes.c_int32),
                 ("collapse_threads", ctypes.c_int32), ("long_walk", ctypes.c_int32), ("npk", ctypes.c_int64),
-                ("gather_ms", ctypes.c_float * 5), ("collapse_ms", ctypes.c_float * 4)]
+                ("gather_ms", ctypes.c_float * 5), ("collapse_ms", ctypes.c_float * 4),
+                ("collapse_order", ctypes.c_int32), ("collapse_ordered_ms", ctypes.c_float * 4)]
 
 
 # context options (include/ppb.h)
 OPT_GRAPHS, OPT_AUTOTUNE, OPT_TUNE_MIN_PEAKS, OPT_BRICK_SHIFT, OPT_COLLAPSE_THREADS = 1, 2, 3, 4, 5
 OPT_FUSED_X = 6
 OPT_GATHER_RING = 7
+OPT_COLLAPSE_ORDER = 8
 OPT_GRAPH_LAUNCHES, OPT_GRAPH_INSTANTIATIONS, OPT_GRAPH_UPDATES = 16, 17, 18
 
 
@@ -503,7 +505,10 @@ class Context:
                         "collapse_threads": e.collapse_threads, "npk": e.npk,
                         "gather_ms": dict(zip(("brick4", "brick8", "brick16", "brick32", "list"),
                                               [round(x, 4) for x in e.gather_ms])),
-                        "collapse_ms": dict(zip(("w1", "w2", "w4", "queue"), [round(x, 4) for x in e.collapse_ms]))})
+                        "collapse_ms": dict(zip(("w1", "w2", "w4", "queue"), [round(x, 4) for x in e.collapse_ms])),
+                        "collapse_order": bool(e.collapse_order),
+                        "collapse_ordered_ms": dict(zip(("w1", "w2", "w4", "queue"),
+                                                        [round(x, 4) for x in e.collapse_ordered_ms]))})
         return out
 
     def stage_ms(self):

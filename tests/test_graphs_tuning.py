@@ -29,6 +29,7 @@ def _defaults(c):
     c.set_option(pp.OPT_BRICK_SHIFT, -2)
     c.set_option(pp.OPT_COLLAPSE_THREADS, 0)
     c.set_option(pp.OPT_TUNE_MIN_PEAKS, 16384)
+    c.set_option(pp.OPT_COLLAPSE_ORDER, -1)
 
 
 def test_graphs_on_and_off_give_the_same_records(tctx):
@@ -84,6 +85,7 @@ def test_autotuner_times_every_candidate_and_keeps_the_records(tctx):
     e = ents[0]
     assert e["n"] == cfg.n and e["comp"] and e["adaptive"] and not e["limited"] and e["npk"] == npk
     assert all(v > 0 for v in e["gather_ms"].values()) and all(v > 0 for v in e["collapse_ms"].values())
+    assert all(v > 0 for v in e["collapse_ordered_ms"].values())
     assert e["brick"] in (0, 4, 8, 16, 32) and e["collapse_threads"] in (0, 1, 2, 4, 8)
     b, _, _ = tctx.run_tile_arrays(cfg, 43, RF)   # runs with the tuned choice, no new entry
     assert len(tctx.tune_entries()) == 1
@@ -111,3 +113,23 @@ def test_tma_staged_gather_gives_the_same_records(tctx, plain):
         tctx.set_option(pp.OPT_GATHER_RING, 0)
     assert len(a) > 100 and a.tobytes() == b.tobytes()
     assert m0.tobytes() == m1.tobytes()
+
+
+def test_collapse_order_gives_the_same_records(tctx):
+    """The collapse kernels taking the peaks by descending crossing shell
+    (PPB_OPT_COLLAPSE_ORDER) give the records of list order, byte for byte,
+    under every collapse width."""
+    _defaults(tctx)
+    cfg = tile_config()
+    try:
+        tctx.set_option(pp.OPT_COLLAPSE_ORDER, 0)
+        ref, _, _ = tctx.run_tile_arrays(cfg, 61, RF)
+        tctx.set_option(pp.OPT_COLLAPSE_ORDER, 1)
+        for w in (0, 1, 2, 4, 8):
+            tctx.set_option(pp.OPT_COLLAPSE_THREADS, w)
+            g, _, _ = tctx.run_tile_arrays(cfg, 61, RF)
+            assert g.tobytes() == ref.tobytes(), w
+    finally:
+        tctx.set_option(pp.OPT_COLLAPSE_ORDER, -1)
+        tctx.set_option(pp.OPT_COLLAPSE_THREADS, 0)
+    assert len(ref) > 100

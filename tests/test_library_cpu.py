@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert pp.load_library().ppb_abi_version() == 3
+    assert pp.load_library().ppb_abi_version() == 4
 
 
 def test_tile_params_layout_matches_the_header():
@@ -40,9 +40,10 @@ def test_tile_params_layout_matches_the_header():
 
 
 def test_tune_entry_layout_and_option_entry_points():
-    # ppb_tune_entry: 8 int32, an int64, 5 + 4 floats (padded to 8 bytes)
-    assert ctypes.sizeof(pp._TuneEntry) == 8 * 4 + 8 + 9 * 4 + 4
+    # ppb_tune_entry: 8 int32, an int64, 5 + 4 floats, an int32, 4 floats
+    assert ctypes.sizeof(pp._TuneEntry) == 8 * 4 + 8 + 9 * 4 + 4 + 4 * 4
     assert pp._TuneEntry.gather_ms.offset == 40
+    assert pp._TuneEntry.collapse_order.offset == 76 and pp._TuneEntry.collapse_ordered_ms.offset == 80
     L = pp.load_library()
     v = ctypes.c_int64()
     n = ctypes.c_int32()
