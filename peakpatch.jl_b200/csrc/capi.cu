@@ -59,7 +59,7 @@ void Slot::release_buffers() {
   tiles.clear();
   tile_lru.clear();
   for (DevBuf* b : {&filt_Rf, &filt_ir2, &filt_np, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
-                    &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &mr_in, &mr_out, &mr_aux,
+                    &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &anchors, &mr_in, &mr_out, &mr_aux,
                     &mr_rec, &mr_axis, &mr_amp, &pft})
     b->release();
   tune_save.release();
@@ -75,7 +75,7 @@ size_t Slot::bytes_held() const {
 size_t Slot::shell_bytes() const {
   size_t b = 0;
   for (const DevBuf* d : {&filt_Rf, &filt_ir2, &filt_np, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool,
-                          &okey, &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &mr_in,
+                          &okey, &okey2, &oidx, &oidx2, &otmp, &tcen, &tcount, &t_aos, &t_lapd, &mlim, &anchors, &mr_in,
                           &mr_out, &mr_aux, &mr_rec, &mr_axis, &mr_amp, &pft})
     b += d->bytes;
   if (iso) b += iso->bytes();
@@ -222,6 +222,8 @@ ShellArgs ppb_ctx::shell_args(Slot& sl, ShellTable& shells, int n, double alatt,
   a.grp_c = shells.d_grp_c.as<int32_t>();
   a.ck_s = shells.d_ck_s.as<int32_t>();
   a.ck_n = shells.d_ck_n.as<int32_t>();
+  a.ck_d = shells.d_ck_d.as<int32_t>();
+  a.nck = (int)shells.ck_s.size();
   a.sh_c0 = shells.d_sh_c0.as<int32_t>();
   a.sh_nc = shells.d_sh_nc.as<int32_t>();
   a.ngroups = shells.ngroups;
@@ -340,6 +342,7 @@ TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool ad
   static const int slot_of[5] = {1, 0, 2, 3, 4};
   static const int widths[4] = {1, 2, 4, 8};
   ShellArgs b = b0;
+  if (comp) launch_shell_anchors(L, b);
   // two rounds over the candidates, keeping each one's faster time, so that
   // the first launches' warm-up (caches, TLB) does not count against one
   for (int c = 0; c < 5; c++) te.gather_ms[c] = 1e30f;
@@ -428,6 +431,8 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
   grow(sl.hdr, std::max<size_t>(1, (size_t)a.npk) * sizeof(PeakHdr));
   grow(sl.geo, std::max<size_t>(1, (size_t)a.npk) * 2 * sizeof(int4));
   grow(sl.mlim, std::max<size_t>(1, (size_t)a.npk) * sizeof(int32_t));
+  sl.anchors.ensure(std::max<size_t>(1, (size_t)a.nck) * kAnchorStride * sizeof(float2));
+  a.ck_K = sl.anchors.as<float2>();
   PPB_CUDA(cudaMemsetAsync(sl.counters.p, 0, 16 * 8, stream));
   // profile pool: sized from the rows per peak of the previous call; peaks
   // run in batches that fit the pool budget, and a batch whose rows overflow
@@ -524,6 +529,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
       if (first && pre) pre();
       PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, kCtlBytes, stream));
       record_event(sl.shell_ev[0], stream);
+      if (comp) launch_shell_anchors(L, b);
       shell_order(sl, b, te.brick_shift);
       launch_shell_gather(L, b, comp, adaptive, gblocks, rmap);
       record_event(sl.shell_ev[1], stream);

@@ -101,7 +101,7 @@ void build_shell_table(ShellTable& st, int nhunt) {
   for (int m = 1; m <= st.nshell; m++) st.rad5[m] = std::pow(st.rad[m], 5);
   // gather schedule (shells 2..mmax; shell m is distinct value m-1)
   st.grp_a.clear(); st.grp_b.clear(); st.grp_c.clear();
-  st.ck_s.clear(); st.ck_n.clear();
+  st.ck_s.clear(); st.ck_n.clear(); st.ck_d.clear();
   st.ch_max = 0;
   st.sh_c0.assign(st.nshell + 1, 0);
   st.sh_nc.assign(st.nshell + 1, 0);
@@ -130,6 +130,12 @@ void build_shell_table(ShellTable& st, int nhunt) {
       const int a = (int)((int64_t)cnt * c / nck), b = (int)((int64_t)cnt * (c + 1) / nck);
       st.ck_s.push_back(s0 + a);
       st.ck_n.push_back(b - a);
+      int dm = 0;
+      for (int i = s0 + a; i < s0 + b; i++) {
+        const int w = st.cell8[i];
+        dm = std::max({dm, std::abs((w << 24) >> 24), std::abs((w << 16) >> 24), std::abs((w << 8) >> 24)});
+      }
+      st.ck_d.push_back(dm);
       st.ch_max = std::max(st.ch_max, b - a);
     }
     in_group += nck;
@@ -215,6 +221,7 @@ void upload_shell_table(ShellTable& st, cudaStream_t s) {
   up(st.d_grp_c, st.grp_c.data(), st.grp_c.size() * 4);
   up(st.d_ck_s, st.ck_s.data(), st.ck_s.size() * 4);
   up(st.d_ck_n, st.ck_n.data(), st.ck_n.size() * 4);
+  up(st.d_ck_d, st.ck_d.data(), st.ck_d.size() * 4);
   up(st.d_sh_c0, st.sh_c0.data(), st.sh_c0.size() * 4);
   up(st.d_sh_nc, st.sh_nc.data(), st.sh_nc.size() * 4);
   up(st.d_ck_p, st.ck_p.data(), st.ck_p.size() * 4);

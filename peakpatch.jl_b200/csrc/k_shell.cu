@@ -16,9 +16,9 @@
 //    16-byte load, four 32-byte records in flight per lane, each one 256-bit
 //    load), lane l then finalises shell l of the group from the
 //    chunk partials, and the cumulative profile Fbar comes from a warp scan
-//    of r^3 Fbar.  Sums are compensated single precision (anchored Fast2Sum:
-//    each rounding error is captured exactly and summed apart) on the
-//    optimised path and double precision on the plain path; in both the
+//    of r^3 Fbar.  Sums are compensated single precision (anchored Fast2Sum
+//    with anchors per chunk: each rounding error is captured exactly and
+//    summed apart) on the optimised path and double precision on the plain path; in both the
 //    addends are the single-precision products the reference forms (Float32
 //    field times Int32 offset).
 //    Adaptive truncation (optimised path): the warp stops gathering once
@@ -74,9 +74,9 @@ template <> struct Acc<false> {      // double precision (the reference's Float6
 };
 
 // Compensated single precision (optimised path): NP packed FP32x2 sums,
-// anchored.  Component i starts at a power of two K_i (per warp, in shared
-// memory) with |x| <= K_i / (2 CH) for each of its addends x, CH the longest
-// chunk, so its running sum s stays in [K_i/2, 3K_i/2]: |s| >= |x| at every
+// anchored.  Component i starts at a power of two K_i (per chunk, from
+// anchor_kernel) with |x| <= K_i / (2 cnt) for each of its addends x, cnt the
+// chunk's cells, so its running sum s stays in [K_i/2, 3K_i/2]: |s| >= |x| at every
 // addition, and Fast2Sum (t = s + x, e = x - (t - s)) gives the exact
 // rounding error e of t in three operations; c collects the e.  The chunk's
 // sum is (s - K_i) + c, where s - K_i is exact (Sterbenz).  One FP32x2
@@ -86,18 +86,18 @@ __device__ __forceinline__ float2 fsub2(float2 a, float2 b) {   // a - b, rounde
 }
 template <int NP> struct AccH {
   float2 s[NP], c[NP];
-  const float2* K;   // the anchors (shared memory)
+  const float2* K;   // the chunk's anchors (anchor_kernel), 32 float2 apart
   __device__ __forceinline__ void zero() {
 #pragma unroll
-    for (int i = 0; i < NP; i++) { s[i] = K[i]; c[i] = make_float2(0.f, 0.f); }
+    for (int i = 0; i < NP; i++) { s[i] = K[32 * i]; c[i] = make_float2(0.f, 0.f); }
   }
   __device__ __forceinline__ void add(int i, float2 x) {
     const float2 t = __fadd2_rn(s[i], x);
     c[i] = __fadd2_rn(c[i], fsub2(x, fsub2(t, s[i])));
     s[i] = t;
   }
-  __device__ __forceinline__ double X(int i) const { return (double)__fsub_rn(s[i].x, K[i].x) + (double)c[i].x; }
-  __device__ __forceinline__ double Y(int i) const { return (double)__fsub_rn(s[i].y, K[i].y) + (double)c[i].y; }
+  __device__ __forceinline__ double X(int i) const { return (double)__fsub_rn(s[i].x, K[32 * i].x) + (double)c[i].x; }
+  __device__ __forceinline__ double Y(int i) const { return (double)__fsub_rn(s[i].y, K[32 * i].y) + (double)c[i].y; }
 };
 
 // smallest power of two >= v (v >= 0 finite; 0 stays 0)
@@ -241,36 +241,43 @@ __device__ __forceinline__ void unpack_cell(int w, int& di, int& dj, int& dk) {
   dk = (w << 8) >> 24;
 }
 
-// shared memory of one gather warp, in doubles: the chunk partials
-constexpr int GATHER_WARP_DOUBLES = (NACC + 1) * 32 + 12;   // + the anchors (12 float2)
+// shared memory of one gather warp, in doubles: the chunk partials, then
+// each lane's copy of its chunk's anchors (component i of lane l at i 32 + l)
+constexpr int GATHER_WARP_DOUBLES = (NACC + 1) * 32 + kAnchorStride * 32;
 
-// The anchors of one warp's compensated sums from the field maxima the pack
-// kernel left after the records.  K = 2^ceil(log2(2 CH M)) with M the
-// largest magnitude of the component's addends (a field maximum, times
-// d_max for the products with an offset), so |x| <= K / (2 CH).
-__device__ __forceinline__ void set_anchors(const ShellArgs& a, float2* K) {
-  const int lane = threadIdx.x & 31;
-  float M[7];   // delta, psi x, y, z, psi2 x, y, z
+// The anchors of the compensated sums, per chunk (thread per chunk of the
+// schedule, before the gather): K = 2^ceil(log2(2 cnt M (1 + 2^-10))) with
+// cnt the chunk's cells and M the largest magnitude of the sum's addends — a
+// field maximum (the pack kernel leaves them after the records), times the
+// chunk's largest offset component for the products with an offset — so
+// that |x| <= K / (2 cnt) for every addend of the chunk.  A smaller anchor
+// leaves a smaller rounding error in the compensation term, so each chunk
+// gets its own.  kAnchorStride float2 per chunk (11 used).
+__global__ void anchor_kernel(ShellArgs a) {
+  // the seven field maxima (delta, psi x, y, z, psi2 x, y, z) from their
+  // slots, reduced by the block (non-negative floats order as their bits)
+  __shared__ unsigned mx[7];
+  if (threadIdx.x < 7) mx[threadIdx.x] = 0u;
+  __syncthreads();
+  for (int i = threadIdx.x; i < 7 * kFmaxSlots; i += blockDim.x) atomicMax(&mx[i / kFmaxSlots], __ldg(a.fmax + i));
+  __syncthreads();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.nck) return;
+  float M[7];
 #pragma unroll
-  for (int f = 0; f < 7; f++) {
-    float m = 0.f;
-    for (int q = lane; q < kFmaxSlots; q += 32) m = fmaxf(m, __uint_as_float(__ldg(a.fmax + f * kFmaxSlots + q)));
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
-    M[f] = m;
-  }
-  if (lane == 0) {
-    const float w = 2.0f * (float)a.ch_max, wd = w * (float)a.d_max;
-    auto k = [](float m, float scale) { return pow2_ceil(m * scale); };
-    K[0] = make_float2(k(M[0], w), k(M[3], wd));
-    K[1] = make_float2(k(M[1], w), k(M[2], w));
-    K[2] = make_float2(k(M[3], w), k(M[4], w));
-    K[3] = make_float2(k(M[5], w), k(M[6], w));
-    for (int i = 4; i < 7; i++) K[i] = make_float2(k(M[0], wd), k(M[0], wd));
-    for (int i = 7; i < 10; i++) K[i] = make_float2(k(M[1], wd), k(M[2], wd));
-    K[10] = make_float2(k(M[3], wd), k(M[3], wd));
-  }
-  __syncwarp();
+  for (int f = 0; f < 7; f++) M[f] = __uint_as_float(mx[f]);
+  const float w = 2.0f * (float)__ldg(a.ck_n + c) * (1.0f + 1.0f / 1024.0f);
+  const float wd = w * (float)__ldg(a.ck_d + c);
+  auto k = [](float m, float scale) { return pow2_ceil(m * scale); };
+  float2* K = a.ck_K + (size_t)c * kAnchorStride;
+  K[0] = make_float2(k(M[0], w), k(M[3], wd));
+  K[1] = make_float2(k(M[1], w), k(M[2], w));
+  K[2] = make_float2(k(M[3], w), k(M[4], w));
+  K[3] = make_float2(k(M[5], w), k(M[6], w));
+  for (int i = 4; i < 7; i++) K[i] = make_float2(k(M[0], wd), k(M[0], wd));
+  for (int i = 7; i < 10; i++) K[i] = make_float2(k(M[1], wd), k(M[2], wd));
+  K[10] = make_float2(k(M[3], wd), k(M[3], wd));
+  K[11] = make_float2(0.f, 0.f);
 }
 
 // One cell's 32-byte record with one 256-bit load (Blackwell's
@@ -533,7 +540,21 @@ template <bool COMP, bool RING>
 __device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, int64_t lin, bool inside, int pi,
                                          int pj, int pk, double* part, int col, Ring* ring) {
   int nsh;
-  const float2* K = reinterpret_cast<const float2*>(part + (NACC + 1) * 32);
+  // the chunk's anchors into this lane's slot (three 32-byte loads), read
+  // from there at the chunk's start and end
+  float2* K = reinterpret_cast<float2*>(part + (NACC + 1) * 32) + col;
+  if constexpr (COMP) {
+    const float4* src = reinterpret_cast<const float4*>(a.ck_K + (size_t)ck * kAnchorStride);
+    float4 u[6];
+    ldg_record(src, u[0], u[1]);
+    ldg_record(src + 2, u[2], u[3]);
+    ldg_record(src + 4, u[4], u[5]);
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      K[32 * (2 * q)] = make_float2(u[q].x, u[q].y);
+      if (2 * q + 1 < 11) K[32 * (2 * q + 1)] = make_float2(u[q].z, u[q].w);
+    }
+  }
   if constexpr (COMP) {
     AccH<11> A;
     A.K = K;
@@ -810,7 +831,6 @@ __global__ void __launch_bounds__(32 * kGatherWarps, PPB_GATHER_MINB) gather_ker
   const int64_t slot = (int64_t)blockIdx.x * kGatherWarps + wib;
   double* stage = a.stage + slot * a.stage_stride;
   double* part = gsm + (size_t)wib * GATHER_WARP_DOUBLES;
-  if (COMP) set_anchors(a, reinterpret_cast<float2*>(part + (NACC + 1) * 32));
   while (true) {
     int q = 0;
     if (lane == 0) q = atomicAdd(a.queue, 1);
@@ -844,7 +864,6 @@ __global__ void __launch_bounds__(32 * kGatherWarps, PPB_GATHER_MINB)
   R.tm = reinterpret_cast<uint64_t>(&tm);
   R.counters = a.counters;
   ring_init(R);
-  if (COMP) set_anchors(a, reinterpret_cast<float2*>(part + (NACC + 1) * 32));
   while (true) {
     int q = 0;
     if (lane == 0) q = atomicAdd(a.queue, 1);
@@ -1622,6 +1641,12 @@ int shell_gather_blocks_per_sm(bool comp, bool adaptive) {
   int b = 0;
   PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, 32 * kGatherWarps, kGatherSmem));
   return b > 0 ? b : 1;
+}
+
+void launch_shell_anchors(Launch L, const ShellArgs& a) {
+  if (a.nck == 0) return;
+  anchor_kernel<<<(a.nck + 127) / 128, 128, 0, L.s>>>(a);
+  PPB_LAUNCHED(*L.count);
 }
 
 void launch_collapse_order_keys(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx) {

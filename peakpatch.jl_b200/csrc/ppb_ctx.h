@@ -97,7 +97,7 @@ struct Slot {
   int max_tiles = 4;                                // sizes kept resident at most
   DevBuf filt_Rf, filt_ir2, filt_np;                // filter bank of the run
   DevBuf g_a, g_D, g_f, chi;                        // growth / chi tables of the run
-  DevBuf stage, counters, ctl, hdr, geo, mlim, pool;   // shell stage
+  DevBuf stage, counters, ctl, hdr, geo, mlim, pool, anchors;   // shell stage
   DevBuf okey, okey2, oidx, oidx2, otmp;            // spatial gather order
   DevBuf tcen, tcount, t_aos, t_lapd;               // multi-tile: centres, peaks per tile, tile fields
   std::unique_ptr<IsoRes> iso;                      // multi-resolution: isolated convolution

@@ -107,7 +107,7 @@ struct ShellTable {
   // (one chunk per lane) that end on a shell boundary.  Group g covers shells
   // [grp_a[g], grp_b[g]] and chunks [grp_c[g], grp_c[g+1]); chunk c holds
   // ck_n[c] cells from ck_s[c]; shell m's chunks start at sh_c0[m] (sh_nc[m]).
-  std::vector<int32_t> grp_a, grp_b, grp_c, ck_s, ck_n, sh_c0, sh_nc;
+  std::vector<int32_t> grp_a, grp_b, grp_c, ck_s, ck_n, ck_d, sh_c0, sh_nc;
   int ngroups = 0;
   int ch_max = 0;                     // longest chunk (cells)
   // cell offsets packed one per 32-bit word: bytes 0..2 = di, dj, dk as
@@ -119,7 +119,7 @@ struct ShellTable {
   // starts at ck_cells[4 ck_p[c]]
   std::vector<int32_t> ck_p, ck_cells;
   DevBuf d_cell8, d_start, d_count, d_r2m, d_rad, d_wlo, d_whi, d_woff, d_wts, d_w1, d_need, d_rad5;
-  DevBuf d_grp_a, d_grp_b, d_grp_c, d_ck_s, d_ck_n, d_sh_c0, d_sh_nc, d_ck_p, d_ck_cells;
+  DevBuf d_grp_a, d_grp_b, d_grp_c, d_ck_s, d_ck_n, d_ck_d, d_sh_c0, d_sh_nc, d_ck_p, d_ck_cells;
 };
 void build_shell_table(ShellTable& st, int nhunt);
 double hRinteg(double u0, double u12);
@@ -231,6 +231,9 @@ struct ShellArgs {
   int64_t npart;            // cells used (full list here)
   int ch_max;               // longest chunk of the schedule (cells)
   int d_max;                // largest |offset component| of the list (nhunt)
+  int nck;                  // chunks of the schedule
+  const int32_t* ck_d;      // per chunk: largest |offset component| of its cells
+  float2* ck_K;             // per chunk: the compensated sums' anchors (kAnchorStride float2)
   const unsigned* fmax;     // the field maxima after the records (pack_fmax)
   DevTable tab;
   const double* akk;        // 1101-entry SPH kernel table
@@ -344,6 +347,9 @@ int shell_gather_blocks_per_sm(bool comp, bool adaptive);
 // per-peak geometry; with key/idx non-null also the spatial gather-order
 // keys (Morton index of the peak's 8^3 brick) and the identity permutation
 void launch_shell_geo(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx);
+// the compensated sums' anchors of every chunk (a.ck_K) from the field maxima
+void launch_shell_anchors(Launch L, const ShellArgs& a);
+constexpr int kAnchorStride = 12;   // float2 per chunk in ShellArgs::ck_K
 // keys (17 bits) and identity indices of the collapse order
 void launch_collapse_order_keys(Launch L, const ShellArgs& a, uint32_t* key, int32_t* idx);
 // ring_map: null for the plain-load gather, else a CUtensorMap of the
