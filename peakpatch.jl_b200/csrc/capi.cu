@@ -230,8 +230,6 @@ ShellArgs ppb_ctx::shell_args(Slot& sl, ShellTable& shells, int n, double alatt,
   a.nshell = shells.nshell;
   a.mmax = std::max(shells.nshell - 1, 1);
   a.npart = shells.ncells;
-  a.ch_max = shells.ch_max;
-  a.d_max = shells.nhunt;
   a.fmax = pack_fmax(const_cast<float4*>(aos), n);
   a.tab = sh.dtab;
   a.akk = sh.akk.as<double>();

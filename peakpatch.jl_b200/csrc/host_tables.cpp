@@ -102,7 +102,6 @@ void build_shell_table(ShellTable& st, int nhunt) {
   // gather schedule (shells 2..mmax; shell m is distinct value m-1)
   st.grp_a.clear(); st.grp_b.clear(); st.grp_c.clear();
   st.ck_s.clear(); st.ck_n.clear(); st.ck_d.clear();
-  st.ch_max = 0;
   st.sh_c0.assign(st.nshell + 1, 0);
   st.sh_nc.assign(st.nshell + 1, 0);
   int in_group = 0;
@@ -136,7 +135,6 @@ void build_shell_table(ShellTable& st, int nhunt) {
         dm = std::max({dm, std::abs((w << 24) >> 24), std::abs((w << 16) >> 24), std::abs((w << 8) >> 24)});
       }
       st.ck_d.push_back(dm);
-      st.ch_max = std::max(st.ch_max, b - a);
     }
     in_group += nck;
     st.grp_b.back() = m;

@@ -109,7 +109,6 @@ struct ShellTable {
   // ck_n[c] cells from ck_s[c]; shell m's chunks start at sh_c0[m] (sh_nc[m]).
   std::vector<int32_t> grp_a, grp_b, grp_c, ck_s, ck_n, ck_d, sh_c0, sh_nc;
   int ngroups = 0;
-  int ch_max = 0;                     // longest chunk (cells)
   // cell offsets packed one per 32-bit word: bytes 0..2 = di, dj, dk as
   // signed 8-bit values (|d| <= nhunt <= 64)
   std::vector<int32_t> cell8;
@@ -229,8 +228,6 @@ struct ShellArgs {
   int nshell;               // distinct r2 values in the list (incl. 0)
   int mmax;                 // finalised shells: nshell - 1
   int64_t npart;            // cells used (full list here)
-  int ch_max;               // longest chunk of the schedule (cells)
-  int d_max;                // largest |offset component| of the list (nhunt)
   int nck;                  // chunks of the schedule
   const int32_t* ck_d;      // per chunk: largest |offset component| of its cells
   float2* ck_K;             // per chunk: the compensated sums' anchors (kAnchorStride float2)
