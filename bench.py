@@ -152,11 +152,11 @@ class ClockSampler:
 # CPU baseline: the oracle (a C++/OpenMP restatement of the reference's CPU
 # run_tile) on a bounded sample of the same workload
 # ---------------------------------------------------------------------------
-def config_dict(n: int, path: str = "optimised") -> dict:
+def config_dict(n: int, world: int, path: str = "optimised") -> dict:
     """The workload's config, the same in both arms."""
     return {"workload": workload_name(n), "nmesh": n, "boxsize": BOX_PER_CELL * n, "filters": 20, "nbuff": 32,
             "ilpt": 2, "ioutshear": 1, "seed": SEED, "path": path,
-            "l2": "inputs larger than L2 (each field 226 MB at 384^3)"}
+            "l2": "inputs larger than L2 (each field 226 MB at 384^3)", "parallelism": f"replicas x{world}"}
 
 
 class CpuTile:
@@ -280,7 +280,7 @@ def run_reference(args, dist: Dist):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.fmean(walls),
             "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 shell sums", "data": "synthetic",
-            "config": config_dict(n),
+            "config": config_dict(n, args.gpus),
             "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "step_values": vals, "stages_s": base["stages_s"], "truncated_shells": base["truncated_shells"],
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -372,8 +372,7 @@ def run_ours(args, dist: Dist):
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, compensated-f32 shell sums, f64 collapse walk",
             "data": "synthetic (seeded Threefry noise, EH P(k))",
-            "config": {**config_dict(n, "plain" if args.plain else "optimised"),
-                       "parallelism": f"replicas x{dist.world}"},
+            "config": config_dict(n, dist.world, "plain" if args.plain else "optimised"),
             "peaks_per_s": npk_tot / (dev_ms / 1000.0), "halos_per_tile": nh_tot / args.steps,
             "peaks_per_tile": npk_tot / args.steps,
             "stage_ms_last_step": stage,
