@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define PPB_ABI_VERSION 4
+#define PPB_ABI_VERSION 5
 
 enum {
   PPB_OK = 0,
@@ -492,6 +492,13 @@ int32_t ppb_last_table_stats(ppb_ctx* ctx, float* ms, int64_t* steps);
  *                     and a radix sort after the gather), 0 list order, -1
  *                     (default) the tuner's choice (list order for batches
  *                     below PPB_OPT_TUNE_MIN_PEAKS).  Same records.
+ *  PPB_OPT_GATHER_TEX  1: the shell gather fetches its records through a
+ *                     texture object over the record array (the texture
+ *                     pipe, beside the load/store pipe; grids with 2 n^3
+ *                     float4 within the device's linear-texture limit);
+ *                     0: 256-bit loads; -1 (default): the tuner times both
+ *                     and keeps the faster (the texture pipe for batches it
+ *                     does not tune).  Same records.
  *  PPB_OPT_GATHER_RING  1: the shell gather stages its records through
  *                     per-lane shared-memory rings filled by TMA
  *                     (tile::gather4 bulk tensor copies, two stages, bounded
@@ -517,6 +524,7 @@ enum {
   PPB_OPT_FUSED_X = 6,
   PPB_OPT_GATHER_RING = 7,
   PPB_OPT_COLLAPSE_ORDER = 8,
+  PPB_OPT_GATHER_TEX = 10,
   PPB_OPT_GRAPH_LAUNCHES = 16,
   PPB_OPT_GRAPH_INSTANTIATIONS = 17,
   PPB_OPT_GRAPH_UPDATES = 18
@@ -537,6 +545,8 @@ typedef struct ppb_tune_entry {
   float collapse_ms[4];       /* collapse kernel: 1, 2, 4 threads per peak, lane work queues (8) */
   int32_t collapse_order;     /* chosen: 1 = peaks by descending crossing shell, 0 = list order */
   float collapse_ordered_ms[4];   /* the collapse widths with that order */
+  int32_t gather_tex;         /* chosen: 1 = records through the texture pipe, 0 = 256-bit loads */
+  float gather_plain_ms;      /* the chosen order with 256-bit loads (0 when no texture was available) */
 } ppb_tune_entry;
 /* Copies up to `cap` entries; *n = the number of entries held. */
 int32_t ppb_tune_entries(ppb_ctx* ctx, ppb_tune_entry* out, int32_t cap, int32_t* n);

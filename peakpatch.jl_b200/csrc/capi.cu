@@ -54,8 +54,42 @@ void Slot::init(int dev) {
   for (auto& e : shell_ev) PPB_CUDA(cudaEventCreate(&e));
 }
 
+void Slot::drop_record_texture() {
+  if (rec_tex) cudaDestroyTextureObject(rec_tex);
+  rec_tex = 0;
+  rec_ptr = nullptr;
+  rec_bytes = 0;
+}
+
+// The record array of the gather as a texture object (linear, float4
+// elements): the gather fetches records through the texture pipe, which
+// leaves the load/store pipe to the cell lists, partials and rows.  Kept per
+// slot and rebuilt when the array changes; every kernel of the slot that used
+// the previous one has completed (run_shells ends each batch with a stream
+// synchronize).
+cudaTextureObject_t Slot::record_texture(const float4* aos, int n) {
+  const size_t elems = (size_t)2 * n * n * n;
+  if (aos == rec_ptr && elems * 16 == rec_bytes) return rec_tex;
+  drop_record_texture();
+  int lim = 0;
+  PPB_CUDA(cudaDeviceGetAttribute(&lim, cudaDevAttrMaxTexture1DLinearWidth, device));
+  rec_ptr = aos;
+  rec_bytes = elems * 16;
+  if (elems > (size_t)lim || elems >= ((size_t)1 << 31)) return 0;   // the plain-load gather
+  cudaResourceDesc rd{};
+  rd.resType = cudaResourceTypeLinear;
+  rd.res.linear.devPtr = const_cast<float4*>(aos);
+  rd.res.linear.desc = cudaCreateChannelDesc<float4>();
+  rd.res.linear.sizeInBytes = rec_bytes;
+  cudaTextureDesc td{};
+  td.readMode = cudaReadModeElementType;
+  PPB_CUDA(cudaCreateTextureObject(&rec_tex, &rd, &td, nullptr));
+  return rec_tex;
+}
+
 void Slot::release_buffers() {
   if (stream) PPB_CUDA(cudaStreamSynchronize(stream));
+  drop_record_texture();
   tiles.clear();
   tile_lru.clear();
   for (DevBuf* b : {&filt_Rf, &filt_ir2, &filt_np, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
@@ -378,6 +412,29 @@ TuneEntry ppb_ctx::tune_shells(Slot& sl, const ShellArgs& b0, bool comp, bool ad
   if (!(te.gather_ms[bi] < 0.97f * te.gather_ms[1])) bi = 1;
   static const int shift_of[5] = {2, 3, 4, 5, -1};
   te.brick_shift = shift_of[bi];
+  // the chosen order with 256-bit loads instead of the texture pipe
+  te.gather_tex = b0.rec_tex != 0;
+  te.gather_plain_ms = 0.f;
+  if (b0.rec_tex) {
+    ShellArgs bp = b0;
+    bp.rec_tex = 0;
+    float best = 1e30f;
+    for (int round = 0; round < 2; round++) {
+      PPB_CUDA(cudaMemsetAsync(sl.ctl.p, 0, kCtlBytes, s));
+      shell_order(sl, bp, te.brick_shift);
+      PPB_CUDA(cudaEventRecord(ev[0], s));
+      launch_shell_gather(L, bp, comp, adaptive, gblocks, rmap);
+      PPB_CUDA(cudaEventRecord(ev[1], s));
+      PPB_CUDA(cudaEventSynchronize(ev[1]));
+      float ms = 0.f;
+      PPB_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+      best = std::min(best, ms);
+    }
+    te.gather_plain_ms = best;
+    // a like-for-like choice of the load path (same order, same kernel
+    // otherwise): the faster unless within 1 %
+    te.gather_tex = !(best < 0.99f * te.gather_ms[bi]);
+  }
   // collapse: the size heuristic's width in list order unless another
   // (width, order) is at least 3 % faster
   const int wd = shell_collapse_width(b.npk, nsm, sl.walk_per_peak);
@@ -414,6 +471,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
                          const std::function<void()>& pre) {
   cudaStream_t stream = sl.stream;
   Launch L{stream, &sl.launches};
+  a.rec_tex = sh.gather_tex.load() != 0 ? sl.record_texture(a.aos, a.n) : 0;
   // the TMA-staged gather (records through per-lane shared-memory rings)
   // when the option asks for it and the records fit a tensor map
   alignas(64) unsigned char ring_map[128];
@@ -519,6 +577,7 @@ void ppb_ctx::run_shells(Slot& sl, ShellArgs& a, bool comp, bool adaptive, Shell
     const int fb = sh.force_brick.load(), fc = sh.force_collapse.load();
     const int fo = sh.collapse_order.load();
     const bool corder_on = fo == 1 || (fo == -1 && te.collapse_order);
+    if (sh.gather_tex.load() == -1 && !te.gather_tex) b.rec_tex = 0;
     if (fb != -2) te.brick_shift = fb;
     if (fc != 0) te.collapse_threads = fc;
     // the sub-batch as one graph: geometry, order, gather, collapse,
@@ -1080,6 +1139,10 @@ int32_t ppb_set_option(ppb_ctx* ctx, int32_t option, int64_t value) {
       PPB_REQUIRE(value >= -1 && value <= 1, "PPB_OPT_COLLAPSE_ORDER takes -1, 0 or 1");
       ctx->sh.collapse_order.store((int)value);
       break;
+    case PPB_OPT_GATHER_TEX:
+      PPB_REQUIRE(value >= -1 && value <= 1, "PPB_OPT_GATHER_TEX takes -1, 0 or 1");
+      ctx->sh.gather_tex.store((int)value);
+      break;
     default:
       throw Error{PPB_ERR_INVALID, "unknown or read-only option"};
   }
@@ -1099,6 +1162,7 @@ int32_t ppb_get_option(ppb_ctx* ctx, int32_t option, int64_t* value) {
     case PPB_OPT_FUSED_X: *value = ctx->sh.fused_x.load(); break;
     case PPB_OPT_GATHER_RING: *value = ctx->sh.gather_ring.load(); break;
     case PPB_OPT_COLLAPSE_ORDER: *value = ctx->sh.collapse_order.load(); break;
+    case PPB_OPT_GATHER_TEX: *value = ctx->sh.gather_tex.load(); break;
     case PPB_OPT_GRAPH_LAUNCHES:
     case PPB_OPT_GRAPH_INSTANTIATIONS:
     case PPB_OPT_GRAPH_UPDATES: {
@@ -1135,6 +1199,8 @@ int32_t ppb_tune_entries(ppb_ctx* ctx, ppb_tune_entry* out, int32_t cap, int32_t
     std::memcpy(e.gather_ms, kv.second.gather_ms, sizeof(e.gather_ms));
     std::memcpy(e.collapse_ms, kv.second.collapse_ms, sizeof(e.collapse_ms));
     e.collapse_order = kv.second.collapse_order ? 1 : 0;
+    e.gather_tex = kv.second.gather_tex ? 1 : 0;
+    e.gather_plain_ms = kv.second.gather_plain_ms;
     std::memcpy(e.collapse_ordered_ms, kv.second.collapse_ordered_ms, sizeof(e.collapse_ordered_ms));
     out[i++] = e;
   }

@@ -297,12 +297,16 @@ __device__ __forceinline__ float small_int_float(int d) {
   return __fsub_rn(__int_as_float(0x4B400000 + d), 12582912.0f);
 }
 
+// where the gather's records come from: 256-bit loads, the texture pipe
+// (a texture object over the record array), or the TMA-staged rings
+enum RecordSource { SRC_LDG = 0, SRC_TEX = 1, SRC_RING = 2 };
+
 // Visit the cells of one chunk (ck_n cells of chunk ck of the schedule),
 // four at a time: the offsets of four cells come packed in one 16-byte load
 // of the chunk-major cell list (loaded one step ahead) and their 32-byte
 // records are in flight together.  cell(h0, h1, di, dj, dk) receives each
 // in-grid cell; returns their number.
-template <class F>
+template <int SRC, class F>
 __device__ __forceinline__ int visit_chunk(const ShellArgs& a, int ck, int cnt, int64_t lin, bool inside, int pi,
                                            int pj, int pk, F&& cell) {
   const int n = a.n, n2 = a.n * a.n;   // n <= 4096: every offset fits 32 bits
@@ -327,7 +331,14 @@ __device__ __forceinline__ int visit_chunk(const ShellArgs& a, int ck, int cnt, 
       ok[u] = in;
       // cells past the chunk or off the grid read the peak cell and are skipped
       const int off = d[u][0] + n * d[u][1] + n2 * d[u][2];
-      ldg_record(aos + 2 * (lin + (in ? off : 0)), ra[u], rb[u]);
+      const int64_t cell = lin + (in ? off : 0);
+      if constexpr (SRC == SRC_TEX) {   // through the texture pipe (2 n^3 < 2^31 float4 elements)
+        const int e = 2 * (int)cell;
+        ra[u] = tex1Dfetch<float4>((cudaTextureObject_t)a.rec_tex, e);
+        rb[u] = tex1Dfetch<float4>((cudaTextureObject_t)a.rec_tex, e + 1);
+      } else {
+        ldg_record(aos + 2 * cell, ra[u], rb[u]);
+      }
     }
     if (c + 4 < cnt) wn = __ldg(cp + (c >> 2) + 1);
 #pragma unroll
@@ -536,7 +547,7 @@ __device__ __forceinline__ int visit_chunk_ring(const ShellArgs& a, Ring& R, int
 
 // the chunk's 19 sums (and its in-grid cell count) into column `col` of the
 // warp's partial table
-template <bool COMP, bool RING>
+template <bool COMP, int SRC>
 __device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, int64_t lin, bool inside, int pi,
                                          int pj, int pk, double* part, int col, Ring* ring) {
   int nsh;
@@ -562,8 +573,8 @@ __device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, in
     auto f = [&](const float4& h0, const float4& h1, float di, float dj, float dk) {
       accumulate_cell_comp(A, h0, h1, di, dj, dk);
     };
-    if constexpr (RING) nsh = visit_chunk_ring(a, *ring, ck, cnt, (int)lin, inside, pi, pj, pk, f);
-    else nsh = visit_chunk(a, ck, cnt, lin, inside, pi, pj, pk, f);
+    if constexpr (SRC == SRC_RING) nsh = visit_chunk_ring(a, *ring, ck, cnt, (int)lin, inside, pi, pj, pk, f);
+    else nsh = visit_chunk<SRC>(a, ck, cnt, lin, inside, pi, pj, pk, f);
     part[0 * 32 + col] = A.X(0);
     part[1 * 32 + col] = A.X(1);
     part[2 * 32 + col] = A.Y(1);
@@ -589,8 +600,8 @@ __device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, in
     auto f = [&](const float4& h0, const float4& h1, float di, float dj, float dk) {
       accumulate_cell(A, h0, h1, di, dj, dk);
     };
-    if constexpr (RING) nsh = visit_chunk_ring(a, *ring, ck, cnt, (int)lin, inside, pi, pj, pk, f);
-    else nsh = visit_chunk(a, ck, cnt, lin, inside, pi, pj, pk, f);
+    if constexpr (SRC == SRC_RING) nsh = visit_chunk_ring(a, *ring, ck, cnt, (int)lin, inside, pi, pj, pk, f);
+    else nsh = visit_chunk<SRC>(a, ck, cnt, lin, inside, pi, pj, pk, f);
 #pragma unroll
     for (int v = 0; v < NACC; v++) part[v * 32 + col] = A.get(v);
   }
@@ -598,7 +609,7 @@ __device__ __forceinline__ int sum_chunk(const ShellArgs& a, int ck, int cnt, in
   return nsh;
 }
 
-template <bool COMP, bool ADAPTIVE, bool RING>
+template <bool COMP, bool ADAPTIVE, int SRC>
 __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double* part, Ring* ring) {
   const int lane = threadIdx.x & 31;
   PeakHdr* hdr = a.hdr + p;
@@ -660,7 +671,7 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
     // (a) lane l sums chunk c0g + l into the shared partial table
     if (lane < ncg) {
       const int s0 = __ldg(a.ck_s + c0g + lane), cnt = s0 < cell_lim ? __ldg(a.ck_n + c0g + lane) : 0;
-      visits += sum_chunk<COMP, RING>(a, c0g + lane, cnt, lin, inside, pi, pj, pk, part, lane, ring);
+      visits += sum_chunk<COMP, SRC>(a, c0g + lane, cnt, lin, inside, pi, pj, pk, part, lane, ring);
     }
     __syncwarp();
     // (b) lane l finalises shell base + l from its chunks (double-precision
@@ -820,10 +831,11 @@ __device__ void gather_one(const ShellArgs& a, int64_t p, double* stage, double*
   }
 }
 
-template <bool COMP, bool ADAPTIVE>
 #ifndef PPB_GATHER_MINB
 #define PPB_GATHER_MINB 4
 #endif
+// SRC: SRC_LDG or SRC_TEX (a.rec_tex set)
+template <bool COMP, bool ADAPTIVE, int SRC>
 __global__ void __launch_bounds__(32 * kGatherWarps, PPB_GATHER_MINB) gather_kernel(ShellArgs a) {
   extern __shared__ double gsm[];
   const int lane = threadIdx.x & 31;
@@ -837,7 +849,7 @@ __global__ void __launch_bounds__(32 * kGatherWarps, PPB_GATHER_MINB) gather_ker
     q = __shfl_sync(FULL, q, 0);
     if (q >= a.npk) break;
     const int64_t p = a.order ? (int64_t)a.order[q] : (int64_t)q;
-    gather_one<COMP, ADAPTIVE, false>(a, p, stage, part, nullptr);
+    gather_one<COMP, ADAPTIVE, SRC>(a, p, stage, part, nullptr);
     __syncwarp();
   }
 }
@@ -870,7 +882,7 @@ __global__ void __launch_bounds__(32 * kGatherWarps, PPB_GATHER_MINB)
     q = __shfl_sync(FULL, q, 0);
     if (q >= a.npk) break;
     const int64_t p = a.order ? (int64_t)a.order[q] : (int64_t)q;
-    gather_one<COMP, ADAPTIVE, true>(a, p, stage, part, &R);
+    gather_one<COMP, ADAPTIVE, SRC_RING>(a, p, stage, part, &R);
     __syncwarp();
   }
   ring_drain(R);
@@ -1635,9 +1647,15 @@ int64_t shell_stage_doubles_per_warp(int nshell) { return (int64_t)ROW * (nshell
 constexpr size_t kGatherSmem = (size_t)kGatherWarps * GATHER_WARP_DOUBLES * sizeof(double);
 
 int shell_gather_blocks_per_sm(bool comp, bool adaptive) {
-  const void* f = comp ? (adaptive ? (const void*)gather_kernel<true, true> : (const void*)gather_kernel<true, false>)
-                       : (adaptive ? (const void*)gather_kernel<false, true> : (const void*)gather_kernel<false, false>);
-  PPB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGatherSmem));
+  const void* fs[2][2][2] = {
+      {{(const void*)gather_kernel<false, false, SRC_LDG>, (const void*)gather_kernel<false, false, SRC_TEX>},
+       {(const void*)gather_kernel<false, true, SRC_LDG>, (const void*)gather_kernel<false, true, SRC_TEX>}},
+      {{(const void*)gather_kernel<true, false, SRC_LDG>, (const void*)gather_kernel<true, false, SRC_TEX>},
+       {(const void*)gather_kernel<true, true, SRC_LDG>, (const void*)gather_kernel<true, true, SRC_TEX>}}};
+  for (int t = 0; t < 2; t++)
+    PPB_CUDA(cudaFuncSetAttribute(fs[comp][adaptive][t], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kGatherSmem));
+  const void* f = fs[comp][adaptive][0];
   int b = 0;
   PPB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, f, 32 * kGatherWarps, kGatherSmem));
   return b > 0 ? b : 1;
@@ -1689,10 +1707,17 @@ void launch_shell_gather(Launch L, const ShellArgs& a, bool comp, bool adaptive,
     return;
   }
   const size_t sm = kGatherSmem;
-  if (comp && adaptive) gather_kernel<true, true><<<grid, block, sm, L.s>>>(a);
-  else if (comp) gather_kernel<true, false><<<grid, block, sm, L.s>>>(a);
-  else if (adaptive) gather_kernel<false, true><<<grid, block, sm, L.s>>>(a);
-  else gather_kernel<false, false><<<grid, block, sm, L.s>>>(a);
+  if (a.rec_tex) {
+    if (comp && adaptive) gather_kernel<true, true, SRC_TEX><<<grid, block, sm, L.s>>>(a);
+    else if (comp) gather_kernel<true, false, SRC_TEX><<<grid, block, sm, L.s>>>(a);
+    else if (adaptive) gather_kernel<false, true, SRC_TEX><<<grid, block, sm, L.s>>>(a);
+    else gather_kernel<false, false, SRC_TEX><<<grid, block, sm, L.s>>>(a);
+  } else {
+    if (comp && adaptive) gather_kernel<true, true, SRC_LDG><<<grid, block, sm, L.s>>>(a);
+    else if (comp) gather_kernel<true, false, SRC_LDG><<<grid, block, sm, L.s>>>(a);
+    else if (adaptive) gather_kernel<false, true, SRC_LDG><<<grid, block, sm, L.s>>>(a);
+    else gather_kernel<false, false, SRC_LDG><<<grid, block, sm, L.s>>>(a);
+  }
   PPB_LAUNCHED(*L.count);
 }
 

@@ -70,6 +70,8 @@ struct TuneEntry {
   float collapse_ms[4] = {};  // 1, 2 and 4 threads per peak, lane queues
   bool collapse_order = false;            // peaks by descending crossing shell
   float collapse_ordered_ms[4] = {};      // the same widths with that order
+  bool gather_tex = true;                 // records through the texture pipe
+  float gather_plain_ms = 0.f;            // the chosen brick with 256-bit loads instead
 };
 
 struct ShellStats {
@@ -98,6 +100,13 @@ struct Slot {
   DevBuf filt_Rf, filt_ir2, filt_np;                // filter bank of the run
   DevBuf g_a, g_D, g_f, chi;                        // growth / chi tables of the run
   DevBuf stage, counters, ctl, hdr, geo, mlim, pool, anchors;   // shell stage
+  // the gather's texture object over a record array (rec_ptr, rec_bytes);
+  // 0 when none or when the array is past the device's linear-texture limit
+  cudaTextureObject_t rec_tex = 0;
+  const void* rec_ptr = nullptr;
+  size_t rec_bytes = 0;
+  cudaTextureObject_t record_texture(const float4* aos, int n);
+  void drop_record_texture();
   DevBuf okey, okey2, oidx, oidx2, otmp;            // spatial gather order
   DevBuf tcen, tcount, t_aos, t_lapd;               // multi-tile: centres, peaks per tile, tile fields
   std::unique_ptr<IsoRes> iso;                      // multi-resolution: isolated convolution
@@ -181,6 +190,7 @@ struct Shared {
   std::atomic<int> fused_x{-1};   // PPB_OPT_FUSED_X
   std::atomic<int> gather_ring{0};   // PPB_OPT_GATHER_RING
   std::atomic<int> collapse_order{-1};   // PPB_OPT_COLLAPSE_ORDER (-1: tuner's choice)
+  std::atomic<int> gather_tex{-1};       // PPB_OPT_GATHER_TEX (-1: tuner's choice)
   std::atomic<int64_t> tune_min_peaks{16384};
   std::atomic<int> force_brick{-2};      // -2: tuner's choice
   std::atomic<int> force_collapse{0};    // 0: tuner's choice

@@ -231,6 +231,7 @@ struct ShellArgs {
   int nck;                  // chunks of the schedule
   const int32_t* ck_d;      // per chunk: largest |offset component| of its cells
   float2* ck_K;             // per chunk: the compensated sums' anchors (kAnchorStride float2)
+  unsigned long long rec_tex;   // texture object over aos (float4 elements), 0: plain loads
   const unsigned* fmax;     // the field maxima after the records (pack_fmax)
   DevTable tab;
   const double* akk;        // 1101-entry SPH kernel table

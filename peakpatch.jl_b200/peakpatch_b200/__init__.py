@@ -87,7 +87,8 @@ class _TuneEntry(ctypes.Structure):
                 ("adaptive", ctypes.c_int32), ("limited", ctypes.c_int32), ("brick_shift", ctypes.c_int32),
                 ("collapse_threads", ctypes.c_int32), ("long_walk", ctypes.c_int32), ("npk", ctypes.c_int64),
                 ("gather_ms", ctypes.c_float * 5), ("collapse_ms", ctypes.c_float * 4),
-                ("collapse_order", ctypes.c_int32), ("collapse_ordered_ms", ctypes.c_float * 4)]
+                ("collapse_order", ctypes.c_int32), ("collapse_ordered_ms", ctypes.c_float * 4),
+                ("gather_tex", ctypes.c_int32), ("gather_plain_ms", ctypes.c_float)]
 
 
 # context options (include/ppb.h)
@@ -95,6 +96,7 @@ OPT_GRAPHS, OPT_AUTOTUNE, OPT_TUNE_MIN_PEAKS, OPT_BRICK_SHIFT, OPT_COLLAPSE_THRE
 OPT_FUSED_X = 6
 OPT_GATHER_RING = 7
 OPT_COLLAPSE_ORDER = 8
+OPT_GATHER_TEX = 10
 OPT_GRAPH_LAUNCHES, OPT_GRAPH_INSTANTIATIONS, OPT_GRAPH_UPDATES = 16, 17, 18
 
 
@@ -508,7 +510,8 @@ class Context:
                         "collapse_ms": dict(zip(("w1", "w2", "w4", "queue"), [round(x, 4) for x in e.collapse_ms])),
                         "collapse_order": bool(e.collapse_order),
                         "collapse_ordered_ms": dict(zip(("w1", "w2", "w4", "queue"),
-                                                        [round(x, 4) for x in e.collapse_ordered_ms]))})
+                                                        [round(x, 4) for x in e.collapse_ordered_ms])),
+                        "gather_tex": bool(e.gather_tex), "gather_plain_ms": round(e.gather_plain_ms, 4)})
         return out
 
     def stage_ms(self):

@@ -30,6 +30,7 @@ def _defaults(c):
     c.set_option(pp.OPT_COLLAPSE_THREADS, 0)
     c.set_option(pp.OPT_TUNE_MIN_PEAKS, 16384)
     c.set_option(pp.OPT_COLLAPSE_ORDER, -1)
+    c.set_option(pp.OPT_GATHER_TEX, -1)
 
 
 def test_graphs_on_and_off_give_the_same_records(tctx):
@@ -133,3 +134,21 @@ def test_collapse_order_gives_the_same_records(tctx):
         tctx.set_option(pp.OPT_COLLAPSE_ORDER, -1)
         tctx.set_option(pp.OPT_COLLAPSE_THREADS, 0)
     assert len(ref) > 100
+
+
+def test_texture_and_plain_record_loads_give_the_same_records(tctx):
+    """The gather's records fetched through the texture pipe (the default) or
+    with 256-bit loads: byte-identical records, tile and multi-tile."""
+    _defaults(tctx)
+    cfg = tile_config()
+    try:
+        tctx.set_option(pp.OPT_GATHER_TEX, 0)
+        a, _, _ = tctx.run_tile_arrays(cfg, 71, RF)
+        m0, _, _ = tctx.run_multitile_arrays(cfg, 5, RF, ntile=2, tiles=[(1, 1, 1), (2, 2, 1)])
+        tctx.set_option(pp.OPT_GATHER_TEX, 1)
+        b, _, _ = tctx.run_tile_arrays(cfg, 71, RF)
+        m1, _, _ = tctx.run_multitile_arrays(cfg, 5, RF, ntile=2, tiles=[(1, 1, 1), (2, 2, 1)])
+        assert tctx.get_option(pp.OPT_GATHER_TEX) == 1
+    finally:
+        tctx.set_option(pp.OPT_GATHER_TEX, -1)
+    assert len(a) > 100 and a.tobytes() == b.tobytes() and m0.tobytes() == m1.tobytes()

@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert pp.load_library().ppb_abi_version() == 4
+    assert pp.load_library().ppb_abi_version() == 5
 
 
 def test_tile_params_layout_matches_the_header():
@@ -40,8 +40,8 @@ def test_tile_params_layout_matches_the_header():
 
 
 def test_tune_entry_layout_and_option_entry_points():
-    # ppb_tune_entry: 8 int32, an int64, 5 + 4 floats, an int32, 4 floats
-    assert ctypes.sizeof(pp._TuneEntry) == 8 * 4 + 8 + 9 * 4 + 4 + 4 * 4
+    # ppb_tune_entry: 8 int32, an int64, 5 + 4 floats, an int32, 4 floats, an int32, a float
+    assert ctypes.sizeof(pp._TuneEntry) == 8 * 4 + 8 + 9 * 4 + 4 + 4 * 4 + 8
     assert pp._TuneEntry.gather_ms.offset == 40
     assert pp._TuneEntry.collapse_order.offset == 76 and pp._TuneEntry.collapse_ordered_ms.offset == 80
     L = pp.load_library()
