@@ -915,6 +915,8 @@ def _apply_options(ctx, args):
         ctx.set_option(pp.OPT_COLLAPSE_THREADS, args.collapse)
     if getattr(args, "gather_ring", -1) >= 0:
         ctx.set_option(pp.OPT_GATHER_RING, args.gather_ring)
+    if getattr(args, "gather_tex", -2) >= -1:
+        ctx.set_option(pp.OPT_GATHER_TEX, args.gather_tex)
     if getattr(args, "collapse_order", -1) >= 0:
         ctx.set_option(pp.OPT_COLLAPSE_ORDER, args.collapse_order)
 
@@ -952,6 +954,8 @@ def main():
     ap.add_argument("--split-n", type=int, default=192, help="nmesh of the --split workload")
     ap.add_argument("--no-graphs", action="store_true", help="launch kernels one by one instead of as CUDA graphs")
     ap.add_argument("--no-autotune", action="store_true", help="default shell-stage choices, no autotuning")
+    ap.add_argument("--gather-tex", type=int, default=-2,
+                    help="gather record loads: 1 texture pipe, 0 256-bit loads, -1 the tuner's choice (default: library)")
     ap.add_argument("--gather-ring", type=int, default=-1,
                     help="1: gather records through TMA-staged shared-memory rings, 0: plain loads (default: library)")
     ap.add_argument("--collapse-order", type=int, default=-1,
