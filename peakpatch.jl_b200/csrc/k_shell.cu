@@ -18,9 +18,11 @@
 //    chunk partials, and the cumulative profile Fbar comes from a warp scan
 //    of r^3 Fbar.  Sums are compensated single precision (anchored Fast2Sum
 //    with anchors per chunk: each rounding error is captured exactly and
-//    summed apart) on the optimised path and double precision on the plain path; in both the
-//    addends are the single-precision products the reference forms (Float32
-//    field times Int32 offset).
+//    summed apart) on the optimised path and double precision on the plain
+//    path; in both the addends are the single-precision products the
+//    reference forms (Float32 field times Int32 offset).  The records come
+//    through the texture pipe or as 256-bit loads (the autotuner's choice),
+//    or, as an option, through TMA-staged shared-memory rings.
 //    Adaptive truncation (optimised path): the warp stops gathering once
 //    every shell later read is in, i.e. all shells up to rad[M] + 2 with
 //    M = max(crossing shell, first shell beyond ir2min, Rf window):
