@@ -168,14 +168,16 @@ def config2(ora, eh_pk, julia_table):
     return cfg, st, sample
 
 
-def test_run_tile_config2_vs_oracle(ctx, config2, eh_pk, julia_table):
+@pytest.mark.parametrize("plain", [False, True])
+def test_run_tile_config2_vs_oracle(ctx, config2, eh_pk, julia_table, plain):
     """The benchmark tile through the default path (fused x pass + peak
-    search at 384^3) against the oracle on a 24,000-peak sample."""
+    search at 384^3) and through the plain path (full spheres, FP64 sums,
+    full 3-D transforms) against the oracle on a 24,000-peak sample."""
     cfg, st, sample = config2
-    rec, rthlmax, npk = _run(ctx, eh_pk, julia_table, cfg, 7, [f[2] for f in filter_bank()])
+    rec, rthlmax, npk = _run(ctx, eh_pk, julia_table, cfg, 7, [f[2] for f in filter_bank()], plain=plain)
     nko = len(st["peaks"]["ipp"])
     m = match_tile(rec, st, sample)
-    print(f"config 2: peaks {npk} / {nko}, {m}")
+    print(f"config 2 {'plain' if plain else 'optimised'}: peaks {npk} / {nko}, {m}")
     assert m["halos"] > 10000
     assert abs(npk - nko) <= MISMATCH * nko, (npk, nko)
     assert m["frac"] <= MISMATCH, m
@@ -228,3 +230,21 @@ def test_reference_example_config(ctx, ora, tmp_path):
     assert m["errs"].get("RTHL", 0.0) <= RTOL
     r2, rthlmax, zo = pp.read_pksc(cfg.fileout)
     assert r2.tobytes() == rec.tobytes() and zo == 0.0
+
+
+def test_config2_record_load_paths_agree(ctx, eh_pk, julia_table):
+    """The benchmark tile's records are the same byte for byte whichever way
+    the gather loads them: the texture pipe, 256-bit loads, or the TMA-staged
+    shared-memory rings."""
+    cfg = bench_config(384, 768.0)
+    out = []
+    try:
+        for tex, ring in ((1, 0), (0, 0), (-1, 1)):
+            ctx.set_option(pp.OPT_GATHER_TEX, tex)
+            ctx.set_option(pp.OPT_GATHER_RING, ring)
+            out.append(_run(ctx, eh_pk, julia_table, cfg, 7, [f[2] for f in filter_bank()])[0])
+    finally:
+        ctx.set_option(pp.OPT_GATHER_TEX, -1)
+        ctx.set_option(pp.OPT_GATHER_RING, 0)
+    assert len(out[0]) > 500000
+    assert out[0].tobytes() == out[1].tobytes() == out[2].tobytes()
