@@ -154,9 +154,12 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 def config_dict(n: int, world: int, path: str = "optimised") -> dict:
     """The workload's config, the same in both arms."""
+    ws = 92 * n ** 3   # fields 8 x 4 B, spectra about 7 x 4 B, records 32 B per cell
     return {"workload": workload_name(n), "nmesh": n, "boxsize": BOX_PER_CELL * n, "filters": 20, "nbuff": 32,
             "ilpt": 2, "ioutshear": 1, "seed": SEED, "path": path,
-            "l2": "inputs larger than L2 (each field 226 MB at 384^3)", "parallelism": f"replicas x{world}"}
+            "l2": f"inputs larger than L2: each tile rewrites its fields ({4 * n ** 3 / 1e6:.0f} MB each), spectra "
+                  f"and records, about {ws / 1e9:.2f} GB against 126 MB of L2",
+            "parallelism": f"replicas x{world}"}
 
 
 class CpuTile:
@@ -889,10 +892,26 @@ def run_table_bench(args, dist: Dist):
 
 
 def _default_extras(args, dist: Dist) -> dict:
-    """The batched shell kernel of 10^6 peaks on a 512^3 field and a shortened
-    serving stream (60 Poisson requests at 4/s), run after the tile benchmark
-    in the default invocation so that one line carries their numbers."""
+    """The batched shell kernel of 10^6 peaks on a 512^3 field, a shortened
+    serving stream (60 Poisson requests at 4/s), the 128^3 tile (config 1,
+    with its CPU figure) and the lightcone chain (config 4), run after the
+    tile benchmark in the default invocation so that one line carries their
+    numbers."""
     out = {}
+    c1 = argparse.Namespace(**vars(args))
+    c1.n, c1.steps, c1.warmup, c1.plain = 128, 20, 3, False
+    l1 = run_ours(c1, dist)
+    cb1 = cpu_baseline(128, budget_s=3.0)
+    out["config1"] = {"metric": METRIC, "value": l1["value"], "unit": METRIC, "config": l1["config"],
+                      "e2e": l1["e2e"], "roofline_frac": l1["roofline"]["frac"],
+                      "halos_per_tile": l1.get("halos_per_tile"),
+                      "cpu_baseline": {k: cb1[k] for k in ("value", "unit", "cores", "kind", "sample")}}
+    c4 = argparse.Namespace(**vars(args))
+    c4.steps, c4.warmup = 3, 3
+    l4 = run_lightcone(c4, dist)
+    out["config4_lightcone"] = {k: l4[k] for k in ("metric", "value", "unit", "config", "ms_per_step") if k in l4}
+    out["config4_lightcone"].update({k: l4[k] for k in ("multitile_ms", "merge_ms", "halos", "halos_after_merge")
+                                     if k in l4})
     a = argparse.Namespace(**vars(args))
     sh = run_shells_bench(a, dist)
     out["shells_batched"] = {k: sh[k] for k in ("metric", "value", "unit", "config", "roofline",
