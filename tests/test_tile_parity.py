@@ -149,9 +149,9 @@ def test_run_tile_config1_vs_oracle(ctx, config1, eh_pk, julia_table, plain):
 
 
 # ------------------------------------------------------------------ config 2
-@pytest.fixture(scope="module")
-def config2(ora, eh_pk, julia_table):
-    cfg = bench_config(384, 768.0)
+def _config2_sample(ora, eh_pk, julia_table, cfg):
+    """The oracle's run_tile stages at 384^3 with analyse_peak on a fixed
+    sample of 24,000 peaks (the same sample every run)."""
     # the same sample every run: 24,000 of the oracle's peaks
     probe = ora.run_tile_stages(ora_config(ora, cfg), 7, *eh_pk, filter_bank(), julia_table,
                                 peak_sample=np.arange(0))
@@ -159,13 +159,18 @@ def config2(ora, eh_pk, julia_table):
     sample = np.sort(np.random.default_rng(2024).choice(npk, size=min(24000, npk), replace=False))
     res = ora.analyse_peaks(probe["fields"], probe["peaks"]["ipp"][sample], probe["Rf"][sample],
                             probe["ir2min"][sample], probe["ZZon"][sample], probe["fcrit"], probe["alatt"],
-                            probe["shells"], julia_table, nbuff=cfg.nbuff)
+                            probe["shells"], julia_table, nbuff=cfg.nbuff, rmax2rs=cfg.rmax2rs)
     full = np.zeros((npk, res.shape[1]))
     full[:, 0] = -1.0
     full[sample] = res
     st = dict(probe, results=full, records=ora.pack_records(ora_config(ora, cfg), probe, full))
     del st["fields"], st["delta_k"]
     return cfg, st, sample
+
+
+@pytest.fixture(scope="module")
+def config2(ora, eh_pk, julia_table):
+    return _config2_sample(ora, eh_pk, julia_table, bench_config(384, 768.0))
 
 
 @pytest.mark.parametrize("plain", [False, True])
@@ -180,6 +185,19 @@ def test_run_tile_config2_vs_oracle(ctx, config2, eh_pk, julia_table, plain):
     print(f"config 2 {'plain' if plain else 'optimised'}: peaks {npk} / {nko}, {m}")
     assert m["halos"] > 10000
     assert abs(npk - nko) <= MISMATCH * nko, (npk, nko)
+    assert m["frac"] <= MISMATCH, m
+    assert m["errs"]["RTHL"] <= RTOL
+
+
+def test_run_tile_config2_rmax2rs_vs_oracle(ctx, ora, eh_pk, julia_table):
+    """The benchmark tile with the reference's default rmax2rs = 1 (each
+    peak's shell list cut at npart cells) against the oracle on the same
+    24,000-peak sample."""
+    cfg, st, sample = _config2_sample(ora, eh_pk, julia_table, bench_config(384, 768.0, rmax2rs=1.0))
+    rec, _, npk = _run(ctx, eh_pk, julia_table, cfg, 7, [f[2] for f in filter_bank()])
+    m = match_tile(rec, st, sample)
+    print(f"config 2 rmax2rs 1: peaks {npk}, {m}")
+    assert m["halos"] > 2000
     assert m["frac"] <= MISMATCH, m
     assert m["errs"]["RTHL"] <= RTOL
 
