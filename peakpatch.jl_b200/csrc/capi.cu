@@ -90,6 +90,7 @@ cudaTextureObject_t Slot::record_texture(const float4* aos, int n) {
 void Slot::release_buffers() {
   if (stream) PPB_CUDA(cudaStreamSynchronize(stream));
   drop_record_texture();
+  merge.release();
   tiles.clear();
   tile_lru.clear();
   for (DevBuf* b : {&filt_Rf, &filt_ir2, &filt_np, &g_a, &g_D, &g_f, &chi, &stage, &counters, &ctl, &hdr, &geo, &pool, &okey,
@@ -101,7 +102,7 @@ void Slot::release_buffers() {
 }
 
 size_t Slot::bytes_held() const {
-  size_t b = shell_bytes();
+  size_t b = shell_bytes() + merge.bytes();
   for (const auto& t : tiles) b += t.second->bytes();
   return b;
 }
@@ -965,13 +966,12 @@ int32_t ppb_merge_catalog(ppb_ctx* ctx, const float* records, int64_t n, int32_t
   *n_out = 0;
   if (n == 0) return PPB_OK;
   Slot& sl = ctx->sync;
-  DevBuf din, dout;
   const size_t bytes = (size_t)n * nfields * 4;
-  const float* d_rec = (const float*)stage_in(din, records, bytes, sl.stream);
+  const float* d_rec = (const float*)stage_in(sl.merge.in, records, bytes, sl.stream);
   float* d_out = out;
   if (!is_device_ptr(out)) {
-    dout.ensure(bytes);
-    d_out = dout.as<float>();
+    sl.merge.out.ensure(bytes);
+    d_out = sl.merge.out.as<float>();
   }
   const int64_t m = merge_catalog_device(sl, d_rec, n, nfields, d_out);
   if (m > 0 && d_out != out) copy_out(out, d_out, (size_t)m * nfields * 4, sl.stream);

@@ -9,9 +9,10 @@
 //    dies when nothing is left.
 // Pass 1 is a greedy suppression: halo i survives iff no surviving halo
 // earlier in the order (stable by index among equal radii) has i within its
-// radius.  Here each halo first collects its suppressors (earlier halos with
-// i inside their radius) from a 256^3-cell grid over the padded domain (the
-// reference's spatial hash), and the survivals are resolved in rounds: a
+// radius.  Here each halo first writes itself into the suppressor lists of
+// the later halos inside its radius, found in a 256^3-cell grid over the
+// padded domain (the reference's spatial hash), and the survivals are
+// resolved in rounds: a
 // halo with a surviving suppressor dies, one whose suppressors are all dead
 // survives.  The fixed point is the sequential result.  Pass 2 is a gather
 // per survivor; its sums add the same terms as the reference (each pair's
@@ -47,7 +48,6 @@ struct MergeArgs {
   int* rank;         // position in the order
   int* scount;       // suppressors per halo, then offsets (n + 1)
   int* sups;         // suppressor lists
-  int dsup;          // cell radius of the suppressor search
   unsigned char* state;   // 0 undecided, 1 alive, 2 dead
   int* changed;
   double rmax;
@@ -106,19 +106,22 @@ __global__ void rank_kernel(const int* order, int64_t n, int* rank) {
   if (q < n) rank[order[q]] = (int)q;
 }
 
-// suppressors of halo i: halos k earlier in the order with |x_i - x_k| < r_k;
-// with fill = false only counts them
-template <bool FILL>
-__global__ void suppressor_kernel(MergeArgs a) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n) return;
-  const double xi = a.x[i], yi = a.y[i], zi = a.z[i];
-  const int ri = a.rank[i];
-  const int c = a.cell[i];
+// suppressors of halo i: halos k earlier in the order with |x_i - x_k| < r_k,
+// found from k's side — each halo scans the cells within its own radius
+// (most radii are a cell or less, where a search within the largest radius
+// from every i scanned 9^3 cells).  COUNT: per-i counts; else each k writes
+// itself into the lists of the halos it suppresses (list order does not
+// matter: the rounds only ask whether any suppressor survives and whether
+// all are dead)
+template <bool COUNT>
+__global__ void suppress_out_kernel(MergeArgs a, int* cursor) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.n) return;
+  const double xk = a.x[k], yk = a.y[k], zk = a.z[k], rk = a.r[k];
+  const int rank_k = a.rank[k];
+  const int c = a.cell[k];
   const int cx = c % NC, cy = (c / NC) % NC, cz = c / (NC * NC);
-  const int D = a.dsup;
-  int cnt = 0;
-  int* out = FILL ? a.sups + a.scount[i] : nullptr;
+  const int D = (int)ceil(rk / a.cs);
   for (int dz = -D; dz <= D; dz++) {
     const int jz = cz + dz;
     if (jz < 0 || jz >= NC) continue;
@@ -130,19 +133,40 @@ __global__ void suppressor_kernel(MergeArgs a) {
         if (jx < 0 || jx >= NC) continue;
         const int cc = jx + NC * (jy + NC * jz);
         for (int q = a.cstart[cc]; q < a.cstart[cc + 1]; q++) {
-          const int k = a.cidx[q];
-          if (a.rank[k] >= ri) continue;
+          const int i = a.cidx[q];
+          if (a.rank[i] <= rank_k) continue;
           // the reference's test, from k's side: dx = x_i - x_k (Exclusion.jl:129-133)
-          const double dist = norm3(xi - a.x[k], yi - a.y[k], zi - a.z[k]);
-          if (dist < a.r[k]) {
-            if (FILL) out[cnt] = k;
-            cnt++;
+          const double dist = norm3(a.x[i] - xk, a.y[i] - yk, a.z[i] - zk);
+          if (dist < rk) {
+            if (COUNT) atomicAdd(a.scount + i, 1);
+            else a.sups[a.scount[i] + atomicAdd(cursor + i, 1)] = (int)k;
           }
         }
       }
     }
   }
-  if (!FILL) a.scount[i] = cnt;
+}
+
+// domain of the catalogue: per block the smallest and largest x, y, z and the
+// largest radius (7 doubles), finished on the host
+__global__ void domain_kernel(MergeArgs a, double* part) {
+  __shared__ double sm[7][256];
+  double v[7] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY, -INFINITY};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double x = a.x[i], y = a.y[i], z = a.z[i], r = a.r[i];
+    v[0] = fmin(v[0], x); v[1] = fmin(v[1], y); v[2] = fmin(v[2], z);
+    v[3] = fmax(v[3], x); v[4] = fmax(v[4], y); v[5] = fmax(v[5], z); v[6] = fmax(v[6], r);
+  }
+  for (int q = 0; q < 7; q++) sm[q][threadIdx.x] = v[q];
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h)
+      for (int q = 0; q < 7; q++)
+        sm[q][threadIdx.x] = q < 3 ? fmin(sm[q][threadIdx.x], sm[q][threadIdx.x + h])
+                                   : fmax(sm[q][threadIdx.x], sm[q][threadIdx.x + h]);
+    __syncthreads();
+  }
+  if (threadIdx.x < 7) part[blockIdx.x * 7 + threadIdx.x] = sm[threadIdx.x][0];
 }
 
 __global__ void resolve_kernel(MergeArgs a) {
@@ -234,10 +258,7 @@ int64_t merge_catalog_device(Slot& sl, const float* d_rec, int64_t n, int nf, fl
   PPB_REQUIRE(n < (1ll << 31), "catalogue too large");
   cudaStream_t s = sl.stream;
   Launch L{s, &sl.launches};
-  struct Bufs {
-    DevBuf x, y, z, r, cell, cstart, cfill, cidx, rank, scount, sups, state, changed, rnew, key, key2, idx, idx2, tmp,
-        flag, off;
-  } b;
+  Slot::MergeBufs& b = sl.merge;
   b.x.ensure(n * 8); b.y.ensure(n * 8); b.z.ensure(n * 8); b.r.ensure(n * 8);
   b.cell.ensure(n * 4);
   const size_t ncell = (size_t)NC * NC * NC;
@@ -269,19 +290,22 @@ int64_t merge_catalog_device(Slot& sl, const float* d_rec, int64_t n, int nf, fl
   const unsigned g = (unsigned)((n + 255) / 256);
   load_kernel<<<g, 256, 0, s>>>(a);
   PPB_LAUNCHED(sl.launches);
-  // domain and largest radius (Merger.jl:43-50)
-  std::vector<double> hx(n), hy(n), hz(n), hr(n);
-  PPB_CUDA(cudaMemcpyAsync(hx.data(), a.x, n * 8, cudaMemcpyDeviceToHost, s));
-  PPB_CUDA(cudaMemcpyAsync(hy.data(), a.y, n * 8, cudaMemcpyDeviceToHost, s));
-  PPB_CUDA(cudaMemcpyAsync(hz.data(), a.z, n * 8, cudaMemcpyDeviceToHost, s));
-  PPB_CUDA(cudaMemcpyAsync(hr.data(), a.r, n * 8, cudaMemcpyDeviceToHost, s));
+  // domain and largest radius (Merger.jl:43-50): block partials on the
+  // device, the last step on the host (min and max are exact in any order)
+  const int nblk = (int)std::min<int64_t>(1184, (n + 255) / 256);
+  b.dom.ensure((size_t)nblk * 7 * 8);
+  domain_kernel<<<nblk, 256, 0, s>>>(a, b.dom.as<double>());
+  PPB_LAUNCHED(sl.launches);
+  std::vector<double> hp((size_t)nblk * 7);
+  PPB_CUDA(cudaMemcpyAsync(hp.data(), b.dom.p, hp.size() * 8, cudaMemcpyDeviceToHost, s));
   PPB_CUDA(cudaStreamSynchronize(s));
-  double mn[3] = {hx[0], hy[0], hz[0]}, mx[3] = {hx[0], hy[0], hz[0]}, rmax = hr[0];
-  for (int64_t i = 1; i < n; i++) {
-    mn[0] = std::min(mn[0], hx[i]); mx[0] = std::max(mx[0], hx[i]);
-    mn[1] = std::min(mn[1], hy[i]); mx[1] = std::max(mx[1], hy[i]);
-    mn[2] = std::min(mn[2], hz[i]); mx[2] = std::max(mx[2], hz[i]);
-    rmax = std::max(rmax, hr[i]);
+  double mn[3] = {hp[0], hp[1], hp[2]}, mx[3] = {hp[3], hp[4], hp[5]}, rmax = hp[6];
+  for (int q = 1; q < nblk; q++) {
+    for (int d = 0; d < 3; d++) {
+      mn[d] = std::min(mn[d], hp[q * 7 + d]);
+      mx[d] = std::max(mx[d], hp[q * 7 + 3 + d]);
+    }
+    rmax = std::max(rmax, hp[q * 7 + 6]);
   }
   const double pad = 2.0 * rmax;
   double Lmax = 0.0;
@@ -291,7 +315,6 @@ int64_t merge_catalog_device(Slot& sl, const float* d_rec, int64_t n, int nf, fl
   }
   a.cs = Lmax / NC;
   a.rmax = rmax;
-  a.dsup = (int)std::ceil(rmax / a.cs);
   // cell lists
   PPB_CUDA(cudaMemsetAsync(b.cstart.p, 0, (ncell + 1) * 4, s));
   PPB_CUDA(cudaMemsetAsync(b.cfill.p, 0, ncell * 4, s));
@@ -318,9 +341,9 @@ int64_t merge_catalog_device(Slot& sl, const float* d_rec, int64_t n, int nf, fl
   rank_kernel<<<g, 256, 0, s>>>(b.idx2.as<int>(), n, a.rank);
   PPB_LAUNCHED(sl.launches);
   // pass 1: suppressor lists, then rounds
-  suppressor_kernel<false><<<g, 256, 0, s>>>(a);
+  PPB_CUDA(cudaMemsetAsync(a.scount, 0, (n + 1) * 4, s));
+  suppress_out_kernel<true><<<g, 256, 0, s>>>(a, nullptr);
   PPB_LAUNCHED(sl.launches);
-  PPB_CUDA(cudaMemsetAsync(a.scount + n, 0, 4, s));
   tb = b.tmp.bytes;
   PPB_CUDA(cub::DeviceScan::ExclusiveSum(b.tmp.p, tb, a.scount, a.scount, (int)(n + 1), s));
   sl.launches++;
@@ -329,7 +352,8 @@ int64_t merge_catalog_device(Slot& sl, const float* d_rec, int64_t n, int nf, fl
   PPB_CUDA(cudaStreamSynchronize(s));
   b.sups.ensure((size_t)std::max(nsup, 1) * 4);
   a.sups = b.sups.as<int>();
-  suppressor_kernel<true><<<g, 256, 0, s>>>(a);
+  PPB_CUDA(cudaMemsetAsync(b.flag.p, 0, (n + 1) * 4, s));   // list cursors
+  suppress_out_kernel<false><<<g, 256, 0, s>>>(a, b.flag.as<int>());
   PPB_LAUNCHED(sl.launches);
   PPB_CUDA(cudaMemsetAsync(a.state, 0, n, s));
   for (int64_t round = 0;; round++) {

@@ -100,6 +100,24 @@ struct Slot {
   DevBuf filt_Rf, filt_ir2, filt_np;                // filter bank of the run
   DevBuf g_a, g_D, g_f, chi;                        // growth / chi tables of the run
   DevBuf stage, counters, ctl, hdr, geo, mlim, pool, anchors;   // shell stage
+  // merge_catalog's buffers, kept between calls (a cudaFree waits for the
+  // whole device)
+  struct MergeBufs {
+    DevBuf in, out, x, y, z, r, cell, cstart, cfill, cidx, rank, scount, sups, state, changed, rnew, key, key2, idx,
+        idx2, tmp, flag, off, dom;
+    void release() {
+      for (DevBuf* b : {&in, &out, &x, &y, &z, &r, &cell, &cstart, &cfill, &cidx, &rank, &scount, &sups, &state,
+                        &changed, &rnew, &key, &key2, &idx, &idx2, &tmp, &flag, &off, &dom})
+        b->release();
+    }
+    size_t bytes() const {
+      size_t t = 0;
+      for (const DevBuf* b : {&in, &out, &x, &y, &z, &r, &cell, &cstart, &cfill, &cidx, &rank, &scount, &sups, &state,
+                              &changed, &rnew, &key, &key2, &idx, &idx2, &tmp, &flag, &off, &dom})
+        t += b->bytes;
+      return t;
+    }
+  } merge;
   // the gather's texture object over a record array (rec_ptr, rec_bytes);
   // 0 when none or when the array is past the device's linear-texture limit
   cudaTextureObject_t rec_tex = 0;
